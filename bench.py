@@ -1,0 +1,346 @@
+#!/usr/bin/env python
+"""bench.py -- time to an FP64 relative residual of 1e-10 for the plain nested
+F3R solve on one B200.
+
+Workload: the nonsymmetric 27-point stencil on a 192^3 grid (7,077,888 rows,
+189,119,224 nonzeros; diagonal 26, neighbours at a positive linear offset
+-1+beta, negative -1-beta, beta = 0.5), symmetrically diagonal-scaled as the
+reference drivers do, stored SELL-C-sigma with C = 32, sigma = 256, SDAINV
+(tol 0.1, acc 1.0) innermost, F3R(m2=8, m3=4, m4=2, c=64) under an fp64
+FGMRES(100), b = A x* with x* ~ U(-1, 1) from mt19937_64(seed = rank).
+Synthetic data (the reference publishes no dataset for this configuration).
+
+One step = one full solve from x0 = 0 to ||b - Ax|| / ||b|| < 1e-10 (the
+implicit Givens estimate, checked against the explicit fp64 residual).  With
+N GPUs every rank solves its own system (replicas, no collective on the data
+path); the time is the max over ranks.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NX = 192
+BETA = 0.5
+SIGMA = 256
+TOL = 1e-10
+PARAMS = dict(m_outer=100, max_restarts=20, m2=8, m3=4, m4=2, c=64, sdainv_tol=0.1, acc=1.0, sell_sigma=SIGMA,
+              rel_tol=TOL, use_graphs=1)
+METRIC = "time to 1e-10 FP64 relative residual, plain F3R (fp64/fp32/fp16 nested FGMRES), 192^3 27-pt nonsymmetric"
+WORKLOAD = "F3R-SDAINV-SELL32s256 stencil27-halfspace beta0.5 192^3 (n=7077888, nnz=189119224), tol 1e-10"
+
+
+def config_dict(extra=None):
+    d = {"workload": WORKLOAD, "grid": [NX, NX, NX], "n": NX ** 3, "nnz": 189119224, "sell": {"C": 32, "sigma": SIGMA},
+         "f3r": {"m_outer": 100, "m2": 8, "m3": 4, "m4": 2, "c": 64, "restarts": 20},
+         "precond": "SDAINV(tol=0.1, acc=1.0)", "rhs": "b = A x*, x* ~ U(-1,1) mt19937_64(rank)",
+         "l2": "inputs larger than L2 (fp16+fp32+fp64 matrix copies 4.6 GB, vectors 12 GB)",
+         "parallelism": "replicas (one independent system per GPU)"}
+    if extra:
+        d.update(extra)
+    return d
+
+
+def make_problem(seed: int):
+    import f3r_b200 as F
+    A = F.stencil27(NX, NX, NX, 2, BETA).scale()
+    n = A.shape[0]
+    xs = F.random_uniform(seed, -1.0, 1.0, n)
+    b = A.spmv(xs)
+    return A, b, xs
+
+
+class Clocks:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.f.read().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.f.name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """dram bytes per launch of the dominant kernel from the committed ncu summary"""
+    path = os.path.join(ROOT, "profiles", "spmv_f16_c2_traffic.txt")
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.startswith("bytes_per_launch"):
+                    return float(line.split("=")[1])
+    except (OSError, ValueError, IndexError):
+        pass
+    return None
+
+
+def spmv_roofline(ctx, A, torch, F):
+    """Dominant kernel: the fp16-matrix SELL SpMV of level 3 (fp16 values,
+    fp32 x and y), timed with CUDA events on the library's stream."""
+    n, nnz = A.shape[0], A.nnz
+    S = F.Sell(ctx, A, sigma=SIGMA, dtypes=(F.F16,))
+    x = torch.randn(n, dtype=torch.float32, device="cuda")
+    y = torch.empty_like(x)
+    for _ in range(5):
+        S.operate(x, y, val_t=F.F16)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 50
+    e0.record(torch.cuda.current_stream())
+    for _ in range(reps):
+        S.operate(x, y, val_t=F.F16)
+    e1.record(torch.cuda.current_stream())
+    torch.cuda.synchronize()
+    dt = e0.elapsed_time(e1) * 1e-3 / reps
+    S.close()
+    alg = nnz * (2 + 4) + 4 * (n + 1) + n * 4 + n * 4
+    peak, src = measured_peak()
+    achieved = alg / dt / 1e9
+    return {"kernel": "k_sell<__half,float,EpiStore<float>> (SELL-32 sigma=256, fp16 A, fp32 x, fp32 y)",
+            "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "peak_source": src, "unit": "GB/s",
+            "frac": round(achieved / peak, 4), "traffic": profiled_traffic(),
+            "algorithmic_bytes": alg, "launch_us": round(dt * 1e6, 2)}
+
+
+def cpu_baseline(A, b, iters_gpu, sample_steps=2):
+    """The reference's own CPU F3R (oracle/_ref, compiled from the reference
+    sources) on this host's cores: a bounded sample of `sample_steps` outer
+    FGMRES steps of the same solve, scaled to the outer-step count of the GPU
+    solve."""
+    cores = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    from oracle import oracle as O
+    try:
+        ref = O.Ref("fast")
+    except FileNotFoundError as e:
+        return {"value": None, "unit": "ms", "cores": cores, "kind": "reference", "sample": f"unavailable: {e}"}
+    rptr, idx, val = A.arrays()
+    r = ref.f3r_solve(0, rptr, idx, val, b, tol=TOL, stop_after=sample_steps)
+    per_step = r["time_s"] / max(r["iters"], 1)
+    return {"value": round(per_step * iters_gpu * 1e3, 1), "unit": "ms", "cores": int(os.environ["OMP_NUM_THREADS"]),
+            "kind": "reference",
+            "sample": f"{r['iters']} outer FGMRES steps of the same 192^3 solve on the host "
+                      f"({ref.name}, SELL-32 + SDAINV, fp16 as _Float16; {per_step:.2f} s/step), "
+                      f"scaled by the GPU solve's {iters_gpu} outer steps"}
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+    import f3r_b200 as F
+
+    A, b, xs = make_problem(seed=rank)
+    n = A.shape[0]
+    ctx = F.Context(local)
+    stream = torch.cuda.Stream()          # one non-default stream for torch and the library
+    torch.cuda.set_stream(stream)
+    ctx.set_stream(stream.cuda_stream)
+    solver = F.Solver(ctx, A, **PARAMS)
+    b_d = torch.from_numpy(b).cuda()
+    x_d = torch.zeros_like(b_d)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(max(args.warmup, 3)):
+        x_d.zero_()
+        r = solver.solve(b_d, x_d)
+    barrier()
+    clocks = Clocks(local)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    results = []
+    e0.record(stream)
+    for _ in range(args.steps):
+        x_d.zero_()
+        results.append(solver.solve(b_d, x_d))
+    e1.record(stream)
+    barrier()
+    ck = clocks.stop()
+    t = e0.elapsed_time(e1) * 1e-3
+    if world > 1:
+        tt = torch.tensor([t], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t = float(tt.item())
+    ms_per = t / args.steps * 1e3
+    r = results[-1]
+    err = float(torch.linalg.norm(x_d.cpu() - torch.from_numpy(xs)) / np.linalg.norm(xs))
+
+    # end to end through the public API with pinned host buffers: b and x0
+    # copied in, x copied out, every step
+    b_h = torch.from_numpy(b).pin_memory()
+    x_h = torch.zeros(n, dtype=torch.float64).pin_memory()
+    x_h.zero_()
+    solver.solve(b_h, x_h)
+    barrier()
+    w0 = time.perf_counter()
+    e0.record(stream)
+    for _ in range(args.steps):
+        x_h.zero_()
+        re = solver.solve(b_h, x_h)
+    e1.record(stream)
+    barrier()
+    t_e2e = max(e0.elapsed_time(e1) * 1e-3, 0.0)
+    wall_e2e = time.perf_counter() - w0
+    if world > 1:
+        tt = torch.tensor([wall_e2e], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        wall_e2e = float(tt.item())
+    e2e_ms = wall_e2e / args.steps * 1e3
+
+    roof = spmv_roofline(ctx, A, torch, F) if rank == 0 else None
+    cpu = cpu_baseline(A, b, r.res_iter) if (rank == 0 and world == 1 and not args.no_cpu_baseline) else None
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(ms_per, 3), "unit": "ms", "n_gpus": world, "steps": args.steps,
+            "warmup": max(args.warmup, 3), "ms_per_step": round(ms_per, 3), "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "mixed: f16 storage/f32 accumulate, f32, f64",
+            "data": "synthetic (seeded 192^3 stencil, b = A x*)",
+            "config": config_dict({"solves_per_s_all_gpus": round(world * args.steps / t, 3)}),
+            "e2e": {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": 2 * n * 8,
+                    "d2h_bytes_per_step": n * 8, "timed_with": "host wall clock around solve() on pinned buffers",
+                    "device_ms": round(t_e2e / args.steps * 1e3, 3)},
+            "gpu_launches": int(sum(x.kernel_launches for x in results)),
+            "solve": {"outer_iters": r.res_iter, "inner_applications": r.inner_applications,
+                      "impl_rel_res": r.impl_rel_res, "expl_rel_res": r.expl_rel_res, "x_rel_err": err,
+                      "restarts": r.restarts, "device_ms_per_solve": round(r.solve_seconds * 1e3, 3),
+                      "kernels_per_solve": r.kernel_launches},
+            "roofline": roof, "cpu_baseline": cpu, "clocks": ck,
+        }
+        print(json.dumps(line), flush=True)
+    solver.close()
+    ctx.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def run_reference(args):
+    """The reference's own CPU F3R (compiled in place from its sources into
+    oracle/_ref) on this host's cores, same metric and workload.  Warm-up 1 is
+    a full solve (its outer-step count is kept); every timed step is a bounded
+    sample of 1 outer step, scaled by that count.  Rank 0 only."""
+    rank = int(os.environ.get("RANK", 0))
+    if rank != 0:
+        return
+    cores = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    from oracle import oracle as O
+    try:
+        ref = O.Ref("fast")
+    except FileNotFoundError as e:
+        print(json.dumps({"impl": "reference", "unavailable": str(e)}))
+        return
+    A, b, _ = make_problem(seed=0)
+    rptr, idx, val = A.arrays()
+    full = ref.f3r_solve(0, rptr, idx, val, b, tol=TOL)
+    iters = full["iters"]
+    samples = []
+    for i in range(max(args.warmup - 1, 0) + args.steps):
+        r = ref.f3r_solve(0, rptr, idx, val, b, tol=TOL, stop_after=1)
+        if i >= max(args.warmup - 1, 0):
+            samples.append(r["time_s"] / max(r["iters"], 1))
+    per_step = statistics.mean(samples)
+    value = per_step * iters * 1e3
+    line = {"impl": "reference", "metric": METRIC, "value": round(value, 1), "unit": "ms", "n_gpus": 0,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(per_step * 1e3, 1),
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "mixed: _Float16 storage/arith, f32, f64", "data": "synthetic (seeded 192^3 stencil, b = A x*)",
+            "config": config_dict({"sell": {"C": 32, "sigma": 1}}),
+            "cpu_baseline": {"value": round(value, 1), "unit": "ms", "cores": int(os.environ["OMP_NUM_THREADS"]),
+                             "kind": "reference",
+                             "sample": f"each step = 1 outer FGMRES step of the 192^3 solve ({ref.name}); value = "
+                                       f"mean step time x {iters} outer steps of a full solve run in warm-up "
+                                       f"({full['time_s']:.2f} s measured, expl res {full['expl_res']:.2e})"},
+            "full_solve_s": round(full["time_s"], 3), "outer_iters": iters,
+            "e2e": {"value": round(value, 1), "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,272 @@
+"""f3r_b200 -- a B200-native (sm_100a) nested mixed-precision F3R solver.
+
+Python view of the C ABI (include/f3r_b200.h), used by the tests and the
+benchmark.  The compute path is the CUDA library libf3r_b200.so; there is no
+CPU fallback: every object here calls into that library and raises if it is
+missing or if no B200 is visible.
+
+Names follow the reference's solver interface (umineko-sparse/models.hpp):
+``Solver.solve(b, x, cond) -> solve_res_t``, ``Sell.operate(in, out)``,
+``Sell.compute_residual(rhs, in, res)``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from typing import Callable, Optional
+
+import numpy as np
+
+from . import _capi
+from ._capi import F16, F32, F64, PRECOND_ILU0_BJ, PRECOND_SDAINV, F3RError, check, lib
+
+__all__ = ["HostMatrix", "Context", "Sell", "Solver", "Params", "solve_res_t", "F3RError", "F64", "F32", "F16",
+           "PRECOND_SDAINV", "PRECOND_ILU0_BJ", "stencil27", "diffusion7", "random_uniform", "host_spmv"]
+
+_NP2DT = {np.dtype(np.float64): F64, np.dtype(np.float32): F32, np.dtype(np.float16): F16}
+
+
+class HostMatrix:
+    """A library-owned host CSR matrix (f3r_host_matrix)."""
+
+    def __init__(self, handle):
+        self._h = C.c_void_p(handle) if not isinstance(handle, C.c_void_p) else handle
+
+    @classmethod
+    def from_csr(cls, rptr, idx, val, ncols=None) -> "HostMatrix":
+        rptr = np.ascontiguousarray(rptr, np.int32)
+        idx = np.ascontiguousarray(idx, np.int32)
+        val = np.ascontiguousarray(val, np.float64)
+        n = len(rptr) - 1
+        v = _capi.CSR(n, ncols if ncols is not None else n, len(idx), rptr.ctypes.data_as(C.POINTER(C.c_int32)),
+                      idx.ctypes.data_as(C.POINTER(C.c_int32)), val.ctypes.data_as(C.POINTER(C.c_double)))
+        h = C.c_void_p()
+        check(lib().f3r_host_matrix_from_csr(C.byref(v), C.byref(h)))
+        return cls(h)
+
+    def view(self) -> _capi.CSR:
+        v = _capi.CSR()
+        check(lib().f3r_host_matrix_view(self._h, C.byref(v)))
+        return v
+
+    @property
+    def shape(self):
+        v = self.view()
+        return (v.nrows, v.ncols)
+
+    @property
+    def nnz(self) -> int:
+        return self.view().nnz
+
+    def arrays(self):
+        """(rptr, idx, val) as numpy copies."""
+        v = self.view()
+        rptr = np.ctypeslib.as_array(v.rptr, (v.nrows + 1,)).copy()
+        if v.nnz == 0:
+            return rptr, np.zeros(0, np.int32), np.zeros(0)
+        idx = np.ctypeslib.as_array(v.idx, (v.nnz,)).copy()
+        val = np.ctypeslib.as_array(v.val, (v.nnz,)).copy()
+        return rptr, idx, val
+
+    def scale(self) -> "HostMatrix":
+        """D^{-1/2} A D^{-1/2} in place (kmm::algorithm::scaling)."""
+        check(lib().f3r_host_scaling(self._h))
+        return self
+
+    def spmv(self, x: np.ndarray) -> np.ndarray:
+        x = np.ascontiguousarray(x, np.float64)
+        y = np.zeros(self.shape[0])
+        v = self.view()
+        check(lib().f3r_host_spmv(C.byref(v), x.ctypes.data, y.ctypes.data))
+        return y
+
+    def sdainv(self, tol=0.1, acc=1.0):
+        """(Z, W^T) with M r = Z (W^T r) (kmm::algorithm::sdainv)."""
+        z, w = C.c_void_p(), C.c_void_p()
+        v = self.view()
+        check(lib().f3r_host_sdainv(C.byref(v), tol, acc, C.byref(z), C.byref(w)))
+        return HostMatrix(z), HostMatrix(w)
+
+    def ilu0_bj(self, blocks=112, acc=1.0):
+        """(L, U) block-Jacobi ILU(0) factors."""
+        l, u = C.c_void_p(), C.c_void_p()
+        v = self.view()
+        check(lib().f3r_host_ilu0_bj(C.byref(v), blocks, acc, C.byref(l), C.byref(u)))
+        return HostMatrix(l), HostMatrix(u)
+
+    def __del__(self):
+        if getattr(self, "_h", None) is not None and _capi is not None and _capi._lib is not None:
+            _capi._lib.f3r_host_matrix_destroy(self._h)
+            self._h = None
+
+
+def stencil27(nx, ny, nz, variant=0, beta=0.5) -> HostMatrix:
+    h = C.c_void_p()
+    check(lib().f3r_problem_stencil27(nx, ny, nz, variant, beta, C.byref(h)))
+    return HostMatrix(h)
+
+
+def diffusion7(nx, ny, nz, sigma=2.5, corr_len=8.0, seed=0) -> HostMatrix:
+    h = C.c_void_p()
+    check(lib().f3r_problem_diffusion7(nx, ny, nz, sigma, corr_len, seed, C.byref(h)))
+    return HostMatrix(h)
+
+
+def random_uniform(seed: int, lo: float, hi: float, n: int) -> np.ndarray:
+    out = np.zeros(n)
+    check(lib().f3r_random_uniform(seed, lo, hi, n, out.ctypes.data))
+    return out
+
+
+def host_spmv(A: HostMatrix, x) -> np.ndarray:
+    return A.spmv(x)
+
+
+class Context:
+    """One device and one CUDA stream (f3r_context)."""
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        check(lib().f3r_context_create(device, C.byref(h)))
+        self._h = h
+        self.device = device
+
+    def set_stream(self, stream_ptr: Optional[int]) -> None:
+        check(lib().f3r_context_set_stream(self._h, C.c_void_p(stream_ptr) if stream_ptr else None))
+
+    def synchronize(self) -> None:
+        check(lib().f3r_context_synchronize(self._h))
+
+    def dot(self, x, y) -> float:
+        """<x, y> of two device tensors (torch) of the same dtype."""
+        dt = _torch_dt(x)
+        out = C.c_double()
+        check(lib().f3r_dot(self._h, dt, x.numel(), C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()), C.byref(out)))
+        return out.value
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and _capi is not None and _capi._lib is not None:
+            _capi._lib.f3r_context_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+
+def _torch_dt(t):
+    import torch
+    return {torch.float64: F64, torch.float32: F32, torch.float16: F16}[t.dtype]
+
+
+class Sell:
+    """Device SELL-32-sigma matrix (f3r_sell) -- CoefficientMatrix::operate /
+    compute_residual on device tensors."""
+
+    def __init__(self, ctx: Context, A: HostMatrix, sigma: int = 1, dtypes=(F64, F32, F16)):
+        mask = 0
+        for d in dtypes:
+            mask |= 1 << d
+        h = C.c_void_p()
+        v = A.view()
+        check(lib().f3r_sell_create(ctx._h, C.byref(v), 32, sigma, mask, C.byref(h)))
+        self._h = h
+        self.ctx = ctx
+
+    def info(self) -> _capi.SellInfo:
+        i = _capi.SellInfo()
+        check(lib().f3r_sell_info_get(self._h, C.byref(i)))
+        return i
+
+    def operate(self, x, y, val_t=None) -> None:
+        """y = A x; val_t defaults to the vector type of x (fp16 for fp16 x)."""
+        xt, yt = _torch_dt(x), _torch_dt(y)
+        vt = xt if val_t is None else val_t
+        check(lib().f3r_sell_operate(self._h, vt, xt, C.c_void_p(x.data_ptr()), yt, C.c_void_p(y.data_ptr())))
+
+    def compute_residual(self, b, x, r, val_t=None) -> None:
+        """r = b - A x."""
+        bt, xt, rt = _torch_dt(b), _torch_dt(x), _torch_dt(r)
+        vt = xt if val_t is None else val_t
+        check(lib().f3r_sell_compute_residual(self._h, vt, bt, C.c_void_p(b.data_ptr()), xt,
+                                              C.c_void_p(x.data_ptr()), rt, C.c_void_p(r.data_ptr())))
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and _capi is not None and _capi._lib is not None:
+            _capi._lib.f3r_sell_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+
+@dataclass
+class solve_res_t:
+    """Mirror of kmm::solve_res_t (umineko-sparse/models.hpp:191-200) plus the
+    explicit residual and device time."""
+    is_solved: bool
+    res_iter: int
+    res_nrm2: float
+    impl_rel_res: float
+    expl_rel_res: float
+    restarts: int
+    inner_applications: int
+    solve_seconds: float
+    kernel_launches: int
+
+
+def Params(**kw) -> _capi.Params:
+    p = _capi.Params()
+    lib().f3r_params_default(C.byref(p))
+    for k, v in kw.items():
+        if not hasattr(p, k):
+            raise KeyError(k)
+        setattr(p, k, v)
+    return p
+
+
+class Solver:
+    """The nested F3R solver (f3r_solver): Restarted(FGMRES<double>(A,
+    FGMRES<float>(A32, FGMRES<float>(A16, R)))) with R the adaptive fp16
+    Richardson over SDAINV or block-Jacobi ILU(0)."""
+
+    def __init__(self, ctx: Context, A: HostMatrix, params: Optional[_capi.Params] = None, **kw):
+        p = params if params is not None else Params(**kw)
+        h = C.c_void_p()
+        v = A.view()
+        check(lib().f3r_solver_create(ctx._h, C.byref(v), C.byref(p), C.byref(h)))
+        self._h = h
+        self.ctx = ctx
+        self.params = p
+        self.n = v.nrows
+
+    def info(self):
+        i = _capi.SellInfo()
+        d = C.c_int32()
+        check(lib().f3r_solver_info(self._h, C.byref(i), C.byref(d)))
+        return i, bool(d.value)
+
+    def solve(self, b, x, cond: Optional[Callable[[int, float], bool]] = None) -> solve_res_t:
+        """Solve A x = b.  b, x: numpy float64 arrays (x is updated in place and
+        holds the initial guess) or torch CUDA float64 tensors."""
+        def ptr(a):
+            if isinstance(a, np.ndarray):
+                if a.dtype != np.float64 or not a.flags.c_contiguous:
+                    raise TypeError("numpy vectors must be contiguous float64")
+                return a.ctypes.data
+            return a.data_ptr()
+        res = _capi.Result()
+        cb = COND_NONE if cond is None else _capi.COND_FN(lambda i, e, u: 1 if cond(i, e) else 0)
+        check(lib().f3r_solver_solve(self._h, C.c_void_p(ptr(b)), C.c_void_p(ptr(x)), cb, None, C.byref(res)))
+        return solve_res_t(bool(res.is_solved), res.res_iter, res.res_nrm2, res.impl_rel_res, res.expl_rel_res,
+                           res.restarts, res.inner_applications, res.solve_seconds, res.kernel_launches)
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and _capi is not None and _capi._lib is not None:
+            _capi._lib.f3r_solver_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+
+COND_NONE = _capi.COND_FN()

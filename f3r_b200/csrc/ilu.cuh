@@ -1,0 +1,171 @@
+// ilu.cuh -- block-Jacobi ILU(0) triangular solves on the GPU.
+//
+// The reference solves each block sequentially on one CPU thread
+// (trsv/bj.hpp:58-98).  Here every block-Jacobi block is one CTA, and inside
+// a block the rows are grouped into dependency levels (level(i) = 1 + the
+// highest level among the rows it reads); a CTA sweeps its levels in order
+// with one __syncthreads() between levels, one thread per row.  The blocks
+// never read each other's rows, so no inter-CTA synchronisation exists.
+// Arithmetic per row follows the reference's order: the forward sweep walks
+// the row's off-diagonals by increasing column, the backward sweep by
+// decreasing column (the reference's 180-degree rotated U, csr.hpp:60-86)
+// and multiplies by the fp16-rounded inverse diagonal formed in fp64
+// (CSR::inverse_last, csr.hpp:60-65).  fp16 values, fp32 accumulation.
+#pragma once
+
+#include <vector>
+
+#include "device.cuh"
+#include "internal.hpp"
+
+namespace f3r {
+
+struct RichState;
+
+struct IluTri {
+  int32_t *rptr = nullptr, *idx = nullptr;  // idx mapped to vector positions
+  __half *val = nullptr;
+  __half *dinv = nullptr;                   // upper only: fp16(1 / u_ii), by row
+  int32_t *order = nullptr;                 // rows in (block, level) order
+  int32_t *lvl_off = nullptr;               // row ranges of the levels, all blocks
+  int32_t *blk_lvl = nullptr;               // per block: first level index (nblocks + 1)
+  int32_t nlevels_max = 0;
+};
+
+template <bool UPPER>
+__global__ void k_trsv_bj(IluTri T, const int32_t *__restrict__ rowpos, const __half *__restrict__ in,
+                          __half *__restrict__ out, const __half *__restrict__ ome) {
+  const int b = blockIdx.x;
+  const int l0 = T.blk_lvl[b], l1 = T.blk_lvl[b + 1];
+  const float om = ome ? __half2float(*ome) : 1.0f;
+  for (int l = l0; l < l1; l++) {
+    const int r0 = T.lvl_off[l], r1 = T.lvl_off[l + 1];
+    for (int q = r0 + threadIdx.x; q < r1; q += blockDim.x) {
+      const int32_t i = T.order[q];
+      const int32_t p = rowpos[i];
+      float t = __half2float(in[p]);
+      if (!UPPER) {
+        const int32_t e = T.rptr[i + 1] - 1;  // last entry is the unit diagonal
+        for (int32_t j = T.rptr[i]; j < e; j++)
+          t = __fmaf_rn(-__half2float(T.val[j]), __half2float(out[T.idx[j]]), t);
+        out[p] = __float2half_rn(t);
+      } else {
+        const int32_t d = T.rptr[i];  // first entry is the diagonal
+        for (int32_t j = T.rptr[i + 1] - 1; j > d; j--)
+          t = __fmaf_rn(-__half2float(T.val[j]), __half2float(out[T.idx[j]]), t);
+        __half h = __float2half_rn(t * __half2float(T.dinv[i]));
+        if (ome) h = __float2half_rn(__half2float(h) * om);
+        out[p] = h;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+struct IluDevice {
+  IluTri L, U;
+  int32_t *rowpos = nullptr;  // original row -> vector position
+  int32_t nblocks = 0;
+  std::vector<void *> allocs;
+
+  template <typename T> cudaError_t up(T **d, const std::vector<T> &h) {
+    cudaError_t e = cudaMalloc((void **)d, sizeof(T) * std::max<size_t>(h.size(), 1));
+    if (e != cudaSuccess) return e;
+    allocs.push_back((void *)*d);
+    return cudaMemcpy(*d, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice);
+  }
+  void release() {
+    for (void *p : allocs) cudaFree(p);
+    allocs.clear();
+  }
+
+  // levels of one triangular factor inside each block-Jacobi block
+  static void levels(const HostCSR &M, bool upper, const std::vector<int32_t> &bptr, std::vector<int32_t> &order,
+                     std::vector<int32_t> &lvl_off, std::vector<int32_t> &blk_lvl, int32_t &maxlev) {
+    const int32_t n = M.n, nb = (int32_t)bptr.size() - 1;
+    std::vector<int32_t> lev(n, 0);
+    order.clear();
+    lvl_off.assign(1, 0);
+    blk_lvl.assign(1, 0);
+    maxlev = 0;
+    for (int32_t b = 0; b < nb; b++) {
+      int32_t nl = 0;
+      if (!upper) {
+        for (int32_t i = bptr[b]; i < bptr[b + 1]; i++) {
+          int32_t lv = 0;
+          for (int32_t j = M.rptr[i]; j < M.rptr[i + 1]; j++)
+            if (M.idx[j] < i) lv = std::max(lv, lev[M.idx[j]] + 1);
+          lev[i] = lv;
+          nl = std::max(nl, lv + 1);
+        }
+      } else {
+        for (int32_t i = bptr[b + 1] - 1; i >= bptr[b]; i--) {
+          int32_t lv = 0;
+          for (int32_t j = M.rptr[i]; j < M.rptr[i + 1]; j++)
+            if (M.idx[j] > i) lv = std::max(lv, lev[M.idx[j]] + 1);
+          lev[i] = lv;
+          nl = std::max(nl, lv + 1);
+        }
+      }
+      // bucket the block's rows by level
+      std::vector<int32_t> cnt(nl + 1, 0);
+      for (int32_t i = bptr[b]; i < bptr[b + 1]; i++) cnt[lev[i] + 1]++;
+      for (int32_t l = 0; l < nl; l++) cnt[l + 1] += cnt[l];
+      const size_t base = order.size();
+      order.resize(base + (bptr[b + 1] - bptr[b]));
+      std::vector<int32_t> fill(cnt.begin(), cnt.end() - 1);
+      for (int32_t i = bptr[b]; i < bptr[b + 1]; i++) order[base + fill[lev[i]]++] = i;
+      for (int32_t l = 0; l < nl; l++) lvl_off.push_back((int32_t)(base + cnt[l + 1]));
+      blk_lvl.push_back(blk_lvl.back() + nl);
+      maxlev = std::max(maxlev, nl);
+    }
+  }
+
+  Status build_tri(IluTri &T, const HostCSR &M, bool upper, const std::vector<int32_t> &bptr,
+                   const std::vector<int32_t> &pos) {
+    std::vector<int32_t> order, lvl_off, blk_lvl, idx(M.idx.size());
+    levels(M, upper, bptr, order, lvl_off, blk_lvl, T.nlevels_max);
+    for (size_t j = 0; j < M.idx.size(); j++) idx[j] = pos[M.idx[j]];
+    // fp16 values rounded once from fp64 (the reference casts CSR<double> to
+    // CSR<__half>, csr.hpp:23-25)
+    std::vector<double> v(M.val.begin(), M.val.end());
+    std::vector<double> dinv;
+    if (upper) {
+      dinv.resize(M.n);
+      for (int32_t i = 0; i < M.n; i++) dinv[i] = 1.0 / M.val[M.rptr[i]];
+    }
+    if (up(&T.rptr, M.rptr) != cudaSuccess || up(&T.idx, idx) != cudaSuccess || up(&T.order, order) != cudaSuccess ||
+        up(&T.lvl_off, lvl_off) != cudaSuccess || up(&T.blk_lvl, blk_lvl) != cudaSuccess)
+      return fail(F3R_ERROR_CUDA, "ILU upload failed");
+    F3R_TRY(to_half(&T.val, v));
+    if (upper) F3R_TRY(to_half(&T.dinv, dinv));
+    return F3R_SUCCESS;
+  }
+
+  Status to_half(__half **d, const std::vector<double> &v);
+
+  Status build(cudaStream_t, const HostCSR &Lh, const HostCSR &Uh, const std::vector<int32_t> &perm, bool permuted,
+               const std::vector<int32_t> &bptr) {
+    const int32_t n = Lh.n;
+    std::vector<int32_t> pos(n);
+    for (int32_t i = 0; i < n; i++) pos[i] = i;
+    if (permuted)
+      for (int32_t s = 0; s < n; s++) pos[perm[s]] = s;
+    nblocks = (int32_t)bptr.size() - 1;
+    if (up(&rowpos, pos) != cudaSuccess) return fail(F3R_ERROR_CUDA, "ILU upload failed");
+    F3R_TRY(build_tri(L, Lh, false, bptr, pos));
+    F3R_TRY(build_tri(U, Uh, true, bptr, pos));
+    return F3R_SUCCESS;
+  }
+
+  // out = U^-1 L^-1 x (tmp holds L^-1 x); ome (nullable) scales the result
+  Status apply(cudaStream_t st, const __half *x, __half *tmp, __half *out, const __half *ome) const {
+    k_trsv_bj<false><<<nblocks, 256, 0, st>>>(L, rowpos, x, tmp, nullptr);
+    k_trsv_bj<true><<<nblocks, 256, 0, st>>>(U, rowpos, tmp, out, ome);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(F3R_ERROR_CUDA, std::string("ILU trsv launch: ") + cudaGetErrorString(e));
+    return F3R_SUCCESS;
+  }
+};
+
+}  // namespace f3r

@@ -1,0 +1,456 @@
+// kernels.cuh -- the F3R level kernels: fused Gram-Schmidt reductions, the
+// device-resident Givens/Hessenberg update, precision casts, and the fp16
+// Richardson operator with its adaptive weights.
+#pragma once
+
+#include "sell.cuh"
+
+namespace f3r {
+
+constexpr int kMaxCols = 128;  // FGMRES basis columns per level (m + 1 <= 128)
+constexpr int kMaxDots = 16;   // dot products fused into an inner-level SpMV
+constexpr int kMaxM4 = 16;
+constexpr int kEwThreads = 256;
+
+template <typename T> struct Cols {
+  const T *p[kMaxCols];
+};
+
+// Running state of the adaptive-weight Richardson operator
+// (f3r-gpu.cpp:106-108, 224-227, 239-240, 253-254, 277-281).
+struct RichState {
+  float sum[kMaxM4];   // sum[k]: 1 + all weights computed so far (fp32, as the reference)
+  __half ome[kMaxM4];  // ome[k]: sum[k] / den rounded to fp16 (the reference's scalar<__half>)
+  float om[kMaxM4];    // weight computed by the current update call
+  int den;             // cnt / period at the last update
+};
+
+// Per-level FGMRES scalars kept on the device (gmres.hpp:61-63).
+template <typename T> struct GivensCtl {
+  T *H;           // (m+1) x m, column-major, ld = ldh
+  T *cs, *sn, *e, *y;
+  T *inv;         // 1 / h_{j+1,j}
+  double *abs_e;  // |e(j+1)| for the host's cond() call (outer level), or nullptr
+  int ldh, j, compute_y;
+  int *err;
+};
+
+// full_grot + final_grot (gmres.hpp:14-38) and, after the level's last step,
+// the back substitution Blas1::trsv (gmres.hpp:41-53).  One thread.
+template <typename T> __device__ void givens_step(const GivensCtl<T> &g, T nrm2) {
+  const int j = g.j;
+  T *Hc = g.H + (size_t)j * g.ldh;
+  const T h = sqrt(nrm2);
+  Hc[j + 1] = h;
+  *g.inv = T(1) / h;
+  if (!(h > T(0)) || !isfinite(h)) atomicExch(g.err, (int)DEV_BREAKDOWN);
+  for (int i = 0; i < j; i++) {
+    const T t = Hc[i];
+    Hc[i] = g.cs[i] * t + g.sn[i] * Hc[i + 1];
+    Hc[i + 1] = -g.sn[i] * t + g.cs[i] * Hc[i + 1];
+  }
+  const T t = sqrt(Hc[j] * Hc[j] + Hc[j + 1] * Hc[j + 1]);
+  g.cs[j] = Hc[j] / t;
+  g.sn[j] = Hc[j + 1] / t;
+  Hc[j] = t;
+  Hc[j + 1] = 0;
+  g.e[j + 1] = -g.sn[j] * g.e[j];
+  g.e[j] = g.cs[j] * g.e[j];
+  if (g.abs_e) *g.abs_e = (double)fabs(g.e[j + 1]);
+  if (g.compute_y) {
+    const int w = j + 1;
+    for (int i = w - 1; i >= 0; i--) {
+      T s = g.e[i];
+      for (int q = w - 1; q > i; q--) s -= g.H[(size_t)q * g.ldh + i] * g.y[q];
+      g.y[i] = s / g.H[(size_t)i * g.ldh + i];
+    }
+  }
+}
+
+// Back substitution only (outer level, after a convergence stop), one thread.
+template <typename T> __global__ void k_trsv_y(T *H, const T *e, T *y, int ldh, int w) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  for (int i = w - 1; i >= 0; i--) {
+    T s = e[i];
+    for (int q = w - 1; q > i; q--) s -= H[(size_t)q * ldh + i] * y[q];
+    y[i] = s / H[(size_t)i * ldh + i];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// SpMV epilogues of the FGMRES levels
+// ---------------------------------------------------------------------------
+
+// Inner levels (fp32 vectors): w = A z stored, and H(j, k) = <w, V(k)>,
+// k = 0..nv-1, fused (CGS dots all use the unmodified w, gmres.hpp:112-114).
+template <int NVT> struct EpiStoreDots {
+  using Red = float;
+  static constexpr int NV = NVT;
+  struct Pre {
+    float v[NVT];
+  };
+  float *y;
+  Cols<float> V;
+  int nv;
+  GridRed gr;
+  float *hcol;
+  __device__ __forceinline__ Pre load(int64_t r) const {
+    Pre p;
+#pragma unroll
+    for (int k = 0; k < NV; k++) p.v[k] = (k < nv) ? __ldg(V.p[k] + r) : 0.0f;
+    return p;
+  }
+  template <typename Acc> __device__ __forceinline__ void row(int64_t r, Acc acc, const Pre &p, Red (&d)[NV]) const {
+    const float yv = (float)acc;
+    y[r] = yv;
+#pragma unroll
+    for (int k = 0; k < NV; k++)
+      if (k < nv) d[k] = __fmaf_rn(yv, p.v[k], d[k]);
+  }
+  template <int W> __device__ __forceinline__ void finish(Red (&d)[NV]) const {
+    float *h = hcol;
+    const int m = nv;
+    grid_reduce<float, NV, W>(d, nv, gr, [h, m](float *tot) {
+      for (int k = 0; k < m; k++) h[k] = tot[k];
+    });
+  }
+};
+
+// Outer level: r = b - A x in fp64 with ||r||^2 fused; the finisher sets
+// e(0) = ||r||, 1/||r|| and |e(0)| for the host (gmres.hpp:87, 100-103).
+struct EpiResidualNorm {
+  using Red = double;
+  static constexpr int NV = 1;
+  struct Pre {
+    double b;
+  };
+  const double *b;
+  double *y;
+  GridRed gr;
+  double *e, *inv, *abs_e;
+  __device__ __forceinline__ Pre load(int64_t r) const { return {b[r]}; }
+  template <typename Acc> __device__ __forceinline__ void row(int64_t r, Acc acc, const Pre &p, Red (&d)[1]) const {
+    const double v = p.b - (double)acc;
+    y[r] = v;
+    d[0] = __fma_rn(v, v, d[0]);
+  }
+  template <int W> __device__ __forceinline__ void finish(Red (&d)[1]) const {
+    double *e_ = e, *inv_ = inv, *ae = abs_e;
+    grid_reduce<double, 1, W>(d, 1, gr, [e_, inv_, ae](double *tot) {
+      const double h = sqrt(tot[0]);
+      e_[0] = h;
+      *inv_ = 1.0 / h;
+      *ae = fabs(h);
+    });
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Gram-Schmidt update, norm, Givens (gmres.hpp:115-119)
+// ---------------------------------------------------------------------------
+// w -= sum_k H(j,k) V(k)   (MULMV order: V(i,0) h0, then fma over k)
+// then ||w||^2 -> h_{j+1,j}, 1/h, Givens rotation, optional back substitution.
+template <typename T, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32) k_cgs_update(T *__restrict__ w, Cols<T> V, int nv, int64_t n,
+                                                           GridRed gr, GivensCtl<T> g) {
+  __shared__ T sh[kMaxCols];
+  const T *hcol = g.H + (size_t)g.j * g.ldh;
+  for (int k = threadIdx.x; k < nv; k += blockDim.x) sh[k] = hcol[k];
+  __syncthreads();
+  T part[1] = {0};
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    T r = V.p[0][i] * sh[0];
+    for (int k = 1; k < nv; k++) r = fmaT(V.p[k][i], sh[k], r);
+    const T wi = w[i] - r;
+    w[i] = wi;
+    part[0] = fmaT(wi, wi, part[0]);
+  }
+  const GivensCtl<T> gg = g;
+  grid_reduce<T, 1, WARPS>(part, 1, gr, [gg](T *tot) { givens_step<T>(gg, tot[0]); });
+}
+
+// H(j, k) = <w, V(k)> for k < nv, fp64 (outer level; nv up to m_outer).
+template <int WARPS>
+__global__ void __launch_bounds__(WARPS * 32) k_multidot_f64(const double *__restrict__ w, Cols<double> V, int nv,
+                                                             int64_t n, GridRed gr, double *hcol) {
+  constexpr int CH = 8;
+  // partials laid out [block][nv]; chunks of CH vectors reuse w from L1
+  double *part = static_cast<double *>(gr.partials);
+  __shared__ double sred[WARPS][CH];
+  __shared__ bool last;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int k0 = 0; k0 < nv; k0 += CH) {
+    double a[CH];
+#pragma unroll
+    for (int c = 0; c < CH; c++) a[c] = 0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+      const double wi = w[i];
+#pragma unroll
+      for (int c = 0; c < CH; c++)
+        if (k0 + c < nv) a[c] = __fma_rn(wi, V.p[k0 + c][i], a[c]);
+    }
+#pragma unroll
+    for (int c = 0; c < CH; c++) {
+      const double s = warp_sum(a[c]);
+      if (lane == 0) sred[warp][c] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x < CH && k0 + threadIdx.x < nv) {
+      double s = 0;
+      for (int q = 0; q < WARPS; q++) s += sred[q][threadIdx.x];
+      part[(size_t)blockIdx.x * nv + k0 + threadIdx.x] = s;
+    }
+    __syncthreads();
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = (atomicAdd(gr.ticket, 1u) == gridDim.x - 1);
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  for (int k = warp; k < nv; k += WARPS) {
+    double s = 0;
+    for (int b = lane; b < (int)gridDim.x; b += 32) s += __ldcg(&part[(size_t)b * nv + k]);
+    s = warp_sum(s);
+    if (lane == 0) hcol[k] = s;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) *gr.ticket = 0;
+}
+
+// v *= *inv  (V(j+1) *= h.inv(), gmres.hpp:117)
+template <typename T> __global__ void k_scale(T *__restrict__ v, const T *__restrict__ inv, int64_t n) {
+  const T s = *inv;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    v[i] *= s;
+}
+
+// Level-2 entry: V2(0) = float(in) (V(0).copy(rhs), gmres.hpp:102) with e(0)=1
+// (normalize=false, gmres.hpp:100-101).  `in` is read through a device
+// pointer slot so one captured graph serves every outer step.
+__global__ void k_level2_enter(const double *const *__restrict__ in_slot, float *__restrict__ v0, float *e,
+                               int64_t n) {
+  const double *in = *in_slot;
+  if (blockIdx.x == 0 && threadIdx.x == 0) e[0] = 1.0f;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    v0[i] = (float)in[i];
+}
+
+// x = Z y (with_init) for the inner levels, x += Z y for the outer level
+// (gmres.hpp:127-131); the sum is formed in the level's type T and converted
+// to the caller's type Out, as MULMV followed by T(...) in the reference.
+template <typename T, typename Out, bool ACCUM>
+__global__ void k_zy(Cols<T> Z, const T *__restrict__ y, int nz, Out *__restrict__ out_direct,
+                     Out *const *__restrict__ out_slot, int64_t n) {
+  __shared__ T sy[kMaxCols];
+  for (int k = threadIdx.x; k < nz; k += blockDim.x) sy[k] = y[k];
+  __syncthreads();
+  Out *out = out_slot ? *out_slot : out_direct;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    T r = Z.p[0][i] * sy[0];
+    for (int k = 1; k < nz; k++) r = fmaT(Z.p[k][i], sy[k], r);
+    if (ACCUM) out[i] += (Out)r;
+    else out[i] = (Out)r;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Level 4: the fp16 Richardson operator R (f3r-gpu.cpp:229-260).  fp16
+// storage, fp32 arithmetic, one rounding to fp16 per stored value.
+// Diagonal SDAINV (W^T, Z both diagonal -- what tol = 0.1 leaves of a scaled
+// stencil) is fused into the vector kernels; general W^T / Z run as SELL
+// SpMVs with fused epilogues.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float h2f(__half h) { return __half2float(h); }
+__device__ __forceinline__ __half f2h(float f) { return __float2half_rn(f); }
+
+struct DiagPre {
+  const __half *w, *z;  // diagonal of W^T and of Z
+  __device__ __forceinline__ float apply(int64_t i, float x) const {
+    const float t = h2f(f2h(h2f(w[i]) * x));  // tmp = W^T x
+    return h2f(f2h(h2f(z[i]) * t));           // hout = Z tmp
+  }
+};
+
+// First half of R: hin = fp16(in * sc); hout = M hin; then, on a call without
+// a weight update, hout *= ome[0] (f3r-gpu.cpp:231-243).
+template <bool SCALE_BY_OME>
+__global__ void k_rich_enter_diag(const float *__restrict__ in, float sc, DiagPre M, __half *__restrict__ hin,
+                                  __half *__restrict__ hout, const RichState *__restrict__ rs, float *e_set,
+                                  int64_t n) {
+  if (e_set && blockIdx.x == 0 && threadIdx.x == 0) e_set[0] = 1.0f;
+  const float om = SCALE_BY_OME ? h2f(rs->ome[0]) : 1.0f;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const __half hi = f2h(in[i] * sc);
+    hin[i] = hi;
+    float ho = M.apply(i, h2f(hi));
+    if (SCALE_BY_OME) ho = h2f(f2h(ho * om));
+    hout[i] = f2h(ho);
+  }
+}
+
+// General preconditioner: hin = fp16(in * sc) only.
+__global__ void k_rich_cast_in(const float *__restrict__ in, float sc, __half *__restrict__ hin, float *e_set,
+                               int64_t n) {
+  if (e_set && blockIdx.x == 0 && threadIdx.x == 0) e_set[0] = 1.0f;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    hin[i] = f2h(in[i] * sc);
+}
+
+// Residual step of R with the diagonal preconditioner fused (no weight
+// update): hr = fp16(hin - A16 hout); t2 = M hr; hnew = fp16(hout + ome[k] t2);
+// the last step writes out = fp32(hnew) / sc (out.copy(hout)).
+struct EpiRichStep {
+  using Red = float;
+  static constexpr int NV = 0;
+  struct Pre {
+    __half hin, hout, w, z, ome;
+  };
+  const __half *hin, *hout;
+  DiagPre M;
+  const RichState *rs;
+  int k;
+  __half *hnext;  // next hout (steps before the last)
+  float *out;     // fp32 result (last step)
+  float isc;
+  __device__ __forceinline__ Pre load(int64_t r) const { return {hin[r], hout[r], M.w[r], M.z[r], rs->ome[k]}; }
+  template <typename Acc> __device__ __forceinline__ void row(int64_t r, Acc acc, const Pre &p, Red (&)[1]) const {
+    const float hr = h2f(f2h(h2f(p.hin) - (float)acc));
+    const float t = h2f(f2h(h2f(p.w) * hr));
+    const float t2 = h2f(f2h(h2f(p.z) * t));
+    const float hn = h2f(f2h(__fmaf_rn(h2f(p.ome), t2, h2f(p.hout))));
+    if (out) out[r] = hn * isc;
+    else hnext[r] = f2h(hn);
+  }
+  template <int W> __device__ __forceinline__ void finish(Red (&)[1]) const {}
+};
+
+// Residual step of an update call (diagonal M): stores hr and t2 = M hr.
+struct EpiRichResPre {
+  using Red = float;
+  static constexpr int NV = 0;
+  struct Pre {
+    __half hin, w, z;
+  };
+  const __half *hin;
+  DiagPre M;
+  __half *hr, *t2;
+  __device__ __forceinline__ Pre load(int64_t r) const { return {hin[r], M.w[r], M.z[r]}; }
+  template <typename Acc> __device__ __forceinline__ void row(int64_t r, Acc acc, const Pre &p, Red (&)[1]) const {
+    const __half h = f2h(h2f(p.hin) - (float)acc);
+    hr[r] = h;
+    const float t = h2f(f2h(h2f(p.w) * h2f(h)));
+    t2[r] = f2h(h2f(p.z) * t);
+  }
+  template <int W> __device__ __forceinline__ void finish(Red (&)[1]) const {}
+};
+
+// Weight computation of an update call: tmp = fp16(A16 v) stored, and
+// dot_ar = <tmp, tmp>, dot_r = <tmp, other> in fp32 (wildcard(., tof32),
+// f3r-gpu.cpp:235-240 / 249-254); the finisher forms the weight and the
+// running mean.  k = 0 also advances den = cnt / period.
+struct EpiRichWeight {
+  using Red = float;
+  static constexpr int NV = 2;
+  struct Pre {
+    __half other;
+  };
+  __half *tmp;
+  const __half *other;
+  GridRed gr;
+  RichState *rs;
+  int k;
+  __device__ __forceinline__ Pre load(int64_t r) const { return {other[r]}; }
+  template <typename Acc> __device__ __forceinline__ void row(int64_t r, Acc acc, const Pre &p, Red (&d)[2]) const {
+    const __half t = f2h((float)acc);
+    tmp[r] = t;
+    const float tv = h2f(t);
+    d[0] = __fmaf_rn(tv, tv, d[0]);
+    d[1] = __fmaf_rn(tv, h2f(p.other), d[1]);
+  }
+  template <int W> __device__ __forceinline__ void finish(Red (&d)[2]) const {
+    RichState *s = rs;
+    const int kk = k;
+    grid_reduce<float, 2, W>(d, 2, gr, [s, kk](float *tot) {
+      const float om = tot[1] / tot[0];
+      s->om[kk] = om;
+      s->sum[kk] += om;
+      if (kk == 0) s->den += 1;
+      s->ome[kk] = __float2half_rn(s->sum[kk] / (float)s->den);
+    });
+  }
+};
+
+// hout = fp16(hout * fp16(om[0]))  (hout *= dot_r / dot_ar, f3r-gpu.cpp:238)
+__global__ void k_rich_scale_om(__half *__restrict__ hout, const RichState *__restrict__ rs, int64_t n) {
+  const float om = h2f(f2h(rs->om[0]));
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    hout[i] = f2h(h2f(hout[i]) * om);
+}
+
+// hout = fp16(hout + om[k] t2) (f3r-gpu.cpp:252), or on the last step out =
+// fp32(that) / sc.  use_ome selects ome[k] (no-update calls, general M).
+__global__ void k_rich_axpy(__half *__restrict__ hout, const __half *__restrict__ t2,
+                            const RichState *__restrict__ rs, int k, int use_ome, float *__restrict__ out,
+                            float isc, int64_t n) {
+  const float om = use_ome ? h2f(rs->ome[k]) : rs->om[k];
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const float hn = h2f(f2h(__fmaf_rn(om, h2f(t2[i]), h2f(hout[i]))));
+    if (out) out[i] = hn * isc;
+    else hout[i] = f2h(hn);
+  }
+}
+
+// out = fp32(hout) / sc (m4 = 1: R is the preconditioner application alone)
+__global__ void k_rich_exit(const __half *__restrict__ hout, float *__restrict__ out, float isc, int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = h2f(hout[i]) * isc;
+}
+
+// General M, Z apply: hout = fp16(Z tmp), then (no-update calls) hout *=
+// ome[0] as a second rounding, as the reference's separate statements.
+struct EpiZScale {
+  using Red = float;
+  using Pre = NoPre;
+  static constexpr int NV = 0;
+  __half *hout;
+  const RichState *rs;
+  int scale;
+  __device__ __forceinline__ Pre load(int64_t) const { return {}; }
+  template <typename Acc> __device__ __forceinline__ void row(int64_t r, Acc acc, const Pre &, Red (&)[1]) const {
+    __half h = f2h((float)acc);
+    if (scale) h = f2h(h2f(h) * h2f(rs->ome[0]));
+    hout[r] = h;
+  }
+  template <int W> __device__ __forceinline__ void finish(Red (&)[1]) const {}
+};
+
+// fp32 -> fp64 / fp16 / fp32 conversion of a value array (matrix copies).
+template <typename To> __global__ void k_convert_vals(const double *__restrict__ in, To *__restrict__ out, int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = cvt<To>(in[i]);
+}
+
+// gather / scatter through a row permutation (SELL-C-sigma system order)
+__global__ void k_permute_gather(const double *__restrict__ in, const int32_t *__restrict__ perm,
+                                 double *__restrict__ out, int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = in[perm[i]];
+}
+__global__ void k_permute_scatter(const double *__restrict__ in, const int32_t *__restrict__ perm,
+                                  double *__restrict__ out, int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    out[perm[i]] = in[i];
+}
+
+// <x, y> with the deterministic grid reduction (kmm::dot)
+template <typename T, typename Acc, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32) k_dot(const T *__restrict__ x, const T *__restrict__ y, int64_t n,
+                                                    GridRed gr, Acc *out) {
+  Acc part[1] = {0};
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    part[0] = fmaT(to_acc<Acc>(x[i]), to_acc<Acc>(y[i]), part[0]);
+  grid_reduce<Acc, 1, WARPS>(part, 1, gr, [out](Acc *tot) { *out = tot[0]; });
+}
+
+}  // namespace f3r

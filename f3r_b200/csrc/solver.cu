@@ -1,0 +1,1095 @@
+// solver.cu -- device objects (context, SELL-C-sigma matrices), the nested
+// F3R solver orchestration, and the C ABI of include/f3r_b200.h.
+//
+// Solver structure (the reference assembles the same nesting in
+// work/src/f3r-gpu.cpp:210-265):
+//   Restarted( FGMRES<double>(A, L2, m_outer, normalize) , max_restarts )
+//   L2 = FGMRES<float>(A32, L3, m2)         fp32 matrix and vectors
+//   L3 = FGMRES<float>(A16, R, m3)          fp16 matrix, fp32 vectors
+//   R  = adaptive-weight Richardson(m4, c)  fp16 vectors, SDAINV / BJ-ILU(0)
+// Levels 2-4 run a fixed number of steps with no host decision, so one outer
+// step's call into L2 is a static sequence of kernels; it is launched
+// asynchronously (optionally as a replayed CUDA graph) and the host
+// synchronises once per outer Arnoldi step to evaluate cond().
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <numeric>
+#include <random>
+#include <string>
+#include <vector>
+
+#include "internal.hpp"
+#include "kernels.cuh"
+#include "ilu.cuh"
+
+namespace f3r {
+
+static thread_local std::string g_err;
+Status fail(Status code, const std::string &msg) {
+  g_err = msg;
+  return code;
+}
+
+#define CUDA_TRY(x)                                                                               \
+  do {                                                                                            \
+    cudaError_t e_ = (x);                                                                         \
+    if (e_ != cudaSuccess)                                                                        \
+      return fail(e_ == cudaErrorMemoryAllocation ? F3R_ERROR_OUT_OF_MEMORY : F3R_ERROR_CUDA,     \
+                  std::string(#x) + ": " + cudaGetErrorString(e_));                               \
+  } while (0)
+
+static inline int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
+
+// ---------------------------------------------------------------------------
+// context
+// ---------------------------------------------------------------------------
+constexpr size_t kPartialBytes = 1u << 20;
+
+struct Context {
+  int device = 0;
+  cudaStream_t own = nullptr, stream = nullptr;
+  int sm_count = 148;
+  int *err = nullptr;          // device error word (DevError)
+  void *partials = nullptr;    // grid-reduction partial sums
+  unsigned int *ticket = nullptr;
+  double *pinned = nullptr;    // host-pinned scalars for D2H reads
+  double *dscratch = nullptr;  // device scalars for f3r_dot
+  int64_t launches = 0;        // kernels issued through this context
+  std::vector<void *> allocs;
+
+  Status alloc(void **p, size_t bytes) {
+    cudaError_t e = cudaMalloc(p, bytes ? bytes : 16);
+    if (e != cudaSuccess)
+      return fail(e == cudaErrorMemoryAllocation ? F3R_ERROR_OUT_OF_MEMORY : F3R_ERROR_CUDA,
+                  std::string("cudaMalloc(") + std::to_string(bytes) + "): " + cudaGetErrorString(e));
+    return F3R_SUCCESS;
+  }
+  GridRed gred() const { return GridRed{partials, ticket}; }
+  int ew_grid(int64_t n) const { return (int)std::max<int64_t>(1, std::min<int64_t>(cdiv(n, kEwThreads), (int64_t)sm_count * 4)); }
+  // checks the device error word (after a synchronisation)
+  Status check_device_error() {
+    int e = 0;
+    CUDA_TRY(cudaMemcpy(&e, err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (e == DEV_OK) return F3R_SUCCESS;
+    CUDA_TRY(cudaMemset(err, 0, sizeof(int)));
+    if (e == DEV_TIMEOUT_SPMV) return fail(F3R_ERROR_TIMEOUT, "a bulk-copy wait in the SpMV kernel exceeded its bound");
+    return fail(F3R_ERROR_BREAKDOWN, "zero or non-finite norm in an Arnoldi step");
+  }
+};
+
+
+// Launches a kernel on the context's bookkeeping (every launch is counted,
+// so a solve can report how many kernels of this library it ran).
+template <typename... KP, typename... A>
+static inline void launch_k(Context &c, void (*k)(KP...), int grid, int block, size_t smem, cudaStream_t st,
+                            A &&...args) {
+  k<<<grid, block, smem, st>>>(std::forward<A>(args)...);
+  c.launches++;
+}
+
+// ---------------------------------------------------------------------------
+// SELL-32 construction on the host
+// ---------------------------------------------------------------------------
+struct SellHost {
+  int32_t n = 0, ncols = 0, nslices = 0, max_width = 0, sigma = 1;
+  int64_t nnz = 0, nnz_pad = 0;
+  std::vector<int32_t> sptr, col, perm;  // perm: storage row -> original row
+  std::vector<double> val;
+};
+
+// renumber = true builds P A P^T (columns mapped to storage order) for the
+// solver's permuted system; false keeps original columns and scatters rows.
+static Status build_sell(const f3r_csr &a, int32_t sigma, bool renumber, SellHost &s,
+                         const std::vector<int32_t> *given_perm = nullptr) {
+  if (sigma < 1) return fail(F3R_ERROR_INVALID_VALUE, "sigma must be >= 1");
+  if (renumber && a.nrows != a.ncols) return fail(F3R_ERROR_INVALID_VALUE, "symmetric permutation needs a square matrix");
+  const int32_t n = a.nrows;
+  s.n = n;
+  s.ncols = a.ncols;
+  s.sigma = sigma;
+  s.nnz = a.nnz;
+  s.nslices = (int32_t)cdiv(n, 32);
+  s.perm.resize(n);
+  std::iota(s.perm.begin(), s.perm.end(), 0);
+  auto len = [&](int32_t r) { return a.rptr[r + 1] - a.rptr[r]; };
+  if (given_perm) {
+    s.perm = *given_perm;
+  } else if (sigma > 1) {
+    // rows ordered by decreasing length inside each window of sigma rows
+    // (SELLsig, matrix/sell.hpp:309-343); stable for equal lengths
+    for (int64_t w0 = 0; w0 < n; w0 += sigma) {
+      const int64_t e = std::min<int64_t>(n, w0 + sigma);
+      std::stable_sort(s.perm.begin() + w0, s.perm.begin() + e,
+                       [&](int32_t x, int32_t y) { return len(x) > len(y); });
+    }
+  }
+  std::vector<int32_t> iperm;
+  if (renumber) {
+    iperm.resize(n);
+    for (int32_t i = 0; i < n; i++) iperm[s.perm[i]] = i;
+  }
+  s.sptr.assign(s.nslices + 1, 0);
+  int32_t mw = 0;
+  for (int32_t sl = 0; sl < s.nslices; sl++) {
+    int32_t w = 0;
+    for (int32_t l = 0; l < 32; l++) {
+      const int64_t r = (int64_t)sl * 32 + l;
+      if (r < n) w = std::max(w, len(s.perm[r]));
+    }
+    mw = std::max(mw, w);
+    if ((int64_t)s.sptr[sl] + w > INT32_MAX / 32) return fail(F3R_ERROR_UNSUPPORTED, "padded matrix exceeds 2^31 entries");
+    s.sptr[sl + 1] = s.sptr[sl] + w;
+  }
+  s.max_width = mw;
+  s.nnz_pad = (int64_t)s.sptr[s.nslices] * 32;
+  s.col.assign(s.nnz_pad, 0);
+  s.val.assign(s.nnz_pad, 0.0);
+#pragma omp parallel for schedule(static)
+  for (int32_t sl = 0; sl < s.nslices; sl++) {
+    const int64_t base = (int64_t)s.sptr[sl] * 32;
+    const int32_t w = s.sptr[sl + 1] - s.sptr[sl];
+    for (int32_t l = 0; l < 32; l++) {
+      const int64_t r = (int64_t)sl * 32 + l;
+      int32_t c = 0, prev = 0;
+      if (r < n) {
+        const int32_t o = s.perm[r];
+        for (int32_t q = a.rptr[o]; q < a.rptr[o + 1]; q++, c++) {
+          prev = renumber ? iperm[a.idx[q]] : a.idx[q];
+          s.col[base + (int64_t)c * 32 + l] = prev;
+          s.val[base + (int64_t)c * 32 + l] = a.val[q];
+        }
+      }
+      for (; c < w; c++) s.col[base + (int64_t)c * 32 + l] = prev;
+    }
+  }
+  return F3R_SUCCESS;
+}
+
+struct DeviceSell {
+  int32_t n = 0, ncols = 0, nslices = 0, max_width = 0, sigma = 1;
+  int64_t nnz = 0, nnz_pad = 0;
+  int32_t *col = nullptr, *sptr = nullptr, *perm = nullptr;
+  double *v64 = nullptr;
+  float *v32 = nullptr;
+  __half *v16 = nullptr;
+  int dtypes = 0;
+  DevSell view() const { return DevSell{col, sptr, perm, n, nslices}; }
+  void release() {
+    cudaFree(col); cudaFree(sptr); cudaFree(perm); cudaFree(v64); cudaFree(v32); cudaFree(v16);
+    col = sptr = perm = nullptr; v64 = nullptr; v32 = nullptr; v16 = nullptr;
+  }
+};
+
+static Status upload_sell(Context &c, const SellHost &h, int dtype_mask, bool scatter_perm, DeviceSell &d) {
+  d.n = h.n; d.ncols = h.ncols; d.nslices = h.nslices; d.max_width = h.max_width; d.sigma = h.sigma;
+  d.nnz = h.nnz; d.nnz_pad = h.nnz_pad; d.dtypes = dtype_mask;
+  const size_t np = (size_t)h.nnz_pad;
+  F3R_TRY(c.alloc((void **)&d.col, np * 4));
+  F3R_TRY(c.alloc((void **)&d.sptr, (size_t)(h.nslices + 1) * 4));
+  CUDA_TRY(cudaMemcpyAsync(d.col, h.col.data(), np * 4, cudaMemcpyHostToDevice, c.stream));
+  CUDA_TRY(cudaMemcpyAsync(d.sptr, h.sptr.data(), (size_t)(h.nslices + 1) * 4, cudaMemcpyHostToDevice, c.stream));
+  if (scatter_perm && h.sigma > 1) {
+    F3R_TRY(c.alloc((void **)&d.perm, (size_t)std::max(h.n, 1) * 4));
+    CUDA_TRY(cudaMemcpyAsync(d.perm, h.perm.data(), (size_t)h.n * 4, cudaMemcpyHostToDevice, c.stream));
+  }
+  double *tmp64 = nullptr;
+  F3R_TRY(c.alloc((void **)&tmp64, np * 8));
+  CUDA_TRY(cudaMemcpyAsync(tmp64, h.val.data(), np * 8, cudaMemcpyHostToDevice, c.stream));
+  const int g = c.ew_grid((int64_t)np);
+  if (dtype_mask & (1 << F3R_F32)) {
+    F3R_TRY(c.alloc((void **)&d.v32, np * 4));
+    launch_k(c, k_convert_vals<float>, g, kEwThreads, 0, c.stream, tmp64, d.v32, (int64_t)np);
+  }
+  if (dtype_mask & (1 << F3R_F16)) {
+    F3R_TRY(c.alloc((void **)&d.v16, np * 2));
+    launch_k(c, k_convert_vals<__half>, g, kEwThreads, 0, c.stream, tmp64, d.v16, (int64_t)np);
+  }
+  CUDA_TRY(cudaGetLastError());
+  if (dtype_mask & (1 << F3R_F64)) {
+    d.v64 = tmp64;
+  } else {
+    CUDA_TRY(cudaStreamSynchronize(c.stream));
+    cudaFree(tmp64);
+  }
+  CUDA_TRY(cudaStreamSynchronize(c.stream));
+  return F3R_SUCCESS;
+}
+
+// ---------------------------------------------------------------------------
+// SpMV launcher
+// ---------------------------------------------------------------------------
+// Raises the kernel's dynamic shared memory limit once per device.  Called
+// before any graph capture for every instantiation the solver uses.
+template <typename V, typename X, typename Epi>
+static Status sell_attr(Context &c) {
+  static int attr_done[64] = {0};
+  if (!attr_done[c.device & 63]) {
+    CUDA_TRY(cudaFuncSetAttribute(
+        k_sell_cfg<V, X, Epi, SellCfg<V>::WARPS, SellCfg<V>::STAGES, SellCfg<V>::KC>,
+        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sell_smem_bytes<V>()));
+    attr_done[c.device & 63] = 1;
+  }
+  return F3R_SUCCESS;
+}
+
+template <typename V, typename X, typename Epi>
+static Status launch_sell(Context &c, const V *val, const DevSell &A, const X *x, const Epi &epi) {
+  if (A.nslices == 0) return F3R_SUCCESS;
+  constexpr int WARPS = SellCfg<V>::WARPS;
+  constexpr size_t smem = sell_smem_bytes<V>();
+  F3R_TRY((sell_attr<V, X, Epi>(c)));
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(cdiv(A.nslices, WARPS), c.sm_count));
+  launch_k(c, k_sell_cfg<V, X, Epi, WARPS, SellCfg<V>::STAGES, SellCfg<V>::KC>, grid, WARPS * 32, smem, c.stream,
+           val, A, x, epi, c.err);
+  CUDA_TRY(cudaGetLastError());
+  return F3R_SUCCESS;
+}
+
+Status IluDevice::to_half(__half **d, const std::vector<double> &v) {
+  double *tmp = nullptr;
+  const size_t nb = std::max<size_t>(v.size(), 1);
+  CUDA_TRY(cudaMalloc((void **)&tmp, nb * sizeof(double)));
+  cudaError_t e = cudaMalloc((void **)d, nb * sizeof(__half));
+  if (e != cudaSuccess) {
+    cudaFree(tmp);
+    return fail(F3R_ERROR_OUT_OF_MEMORY, "ILU values");
+  }
+  allocs.push_back((void *)*d);
+  CUDA_TRY(cudaMemcpy(tmp, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice));
+  const int64_t n = (int64_t)v.size();
+  const int g = (int)std::max<int64_t>(1, std::min<int64_t>(cdiv(n, kEwThreads), 1024));
+  k_convert_vals<__half><<<g, kEwThreads>>>(tmp, *d, n);
+  CUDA_TRY(cudaDeviceSynchronize());
+  cudaFree(tmp);
+  return F3R_SUCCESS;
+}
+
+}  // namespace f3r
+
+using namespace f3r;
+
+struct f3r_context : Context {};
+
+struct f3r_sell {
+  f3r_context *ctx = nullptr;
+  DeviceSell d;
+};
+
+// ---------------------------------------------------------------------------
+// solver
+// ---------------------------------------------------------------------------
+namespace f3r {
+
+template <typename T> struct Level {
+  int m = 0;
+  T *V = nullptr, *Z = nullptr;  // column-major n x (m+1), n x m (level 3 V column 0 is an alias)
+  T *H = nullptr, *cs = nullptr, *sn = nullptr, *e = nullptr, *y = nullptr, *inv = nullptr;
+};
+
+struct Solver {
+  f3r_context *ctx = nullptr;
+  f3r_params p{};
+  int32_t n = 0;
+  DeviceSell A;
+  std::vector<int32_t> perm;  // storage row -> original row (sigma > 1)
+  int32_t *perm_d = nullptr;
+  // preconditioner
+  int precond_diag = 0;
+  __half *wd = nullptr, *zd = nullptr;
+  DeviceSell W, Z;    // general SDAINV factors (permuted system)
+  IluDevice ilu;      // block-Jacobi ILU(0), level scheduled
+  // levels
+  Level<double> L1;
+  Level<float> L2, L3;
+  double *abs_e = nullptr;
+  __half *hin = nullptr, *hout = nullptr, *hout2 = nullptr, *tmp = nullptr, *tmp2 = nullptr, *hr = nullptr;
+  RichState *rs = nullptr;
+  const double **in_slot = nullptr;
+  double **out_slot = nullptr;
+  double *b_d = nullptr, *x_d = nullptr, *bp_d = nullptr, *xp_d = nullptr, *r_d = nullptr;
+  int64_t cnt = 0;
+  int64_t r_calls = 0;
+  std::vector<void *> allocs;
+  std::map<std::vector<bool>, std::pair<cudaGraphExec_t, int64_t>> graphs;  // exec, kernels in it
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+
+  Context &C() { return *ctx; }
+  template <typename T> Status alloc(T **p, size_t count) {
+    F3R_TRY(ctx->alloc((void **)p, count * sizeof(T)));
+    allocs.push_back((void *)*p);
+    return F3R_SUCCESS;
+  }
+  ~Solver() {
+    for (auto &kv : graphs) cudaGraphExecDestroy(kv.second.first);
+    for (void *q : allocs) cudaFree(q);
+    A.release(); W.release(); Z.release(); ilu.release();
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+  }
+
+  template <typename T> Status make_level(Level<T> &L, int m, bool own_v0) {
+    L.m = m;
+    const size_t nn = (size_t)std::max(n, 1);
+    F3R_TRY(alloc(&L.V, nn * (size_t)(m + (own_v0 ? 1 : 0))));
+    F3R_TRY(alloc(&L.Z, nn * (size_t)m));
+    F3R_TRY(alloc(&L.H, (size_t)(m + 1) * m));
+    F3R_TRY(alloc(&L.cs, (size_t)m));
+    F3R_TRY(alloc(&L.sn, (size_t)m));
+    F3R_TRY(alloc(&L.e, (size_t)m + 1));
+    F3R_TRY(alloc(&L.y, (size_t)m));
+    F3R_TRY(alloc(&L.inv, 1));
+    CUDA_TRY(cudaMemset(L.H, 0, sizeof(T) * (size_t)(m + 1) * m));
+    CUDA_TRY(cudaMemset(L.e, 0, sizeof(T) * (size_t)(m + 1)));
+    return F3R_SUCCESS;
+  }
+
+  // ---- level 4: R(in) -> out -------------------------------------------------
+  Status rich_apply(const float *in, float *out, float *e_set) {
+    const int64_t N = n;
+    const int g = C().ew_grid(N);
+    cudaStream_t st = C().stream;
+    ++cnt;
+    ++r_calls;
+    const bool upd = (cnt % p.c) == 0;
+    const float sc = std::ldexp(1.0f, p.half_scale_log2), isc = std::ldexp(1.0f, -p.half_scale_log2);
+    const DevSell Av = A.view();
+    if (precond_diag) {
+      const DiagPre M{wd, zd};
+      if (!upd) {
+        launch_k(C(), k_rich_enter_diag<true>, g, kEwThreads, 0, st, in, sc, M, hin, hout, rs, e_set, N);
+        __half *cur = hout, *nxt = hout2;
+        for (int k = 1; k < p.m4; k++) {
+          const bool last = (k == p.m4 - 1);
+          EpiRichStep epi{hin, cur, M, rs, k, last ? nullptr : nxt, last ? out : nullptr, isc};
+          F3R_TRY(launch_sell(C(), A.v16, Av, (const __half *)cur, epi));
+          std::swap(cur, nxt);
+        }
+        if (p.m4 == 1) launch_k(C(), k_rich_exit, g, kEwThreads, 0, st, hout, out, isc, N);
+      } else {
+        launch_k(C(), k_rich_enter_diag<false>, g, kEwThreads, 0, st, in, sc, M, hin, hout, rs, e_set, N);
+        F3R_TRY(launch_sell(C(), A.v16, Av, (const __half *)hout, EpiRichWeight{tmp, hin, C().gred(), rs, 0}));
+        launch_k(C(), k_rich_scale_om, g, kEwThreads, 0, st, hout, rs, N);
+        for (int k = 1; k < p.m4; k++) {
+          const bool last = (k == p.m4 - 1);
+          F3R_TRY(launch_sell(C(), A.v16, Av, (const __half *)hout, EpiRichResPre{hin, M, hr, tmp2}));
+          F3R_TRY(launch_sell(C(), A.v16, Av, (const __half *)tmp2, EpiRichWeight{tmp, hr, C().gred(), rs, k}));
+          launch_k(C(), k_rich_axpy, g, kEwThreads, 0, st, hout, tmp2, rs, k, 0, last ? out : nullptr, isc, N);
+        }
+        if (p.m4 == 1) launch_k(C(), k_rich_exit, g, kEwThreads, 0, st, hout, out, isc, N);
+      }
+    } else {
+      // general preconditioner: M = Z W^T (SDAINV) or U^-1 L^-1 (ILU)
+      launch_k(C(), k_rich_cast_in, g, kEwThreads, 0, st, in, sc, hin, e_set, N);
+      F3R_TRY(prec_apply(hin, hout, !upd));
+      if (upd) {
+        F3R_TRY(launch_sell(C(), A.v16, Av, (const __half *)hout, EpiRichWeight{tmp, hin, C().gred(), rs, 0}));
+        launch_k(C(), k_rich_scale_om, g, kEwThreads, 0, st, hout, rs, N);
+      }
+      for (int k = 1; k < p.m4; k++) {
+        const bool last = (k == p.m4 - 1);
+        F3R_TRY(launch_sell(C(), A.v16, Av, (const __half *)hout, EpiResidual<__half, __half>{hin, hr, nullptr}));
+        F3R_TRY(prec_apply(hr, tmp2, false));
+        if (upd) F3R_TRY(launch_sell(C(), A.v16, Av, (const __half *)tmp2, EpiRichWeight{tmp, hr, C().gred(), rs, k}));
+        launch_k(C(), k_rich_axpy, g, kEwThreads, 0, st, hout, tmp2, rs, k, upd ? 0 : 1, last ? out : nullptr, isc, N);
+      }
+      if (p.m4 == 1) launch_k(C(), k_rich_exit, g, kEwThreads, 0, st, hout, out, isc, N);
+    }
+    CUDA_TRY(cudaGetLastError());
+    return F3R_SUCCESS;
+  }
+
+  // out = M x for the general preconditioners; scale_ome multiplies by ome[0]
+  Status prec_apply(const __half *x, __half *out, bool scale_ome) {
+    if (p.precond == F3R_PRECOND_SDAINV) {
+      F3R_TRY(launch_sell(C(), W.v16, W.view(), x, EpiStore<__half>{tmp, nullptr}));
+      F3R_TRY(launch_sell(C(), Z.v16, Z.view(), (const __half *)tmp, EpiZScale{out, rs, scale_ome ? 1 : 0}));
+    } else {
+      F3R_TRY(ilu.apply(C().stream, x, tmp, out, scale_ome ? &rs->ome[0] : nullptr));
+    }
+    return F3R_SUCCESS;
+  }
+
+  // w = A z with H(j, 0..nv-1) = <w, V(k)> fused; the dot count picks the
+  // smallest epilogue instantiation (registers)
+  template <typename V>
+  Status spmv_dots(const V *vals, const float *z, float *w, const Cols<float> &Vc, int nv, float *hcol) {
+    if (nv <= 4) return launch_sell(C(), vals, A.view(), z, EpiStoreDots<4>{w, Vc, nv, C().gred(), hcol});
+    if (nv <= 8) return launch_sell(C(), vals, A.view(), z, EpiStoreDots<8>{w, Vc, nv, C().gred(), hcol});
+    return launch_sell(C(), vals, A.view(), z, EpiStoreDots<kMaxDots>{w, Vc, nv, C().gred(), hcol});
+  }
+
+  // ---- level 3: FGMRES<float>(A16, R, m3), input V2 column, output Z2 col ----
+  Status level3(const float *in, float *out) {
+    Level<float> &L = L3;
+    const int64_t N = n;
+    Cols<float> V{}, Zc{};
+    V.p[0] = in;
+    for (int k = 1; k <= L.m; k++) V.p[k] = L.V + (size_t)(k - 1) * N;
+    for (int k = 0; k < L.m; k++) Zc.p[k] = L.Z + (size_t)k * N;
+    for (int j = 0; j < L.m; j++) {
+      float *zj = L.Z + (size_t)j * N;
+      float *w = L.V + (size_t)j * N;  // V(j+1)
+      F3R_TRY(rich_apply(V.p[j], zj, j == 0 ? L.e : nullptr));
+      F3R_TRY(spmv_dots(A.v16, zj, w, V, j + 1, L.H + (size_t)j * (L.m + 1)));
+      GivensCtl<float> g{L.H, L.cs, L.sn, L.e, L.y, L.inv, nullptr, L.m + 1, j, j == L.m - 1, C().err};
+      launch_k(C(), k_cgs_update<float, 8>, C().ew_grid(N), 256, 0, C().stream, w, V, j + 1, N, C().gred(), g);
+      if (j < L.m - 1) launch_k(C(), k_scale<float>, C().ew_grid(N), kEwThreads, 0, C().stream, w, L.inv, N);
+    }
+    launch_k(C(), k_zy<float, float, false>, C().ew_grid(N), kEwThreads, 0, C().stream, Zc, L.y, L.m, out, nullptr, N);
+    CUDA_TRY(cudaGetLastError());
+    return F3R_SUCCESS;
+  }
+
+  // ---- level 2: FGMRES<float>(A32, L3, m2); in/out through the slots -------
+  Status level2() {
+    Level<float> &L = L2;
+    const int64_t N = n;
+    Cols<float> V{}, Zc{};
+    for (int k = 0; k <= L.m; k++) V.p[k] = L.V + (size_t)k * N;
+    for (int k = 0; k < L.m; k++) Zc.p[k] = L.Z + (size_t)k * N;
+    launch_k(C(), k_level2_enter, C().ew_grid(N), kEwThreads, 0, C().stream, in_slot, L.V, L.e, N);
+    for (int j = 0; j < L.m; j++) {
+      float *zj = L.Z + (size_t)j * N;
+      float *w = L.V + (size_t)(j + 1) * N;
+      F3R_TRY(level3(V.p[j], zj));
+      F3R_TRY(spmv_dots(A.v32, zj, w, V, j + 1, L.H + (size_t)j * (L.m + 1)));
+      GivensCtl<float> g{L.H, L.cs, L.sn, L.e, L.y, L.inv, nullptr, L.m + 1, j, j == L.m - 1, C().err};
+      launch_k(C(), k_cgs_update<float, 8>, C().ew_grid(N), 256, 0, C().stream, w, V, j + 1, N, C().gred(), g);
+      if (j < L.m - 1) launch_k(C(), k_scale<float>, C().ew_grid(N), kEwThreads, 0, C().stream, w, L.inv, N);
+    }
+    launch_k(C(), k_zy<float, double, false>, C().ew_grid(N), kEwThreads, 0, C().stream, Zc, L.y, L.m, nullptr, out_slot, N);
+    CUDA_TRY(cudaGetLastError());
+    return F3R_SUCCESS;
+  }
+
+  // One call into level 2 for outer column j, replayed from a CUDA graph
+  // keyed by which Richardson calls inside it update their weights.
+  Status level2_call(const double *in, double *out) {
+    CUDA_TRY(cudaMemcpyAsync((void *)in_slot, &in, sizeof(in), cudaMemcpyHostToDevice, C().stream));
+    CUDA_TRY(cudaMemcpyAsync((void *)out_slot, &out, sizeof(out), cudaMemcpyHostToDevice, C().stream));
+    // the legacy / per-thread default streams cannot be captured
+    const cudaStream_t cs = C().stream;
+    if (!p.use_graphs || cs == 0 || cs == cudaStreamLegacy || cs == cudaStreamPerThread) return level2();
+    const int calls = p.m2 * p.m3;
+    std::vector<bool> key(calls);
+    for (int i = 0; i < calls; i++) key[i] = ((cnt + 1 + i) % p.c) == 0;
+    auto it = graphs.find(key);
+    if (it == graphs.end()) {
+      const int64_t cnt0 = cnt, rc0 = r_calls, l0 = C().launches;
+      cudaGraph_t graph = nullptr;
+      CUDA_TRY(cudaStreamBeginCapture(C().stream, cudaStreamCaptureModeThreadLocal));
+      Status s = level2();
+      cudaError_t ce = cudaStreamEndCapture(C().stream, &graph);
+      if (s != F3R_SUCCESS) {
+        if (graph) cudaGraphDestroy(graph);
+        return s;
+      }
+      if (ce != cudaSuccess) return fail(F3R_ERROR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+      cudaGraphExec_t exec = nullptr;
+      ce = cudaGraphInstantiate(&exec, graph, 0);
+      cudaGraphDestroy(graph);
+      if (ce != cudaSuccess) return fail(F3R_ERROR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ce));
+      it = graphs.emplace(key, std::make_pair(exec, C().launches - l0)).first;
+      cnt = cnt0;  // capture advanced the counters without running anything
+      r_calls = rc0;
+      C().launches = l0;
+    }
+    CUDA_TRY(cudaGraphLaunch(it->second.first, C().stream));
+    C().launches += it->second.second;
+    cnt += calls;
+    r_calls += calls;
+    return F3R_SUCCESS;
+  }
+
+  Status read_abs_e(double *v) {
+    CUDA_TRY(cudaMemcpyAsync(C().pinned, abs_e, sizeof(double), cudaMemcpyDeviceToHost, C().stream));
+    CUDA_TRY(cudaStreamSynchronize(C().stream));
+    F3R_TRY(C().check_device_error());
+    *v = C().pinned[0];
+    return F3R_SUCCESS;
+  }
+
+  // ---- level 1 inside Restarted (gmres.hpp:85-134, restart.hpp:26-36) -------
+  Status solve(const double *b_user, double *x_user, f3r_cond_fn cond, void *user, f3r_result *res) {
+    const int64_t N = n;
+    cudaStream_t st = C().stream;
+    const int g = C().ew_grid(N);
+    auto is_dev = [&](const void *q) {
+      cudaPointerAttributes a{};
+      if (cudaPointerGetAttributes(&a, q) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+      }
+      return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+    };
+    const bool b_dev = is_dev(b_user), x_dev = is_dev(x_user);
+    const double *b = b_user;
+    double *x = x_user;
+    if (!b_dev) {
+      CUDA_TRY(cudaMemcpyAsync(b_d, b_user, sizeof(double) * N, cudaMemcpyHostToDevice, st));
+      b = b_d;
+    }
+    if (!x_dev) {
+      CUDA_TRY(cudaMemcpyAsync(x_d, x_user, sizeof(double) * N, cudaMemcpyHostToDevice, st));
+      x = x_d;
+    }
+    CUDA_TRY(cudaEventRecord(ev0, st));
+    const int64_t launches0 = C().launches;
+    // permuted system (SELL-C-sigma order)
+    const double *bs = b;
+    double *xs = x;
+    if (perm_d) {
+      launch_k(C(), k_permute_gather, g, kEwThreads, 0, st, b, perm_d, bp_d, N);
+      launch_k(C(), k_permute_gather, g, kEwThreads, 0, st, x, perm_d, xp_d, N);
+      bs = bp_d;
+      xs = xp_d;
+    }
+    // per-solve Richardson state (f3r-gpu.cpp:277-281)
+    cnt = p.c;
+    r_calls = 0;
+    {
+      RichState h{};
+      for (int k = 0; k < kMaxM4; k++) {
+        h.sum[k] = 1.0f;
+        h.ome[k] = __float2half(1.0f);
+        h.om[k] = 0.0f;
+      }
+      h.den = 1;
+      CUDA_TRY(cudaMemcpyAsync(rs, &h, sizeof(h), cudaMemcpyHostToDevice, st));
+      CUDA_TRY(cudaStreamSynchronize(st));
+    }
+    // ||b|| for the relative stop test
+    double nb = 0;
+    launch_k(C(), k_dot<double, double, 8>, g, 256, 0, st, bs, bs, N, C().gred(), C().dscratch);
+    CUDA_TRY(cudaMemcpyAsync(C().pinned, C().dscratch, sizeof(double), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    nb = std::sqrt(C().pinned[0]);
+    auto stop = [&](int i, double e) -> bool {
+      if (cond) return cond(i, e, user) != 0;
+      return nb > 0 ? (e / nb < p.rel_tol) : (e == 0);
+    };
+
+    Level<double> &L = L1;
+    Cols<double> V{}, Zc{};
+    for (int k = 0; k <= L.m; k++) V.p[k] = L.V + (size_t)k * N;
+    for (int k = 0; k < L.m; k++) Zc.p[k] = L.Z + (size_t)k * N;
+    f3r_result out{};
+    int restarts = 0;
+    double last_e = 0;
+    bool solved = false;
+    while (!solved && restarts < p.max_restarts) {
+      restarts++;
+      // r = b - A x with ||r|| fused (gmres.hpp:87, 100)
+      F3R_TRY(launch_sell(C(), A.v64, A.view(), (const double *)xs,
+                          EpiResidualNorm{bs, L.V, C().gred(), L.e, L.inv, abs_e}));
+      double h0;
+      F3R_TRY(read_abs_e(&h0));
+      last_e = h0;
+      if (stop(0, h0)) {
+        solved = true;
+        break;
+      }
+      launch_k(C(), k_scale<double>, g, kEwThreads, 0, st, L.V, L.inv, N);
+      int j = 0;
+      bool conv = false;
+      for (; j < L.m; j++) {
+        double *zj = L.Z + (size_t)j * N;
+        double *w = L.V + (size_t)(j + 1) * N;
+        F3R_TRY(level2_call(V.p[j], zj));
+        F3R_TRY(launch_sell(C(), A.v64, A.view(), (const double *)zj, EpiStore<double>{w, nullptr}));
+        launch_k(C(), k_multidot_f64<8>, g, 256, 0, st, w, V, j + 1, N, C().gred(), L.H + (size_t)j * (L.m + 1));
+        GivensCtl<double> gc{L.H, L.cs, L.sn, L.e, L.y, L.inv, abs_e, L.m + 1, j, 0, C().err};
+        launch_k(C(), k_cgs_update<double, 8>, g, 256, 0, st, w, V, j + 1, N, C().gred(), gc);
+        CUDA_TRY(cudaGetLastError());
+        double ej;
+        F3R_TRY(read_abs_e(&ej));
+        last_e = ej;
+        out.res_iter++;
+        if (stop(j + 1, ej)) {
+          j++;
+          conv = true;
+          break;
+        }
+        if (j < L.m - 1) launch_k(C(), k_scale<double>, g, kEwThreads, 0, st, w, L.inv, N);
+      }
+      launch_k(C(), k_trsv_y<double>, 1, 32, 0, st, L.H, L.e, L.y, L.m + 1, j);
+      launch_k(C(), k_zy<double, double, true>, g, kEwThreads, 0, st, Zc, L.y, j, xs, nullptr, N);
+      CUDA_TRY(cudaGetLastError());
+      if (conv) solved = true;
+    }
+    if (perm_d) launch_k(C(), k_permute_scatter, g, kEwThreads, 0, st, xs, perm_d, x, N);
+    CUDA_TRY(cudaEventRecord(ev1, st));
+    out.kernel_launches = C().launches - launches0;
+    // explicit residual ||b - A x|| / ||b|| in fp64 (outside the timed region,
+    // as the drivers, f3r-gpu.cpp:99-102)
+    F3R_TRY(launch_sell(C(), A.v64, A.view(), (const double *)xs, EpiResidual<double, double>{bs, r_d, nullptr}));
+    launch_k(C(), k_dot<double, double, 8>, g, 256, 0, st, r_d, r_d, N, C().gred(), C().dscratch);
+    CUDA_TRY(cudaMemcpyAsync(C().pinned, C().dscratch, sizeof(double), cudaMemcpyDeviceToHost, st));
+    if (!x_dev) CUDA_TRY(cudaMemcpyAsync(x_user, x, sizeof(double) * N, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    F3R_TRY(C().check_device_error());
+    float ms = 0;
+    CUDA_TRY(cudaEventElapsedTime(&ms, ev0, ev1));
+    out.is_solved = solved ? 1 : 0;
+    out.res_nrm2 = last_e;
+    out.impl_rel_res = nb > 0 ? last_e / nb : last_e;
+    out.expl_rel_res = nb > 0 ? std::sqrt(C().pinned[0]) / nb : std::sqrt(C().pinned[0]);
+    out.restarts = restarts;
+    out.inner_applications = r_calls;
+    out.solve_seconds = ms * 1e-3;
+    if (res) *res = out;
+    return F3R_SUCCESS;
+  }
+};
+
+static Status make_solver(f3r_context *ctx, const f3r_csr *a, const f3r_params *pp, Solver **out) {
+  F3R_TRY(check_csr(a));
+  if (a->nrows != a->ncols) return fail(F3R_ERROR_INVALID_VALUE, "the system matrix must be square");
+  f3r_params p = *pp;
+  if (p.m_outer < 1 || p.m_outer + 1 > kMaxCols || p.m2 < 1 || p.m2 + 1 > kMaxDots || p.m3 < 1 ||
+      p.m3 + 1 > kMaxDots || p.m4 < 1 || p.m4 > kMaxM4 || p.c < 1 || p.max_restarts < 1)
+    return fail(F3R_ERROR_INVALID_VALUE,
+                "need 1 <= m_outer <= 127, 1 <= m2, m3 <= 15, 1 <= m4 <= 16, c >= 1, max_restarts >= 1");
+  if (p.sell_c != 32) return fail(F3R_ERROR_UNSUPPORTED, "only SELL slice height 32 is implemented");
+  if (p.precond != F3R_PRECOND_SDAINV && p.precond != F3R_PRECOND_ILU0_BJ)
+    return fail(F3R_ERROR_INVALID_VALUE, "unknown preconditioner");
+  if (p.half_scale_log2 < 0 || p.half_scale_log2 > 20) return fail(F3R_ERROR_INVALID_VALUE, "half_scale_log2 in [0, 20]");
+  auto s = std::make_unique<Solver>();
+  s->ctx = ctx;
+  s->p = p;
+  s->n = a->nrows;
+  const int32_t n = a->nrows;
+  CUDA_TRY(cudaSetDevice(ctx->device));
+  // system matrix in SELL-C-sigma order with all three value copies
+  SellHost h;
+  F3R_TRY(build_sell(*a, p.sell_sigma, true, h));
+  F3R_TRY(upload_sell(*ctx, h, (1 << F3R_F64) | (1 << F3R_F32) | (1 << F3R_F16), false, s->A));
+  s->perm = h.perm;
+  if (p.sell_sigma > 1) {
+    F3R_TRY(s->alloc(&s->perm_d, (size_t)std::max(n, 1)));
+    CUDA_TRY(cudaMemcpy(s->perm_d, h.perm.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice));
+  }
+  // the preconditioner, in the permuted order as well
+  HostCSR Ah(n, n, a->nnz);
+  std::memcpy(Ah.rptr.data(), a->rptr, sizeof(int32_t) * (n + 1));
+  std::memcpy(Ah.idx.data(), a->idx, sizeof(int32_t) * a->nnz);
+  std::memcpy(Ah.val.data(), a->val, sizeof(double) * a->nnz);
+  if (p.precond == F3R_PRECOND_SDAINV) {
+    HostCSR *zr = nullptr, *wr = nullptr;
+    F3R_TRY(sdainv(Ah, p.sdainv_tol, p.acc, &zr, &wr));
+    std::unique_ptr<HostCSR> Zh(zr), Wh(wr);
+    bool diag = true;
+    for (int32_t i = 0; i < n && diag; i++) {
+      diag &= (Zh->rptr[i + 1] - Zh->rptr[i] == 1 && Zh->idx[Zh->rptr[i]] == i);
+      diag &= (Wh->rptr[i + 1] - Wh->rptr[i] == 1 && Wh->idx[Wh->rptr[i]] == i);
+    }
+    if (diag) {
+      s->precond_diag = 1;
+      std::vector<double> wdv(n), zdv(n);
+      for (int32_t i = 0; i < n; i++) {
+        wdv[i] = Wh->val[Wh->rptr[h.perm[i]]];
+        zdv[i] = Zh->val[Zh->rptr[h.perm[i]]];
+      }
+      double *tmp = nullptr;
+      F3R_TRY(ctx->alloc((void **)&tmp, sizeof(double) * std::max(n, 1)));
+      F3R_TRY(s->alloc(&s->wd, (size_t)std::max(n, 1)));
+      F3R_TRY(s->alloc(&s->zd, (size_t)std::max(n, 1)));
+      CUDA_TRY(cudaMemcpy(tmp, wdv.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+      launch_k(*ctx, k_convert_vals<__half>, ctx->ew_grid(n), kEwThreads, 0, ctx->stream, tmp, s->wd, n);
+      CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+      CUDA_TRY(cudaMemcpy(tmp, zdv.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+      launch_k(*ctx, k_convert_vals<__half>, ctx->ew_grid(n), kEwThreads, 0, ctx->stream, tmp, s->zd, n);
+      CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+      cudaFree(tmp);
+    } else {
+      // W^T and Z as SELL matrices of the permuted system (same sigma order)
+      SellHost hw, hz;
+      f3r_csr wv = Wh->view(), zv = Zh->view();
+      F3R_TRY(build_sell(wv, p.sell_sigma, true, hw, &h.perm));
+      F3R_TRY(build_sell(zv, p.sell_sigma, true, hz, &h.perm));
+      F3R_TRY(upload_sell(*ctx, hw, 1 << F3R_F16, false, s->W));
+      F3R_TRY(upload_sell(*ctx, hz, 1 << F3R_F16, false, s->Z));
+    }
+  } else {
+    HostCSR *lr = nullptr, *ur = nullptr;
+    std::vector<int32_t> bptr;
+    F3R_TRY(ilu0_bj(Ah, p.ilu_blocks, p.acc, &lr, &ur, &bptr));
+    std::unique_ptr<HostCSR> Lh(lr), Uh(ur);
+    F3R_TRY(s->ilu.build(ctx->stream, *Lh, *Uh, h.perm, p.sell_sigma > 1, bptr));
+  }
+  // level storage
+  F3R_TRY(s->make_level(s->L1, p.m_outer, true));
+  F3R_TRY(s->make_level(s->L2, p.m2, true));
+  F3R_TRY(s->make_level(s->L3, p.m3, false));
+  const size_t nn = (size_t)std::max(n, 1);
+  F3R_TRY(s->alloc(&s->abs_e, 1));
+  F3R_TRY(s->alloc(&s->hin, nn));
+  F3R_TRY(s->alloc(&s->hout, nn));
+  F3R_TRY(s->alloc(&s->hout2, nn));
+  F3R_TRY(s->alloc(&s->tmp, nn));
+  F3R_TRY(s->alloc(&s->tmp2, nn));
+  F3R_TRY(s->alloc(&s->hr, nn));
+  CUDA_TRY(cudaMemset(s->tmp2, 0, nn * sizeof(__half)));
+  F3R_TRY(s->alloc(&s->rs, 1));
+  F3R_TRY(s->alloc(&s->in_slot, 1));
+  F3R_TRY(s->alloc(&s->out_slot, 1));
+  F3R_TRY(s->alloc(&s->b_d, nn));
+  F3R_TRY(s->alloc(&s->x_d, nn));
+  F3R_TRY(s->alloc(&s->r_d, nn));
+  if (s->perm_d) {
+    F3R_TRY(s->alloc(&s->bp_d, nn));
+    F3R_TRY(s->alloc(&s->xp_d, nn));
+  }
+  CUDA_TRY(cudaEventCreate(&s->ev0));
+  CUDA_TRY(cudaEventCreate(&s->ev1));
+  // every SpMV instantiation the solve may launch, configured before capture
+  Context &cx = *ctx;
+  F3R_TRY((sell_attr<double, double, EpiResidualNorm>(cx)));
+  F3R_TRY((sell_attr<double, double, EpiStore<double>>(cx)));
+  F3R_TRY((sell_attr<double, double, EpiResidual<double, double>>(cx)));
+  F3R_TRY((sell_attr<float, float, EpiStoreDots<4>>(cx)));
+  F3R_TRY((sell_attr<float, float, EpiStoreDots<8>>(cx)));
+  F3R_TRY((sell_attr<float, float, EpiStoreDots<kMaxDots>>(cx)));
+  F3R_TRY((sell_attr<__half, float, EpiStoreDots<4>>(cx)));
+  F3R_TRY((sell_attr<__half, float, EpiStoreDots<8>>(cx)));
+  F3R_TRY((sell_attr<__half, float, EpiStoreDots<kMaxDots>>(cx)));
+  F3R_TRY((sell_attr<__half, __half, EpiRichStep>(cx)));
+  F3R_TRY((sell_attr<__half, __half, EpiRichWeight>(cx)));
+  F3R_TRY((sell_attr<__half, __half, EpiRichResPre>(cx)));
+  F3R_TRY((sell_attr<__half, __half, EpiResidual<__half, __half>>(cx)));
+  F3R_TRY((sell_attr<__half, __half, EpiStore<__half>>(cx)));
+  F3R_TRY((sell_attr<__half, __half, EpiZScale>(cx)));
+  CUDA_TRY(cudaDeviceSynchronize());
+  *out = s.release();
+  return F3R_SUCCESS;
+}
+
+}  // namespace f3r
+
+struct f3r_solver {
+  f3r::Solver *s = nullptr;
+};
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+const char *f3r_last_error_string(void) { return f3r::g_err.c_str(); }
+
+const char *f3r_status_string(f3r_status s) {
+  switch (s) {
+  case F3R_SUCCESS: return "success";
+  case F3R_ERROR_INVALID_VALUE: return "invalid value";
+  case F3R_ERROR_CUDA: return "CUDA error";
+  case F3R_ERROR_OUT_OF_MEMORY: return "out of memory";
+  case F3R_ERROR_BREAKDOWN: return "breakdown";
+  case F3R_ERROR_TIMEOUT: return "device wait timed out";
+  case F3R_ERROR_UNSUPPORTED: return "unsupported";
+  case F3R_ERROR_NO_DEVICE: return "no CUDA device";
+  }
+  return "unknown status";
+}
+
+// ---- host matrices ----------------------------------------------------------
+f3r_status f3r_host_matrix_from_csr(const f3r_csr *a, f3r_host_matrix **out) {
+  if (!out) return fail(F3R_ERROR_INVALID_VALUE, "out is null");
+  F3R_TRY(check_csr(a));
+  auto *h = new f3r_host_matrix;
+  h->m.reset(new HostCSR(a->nrows, a->ncols, a->nnz));
+  std::memcpy(h->m->rptr.data(), a->rptr, sizeof(int32_t) * (a->nrows + 1));
+  if (a->nnz) {
+    std::memcpy(h->m->idx.data(), a->idx, sizeof(int32_t) * a->nnz);
+    std::memcpy(h->m->val.data(), a->val, sizeof(double) * a->nnz);
+  }
+  *out = h;
+  return F3R_SUCCESS;
+}
+f3r_status f3r_host_matrix_view(const f3r_host_matrix *m, f3r_csr *view) {
+  if (!m || !view) return fail(F3R_ERROR_INVALID_VALUE, "null argument");
+  *view = m->m->view();
+  return F3R_SUCCESS;
+}
+void f3r_host_matrix_destroy(f3r_host_matrix *m) { delete m; }
+
+f3r_status f3r_problem_stencil27(int32_t nx, int32_t ny, int32_t nz, int32_t variant, double beta,
+                                 f3r_host_matrix **out) {
+  if (!out || nx < 1 || ny < 1 || nz < 1 || variant < 0 || variant > 2)
+    return fail(F3R_ERROR_INVALID_VALUE, "stencil27: grid sizes >= 1, variant in 0..2");
+  if ((int64_t)nx * ny * nz * 27 > INT32_MAX) return fail(F3R_ERROR_UNSUPPORTED, "stencil27: nnz exceeds int32");
+  auto *h = new f3r_host_matrix;
+  h->m.reset(stencil27(nx, ny, nz, variant, beta));
+  *out = h;
+  return F3R_SUCCESS;
+}
+f3r_status f3r_problem_diffusion7(int32_t nx, int32_t ny, int32_t nz, double sigma, double corr_len, uint64_t seed,
+                                  f3r_host_matrix **out) {
+  if (!out || nx < 1 || ny < 1 || nz < 1 || sigma < 0 || corr_len < 0)
+    return fail(F3R_ERROR_INVALID_VALUE, "diffusion7: grid sizes >= 1, sigma and corr_len >= 0");
+  if ((int64_t)nx * ny * nz * 7 > INT32_MAX) return fail(F3R_ERROR_UNSUPPORTED, "diffusion7: nnz exceeds int32");
+  auto *h = new f3r_host_matrix;
+  h->m.reset(diffusion7(nx, ny, nz, sigma, corr_len, seed));
+  *out = h;
+  return F3R_SUCCESS;
+}
+f3r_status f3r_host_scaling(f3r_host_matrix *m) {
+  if (!m) return fail(F3R_ERROR_INVALID_VALUE, "null matrix");
+  scaling(*m->m);
+  return F3R_SUCCESS;
+}
+f3r_status f3r_host_spmv(const f3r_csr *a, const double *x, double *y) {
+  F3R_TRY(check_csr(a));
+  if (!x || !y) return fail(F3R_ERROR_INVALID_VALUE, "null vector");
+  host_spmv(*a, x, y);
+  return F3R_SUCCESS;
+}
+f3r_status f3r_random_uniform(uint64_t seed, double lo, double hi, int64_t n, double *out) {
+  if (!out || n < 0) return fail(F3R_ERROR_INVALID_VALUE, "bad output");
+  std::mt19937_64 eng(seed);
+  std::uniform_real_distribution<double> d(lo, hi);
+  for (int64_t i = 0; i < n; i++) out[i] = d(eng);
+  return F3R_SUCCESS;
+}
+f3r_status f3r_host_sdainv(const f3r_csr *a, double tol, double acc, f3r_host_matrix **z, f3r_host_matrix **wt) {
+  F3R_TRY(check_csr(a));
+  if (!z || !wt) return fail(F3R_ERROR_INVALID_VALUE, "null output");
+  HostCSR A(a->nrows, a->ncols, a->nnz);
+  std::memcpy(A.rptr.data(), a->rptr, sizeof(int32_t) * (a->nrows + 1));
+  std::memcpy(A.idx.data(), a->idx, sizeof(int32_t) * a->nnz);
+  std::memcpy(A.val.data(), a->val, sizeof(double) * a->nnz);
+  HostCSR *zr = nullptr, *wr = nullptr;
+  F3R_TRY(sdainv(A, tol, acc, &zr, &wr));
+  *z = new f3r_host_matrix;
+  (*z)->m.reset(zr);
+  *wt = new f3r_host_matrix;
+  (*wt)->m.reset(wr);
+  return F3R_SUCCESS;
+}
+f3r_status f3r_host_ilu0_bj(const f3r_csr *a, int32_t blocks, double acc, f3r_host_matrix **l, f3r_host_matrix **u) {
+  F3R_TRY(check_csr(a));
+  if (!l || !u) return fail(F3R_ERROR_INVALID_VALUE, "null output");
+  HostCSR A(a->nrows, a->ncols, a->nnz);
+  std::memcpy(A.rptr.data(), a->rptr, sizeof(int32_t) * (a->nrows + 1));
+  std::memcpy(A.idx.data(), a->idx, sizeof(int32_t) * a->nnz);
+  std::memcpy(A.val.data(), a->val, sizeof(double) * a->nnz);
+  HostCSR *lr = nullptr, *ur = nullptr;
+  F3R_TRY(ilu0_bj(A, blocks, acc, &lr, &ur, nullptr));
+  *l = new f3r_host_matrix;
+  (*l)->m.reset(lr);
+  *u = new f3r_host_matrix;
+  (*u)->m.reset(ur);
+  return F3R_SUCCESS;
+}
+
+// ---- context ----------------------------------------------------------------
+f3r_status f3r_context_create(int32_t device, f3r_context **out) {
+  if (!out) return fail(F3R_ERROR_INVALID_VALUE, "out is null");
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+    cudaGetLastError();
+    return fail(F3R_ERROR_NO_DEVICE, "no CUDA device is visible");
+  }
+  if (device < 0 || device >= count) return fail(F3R_ERROR_INVALID_VALUE, "device ordinal out of range");
+  CUDA_TRY(cudaSetDevice(device));
+  int major = 0;
+  CUDA_TRY(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device));
+  if (major != 10) return fail(F3R_ERROR_UNSUPPORTED, "this library is built for sm_100a (B200) only");
+  auto c = std::make_unique<f3r_context>();
+  c->device = device;
+  CUDA_TRY(cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device));
+  CUDA_TRY(cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking));
+  c->stream = c->own;
+  F3R_TRY(c->alloc((void **)&c->err, sizeof(int)));
+  F3R_TRY(c->alloc(&c->partials, kPartialBytes));
+  F3R_TRY(c->alloc((void **)&c->ticket, sizeof(unsigned int) * 4));
+  F3R_TRY(c->alloc((void **)&c->dscratch, sizeof(double) * 4));
+  CUDA_TRY(cudaMemset(c->err, 0, sizeof(int)));
+  CUDA_TRY(cudaMemset(c->ticket, 0, sizeof(unsigned int) * 4));
+  CUDA_TRY(cudaHostAlloc((void **)&c->pinned, sizeof(double) * 8, cudaHostAllocDefault));
+  *out = c.release();
+  return F3R_SUCCESS;
+}
+void f3r_context_destroy(f3r_context *ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  cudaFree(ctx->err);
+  cudaFree(ctx->partials);
+  cudaFree(ctx->ticket);
+  cudaFree(ctx->dscratch);
+  cudaFreeHost(ctx->pinned);
+  if (ctx->own) cudaStreamDestroy(ctx->own);
+  delete ctx;
+}
+f3r_status f3r_context_set_stream(f3r_context *ctx, void *stream) {
+  if (!ctx) return fail(F3R_ERROR_INVALID_VALUE, "null context");
+  ctx->stream = stream ? (cudaStream_t)stream : ctx->own;
+  return F3R_SUCCESS;
+}
+f3r_status f3r_context_synchronize(f3r_context *ctx) {
+  if (!ctx) return fail(F3R_ERROR_INVALID_VALUE, "null context");
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  return ctx->check_device_error();
+}
+
+// ---- SELL -------------------------------------------------------------------
+f3r_status f3r_sell_create(f3r_context *ctx, const f3r_csr *a, int32_t slice_height, int32_t sigma,
+                           int32_t dtype_mask, f3r_sell **out) {
+  if (!ctx || !out) return fail(F3R_ERROR_INVALID_VALUE, "null argument");
+  if (slice_height != 32) return fail(F3R_ERROR_UNSUPPORTED, "only slice height 32 is implemented");
+  if ((dtype_mask & 7) == 0 || (dtype_mask & ~7)) return fail(F3R_ERROR_INVALID_VALUE, "dtype_mask must select f64/f32/f16");
+  F3R_TRY(check_csr(a));
+  CUDA_TRY(cudaSetDevice(ctx->device));
+  SellHost h;
+  F3R_TRY(build_sell(*a, sigma, false, h));
+  auto m = std::make_unique<f3r_sell>();
+  m->ctx = ctx;
+  Status s = upload_sell(*ctx, h, dtype_mask, true, m->d);
+  if (s != F3R_SUCCESS) {
+    m->d.release();
+    return s;
+  }
+  *out = m.release();
+  return F3R_SUCCESS;
+}
+f3r_status f3r_sell_info_get(const f3r_sell *m, f3r_sell_info *info) {
+  if (!m || !info) return fail(F3R_ERROR_INVALID_VALUE, "null argument");
+  info->nrows = m->d.n;
+  info->ncols = m->d.ncols;
+  info->nnz = (int32_t)m->d.nnz;
+  info->slice_height = 32;
+  info->sigma = m->d.sigma;
+  info->nslices = m->d.nslices;
+  info->nnz_padded = m->d.nnz_pad;
+  info->max_width = m->d.max_width;
+  info->dtypes = m->d.dtypes;
+  return F3R_SUCCESS;
+}
+void f3r_sell_destroy(f3r_sell *m) {
+  if (!m) return;
+  cudaSetDevice(m->ctx->device);
+  cudaStreamSynchronize(m->ctx->stream);
+  m->d.release();
+  delete m;
+}
+
+f3r_status f3r_sell_operate(f3r_sell *m, f3r_dtype val_t, f3r_dtype in_t, const void *in, f3r_dtype out_t, void *out) {
+  if (!m || !in || !out) return fail(F3R_ERROR_INVALID_VALUE, "null argument");
+  Context &c = *m->ctx;
+  const DeviceSell &d = m->d;
+  if (!(d.dtypes & (1 << val_t))) return fail(F3R_ERROR_INVALID_VALUE, "matrix holds no copy of that value type");
+  const DevSell A = d.view();
+  if (val_t == F3R_F64 && in_t == F3R_F64 && out_t == F3R_F64)
+    return launch_sell(c, d.v64, A, (const double *)in, EpiStore<double>{(double *)out, A.perm});
+  if (val_t == F3R_F32 && in_t == F3R_F32 && out_t == F3R_F32)
+    return launch_sell(c, d.v32, A, (const float *)in, EpiStore<float>{(float *)out, A.perm});
+  if (val_t == F3R_F16 && in_t == F3R_F32 && out_t == F3R_F32)
+    return launch_sell(c, d.v16, A, (const float *)in, EpiStore<float>{(float *)out, A.perm});
+  if (val_t == F3R_F16 && in_t == F3R_F16 && out_t == F3R_F16)
+    return launch_sell(c, d.v16, A, (const __half *)in, EpiStore<__half>{(__half *)out, A.perm});
+  if (val_t == F3R_F16 && in_t == F3R_F16 && out_t == F3R_F32)
+    return launch_sell(c, d.v16, A, (const __half *)in, EpiStore<float>{(float *)out, A.perm});
+  return fail(F3R_ERROR_UNSUPPORTED, "unsupported (val, in, out) type combination");
+}
+
+f3r_status f3r_sell_compute_residual(f3r_sell *m, f3r_dtype val_t, f3r_dtype rhs_t, const void *rhs, f3r_dtype in_t,
+                                     const void *in, f3r_dtype res_t, void *res) {
+  if (!m || !rhs || !in || !res) return fail(F3R_ERROR_INVALID_VALUE, "null argument");
+  Context &c = *m->ctx;
+  const DeviceSell &d = m->d;
+  if (!(d.dtypes & (1 << val_t))) return fail(F3R_ERROR_INVALID_VALUE, "matrix holds no copy of that value type");
+  const DevSell A = d.view();
+  if (val_t == F3R_F64 && rhs_t == F3R_F64 && in_t == F3R_F64 && res_t == F3R_F64)
+    return launch_sell(c, d.v64, A, (const double *)in, EpiResidual<double, double>{(const double *)rhs, (double *)res, A.perm});
+  if (val_t == F3R_F32 && rhs_t == F3R_F32 && in_t == F3R_F32 && res_t == F3R_F32)
+    return launch_sell(c, d.v32, A, (const float *)in, EpiResidual<float, float>{(const float *)rhs, (float *)res, A.perm});
+  if (val_t == F3R_F16 && rhs_t == F3R_F16 && in_t == F3R_F16 && res_t == F3R_F16)
+    return launch_sell(c, d.v16, A, (const __half *)in, EpiResidual<__half, __half>{(const __half *)rhs, (__half *)res, A.perm});
+  return fail(F3R_ERROR_UNSUPPORTED, "unsupported (val, rhs, in, res) type combination");
+}
+
+f3r_status f3r_dot(f3r_context *ctx, f3r_dtype t, int64_t n, const void *x, const void *y, double *result) {
+  if (!ctx || !result || n < 0 || (n > 0 && (!x || !y))) return fail(F3R_ERROR_INVALID_VALUE, "bad argument");
+  Context &c = *ctx;
+  const int g = c.ew_grid(n);
+  if (t == F3R_F64) {
+    launch_k(c, k_dot<double, double, 8>, g, 256, 0, c.stream, (const double *)x, (const double *)y, n, c.gred(), c.dscratch);
+  } else if (t == F3R_F32) {
+    launch_k(c, k_dot<float, float, 8>, g, 256, 0, c.stream, (const float *)x, (const float *)y, n, c.gred(), (float *)c.dscratch);
+  } else {
+    launch_k(c, k_dot<__half, float, 8>, g, 256, 0, c.stream, (const __half *)x, (const __half *)y, n, c.gred(), (float *)c.dscratch);
+  }
+  CUDA_TRY(cudaGetLastError());
+  CUDA_TRY(cudaMemcpyAsync(c.pinned, c.dscratch, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+  CUDA_TRY(cudaStreamSynchronize(c.stream));
+  if (t == F3R_F64) *result = c.pinned[0];
+  else {
+    float f;
+    std::memcpy(&f, c.pinned, sizeof(float));
+    *result = f;
+  }
+  return F3R_SUCCESS;
+}
+
+// ---- solver -----------------------------------------------------------------
+void f3r_params_default(f3r_params *p) {
+  if (!p) return;
+  std::memset(p, 0, sizeof(*p));
+  p->m_outer = 100;
+  p->max_restarts = 20;
+  p->m2 = 8;
+  p->m3 = 4;
+  p->m4 = 2;
+  p->c = 64;
+  p->precond = F3R_PRECOND_SDAINV;
+  p->ilu_blocks = 112;
+  p->sdainv_tol = 0.1;
+  p->acc = 1.0;
+  p->sell_c = 32;
+  p->sell_sigma = 1;
+  p->rel_tol = 1e-8;
+  p->half_scale_log2 = 0;
+  p->use_graphs = 1;
+}
+
+f3r_status f3r_solver_create(f3r_context *ctx, const f3r_csr *a, const f3r_params *p, f3r_solver **out) {
+  if (!ctx || !a || !p || !out) return fail(F3R_ERROR_INVALID_VALUE, "null argument");
+  Solver *s = nullptr;
+  F3R_TRY(make_solver(ctx, a, p, &s));
+  *out = new f3r_solver{s};
+  return F3R_SUCCESS;
+}
+f3r_status f3r_solver_solve(f3r_solver *s, const double *b, double *x, f3r_cond_fn cond, void *user,
+                            f3r_result *result) {
+  if (!s || !b || !x) return fail(F3R_ERROR_INVALID_VALUE, "null argument");
+  CUDA_TRY(cudaSetDevice(s->s->ctx->device));
+  return s->s->solve(b, x, cond, user, result);
+}
+f3r_status f3r_solver_info(const f3r_solver *s, f3r_sell_info *a_info, int32_t *precond_diagonal) {
+  if (!s) return fail(F3R_ERROR_INVALID_VALUE, "null solver");
+  if (a_info) {
+    const DeviceSell &d = s->s->A;
+    a_info->nrows = d.n;
+    a_info->ncols = d.ncols;
+    a_info->nnz = (int32_t)d.nnz;
+    a_info->slice_height = 32;
+    a_info->sigma = d.sigma;
+    a_info->nslices = d.nslices;
+    a_info->nnz_padded = d.nnz_pad;
+    a_info->max_width = d.max_width;
+    a_info->dtypes = d.dtypes;
+  }
+  if (precond_diagonal) *precond_diagonal = s->s->precond_diag;
+  return F3R_SUCCESS;
+}
+void f3r_solver_destroy(f3r_solver *s) {
+  if (!s) return;
+  cudaSetDevice(s->s->ctx->device);
+  cudaStreamSynchronize(s->s->ctx->stream);
+  delete s->s;
+  delete s;
+}
+
+}  // extern "C"

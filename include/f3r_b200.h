@@ -1,0 +1,229 @@
+/*
+ * f3r_b200.h -- C ABI of the B200-native nested mixed-precision F3R solver.
+ *
+ * The reference (suzuki-hpc/F3R) has no C interface: its plugin surface is the
+ * type-erased C++ concepts in library/umineko-sparse/models.hpp
+ * (Operator / CoefficientMatrix / Solver, solve(b, x, cond) -> solve_res_t),
+ * and the F3R method itself is assembled in the experiment drivers
+ * (work/src/f3r-gpu.cpp:210-265, work/src/f3r.cpp:195-248).  Each entry point
+ * below names the reference interface it replaces.  A C++ adapter with the
+ * reference's names lives in f3r_b200.hpp.
+ *
+ * Conventions
+ *  - Every function returns an f3r_status; nothing calls exit().  The reference
+ *    prints and exits on bad input (matrix/io.hpp:255-256, csr.hpp:111-114).
+ *  - f3r_last_error_string() gives a message for the last failure on the
+ *    calling thread.
+ *  - Matrices cross the boundary as host CSR (f3r_csr, borrowed for the call).
+ *    idx_t is int32 as in the reference (core/interface.hpp:8).
+ *  - Device objects belong to an f3r_context (one device, one CUDA stream).
+ *    Objects are not thread-safe; different contexts may run concurrently.
+ *  - Vectors passed to f3r_sell_* / f3r_dot are device pointers.  The solve
+ *    call accepts host or device pointers for b and x.
+ */
+#ifndef F3R_B200_H
+#define F3R_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define F3R_B200_VERSION_MAJOR 0
+#define F3R_B200_VERSION_MINOR 1
+
+typedef enum f3r_status {
+  F3R_SUCCESS = 0,
+  F3R_ERROR_INVALID_VALUE = 1,  /* bad argument, shape or parameter */
+  F3R_ERROR_CUDA = 2,           /* a CUDA runtime call failed */
+  F3R_ERROR_OUT_OF_MEMORY = 3,
+  F3R_ERROR_BREAKDOWN = 5,      /* zero or non-finite norm in an Arnoldi step */
+  F3R_ERROR_TIMEOUT = 7,        /* a bounded device wait gave up */
+  F3R_ERROR_UNSUPPORTED = 8,
+  F3R_ERROR_NO_DEVICE = 9
+} f3r_status;
+
+typedef enum f3r_dtype { F3R_F64 = 0, F3R_F32 = 1, F3R_F16 = 2 } f3r_dtype;
+
+typedef enum f3r_precond {
+  F3R_PRECOND_SDAINV = 0,  /* SDAINV Z*(W^T r), as work/src/f3r-gpu.cpp:74,215-216 */
+  F3R_PRECOND_ILU0_BJ = 1  /* block-Jacobi ILU(0), as work/src/f3r.cpp:57-58,200-201 */
+} f3r_precond;
+
+/* Host CSR matrix, borrowed for the duration of a call.  Rows sorted by
+ * column.  Replaces kmm::CSR<double, host> (matrix/csr.hpp:12-30). */
+typedef struct f3r_csr {
+  int32_t nrows, ncols, nnz;
+  const int32_t *rptr; /* nrows + 1 */
+  const int32_t *idx;  /* nnz */
+  const double *val;   /* nnz */
+} f3r_csr;
+
+/* Solver parameters; defaults as the F3R drivers (f3r_params_default). */
+typedef struct f3r_params {
+  int32_t m_outer;         /* outer fp64 FGMRES restart length: 100 (f3r-gpu.cpp:264) */
+  int32_t max_restarts;    /* Restarted cap: 20 (f3r-gpu.cpp:265) */
+  int32_t m2, m3, m4;      /* fp32 level, fp16-matrix level, Richardson steps: 8, 4, 2 */
+  int32_t c;               /* adaptive-weight period: 64 (suite-gpu.py:49) */
+  int32_t precond;         /* f3r_precond */
+  int32_t ilu_blocks;      /* block-Jacobi blocks: 112 (f3r.cpp:57) */
+  double sdainv_tol;       /* drop tolerance: 0.1 (f3r-gpu.cpp:74) */
+  double acc;              /* diagonal shift for SDAINV / ILU: 1.0 */
+  int32_t sell_c;          /* SELL slice height: 32 (the only one the kernels take) */
+  int32_t sell_sigma;      /* SELL sorting window: 1 = no sorting */
+  double rel_tol;          /* stop when |implicit residual| / ||b|| < rel_tol and no
+                              cond callback is given: 1e-8 (f3r-gpu.cpp:18) */
+  int32_t half_scale_log2; /* 0: plain fp32->fp16 cast of the Richardson input, as the
+                              reference (f3r-gpu.cpp:231); k>0: scale it by 2^k and
+                              back (a linear operator, so the result is unchanged in
+                              exact arithmetic) */
+  int32_t use_graphs;      /* 1: replay the fixed inner levels as CUDA graphs */
+  int32_t reserved[8];
+} f3r_params;
+
+/* Solve outcome.  The first three fields are solve_res_t
+ * (umineko-sparse/models.hpp:191-200). */
+typedef struct f3r_result {
+  int32_t is_solved;
+  int32_t res_iter;          /* outer FGMRES steps over all restarts */
+  double res_nrm2;           /* |e| of the last Givens estimate (absolute) */
+  double impl_rel_res;       /* res_nrm2 / ||b|| */
+  double expl_rel_res;       /* ||b - A x|| / ||b|| recomputed in fp64 */
+  int32_t restarts;          /* outer FGMRES calls */
+  int32_t reserved0;
+  int64_t inner_applications;/* Richardson applications (the reference's Iter) */
+  double solve_seconds;      /* device time of the solve (CUDA events) */
+  int64_t kernel_launches;   /* kernels of this library the solve ran (graph nodes included) */
+} f3r_result;
+
+/* cond(i, |e|): nonzero stops the solve; the reference's
+ * std::function<bool(int, double)> (models.hpp:208-211). */
+typedef int (*f3r_cond_fn)(int32_t iter, double res_nrm2, void *user);
+
+typedef struct f3r_host_matrix f3r_host_matrix;
+typedef struct f3r_context f3r_context;
+typedef struct f3r_sell f3r_sell;
+typedef struct f3r_solver f3r_solver;
+
+typedef struct f3r_sell_info {
+  int32_t nrows, ncols, nnz;
+  int32_t slice_height, sigma, nslices;
+  int64_t nnz_padded;       /* stored entries including slice padding */
+  int32_t max_width;        /* widest slice (entries per row) */
+  int32_t dtypes;           /* bit (1 << f3r_dtype) set for each value copy held */
+} f3r_sell_info;
+
+/* ---------------------------------------------------------------- errors */
+const char *f3r_last_error_string(void);
+const char *f3r_status_string(f3r_status s);
+
+/* ------------------------------------------------------- host matrices
+ * Host-side set-up, native C++.  The reference does all of this on the host
+ * too (matrix/algorithm.hpp, preconditioner/ainv.hpp, preconditioner/ilu.hpp). */
+f3r_status f3r_host_matrix_from_csr(const f3r_csr *a, f3r_host_matrix **out);
+f3r_status f3r_host_matrix_view(const f3r_host_matrix *m, f3r_csr *view);
+void f3r_host_matrix_destroy(f3r_host_matrix *m);
+
+/* 27-point stencil on an nx*ny*nz grid (diagonal 26, neighbours -1).
+ * variant 0: matrix/hpcg.cpp:13-57.  1: matrix/hpgmp.cpp:13-57 (pure +-z
+ * neighbours -1-beta / -1+beta).  2: half-space nonsymmetric form (neighbours
+ * at a positive linear offset -1+beta, negative -1-beta).  Any grid size. */
+f3r_status f3r_problem_stencil27(int32_t nx, int32_t ny, int32_t nz, int32_t variant,
+                                 double beta, f3r_host_matrix **out);
+
+/* 7-point variable-coefficient diffusion: face coefficient = harmonic mean of
+ * exp(g) of the two cells, g a seeded Gaussian random field (std sigma,
+ * correlation length corr_len cells), Dirichlet boundary folded into the
+ * diagonal.  No reference counterpart (a synthetic stress matrix). */
+f3r_status f3r_problem_diffusion7(int32_t nx, int32_t ny, int32_t nz, double sigma,
+                                  double corr_len, uint64_t seed, f3r_host_matrix **out);
+
+/* D^{-1/2} A D^{-1/2} with D = |diag(A)|, in place.  Replaces
+ * kmm::algorithm::scaling (matrix/algorithm.hpp:45-59). */
+f3r_status f3r_host_scaling(f3r_host_matrix *m);
+
+/* y = A x on the host in fp64 (set-up of right-hand sides b = A x*). */
+f3r_status f3r_host_spmv(const f3r_csr *a, const double *x, double *y);
+
+/* n values uniform in [lo, hi) from std::mt19937_64(seed), the generator
+ * the reference uses for right-hand sides (matrix/io.hpp:112-118,
+ * core/tensor.hpp:253-265). */
+f3r_status f3r_random_uniform(uint64_t seed, double lo, double hi, int64_t n, double *out);
+
+/* SDAINV factors: returns Z and W^T so that M r = Z (W^T r).  Replaces
+ * kmm::algorithm::sdainv (preconditioner/ainv.hpp:27-65, 268-329). */
+f3r_status f3r_host_sdainv(const f3r_csr *a, double tol, double acc, f3r_host_matrix **z,
+                           f3r_host_matrix **wt);
+
+/* Block-Jacobi ILU(0): L (unit diagonal stored last in each row) and U
+ * (diagonal first).  Replaces CSR::duplicate_block_diagonal + algorithm::ilup
+ * + algorithm::split (csr.hpp:109-155, ilu.hpp:128-164, algorithm.hpp:9-43).
+ * Rejects block counts for which the reference's block pointers overrun
+ * ((blocks-1) * ceil(n/blocks) > n). */
+f3r_status f3r_host_ilu0_bj(const f3r_csr *a, int32_t blocks, double acc, f3r_host_matrix **l,
+                            f3r_host_matrix **u);
+
+/* ---------------------------------------------------------------- context */
+f3r_status f3r_context_create(int32_t device, f3r_context **out);
+void f3r_context_destroy(f3r_context *ctx);
+/* Use an external CUDA stream (cudaStream_t) instead of the context's own;
+ * NULL restores the context's stream. */
+f3r_status f3r_context_set_stream(f3r_context *ctx, void *stream);
+f3r_status f3r_context_synchronize(f3r_context *ctx);
+
+/* -------------------------------------------------------- SELL-C-sigma
+ * Device sparse matrix.  Replaces kmm::SELL<32, T, device> (matrix/sell.hpp:
+ * 37-97) and SELLsig<32, sigma, T, device> (sell.hpp:99-166).  One column
+ * index array is shared by the fp64 / fp32 / fp16 value copies selected by
+ * dtype_mask (bit 1 << f3r_dtype). */
+f3r_status f3r_sell_create(f3r_context *ctx, const f3r_csr *a, int32_t slice_height,
+                           int32_t sigma, int32_t dtype_mask, f3r_sell **out);
+f3r_status f3r_sell_info_get(const f3r_sell *m, f3r_sell_info *info);
+void f3r_sell_destroy(f3r_sell *m);
+
+/* out = A in, values at val_t, accumulation in fp64 for fp64 values and fp32
+ * otherwise.  Replaces SELL::operate (sell.hpp:56-71) / CoefficientMatrix::
+ * operate (models.hpp:133-136).  Supported (val_t, in_t, out_t): (F64, F64,
+ * F64), (F32, F32, F32), (F16, F32, F32), (F16, F16, F16), (F16, F16, F32). */
+f3r_status f3r_sell_operate(f3r_sell *m, f3r_dtype val_t, f3r_dtype in_t, const void *in,
+                            f3r_dtype out_t, void *out);
+
+/* res = rhs - A in.  Replaces SELL::compute_residual (sell.hpp:72-89) /
+ * CoefficientMatrix::compute_residual (models.hpp:137-141).  Supported:
+ * all three types equal to val_t's vector type (F64/F64, F32/F32, F16/F16). */
+f3r_status f3r_sell_compute_residual(f3r_sell *m, f3r_dtype val_t, f3r_dtype rhs_t,
+                                     const void *rhs, f3r_dtype in_t, const void *in,
+                                     f3r_dtype res_t, void *res);
+
+/* *result = <x, y> over n entries (fp64 for F64, fp32 accumulation otherwise;
+ * F16 inputs are widened to fp32 as the reference's wildcard(., tof32),
+ * f3r-gpu.cpp:236).  Replaces kmm::dot (core/tensor.hpp:509-537, 686-688).
+ * Synchronises the context's stream. */
+f3r_status f3r_dot(f3r_context *ctx, f3r_dtype t, int64_t n, const void *x, const void *y,
+                   double *result);
+
+/* ----------------------------------------------------------------- solver
+ * The nested F3R solver: Restarted<double>( FGMRES<double>(A, FGMRES<float>(
+ * A32, FGMRES<float>(A16, R, m3), m2), m_outer), max_restarts ), with R the
+ * adaptive-weight fp16 Richardson over the preconditioner (f3r-gpu.cpp:
+ * 229-265).  `a` is the system matrix as solved (apply f3r_host_scaling first
+ * to match the drivers, f3r-gpu.cpp:65).  The preconditioner is built here. */
+void f3r_params_default(f3r_params *p);
+f3r_status f3r_solver_create(f3r_context *ctx, const f3r_csr *a, const f3r_params *p,
+                             f3r_solver **out);
+/* Solve A x = b.  x holds the initial guess on entry.  b and x may be host
+ * or device pointers.  cond may be NULL (then rel_tol applies).  Replaces
+ * Restarted::solve / Solver::solve (solver/restart.hpp:26-36,
+ * models.hpp:207-211). */
+f3r_status f3r_solver_solve(f3r_solver *s, const double *b, double *x, f3r_cond_fn cond,
+                            void *user, f3r_result *result);
+f3r_status f3r_solver_info(const f3r_solver *s, f3r_sell_info *a_info, int32_t *precond_diagonal);
+void f3r_solver_destroy(f3r_solver *s);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* F3R_B200_H */

@@ -1,0 +1,141 @@
+"""Nested F3R solves on the GPU against the oracle's restatement and the
+reference's own solve (compiled in place, run on the host)."""
+import numpy as np
+import pytest
+import torch
+
+import f3r_b200 as F
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    return F.Context(0)
+
+
+def system(nx, variant=2, seed=0):
+    A = F.stencil27(nx, nx, nx, variant, 0.5).scale()
+    n = A.shape[0]
+    xs = F.random_uniform(seed, -1.0, 1.0, n)
+    b = A.spmv(xs)
+    return A, b, xs
+
+
+def oracle_solve(A, b, precond=O.PRECOND_SDAINV, blocks=16, **kw):
+    rptr, idx, val = A.arrays()
+    M = O.Mat.from_csr(rptr, idx, val)
+    if precond == O.PRECOND_SDAINV:
+        Z, W = O.sdainv(M)
+        P1, P2 = W, Z
+    else:
+        P1, P2 = O.ilu0_bj(M, blocks)
+    p = O.params(precond=precond, **kw)
+    return O.f3r_solve(M, P1, P2, b, p)
+
+
+@pytest.mark.parametrize("nx,graphs", [(16, 1), (24, 0), (32, 1)])
+def test_solve_matches_oracle(ctx, nx, graphs):
+    A, b, xs = system(nx)
+    S = F.Solver(ctx, A, rel_tol=1e-10, use_graphs=graphs)
+    x = np.zeros_like(b)
+    r = S.solve(b, x)
+    o = oracle_solve(A, b, tol=1e-10)
+    assert r.is_solved and o["solved"]
+    assert r.expl_rel_res <= 1e-10
+    assert abs(r.res_iter - o["iters"]) <= 1
+    assert r.inner_applications == r.res_iter * 32
+    assert np.linalg.norm(x - xs) / np.linalg.norm(xs) < 1e-7
+
+
+def test_solve_matches_reference(ctx):
+    ref = O.Ref("golden")
+    A, b, _ = system(24, variant=1)
+    rptr, idx, val = A.arrays()
+    rr = ref.f3r_solve(0, rptr, idx, val, b, tol=1e-10)
+    S = F.Solver(ctx, A, rel_tol=1e-10)
+    x = np.zeros_like(b)
+    r = S.solve(b, x)
+    assert rr["solved"] and r.is_solved
+    assert abs(r.res_iter - rr["iters"]) <= 1
+    assert r.expl_rel_res <= 1e-10
+
+
+def test_history_and_cond(ctx):
+    A, b, _ = system(20)
+    seen = []
+
+    def cond(i, e):
+        seen.append((i, e))
+        return e / np.linalg.norm(b) < 1e-9
+
+    S = F.Solver(ctx, A)
+    x = np.zeros_like(b)
+    r = S.solve(b, x, cond)
+    assert r.is_solved
+    assert seen[0][0] == 0 and [s[0] for s in seen[1:]] == list(range(1, len(seen)))
+    o = oracle_solve(A, b, tol=1e-9)
+    got = np.array([e for _, e in seen[1:]]) / np.linalg.norm(b)
+    assert len(got) == len(o["hist"]) or abs(len(got) - len(o["hist"])) <= 1
+    k = min(len(got), len(o["hist"]))
+    # first outer step: same residual reduction within fp16 noise
+    assert abs(np.log10(got[0]) - np.log10(o["hist"][0])) < 0.5
+
+
+def test_device_pointers_and_x0(ctx):
+    A, b, xs = system(16)
+    S = F.Solver(ctx, A, rel_tol=1e-10)
+    bt = torch.from_numpy(b).cuda()
+    xt = torch.zeros_like(bt)
+    r = S.solve(bt, xt)
+    assert r.is_solved and r.expl_rel_res <= 1e-10
+    # warm start from the solution: converged at step 0
+    r2 = S.solve(bt, xt)
+    assert r2.is_solved and r2.res_iter == 0
+
+
+@pytest.mark.parametrize("sigma", [1, 256])
+def test_sigma_and_m4(ctx, sigma):
+    A, b, xs = system(20)
+    for m4 in (1, 2, 3):
+        S = F.Solver(ctx, A, rel_tol=1e-10, sell_sigma=sigma, m4=m4, c=4)
+        x = np.zeros_like(b)
+        r = S.solve(b, x)
+        o = oracle_solve(A, b, tol=1e-10, m4=m4, c=4)
+        assert r.is_solved and r.expl_rel_res <= 1e-10, (sigma, m4)
+        assert abs(r.res_iter - o["iters"]) <= 1, (sigma, m4, r.res_iter, o["iters"])
+
+
+def test_general_sdainv(ctx):
+    """non-diagonal SDAINV factors (log-normal diffusion) through SELL SpMVs"""
+    A = F.diffusion7(16, 16, 16, 1.5, 3.0, 3).scale()
+    n = A.shape[0]
+    xs = F.random_uniform(1, -1, 1, n)
+    b = A.spmv(xs)
+    S = F.Solver(ctx, A, rel_tol=1e-10, c=8)
+    _, diag = S.info()
+    assert not diag
+    x = np.zeros_like(b)
+    r = S.solve(b, x)
+    o = oracle_solve(A, b, tol=1e-10, c=8)
+    assert r.is_solved and r.expl_rel_res <= 1e-10
+    assert abs(r.res_iter - o["iters"]) <= max(1, 0.1 * o["iters"])
+
+
+def test_ilu_bj(ctx):
+    A, b, xs = system(16, variant=0)
+    S = F.Solver(ctx, A, rel_tol=1e-10, precond=F.PRECOND_ILU0_BJ, ilu_blocks=16)
+    x = np.zeros_like(b)
+    r = S.solve(b, x)
+    o = oracle_solve(A, b, precond=O.PRECOND_ILU0_BJ, blocks=16, tol=1e-10)
+    assert r.is_solved and r.expl_rel_res <= 1e-10
+    assert abs(r.res_iter - o["iters"]) <= 1
+
+
+def test_invalid_params(ctx):
+    A = F.stencil27(8, 8, 8).scale()
+    with pytest.raises(F.F3RError):
+        F.Solver(ctx, A, m2=40)
+    with pytest.raises(F.F3RError):
+        F.Solver(ctx, A, precond=F.PRECOND_ILU0_BJ, ilu_blocks=112)

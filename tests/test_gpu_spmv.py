@@ -1,0 +1,144 @@
+"""SELL-32(-sigma) SpMV / residual / dot on the GPU against the oracle.
+
+The oracle's fma-chain SpMV in stored column order is the CUDA kernel's exact
+arithmetic, so fp64 and fp32 results must agree bit for bit, and fp16 results
+(fp32 accumulation, one rounding at the store) as well.  The reference's own
+fp16-accumulating SpMV is compared within the bound nnz_row * 2^-11 * |A||x|.
+"""
+import numpy as np
+import pytest
+import torch
+
+import f3r_b200 as F
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    return F.Context(0)
+
+
+def ragged_matrix(n=1000, m=None, seed=0, empty_every=7):
+    """random sparse matrix with empty rows and rows of very different lengths"""
+    m = n if m is None else m
+    rng = np.random.default_rng(seed)
+    rptr = [0]
+    idx, val = [], []
+    for i in range(n):
+        k = 0 if i % empty_every == 3 else int(rng.integers(1, 70 if i % 97 == 0 else 12))
+        cols = np.sort(rng.choice(m, size=min(k, m), replace=False))
+        idx.extend(cols.tolist())
+        val.extend(rng.standard_normal(len(cols)).tolist())
+        rptr.append(len(idx))
+    return np.array(rptr, np.int32), np.array(idx, np.int32), np.array(val)
+
+
+CASES = [("stencil", None), ("ragged", None)]
+
+
+def matrices():
+    A = F.stencil27(12, 13, 11, 2, 0.5).scale()
+    yield "stencil27", A
+    yield "ragged", F.HostMatrix.from_csr(*ragged_matrix(1000))
+    yield "ragged_odd", F.HostMatrix.from_csr(*ragged_matrix(77, seed=3))
+    yield "diffusion7", F.diffusion7(10, 9, 8, 2.5, 3.0, 1).scale()
+
+
+@pytest.mark.parametrize("sigma", [1, 256])
+def test_operate_bitexact(ctx, sigma):
+    for name, A in matrices():
+        rptr, idx, val = A.arrays()
+        n = A.shape[0]
+        S = F.Sell(ctx, A, sigma=sigma)
+        rng = np.random.default_rng(1)
+        x64 = rng.standard_normal(n)
+        x32 = x64.astype(np.float32)
+        x16 = (x64 * 0.25).astype(np.float16)
+        cases = [
+            (F.F64, x64, torch.float64, O.DT_F64, O.DT_F64, O.DT_F64),
+            (F.F32, x32, torch.float32, O.DT_F32, O.DT_F32, O.DT_F32),
+            (F.F16, x32, torch.float32, O.DT_F16, O.DT_F32, O.DT_F32),
+            (F.F16, x16, torch.float16, O.DT_F16, O.DT_F16, O.DT_F32),
+        ]
+        for vt, x, ydt, ov, oy, oacc in cases:
+            xt = torch.from_numpy(x).cuda()
+            yt = torch.zeros(n, dtype=ydt, device="cuda")
+            S.operate(xt, yt, val_t=vt)
+            torch.cuda.synchronize()
+            ref = O.spmv(rptr, idx, val, x, ov, oy, oacc)
+            assert np.array_equal(yt.cpu().numpy().view(np.uint8), ref.view(np.uint8)), (name, vt, x.dtype)
+        # fp16 vector output
+        xt = torch.from_numpy(x16).cuda()
+        yt = torch.zeros(n, dtype=torch.float16, device="cuda")
+        S.operate(xt, yt)
+        torch.cuda.synchronize()
+        ref = O.spmv(rptr, idx, val, x16, O.DT_F16, O.DT_F16, O.DT_F32)
+        assert np.array_equal(yt.cpu().numpy().view(np.uint16), ref.view(np.uint16)), name
+        info = S.info()
+        assert info.nrows == n and info.nnz == len(idx) and info.nnz_padded >= len(idx)
+        S.close()
+
+
+@pytest.mark.parametrize("sigma", [1, 32])
+def test_residual_bitexact(ctx, sigma):
+    for name, A in matrices():
+        rptr, idx, val = A.arrays()
+        n = A.shape[0]
+        S = F.Sell(ctx, A, sigma=sigma)
+        rng = np.random.default_rng(2)
+        for dt, odt in ((np.float64, O.DT_F64), (np.float32, O.DT_F32), (np.float16, O.DT_F16)):
+            x = (rng.standard_normal(n) * 0.1).astype(dt)
+            b = rng.standard_normal(n).astype(dt)
+            tdt = {np.float64: torch.float64, np.float32: torch.float32, np.float16: torch.float16}[dt]
+            r = torch.zeros(n, dtype=tdt, device="cuda")
+            S.compute_residual(torch.from_numpy(b).cuda(), torch.from_numpy(x).cuda(), r)
+            torch.cuda.synchronize()
+            acc = O.DT_F64 if dt == np.float64 else O.DT_F32
+            ref = O.spmv(rptr, idx, val, x, odt, odt, acc, b=b)
+            assert np.array_equal(r.cpu().numpy().view(np.uint8), ref.view(np.uint8)), (name, dt)
+        S.close()
+
+
+def test_fp16_within_reference_bound(ctx):
+    """against the reference's fp16-accumulated SELL<32,__half>::operate"""
+    ref = O.Ref("golden")
+    A = F.stencil27(16, 16, 16, 2, 0.5).scale()
+    rptr, idx, val = A.arrays()
+    n = A.shape[0]
+    x16 = np.random.default_rng(5).standard_normal(n).astype(np.float16)
+    S = F.Sell(ctx, A)
+    y = torch.zeros(n, dtype=torch.float16, device="cuda")
+    S.operate(torch.from_numpy(x16).cuda(), y)
+    got = y.cpu().numpy().astype(np.float64)
+    want = ref.sell32_operate(rptr, idx, val, 3, x16).astype(np.float64)
+    absAx = O.spmv(rptr, idx, np.abs(val), np.abs(x16.astype(np.float64)), O.DT_F64, O.DT_F64, O.DT_F64)
+    rowlen = np.diff(rptr)
+    bound = rowlen * 2.0 ** -11 * absAx + 2.0 ** -24
+    assert np.all(np.abs(got - want) <= 2 * bound)
+
+
+def test_dot(ctx):
+    rng = np.random.default_rng(3)
+    for n in (0, 1, 1000, 1 << 20):
+        a = rng.standard_normal(n)
+        b = rng.standard_normal(n)
+        got = ctx.dot(torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda())
+        assert abs(got - float(a @ b)) <= 1e-12 * (np.abs(a) @ np.abs(b) + 1)
+        a32, b32 = a.astype(np.float32), b.astype(np.float32)
+        got = ctx.dot(torch.from_numpy(a32).cuda(), torch.from_numpy(b32).cuda())
+        assert abs(got - float(a32.astype(np.float64) @ b32)) <= 1e-5 * (np.abs(a) @ np.abs(b) + 1)
+
+
+def test_empty_and_bad_inputs(ctx):
+    A = F.HostMatrix.from_csr(np.zeros(5, np.int32), np.zeros(0, np.int32), np.zeros(0))
+    S = F.Sell(ctx, A)
+    y = torch.ones(4, dtype=torch.float64, device="cuda")
+    S.operate(torch.ones(4, dtype=torch.float64, device="cuda"), y)
+    torch.cuda.synchronize()
+    assert torch.all(y == 0)
+    with pytest.raises(F.F3RError):
+        F.HostMatrix.from_csr(np.array([0, 2], np.int32), np.array([1, 0], np.int32), np.ones(2))
+    with pytest.raises(F.F3RError):
+        F.Sell(ctx, F.stencil27(4, 4, 4), sigma=0)
