@@ -79,6 +79,7 @@ SIGNATURES = {
     "f3r_sell_operate": (C.c_int, [_vp, C.c_int, C.c_int, _vp, C.c_int, _vp]),
     "f3r_sell_compute_residual": (C.c_int, [_vp, C.c_int, C.c_int, _vp, C.c_int, _vp, C.c_int, _vp]),
     "f3r_dot": (C.c_int, [_vp, C.c_int, C.c_int64, _vp, _vp, C.POINTER(C.c_double)]),
+    "f3r_dot_noalloc": (C.c_int, [C.c_int, C.c_int64, _vp, _vp, _vp, _vp]),
     "f3r_params_default": (None, [C.POINTER(Params)]),
     "f3r_solver_create": (C.c_int, [_vp, C.POINTER(CSR), C.POINTER(Params), _pp]),
     "f3r_solver_solve": (C.c_int, [_vp, _vp, _vp, COND_FN, _vp, C.POINTER(Result)]),

@@ -204,6 +204,20 @@ f3r_status f3r_sell_compute_residual(f3r_sell *m, f3r_dtype val_t, f3r_dtype rhs
 f3r_status f3r_dot(f3r_context *ctx, f3r_dtype t, int64_t n, const void *x, const void *y,
                    double *result);
 
+/* *result (a DEVICE pointer, written by the kernel) = <x, y> over n entries,
+ * like f3r_dot but without a context and without allocating anything: for
+ * callers that cannot call cudaMalloc (code running inside an allocator's own
+ * bookkeeping, or a device whose memory is all held by a pool the caller
+ * does not control).  No counterpart in the reference.  Its reduction scratch
+ * is a fixed 64 KB (+256 B) device array inside the library, held on every
+ * GPU that loads the library until exit; n is limited to 33,554,432 elements
+ * (larger n returns F3R_ERROR_INVALID_VALUE).  Asynchronous on `stream`
+ * (cudaStream_t; NULL = the default stream).  The first call on a device
+ * looks up the array's device address, so make it before any stream
+ * capture.  Calls that overlap on the GPU share the array and race. */
+f3r_status f3r_dot_noalloc(f3r_dtype t, int64_t n, const void *x, const void *y, double *result,
+                           void *stream);
+
 /* ----------------------------------------------------------------- solver
  * The nested F3R solver: Restarted<double>( FGMRES<double>(A, FGMRES<float>(
  * A32, FGMRES<float>(A16, R, m3), m2), m_outer), max_restarts ), with R the
