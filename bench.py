@@ -43,8 +43,15 @@ METRIC = "time to 1e-10 FP64 relative residual, plain F3R (fp64/fp32/fp16 nested
 WORKLOAD = "F3R-SDAINV-SELL32s256 stencil27-halfspace beta0.5 192^3 (n=7077888, nnz=189119224), tol 1e-10"
 
 
+def set_size(nx):
+    global NX, WORKLOAD
+    NX = nx
+    nnz = 27 * nx ** 3 - 54 * nx ** 2 + 36 * nx - 8
+    WORKLOAD = (f"F3R-SDAINV-SELL32s256 stencil27-halfspace beta0.5 {nx}^3 (n={nx ** 3}, nnz={nnz}), tol 1e-10")
+
+
 def config_dict(extra=None):
-    d = {"workload": WORKLOAD, "grid": [NX, NX, NX], "n": NX ** 3, "nnz": 189119224, "sell": {"C": 32, "sigma": SIGMA},
+    d = {"workload": WORKLOAD, "grid": [NX, NX, NX], "n": NX ** 3, "nnz": 27 * NX ** 3 - 54 * NX ** 2 + 36 * NX - 8, "sell": {"C": 32, "sigma": SIGMA},
          "f3r": {"m_outer": 100, "m2": 8, "m3": 4, "m4": 2, "c": 64, "restarts": 20},
          "precond": "SDAINV(tol=0.1, acc=1.0)", "rhs": "b = A x*, x* ~ U(-1,1) mt19937_64(rank)",
          "l2": "inputs larger than L2 (fp16+fp32+fp64 matrix copies 4.6 GB, vectors 12 GB)",
@@ -52,6 +59,23 @@ def config_dict(extra=None):
     if extra:
         d.update(extra)
     return d
+
+
+def replica_seed(rank: int) -> int:
+    """With N GPUs each rank solves its own system (replicas, no collective on
+    the data path): x* ~ U(-1, 1) from mt19937_64(seed = rank)."""
+    return rank
+
+
+def max_over_ranks(value: float, world: int, device=None) -> float:
+    """The job's time is the slowest rank's (all_reduce MAX; identity at N=1)."""
+    if world <= 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
 
 
 def make_problem(seed: int):
@@ -136,25 +160,24 @@ def profiled_traffic():
     return None
 
 
-def spmv_roofline(ctx, A, torch, F):
+def spmv_roofline(solver, A, torch, F):
     """Dominant kernel: the fp16-matrix SELL SpMV of level 3 (fp16 values,
-    fp32 x and y), timed with CUDA events on the library's stream."""
+    fp32 x and y) on the solver's own matrix, timed with CUDA events on the
+    stream the library launches on."""
     n, nnz = A.shape[0], A.nnz
-    S = F.Sell(ctx, A, sigma=SIGMA, dtypes=(F.F16,))
     x = torch.randn(n, dtype=torch.float32, device="cuda")
     y = torch.empty_like(x)
     for _ in range(5):
-        S.operate(x, y, val_t=F.F16)
+        solver.operate(x, y, val_t=F.F16)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     reps = 50
     e0.record(torch.cuda.current_stream())
     for _ in range(reps):
-        S.operate(x, y, val_t=F.F16)
+        solver.operate(x, y, val_t=F.F16)
     e1.record(torch.cuda.current_stream())
     torch.cuda.synchronize()
     dt = e0.elapsed_time(e1) * 1e-3 / reps
-    S.close()
     alg = nnz * (2 + 4) + 4 * (n + 1) + n * 4 + n * 4
     peak, src = measured_peak()
     achieved = alg / dt / 1e9
@@ -198,7 +221,7 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
     import f3r_b200 as F
 
-    A, b, xs = make_problem(seed=rank)
+    A, b, xs = make_problem(seed=replica_seed(rank))
     n = A.shape[0]
     ctx = F.Context(local)
     stream = torch.cuda.Stream()          # one non-default stream for torch and the library
@@ -221,18 +244,16 @@ def run_ours(args):
     clocks.start()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     results = []
+    torch.cuda.nvtx.range_push("timed")
     e0.record(stream)
     for _ in range(args.steps):
         x_d.zero_()
         results.append(solver.solve(b_d, x_d))
     e1.record(stream)
+    torch.cuda.nvtx.range_pop()
     barrier()
     ck = clocks.stop()
-    t = e0.elapsed_time(e1) * 1e-3
-    if world > 1:
-        tt = torch.tensor([t], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t = float(tt.item())
+    t = max_over_ranks(e0.elapsed_time(e1) * 1e-3, world, "cuda")
     ms_per = t / args.steps * 1e3
     r = results[-1]
     err = float(torch.linalg.norm(x_d.cpu() - torch.from_numpy(xs)) / np.linalg.norm(xs))
@@ -252,14 +273,10 @@ def run_ours(args):
     e1.record(stream)
     barrier()
     t_e2e = max(e0.elapsed_time(e1) * 1e-3, 0.0)
-    wall_e2e = time.perf_counter() - w0
-    if world > 1:
-        tt = torch.tensor([wall_e2e], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        wall_e2e = float(tt.item())
+    wall_e2e = max_over_ranks(time.perf_counter() - w0, world, "cuda")
     e2e_ms = wall_e2e / args.steps * 1e3
 
-    roof = spmv_roofline(ctx, A, torch, F) if rank == 0 else None
+    roof = spmv_roofline(solver, A, torch, F) if rank == 0 else None
     cpu = cpu_baseline(A, b, r.res_iter) if (rank == 0 and world == 1 and not args.no_cpu_baseline) else None
     if rank == 0:
         line = {
@@ -335,7 +352,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--nx", type=int, default=NX, help="grid edge (the benchmark is 192; smaller sizes for profiling)")
     args = ap.parse_args()
+    set_size(args.nx)
     if args.impl == "reference":
         run_reference(args)
     else:

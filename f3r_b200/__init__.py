@@ -162,8 +162,8 @@ class Sell:
     """Device SELL-32-sigma matrix (f3r_sell) -- CoefficientMatrix::operate /
     compute_residual on device tensors."""
 
-    def __init__(self, ctx: Context, A: HostMatrix, sigma: int = 1, dtypes=(F64, F32, F16)):
-        mask = 0
+    def __init__(self, ctx: Context, A: HostMatrix, sigma: int = 1, dtypes=(F64, F32, F16), index16: bool = False):
+        mask = _capi.SELL_INDEX16 if index16 else 0
         for d in dtypes:
             mask |= 1 << d
         h = C.c_void_p()
@@ -244,6 +244,12 @@ class Solver:
         d = C.c_int32()
         check(lib().f3r_solver_info(self._h, C.byref(i), C.byref(d)))
         return i, bool(d.value)
+
+    def operate(self, x, y, val_t=None) -> None:
+        """y = A x with the solver's own device matrix (storage order P A P^T)."""
+        xt, yt = _torch_dt(x), _torch_dt(y)
+        vt = xt if val_t is None else val_t
+        check(lib().f3r_solver_operate(self._h, vt, xt, C.c_void_p(x.data_ptr()), yt, C.c_void_p(y.data_ptr())))
 
     def solve(self, b, x, cond: Optional[Callable[[int, float], bool]] = None) -> solve_res_t:
         """Solve A x = b.  b, x: numpy float64 arrays (x is updated in place and

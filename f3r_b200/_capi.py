@@ -15,6 +15,7 @@ F3R_SUCCESS = 0
 STATUS = {0: "SUCCESS", 1: "INVALID_VALUE", 2: "CUDA", 3: "OUT_OF_MEMORY", 5: "BREAKDOWN", 7: "TIMEOUT",
           8: "UNSUPPORTED", 9: "NO_DEVICE"}
 F64, F32, F16 = 0, 1, 2
+SELL_INDEX16 = 1 << 8
 PRECOND_SDAINV, PRECOND_ILU0_BJ = 0, 1
 
 
@@ -34,7 +35,7 @@ class Params(C.Structure):
                 ("m4", C.c_int32), ("c", C.c_int32), ("precond", C.c_int32), ("ilu_blocks", C.c_int32),
                 ("sdainv_tol", C.c_double), ("acc", C.c_double), ("sell_c", C.c_int32), ("sell_sigma", C.c_int32),
                 ("rel_tol", C.c_double), ("half_scale_log2", C.c_int32), ("use_graphs", C.c_int32),
-                ("reserved", C.c_int32 * 8)]
+                ("sell_index16", C.c_int32), ("reserved", C.c_int32 * 7)]
 
 
 class Result(C.Structure):
@@ -47,7 +48,7 @@ class Result(C.Structure):
 class SellInfo(C.Structure):
     _fields_ = [("nrows", C.c_int32), ("ncols", C.c_int32), ("nnz", C.c_int32), ("slice_height", C.c_int32),
                 ("sigma", C.c_int32), ("nslices", C.c_int32), ("nnz_padded", C.c_int64), ("max_width", C.c_int32),
-                ("dtypes", C.c_int32)]
+                ("dtypes", C.c_int32), ("index_bits", C.c_int32)]
 
 
 COND_FN = C.CFUNCTYPE(C.c_int, C.c_int32, C.c_double, C.c_void_p)
@@ -84,6 +85,7 @@ SIGNATURES = {
     "f3r_solver_create": (C.c_int, [_vp, C.POINTER(CSR), C.POINTER(Params), _pp]),
     "f3r_solver_solve": (C.c_int, [_vp, _vp, _vp, COND_FN, _vp, C.POINTER(Result)]),
     "f3r_solver_info": (C.c_int, [_vp, C.POINTER(SellInfo), C.POINTER(C.c_int32)]),
+    "f3r_solver_operate": (C.c_int, [_vp, C.c_int, C.c_int, _vp, C.c_int, _vp]),
     "f3r_solver_destroy": (None, [_vp]),
 }
 

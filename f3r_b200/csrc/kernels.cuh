@@ -16,6 +16,18 @@ template <typename T> struct Cols {
   const T *p[kMaxCols];
 };
 
+// 16-byte (or narrower) vector access; every vector this library allocates
+// starts on a 64-byte boundary with columns padded to 8 elements.
+template <typename T, int N> struct alignas(sizeof(T) * N) VecN {
+  T v[N];
+};
+template <typename T, int N> __device__ __forceinline__ VecN<T, N> ldv(const T *p) {
+  return *reinterpret_cast<const VecN<T, N> *>(p);
+}
+template <typename T, int N> __device__ __forceinline__ void stv(T *p, const VecN<T, N> &v) {
+  *reinterpret_cast<VecN<T, N> *>(p) = v;
+}
+
 // Running state of the adaptive-weight Richardson operator
 // (f3r-gpu.cpp:106-108, 224-227, 239-240, 253-254, 277-281).
 struct RichState {
@@ -86,8 +98,11 @@ template <typename T> __global__ void k_trsv_y(T *H, const T *e, T *y, int ldh, 
 template <int NVT> struct EpiStoreDots {
   using Red = float;
   static constexpr int NV = NVT;
+  // up to 4 basis values are fetched ahead of the multiply-add chain; wider
+  // epilogues read them afterwards (their registers would spill)
+  static constexpr bool PRE = NVT <= 4;
   struct Pre {
-    float v[NVT];
+    float v[PRE ? NVT : 1];
   };
   float *y;
   Cols<float> V;
@@ -96,8 +111,10 @@ template <int NVT> struct EpiStoreDots {
   float *hcol;
   __device__ __forceinline__ Pre load(int64_t r) const {
     Pre p;
+    if (PRE) {
 #pragma unroll
-    for (int k = 0; k < NV; k++) p.v[k] = (k < nv) ? __ldg(V.p[k] + r) : 0.0f;
+      for (int k = 0; k < (PRE ? NVT : 1); k++) p.v[k] = (k < nv) ? __ldg(V.p[k] + r) : 0.0f;
+    }
     return p;
   }
   template <typename Acc> __device__ __forceinline__ void row(int64_t r, Acc acc, const Pre &p, Red (&d)[NV]) const {
@@ -105,7 +122,7 @@ template <int NVT> struct EpiStoreDots {
     y[r] = yv;
 #pragma unroll
     for (int k = 0; k < NV; k++)
-      if (k < nv) d[k] = __fmaf_rn(yv, p.v[k], d[k]);
+      if (k < nv) d[k] = __fmaf_rn(yv, PRE ? p.v[PRE ? k : 0] : __ldg(V.p[k] + r), d[k]);
   }
   template <int W> __device__ __forceinline__ void finish(Red (&d)[NV]) const {
     float *h = hcol;
@@ -153,12 +170,37 @@ struct EpiResidualNorm {
 template <typename T, int WARPS>
 __global__ void __launch_bounds__(WARPS * 32) k_cgs_update(T *__restrict__ w, Cols<T> V, int nv, int64_t n,
                                                            GridRed gr, GivensCtl<T> g) {
+  constexpr int N = 16 / sizeof(T);
   __shared__ T sh[kMaxCols];
   const T *hcol = g.H + (size_t)g.j * g.ldh;
   for (int k = threadIdx.x; k < nv; k += blockDim.x) sh[k] = hcol[k];
   __syncthreads();
   T part[1] = {0};
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t nq = n / N;
+  for (int64_t q = tid; q < nq; q += stride) {
+    const int64_t i = q * N;
+    const VecN<T, N> a = ldv<T, N>(V.p[0] + i);
+    T r[N];
+#pragma unroll
+    for (int e = 0; e < N; e++) r[e] = a.v[e] * sh[0];
+#pragma unroll 4
+    for (int k = 1; k < nv; k++) {
+      const VecN<T, N> b = ldv<T, N>(V.p[k] + i);
+      const T hk = sh[k];
+#pragma unroll
+      for (int e = 0; e < N; e++) r[e] = fmaT(b.v[e], hk, r[e]);
+    }
+    VecN<T, N> wv = ldv<T, N>(w + i);
+#pragma unroll
+    for (int e = 0; e < N; e++) {
+      wv.v[e] -= r[e];
+      part[0] = fmaT(wv.v[e], wv.v[e], part[0]);
+    }
+    stv<T, N>(w + i, wv);
+  }
+  for (int64_t i = nq * N + tid; i < n; i += stride) {
     T r = V.p[0][i] * sh[0];
     for (int k = 1; k < nv; k++) r = fmaT(V.p[k][i], sh[k], r);
     const T wi = w[i] - r;
@@ -220,20 +262,52 @@ __global__ void __launch_bounds__(WARPS * 32) k_multidot_f64(const double *__res
 
 // v *= *inv  (V(j+1) *= h.inv(), gmres.hpp:117)
 template <typename T> __global__ void k_scale(T *__restrict__ v, const T *__restrict__ inv, int64_t n) {
+  constexpr int N = 16 / sizeof(T);
   const T s = *inv;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    v[i] *= s;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x, tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t nq = n / N;
+  for (int64_t q = tid; q < nq; q += stride) {
+    VecN<T, N> a = ldv<T, N>(v + q * N);
+#pragma unroll
+    for (int e = 0; e < N; e++) a.v[e] *= s;
+    stv<T, N>(v + q * N, a);
+  }
+  for (int64_t i = nq * N + tid; i < n; i += stride) v[i] *= s;
 }
 
-// Level-2 entry: V2(0) = float(in) (V(0).copy(rhs), gmres.hpp:102) with e(0)=1
-// (normalize=false, gmres.hpp:100-101).  `in` is read through a device
-// pointer slot so one captured graph serves every outer step.
-__global__ void k_level2_enter(const double *const *__restrict__ in_slot, float *__restrict__ v0, float *e,
-                               int64_t n) {
-  const double *in = *in_slot;
+// Level-2 entry.  The outer basis vector V1(j) is normalised here, in place
+// (V(j+1) *= h.inv(), gmres.hpp:117; the factor 1/h was left by the outer
+// level's reduction), then cast: V2(0) = float(V1(j)) (V(0).copy(rhs),
+// gmres.hpp:102), with e(0) = 1 (normalize=false, gmres.hpp:100-101).  `in`
+// is read through a device pointer slot so one captured graph serves every
+// outer step.
+__global__ void k_level2_enter(double *const *__restrict__ in_slot, const double *__restrict__ inv,
+                               float *__restrict__ v0, float *e, int64_t n) {
+  double *in = *in_slot;
+  const double s = *inv;
   if (blockIdx.x == 0 && threadIdx.x == 0) e[0] = 1.0f;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    v0[i] = (float)in[i];
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x, tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t nq = n / 4;
+  for (int64_t q = tid; q < nq; q += stride) {
+    VecN<double, 2> a = ldv<double, 2>(in + 4 * q), b = ldv<double, 2>(in + 4 * q + 2);
+    a.v[0] *= s;
+    a.v[1] *= s;
+    b.v[0] *= s;
+    b.v[1] *= s;
+    stv<double, 2>(in + 4 * q, a);
+    stv<double, 2>(in + 4 * q + 2, b);
+    VecN<float, 4> o;
+    o.v[0] = (float)a.v[0];
+    o.v[1] = (float)a.v[1];
+    o.v[2] = (float)b.v[0];
+    o.v[3] = (float)b.v[1];
+    stv<float, 4>(v0 + 4 * q, o);
+  }
+  for (int64_t i = nq * 4 + tid; i < n; i += stride) {
+    const double v = in[i] * s;
+    in[i] = v;
+    v0[i] = (float)v;
+  }
 }
 
 // x = Z y (with_init) for the inner levels, x += Z y for the outer level
@@ -242,11 +316,33 @@ __global__ void k_level2_enter(const double *const *__restrict__ in_slot, float 
 template <typename T, typename Out, bool ACCUM>
 __global__ void k_zy(Cols<T> Z, const T *__restrict__ y, int nz, Out *__restrict__ out_direct,
                      Out *const *__restrict__ out_slot, int64_t n) {
+  constexpr int N = 16 / sizeof(T);
   __shared__ T sy[kMaxCols];
   for (int k = threadIdx.x; k < nz; k += blockDim.x) sy[k] = y[k];
   __syncthreads();
   Out *out = out_slot ? *out_slot : out_direct;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x, tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t nq = n / N;
+  for (int64_t q = tid; q < nq; q += stride) {
+    const int64_t i = q * N;
+    const VecN<T, N> a = ldv<T, N>(Z.p[0] + i);
+    T r[N];
+#pragma unroll
+    for (int e = 0; e < N; e++) r[e] = a.v[e] * sy[0];
+#pragma unroll 4
+    for (int k = 1; k < nz; k++) {
+      const VecN<T, N> b = ldv<T, N>(Z.p[k] + i);
+      const T yk = sy[k];
+#pragma unroll
+      for (int e = 0; e < N; e++) r[e] = fmaT(b.v[e], yk, r[e]);
+    }
+    VecN<Out, N> o;
+    if (ACCUM) o = ldv<Out, N>(out + i);
+#pragma unroll
+    for (int e = 0; e < N; e++) o.v[e] = ACCUM ? o.v[e] + (Out)r[e] : (Out)r[e];
+    stv<Out, N>(out + i, o);
+  }
+  for (int64_t i = nq * N + tid; i < n; i += stride) {
     T r = Z.p[0][i] * sy[0];
     for (int k = 1; k < nz; k++) r = fmaT(Z.p[k][i], sy[k], r);
     if (ACCUM) out[i] += (Out)r;
@@ -272,16 +368,48 @@ struct DiagPre {
   }
 };
 
-// First half of R: hin = fp16(in * sc); hout = M hin; then, on a call without
-// a weight update, hout *= ome[0] (f3r-gpu.cpp:231-243).
+// First half of R.  The level-3 basis vector is normalised here, in place,
+// when its 1/h factor is given (V(j+1) *= h.inv(), gmres.hpp:117 -- deferred
+// from the Gram-Schmidt step to save a pass); then hin = fp16(in * sc),
+// hout = M hin, and on a call without a weight update hout *= ome[0]
+// (f3r-gpu.cpp:231-243).
 template <bool SCALE_BY_OME>
-__global__ void k_rich_enter_diag(const float *__restrict__ in, float sc, DiagPre M, __half *__restrict__ hin,
-                                  __half *__restrict__ hout, const RichState *__restrict__ rs, float *e_set,
-                                  int64_t n) {
+__global__ void k_rich_enter_diag(float *__restrict__ in, const float *__restrict__ in_inv, float sc, DiagPre M,
+                                  __half *__restrict__ hin, __half *__restrict__ hout,
+                                  const RichState *__restrict__ rs, float *e_set, int64_t n) {
   if (e_set && blockIdx.x == 0 && threadIdx.x == 0) e_set[0] = 1.0f;
   const float om = SCALE_BY_OME ? h2f(rs->ome[0]) : 1.0f;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    const __half hi = f2h(in[i] * sc);
+  const float s = in_inv ? *in_inv : 1.0f;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x, tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t nq = n / 4;
+  for (int64_t q = tid; q < nq; q += stride) {
+    const int64_t i = 4 * q;
+    VecN<float, 4> v = ldv<float, 4>(in + i);
+    if (in_inv) {
+#pragma unroll
+      for (int e = 0; e < 4; e++) v.v[e] *= s;
+      stv<float, 4>(in + i, v);
+    }
+    const VecN<__half, 4> w = ldv<__half, 4>(M.w + i), z = ldv<__half, 4>(M.z + i);
+    VecN<__half, 4> hi, ho;
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+      hi.v[e] = f2h(v.v[e] * sc);
+      const float t = h2f(f2h(h2f(w.v[e]) * h2f(hi.v[e])));
+      float o = h2f(f2h(h2f(z.v[e]) * t));
+      if (SCALE_BY_OME) o = h2f(f2h(o * om));
+      ho.v[e] = f2h(o);
+    }
+    stv<__half, 4>(hin + i, hi);
+    stv<__half, 4>(hout + i, ho);
+  }
+  for (int64_t i = nq * 4 + tid; i < n; i += stride) {
+    float v = in[i];
+    if (in_inv) {
+      v *= s;
+      in[i] = v;
+    }
+    const __half hi = f2h(v * sc);
     hin[i] = hi;
     float ho = M.apply(i, h2f(hi));
     if (SCALE_BY_OME) ho = h2f(f2h(ho * om));
@@ -289,12 +417,19 @@ __global__ void k_rich_enter_diag(const float *__restrict__ in, float sc, DiagPr
   }
 }
 
-// General preconditioner: hin = fp16(in * sc) only.
-__global__ void k_rich_cast_in(const float *__restrict__ in, float sc, __half *__restrict__ hin, float *e_set,
-                               int64_t n) {
+// General preconditioner: (normalise in place), hin = fp16(in * sc) only.
+__global__ void k_rich_cast_in(float *__restrict__ in, const float *__restrict__ in_inv, float sc,
+                               __half *__restrict__ hin, float *e_set, int64_t n) {
   if (e_set && blockIdx.x == 0 && threadIdx.x == 0) e_set[0] = 1.0f;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    hin[i] = f2h(in[i] * sc);
+  const float s = in_inv ? *in_inv : 1.0f;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    float v = in[i];
+    if (in_inv) {
+      v *= s;
+      in[i] = v;
+    }
+    hin[i] = f2h(v * sc);
+  }
 }
 
 // Residual step of R with the diagonal preconditioner fused (no weight

@@ -28,11 +28,21 @@
 
 namespace f3r {
 
+// Column indices come in one of two forms:
+//  * col:   int32 per entry;
+//  * dcol + cbase: a uint16 offset per entry from an int32 base per slice
+//    column, used when every slice column's indices fit in a 65536 window --
+//    2 + 4/32 bytes per entry instead of 4.  The bases of slice s start at
+//    cbptr[s], a multiple of 4, so a chunk's bases are one 16-byte aligned
+//    bulk copy like its values and offsets.
 struct DevSell {
-  const int32_t *col;   // (sptr[nslices]) * 32
-  const int32_t *sptr;  // nslices + 1, in units of 32 entries
-  const int32_t *perm;  // storage row -> output row, or nullptr (identity)
-  int32_t n;            // rows (outputs written only for storage rows < n)
+  const int32_t *col;     // (sptr[nslices]) * 32, or nullptr
+  const uint16_t *dcol;   // (sptr[nslices]) * 32, or nullptr
+  const int32_t *cbase;   // cbptr[nslices] (+ padding), with dcol
+  const int32_t *cbptr;   // nslices + 1, with dcol
+  const int32_t *sptr;    // nslices + 1, in units of 32 entries
+  const int32_t *perm;    // storage row -> output row, or nullptr (identity)
+  int32_t n;              // rows (outputs written only for storage rows < n)
   int32_t nslices;
 };
 
@@ -47,20 +57,25 @@ template <> struct SellCfg<__half> { static constexpr int WARPS = 24, STAGES = 2
 template <> struct SellCfg<float> { static constexpr int WARPS = 24, STAGES = 2, KC = 16; };
 template <> struct SellCfg<double> { static constexpr int WARPS = 16, STAGES = 2, KC = 16; };
 
-template <typename V, int WARPS, int STAGES, int KC>
+template <typename V, typename CI, int WARPS, int STAGES, int KC>
 constexpr size_t sell_smem_bytes_cfg() {
-  return (size_t)WARPS * STAGES * ((size_t)KC * 32 * (sizeof(V) + 4)) + (size_t)WARPS * STAGES * sizeof(uint64_t);
+  return (size_t)WARPS * STAGES * ((size_t)KC * 32 * (sizeof(V) + sizeof(CI)) + (sizeof(CI) == 2 ? KC * 4 : 0)) +
+         (size_t)WARPS * STAGES * sizeof(uint64_t);
 }
-template <typename V>
+template <typename V, typename CI>
 constexpr size_t sell_smem_bytes() {
-  return sell_smem_bytes_cfg<V, SellCfg<V>::WARPS, SellCfg<V>::STAGES, SellCfg<V>::KC>();
+  return sell_smem_bytes_cfg<V, CI, SellCfg<V>::WARPS, SellCfg<V>::STAGES, SellCfg<V>::KC>();
 }
 
-template <typename V, typename X, typename Epi, int WARPS, int STAGES, int KC>
+// CI: the stored index type, int32_t (col) or uint16_t (dcol + cbase).
+template <typename V, typename X, typename Epi, int WARPS, int STAGES, int KC, typename CI = int32_t>
 __global__ void __launch_bounds__(WARPS * 32, 1)
     k_sell_cfg(const V *__restrict__ val, DevSell A, const X *__restrict__ x, Epi epi, int *err) {
   using Acc = typename acc_of<V>::type;
-  constexpr uint32_t VB = KC * 32 * sizeof(V), CB = KC * 32 * 4, SB = VB + CB;
+  constexpr bool C16 = sizeof(CI) == 2;
+  static_assert(KC % 4 == 0, "chunk width must keep the bases 16-byte aligned");
+  constexpr uint32_t VB = KC * 32 * sizeof(V), CB = KC * 32 * sizeof(CI), BB = C16 ? KC * 4 : 0, SB = VB + CB + BB;
+  const CI *cidx = C16 ? reinterpret_cast<const CI *>(A.dcol) : reinterpret_cast<const CI *>(A.col);
   extern __shared__ __align__(128) unsigned char smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   unsigned char *buf = smem + (size_t)warp * STAGES * SB;
@@ -88,9 +103,11 @@ __global__ void __launch_bounds__(WARPS * 32, 1)
       if (lane == 0) {
         const size_t off = ((size_t)s0 + fk) * 32;
         fence_proxy_async_smem();
-        mbar_arrive_expect_tx(&bars[fst], (uint32_t)kc * 32u * (uint32_t)(sizeof(V) + 4));
+        const uint32_t bb = C16 ? (uint32_t)((kc + 3) & ~3) * 4u : 0u;
+        mbar_arrive_expect_tx(&bars[fst], (uint32_t)kc * 32u * (uint32_t)(sizeof(V) + sizeof(CI)) + bb);
         bulk_g2s(buf + (size_t)fst * SB, val + off, (uint32_t)kc * 32u * (uint32_t)sizeof(V), &bars[fst], pol);
-        bulk_g2s(buf + (size_t)fst * SB + VB, A.col + off, (uint32_t)kc * 32u * 4u, &bars[fst], pol);
+        bulk_g2s(buf + (size_t)fst * SB + VB, cidx + off, (uint32_t)kc * 32u * (uint32_t)sizeof(CI), &bars[fst], pol);
+        if (C16) bulk_g2s(buf + (size_t)fst * SB + VB + CB, A.cbase + A.cbptr[fs] + fk, bb, &bars[fst], pol);
       }
       fst = (fst + 1 == STAGES) ? 0 : fst + 1;
       inflight++;
@@ -131,14 +148,16 @@ __global__ void __launch_bounds__(WARPS * 32, 1)
     }
     phase ^= 1u << cst;
     const V *sv = reinterpret_cast<const V *>(buf + (size_t)cst * SB);
-    const int32_t *sc = reinterpret_cast<const int32_t *>(buf + (size_t)cst * SB + VB);
+    const CI *sc = reinterpret_cast<const CI *>(buf + (size_t)cst * SB + VB);
+    const int32_t *sb = reinterpret_cast<const int32_t *>(buf + (size_t)cst * SB + VB + CB);
     V vv[KC];
     int32_t cc[KC];
 #pragma unroll
     for (int k = 0; k < KC; k++) {
       if (k < kc) {
         vv[k] = sv[k * 32 + lane];
-        cc[k] = sc[k * 32 + lane];
+        if (C16) cc[k] = sb[k] + (int32_t)sc[k * 32 + lane];
+        else cc[k] = (int32_t)sc[k * 32 + lane];
       }
     }
     // the chunk is in registers: release the stage to the copy engine now

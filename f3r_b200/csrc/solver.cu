@@ -97,7 +97,43 @@ struct SellHost {
   int64_t nnz = 0, nnz_pad = 0;
   std::vector<int32_t> sptr, col, perm;  // perm: storage row -> original row
   std::vector<double> val;
+  std::vector<uint16_t> dcol;            // 16-bit offsets (when they fit)
+  std::vector<int32_t> cbase;            // base of each slice column, slice s from cbptr[s]
+  std::vector<int32_t> cbptr;            // nslices + 1, multiples of 4
 };
+
+// Re-expresses the column indices as 16-bit offsets from the smallest index
+// of each slice column, if every slice column spans fewer than 65536 columns.
+static bool compress_index16(SellHost &s) {
+  const int64_t ncolsl = s.sptr[s.nslices];
+  std::vector<int32_t> base(ncolsl);
+  bool ok = true;
+#pragma omp parallel for schedule(static) reduction(&& : ok)
+  for (int64_t c = 0; c < ncolsl; c++) {
+    int32_t lo = INT32_MAX, hi = INT32_MIN;
+    for (int l = 0; l < 32; l++) {
+      const int32_t v = s.col[c * 32 + l];
+      lo = std::min(lo, v);
+      hi = std::max(hi, v);
+    }
+    base[c] = lo;
+    ok = ok && ((int64_t)hi - lo <= 65535);
+  }
+  if (!ok) return false;
+  s.dcol.resize(s.col.size());
+#pragma omp parallel for schedule(static)
+  for (int64_t c = 0; c < ncolsl; c++)
+    for (int l = 0; l < 32; l++) s.dcol[c * 32 + l] = (uint16_t)(s.col[c * 32 + l] - base[c]);
+  // bases laid out per slice from a multiple of 4 (16-byte aligned copies)
+  s.cbptr.assign(s.nslices + 1, 0);
+  for (int32_t sl = 0; sl < s.nslices; sl++) s.cbptr[sl + 1] = s.cbptr[sl] + ((s.sptr[sl + 1] - s.sptr[sl] + 3) & ~3);
+  s.cbase.assign((size_t)s.cbptr[s.nslices] + 4, 0);
+#pragma omp parallel for schedule(static)
+  for (int32_t sl = 0; sl < s.nslices; sl++)
+    for (int32_t k = 0; k < s.sptr[sl + 1] - s.sptr[sl]; k++) s.cbase[s.cbptr[sl] + k] = base[s.sptr[sl] + k];
+  std::vector<int32_t>().swap(s.col);
+  return true;
+}
 
 // renumber = true builds P A P^T (columns mapped to storage order) for the
 // solver's permuted system; false keeps original columns and scatters rows.
@@ -170,15 +206,19 @@ static Status build_sell(const f3r_csr &a, int32_t sigma, bool renumber, SellHos
 struct DeviceSell {
   int32_t n = 0, ncols = 0, nslices = 0, max_width = 0, sigma = 1;
   int64_t nnz = 0, nnz_pad = 0;
-  int32_t *col = nullptr, *sptr = nullptr, *perm = nullptr;
+  int32_t *col = nullptr, *sptr = nullptr, *perm = nullptr, *cbase = nullptr, *cbptr = nullptr;
+  uint16_t *dcol = nullptr;
   double *v64 = nullptr;
   float *v32 = nullptr;
   __half *v16 = nullptr;
   int dtypes = 0;
-  DevSell view() const { return DevSell{col, sptr, perm, n, nslices}; }
+  int index_bits() const { return dcol ? 16 : 32; }
+  DevSell view() const { return DevSell{col, dcol, cbase, cbptr, sptr, perm, n, nslices}; }
   void release() {
-    cudaFree(col); cudaFree(sptr); cudaFree(perm); cudaFree(v64); cudaFree(v32); cudaFree(v16);
-    col = sptr = perm = nullptr; v64 = nullptr; v32 = nullptr; v16 = nullptr;
+    cudaFree(col); cudaFree(sptr); cudaFree(perm); cudaFree(cbase); cudaFree(cbptr); cudaFree(dcol);
+    cbptr = nullptr;
+    cudaFree(v64); cudaFree(v32); cudaFree(v16);
+    col = sptr = perm = cbase = nullptr; dcol = nullptr; v64 = nullptr; v32 = nullptr; v16 = nullptr;
   }
 };
 
@@ -186,9 +226,19 @@ static Status upload_sell(Context &c, const SellHost &h, int dtype_mask, bool sc
   d.n = h.n; d.ncols = h.ncols; d.nslices = h.nslices; d.max_width = h.max_width; d.sigma = h.sigma;
   d.nnz = h.nnz; d.nnz_pad = h.nnz_pad; d.dtypes = dtype_mask;
   const size_t np = (size_t)h.nnz_pad;
-  F3R_TRY(c.alloc((void **)&d.col, np * 4));
+  if (!h.dcol.empty()) {
+    const size_t nc = h.cbase.size();
+    F3R_TRY(c.alloc((void **)&d.dcol, np * 2));
+    F3R_TRY(c.alloc((void **)&d.cbase, nc * 4));
+    F3R_TRY(c.alloc((void **)&d.cbptr, (size_t)(h.nslices + 1) * 4));
+    CUDA_TRY(cudaMemcpyAsync(d.dcol, h.dcol.data(), np * 2, cudaMemcpyHostToDevice, c.stream));
+    CUDA_TRY(cudaMemcpyAsync(d.cbase, h.cbase.data(), nc * 4, cudaMemcpyHostToDevice, c.stream));
+    CUDA_TRY(cudaMemcpyAsync(d.cbptr, h.cbptr.data(), (size_t)(h.nslices + 1) * 4, cudaMemcpyHostToDevice, c.stream));
+  } else {
+    F3R_TRY(c.alloc((void **)&d.col, np * 4));
+    CUDA_TRY(cudaMemcpyAsync(d.col, h.col.data(), np * 4, cudaMemcpyHostToDevice, c.stream));
+  }
   F3R_TRY(c.alloc((void **)&d.sptr, (size_t)(h.nslices + 1) * 4));
-  CUDA_TRY(cudaMemcpyAsync(d.col, h.col.data(), np * 4, cudaMemcpyHostToDevice, c.stream));
   CUDA_TRY(cudaMemcpyAsync(d.sptr, h.sptr.data(), (size_t)(h.nslices + 1) * 4, cudaMemcpyHostToDevice, c.stream));
   if (scatter_perm && h.sigma > 1) {
     F3R_TRY(c.alloc((void **)&d.perm, (size_t)std::max(h.n, 1) * 4));
@@ -227,8 +277,11 @@ static Status sell_attr(Context &c) {
   static int attr_done[64] = {0};
   if (!attr_done[c.device & 63]) {
     CUDA_TRY(cudaFuncSetAttribute(
-        k_sell_cfg<V, X, Epi, SellCfg<V>::WARPS, SellCfg<V>::STAGES, SellCfg<V>::KC>,
-        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sell_smem_bytes<V>()));
+        k_sell_cfg<V, X, Epi, SellCfg<V>::WARPS, SellCfg<V>::STAGES, SellCfg<V>::KC, int32_t>,
+        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sell_smem_bytes<V, int32_t>()));
+    CUDA_TRY(cudaFuncSetAttribute(
+        k_sell_cfg<V, X, Epi, SellCfg<V>::WARPS, SellCfg<V>::STAGES, SellCfg<V>::KC, uint16_t>,
+        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sell_smem_bytes<V, uint16_t>()));
     attr_done[c.device & 63] = 1;
   }
   return F3R_SUCCESS;
@@ -238,11 +291,14 @@ template <typename V, typename X, typename Epi>
 static Status launch_sell(Context &c, const V *val, const DevSell &A, const X *x, const Epi &epi) {
   if (A.nslices == 0) return F3R_SUCCESS;
   constexpr int WARPS = SellCfg<V>::WARPS;
-  constexpr size_t smem = sell_smem_bytes<V>();
   F3R_TRY((sell_attr<V, X, Epi>(c)));
   const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(cdiv(A.nslices, WARPS), c.sm_count));
-  launch_k(c, k_sell_cfg<V, X, Epi, WARPS, SellCfg<V>::STAGES, SellCfg<V>::KC>, grid, WARPS * 32, smem, c.stream,
-           val, A, x, epi, c.err);
+  if (A.dcol)
+    launch_k(c, k_sell_cfg<V, X, Epi, WARPS, SellCfg<V>::STAGES, SellCfg<V>::KC, uint16_t>, grid, WARPS * 32,
+             sell_smem_bytes<V, uint16_t>(), c.stream, val, A, x, epi, c.err);
+  else
+    launch_k(c, k_sell_cfg<V, X, Epi, WARPS, SellCfg<V>::STAGES, SellCfg<V>::KC, int32_t>, grid, WARPS * 32,
+             sell_smem_bytes<V, int32_t>(), c.stream, val, A, x, epi, c.err);
   CUDA_TRY(cudaGetLastError());
   return F3R_SUCCESS;
 }
@@ -292,6 +348,7 @@ struct Solver {
   f3r_context *ctx = nullptr;
   f3r_params p{};
   int32_t n = 0;
+  int64_t ldn = 0;  // column stride of the Krylov bases: n rounded up to 8 (64-byte aligned columns)
   DeviceSell A;
   std::vector<int32_t> perm;  // storage row -> original row (sigma > 1)
   int32_t *perm_d = nullptr;
@@ -306,7 +363,7 @@ struct Solver {
   double *abs_e = nullptr;
   __half *hin = nullptr, *hout = nullptr, *hout2 = nullptr, *tmp = nullptr, *tmp2 = nullptr, *hr = nullptr;
   RichState *rs = nullptr;
-  const double **in_slot = nullptr;
+  double **in_slot = nullptr;
   double **out_slot = nullptr;
   double *b_d = nullptr, *x_d = nullptr, *bp_d = nullptr, *xp_d = nullptr, *r_d = nullptr;
   int64_t cnt = 0;
@@ -331,7 +388,7 @@ struct Solver {
 
   template <typename T> Status make_level(Level<T> &L, int m, bool own_v0) {
     L.m = m;
-    const size_t nn = (size_t)std::max(n, 1);
+    const size_t nn = (size_t)std::max<int64_t>(ldn, 8);
     F3R_TRY(alloc(&L.V, nn * (size_t)(m + (own_v0 ? 1 : 0))));
     F3R_TRY(alloc(&L.Z, nn * (size_t)m));
     F3R_TRY(alloc(&L.H, (size_t)(m + 1) * m));
@@ -346,9 +403,12 @@ struct Solver {
   }
 
   // ---- level 4: R(in) -> out -------------------------------------------------
-  Status rich_apply(const float *in, float *out, float *e_set) {
+  // in_inv: 1/h of the basis vector `in` when its normalisation is still
+  // pending (done in place by the first kernel), else nullptr
+  Status rich_apply(float *in, float *out, float *e_set, const float *in_inv) {
     const int64_t N = n;
     const int g = C().ew_grid(N);
+    const int gv = C().ew_grid(cdiv(N, 4));
     cudaStream_t st = C().stream;
     ++cnt;
     ++r_calls;
@@ -358,7 +418,7 @@ struct Solver {
     if (precond_diag) {
       const DiagPre M{wd, zd};
       if (!upd) {
-        launch_k(C(), k_rich_enter_diag<true>, g, kEwThreads, 0, st, in, sc, M, hin, hout, rs, e_set, N);
+        launch_k(C(), k_rich_enter_diag<true>, gv, kEwThreads, 0, st, in, in_inv, sc, M, hin, hout, rs, e_set, N);
         __half *cur = hout, *nxt = hout2;
         for (int k = 1; k < p.m4; k++) {
           const bool last = (k == p.m4 - 1);
@@ -368,7 +428,7 @@ struct Solver {
         }
         if (p.m4 == 1) launch_k(C(), k_rich_exit, g, kEwThreads, 0, st, hout, out, isc, N);
       } else {
-        launch_k(C(), k_rich_enter_diag<false>, g, kEwThreads, 0, st, in, sc, M, hin, hout, rs, e_set, N);
+        launch_k(C(), k_rich_enter_diag<false>, gv, kEwThreads, 0, st, in, in_inv, sc, M, hin, hout, rs, e_set, N);
         F3R_TRY(launch_sell(C(), A.v16, Av, (const __half *)hout, EpiRichWeight{tmp, hin, C().gred(), rs, 0}));
         launch_k(C(), k_rich_scale_om, g, kEwThreads, 0, st, hout, rs, N);
         for (int k = 1; k < p.m4; k++) {
@@ -381,7 +441,7 @@ struct Solver {
       }
     } else {
       // general preconditioner: M = Z W^T (SDAINV) or U^-1 L^-1 (ILU)
-      launch_k(C(), k_rich_cast_in, g, kEwThreads, 0, st, in, sc, hin, e_set, N);
+      launch_k(C(), k_rich_cast_in, g, kEwThreads, 0, st, in, in_inv, sc, hin, e_set, N);
       F3R_TRY(prec_apply(hin, hout, !upd));
       if (upd) {
         F3R_TRY(launch_sell(C(), A.v16, Av, (const __half *)hout, EpiRichWeight{tmp, hin, C().gred(), rs, 0}));
@@ -421,23 +481,29 @@ struct Solver {
   }
 
   // ---- level 3: FGMRES<float>(A16, R, m3), input V2 column, output Z2 col ----
-  Status level3(const float *in, float *out) {
+  // The normalisation V(j+1) *= 1/h of every basis vector is deferred to the
+  // first kernel that reads it next (the Richardson entry), which scales it
+  // in place; the last basis vector of a level is never read again and is
+  // left unscaled.  in_inv is the pending factor of `in` (nullptr if none).
+  Status level3(float *in, float *out, const float *in_inv) {
     Level<float> &L = L3;
     const int64_t N = n;
+    const int gv = C().ew_grid(cdiv(N, 4));
+    float *Vp[kMaxCols];
     Cols<float> V{}, Zc{};
-    V.p[0] = in;
-    for (int k = 1; k <= L.m; k++) V.p[k] = L.V + (size_t)(k - 1) * N;
-    for (int k = 0; k < L.m; k++) Zc.p[k] = L.Z + (size_t)k * N;
+    Vp[0] = in;
+    for (int k = 1; k <= L.m; k++) Vp[k] = L.V + (size_t)(k - 1) * ldn;
+    for (int k = 0; k <= L.m; k++) V.p[k] = Vp[k];
+    for (int k = 0; k < L.m; k++) Zc.p[k] = L.Z + (size_t)k * ldn;
     for (int j = 0; j < L.m; j++) {
-      float *zj = L.Z + (size_t)j * N;
-      float *w = L.V + (size_t)j * N;  // V(j+1)
-      F3R_TRY(rich_apply(V.p[j], zj, j == 0 ? L.e : nullptr));
+      float *zj = L.Z + (size_t)j * ldn;
+      float *w = Vp[j + 1];
+      F3R_TRY(rich_apply(Vp[j], zj, j == 0 ? L.e : nullptr, j == 0 ? in_inv : L.inv));
       F3R_TRY(spmv_dots(A.v16, zj, w, V, j + 1, L.H + (size_t)j * (L.m + 1)));
       GivensCtl<float> g{L.H, L.cs, L.sn, L.e, L.y, L.inv, nullptr, L.m + 1, j, j == L.m - 1, C().err};
-      launch_k(C(), k_cgs_update<float, 8>, C().ew_grid(N), 256, 0, C().stream, w, V, j + 1, N, C().gred(), g);
-      if (j < L.m - 1) launch_k(C(), k_scale<float>, C().ew_grid(N), kEwThreads, 0, C().stream, w, L.inv, N);
+      launch_k(C(), k_cgs_update<float, 8>, gv, 256, 0, C().stream, w, V, j + 1, N, C().gred(), g);
     }
-    launch_k(C(), k_zy<float, float, false>, C().ew_grid(N), kEwThreads, 0, C().stream, Zc, L.y, L.m, out, nullptr, N);
+    launch_k(C(), k_zy<float, float, false>, gv, kEwThreads, 0, C().stream, Zc, L.y, L.m, out, nullptr, N);
     CUDA_TRY(cudaGetLastError());
     return F3R_SUCCESS;
   }
@@ -446,27 +512,30 @@ struct Solver {
   Status level2() {
     Level<float> &L = L2;
     const int64_t N = n;
+    const int gv = C().ew_grid(cdiv(N, 4));
+    float *Vp[kMaxCols];
     Cols<float> V{}, Zc{};
-    for (int k = 0; k <= L.m; k++) V.p[k] = L.V + (size_t)k * N;
-    for (int k = 0; k < L.m; k++) Zc.p[k] = L.Z + (size_t)k * N;
-    launch_k(C(), k_level2_enter, C().ew_grid(N), kEwThreads, 0, C().stream, in_slot, L.V, L.e, N);
+    for (int k = 0; k <= L.m; k++) V.p[k] = Vp[k] = L.V + (size_t)k * ldn;
+    for (int k = 0; k < L.m; k++) Zc.p[k] = L.Z + (size_t)k * ldn;
+    // normalises the outer basis vector in place (its 1/h is L1.inv) and casts it
+    launch_k(C(), k_level2_enter, gv, kEwThreads, 0, C().stream, (double *const *)in_slot, (const double *)L1.inv, L.V,
+             L.e, N);
     for (int j = 0; j < L.m; j++) {
-      float *zj = L.Z + (size_t)j * N;
-      float *w = L.V + (size_t)(j + 1) * N;
-      F3R_TRY(level3(V.p[j], zj));
+      float *zj = L.Z + (size_t)j * ldn;
+      float *w = Vp[j + 1];
+      F3R_TRY(level3(Vp[j], zj, j == 0 ? nullptr : L.inv));
       F3R_TRY(spmv_dots(A.v32, zj, w, V, j + 1, L.H + (size_t)j * (L.m + 1)));
       GivensCtl<float> g{L.H, L.cs, L.sn, L.e, L.y, L.inv, nullptr, L.m + 1, j, j == L.m - 1, C().err};
-      launch_k(C(), k_cgs_update<float, 8>, C().ew_grid(N), 256, 0, C().stream, w, V, j + 1, N, C().gred(), g);
-      if (j < L.m - 1) launch_k(C(), k_scale<float>, C().ew_grid(N), kEwThreads, 0, C().stream, w, L.inv, N);
+      launch_k(C(), k_cgs_update<float, 8>, gv, 256, 0, C().stream, w, V, j + 1, N, C().gred(), g);
     }
-    launch_k(C(), k_zy<float, double, false>, C().ew_grid(N), kEwThreads, 0, C().stream, Zc, L.y, L.m, nullptr, out_slot, N);
+    launch_k(C(), k_zy<float, double, false>, gv, kEwThreads, 0, C().stream, Zc, L.y, L.m, nullptr, out_slot, N);
     CUDA_TRY(cudaGetLastError());
     return F3R_SUCCESS;
   }
 
   // One call into level 2 for outer column j, replayed from a CUDA graph
   // keyed by which Richardson calls inside it update their weights.
-  Status level2_call(const double *in, double *out) {
+  Status level2_call(double *in, double *out) {
     CUDA_TRY(cudaMemcpyAsync((void *)in_slot, &in, sizeof(in), cudaMemcpyHostToDevice, C().stream));
     CUDA_TRY(cudaMemcpyAsync((void *)out_slot, &out, sizeof(out), cudaMemcpyHostToDevice, C().stream));
     // the legacy / per-thread default streams cannot be captured
@@ -525,14 +594,18 @@ struct Solver {
       return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
     };
     const bool b_dev = is_dev(b_user), x_dev = is_dev(x_user);
+    // x is updated with 16-byte vector accesses: a device x that is not
+    // 16-byte aligned is worked on in an internal copy
+    const bool x_direct = x_dev && (reinterpret_cast<uintptr_t>(x_user) % 16 == 0);
     const double *b = b_user;
     double *x = x_user;
     if (!b_dev) {
       CUDA_TRY(cudaMemcpyAsync(b_d, b_user, sizeof(double) * N, cudaMemcpyHostToDevice, st));
       b = b_d;
     }
-    if (!x_dev) {
-      CUDA_TRY(cudaMemcpyAsync(x_d, x_user, sizeof(double) * N, cudaMemcpyHostToDevice, st));
+    if (!x_direct) {
+      CUDA_TRY(cudaMemcpyAsync(x_d, x_user, sizeof(double) * N, x_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                               st));
       x = x_d;
     }
     CUDA_TRY(cudaEventRecord(ev0, st));
@@ -573,8 +646,9 @@ struct Solver {
 
     Level<double> &L = L1;
     Cols<double> V{}, Zc{};
-    for (int k = 0; k <= L.m; k++) V.p[k] = L.V + (size_t)k * N;
-    for (int k = 0; k < L.m; k++) Zc.p[k] = L.Z + (size_t)k * N;
+    const int gv = C().ew_grid(cdiv(N, 2));
+    for (int k = 0; k <= L.m; k++) V.p[k] = L.V + (size_t)k * ldn;
+    for (int k = 0; k < L.m; k++) Zc.p[k] = L.Z + (size_t)k * ldn;
     f3r_result out{};
     int restarts = 0;
     double last_e = 0;
@@ -591,17 +665,17 @@ struct Solver {
         solved = true;
         break;
       }
-      launch_k(C(), k_scale<double>, g, kEwThreads, 0, st, L.V, L.inv, N);
+      // V(0) = r / ||r|| happens inside the level-2 entry kernel (in place)
       int j = 0;
       bool conv = false;
       for (; j < L.m; j++) {
-        double *zj = L.Z + (size_t)j * N;
-        double *w = L.V + (size_t)(j + 1) * N;
-        F3R_TRY(level2_call(V.p[j], zj));
+        double *zj = L.Z + (size_t)j * ldn;
+        double *w = L.V + (size_t)(j + 1) * ldn;
+        F3R_TRY(level2_call(L.V + (size_t)j * ldn, zj));
         F3R_TRY(launch_sell(C(), A.v64, A.view(), (const double *)zj, EpiStore<double>{w, nullptr}));
         launch_k(C(), k_multidot_f64<8>, g, 256, 0, st, w, V, j + 1, N, C().gred(), L.H + (size_t)j * (L.m + 1));
         GivensCtl<double> gc{L.H, L.cs, L.sn, L.e, L.y, L.inv, abs_e, L.m + 1, j, 0, C().err};
-        launch_k(C(), k_cgs_update<double, 8>, g, 256, 0, st, w, V, j + 1, N, C().gred(), gc);
+        launch_k(C(), k_cgs_update<double, 8>, gv, 256, 0, st, w, V, j + 1, N, C().gred(), gc);
         CUDA_TRY(cudaGetLastError());
         double ej;
         F3R_TRY(read_abs_e(&ej));
@@ -612,10 +686,10 @@ struct Solver {
           conv = true;
           break;
         }
-        if (j < L.m - 1) launch_k(C(), k_scale<double>, g, kEwThreads, 0, st, w, L.inv, N);
+        // w = V(j+1) is normalised by the next step's level-2 entry kernel
       }
       launch_k(C(), k_trsv_y<double>, 1, 32, 0, st, L.H, L.e, L.y, L.m + 1, j);
-      launch_k(C(), k_zy<double, double, true>, g, kEwThreads, 0, st, Zc, L.y, j, xs, nullptr, N);
+      launch_k(C(), k_zy<double, double, true>, gv, kEwThreads, 0, st, Zc, L.y, j, xs, nullptr, N);
       CUDA_TRY(cudaGetLastError());
       if (conv) solved = true;
     }
@@ -627,7 +701,9 @@ struct Solver {
     F3R_TRY(launch_sell(C(), A.v64, A.view(), (const double *)xs, EpiResidual<double, double>{bs, r_d, nullptr}));
     launch_k(C(), k_dot<double, double, 8>, g, 256, 0, st, r_d, r_d, N, C().gred(), C().dscratch);
     CUDA_TRY(cudaMemcpyAsync(C().pinned, C().dscratch, sizeof(double), cudaMemcpyDeviceToHost, st));
-    if (!x_dev) CUDA_TRY(cudaMemcpyAsync(x_user, x, sizeof(double) * N, cudaMemcpyDeviceToHost, st));
+    if (!x_direct)
+      CUDA_TRY(cudaMemcpyAsync(x_user, x, sizeof(double) * N, x_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                               st));
     CUDA_TRY(cudaStreamSynchronize(st));
     F3R_TRY(C().check_device_error());
     float ms = 0;
@@ -660,16 +736,20 @@ static Status make_solver(f3r_context *ctx, const f3r_csr *a, const f3r_params *
   s->ctx = ctx;
   s->p = p;
   s->n = a->nrows;
+  s->ldn = ((int64_t)a->nrows + 7) / 8 * 8;
   const int32_t n = a->nrows;
   CUDA_TRY(cudaSetDevice(ctx->device));
   // system matrix in SELL-C-sigma order with all three value copies
   SellHost h;
   F3R_TRY(build_sell(*a, p.sell_sigma, true, h));
+  const std::vector<int32_t> hperm = h.perm;
+  if (p.sell_index16) compress_index16(h);
   F3R_TRY(upload_sell(*ctx, h, (1 << F3R_F64) | (1 << F3R_F32) | (1 << F3R_F16), false, s->A));
-  s->perm = h.perm;
+  h = SellHost();  // release the host copy (up to several GB)
+  s->perm = hperm;
   if (p.sell_sigma > 1) {
     F3R_TRY(s->alloc(&s->perm_d, (size_t)std::max(n, 1)));
-    CUDA_TRY(cudaMemcpy(s->perm_d, h.perm.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(s->perm_d, hperm.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice));
   }
   // the preconditioner, in the permuted order as well
   HostCSR Ah(n, n, a->nnz);
@@ -689,8 +769,8 @@ static Status make_solver(f3r_context *ctx, const f3r_csr *a, const f3r_params *
       s->precond_diag = 1;
       std::vector<double> wdv(n), zdv(n);
       for (int32_t i = 0; i < n; i++) {
-        wdv[i] = Wh->val[Wh->rptr[h.perm[i]]];
-        zdv[i] = Zh->val[Zh->rptr[h.perm[i]]];
+        wdv[i] = Wh->val[Wh->rptr[hperm[i]]];
+        zdv[i] = Zh->val[Zh->rptr[hperm[i]]];
       }
       double *tmp = nullptr;
       F3R_TRY(ctx->alloc((void **)&tmp, sizeof(double) * std::max(n, 1)));
@@ -707,8 +787,12 @@ static Status make_solver(f3r_context *ctx, const f3r_csr *a, const f3r_params *
       // W^T and Z as SELL matrices of the permuted system (same sigma order)
       SellHost hw, hz;
       f3r_csr wv = Wh->view(), zv = Zh->view();
-      F3R_TRY(build_sell(wv, p.sell_sigma, true, hw, &h.perm));
-      F3R_TRY(build_sell(zv, p.sell_sigma, true, hz, &h.perm));
+      F3R_TRY(build_sell(wv, p.sell_sigma, true, hw, &hperm));
+      F3R_TRY(build_sell(zv, p.sell_sigma, true, hz, &hperm));
+      if (p.sell_index16) {
+        compress_index16(hw);
+        compress_index16(hz);
+      }
       F3R_TRY(upload_sell(*ctx, hw, 1 << F3R_F16, false, s->W));
       F3R_TRY(upload_sell(*ctx, hz, 1 << F3R_F16, false, s->Z));
     }
@@ -717,7 +801,7 @@ static Status make_solver(f3r_context *ctx, const f3r_csr *a, const f3r_params *
     std::vector<int32_t> bptr;
     F3R_TRY(ilu0_bj(Ah, p.ilu_blocks, p.acc, &lr, &ur, &bptr));
     std::unique_ptr<HostCSR> Lh(lr), Uh(ur);
-    F3R_TRY(s->ilu.build(ctx->stream, *Lh, *Uh, h.perm, p.sell_sigma > 1, bptr));
+    F3R_TRY(s->ilu.build(ctx->stream, *Lh, *Uh, hperm, p.sell_sigma > 1, bptr));
   }
   // level storage
   F3R_TRY(s->make_level(s->L1, p.m_outer, true));
@@ -899,7 +983,9 @@ f3r_status f3r_context_create(int32_t device, f3r_context **out) {
   auto c = std::make_unique<f3r_context>();
   c->device = device;
   CUDA_TRY(cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device));
-  CUDA_TRY(cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking));
+  // a blocking stream: ordered with the legacy default stream, so device
+  // buffers written there (e.g. by torch) are complete when our kernels run
+  CUDA_TRY(cudaStreamCreate(&c->own));
   c->stream = c->own;
   F3R_TRY(c->alloc((void **)&c->err, sizeof(int)));
   F3R_TRY(c->alloc(&c->partials, kPartialBytes));
@@ -939,14 +1025,16 @@ f3r_status f3r_sell_create(f3r_context *ctx, const f3r_csr *a, int32_t slice_hei
                            int32_t dtype_mask, f3r_sell **out) {
   if (!ctx || !out) return fail(F3R_ERROR_INVALID_VALUE, "null argument");
   if (slice_height != 32) return fail(F3R_ERROR_UNSUPPORTED, "only slice height 32 is implemented");
-  if ((dtype_mask & 7) == 0 || (dtype_mask & ~7)) return fail(F3R_ERROR_INVALID_VALUE, "dtype_mask must select f64/f32/f16");
+  if ((dtype_mask & 7) == 0 || (dtype_mask & ~(7 | F3R_SELL_INDEX16)))
+    return fail(F3R_ERROR_INVALID_VALUE, "dtype_mask must select f64/f32/f16 (plus F3R_SELL_INDEX16)");
   F3R_TRY(check_csr(a));
   CUDA_TRY(cudaSetDevice(ctx->device));
   SellHost h;
   F3R_TRY(build_sell(*a, sigma, false, h));
+  if (dtype_mask & F3R_SELL_INDEX16) compress_index16(h);
   auto m = std::make_unique<f3r_sell>();
   m->ctx = ctx;
-  Status s = upload_sell(*ctx, h, dtype_mask, true, m->d);
+  Status s = upload_sell(*ctx, h, dtype_mask & 7, true, m->d);
   if (s != F3R_SUCCESS) {
     m->d.release();
     return s;
@@ -965,6 +1053,7 @@ f3r_status f3r_sell_info_get(const f3r_sell *m, f3r_sell_info *info) {
   info->nnz_padded = m->d.nnz_pad;
   info->max_width = m->d.max_width;
   info->dtypes = m->d.dtypes;
+  info->index_bits = m->d.index_bits();
   return F3R_SUCCESS;
 }
 void f3r_sell_destroy(f3r_sell *m) {
@@ -1080,10 +1169,30 @@ f3r_status f3r_solver_info(const f3r_solver *s, f3r_sell_info *a_info, int32_t *
     a_info->nnz_padded = d.nnz_pad;
     a_info->max_width = d.max_width;
     a_info->dtypes = d.dtypes;
+    a_info->index_bits = d.index_bits();
   }
   if (precond_diagonal) *precond_diagonal = s->s->precond_diag;
   return F3R_SUCCESS;
 }
+f3r_status f3r_solver_operate(f3r_solver *s, f3r_dtype val_t, f3r_dtype in_t, const void *in, f3r_dtype out_t,
+                              void *out) {
+  if (!s || !in || !out) return fail(F3R_ERROR_INVALID_VALUE, "null argument");
+  Context &c = *s->s->ctx;
+  const DeviceSell &d = s->s->A;
+  const DevSell A = d.view();
+  if (val_t == F3R_F64 && in_t == F3R_F64 && out_t == F3R_F64)
+    return launch_sell(c, d.v64, A, (const double *)in, EpiStore<double>{(double *)out, nullptr});
+  if (val_t == F3R_F32 && in_t == F3R_F32 && out_t == F3R_F32)
+    return launch_sell(c, d.v32, A, (const float *)in, EpiStore<float>{(float *)out, nullptr});
+  if (val_t == F3R_F16 && in_t == F3R_F32 && out_t == F3R_F32)
+    return launch_sell(c, d.v16, A, (const float *)in, EpiStore<float>{(float *)out, nullptr});
+  if (val_t == F3R_F16 && in_t == F3R_F16 && out_t == F3R_F16)
+    return launch_sell(c, d.v16, A, (const __half *)in, EpiStore<__half>{(__half *)out, nullptr});
+  if (val_t == F3R_F16 && in_t == F3R_F16 && out_t == F3R_F32)
+    return launch_sell(c, d.v16, A, (const __half *)in, EpiStore<float>{(float *)out, nullptr});
+  return fail(F3R_ERROR_UNSUPPORTED, "unsupported (val, in, out) type combination");
+}
+
 void f3r_solver_destroy(f3r_solver *s) {
   if (!s) return;
   cudaSetDevice(s->s->ctx->device);

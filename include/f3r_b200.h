@@ -80,7 +80,11 @@ typedef struct f3r_params {
                               back (a linear operator, so the result is unchanged in
                               exact arithmetic) */
   int32_t use_graphs;      /* 1: replay the fixed inner levels as CUDA graphs */
-  int32_t reserved[8];
+  int32_t sell_index16;    /* 0: 32-bit column indices; 1: 16-bit offsets from a per-slice-column
+                              base when every slice column fits a 65536 window (32-bit otherwise).
+                              Fewer bytes, but on B200 the 32-bit form streams faster (the SpMV
+                              is bound by copies in flight, not by bytes) */
+  int32_t reserved[7];
 } f3r_params;
 
 /* Solve outcome.  The first three fields are solve_res_t
@@ -113,7 +117,12 @@ typedef struct f3r_sell_info {
   int64_t nnz_padded;       /* stored entries including slice padding */
   int32_t max_width;        /* widest slice (entries per row) */
   int32_t dtypes;           /* bit (1 << f3r_dtype) set for each value copy held */
+  int32_t index_bits;       /* 16 (offsets from per-slice-column bases) or 32 */
 } f3r_sell_info;
+
+/* f3r_sell_create dtype_mask flag: store the column indices as 16-bit offsets
+ * when they fit (see f3r_params.sell_index16). */
+#define F3R_SELL_INDEX16 (1 << 8)
 
 /* ---------------------------------------------------------------- errors */
 const char *f3r_last_error_string(void);
@@ -177,7 +186,8 @@ f3r_status f3r_context_synchronize(f3r_context *ctx);
  * Device sparse matrix.  Replaces kmm::SELL<32, T, device> (matrix/sell.hpp:
  * 37-97) and SELLsig<32, sigma, T, device> (sell.hpp:99-166).  One column
  * index array is shared by the fp64 / fp32 / fp16 value copies selected by
- * dtype_mask (bit 1 << f3r_dtype). */
+ * dtype_mask (bit 1 << f3r_dtype); with F3R_SELL_INDEX16 the indices are
+ * stored as 16-bit offsets when they fit. */
 f3r_status f3r_sell_create(f3r_context *ctx, const f3r_csr *a, int32_t slice_height,
                            int32_t sigma, int32_t dtype_mask, f3r_sell **out);
 f3r_status f3r_sell_info_get(const f3r_sell *m, f3r_sell_info *info);
@@ -234,6 +244,13 @@ f3r_status f3r_solver_create(f3r_context *ctx, const f3r_csr *a, const f3r_param
 f3r_status f3r_solver_solve(f3r_solver *s, const double *b, double *x, f3r_cond_fn cond,
                             void *user, f3r_result *result);
 f3r_status f3r_solver_info(const f3r_solver *s, f3r_sell_info *a_info, int32_t *precond_diagonal);
+/* out = A in with the solver's own device copy of A (the matrix its levels
+ * use: SELL-C-sigma, rows and columns in the solver's storage order P A P^T,
+ * so with sigma > 1 `in` and `out` are in that order too).  Same type
+ * combinations as f3r_sell_operate.  The kernel-level view of
+ * CoefficientMatrix::operate (models.hpp:133-136) on the solved system. */
+f3r_status f3r_solver_operate(f3r_solver *s, f3r_dtype val_t, f3r_dtype in_t, const void *in, f3r_dtype out_t,
+                              void *out);
 void f3r_solver_destroy(f3r_solver *s);
 
 #ifdef __cplusplus

@@ -1,0 +1,144 @@
+"""Generates the golden fixtures in tests/golden/ from the reference itself.
+
+Runs the reference's own code, compiled in place from the reference tree into
+oracle/_ref/libf3r_ref.so (oracle/Makefile, deterministic flags: no FMA
+contraction, one OpenMP thread), and records its outputs:
+
+  generators.npz   matrix/hpcg.cpp and matrix/hpgmp.cpp stencils (+ the
+                   half-space variant through io::CSR), small grids
+  setup.npz        algorithm::scaling, csr_to_sell<32>, algorithm::sdainv,
+                   block-Jacobi ILU(0) factors and their fp16 BJ solves
+  spmv.npz         SELL<32>::operate / compute_residual at the F3R level types
+  solves.npz       full F3R solves (SDAINV + SELL-32, and BJ-ILU(0) + CSR):
+                   outer iteration counts, residual histories, final residuals
+
+Usage (needs the reference tree; the fixtures are committed):
+    OMP_NUM_THREADS=1 python tests/golden/gen_golden.py [--big]
+--big adds the 64^3 CPU configuration and the 192^3 GPU configuration solve
+(about a minute of CPU each).
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+os.environ.setdefault("OMP_NUM_THREADS", "1")
+
+from oracle import oracle as O  # noqa: E402
+
+
+def rhs_for(ref, rptr, idx, val, seed):
+    """b = A x*, x* ~ U(-1, 1) from a fixed numpy seed (fp64 SpMV of the reference)."""
+    n = len(rptr) - 1
+    xs = np.random.default_rng(seed).uniform(-1.0, 1.0, n)
+    b = ref.sell32_operate(rptr, idx, val, 0, xs)
+    return xs, b
+
+
+def main(big: bool):
+    O.build()
+    ref = O.Ref("golden")
+    out = {}
+
+    # ---- generators -------------------------------------------------------
+    g = {}
+    for variant in (0, 1, 2):
+        for dims in ((5, 6, 7), (8, 8, 8)):
+            r, i, v = ref.gen27(*dims, variant=variant, beta=0.5)
+            key = f"v{variant}_{dims[0]}x{dims[1]}x{dims[2]}"
+            g[key + "_rptr"], g[key + "_idx"], g[key + "_val"] = r, i, v
+    np.savez_compressed(os.path.join(HERE, "generators.npz"), **g)
+
+    # ---- set-up: scaling, SELL, SDAINV, ILU -------------------------------
+    s = {}
+    r, i, v = ref.gen27(8, 8, 8, variant=1)
+    vs = ref.scaling(r, i, v)
+    s["hpgmp8_rptr"], s["hpgmp8_idx"], s["hpgmp8_val"], s["hpgmp8_scaled"] = r, i, v, vs
+    sp, si, sv = ref.sell32(r, i, vs)
+    s["hpgmp8_sell_sptr"], s["hpgmp8_sell_idx"], s["hpgmp8_sell_val"] = sp, si, sv
+    # a ragged matrix: 7-point diffusion with random coefficients, odd size
+    import f3r_b200 as F  # host-side generator only (no GPU needed)
+    D = F.diffusion7(6, 7, 9, 1.5, 2.0, 5)
+    dr, di, dv = D.arrays()
+    dvs = ref.scaling(dr, di, dv)
+    s["diff_rptr"], s["diff_idx"], s["diff_val"], s["diff_scaled"] = dr, di, dv, dvs
+    sp, si, sv = ref.sell32(dr, di, dvs)
+    s["diff_sell_sptr"], s["diff_sell_idx"], s["diff_sell_val"] = sp, si, sv
+    for name, (rr, ii, vv) in (("hpgmp8", (r, i, vs)), ("diff", (dr, di, dvs))):
+        (zr, zi, zv), (wr, wi, wv) = ref.sdainv(rr, ii, vv, 0.1, 1.0)
+        s[f"{name}_Z_rptr"], s[f"{name}_Z_idx"], s[f"{name}_Z_val"] = zr, zi, zv
+        s[f"{name}_W_rptr"], s[f"{name}_W_idx"], s[f"{name}_W_val"] = wr, wi, wv
+        (zr, zi, zv), (wr, wi, wv) = ref.sdainv(rr, ii, vv, 0.05, 1.2)
+        s[f"{name}_Zb_rptr"], s[f"{name}_Zb_idx"], s[f"{name}_Zb_val"] = zr, zi, zv
+        s[f"{name}_Wb_rptr"], s[f"{name}_Wb_idx"], s[f"{name}_Wb_val"] = wr, wi, wv
+    hr, hi, hv = ref.gen27(8, 8, 8, variant=0)
+    hvs = ref.scaling(hr, hi, hv)
+    x16 = np.random.default_rng(3).standard_normal(len(hr) - 1).astype(np.float16)
+    for blocks, acc in ((16, 1.0), (7, 1.3)):
+        (L, U), lo, up = ref.ilu0_bj(hr, hi, hvs, blocks, acc, solve_in=x16)
+        key = f"hpcg8_ilu{blocks}"
+        s[key + "_L_rptr"], s[key + "_L_idx"], s[key + "_L_val"] = L
+        s[key + "_U_rptr"], s[key + "_U_idx"], s[key + "_U_val"] = U
+        s[key + "_lower"], s[key + "_upper"] = lo, up
+    s["hpcg8_rptr"], s["hpcg8_idx"], s["hpcg8_scaled"], s["bj_in"] = hr, hi, hvs, x16
+    np.savez_compressed(os.path.join(HERE, "setup.npz"), **s)
+
+    # ---- SpMV kinds --------------------------------------------------------
+    m = {}
+    rng = np.random.default_rng(11)
+    for name, (rr, ii, vv) in (("hpgmp8", (r, i, vs)), ("diff", (dr, di, dvs))):
+        n = len(rr) - 1
+        x64 = rng.standard_normal(n)
+        m[f"{name}_x64"] = x64
+        m[f"{name}_y0"] = ref.sell32_operate(rr, ii, vv, 0, x64)
+        m[f"{name}_y1"] = ref.sell32_operate(rr, ii, vv, 1, x64.astype(np.float32))
+        m[f"{name}_y2"] = ref.sell32_operate(rr, ii, vv, 2, x64.astype(np.float32))
+        m[f"{name}_y3"] = ref.sell32_operate(rr, ii, vv, 3, (0.25 * x64).astype(np.float16))
+        b64 = rng.standard_normal(n)
+        m[f"{name}_b64"] = b64
+        m[f"{name}_r0"] = ref.sell32_residual(rr, ii, vv, 0, b64, x64)
+        m[f"{name}_r3"] = ref.sell32_residual(rr, ii, vv, 3, b64.astype(np.float16),
+                                              (0.1 * x64).astype(np.float16))
+    np.savez_compressed(os.path.join(HERE, "spmv.npz"), **m)
+
+    # ---- solves --------------------------------------------------------------
+    sol = {}
+    cases = [("sdainv_hpgmp16", 0, (16, 16, 16, 1), 0), ("sdainv_half16", 0, (16, 16, 16, 2), 1),
+             ("sdainv_diff12", 0, None, 2), ("bjilu_hpcg16", 1, (16, 16, 16, 0), 3)]
+    if big:
+        cases += [("bjilu_hpcg64", 1, (64, 64, 64, 0), 4), ("sdainv_half192", 0, (192, 192, 192, 2), 5)]
+    for name, config, spec, seed in cases:
+        if spec is None:
+            D = F.diffusion7(12, 12, 12, 1.5, 3.0, 9)
+            rr, ii, vv = D.arrays()
+        else:
+            rr, ii, vv = ref.gen27(*spec[:3], variant=spec[3], beta=0.5)
+        vv = ref.scaling(rr, ii, vv)
+        xs, b = rhs_for(ref, rr, ii, vv, seed)
+        blocks = 16 if spec is not None and spec[0] == 16 else 112
+        res = ref.f3r_solve(config, rr, ii, vv, b, tol=1e-10, c=64 if spec and spec[0] >= 64 else 8,
+                            blocks=blocks)
+        print(name, res["iters"], res["impl_res"], res["expl_res"], res["time_s"])
+        sol[name + "_iters"] = np.array(res["iters"])
+        sol[name + "_hist"] = res["hist"]
+        sol[name + "_expl"] = np.array(res["expl_res"])
+        sol[name + "_seed"] = np.array(seed)
+        sol[name + "_blocks"] = np.array(blocks)
+        if len(rr) - 1 <= 8192:
+            sol[name + "_x"] = res["x"]
+    existing = os.path.join(HERE, "solves.npz")
+    if not big and os.path.exists(existing):
+        old = dict(np.load(existing))
+        for k, v in old.items():
+            if k not in sol:
+                sol[k] = v
+    np.savez_compressed(existing, **sol)
+
+
+if __name__ == "__main__":
+    main("--big" in sys.argv)

@@ -35,10 +35,11 @@ def oracle_solve(A, b, precond=O.PRECOND_SDAINV, blocks=16, **kw):
     return O.f3r_solve(M, P1, P2, b, p)
 
 
-@pytest.mark.parametrize("nx,graphs", [(16, 1), (24, 0), (32, 1)])
-def test_solve_matches_oracle(ctx, nx, graphs):
+@pytest.mark.parametrize("nx,graphs,index16", [(16, 1, 0), (24, 0, 0), (32, 1, 0), (24, 1, 1)])
+def test_solve_matches_oracle(ctx, nx, graphs, index16):
     A, b, xs = system(nx)
-    S = F.Solver(ctx, A, rel_tol=1e-10, use_graphs=graphs)
+    S = F.Solver(ctx, A, rel_tol=1e-10, use_graphs=graphs, sell_index16=index16)
+    assert S.info()[0].index_bits == (16 if index16 else 32)
     x = np.zeros_like(b)
     r = S.solve(b, x)
     o = oracle_solve(A, b, tol=1e-10)

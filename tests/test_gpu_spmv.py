@@ -46,12 +46,13 @@ def matrices():
     yield "diffusion7", F.diffusion7(10, 9, 8, 2.5, 3.0, 1).scale()
 
 
-@pytest.mark.parametrize("sigma", [1, 256])
-def test_operate_bitexact(ctx, sigma):
+@pytest.mark.parametrize("sigma,index16", [(1, False), (256, False), (1, True), (256, True)])
+def test_operate_bitexact(ctx, sigma, index16):
     for name, A in matrices():
         rptr, idx, val = A.arrays()
         n = A.shape[0]
-        S = F.Sell(ctx, A, sigma=sigma)
+        S = F.Sell(ctx, A, sigma=sigma, index16=index16)
+        assert S.info().index_bits == (16 if index16 else 32)
         rng = np.random.default_rng(1)
         x64 = rng.standard_normal(n)
         x32 = x64.astype(np.float32)
@@ -81,12 +82,12 @@ def test_operate_bitexact(ctx, sigma):
         S.close()
 
 
-@pytest.mark.parametrize("sigma", [1, 32])
-def test_residual_bitexact(ctx, sigma):
+@pytest.mark.parametrize("sigma,index16", [(1, False), (32, False), (32, True)])
+def test_residual_bitexact(ctx, sigma, index16):
     for name, A in matrices():
         rptr, idx, val = A.arrays()
         n = A.shape[0]
-        S = F.Sell(ctx, A, sigma=sigma)
+        S = F.Sell(ctx, A, sigma=sigma, index16=index16)
         rng = np.random.default_rng(2)
         for dt, odt in ((np.float64, O.DT_F64), (np.float32, O.DT_F32), (np.float16, O.DT_F16)):
             x = (rng.standard_normal(n) * 0.1).astype(dt)
@@ -99,6 +100,21 @@ def test_residual_bitexact(ctx, sigma):
             ref = O.spmv(rptr, idx, val, x, odt, odt, acc, b=b)
             assert np.array_equal(r.cpu().numpy().view(np.uint8), ref.view(np.uint8)), (name, dt)
         S.close()
+
+
+def test_wide_columns_fall_back_to_32bit(ctx):
+    """rows whose columns spread over more than 65536 keep 32-bit indices"""
+    n = 70000
+    rptr, idx, val = ragged_matrix(n, seed=11, empty_every=5)
+    A = F.HostMatrix.from_csr(rptr, idx, val)
+    S = F.Sell(ctx, A, index16=True)
+    assert S.info().index_bits == 32
+    x = np.random.default_rng(4).standard_normal(n)
+    y = torch.zeros(n, dtype=torch.float64, device="cuda")
+    S.operate(torch.from_numpy(x).cuda(), y)
+    torch.cuda.synchronize()
+    ref = O.spmv(rptr, idx, val, x, O.DT_F64, O.DT_F64, O.DT_F64)
+    assert np.array_equal(y.cpu().numpy(), ref)
 
 
 def test_fp16_within_reference_bound(ctx):

@@ -1,0 +1,160 @@
+"""Pins the oracle (and the library's host-side set-up) to the reference.
+
+The golden fixtures in tests/golden/ were recorded from the reference's own
+code compiled in place (tests/golden/gen_golden.py).  Here the C restatement
+(oracle/f3r_oracle.c) and the product's host routines (f3r_b200, CPU only)
+must reproduce them: bit for bit for every integer / index structure and for
+the fp64 set-up arithmetic, and on iteration counts and residuals for solves.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import f3r_b200 as F
+from oracle import oracle as O
+
+G = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def load(name):
+    return dict(np.load(os.path.join(G, name)))
+
+
+def same(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return a.shape == b.shape and np.array_equal(a.view(np.uint8), b.view(np.uint8))
+
+
+def test_generators():
+    g = load("generators.npz")
+    for variant in (0, 1, 2):
+        for dims in ((5, 6, 7), (8, 8, 8)):
+            key = f"v{variant}_{dims[0]}x{dims[1]}x{dims[2]}"
+            want = (g[key + "_rptr"], g[key + "_idx"], g[key + "_val"])
+            got = O.stencil27(*dims, variant=variant, beta=0.5)
+            assert all(same(a, b) for a, b in zip(got, want)), key
+            lib = F.stencil27(*dims, variant, 0.5).arrays()
+            assert all(same(a, b) for a, b in zip(lib, want)), key
+
+
+def test_scaling_and_sell():
+    s = load("setup.npz")
+    for name in ("hpgmp8", "diff"):
+        r, i, v = s[f"{name}_rptr"], s[f"{name}_idx"], s[f"{name}_val"]
+        assert same(O.scaling(r, i, v), s[f"{name}_scaled"])
+        H = F.HostMatrix.from_csr(r, i, v).scale()
+        assert same(H.arrays()[2], s[f"{name}_scaled"])
+        sell = O.csr_to_sell(r, i, s[f"{name}_scaled"])
+        assert same(sell[0], s[f"{name}_sell_sptr"])
+        assert same(sell[1], s[f"{name}_sell_idx"])
+        assert same(sell[2], s[f"{name}_sell_val"])
+
+
+@pytest.mark.parametrize("suffix,tol,acc", [("", 0.1, 1.0), ("b", 0.05, 1.2)])
+def test_sdainv(suffix, tol, acc):
+    s = load("setup.npz")
+    for name in ("hpgmp8", "diff"):
+        r, i, v = s[f"{name}_rptr"], s[f"{name}_idx"], s[f"{name}_scaled"]
+        Zo, Wo = O.sdainv(O.Mat.from_csr(r, i, v), tol, acc)
+        Zl, Wl = F.HostMatrix.from_csr(r, i, v).sdainv(tol, acc)
+        for tag, o, l in (("Z", Zo, Zl), ("W", Wo, Wl)):
+            want = (s[f"{name}_{tag}{suffix}_rptr"], s[f"{name}_{tag}{suffix}_idx"], s[f"{name}_{tag}{suffix}_val"])
+            assert all(same(a, b) for a, b in zip(o.csr(), want)), (name, tag)
+            assert all(same(a, b) for a, b in zip(l.arrays(), want)), (name, tag)
+
+
+@pytest.mark.parametrize("blocks,acc", [(16, 1.0), (7, 1.3)])
+def test_ilu0_bj_and_trsv(blocks, acc):
+    s = load("setup.npz")
+    r, i, v = s["hpcg8_rptr"], s["hpcg8_idx"], s["hpcg8_scaled"]
+    key = f"hpcg8_ilu{blocks}"
+    Lo, Uo = O.ilu0_bj(O.Mat.from_csr(r, i, v), blocks, acc)
+    Ll, Ul = F.HostMatrix.from_csr(r, i, v).ilu0_bj(blocks, acc)
+    for tag, o, l in (("L", Lo, Ll), ("U", Uo, Ul)):
+        want = (s[f"{key}_{tag}_rptr"], s[f"{key}_{tag}_idx"], s[f"{key}_{tag}_val"])
+        assert all(same(a, b) for a, b in zip(o.csr(), want)), tag
+        assert all(same(a, b) for a, b in zip(l.arrays(), want)), tag
+    # the reference's fp16 BJ sweeps (fp16 arithmetic) are reproduced exactly
+    assert same(O.trsv(Lo, False, s["bj_in"]), s[key + "_lower"])
+    assert same(O.trsv(Uo, True, s["bj_in"]), s[key + "_upper"])
+
+
+def test_ilu_rejects_overrunning_block_counts():
+    s = load("setup.npz")
+    A = O.Mat.from_csr(s["hpcg8_rptr"], s["hpcg8_idx"], s["hpcg8_scaled"])
+    with pytest.raises(ValueError):
+        O.ilu0_bj(A, 112)  # 512 rows: (112-1)*ceil(512/112) > 512
+    with pytest.raises(F.F3RError):
+        F.HostMatrix.from_csr(s["hpcg8_rptr"], s["hpcg8_idx"], s["hpcg8_scaled"]).ilu0_bj(112)
+
+
+def test_spmv_kinds():
+    s = load("setup.npz")
+    m = load("spmv.npz")
+    for name in ("hpgmp8", "diff"):
+        r, i, v = s[f"{name}_rptr"], s[f"{name}_idx"], s[f"{name}_scaled"]
+        x64 = m[f"{name}_x64"]
+        # fp64 and fp32: the reference's expression order (no fma) is exact
+        assert same(O.spmv(r, i, v, x64, O.DT_F64, O.DT_F64, O.DT_F64, ref_mul_add=True), m[f"{name}_y0"])
+        assert same(O.spmv(r, i, v, x64.astype(np.float32), O.DT_F32, O.DT_F32, O.DT_F32, ref_mul_add=True),
+                    m[f"{name}_y1"])
+        assert same(O.spmv(r, i, v, x64.astype(np.float32), O.DT_F16, O.DT_F32, O.DT_F32, ref_mul_add=True),
+                    m[f"{name}_y2"])
+        assert same(O.spmv(r, i, v, m[f"{name}_b64"] * 0 + x64, O.DT_F64, O.DT_F64, O.DT_F64, ref_mul_add=True,
+                           b=m[f"{name}_b64"]), m[f"{name}_r0"])
+        # fp16 x fp16 accumulated in fp16 (the reference) vs fp32 accumulation
+        # (this library): within nnz_row * 2^-11 * |A||x|
+        x16 = (0.25 * x64).astype(np.float16)
+        got = O.spmv(r, i, v, x16, O.DT_F16, O.DT_F16, O.DT_F32).astype(np.float64)
+        want = m[f"{name}_y3"].astype(np.float64)
+        absAx = O.spmv(r, i, np.abs(v), np.abs(x16.astype(np.float64)), O.DT_F64, O.DT_F64, O.DT_F64)
+        bound = np.diff(r) * 2.0 ** -11 * absAx + 2.0 ** -24
+        assert np.all(np.abs(got - want) <= 2 * bound), name
+        # and the oracle's fp16-accumulation model is close to the reference's
+        got16 = O.spmv(r, i, v, x16, O.DT_F16, O.DT_F16, O.DT_F16).astype(np.float64)
+        assert np.all(np.abs(got16 - want) <= 2 * bound), name
+
+
+def _problem(name):
+    if name.startswith("sdainv_diff"):
+        D = F.diffusion7(12, 12, 12, 1.5, 3.0, 9)
+        return D.arrays()
+    spec = {"sdainv_hpgmp16": (16, 16, 16, 1), "sdainv_half16": (16, 16, 16, 2), "bjilu_hpcg16": (16, 16, 16, 0),
+            "bjilu_hpcg64": (64, 64, 64, 0), "sdainv_half192": (192, 192, 192, 2)}[name]
+    return O.stencil27(*spec[:3], variant=spec[3], beta=0.5)
+
+
+def golden_system(name):
+    """The exact (A, b) the reference solved: scaled matrix and b = A x* (fp64,
+    reference expression order)."""
+    sol = load("solves.npz")
+    r, i, v = _problem(name)
+    v = O.scaling(r, i, v)
+    seed = int(sol[name + "_seed"])
+    xs = np.random.default_rng(seed).uniform(-1.0, 1.0, len(r) - 1)
+    b = O.spmv(r, i, v, xs, O.DT_F64, O.DT_F64, O.DT_F64, ref_mul_add=True)
+    return r, i, v, b, xs, sol
+
+
+@pytest.mark.parametrize("name", ["sdainv_hpgmp16", "sdainv_half16", "sdainv_diff12", "bjilu_hpcg16"])
+def test_oracle_solve_matches_reference(name):
+    r, i, v, b, xs, sol = golden_system(name)
+    A = O.Mat.from_csr(r, i, v)
+    if name.startswith("sdainv"):
+        Z, W = O.sdainv(A)
+        P1, P2, pc = W, Z, O.PRECOND_SDAINV
+    else:
+        P1, P2 = O.ilu0_bj(A, int(sol[name + "_blocks"]))
+        pc = O.PRECOND_ILU0_BJ
+    for arith in (O.ARITH_PRODUCT, O.ARITH_REF):
+        o = O.f3r_solve(A, P1, P2, b, O.params(precond=pc, c=8, tol=1e-10, arith=arith))
+        assert o["solved"]
+        assert abs(o["iters"] - int(sol[name + "_iters"])) <= 1, (name, arith)
+        res = np.linalg.norm(b - O.spmv(r, i, v, o["x"], O.DT_F64, O.DT_F64, O.DT_F64)) / np.linalg.norm(b)
+        assert res < 1e-10
+        # the first outer step reduces the residual by the same order of magnitude
+        h = sol[name + "_hist"]
+        assert abs(np.log10(o["hist"][0]) - np.log10(h[0])) < 1.0, (o["hist"][0], h[0])
+        if name + "_x" in sol:
+            assert np.linalg.norm(o["x"] - sol[name + "_x"]) / np.linalg.norm(sol[name + "_x"]) < 1e-8
