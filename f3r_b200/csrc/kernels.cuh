@@ -95,12 +95,12 @@ template <typename T> __global__ void k_trsv_y(T *H, const T *e, T *y, int ldh, 
 
 // Inner levels (fp32 vectors): w = A z stored, and H(j, k) = <w, V(k)>,
 // k = 0..nv-1, fused (CGS dots all use the unmodified w, gmres.hpp:112-114).
-template <int NVT> struct EpiStoreDots {
+template <int NVT, bool PREFETCH = (NVT <= 4)> struct EpiStoreDots {
   using Red = float;
   static constexpr int NV = NVT;
   // up to 4 basis values are fetched ahead of the multiply-add chain; wider
   // epilogues read them afterwards (their registers would spill)
-  static constexpr bool PRE = NVT <= 4;
+  static constexpr bool PRE = PREFETCH;
   struct Pre {
     float v[PRE ? NVT : 1];
   };
@@ -258,6 +258,42 @@ __global__ void __launch_bounds__(WARPS * 32) k_multidot_f64(const double *__res
   }
   __syncthreads();
   if (threadIdx.x == 0) *gr.ticket = 0;
+}
+
+// H(j, k) = <w, V(k)> for k < nv in fp32 (inner levels), one pass over w and
+// the nv basis columns with 16-byte loads; the fp32 accumulators of a thread
+// are reduced per block and then in block order by the last block.  This is
+// the CGS dot phase (gmres.hpp:112-114, all dots with the unmodified w).
+template <int MAXV, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32) k_multidot_f32(const float *__restrict__ w, Cols<float> V, int nv,
+                                                             int64_t n, GridRed gr, float *hcol) {
+  float a[MAXV];
+#pragma unroll
+  for (int k = 0; k < MAXV; k++) a[k] = 0.0f;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x, tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t nq = n / 4;
+  for (int64_t q = tid; q < nq; q += stride) {
+    const VecN<float, 4> wv = ldv<float, 4>(w + 4 * q);
+#pragma unroll
+    for (int k = 0; k < MAXV; k++) {
+      if (k < nv) {
+        const VecN<float, 4> v = ldv<float, 4>(V.p[k] + 4 * q);
+#pragma unroll
+        for (int e = 0; e < 4; e++) a[k] = __fmaf_rn(wv.v[e], v.v[e], a[k]);
+      }
+    }
+  }
+  for (int64_t i = nq * 4 + tid; i < n; i += stride) {
+    const float wi = w[i];
+#pragma unroll
+    for (int k = 0; k < MAXV; k++)
+      if (k < nv) a[k] = __fmaf_rn(wi, V.p[k][i], a[k]);
+  }
+  float *h = hcol;
+  const int m = nv;
+  grid_reduce<float, MAXV, WARPS>(a, nv, gr, [h, m](float *tot) {
+    for (int k = 0; k < m; k++) h[k] = tot[k];
+  });
 }
 
 // v *= *inv  (V(j+1) *= h.inv(), gmres.hpp:117)
@@ -435,7 +471,7 @@ __global__ void k_rich_cast_in(float *__restrict__ in, const float *__restrict__
 // Residual step of R with the diagonal preconditioner fused (no weight
 // update): hr = fp16(hin - A16 hout); t2 = M hr; hnew = fp16(hout + ome[k] t2);
 // the last step writes out = fp32(hnew) / sc (out.copy(hout)).
-struct EpiRichStep {
+template <bool PREFETCH = true> struct EpiRichStepT {
   using Red = float;
   static constexpr int NV = 0;
   struct Pre {
@@ -448,8 +484,12 @@ struct EpiRichStep {
   __half *hnext;  // next hout (steps before the last)
   float *out;     // fp32 result (last step)
   float isc;
-  __device__ __forceinline__ Pre load(int64_t r) const { return {hin[r], hout[r], M.w[r], M.z[r], rs->ome[k]}; }
-  template <typename Acc> __device__ __forceinline__ void row(int64_t r, Acc acc, const Pre &p, Red (&)[1]) const {
+  __device__ __forceinline__ Pre load(int64_t r) const {
+    if (PREFETCH) return {hin[r], hout[r], M.w[r], M.z[r], rs->ome[k]};
+    return {};
+  }
+  template <typename Acc> __device__ __forceinline__ void row(int64_t r, Acc acc, const Pre &pp, Red (&)[1]) const {
+    const Pre p = PREFETCH ? pp : Pre{hin[r], hout[r], M.w[r], M.z[r], rs->ome[k]};
     const float hr = h2f(f2h(h2f(p.hin) - (float)acc));
     const float t = h2f(f2h(h2f(p.w) * hr));
     const float t2 = h2f(f2h(h2f(p.z) * t));
@@ -459,6 +499,7 @@ struct EpiRichStep {
   }
   template <int W> __device__ __forceinline__ void finish(Red (&)[1]) const {}
 };
+using EpiRichStep = EpiRichStepT<true>;
 
 // Residual step of an update call (diagonal M): stores hr and t2 = M hr.
 struct EpiRichResPre {

@@ -45,7 +45,6 @@ static inline int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
 // ---------------------------------------------------------------------------
 // context
 // ---------------------------------------------------------------------------
-constexpr size_t kPartialBytes = 1u << 20;
 
 struct Context {
   int device = 0;
@@ -67,7 +66,9 @@ struct Context {
     return F3R_SUCCESS;
   }
   GridRed gred() const { return GridRed{partials, ticket}; }
-  int ew_grid(int64_t n) const { return (int)std::max<int64_t>(1, std::min<int64_t>(cdiv(n, kEwThreads), (int64_t)sm_count * 4)); }
+  // grid for the elementwise / reduction kernels: up to 8 blocks of 256 per SM
+  // (full thread occupancy); partial-sum buffers are sized for this bound
+  int ew_grid(int64_t n) const { return (int)std::max<int64_t>(1, std::min<int64_t>(cdiv(n, kEwThreads), (int64_t)sm_count * 8)); }
   // checks the device error word (after a synchronisation)
   Status check_device_error() {
     int e = 0;
@@ -473,11 +474,32 @@ struct Solver {
 
   // w = A z with H(j, 0..nv-1) = <w, V(k)> fused; the dot count picks the
   // smallest epilogue instantiation (registers)
+  //
+  // The dots can ride in the SpMV epilogue (one read of w less) or run as a
+  // separate vectorised pass.  On B200 the SELL kernel is bound by the
+  // latency of each warp's slice loop, and the fused epilogue stretches it:
+  // 239 us fused against 187 + ~20 us separate for the 192^3 fp16 product, so
+  // the fp16 level uses the separate pass; the fp32 level keeps the fusion
+  // for up to 4 dots (its product streams more bytes per slice and hides the
+  // epilogue: 244 us fused against 228 + ~20 us) and separates wider ones.
   template <typename V>
   Status spmv_dots(const V *vals, const float *z, float *w, const Cols<float> &Vc, int nv, float *hcol) {
+    if (sizeof(V) == 2 || nv > 4) {
+      F3R_TRY(launch_sell(C(), vals, A.view(), z, EpiStore<float>{w, nullptr}));
+      const int gv = C().ew_grid(cdiv(n, 4));
+      if (nv <= 4)
+        launch_k(C(), k_multidot_f32<4, 8>, gv, 256, 0, C().stream, (const float *)w, Vc, nv, (int64_t)n, C().gred(),
+                 hcol);
+      else if (nv <= 8)
+        launch_k(C(), k_multidot_f32<8, 8>, gv, 256, 0, C().stream, (const float *)w, Vc, nv, (int64_t)n, C().gred(),
+                 hcol);
+      else
+        launch_k(C(), k_multidot_f32<kMaxDots, 8>, gv, 256, 0, C().stream, (const float *)w, Vc, nv, (int64_t)n,
+                 C().gred(), hcol);
+      return F3R_SUCCESS;
+    }
     if (nv <= 4) return launch_sell(C(), vals, A.view(), z, EpiStoreDots<4>{w, Vc, nv, C().gred(), hcol});
-    if (nv <= 8) return launch_sell(C(), vals, A.view(), z, EpiStoreDots<8>{w, Vc, nv, C().gred(), hcol});
-    return launch_sell(C(), vals, A.view(), z, EpiStoreDots<kMaxDots>{w, Vc, nv, C().gred(), hcol});
+    return launch_sell(C(), vals, A.view(), z, EpiStoreDots<8>{w, Vc, nv, C().gred(), hcol});
   }
 
   // ---- level 3: FGMRES<float>(A16, R, m3), input V2 column, output Z2 col ----
@@ -844,6 +866,8 @@ static Status make_solver(f3r_context *ctx, const f3r_csr *a, const f3r_params *
   F3R_TRY((sell_attr<__half, __half, EpiRichResPre>(cx)));
   F3R_TRY((sell_attr<__half, __half, EpiResidual<__half, __half>>(cx)));
   F3R_TRY((sell_attr<__half, __half, EpiStore<__half>>(cx)));
+  F3R_TRY((sell_attr<__half, float, EpiStore<float>>(cx)));
+  F3R_TRY((sell_attr<float, float, EpiStore<float>>(cx)));
   F3R_TRY((sell_attr<__half, __half, EpiZScale>(cx)));
   CUDA_TRY(cudaDeviceSynchronize());
   *out = s.release();
@@ -988,7 +1012,9 @@ f3r_status f3r_context_create(int32_t device, f3r_context **out) {
   CUDA_TRY(cudaStreamCreate(&c->own));
   c->stream = c->own;
   F3R_TRY(c->alloc((void **)&c->err, sizeof(int)));
-  F3R_TRY(c->alloc(&c->partials, kPartialBytes));
+  // one partial sum per block and dot: at most 8 blocks per SM (ew_grid) and
+  // kMaxCols dots (the outer multi-dot), in fp64
+  F3R_TRY(c->alloc(&c->partials, (size_t)c->sm_count * 8 * kMaxCols * sizeof(double)));
   F3R_TRY(c->alloc((void **)&c->ticket, sizeof(unsigned int) * 4));
   F3R_TRY(c->alloc((void **)&c->dscratch, sizeof(double) * 4));
   CUDA_TRY(cudaMemset(c->err, 0, sizeof(int)));
