@@ -190,6 +190,14 @@ class Sell:
         check(lib().f3r_sell_compute_residual(self._h, vt, bt, C.c_void_p(b.data_ptr()), xt,
                                               C.c_void_p(x.data_ptr()), rt, C.c_void_p(r.data_ptr())))
 
+    def tune(self, val_t=F16, reps=20):
+        """Times out = A x at every launch shape the library carries (fastest first)."""
+        buf = (_capi.TuneEntry * 64)()
+        cnt = C.c_int32()
+        check(lib().f3r_sell_tune(self._h, val_t, reps, buf, 64, C.byref(cnt)))
+        return [dict(warps=e.warps, stages=e.stages, kc=e.kc, index_bits=e.index_bits, default=bool(e.is_default),
+                     us=e.microseconds, gbs=e.gbs_algorithmic) for e in buf[:cnt.value]]
+
     def close(self):
         if getattr(self, "_h", None) is not None and _capi is not None and _capi._lib is not None:
             _capi._lib.f3r_sell_destroy(self._h)

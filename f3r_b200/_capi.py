@@ -51,6 +51,12 @@ class SellInfo(C.Structure):
                 ("dtypes", C.c_int32), ("index_bits", C.c_int32)]
 
 
+class TuneEntry(C.Structure):
+    _fields_ = [("warps", C.c_int32), ("stages", C.c_int32), ("kc", C.c_int32), ("index_bits", C.c_int32),
+                ("is_default", C.c_int32), ("reserved", C.c_int32), ("microseconds", C.c_double),
+                ("gbs_algorithmic", C.c_double)]
+
+
 COND_FN = C.CFUNCTYPE(C.c_int, C.c_int32, C.c_double, C.c_void_p)
 
 _vp = C.c_void_p
@@ -77,6 +83,7 @@ SIGNATURES = {
     "f3r_sell_create": (C.c_int, [_vp, C.POINTER(CSR), C.c_int32, C.c_int32, C.c_int32, _pp]),
     "f3r_sell_info_get": (C.c_int, [_vp, C.POINTER(SellInfo)]),
     "f3r_sell_destroy": (None, [_vp]),
+    "f3r_sell_tune": (C.c_int, [_vp, C.c_int, C.c_int32, C.POINTER(TuneEntry), C.c_int32, C.POINTER(C.c_int32)]),
     "f3r_sell_operate": (C.c_int, [_vp, C.c_int, C.c_int, _vp, C.c_int, _vp]),
     "f3r_sell_compute_residual": (C.c_int, [_vp, C.c_int, C.c_int, _vp, C.c_int, _vp, C.c_int, _vp]),
     "f3r_dot": (C.c_int, [_vp, C.c_int, C.c_int64, _vp, _vp, C.POINTER(C.c_double)]),

@@ -11,6 +11,9 @@ namespace f3r {
 // Device-side error codes written to the context's error word.
 enum DevError : int { DEV_OK = 0, DEV_TIMEOUT_SPMV = 1, DEV_BREAKDOWN = 2 };
 
+// Threads per block of the elementwise / reduction kernels.
+constexpr int kEwThreads = 256;
+
 // Bound for every spin-wait on an mbarrier: ~2 s of %globaltimer.
 constexpr unsigned long long kWaitLimitNs = 2000000000ull;
 

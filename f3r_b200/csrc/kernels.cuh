@@ -10,7 +10,6 @@ namespace f3r {
 constexpr int kMaxCols = 128;  // FGMRES basis columns per level (m + 1 <= 128)
 constexpr int kMaxDots = 16;   // dot products fused into an inner-level SpMV
 constexpr int kMaxM4 = 16;
-constexpr int kEwThreads = 256;
 
 template <typename T> struct Cols {
   const T *p[kMaxCols];

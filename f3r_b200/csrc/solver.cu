@@ -23,6 +23,7 @@
 #include "internal.hpp"
 #include "kernels.cuh"
 #include "ilu.cuh"
+#include "objects.cuh"
 
 namespace f3r {
 
@@ -30,64 +31,6 @@ static thread_local std::string g_err;
 Status fail(Status code, const std::string &msg) {
   g_err = msg;
   return code;
-}
-
-#define CUDA_TRY(x)                                                                               \
-  do {                                                                                            \
-    cudaError_t e_ = (x);                                                                         \
-    if (e_ != cudaSuccess)                                                                        \
-      return fail(e_ == cudaErrorMemoryAllocation ? F3R_ERROR_OUT_OF_MEMORY : F3R_ERROR_CUDA,     \
-                  std::string(#x) + ": " + cudaGetErrorString(e_));                               \
-  } while (0)
-
-static inline int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
-
-// ---------------------------------------------------------------------------
-// context
-// ---------------------------------------------------------------------------
-
-struct Context {
-  int device = 0;
-  cudaStream_t own = nullptr, stream = nullptr;
-  int sm_count = 148;
-  int *err = nullptr;          // device error word (DevError)
-  void *partials = nullptr;    // grid-reduction partial sums
-  unsigned int *ticket = nullptr;
-  double *pinned = nullptr;    // host-pinned scalars for D2H reads
-  double *dscratch = nullptr;  // device scalars for f3r_dot
-  int64_t launches = 0;        // kernels issued through this context
-  std::vector<void *> allocs;
-
-  Status alloc(void **p, size_t bytes) {
-    cudaError_t e = cudaMalloc(p, bytes ? bytes : 16);
-    if (e != cudaSuccess)
-      return fail(e == cudaErrorMemoryAllocation ? F3R_ERROR_OUT_OF_MEMORY : F3R_ERROR_CUDA,
-                  std::string("cudaMalloc(") + std::to_string(bytes) + "): " + cudaGetErrorString(e));
-    return F3R_SUCCESS;
-  }
-  GridRed gred() const { return GridRed{partials, ticket}; }
-  // grid for the elementwise / reduction kernels: up to 8 blocks of 256 per SM
-  // (full thread occupancy); partial-sum buffers are sized for this bound
-  int ew_grid(int64_t n) const { return (int)std::max<int64_t>(1, std::min<int64_t>(cdiv(n, kEwThreads), (int64_t)sm_count * 8)); }
-  // checks the device error word (after a synchronisation)
-  Status check_device_error() {
-    int e = 0;
-    CUDA_TRY(cudaMemcpy(&e, err, sizeof(int), cudaMemcpyDeviceToHost));
-    if (e == DEV_OK) return F3R_SUCCESS;
-    CUDA_TRY(cudaMemset(err, 0, sizeof(int)));
-    if (e == DEV_TIMEOUT_SPMV) return fail(F3R_ERROR_TIMEOUT, "a bulk-copy wait in the SpMV kernel exceeded its bound");
-    return fail(F3R_ERROR_BREAKDOWN, "zero or non-finite norm in an Arnoldi step");
-  }
-};
-
-
-// Launches a kernel on the context's bookkeeping (every launch is counted,
-// so a solve can report how many kernels of this library it ran).
-template <typename... KP, typename... A>
-static inline void launch_k(Context &c, void (*k)(KP...), int grid, int block, size_t smem, cudaStream_t st,
-                            A &&...args) {
-  k<<<grid, block, smem, st>>>(std::forward<A>(args)...);
-  c.launches++;
 }
 
 // ---------------------------------------------------------------------------
@@ -204,25 +147,6 @@ static Status build_sell(const f3r_csr &a, int32_t sigma, bool renumber, SellHos
   return F3R_SUCCESS;
 }
 
-struct DeviceSell {
-  int32_t n = 0, ncols = 0, nslices = 0, max_width = 0, sigma = 1;
-  int64_t nnz = 0, nnz_pad = 0;
-  int32_t *col = nullptr, *sptr = nullptr, *perm = nullptr, *cbase = nullptr, *cbptr = nullptr;
-  uint16_t *dcol = nullptr;
-  double *v64 = nullptr;
-  float *v32 = nullptr;
-  __half *v16 = nullptr;
-  int dtypes = 0;
-  int index_bits() const { return dcol ? 16 : 32; }
-  DevSell view() const { return DevSell{col, dcol, cbase, cbptr, sptr, perm, n, nslices}; }
-  void release() {
-    cudaFree(col); cudaFree(sptr); cudaFree(perm); cudaFree(cbase); cudaFree(cbptr); cudaFree(dcol);
-    cbptr = nullptr;
-    cudaFree(v64); cudaFree(v32); cudaFree(v16);
-    col = sptr = perm = cbase = nullptr; dcol = nullptr; v64 = nullptr; v32 = nullptr; v16 = nullptr;
-  }
-};
-
 static Status upload_sell(Context &c, const SellHost &h, int dtype_mask, bool scatter_perm, DeviceSell &d) {
   d.n = h.n; d.ncols = h.ncols; d.nslices = h.nslices; d.max_width = h.max_width; d.sigma = h.sigma;
   d.nnz = h.nnz; d.nnz_pad = h.nnz_pad; d.dtypes = dtype_mask;
@@ -271,39 +195,6 @@ static Status upload_sell(Context &c, const SellHost &h, int dtype_mask, bool sc
 // ---------------------------------------------------------------------------
 // SpMV launcher
 // ---------------------------------------------------------------------------
-// Raises the kernel's dynamic shared memory limit once per device.  Called
-// before any graph capture for every instantiation the solver uses.
-template <typename V, typename X, typename Epi>
-static Status sell_attr(Context &c) {
-  static int attr_done[64] = {0};
-  if (!attr_done[c.device & 63]) {
-    CUDA_TRY(cudaFuncSetAttribute(
-        k_sell_cfg<V, X, Epi, SellCfg<V>::WARPS, SellCfg<V>::STAGES, SellCfg<V>::KC, int32_t>,
-        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sell_smem_bytes<V, int32_t>()));
-    CUDA_TRY(cudaFuncSetAttribute(
-        k_sell_cfg<V, X, Epi, SellCfg<V>::WARPS, SellCfg<V>::STAGES, SellCfg<V>::KC, uint16_t>,
-        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sell_smem_bytes<V, uint16_t>()));
-    attr_done[c.device & 63] = 1;
-  }
-  return F3R_SUCCESS;
-}
-
-template <typename V, typename X, typename Epi>
-static Status launch_sell(Context &c, const V *val, const DevSell &A, const X *x, const Epi &epi) {
-  if (A.nslices == 0) return F3R_SUCCESS;
-  constexpr int WARPS = SellCfg<V>::WARPS;
-  F3R_TRY((sell_attr<V, X, Epi>(c)));
-  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(cdiv(A.nslices, WARPS), c.sm_count));
-  if (A.dcol)
-    launch_k(c, k_sell_cfg<V, X, Epi, WARPS, SellCfg<V>::STAGES, SellCfg<V>::KC, uint16_t>, grid, WARPS * 32,
-             sell_smem_bytes<V, uint16_t>(), c.stream, val, A, x, epi, c.err);
-  else
-    launch_k(c, k_sell_cfg<V, X, Epi, WARPS, SellCfg<V>::STAGES, SellCfg<V>::KC, int32_t>, grid, WARPS * 32,
-             sell_smem_bytes<V, int32_t>(), c.stream, val, A, x, epi, c.err);
-  CUDA_TRY(cudaGetLastError());
-  return F3R_SUCCESS;
-}
-
 Status IluDevice::to_half(__half **d, const std::vector<double> &v) {
   double *tmp = nullptr;
   const size_t nb = std::max<size_t>(v.size(), 1);
@@ -326,13 +217,6 @@ Status IluDevice::to_half(__half **d, const std::vector<double> &v) {
 }  // namespace f3r
 
 using namespace f3r;
-
-struct f3r_context : Context {};
-
-struct f3r_sell {
-  f3r_context *ctx = nullptr;
-  DeviceSell d;
-};
 
 // ---------------------------------------------------------------------------
 // solver

@@ -1,0 +1,43 @@
+"""Launch-shape and layout sweep of the SELL SpMV (the library's autotuner).
+
+    python -m f3r_b200.tune [--nx 192] [--reps 20]
+
+Builds the nonsymmetric 27-point matrix of the benchmark (scaled), stores it
+as SELL-32 with sigma in {1, 256} and 32- or 16-bit column indices, and times
+out = A x for fp16 values (fp32 vectors), fp32 and fp64 at every launch shape
+the library carries (f3r_sell_tune).  Prints one markdown table per case.
+"""
+from __future__ import annotations
+
+import argparse
+
+import f3r_b200 as F
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--nx", type=int, default=192)
+    ap.add_argument("--reps", type=int, default=20)
+    args = ap.parse_args()
+    A = F.stencil27(args.nx, args.nx, args.nx, 2, 0.5).scale()
+    ctx = F.Context(0)
+    print(f"# SELL SpMV launch-shape sweep, {args.nx}^3 27-point (n={A.shape[0]}, nnz={A.nnz})\n")
+    for sigma in (1, 256):
+        for index16 in (False, True):
+            S = F.Sell(ctx, A, sigma=sigma, index16=index16)
+            bits = S.info().index_bits
+            for vt, name in ((F.F16, "fp16 values x fp32 vectors"), (F.F32, "fp32"), (F.F64, "fp64")):
+                rows = S.tune(vt, args.reps)
+                print(f"## sigma={sigma}, {bits}-bit indices, {name}\n")
+                print("| warps | stages | cols/copy | us | GB/s (algorithmic) | default |")
+                print("|---|---|---|---|---|---|")
+                for r in rows:
+                    print(f"| {r['warps']} | {r['stages']} | {r['kc']} | {r['us']:.1f} | {r['gbs']:.0f} | "
+                          f"{'yes' if r['default'] else ''} |")
+                print()
+            S.close()
+    ctx.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -207,6 +207,23 @@ f3r_status f3r_sell_compute_residual(f3r_sell *m, f3r_dtype val_t, f3r_dtype rhs
                                      const void *rhs, f3r_dtype in_t, const void *in,
                                      f3r_dtype res_t, void *res);
 
+/* One launch shape of the SELL SpMV and its measured time (f3r_sell_tune). */
+typedef struct f3r_tune_entry {
+  int32_t warps, stages, kc;  /* warps per CTA, bulk-copy stages per warp, columns per copy */
+  int32_t index_bits;         /* 32 or 16 (the matrix's index form) */
+  int32_t is_default;         /* 1 for the shape the library launches */
+  int32_t reserved;
+  double microseconds;        /* mean time of one product out = A x */
+  double gbs_algorithmic;     /* (nnz*(s_val+4) + 4(n+1) + n*s_x + n*s_y) / time */
+} f3r_tune_entry;
+
+/* Launch-shape autotuner: times out = A x (fp16 values with fp32 vectors,
+ * fp32, or fp64) on this matrix at every launch shape the library carries,
+ * reps launches each, and returns up to cap entries, fastest first.  No
+ * reference counterpart (the reference has one kernel shape). */
+f3r_status f3r_sell_tune(f3r_sell *m, f3r_dtype val_t, int32_t reps, f3r_tune_entry *out, int32_t cap,
+                         int32_t *count);
+
 /* *result = <x, y> over n entries (fp64 for F64, fp32 accumulation otherwise;
  * F16 inputs are widened to fp32 as the reference's wildcard(., tof32),
  * f3r-gpu.cpp:236).  Replaces kmm::dot (core/tensor.hpp:509-537, 686-688).

@@ -158,3 +158,14 @@ def test_empty_and_bad_inputs(ctx):
         F.HostMatrix.from_csr(np.array([0, 2], np.int32), np.array([1, 0], np.int32), np.ones(2))
     with pytest.raises(F.F3RError):
         F.Sell(ctx, F.stencil27(4, 4, 4), sigma=0)
+
+
+def test_tune_times_every_shape(ctx):
+    A = F.stencil27(24, 24, 24, 2, 0.5).scale()
+    S = F.Sell(ctx, A)
+    for vt in (F.F16, F.F32, F.F64):
+        rows = S.tune(vt, reps=3)
+        assert len(rows) >= 3  # shapes whose rings exceed the shared memory are skipped
+        assert sum(r["default"] for r in rows) == 1
+        assert all(r["us"] > 0 for r in rows)
+        assert rows == sorted(rows, key=lambda r: r["us"])
