@@ -35,7 +35,7 @@ class Params(C.Structure):
                 ("m4", C.c_int32), ("c", C.c_int32), ("precond", C.c_int32), ("ilu_blocks", C.c_int32),
                 ("sdainv_tol", C.c_double), ("acc", C.c_double), ("sell_c", C.c_int32), ("sell_sigma", C.c_int32),
                 ("rel_tol", C.c_double), ("half_scale_log2", C.c_int32), ("use_graphs", C.c_int32),
-                ("sell_index16", C.c_int32), ("reserved", C.c_int32 * 7)]
+                ("sell_index16", C.c_int32), ("static_weight", C.c_double), ("reserved", C.c_int32 * 8)]
 
 
 class Result(C.Structure):

@@ -210,34 +210,36 @@ __global__ void __launch_bounds__(WARPS * 32) k_cgs_update(T *__restrict__ w, Co
   grid_reduce<T, 1, WARPS>(part, 1, gr, [gg](T *tot) { givens_step<T>(gg, tot[0]); });
 }
 
-// H(j, k) = <w, V(k)> for k < nv, fp64 (outer level; nv up to m_outer).
-template <int WARPS>
-__global__ void __launch_bounds__(WARPS * 32) k_multidot_f64(const double *__restrict__ w, Cols<double> V, int nv,
-                                                             int64_t n, GridRed gr, double *hcol) {
+// H(j, k) = <w, V(k)> for k < nv (any nv up to kMaxCols): vectors taken in
+// chunks of 8 with w re-read from L1/L2 per chunk; used by the outer fp64
+// level and by inner fp32 levels with more than 8 basis vectors.
+template <typename T, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32) k_multidot_chunked(const T *__restrict__ w, Cols<T> V, int nv,
+                                                                 int64_t n, GridRed gr, T *hcol) {
   constexpr int CH = 8;
-  // partials laid out [block][nv]; chunks of CH vectors reuse w from L1
-  double *part = static_cast<double *>(gr.partials);
-  __shared__ double sred[WARPS][CH];
+  // partials laid out [block][nv]
+  T *part = static_cast<T *>(gr.partials);
+  __shared__ T sred[WARPS][CH];
   __shared__ bool last;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int k0 = 0; k0 < nv; k0 += CH) {
-    double a[CH];
+    T a[CH];
 #pragma unroll
     for (int c = 0; c < CH; c++) a[c] = 0;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-      const double wi = w[i];
+      const T wi = w[i];
 #pragma unroll
       for (int c = 0; c < CH; c++)
-        if (k0 + c < nv) a[c] = __fma_rn(wi, V.p[k0 + c][i], a[c]);
+        if (k0 + c < nv) a[c] = fmaT(wi, V.p[k0 + c][i], a[c]);
     }
 #pragma unroll
     for (int c = 0; c < CH; c++) {
-      const double s = warp_sum(a[c]);
+      const T s = warp_sum(a[c]);
       if (lane == 0) sred[warp][c] = s;
     }
     __syncthreads();
     if (threadIdx.x < CH && k0 + threadIdx.x < nv) {
-      double s = 0;
+      T s = 0;
       for (int q = 0; q < WARPS; q++) s += sred[q][threadIdx.x];
       part[(size_t)blockIdx.x * nv + k0 + threadIdx.x] = s;
     }
@@ -250,7 +252,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_multidot_f64(const double *__res
   if (!last) return;
   __threadfence();
   for (int k = warp; k < nv; k += WARPS) {
-    double s = 0;
+    T s = 0;
     for (int b = lane; b < (int)gridDim.x; b += 32) s += __ldcg(&part[(size_t)b * nv + k]);
     s = warp_sum(s);
     if (lane == 0) hcol[k] = s;

@@ -297,7 +297,7 @@ struct Solver {
     cudaStream_t st = C().stream;
     ++cnt;
     ++r_calls;
-    const bool upd = (cnt % p.c) == 0;
+    const bool upd = p.static_weight <= 0 && (cnt % p.c) == 0;  // F3R-Static never updates
     const float sc = std::ldexp(1.0f, p.half_scale_log2), isc = std::ldexp(1.0f, -p.half_scale_log2);
     const DevSell Av = A.view();
     if (precond_diag) {
@@ -378,8 +378,8 @@ struct Solver {
         launch_k(C(), k_multidot_f32<8, 8>, gv, 256, 0, C().stream, (const float *)w, Vc, nv, (int64_t)n, C().gred(),
                  hcol);
       else
-        launch_k(C(), k_multidot_f32<kMaxDots, 8>, gv, 256, 0, C().stream, (const float *)w, Vc, nv, (int64_t)n,
-                 C().gred(), hcol);
+        launch_k(C(), k_multidot_chunked<float, 8>, C().ew_grid(n), 256, 0, C().stream, (const float *)w, Vc, nv,
+                 (int64_t)n, C().gred(), hcol);
       return F3R_SUCCESS;
     }
     if (nv <= 4) return launch_sell(C(), vals, A.view(), z, EpiStoreDots<4>{w, Vc, nv, C().gred(), hcol});
@@ -429,7 +429,8 @@ struct Solver {
     for (int j = 0; j < L.m; j++) {
       float *zj = L.Z + (size_t)j * ldn;
       float *w = Vp[j + 1];
-      F3R_TRY(level3(Vp[j], zj, j == 0 ? nullptr : L.inv));
+      if (p.m3 > 0) F3R_TRY(level3(Vp[j], zj, j == 0 ? nullptr : L.inv));
+      else F3R_TRY(rich_apply(Vp[j], zj, nullptr, j == 0 ? nullptr : L.inv));  // depth 2: R directly
       F3R_TRY(spmv_dots(A.v32, zj, w, V, j + 1, L.H + (size_t)j * (L.m + 1)));
       GivensCtl<float> g{L.H, L.cs, L.sn, L.e, L.y, L.inv, nullptr, L.m + 1, j, j == L.m - 1, C().err};
       launch_k(C(), k_cgs_update<float, 8>, gv, 256, 0, C().stream, w, V, j + 1, N, C().gred(), g);
@@ -447,7 +448,7 @@ struct Solver {
     // the legacy / per-thread default streams cannot be captured
     const cudaStream_t cs = C().stream;
     if (!p.use_graphs || cs == 0 || cs == cudaStreamLegacy || cs == cudaStreamPerThread) return level2();
-    const int calls = p.m2 * p.m3;
+    const int calls = p.m2 * std::max(p.m3, 1);
     std::vector<bool> key(calls);
     for (int i = 0; i < calls; i++) key[i] = ((cnt + 1 + i) % p.c) == 0;
     auto it = graphs.find(key);
@@ -532,7 +533,8 @@ struct Solver {
       RichState h{};
       for (int k = 0; k < kMaxM4; k++) {
         h.sum[k] = 1.0f;
-        h.ome[k] = __float2half(1.0f);
+        // F3R-Static: the fixed weight in the reference's fp16 scalar (static.cpp:99-100)
+        h.ome[k] = __float2half(p.static_weight > 0 ? (float)p.static_weight : 1.0f);
         h.om[k] = 0.0f;
       }
       h.den = 1;
@@ -579,7 +581,7 @@ struct Solver {
         double *w = L.V + (size_t)(j + 1) * ldn;
         F3R_TRY(level2_call(L.V + (size_t)j * ldn, zj));
         F3R_TRY(launch_sell(C(), A.v64, A.view(), (const double *)zj, EpiStore<double>{w, nullptr}));
-        launch_k(C(), k_multidot_f64<8>, g, 256, 0, st, w, V, j + 1, N, C().gred(), L.H + (size_t)j * (L.m + 1));
+        launch_k(C(), k_multidot_chunked<double, 8>, g, 256, 0, st, w, V, j + 1, N, C().gred(), L.H + (size_t)j * (L.m + 1));
         GivensCtl<double> gc{L.H, L.cs, L.sn, L.e, L.y, L.inv, abs_e, L.m + 1, j, 0, C().err};
         launch_k(C(), k_cgs_update<double, 8>, gv, 256, 0, st, w, V, j + 1, N, C().gred(), gc);
         CUDA_TRY(cudaGetLastError());
@@ -630,10 +632,11 @@ static Status make_solver(f3r_context *ctx, const f3r_csr *a, const f3r_params *
   F3R_TRY(check_csr(a));
   if (a->nrows != a->ncols) return fail(F3R_ERROR_INVALID_VALUE, "the system matrix must be square");
   f3r_params p = *pp;
-  if (p.m_outer < 1 || p.m_outer + 1 > kMaxCols || p.m2 < 1 || p.m2 + 1 > kMaxDots || p.m3 < 1 ||
-      p.m3 + 1 > kMaxDots || p.m4 < 1 || p.m4 > kMaxM4 || p.c < 1 || p.max_restarts < 1)
+  if (p.m_outer < 1 || p.m_outer + 1 > kMaxCols || p.m2 < 1 || p.m2 + 1 > kMaxCols || p.m3 < 0 ||
+      p.m3 + 1 > kMaxCols || p.m4 < 1 || p.m4 > kMaxM4 || p.c < 1 || p.max_restarts < 1 || p.static_weight < 0)
     return fail(F3R_ERROR_INVALID_VALUE,
-                "need 1 <= m_outer <= 127, 1 <= m2, m3 <= 15, 1 <= m4 <= 16, c >= 1, max_restarts >= 1");
+                "need 1 <= m_outer, m2 <= 127, 0 <= m3 <= 127, 1 <= m4 <= 16, c >= 1, max_restarts >= 1, "
+                "static_weight >= 0");
   if (p.sell_c != 32) return fail(F3R_ERROR_UNSUPPORTED, "only SELL slice height 32 is implemented");
   if (p.precond != F3R_PRECOND_SDAINV && p.precond != F3R_PRECOND_ILU0_BJ)
     return fail(F3R_ERROR_INVALID_VALUE, "unknown preconditioner");
@@ -712,7 +715,7 @@ static Status make_solver(f3r_context *ctx, const f3r_csr *a, const f3r_params *
   // level storage
   F3R_TRY(s->make_level(s->L1, p.m_outer, true));
   F3R_TRY(s->make_level(s->L2, p.m2, true));
-  F3R_TRY(s->make_level(s->L3, p.m3, false));
+  if (p.m3 > 0) F3R_TRY(s->make_level(s->L3, p.m3, false));
   const size_t nn = (size_t)std::max(n, 1);
   F3R_TRY(s->alloc(&s->abs_e, 1));
   F3R_TRY(s->alloc(&s->hin, nn));

@@ -65,7 +65,10 @@ typedef struct f3r_csr {
 typedef struct f3r_params {
   int32_t m_outer;         /* outer fp64 FGMRES restart length: 100 (f3r-gpu.cpp:264) */
   int32_t max_restarts;    /* Restarted cap: 20 (f3r-gpu.cpp:265) */
-  int32_t m2, m3, m4;      /* fp32 level, fp16-matrix level, Richardson steps: 8, 4, 2 */
+  int32_t m2, m3, m4;      /* fp32 level, fp16-matrix level, Richardson steps: 8, 4, 2.
+                              m3 = 0 drops the fp16-matrix level: the fp32 level then applies
+                              R directly (the depth-2 "F2" ablation, work/src/depth.cpp:157-162,
+                              with m4 = 1 and static_weight = 1) */
   int32_t c;               /* adaptive-weight period: 64 (suite-gpu.py:49) */
   int32_t precond;         /* f3r_precond */
   int32_t ilu_blocks;      /* block-Jacobi blocks: 112 (f3r.cpp:57) */
@@ -84,7 +87,10 @@ typedef struct f3r_params {
                               base when every slice column fits a 65536 window (32-bit otherwise).
                               Fewer bytes, but on B200 the 32-bit form streams faster (the SpMV
                               is bound by copies in flight, not by bytes) */
-  int32_t reserved[7];
+  double static_weight;    /* 0: adaptive weights (F3R).  w > 0: fixed weight w for every
+                              Richardson step, never updated ("F3R-Static",
+                              work/src/static.cpp:99-114) */
+  int32_t reserved[8];
 } f3r_params;
 
 /* Solve outcome.  The first three fields are solve_res_t

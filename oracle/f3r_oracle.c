@@ -593,6 +593,7 @@ typedef struct {
   int32_t arith;       /* ARITH_PRODUCT or ARITH_REF */
   int32_t half_scale_log2; /* 0: plain fp32->fp16 cast (reference); k: scale by 2^k */
   double tol;          /* stop when implicit residual / ||b|| < tol */
+  double static_weight; /* > 0: F3R-Static, fixed weight (work/src/static.cpp:99-114) */
 } or_f3r_params;
 
 #define MAXM4 16
@@ -678,7 +679,7 @@ static void level4(f3r_ctx *c, const float *in, float *out) {
   float sc = ldexpf(1.0f, c->p.half_scale_log2), isc = ldexpf(1.0f, -c->p.half_scale_log2);
   c->r_calls++;
   ++c->cnt;
-  int upd = (c->cnt % c->p.c == 0);
+  int upd = (c->p.static_weight <= 0) && (c->cnt % c->p.c == 0);
   for (int32_t i = 0; i < n; i++) c->hin[i] = (f16)(in[i] * sc);
   prec_apply(c, c->hin, c->hout, c->tmp);
   if (upd) {
@@ -759,15 +760,15 @@ static void level_inner(f3r_ctx *c, int level, const float *in, float *out) {
   float *V = (float *)malloc(sizeof(float) * (size_t)n * (m + 1));
   float *Z = (float *)malloc(sizeof(float) * (size_t)n * m);
   float *H = (float *)calloc((size_t)(m + 1) * m, sizeof(float));
-  float cs[64], sn[64], e[65], y[64];
+  float cs[128], sn[128], e[129], y[128];
   memset(e, 0, sizeof(e));
   e[0] = 1.0f;
   memcpy(V, in, sizeof(float) * (size_t)n);
   const or_mat *A = c->A;
   for (int j = 0; j < m; j++) {
     float *vj = V + (size_t)n * j, *zj = Z + (size_t)n * j, *w = V + (size_t)n * (j + 1);
-    if (level == 2) level_inner(c, 3, vj, zj);
-    else level4(c, vj, zj);
+    if (level == 2 && c->p.m3 > 0) level_inner(c, 3, vj, zj);
+    else level4(c, vj, zj);  /* level 3, or level 2 of the depth-2 form (work/src/depth.cpp:157-162) */
     for (int32_t i = 0; i < n; i++) {
       float t = 0.0f;
       if (level == 2)
@@ -808,7 +809,7 @@ int or_f3r_solve(const or_mat *A, const or_mat *P1, const or_mat *P2, const doub
   memset(&c, 0, sizeof(c));
   int32_t n = A->n;
   c.n = n; c.A = A; c.P1 = P1; c.P2 = P2; c.p = *p;
-  if (p->m2 > 63 || p->m3 > 63 || p->m4 > MAXM4 || p->m1 > 4096) return -1;
+  if (p->m2 > 127 || p->m3 > 127 || p->m3 < 0 || p->m4 > MAXM4 || p->m1 > 4096) return -1;
   c.v32 = (float *)malloc(sizeof(float) * (size_t)A->nnz);
   c.v16 = (f16 *)malloc(sizeof(f16) * (size_t)A->nnz);
   for (int32_t q = 0; q < A->nnz; q++) { c.v32[q] = (float)A->val[q]; c.v16[q] = (f16)A->val[q]; }
@@ -816,7 +817,10 @@ int or_f3r_solve(const or_mat *A, const or_mat *P1, const or_mat *P2, const doub
   c.tmp2 = malloc(sizeof(f16) * n); c.hr = malloc(sizeof(f16) * n);
   /* per-solve reset (f3r-gpu.cpp:277-281) */
   c.cnt = p->c;
-  for (int k = 0; k < MAXM4; k++) { c.sum[k] = 1.0f; c.ome[k] = (f16)1.0f; }
+  for (int k = 0; k < MAXM4; k++) {
+    c.sum[k] = 1.0f;
+    c.ome[k] = (f16)(p->static_weight > 0 ? (float)p->static_weight : 1.0f);
+  }
 
   int m = p->m1;
   double *V = (double *)malloc(sizeof(double) * (size_t)n * (m + 1));

@@ -91,12 +91,12 @@ def lib() -> C.CDLL:
 class F3RParams(C.Structure):
     _fields_ = [("m1", C.c_int32), ("restarts", C.c_int32), ("m2", C.c_int32), ("m3", C.c_int32),
                 ("m4", C.c_int32), ("c", C.c_int32), ("precond", C.c_int32), ("arith", C.c_int32),
-                ("half_scale_log2", C.c_int32), ("tol", C.c_double)]
+                ("half_scale_log2", C.c_int32), ("tol", C.c_double), ("static_weight", C.c_double)]
 
 
 def params(m1=100, restarts=20, m2=8, m3=4, m4=2, c=64, precond=PRECOND_SDAINV, arith=ARITH_PRODUCT,
-           half_scale_log2=0, tol=1e-10) -> F3RParams:
-    return F3RParams(m1, restarts, m2, m3, m4, c, precond, arith, half_scale_log2, tol)
+           half_scale_log2=0, tol=1e-10, static_weight=0.0) -> F3RParams:
+    return F3RParams(m1, restarts, m2, m3, m4, c, precond, arith, half_scale_log2, tol, static_weight)
 
 
 class Mat:
@@ -291,7 +291,7 @@ class Ref:
         L.ref_f3r_solve.restype = C.c_int
         L.ref_f3r_solve.argtypes = [C.c_int, C.c_int32, C.c_int32, _i32p, _i32p, _f64p, _f64p, _f64p,
                                     C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
-                                    C.c_double, C.c_int, _f64p, _f64p, C.c_int, C.c_int]
+                                    C.c_double, C.c_int, _f64p, _f64p, C.c_int, C.c_int, C.c_double]
 
     def gen27(self, nx, ny, nz, variant=0, beta=0.5):
         n = nx * ny * nz
@@ -392,13 +392,13 @@ class Ref:
             self.L.ref_pair_free(h)
 
     def f3r_solve(self, config, rptr, idx, val, b, m2=8, m3=4, m4=2, c=64, restarts=20, tol=1e-10,
-                  acc=1.0, sdainv_tol=0.1, blocks=112, hist_cap=4096, stop_after=0):
+                  acc=1.0, sdainv_tol=0.1, blocks=112, hist_cap=4096, stop_after=0, weight=1.0):
         n = len(rptr) - 1
         x = np.zeros(n)
         out = np.zeros(5)
         hist = np.zeros(hist_cap)
         nh = self.L.ref_f3r_solve(config, n, len(idx), rptr, idx, np.ascontiguousarray(val, np.float64),
                                   np.ascontiguousarray(b, np.float64), x, m2, m3, m4, c, restarts, tol, acc,
-                                  sdainv_tol, blocks, out, hist, hist_cap, stop_after)
+                                  sdainv_tol, blocks, out, hist, hist_cap, stop_after, weight)
         return dict(x=x, time_s=out[0], iters=int(out[1]), impl_res=out[2], expl_res=out[3],
                     solved=bool(out[4]), hist=hist[:min(nh, hist_cap)].copy())

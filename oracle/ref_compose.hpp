@@ -237,4 +237,84 @@ inline solve_out f3r_bjilu_csr(const CSR<double, host> &data, const double *b, d
   return run_solve(solver, A, b, x, n, tol, hist, hist_cap);
 }
 
+// F3R-Static (work/src/static.cpp:99-119): the fixed-weight Richardson over
+// BJ-ILU(0) in fp16, CSR matrices.
+inline solve_out f3r_static_bjilu_csr(const CSR<double, host> &data, const double *b, double *x, int m2, int m3,
+                                      int m4, double weight, int restarts, double tol, double acc, int blocks,
+                                      double *hist, int hist_cap) {
+  using tag = host;
+  const int32_t n = data.nrows();
+  auto A = CSR<double, tag>(data);
+  impl::pool<double, tag>::init(n);
+  impl::pool<float, tag>::init(n);
+  impl::pool<h16, tag>::init(n);
+  auto bd = data.duplicate_block_diagonal(blocks, 1);
+  auto [l, u] = algorithm::split(algorithm::ilup(bd, 0, acc, blocks, 1));
+  auto A16 = CSR<h16, tag>(A);
+  auto L = trsv::l::BJ<CSR<h16, host>>(l, {blocks});
+  auto U = trsv::du::BJ<CSR<h16, host>>(u, {blocks});
+  auto tmp = vector<h16, tag>(n);
+  auto tmp2 = vector<h16, tag>(n);
+  auto hin = vector<h16, tag>(n);
+  auto hout = vector<h16, tag>(n);
+  auto hr = vector<h16, tag>(n);
+  scalar<h16, tag> ome;
+  ome.fill(h16(weight));
+  auto R = Operator<tag>(data.get_shape(), [&](auto in, auto out) {
+    hin.copy(in);
+    L.solve(hin, tmp);
+    U.solve(tmp, hout);
+    hout *= ome;
+    for (int k = 1; k < m4; k++) {
+      A16.compute_residual(hin, hout, hr);
+      L.solve(hr, tmp);
+      U.solve(tmp, tmp2);
+      hout += ome * tmp2;
+    }
+    out.copy(hout);
+  });
+  auto A32 = CSR<float, tag>(A);
+  auto MM = FGMRES<float, tag>(A16, R, {m3, false});
+  auto MMM = FGMRES<float, tag>(A32, MM, {m2, false});
+  auto inner = Solver<tag>(FGMRES<double, tag>(A, MMM, {100, true}));
+  auto solver = Restarted<double, tag>(A, inner, {restarts});
+  return run_solve(solver, A, b, x, n, tol, hist, hist_cap);
+}
+
+// Depth ablations with fp32 levels (work/src/depth.cpp:122-162): M is the
+// fp16 BJ-ILU(0) sweep pair; depth 3 = FGMRES<float>(A32, FGMRES<float>(A16,
+// M, m3), m2), depth 2 = FGMRES<float>(A32, M, m2).
+inline solve_out depth_bjilu_csr(const CSR<double, host> &data, const double *b, double *x, int depth, int m2,
+                                 int m3, int restarts, double tol, double acc, int blocks, double *hist,
+                                 int hist_cap) {
+  using tag = host;
+  const int32_t n = data.nrows();
+  auto A = CSR<double, tag>(data);
+  impl::pool<double, tag>::init(n);
+  impl::pool<float, tag>::init(n);
+  impl::pool<h16, tag>::init(n);
+  auto bd = data.duplicate_block_diagonal(blocks, 1);
+  auto [l, u] = algorithm::split(algorithm::ilup(bd, 0, acc, blocks, 1));
+  auto L = trsv::l::BJ<CSR<h16, host>>(l, {blocks});
+  auto U = trsv::du::BJ<CSR<h16, host>>(u, {blocks});
+  auto tmp = vector<h16, tag>(n);
+  auto M = Operator<tag>(data.get_shape(), [&](auto in, auto out) {
+    L.solve(in, tmp);
+    U.solve(tmp, out);
+  });
+  auto A16 = CSR<h16, tag>(A);
+  auto A32 = CSR<float, tag>(A);
+  if (depth == 3) {
+    auto F = FGMRES<float, tag>(A16, M, {m3, false});
+    auto inner = FGMRES<float, tag>(A32, F, {m2, false});
+    auto solver_ = Solver<tag>(FGMRES<double, tag>(A, inner, {100, true}));
+    auto solver = Restarted<double, tag>(A, solver_, {restarts});
+    return run_solve(solver, A, b, x, n, tol, hist, hist_cap);
+  }
+  auto inner = FGMRES<float, tag>(A32, M, {m2, false});
+  auto solver_ = Solver<tag>(FGMRES<double, tag>(A, inner, {100, true}));
+  auto solver = Restarted<double, tag>(A, solver_, {restarts});
+  return run_solve(solver, A, b, x, n, tol, hist, hist_cap);
+}
+
 }  // namespace refc

@@ -138,19 +138,26 @@ void ref_bj_solve_f16(void *h, int blocks, int upper, const uint16_t *in, uint16
 void ref_pair_free(void *h) { delete (pair_t *)h; }
 
 // Full F3R solves (stop_after > 0: only that many outer steps).  config 0: SDAINV + SELL-32 (f3r-gpu.cpp:210-265);
-// config 1: BJ-ILU(0) + CSR (f3r.cpp:195-248).  A must already be scaled.
+// config 1: BJ-ILU(0) + CSR (f3r.cpp:195-248); config 2: F3R-Static with
+// weight `weight` over BJ-ILU(0) (static.cpp:99-119); configs 3 / 4: the
+// depth-3 / depth-2 fp32 ablations over BJ-ILU(0) (depth.cpp:140-162).  A
+// must already be scaled.
 // out[0..4] = time_s, iters, impl_res, expl_res, solved; returns n_hist.
 int ref_f3r_solve(int config, int32_t n, int32_t nnz, const int32_t *rptr, const int32_t *idx,
                   const double *val, const double *b, double *x, int m2, int m3, int m4, int c,
                   int restarts, double tol, double acc, double sdainv_tol, int blocks,
-                  double *out, double *hist, int hist_cap, int stop_after) {
+                  double *out, double *hist, int hist_cap, int stop_after, double weight) {
   refc::g_stop_after = stop_after;
   auto a = refc::make_csr(n, nnz, rptr, idx, val);
-  refc::solve_out o =
-      config == 0 ? refc::f3r_sdainv_sell(a, b, x, m2, m3, m4, c, restarts, tol, acc, sdainv_tol,
-                                          hist, hist_cap)
-                  : refc::f3r_bjilu_csr(a, b, x, m2, m3, m4, c, restarts, tol, acc, blocks, hist,
-                                        hist_cap);
+  refc::solve_out o;
+  if (config == 0)
+    o = refc::f3r_sdainv_sell(a, b, x, m2, m3, m4, c, restarts, tol, acc, sdainv_tol, hist, hist_cap);
+  else if (config == 1)
+    o = refc::f3r_bjilu_csr(a, b, x, m2, m3, m4, c, restarts, tol, acc, blocks, hist, hist_cap);
+  else if (config == 2)
+    o = refc::f3r_static_bjilu_csr(a, b, x, m2, m3, m4, weight, restarts, tol, acc, blocks, hist, hist_cap);
+  else
+    o = refc::depth_bjilu_csr(a, b, x, config == 3 ? 3 : 2, m2, m3, restarts, tol, acc, blocks, hist, hist_cap);
   out[0] = o.time_s;
   out[1] = o.iters;
   out[2] = o.impl_res;

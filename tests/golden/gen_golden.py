@@ -112,6 +112,11 @@ def main(big: bool):
              ("sdainv_diff12", 0, None, 2), ("bjilu_hpcg16", 1, (16, 16, 16, 0), 3)]
     if big:
         cases += [("bjilu_hpcg64", 1, (64, 64, 64, 0), 4), ("sdainv_half192", 0, (192, 192, 192, 2), 5)]
+    # F3R-Static (static.cpp) and the fp32 depth ablations (depth.cpp), BJ-ILU(0)
+    variants = {"static_hpgmp16": dict(config=2, m2=8, m3=4, m4=2, weight=1.2),
+                "depth3_hpgmp16": dict(config=3, m2=8, m3=8, m4=1, weight=1.0),
+                "depth2_hpgmp16": dict(config=4, m2=64, m3=0, m4=1, weight=1.0)}
+    cases += [(k, v["config"], (16, 16, 16, 1), 6 + j) for j, (k, v) in enumerate(variants.items())]
     for name, config, spec, seed in cases:
         if spec is None:
             D = F.diffusion7(12, 12, 12, 1.5, 3.0, 9)
@@ -121,8 +126,9 @@ def main(big: bool):
         vv = ref.scaling(rr, ii, vv)
         xs, b = rhs_for(ref, rr, ii, vv, seed)
         blocks = 16 if spec is not None and spec[0] == 16 else 112
+        extra = {k: v for k, v in variants.get(name, {}).items() if k != "config"}
         res = ref.f3r_solve(config, rr, ii, vv, b, tol=1e-10, c=64 if spec and spec[0] >= 64 else 8,
-                            blocks=blocks)
+                            blocks=blocks, **extra)
         print(name, res["iters"], res["impl_res"], res["expl_res"], res["time_s"])
         sol[name + "_iters"] = np.array(res["iters"])
         sol[name + "_hist"] = res["hist"]

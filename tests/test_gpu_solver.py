@@ -136,7 +136,8 @@ def test_ilu_bj(ctx):
 
 def test_invalid_params(ctx):
     A = F.stencil27(8, 8, 8).scale()
-    with pytest.raises(F.F3RError):
-        F.Solver(ctx, A, m2=40)
+    for bad in (dict(m2=200), dict(m3=-1), dict(m3=128), dict(static_weight=-1.0), dict(m4=17)):
+        with pytest.raises(F.F3RError):
+            F.Solver(ctx, A, **bad)
     with pytest.raises(F.F3RError):
         F.Solver(ctx, A, precond=F.PRECOND_ILU0_BJ, ilu_blocks=112)

@@ -121,6 +121,7 @@ def _problem(name):
         D = F.diffusion7(12, 12, 12, 1.5, 3.0, 9)
         return D.arrays()
     spec = {"sdainv_hpgmp16": (16, 16, 16, 1), "sdainv_half16": (16, 16, 16, 2), "bjilu_hpcg16": (16, 16, 16, 0),
+            "static_hpgmp16": (16, 16, 16, 1), "depth3_hpgmp16": (16, 16, 16, 1), "depth2_hpgmp16": (16, 16, 16, 1),
             "bjilu_hpcg64": (64, 64, 64, 0), "sdainv_half192": (192, 192, 192, 2)}[name]
     return O.stencil27(*spec[:3], variant=spec[3], beta=0.5)
 
@@ -158,3 +159,21 @@ def test_oracle_solve_matches_reference(name):
         assert abs(np.log10(o["hist"][0]) - np.log10(h[0])) < 1.0, (o["hist"][0], h[0])
         if name + "_x" in sol:
             assert np.linalg.norm(o["x"] - sol[name + "_x"]) / np.linalg.norm(sol[name + "_x"]) < 1e-8
+
+
+# F3R-Static (static.cpp:99-119) and the fp32 depth ablations (depth.cpp:140-162)
+# as parameter sets of the same nested solver
+VARIANTS = {"static_hpgmp16": dict(m2=8, m3=4, m4=2, static_weight=1.2),
+            "depth3_hpgmp16": dict(m2=8, m3=8, m4=1, static_weight=1.0),
+            "depth2_hpgmp16": dict(m2=64, m3=0, m4=1, static_weight=1.0)}
+
+
+@pytest.mark.parametrize("name", sorted(VARIANTS))
+def test_oracle_variants_match_reference(name):
+    r, i, v, b, xs, sol = golden_system(name)
+    A = O.Mat.from_csr(r, i, v)
+    L, U = O.ilu0_bj(A, int(sol[name + "_blocks"]))
+    o = O.f3r_solve(A, L, U, b, O.params(precond=O.PRECOND_ILU0_BJ, c=8, tol=1e-10, **VARIANTS[name]))
+    ref_iters = int(sol[name + "_iters"])
+    assert o["solved"]
+    assert abs(o["iters"] - ref_iters) <= max(1, round(0.1 * ref_iters)), (o["iters"], ref_iters)
