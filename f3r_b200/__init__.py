@@ -21,7 +21,8 @@ from . import _capi
 from ._capi import F16, F32, F64, PRECOND_ILU0_BJ, PRECOND_SDAINV, F3RError, check, lib
 
 __all__ = ["HostMatrix", "Context", "Sell", "Solver", "Params", "solve_res_t", "F3RError", "F64", "F32", "F16",
-           "PRECOND_SDAINV", "PRECOND_ILU0_BJ", "stencil27", "diffusion7", "random_uniform", "host_spmv"]
+           "PRECOND_SDAINV", "PRECOND_ILU0_BJ", "stencil27", "diffusion7", "random_uniform", "host_spmv",
+           "read_matrix", "read_system", "read_vector", "write_vector", "CSV_HEADER", "csv_row"]
 
 _NP2DT = {np.dtype(np.float64): F64, np.dtype(np.float32): F32, np.dtype(np.float16): F16}
 
@@ -94,6 +95,11 @@ class HostMatrix:
         check(lib().f3r_host_ilu0_bj(C.byref(v), blocks, acc, C.byref(l), C.byref(u)))
         return HostMatrix(l), HostMatrix(u)
 
+    def write_mm(self, path) -> None:
+        """Matrix Market "coordinate real general" file, %.17g values."""
+        v = self.view()
+        check(lib().f3r_mm_write(_path(path), C.byref(v)))
+
     def __del__(self):
         if getattr(self, "_h", None) is not None and _capi is not None and _capi._lib is not None:
             _capi._lib.f3r_host_matrix_destroy(self._h)
@@ -120,6 +126,53 @@ def random_uniform(seed: int, lo: float, hi: float, n: int) -> np.ndarray:
 
 def host_spmv(A: HostMatrix, x) -> np.ndarray:
     return A.spmv(x)
+
+
+# ---- Matrix Market files and the drivers' CSV line (matrix/io.hpp, f3r-gpu.cpp)
+
+def _path(p) -> bytes:
+    import os
+    return os.fsencode(p)
+
+
+def read_matrix(path) -> HostMatrix:
+    """A "matrix coordinate" file as CSR (io::mm::read_matrix + io::CSR)."""
+    h = C.c_void_p()
+    check(lib().f3r_mm_read(_path(path), C.byref(h)))
+    return HostMatrix(h)
+
+
+def read_vector(path, n: int) -> np.ndarray:
+    """An n x 1 "matrix array real general" file."""
+    out = np.zeros(n)
+    check(lib().f3r_mm_read_vector(_path(path), n, out.ctypes.data))
+    return out
+
+
+def read_system(path):
+    """(A, b, b_from_file) as io::mm::read_system with the drivers' init:
+    b from "<stem>_b.mtx" if it exists, else U(0, 1) from mt19937_64(0)."""
+    A = read_matrix(path)
+    b = np.zeros(A.shape[0])
+    ff = C.c_int32(0)
+    check(lib().f3r_mm_read_rhs(_path(path), len(b), b.ctypes.data, C.byref(ff)))
+    return A, b, bool(ff.value)
+
+
+def write_vector(path, x) -> None:
+    x = np.ascontiguousarray(x, np.float64)
+    check(lib().f3r_mm_write_vector(_path(path), len(x), x.ctypes.data))
+
+
+CSV_HEADER = "Problem,Method,Prec,M2,M3,M4,W,Precond,ACC,Time,Iter,ImplRes,ExplRes"
+
+
+def csv_row(problem, method, prec, m2, m3, m4, w, precond, acc, time_s, iters, impl_res, expl_res) -> str:
+    """One result line in the drivers' format (f3r-gpu.cpp:94-103, 267-272):
+    Time, ImplRes and ExplRes as C's %e, Iter as an integer, the other
+    fields as given (ACC as typed on the command line)."""
+    return "%s,%s,%s,%d,%d,%d,%s,%s,%s,%e,%d,%e,%e" % (problem, method, prec, m2, m3, m4, w, precond, acc, time_s,
+                                                        iters, impl_res, expl_res)
 
 
 class Context:

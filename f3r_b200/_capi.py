@@ -74,6 +74,11 @@ SIGNATURES = {
     "f3r_host_scaling": (C.c_int, [_vp]),
     "f3r_host_spmv": (C.c_int, [C.POINTER(CSR), _vp, _vp]),
     "f3r_random_uniform": (C.c_int, [C.c_uint64, C.c_double, C.c_double, C.c_int64, _vp]),
+    "f3r_mm_read": (C.c_int, [C.c_char_p, C.POINTER(_vp)]),
+    "f3r_mm_read_vector": (C.c_int, [C.c_char_p, C.c_int64, _vp]),
+    "f3r_mm_read_rhs": (C.c_int, [C.c_char_p, C.c_int64, _vp, C.POINTER(C.c_int32)]),
+    "f3r_mm_write": (C.c_int, [C.c_char_p, C.POINTER(CSR)]),
+    "f3r_mm_write_vector": (C.c_int, [C.c_char_p, C.c_int64, _vp]),
     "f3r_host_sdainv": (C.c_int, [C.POINTER(CSR), C.c_double, C.c_double, _pp, _pp]),
     "f3r_host_ilu0_bj": (C.c_int, [C.POINTER(CSR), C.c_int32, C.c_double, _pp, _pp]),
     "f3r_context_create": (C.c_int, [C.c_int32, _pp]),

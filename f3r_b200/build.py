@@ -14,6 +14,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libf3r_b200.so")
+DRIVER_SRC = os.path.join(HERE, "driver", "f3r_run.cpp")
+DRIVER = os.path.join(HERE, "bin", "f3r-run")
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -43,10 +45,23 @@ def headers():
 
 
 def up_to_date() -> bool:
-    if not os.path.exists(LIB):
+    if not os.path.exists(LIB) or not os.path.exists(DRIVER):
         return False
-    t = os.path.getmtime(LIB)
-    return all(os.path.getmtime(f) <= t for f in sources() + headers())
+    t = min(os.path.getmtime(LIB), os.path.getmtime(DRIVER))
+    return all(os.path.getmtime(f) <= t for f in sources() + headers() + [DRIVER_SRC])
+
+
+def build_driver(verbose: bool = False) -> str:
+    """The command-line driver (bin/f3r-run), linked against the library with
+    an rpath to it, so it runs from the source tree."""
+    os.makedirs(os.path.dirname(DRIVER), exist_ok=True)
+    cmd = [nvcc(), DRIVER_SRC, "-o", DRIVER, "-std=c++17", "-O2", "-ccbin", "/usr/bin/g++",
+           "-I", os.path.join(os.path.dirname(HERE), "include"), "-L", HERE, "-lf3r_b200",
+           "-Xlinker", "-rpath,$ORIGIN/.."]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True)
+    return DRIVER
 
 
 def build(force: bool = False, verbose: bool = False, extra=()) -> str:
@@ -80,6 +95,7 @@ def build(force: bool = False, verbose: bool = False, extra=()) -> str:
     if verbose:
         print(" ".join(link))
     subprocess.run(link, check=True)
+    build_driver(verbose)
     return LIB
 
 

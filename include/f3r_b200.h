@@ -103,7 +103,8 @@ typedef struct f3r_result {
   double expl_rel_res;       /* ||b - A x|| / ||b|| recomputed in fp64 */
   int32_t restarts;          /* outer FGMRES calls */
   int32_t reserved0;
-  int64_t inner_applications;/* Richardson applications (the reference's Iter) */
+  int64_t inner_applications;/* Richardson applications; the drivers' CSV Iter is this times m4
+                                (res_iter * m2 * m3 * m4, f3r-gpu.cpp:94-98,280-282) */
   double solve_seconds;      /* device time of the solve (CUDA events) */
   int64_t kernel_launches;   /* kernels of this library the solve ran (graph nodes included) */
 } f3r_result;
@@ -180,11 +181,36 @@ f3r_status f3r_host_sdainv(const f3r_csr *a, double tol, double acc, f3r_host_ma
 f3r_status f3r_host_ilu0_bj(const f3r_csr *a, int32_t blocks, double acc, f3r_host_matrix **l,
                             f3r_host_matrix **u);
 
+/* ---------------------------------------------------------- Matrix Market
+ * The on-disk formats either side of the solve (umineko-sparse/matrix/io.hpp).
+ *
+ * f3r_mm_read: a "matrix coordinate" file (real or integer; general or
+ * symmetric) as host CSR.  Replaces io::mm::read_matrix + io::CSR(COO)
+ * (io.hpp:91-96, 44-60, 129-192): explicit off-diagonal zeros are dropped,
+ * symmetric files expanded, rows sorted by column, duplicates kept.
+ * Pattern, complex, skew-symmetric and hermitian files are refused
+ * (F3R_ERROR_UNSUPPORTED) where the reference would misread them. */
+f3r_status f3r_mm_read(const char *path, f3r_host_matrix **out);
+/* An n x 1 "matrix array real general" file into x[0..n) (io.hpp:196-216). */
+f3r_status f3r_mm_read_vector(const char *path, int64_t n, double *x);
+/* The right-hand side io::mm::read_system pairs with a matrix file
+ * (io.hpp:104-126): "<stem>_b.mtx" ("_b" inserted before the last four
+ * characters of matrix_path) when it exists, else n values U(0, 1) from
+ * std::mt19937_64(0), the drivers' init (f3r-gpu.cpp:60).  *from_file (may be
+ * NULL) is 1 when the file was read. */
+f3r_status f3r_mm_read_rhs(const char *matrix_path, int64_t n, double *b, int32_t *from_file);
+/* Writes a general coordinate file (1-based, %.17g values: exact round trip). */
+f3r_status f3r_mm_write(const char *path, const f3r_csr *a);
+/* Writes an n x 1 array file (%.17g). */
+f3r_status f3r_mm_write_vector(const char *path, int64_t n, const double *x);
+
 /* ---------------------------------------------------------------- context */
 f3r_status f3r_context_create(int32_t device, f3r_context **out);
 void f3r_context_destroy(f3r_context *ctx);
 /* Use an external CUDA stream (cudaStream_t) instead of the context's own;
- * NULL restores the context's stream. */
+ * NULL restores the context's stream.  The context's own stream is a
+ * blocking stream: it orders with work on the legacy default stream, so a
+ * caller that fills inputs on the default stream needs no extra sync. */
 f3r_status f3r_context_set_stream(f3r_context *ctx, void *stream);
 f3r_status f3r_context_synchronize(f3r_context *ctx);
 

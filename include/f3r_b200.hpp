@@ -18,6 +18,7 @@
 #include <memory>
 #include <stdexcept>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "f3r_b200.h"
@@ -71,6 +72,8 @@ class CSR {
   int32_t ncols() const { return view().ncols; }
   int32_t nnz() const { return view().nnz; }
   f3r_host_matrix *handle() const { return h_.get(); }
+  // takes ownership of a matrix returned by the C ABI
+  static CSR adopt(f3r_host_matrix *h) { return CSR(h); }
   // y = A x on the host in fp64
   void operate(const double *x, double *y) const {
     f3r_csr v = view();
@@ -81,6 +84,35 @@ class CSR {
   explicit CSR(f3r_host_matrix *h) : h_(h, f3r_host_matrix_destroy) {}
   std::shared_ptr<f3r_host_matrix> h_;
 };
+
+// kmm::io::mm (matrix/io.hpp:89-217): Matrix Market files either side of the solve.
+namespace io {
+namespace mm {
+// io::mm::read_matrix + io::CSR(COO) (io.hpp:91-96, 44-60)
+inline CSR read_matrix(const std::string &path) {
+  f3r_host_matrix *h = nullptr;
+  check(f3r_mm_read(path.c_str(), &h));
+  return CSR::adopt(h);
+}
+// io::mm::read_system (io.hpp:104-126) with the drivers' init: b from
+// "<stem>_b.mtx" when present, else U(0, 1) from std::mt19937_64(0)
+inline std::pair<CSR, std::vector<double>> read_system(const std::string &path, bool *b_from_file = nullptr) {
+  CSR a = read_matrix(path);
+  std::vector<double> b(a.nrows());
+  int32_t ff = 0;
+  check(f3r_mm_read_rhs(path.c_str(), (int64_t)b.size(), b.data(), &ff));
+  if (b_from_file) *b_from_file = ff != 0;
+  return {std::move(a), std::move(b)};
+}
+inline void write(const std::string &path, const CSR &a) {
+  f3r_csr v = a.view();
+  check(f3r_mm_write(path.c_str(), &v));
+}
+inline void write_vector(const std::string &path, const std::vector<double> &x) {
+  check(f3r_mm_write_vector(path.c_str(), (int64_t)x.size(), x.data()));
+}
+}  // namespace mm
+}  // namespace io
 
 namespace algorithm {
 // kmm::algorithm::scaling (algorithm.hpp:45-59)

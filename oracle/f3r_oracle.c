@@ -7,8 +7,9 @@
  * cpu_baseline leg may load it; the product library (f3r_b200/) never does.
  *
  * Every function names the reference file:line it restates.  The oracle is
- * pinned against the reference itself: oracle/ref_driver.cpp compiles the
- * reference headers into oracle/_ref/, tests/golden/gen_golden.py runs it and
+ * pinned against the reference itself: oracle/ref_lib.cpp and ref_gen.cpp
+ * compile the reference headers into oracle/_ref/ (oracle/Makefile),
+ * tests/golden/gen_golden.py runs them and
  * commits golden vectors, and tests/test_oracle_pins.py checks this file
  * against them.
  *

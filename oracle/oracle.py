@@ -288,6 +288,12 @@ class Ref:
         L.ref_pair_copy.argtypes = [C.c_void_p, C.c_int, _i32p, _i32p, _f64p]
         L.ref_bj_solve_f16.argtypes = [C.c_void_p, C.c_int, C.c_int, _u16p, _u16p]
         L.ref_pair_free.argtypes = [C.c_void_p]
+        L.ref_gen27_save.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_char_p]
+        L.ref_mm_read_system.restype = C.c_void_p
+        L.ref_mm_read_system.argtypes = [C.c_char_p]
+        L.ref_mm_dims.argtypes = [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
+        L.ref_mm_copy.argtypes = [C.c_void_p, _i32p, _i32p, _f64p, _f64p]
+        L.ref_mm_free.argtypes = [C.c_void_p]
         L.ref_f3r_solve.restype = C.c_int
         L.ref_f3r_solve.argtypes = [C.c_int, C.c_int32, C.c_int32, _i32p, _i32p, _f64p, _f64p, _f64p,
                                     C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
@@ -364,6 +370,25 @@ class Ref:
             self.L.ref_pair_copy(h, which, r, i, v)
             mats.append((r, i[:nnz], v[:nnz]))
         return mats
+
+    def gen27_save(self, variant, nx, ny, nz, path):
+        """the reference generator's own .mtx writer (variant 0 hpcg, 1 hpgmp)"""
+        self.L.ref_gen27_save(variant, nx, ny, nz, os.fsencode(path))
+
+    def mm_read_system(self, path):
+        """(rptr, idx, val, b): io::mm::read_system + io::CSR with the drivers' init"""
+        h = self.L.ref_mm_read_system(os.fsencode(path))
+        try:
+            n, nnz = C.c_int32(), C.c_int32()
+            self.L.ref_mm_dims(h, C.byref(n), C.byref(nnz))
+            r = np.zeros(n.value + 1, np.int32)
+            i = np.zeros(max(nnz.value, 1), np.int32)
+            v = np.zeros(max(nnz.value, 1), np.float64)
+            b = np.zeros(max(n.value, 1), np.float64)
+            self.L.ref_mm_copy(h, r, i, v, b)
+            return r, i[:nnz.value], v[:nnz.value], b[:n.value]
+        finally:
+            self.L.ref_mm_free(h)
 
     def sdainv(self, rptr, idx, val, tol=0.1, acc=1.0):
         """returns (Z, Wt) as CSR tuples"""

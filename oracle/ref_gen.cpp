@@ -83,3 +83,39 @@ extern "C" int64_t ref_gen27_halfspace(int nx, int ny, int nz, double beta, int3
   c.nnz = cnt;
   return to_csr(c, rptr, idx, val);
 }
+
+// The reference generators' own file writer (matrix/hpcg.cpp:60-69,
+// matrix/hpgmp.cpp): the .mtx files its suites read (hpcg_7_7_7.mtx, ...).
+extern "C" void ref_gen27_save(int variant, int nx, int ny, int nz, const char *path) {
+  if (variant == 0)
+    ref_hpcg::save_matrix_market(path, ref_hpcg::generate_hpcg(nx, ny, nz));
+  else
+    ref_hpgmp::save_matrix_market(path, ref_hpgmp::generate_hpgmp(nx, ny, nz, 0.5));
+}
+
+// io::mm::read_system + io::CSR (matrix/io.hpp:104-126, 44-60) with the
+// drivers' init (work/src/f3r-gpu.cpp:60), as a handle.
+namespace {
+struct mm_system {
+  kmm::CSR<double, kmm::host> a;
+  kmm::vector<double, kmm::host> b;
+};
+}  // namespace
+extern "C" void *ref_mm_read_system(const char *path) {
+  using namespace kmm;
+  auto [coo, rhs] = io::mm::read_system(path, [](vector<double, host> v) { v.random<0, 1>(std::mt19937_64(0)); });
+  return new mm_system{CSR<double, host>(io::CSR(coo)), rhs};
+}
+extern "C" void ref_mm_dims(void *h, int32_t *n, int32_t *nnz) {
+  auto *s = (mm_system *)h;
+  *n = s->a.nrows();
+  *nnz = s->a.nnz();
+}
+extern "C" void ref_mm_copy(void *h, int32_t *rptr, int32_t *idx, double *val, double *b) {
+  auto *s = (mm_system *)h;
+  std::memcpy(rptr, s->a.rptr.raw(), sizeof(int32_t) * (s->a.nrows() + 1));
+  std::memcpy(idx, s->a.idx.raw(), sizeof(int32_t) * s->a.nnz());
+  std::memcpy(val, s->a.val.raw(), sizeof(double) * s->a.nnz());
+  std::memcpy(b, s->b.raw(), sizeof(double) * s->a.nrows());
+}
+extern "C" void ref_mm_free(void *h) { delete (mm_system *)h; }

@@ -11,6 +11,11 @@ contraction, one OpenMP thread), and records its outputs:
   spmv.npz         SELL<32>::operate / compute_residual at the F3R level types
   solves.npz       full F3R solves (SDAINV + SELL-32, and BJ-ILU(0) + CSR):
                    outer iteration counts, residual histories, final residuals
+  mm/*.mtx, mm.npz Matrix Market inputs (two written by the reference's own
+                   stencil generators, the rest hand-made to cover comments,
+                   symmetric expansion, explicit zeros, integer fields,
+                   unsorted and rectangular input, a "_b" right-hand side)
+                   and what io::mm::read_system + io::CSR make of them
 
 Usage (needs the reference tree; the fixtures are committed):
     OMP_NUM_THREADS=1 python tests/golden/gen_golden.py [--big]
@@ -40,9 +45,85 @@ def rhs_for(ref, rptr, idx, val, seed):
     return xs, b
 
 
+MM_HAND = {
+    # symmetric, comments and a blank line, an explicit off-diagonal zero
+    # (dropped), an explicit zero on the diagonal (kept), entries out of
+    # order, exponent and integer spellings; with a right-hand side file
+    "sym_mixed.mtx": """%%MatrixMarket matrix coordinate real symmetric
+% a comment line
+%another one
+
+6 6 12
+1 1 4.0
+3 1 -1.25e0
+2 2 5
+6 2 -0.5
+3 3 6.5
+4 3 0
+4 4 3.0E+00
+5 5 0.0
+2 1 -1
+6 6 7.25
+5 4 1e-3
+6 5 -2.5
+""",
+    "sym_mixed_b.mtx": """%%MatrixMarket matrix array real general
+% b
+6 1
+1.0
+-2.0
+3.5e-1
+0
+4
+-0.125
+""",
+    # integer field, general, rows out of order, a zero off-diagonal
+    "gen_int.mtx": """%%MatrixMarket matrix coordinate integer general
+5 5 11
+5 5 9
+1 1 3
+2 1 -1
+1 3 2
+3 3 4
+2 2 6
+4 2 0
+4 4 8
+3 5 -2
+5 1 1
+4 3 -3
+""",
+    # rectangular (read_matrix does not require a square matrix)
+    "rect.mtx": """%%MatrixMarket matrix coordinate real general
+3 5 6
+1 5 1.5
+1 2 -2
+2 4 3
+3 1 4
+3 3 5
+2 1 6
+""",
+}
+
+
+def mm_fixtures(ref):
+    d = os.path.join(HERE, "mm")
+    os.makedirs(d, exist_ok=True)
+    for name, text in MM_HAND.items():
+        with open(os.path.join(d, name), "w") as f:
+            f.write(text)
+    ref.gen27_save(0, 3, 4, 3, os.path.join(d, "hpcg_3_4_3.mtx"))
+    ref.gen27_save(1, 4, 3, 3, os.path.join(d, "hpgmp_4_3_3.mtx"))
+    out = {}
+    for name in ("sym_mixed", "gen_int", "rect", "hpcg_3_4_3", "hpgmp_4_3_3"):
+        r, i, v, b = ref.mm_read_system(os.path.join(d, name + ".mtx"))
+        out[name + "_rptr"], out[name + "_idx"], out[name + "_val"], out[name + "_b"] = r, i, v, b
+    np.savez_compressed(os.path.join(HERE, "mm.npz"), **out)
+
+
 def main(big: bool):
     O.build()
     ref = O.Ref("golden")
+    mm_fixtures(ref)
     out = {}
 
     # ---- generators -------------------------------------------------------
