@@ -18,10 +18,12 @@ from typing import Callable, Optional
 import numpy as np
 
 from . import _capi
-from ._capi import F16, F32, F64, PRECOND_ILU0_BJ, PRECOND_SDAINV, F3RError, check, lib
+from ._capi import (F16, F32, F64, PRECOND_ILU0_BAJ, PRECOND_ILU0_BJ, PRECOND_ILU0_JACOBI, PRECOND_SDAINV, TRSV_BAJ,
+                    TRSV_D_UPPER, TRSV_JACOBI, TRSV_LOWER, TRSV_LOWER_D, F3RError, check, lib)
 
 __all__ = ["HostMatrix", "Context", "Sell", "Solver", "Params", "solve_res_t", "F3RError", "F64", "F32", "F16",
-           "PRECOND_SDAINV", "PRECOND_ILU0_BJ", "stencil27", "diffusion7", "random_uniform", "host_spmv",
+           "PRECOND_SDAINV", "PRECOND_ILU0_BJ", "PRECOND_ILU0_JACOBI", "PRECOND_ILU0_BAJ", "Trsv", "TRSV_LOWER",
+           "TRSV_LOWER_D", "TRSV_D_UPPER", "TRSV_JACOBI", "TRSV_BAJ", "stencil27", "diffusion7", "random_uniform", "host_spmv",
            "read_matrix", "read_system", "read_vector", "write_vector", "CSV_HEADER", "csv_row"]
 
 _NP2DT = {np.dtype(np.float64): F64, np.dtype(np.float32): F32, np.dtype(np.float16): F16}
@@ -254,6 +256,31 @@ class Sell:
     def close(self):
         if getattr(self, "_h", None) is not None and _capi is not None and _capi._lib is not None:
             _capi._lib.f3r_sell_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+
+class Trsv:
+    """Jacobi-iteration triangular solve on the device (f3r_trsv):
+    trsv::{l,ld,du}::Jacobi / BAJ <SELL<32, __half>> (trsv/jacobi.hpp,
+    trsv/baj.hpp).  ``solve(in, out)`` takes fp16 device tensors."""
+
+    def __init__(self, ctx: Context, M: HostMatrix, form: int, kind: int = TRSV_JACOBI, iters: int = 2,
+                 omega: float = 1.0):
+        h = C.c_void_p()
+        v = M.view()
+        check(lib().f3r_trsv_create(ctx._h, C.byref(v), form, kind, iters, omega, C.byref(h)))
+        self._h = h
+        self.ctx = ctx
+
+    def solve(self, x, y) -> None:
+        check(lib().f3r_trsv_solve(self._h, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr())))
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and _capi is not None and _capi._lib is not None:
+            _capi._lib.f3r_trsv_destroy(self._h)
             self._h = None
 
     def __del__(self):

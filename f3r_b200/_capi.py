@@ -16,7 +16,9 @@ STATUS = {0: "SUCCESS", 1: "INVALID_VALUE", 2: "CUDA", 3: "OUT_OF_MEMORY", 5: "B
           8: "UNSUPPORTED", 9: "NO_DEVICE"}
 F64, F32, F16 = 0, 1, 2
 SELL_INDEX16 = 1 << 8
-PRECOND_SDAINV, PRECOND_ILU0_BJ = 0, 1
+PRECOND_SDAINV, PRECOND_ILU0_BJ, PRECOND_ILU0_JACOBI, PRECOND_ILU0_BAJ = 0, 1, 2, 3
+TRSV_LOWER, TRSV_LOWER_D, TRSV_D_UPPER = 0, 1, 2
+TRSV_JACOBI, TRSV_BAJ = 0, 1
 
 
 class F3RError(RuntimeError):
@@ -35,7 +37,8 @@ class Params(C.Structure):
                 ("m4", C.c_int32), ("c", C.c_int32), ("precond", C.c_int32), ("ilu_blocks", C.c_int32),
                 ("sdainv_tol", C.c_double), ("acc", C.c_double), ("sell_c", C.c_int32), ("sell_sigma", C.c_int32),
                 ("rel_tol", C.c_double), ("half_scale_log2", C.c_int32), ("use_graphs", C.c_int32),
-                ("sell_index16", C.c_int32), ("static_weight", C.c_double), ("reserved", C.c_int32 * 8)]
+                ("sell_index16", C.c_int32), ("static_weight", C.c_double), ("trsv_iters", C.c_int32),
+                ("reserved0", C.c_int32), ("trsv_omega", C.c_double), ("reserved", C.c_int32 * 8)]
 
 
 class Result(C.Structure):
@@ -75,6 +78,9 @@ SIGNATURES = {
     "f3r_host_spmv": (C.c_int, [C.POINTER(CSR), _vp, _vp]),
     "f3r_random_uniform": (C.c_int, [C.c_uint64, C.c_double, C.c_double, C.c_int64, _vp]),
     "f3r_mm_read": (C.c_int, [C.c_char_p, C.POINTER(_vp)]),
+    "f3r_trsv_create": (C.c_int, [_vp, C.POINTER(CSR), C.c_int32, C.c_int32, C.c_int32, C.c_double, C.POINTER(_vp)]),
+    "f3r_trsv_solve": (C.c_int, [_vp, _vp, _vp]),
+    "f3r_trsv_destroy": (None, [_vp]),
     "f3r_mm_read_vector": (C.c_int, [C.c_char_p, C.c_int64, _vp]),
     "f3r_mm_read_rhs": (C.c_int, [C.c_char_p, C.c_int64, _vp, C.POINTER(C.c_int32)]),
     "f3r_mm_write": (C.c_int, [C.c_char_p, C.POINTER(CSR)]),

@@ -125,6 +125,28 @@ inline Status launch_sell(Context &c, const V *val, const DevSell &A, const X *x
 }
 
 
+// ---------------------------------------------------------------------------
+// SELL-32 construction on the host (solver.cu)
+// ---------------------------------------------------------------------------
+struct SellHost {
+  int32_t n = 0, ncols = 0, nslices = 0, max_width = 0, sigma = 1;
+  int64_t nnz = 0, nnz_pad = 0;
+  std::vector<int32_t> sptr, col, perm;  // perm: storage row -> original row
+  std::vector<double> val;
+  std::vector<uint16_t> dcol;            // 16-bit offsets (when they fit)
+  std::vector<int32_t> cbase;            // base of each slice column, slice s from cbptr[s]
+  std::vector<int32_t> cbptr;            // nslices + 1, multiples of 4
+};
+
+// Rows sorted by decreasing length in windows of sigma (renumber: columns
+// mapped to the storage order too, P A P^T); given_perm fixes the order.
+Status build_sell(const f3r_csr &a, int32_t sigma, bool renumber, SellHost &s,
+                  const std::vector<int32_t> *given_perm = nullptr);
+// 16-bit column offsets when every slice column fits a 65536 window
+bool compress_index16(SellHost &s);
+// Uploads the value copies selected by dtype_mask (bit 1 << f3r_dtype).
+Status upload_sell(Context &c, const SellHost &h, int dtype_mask, bool scatter_perm, DeviceSell &d);
+
 }  // namespace f3r
 
 struct f3r_context : f3r::Context {};

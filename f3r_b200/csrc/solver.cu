@@ -24,6 +24,7 @@
 #include "kernels.cuh"
 #include "ilu.cuh"
 #include "objects.cuh"
+#include "trsv.hpp"
 
 namespace f3r {
 
@@ -36,19 +37,9 @@ Status fail(Status code, const std::string &msg) {
 // ---------------------------------------------------------------------------
 // SELL-32 construction on the host
 // ---------------------------------------------------------------------------
-struct SellHost {
-  int32_t n = 0, ncols = 0, nslices = 0, max_width = 0, sigma = 1;
-  int64_t nnz = 0, nnz_pad = 0;
-  std::vector<int32_t> sptr, col, perm;  // perm: storage row -> original row
-  std::vector<double> val;
-  std::vector<uint16_t> dcol;            // 16-bit offsets (when they fit)
-  std::vector<int32_t> cbase;            // base of each slice column, slice s from cbptr[s]
-  std::vector<int32_t> cbptr;            // nslices + 1, multiples of 4
-};
-
 // Re-expresses the column indices as 16-bit offsets from the smallest index
 // of each slice column, if every slice column spans fewer than 65536 columns.
-static bool compress_index16(SellHost &s) {
+bool compress_index16(SellHost &s) {
   const int64_t ncolsl = s.sptr[s.nslices];
   std::vector<int32_t> base(ncolsl);
   bool ok = true;
@@ -81,8 +72,8 @@ static bool compress_index16(SellHost &s) {
 
 // renumber = true builds P A P^T (columns mapped to storage order) for the
 // solver's permuted system; false keeps original columns and scatters rows.
-static Status build_sell(const f3r_csr &a, int32_t sigma, bool renumber, SellHost &s,
-                         const std::vector<int32_t> *given_perm = nullptr) {
+Status build_sell(const f3r_csr &a, int32_t sigma, bool renumber, SellHost &s,
+                  const std::vector<int32_t> *given_perm) {
   if (sigma < 1) return fail(F3R_ERROR_INVALID_VALUE, "sigma must be >= 1");
   if (renumber && a.nrows != a.ncols) return fail(F3R_ERROR_INVALID_VALUE, "symmetric permutation needs a square matrix");
   const int32_t n = a.nrows;
@@ -147,7 +138,7 @@ static Status build_sell(const f3r_csr &a, int32_t sigma, bool renumber, SellHos
   return F3R_SUCCESS;
 }
 
-static Status upload_sell(Context &c, const SellHost &h, int dtype_mask, bool scatter_perm, DeviceSell &d) {
+Status upload_sell(Context &c, const SellHost &h, int dtype_mask, bool scatter_perm, DeviceSell &d) {
   d.n = h.n; d.ncols = h.ncols; d.nslices = h.nslices; d.max_width = h.max_width; d.sigma = h.sigma;
   d.nnz = h.nnz; d.nnz_pad = h.nnz_pad; d.dtypes = dtype_mask;
   const size_t np = (size_t)h.nnz_pad;
@@ -242,6 +233,7 @@ struct Solver {
   __half *wd = nullptr, *zd = nullptr;
   DeviceSell W, Z;    // general SDAINV factors (permuted system)
   IluDevice ilu;      // block-Jacobi ILU(0), level scheduled
+  JacobiTrsv jl, ju;  // the same factors solved by Jacobi / BAJ sweeps
   // levels
   Level<double> L1;
   Level<float> L2, L3;
@@ -266,7 +258,7 @@ struct Solver {
   ~Solver() {
     for (auto &kv : graphs) cudaGraphExecDestroy(kv.second.first);
     for (void *q : allocs) cudaFree(q);
-    A.release(); W.release(); Z.release(); ilu.release();
+    A.release(); W.release(); Z.release(); ilu.release(); jl.release(); ju.release();
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
   }
@@ -350,8 +342,12 @@ struct Solver {
     if (p.precond == F3R_PRECOND_SDAINV) {
       F3R_TRY(launch_sell(C(), W.v16, W.view(), x, EpiStore<__half>{tmp, nullptr}));
       F3R_TRY(launch_sell(C(), Z.v16, Z.view(), (const __half *)tmp, EpiZScale{out, rs, scale_ome ? 1 : 0}));
-    } else {
+    } else if (p.precond == F3R_PRECOND_ILU0_BJ) {
       F3R_TRY(ilu.apply(C().stream, x, tmp, out, scale_ome ? &rs->ome[0] : nullptr));
+      C().launches += 2;
+    } else {
+      F3R_TRY(jl.apply(C(), x, tmp, nullptr));
+      F3R_TRY(ju.apply(C(), tmp, out, scale_ome ? &rs->ome[0] : nullptr));
     }
     return F3R_SUCCESS;
   }
@@ -638,7 +634,7 @@ static Status make_solver(f3r_context *ctx, const f3r_csr *a, const f3r_params *
                 "need 1 <= m_outer, m2 <= 127, 0 <= m3 <= 127, 1 <= m4 <= 16, c >= 1, max_restarts >= 1, "
                 "static_weight >= 0");
   if (p.sell_c != 32) return fail(F3R_ERROR_UNSUPPORTED, "only SELL slice height 32 is implemented");
-  if (p.precond != F3R_PRECOND_SDAINV && p.precond != F3R_PRECOND_ILU0_BJ)
+  if (p.precond < F3R_PRECOND_SDAINV || p.precond > F3R_PRECOND_ILU0_BAJ)
     return fail(F3R_ERROR_INVALID_VALUE, "unknown preconditioner");
   if (p.half_scale_log2 < 0 || p.half_scale_log2 > 20) return fail(F3R_ERROR_INVALID_VALUE, "half_scale_log2 in [0, 20]");
   auto s = std::make_unique<Solver>();
@@ -710,7 +706,15 @@ static Status make_solver(f3r_context *ctx, const f3r_csr *a, const f3r_params *
     std::vector<int32_t> bptr;
     F3R_TRY(ilu0_bj(Ah, p.ilu_blocks, p.acc, &lr, &ur, &bptr));
     std::unique_ptr<HostCSR> Lh(lr), Uh(ur);
-    F3R_TRY(s->ilu.build(ctx->stream, *Lh, *Uh, hperm, p.sell_sigma > 1, bptr));
+    if (p.precond == F3R_PRECOND_ILU0_BJ) {
+      F3R_TRY(s->ilu.build(ctx->stream, *Lh, *Uh, hperm, p.sell_sigma > 1, bptr));
+    } else {
+      const int kind = p.precond == F3R_PRECOND_ILU0_BAJ ? TRSV_BAJ : TRSV_JACOBI;
+      F3R_TRY(jacobi_trsv_prepare(*ctx));
+      F3R_TRY(s->jl.build(*ctx, *Lh, FORM_LOWER, kind, p.trsv_iters, p.trsv_omega, p.sell_sigma > 1 ? &hperm : nullptr));
+      F3R_TRY(s->ju.build(*ctx, *Uh, FORM_D_UPPER, kind, p.trsv_iters, p.trsv_omega,
+                          p.sell_sigma > 1 ? &hperm : nullptr));
+    }
   }
   // level storage
   F3R_TRY(s->make_level(s->L1, p.m_outer, true));
@@ -1054,6 +1058,8 @@ void f3r_params_default(f3r_params *p) {
   p->rel_tol = 1e-8;
   p->half_scale_log2 = 0;
   p->use_graphs = 1;
+  p->trsv_iters = 2;
+  p->trsv_omega = 1.0;
 }
 
 f3r_status f3r_solver_create(f3r_context *ctx, const f3r_csr *a, const f3r_params *p, f3r_solver **out) {

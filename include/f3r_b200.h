@@ -48,8 +48,13 @@ typedef enum f3r_status {
 typedef enum f3r_dtype { F3R_F64 = 0, F3R_F32 = 1, F3R_F16 = 2 } f3r_dtype;
 
 typedef enum f3r_precond {
-  F3R_PRECOND_SDAINV = 0,  /* SDAINV Z*(W^T r), as work/src/f3r-gpu.cpp:74,215-216 */
-  F3R_PRECOND_ILU0_BJ = 1  /* block-Jacobi ILU(0), as work/src/f3r.cpp:57-58,200-201 */
+  F3R_PRECOND_SDAINV = 0,      /* SDAINV Z*(W^T r), as work/src/f3r-gpu.cpp:74,215-216 */
+  F3R_PRECOND_ILU0_BJ = 1,     /* block-Jacobi ILU(0), exact triangular solves, as
+                                  work/src/f3r.cpp:57-58,200-201 */
+  F3R_PRECOND_ILU0_JACOBI = 2, /* the same ILU(0) factors, triangular solves by trsv_iters
+                                  Jacobi sweeps (trsv/jacobi.hpp:290-505) */
+  F3R_PRECOND_ILU0_BAJ = 3     /* ... by trsv_iters in-place BAJ sweeps (trsv/baj.hpp:95-190);
+                                  results depend on scheduling before convergence */
 } f3r_precond;
 
 /* Host CSR matrix, borrowed for the duration of a call.  Rows sorted by
@@ -90,6 +95,10 @@ typedef struct f3r_params {
   double static_weight;    /* 0: adaptive weights (F3R).  w > 0: fixed weight w for every
                               Richardson step, never updated ("F3R-Static",
                               work/src/static.cpp:99-114) */
+  int32_t trsv_iters;      /* ILU0_JACOBI: sweeps per triangular solve (Jacobi max_ier, 2);
+                              ILU0_BAJ: BAJ max_iter (the first is the diagonal scaling) */
+  int32_t reserved0;
+  double trsv_omega;       /* ILU0_JACOBI: damping omega in (0, 2], 1.0 */
   int32_t reserved[8];
 } f3r_params;
 
@@ -203,6 +212,27 @@ f3r_status f3r_mm_read_rhs(const char *matrix_path, int64_t n, double *b, int32_
 f3r_status f3r_mm_write(const char *path, const f3r_csr *a);
 /* Writes an n x 1 array file (%.17g). */
 f3r_status f3r_mm_write_vector(const char *path, int64_t n, const double *x);
+
+/* ------------------------------------------------- Jacobi triangular solves
+ * trsv::{l,ld,du}::Jacobi<SELL<32, __half>> and BAJ<SELL<32, __half>>
+ * (trsv/jacobi.hpp:290-505, trsv/baj.hpp:95-190) on the device: `iters`
+ * parallel sweeps instead of a sequential triangular solve.  The factor is
+ * given in its stored form (host CSR); vectors are fp16 device pointers. */
+typedef struct f3r_trsv f3r_trsv;
+typedef enum f3r_trsv_form {
+  F3R_TRSV_LOWER = 0,   /* lower, unit diagonal stored last in each row (not read) */
+  F3R_TRSV_LOWER_D = 1, /* lower, diagonal stored last */
+  F3R_TRSV_D_UPPER = 2  /* upper, diagonal stored first */
+} f3r_trsv_form;
+typedef enum f3r_trsv_kind {
+  F3R_TRSV_JACOBI = 0, /* y0 = w D^-1 in; iters sweeps y = w D^-1 (in - N y) + (1 - w) y */
+  F3R_TRSV_BAJ = 1     /* y = D^-1 in; iters - 1 in-place sweeps y = D^-1 (in - N y) */
+} f3r_trsv_kind;
+f3r_status f3r_trsv_create(f3r_context *ctx, const f3r_csr *m, int32_t form, int32_t kind, int32_t iters,
+                           double omega, f3r_trsv **out);
+/* out = the approximate M^-1 in, on the context's stream; in must not be out. */
+f3r_status f3r_trsv_solve(f3r_trsv *t, const void *in, void *out);
+void f3r_trsv_destroy(f3r_trsv *t);
 
 /* ---------------------------------------------------------------- context */
 f3r_status f3r_context_create(int32_t device, f3r_context **out);

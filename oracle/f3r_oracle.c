@@ -29,7 +29,8 @@ typedef _Float16 f16;
 
 enum { DT_F64 = 0, DT_F32 = 1, DT_F16 = 2 };
 enum { ARITH_PRODUCT = 0, ARITH_REF = 1 };
-enum { PRECOND_SDAINV = 0, PRECOND_ILU0_BJ = 1 };
+enum { PRECOND_SDAINV = 0, PRECOND_ILU0_BJ = 1, PRECOND_ILU0_JACOBI = 2, PRECOND_ILU0_BAJ = 3 };
+enum { FORM_LOWER = 0, FORM_LOWER_D = 1, FORM_D_UPPER = 2 };
 
 /* ------------------------------------------------------------------------ */
 /* owned CSR matrix (values in fp64)                                        */
@@ -555,6 +556,108 @@ void or_trsv_upper(const or_mat *U, int val_t, const void *in, int x_t, void *ou
 }
 
 /* ------------------------------------------------------------------------ */
+/* Jacobi-iteration triangular solves on fp16 vectors.                      */
+/*                                                                          */
+/* Jacobi (trsv/jacobi.hpp:290-505): y0 = om D^-1 in, then `iters` sweeps    */
+/* y <- om D^-1 (in - N y) + (1 - om) y, N the strictly triangular part,    */
+/* double-buffered.  BAJ (trsv/baj.hpp:95-190): y = D^-1 in, then iters-1   */
+/* sweeps y <- D^-1 (in - N y) in place, rows in solve order (the reference */
+/* on one thread; on more threads a row may see older values).  Forms       */
+/* (matrix/base.hpp): LOWER unit diagonal stored last (not read), LOWER_D   */
+/* diagonal stored last, D_UPPER diagonal stored first; D^-1 is the fp16    */
+/* rounding of the fp64 reciprocal (CSR::inverse_last, csr.hpp:60-65).      */
+/*                                                                          */
+/* ARITH_PRODUCT (the CUDA path): acc = fp32 fma chain over N's entries by  */
+/* increasing column from 0, r = in - acc, q = r * dinv (fp32),             */
+/* y = fmaf(om, q, (1 - om) * y_old) with om = (float)omega; init           */
+/* y0 = om * (in * dinv).  ARITH_REF (the reference's expressions): t = in, */
+/* t -= v * x in fp16 (lower forms by increasing column, D_UPPER by         */
+/* decreasing column: its 180-degree rotated copy), the update in double:   */
+/* om * t * dinv + (1 - om) * y_old, one rounding to fp16.                  */
+/* ------------------------------------------------------------------------ */
+static void tri_parts(const or_mat *M, int form, int32_t i, int32_t *b, int32_t *e, int32_t *d) {
+  if (form == FORM_D_UPPER) { *d = M->rptr[i]; *b = M->rptr[i] + 1; *e = M->rptr[i + 1]; }
+  else { *d = M->rptr[i + 1] - 1; *b = M->rptr[i]; *e = M->rptr[i + 1] - 1; }
+}
+
+static double tri_sum_ref(const or_mat *M, int form, int32_t i, const f16 *in, const f16 *x) {
+  int32_t b, e, d;
+  tri_parts(M, form, i, &b, &e, &d);
+  f16 t = in[i];
+  if (form == FORM_D_UPPER) {
+    for (int32_t j = e - 1; j >= b; j--) t = (f16)((float)t - (float)(f16)((float)(f16)M->val[j] * (float)x[M->idx[j]]));
+  } else {
+    for (int32_t j = b; j < e; j++) t = (f16)((float)t - (float)(f16)((float)(f16)M->val[j] * (float)x[M->idx[j]]));
+  }
+  return (double)t;
+}
+
+static float tri_sum_prod(const or_mat *M, int form, int32_t i, const f16 *in, const f16 *x) {
+  int32_t b, e, d;
+  tri_parts(M, form, i, &b, &e, &d);
+  float acc = 0.0f;
+  for (int32_t j = b; j < e; j++) acc = fmaf((float)(f16)M->val[j], (float)x[M->idx[j]], acc);
+  return (float)in[i] - acc;
+}
+
+void or_jacobi_trsv(const or_mat *M, int form, int baj, int32_t iters, double omega, int arith, const f16 *in,
+                    f16 *out) {
+  int32_t n = M->n;
+  f16 *dinv = (f16 *)malloc(sizeof(f16) * (n > 0 ? n : 1));
+  for (int32_t i = 0; i < n; i++) {
+    int32_t b, e, d;
+    tri_parts(M, form, i, &b, &e, &d);
+    dinv[i] = form == FORM_LOWER ? (f16)1.0f : (f16)(1.0 / M->val[d]);
+  }
+  const int has_d = form != FORM_LOWER;
+  if (baj) {
+    for (int32_t i = 0; i < n; i++) {
+      if (arith == ARITH_REF) out[i] = has_d ? (f16)((float)in[i] * (float)dinv[i]) : in[i];
+      else out[i] = has_d ? (f16)((float)in[i] * (float)dinv[i]) : in[i];
+    }
+    for (int32_t k = 1; k < iters; k++) {
+      for (int32_t q = 0; q < n; q++) {
+        int32_t i = form == FORM_D_UPPER ? n - 1 - q : q;
+        if (arith == ARITH_REF) {
+          f16 t = (f16)tri_sum_ref(M, form, i, in, out);
+          out[i] = has_d ? (f16)((float)t * (float)dinv[i]) : t;
+        } else {
+          float r = tri_sum_prod(M, form, i, in, out);
+          out[i] = (f16)(has_d ? r * (float)dinv[i] : r);
+        }
+      }
+    }
+    free(dinv);
+    return;
+  }
+  f16 *y = (f16 *)malloc(sizeof(f16) * (n > 0 ? n : 1));
+  f16 *z = (f16 *)malloc(sizeof(f16) * (n > 0 ? n : 1));
+  const float om = (float)omega, omc = 1.0f - om;
+  for (int32_t i = 0; i < n; i++) {
+    if (arith == ARITH_REF)
+      y[i] = (f16)(has_d ? omega * (double)in[i] * (double)dinv[i] : omega * (double)in[i]);
+    else
+      y[i] = (f16)(om * (has_d ? (float)in[i] * (float)dinv[i] : (float)in[i]));
+  }
+  for (int32_t k = 0; k < iters; k++) {
+    for (int32_t i = 0; i < n; i++) {
+      if (arith == ARITH_REF) {
+        double t = tri_sum_ref(M, form, i, in, y);
+        z[i] = (f16)(has_d ? omega * t * (double)dinv[i] + (1.0 - omega) * (double)y[i]
+                           : omega * t + (1.0 - omega) * (double)y[i]);
+      } else {
+        float r = tri_sum_prod(M, form, i, in, y);
+        float q = has_d ? r * (float)dinv[i] : r;
+        z[i] = (f16)fmaf(om, q, omc * (float)y[i]);
+      }
+    }
+    f16 *t = y; y = z; z = t;
+  }
+  memcpy(out, y, sizeof(f16) * n);
+  free(y); free(z); free(dinv);
+}
+
+/* ------------------------------------------------------------------------ */
 /* Reductions.  The reference reduces with OpenMP (host) or a three-stage   */
 /* tree (device); neither order is reproducible, so the oracle sums in      */
 /* blocks of 256 in the vector's arithmetic type.                           */
@@ -595,6 +698,9 @@ typedef struct {
   int32_t half_scale_log2; /* 0: plain fp32->fp16 cast (reference); k: scale by 2^k */
   double tol;          /* stop when implicit residual / ||b|| < tol */
   double static_weight; /* > 0: F3R-Static, fixed weight (work/src/static.cpp:99-114) */
+  int32_t trsv_iters;  /* PRECOND_ILU0_JACOBI / _BAJ: sweeps (max_ier / max_iter) */
+  int32_t pad_;
+  double trsv_omega;   /* PRECOND_ILU0_JACOBI: damping omega */
 } or_f3r_params;
 
 #define MAXM4 16
@@ -654,10 +760,14 @@ static void prec_apply(f3r_ctx *c, const f16 *x, f16 *y, f16 *work) {
   if (c->p.precond == PRECOND_SDAINV) {
     csr16_apply(c, c->P1, x, work);
     csr16_apply(c, c->P2, work, y);
-  } else {
+  } else if (c->p.precond == PRECOND_ILU0_BJ) {
     int pf = (c->p.arith == ARITH_PRODUCT);
     or_trsv_lower(c->P1, DT_F16, x, DT_F16, work, pf);
     or_trsv_upper(c->P2, DT_F16, work, DT_F16, y, pf);
+  } else {
+    int baj = c->p.precond == PRECOND_ILU0_BAJ;
+    or_jacobi_trsv(c->P1, FORM_LOWER, baj, c->p.trsv_iters, c->p.trsv_omega, c->p.arith, x, work);
+    or_jacobi_trsv(c->P2, FORM_D_UPPER, baj, c->p.trsv_iters, c->p.trsv_omega, c->p.arith, work, y);
   }
 }
 

@@ -24,7 +24,8 @@ REF_DIR = os.path.join(HERE, "_ref")
 
 DT_F64, DT_F32, DT_F16 = 0, 1, 2
 ARITH_PRODUCT, ARITH_REF = 0, 1
-PRECOND_SDAINV, PRECOND_ILU0_BJ = 0, 1
+PRECOND_SDAINV, PRECOND_ILU0_BJ, PRECOND_ILU0_JACOBI, PRECOND_ILU0_BAJ = 0, 1, 2, 3
+FORM_LOWER, FORM_LOWER_D, FORM_D_UPPER = 0, 1, 2
 
 _i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
 _f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
@@ -71,6 +72,7 @@ def lib() -> C.CDLL:
         L.or_ilu0_bj.restype = C.c_int
         L.or_ilu0_bj.argtypes = [C.c_void_p, C.c_int32, C.c_double, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]
         L.or_trsv_lower.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_int]
+        L.or_jacobi_trsv.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int32, C.c_double, C.c_int, _u16p, _u16p]
         L.or_trsv_upper.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_int]
         L.or_dot_f32.restype = C.c_float
         L.or_dot_f32.argtypes = [C.c_int32, _f32p, _f32p]
@@ -91,12 +93,14 @@ def lib() -> C.CDLL:
 class F3RParams(C.Structure):
     _fields_ = [("m1", C.c_int32), ("restarts", C.c_int32), ("m2", C.c_int32), ("m3", C.c_int32),
                 ("m4", C.c_int32), ("c", C.c_int32), ("precond", C.c_int32), ("arith", C.c_int32),
-                ("half_scale_log2", C.c_int32), ("tol", C.c_double), ("static_weight", C.c_double)]
+                ("half_scale_log2", C.c_int32), ("tol", C.c_double), ("static_weight", C.c_double),
+                ("trsv_iters", C.c_int32), ("pad_", C.c_int32), ("trsv_omega", C.c_double)]
 
 
 def params(m1=100, restarts=20, m2=8, m3=4, m4=2, c=64, precond=PRECOND_SDAINV, arith=ARITH_PRODUCT,
-           half_scale_log2=0, tol=1e-10, static_weight=0.0) -> F3RParams:
-    return F3RParams(m1, restarts, m2, m3, m4, c, precond, arith, half_scale_log2, tol, static_weight)
+           half_scale_log2=0, tol=1e-10, static_weight=0.0, trsv_iters=3, trsv_omega=1.0) -> F3RParams:
+    return F3RParams(m1, restarts, m2, m3, m4, c, precond, arith, half_scale_log2, tol, static_weight, trsv_iters,
+                     0, trsv_omega)
 
 
 class Mat:
@@ -198,6 +202,17 @@ def trsv(M: Mat, upper: bool, x: np.ndarray, prod_fma=False):
     return out
 
 
+def jacobi_trsv(M: Mat, form: int, x: np.ndarray, iters: int, omega: float = 1.0, baj: bool = False,
+                arith: int = ARITH_PRODUCT) -> np.ndarray:
+    """Jacobi (trsv/jacobi.hpp) or BAJ (trsv/baj.hpp, one-thread row order)
+    triangular solve of fp16 vectors; form FORM_LOWER / FORM_LOWER_D /
+    FORM_D_UPPER."""
+    xin = np.ascontiguousarray(x, np.float16).view(np.uint16)
+    out = np.zeros(len(xin), np.uint16)
+    lib().or_jacobi_trsv(M.ptr, form, int(baj), iters, omega, arith, xin, out)
+    return out.view(np.float16)
+
+
 def f3r_solve(A: Mat, P1: Mat, P2: Mat, b, p: F3RParams, x0=None, hist_cap=4096):
     n = len(b)
     x = np.zeros(n) if x0 is None else np.array(x0, np.float64)
@@ -288,6 +303,8 @@ class Ref:
         L.ref_pair_copy.argtypes = [C.c_void_p, C.c_int, _i32p, _i32p, _f64p]
         L.ref_bj_solve_f16.argtypes = [C.c_void_p, C.c_int, C.c_int, _u16p, _u16p]
         L.ref_pair_free.argtypes = [C.c_void_p]
+        L.ref_jacobi_trsv_f16.argtypes = [C.c_int32, C.c_int32, _i32p, _i32p, _f64p, C.c_int, C.c_int, C.c_int,
+                                          C.c_double, _u16p, _u16p]
         L.ref_gen27_save.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_char_p]
         L.ref_mm_read_system.restype = C.c_void_p
         L.ref_mm_read_system.argtypes = [C.c_char_p]
@@ -370,6 +387,16 @@ class Ref:
             self.L.ref_pair_copy(h, which, r, i, v)
             mats.append((r, i[:nnz], v[:nnz]))
         return mats
+
+    def jacobi_trsv(self, rptr, idx, val, form, x16, iters, omega=1.0, baj=False, csr=False):
+        """trsv::{l,ld,du}::Jacobi / BAJ <SELL<32, _Float16>> (or <CSR<_Float16>>) solve of fp16 x"""
+        n = len(rptr) - 1
+        xin = np.ascontiguousarray(x16, np.float16).view(np.uint16)
+        out = np.zeros(n, np.uint16)
+        self.L.ref_jacobi_trsv_f16(n, len(idx), np.ascontiguousarray(rptr, np.int32), np.ascontiguousarray(idx, np.int32),
+                                   np.ascontiguousarray(val, np.float64), form, int(baj) + 2 * int(csr), iters, omega, xin,
+                                   out)
+        return out.view(np.float16)
 
     def gen27_save(self, variant, nx, ny, nz, path):
         """the reference generator's own .mtx writer (variant 0 hpcg, 1 hpgmp)"""

@@ -27,7 +27,9 @@
 #include "umineko-sparse/preconditioner/ilu.hpp"
 #include "umineko-sparse/solver/gmres.hpp"
 #include "umineko-sparse/solver/restart.hpp"
+#include "umineko-sparse/trsv/baj.hpp"
 #include "umineko-sparse/trsv/bj.hpp"
+#include "umineko-sparse/trsv/jacobi.hpp"
 
 namespace refc {
 

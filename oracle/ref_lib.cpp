@@ -137,6 +137,36 @@ void ref_bj_solve_f16(void *h, int blocks, int upper, const uint16_t *in, uint16
 }
 void ref_pair_free(void *h) { delete (pair_t *)h; }
 
+// Jacobi-iteration triangular solves in fp16: Jacobi on SELL<32>
+// (trsv/jacobi.hpp:290-505, kind 0), BAJ on SELL<32> (trsv/baj.hpp:95-190,
+// kind 1), and the same two on CSR (jacobi.hpp:27-141, baj.hpp:27-93; kinds
+// 2, 3); form 0 lower (unit diagonal last), 1 lower_d (diagonal last),
+// 2 d_upper (diagonal first).
+void ref_jacobi_trsv_f16(int32_t n, int32_t nnz, const int32_t *rptr, const int32_t *idx, const double *val,
+                         int form, int kind, int iters, double omega, const uint16_t *in, uint16_t *out) {
+  auto m = refc::make_csr(n, nnz, rptr, idx, val);
+  auto iv = vector<h16, host>(n), ov = vector<h16, host>(n);
+  std::memcpy(iv.raw(), in, 2 * n);
+  if (kind == 0) {
+    if (form == 0) trsv::l::Jacobi<SELL<32, h16, host>>(m, {iters, omega}).solve(iv, ov);
+    if (form == 1) trsv::ld::Jacobi<SELL<32, h16, host>>(m, {iters, omega}).solve(iv, ov);
+    if (form == 2) trsv::du::Jacobi<SELL<32, h16, host>>(m, {iters, omega}).solve(iv, ov);
+  } else if (kind == 1) {
+    if (form == 0) trsv::l::BAJ<SELL<32, h16, host>>(m, {iters, omega}).solve(iv, ov);
+    if (form == 1) trsv::ld::BAJ<SELL<32, h16, host>>(m, {iters, omega}).solve(iv, ov);
+    if (form == 2) trsv::du::BAJ<SELL<32, h16, host>>(m, {iters, omega}).solve(iv, ov);
+  } else if (kind == 2) {
+    if (form == 0) trsv::l::Jacobi<CSR<h16, host>>(m, {iters, omega}).solve(iv, ov);
+    if (form == 1) trsv::ld::Jacobi<CSR<h16, host>>(m, {iters, omega}).solve(iv, ov);
+    if (form == 2) trsv::du::Jacobi<CSR<h16, host>>(m, {iters, omega}).solve(iv, ov);
+  } else {
+    if (form == 0) trsv::l::BAJ<CSR<h16, host>>(m, {iters, omega}).solve(iv, ov);
+    if (form == 1) trsv::ld::BAJ<CSR<h16, host>>(m, {iters, omega}).solve(iv, ov);
+    if (form == 2) trsv::du::BAJ<CSR<h16, host>>(m, {iters, omega}).solve(iv, ov);
+  }
+  std::memcpy(out, ov.raw(), 2 * n);
+}
+
 // Full F3R solves (stop_after > 0: only that many outer steps).  config 0: SDAINV + SELL-32 (f3r-gpu.cpp:210-265);
 // config 1: BJ-ILU(0) + CSR (f3r.cpp:195-248); config 2: F3R-Static with
 // weight `weight` over BJ-ILU(0) (static.cpp:99-119); configs 3 / 4: the

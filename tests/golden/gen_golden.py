@@ -11,6 +11,9 @@ contraction, one OpenMP thread), and records its outputs:
   spmv.npz         SELL<32>::operate / compute_residual at the F3R level types
   solves.npz       full F3R solves (SDAINV + SELL-32, and BJ-ILU(0) + CSR):
                    outer iteration counts, residual histories, final residuals
+  trsv.npz         Jacobi-iteration and BAJ triangular solves (trsv/jacobi.hpp,
+                   trsv/baj.hpp) in fp16 on the BJ-ILU(0) factors of setup.npz
+                   and on a lower triangle with a real diagonal
   mm/*.mtx, mm.npz Matrix Market inputs (two written by the reference's own
                    stencil generators, the rest hand-made to cover comments,
                    symmetric expansion, explicit zeros, integer fields,
@@ -120,6 +123,39 @@ def mm_fixtures(ref):
     np.savez_compressed(os.path.join(HERE, "mm.npz"), **out)
 
 
+TRSV_CASES = [  # (kind, iters, omega): Jacobi on SELL, BAJ on SELL, and the CSR forms
+    ("jac", 0, 1.0), ("jac", 1, 1.0), ("jac", 2, 0.7), ("jac", 5, 1.0), ("jac", 3, 1.2),
+    ("baj", 1, 1.0), ("baj", 2, 1.0), ("baj", 6, 1.0),
+    ("jaccsr", 3, 0.8), ("bajcsr", 1, 1.0), ("bajcsr", 3, 1.0)]
+
+
+def tril_with_diagonal(rptr, idx, val):
+    """lower triangle (diagonal last) of a CSR matrix"""
+    rows = np.repeat(np.arange(len(rptr) - 1), np.diff(rptr))
+    keep = idx <= rows
+    r = np.concatenate([[0], np.cumsum(np.bincount(rows[keep], minlength=len(rptr) - 1))]).astype(np.int32)
+    return r, idx[keep].astype(np.int32), val[keep].astype(np.float64)
+
+
+def trsv_fixtures(ref, s):
+    """s: the setup.npz dictionary (hpcg8 ILU factors, bj_in)"""
+    t = {}
+    r, i, v = ref.gen27(8, 8, 8, variant=0)  # unscaled: diagonal 26
+    tl = tril_with_diagonal(r, i, v)
+    t["tl_rptr"], t["tl_idx"], t["tl_val"] = tl
+    key = "hpcg8_ilu16"
+    mats = {"L": (s[key + "_L_rptr"], s[key + "_L_idx"], s[key + "_L_val"], 0), "Tl": tl + (1,),
+            "U": (s[key + "_U_rptr"], s[key + "_U_idx"], s[key + "_U_val"], 2)}
+    for name, (mr, mi, mv, form) in mats.items():
+        for kind, iters, om in TRSV_CASES:
+            if kind == "baj" and name == "U" and iters == 1:
+                continue  # the SELL form's d_upper init pairs in[i] with row n-1-i's diagonal (baj.hpp:161-170)
+            out = ref.jacobi_trsv(mr, mi, mv, form, s["bj_in"], iters, om, baj=kind.startswith("baj"),
+                                  csr=kind.endswith("csr"))
+            t[f"{name}_{kind}_{iters}_{om}"] = out
+    np.savez_compressed(os.path.join(HERE, "trsv.npz"), **t)
+
+
 def main(big: bool):
     O.build()
     ref = O.Ref("golden")
@@ -168,6 +204,7 @@ def main(big: bool):
         s[key + "_lower"], s[key + "_upper"] = lo, up
     s["hpcg8_rptr"], s["hpcg8_idx"], s["hpcg8_scaled"], s["bj_in"] = hr, hi, hvs, x16
     np.savez_compressed(os.path.join(HERE, "setup.npz"), **s)
+    trsv_fixtures(ref, s)
 
     # ---- SpMV kinds --------------------------------------------------------
     m = {}

@@ -1,0 +1,133 @@
+"""Jacobi-iteration triangular solves on the GPU (f3r_trsv, and the
+PRECOND_ILU0_JACOBI / PRECOND_ILU0_BAJ solver options) against the oracle
+(bit for bit in the product arithmetic) and the reference's own solves
+(tests/golden/trsv.npz, recorded from trsv/jacobi.hpp and trsv/baj.hpp)."""
+import numpy as np
+import pytest
+import torch
+
+import f3r_b200 as F
+from oracle import oracle as O
+from test_oracle_pins import load, same, trsv_matrices
+
+pytestmark = pytest.mark.gpu
+
+FORMS = {O.FORM_LOWER: F.TRSV_LOWER, O.FORM_LOWER_D: F.TRSV_LOWER_D, O.FORM_D_UPPER: F.TRSV_D_UPPER}
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    return F.Context(0)
+
+
+def gpu_trsv(ctx, csr, form, x, iters, omega=1.0, baj=False):
+    T = F.Trsv(ctx, F.HostMatrix.from_csr(*csr), FORMS[form], F.TRSV_BAJ if baj else F.TRSV_JACOBI, iters, omega)
+    xin = torch.from_numpy(np.ascontiguousarray(x, np.float16)).cuda()
+    out = torch.empty_like(xin)
+    torch.cuda.synchronize()
+    T.solve(xin, out)
+    ctx.synchronize()
+    return out.cpu().numpy()
+
+
+@pytest.mark.parametrize("name", ["L", "Tl", "U"])
+def test_jacobi_bit_exact_against_oracle(ctx, name):
+    x = load("setup.npz")["bj_in"]
+    r, i, v, form = trsv_matrices()[name]
+    M = O.Mat.from_csr(r, i, v)
+    for iters in (0, 1, 2, 5):
+        for om in (1.0, 0.7, 1.3):
+            got = gpu_trsv(ctx, (r, i, v), form, x, iters, om)
+            want = O.jacobi_trsv(M, form, x, iters, om, False, O.ARITH_PRODUCT)
+            assert same(got, want), (name, iters, om)
+
+
+def test_jacobi_close_to_reference(ctx):
+    x = load("setup.npz")["bj_in"]
+    mats = trsv_matrices()
+    for key, want in load("trsv.npz").items():
+        if key.startswith("tl_"):
+            continue
+        name, kind, iters, om = key.split("_")
+        if not kind.startswith("jac"):
+            continue
+        r, i, v, form = mats[name]
+        got = gpu_trsv(ctx, (r, i, v), form, x, int(iters), float(om)).astype(np.float64)
+        w = want.astype(np.float64)
+        assert np.max(np.abs(got - w)) <= 4 * 2.0 ** -11 * np.max(np.abs(w)), key
+
+
+@pytest.mark.parametrize("name", ["L", "Tl", "U"])
+def test_baj_first_step_and_fixed_point(ctx, name):
+    """BAJ's sweeps race by design; its first step (the diagonal scaling) and
+    its fixed point (reached once the sweeps outnumber the dependency chain)
+    are deterministic and equal the oracle's, bit for bit, and the fixed
+    point is the one synchronous Jacobi reaches too"""
+    x = load("setup.npz")["bj_in"]
+    r, i, v, form = trsv_matrices()[name]
+    M = O.Mat.from_csr(r, i, v)
+    got1 = gpu_trsv(ctx, (r, i, v), form, x, 1, baj=True)
+    assert same(got1, O.jacobi_trsv(M, form, x, 1, 1.0, True, O.ARITH_PRODUCT))
+    n = len(r) - 1
+    fixed = O.jacobi_trsv(M, form, x, n + 1, 1.0, True, O.ARITH_PRODUCT)
+    got = gpu_trsv(ctx, (r, i, v), form, x, n + 1, baj=True)
+    assert same(got, fixed)
+    # synchronous Jacobi (omega 1) lands on the same values (up to the sign of zeros)
+    jac = gpu_trsv(ctx, (r, i, v), form, x, n, 1.0)
+    assert np.array_equal(jac.astype(np.float32), fixed.astype(np.float32))
+
+
+def test_jacobi_global_ilu_64(ctx):
+    """one global ILU(0) (a single block) of the 64^3 27-point matrix:
+    262144 rows, three sweeps per factor, bit exact"""
+    r, i, v = O.stencil27(64, 64, 64, variant=1)
+    v = O.scaling(r, i, v)
+    L, U = O.ilu0_bj(O.Mat.from_csr(r, i, v), 1)
+    x = np.random.default_rng(5).standard_normal(len(r) - 1).astype(np.float16)
+    for Mt, form in ((L, O.FORM_LOWER), (U, O.FORM_D_UPPER)):
+        csr = Mt.csr()
+        got = gpu_trsv(ctx, csr, form, x, 3, 0.9)
+        assert same(got, O.jacobi_trsv(Mt, form, x, 3, 0.9, False, O.ARITH_PRODUCT))
+
+
+def test_trsv_rejects_bad_input(ctx):
+    r, i, v, form = trsv_matrices()["U"]
+    with pytest.raises(F.F3RError, match="diagonal"):  # an upper factor read as lower
+        F.Trsv(ctx, F.HostMatrix.from_csr(r, i, v), F.TRSV_LOWER)
+    with pytest.raises(F.F3RError):
+        F.Trsv(ctx, F.HostMatrix.from_csr(r, i, v), F.TRSV_D_UPPER, F.TRSV_BAJ, 0)
+    with pytest.raises(F.F3RError):
+        F.Trsv(ctx, F.HostMatrix.from_csr(r, i, v), F.TRSV_D_UPPER, F.TRSV_JACOBI, 2, 2.5)
+    T = F.Trsv(ctx, F.HostMatrix.from_csr(r, i, v), F.TRSV_D_UPPER)
+    x = torch.zeros(len(r) - 1, dtype=torch.float16, device="cuda")
+    with pytest.raises(F.F3RError, match="alias"):
+        T.solve(x, x)
+
+
+def _system(variant, nx, seed=0):
+    r, i, v = O.stencil27(nx, nx, nx, variant=variant)
+    v = O.scaling(r, i, v)
+    xs = np.random.default_rng(seed).uniform(-1, 1, len(r) - 1)
+    b = O.spmv(r, i, v, xs, O.DT_F64, O.DT_F64, O.DT_F64)
+    return r, i, v, b
+
+
+@pytest.mark.parametrize("blocks,iters,omega", [(16, 2, 1.0), (1, 3, 1.0), (1, 2, 0.8)])
+def test_solver_with_jacobi_ilu(ctx, blocks, iters, omega):
+    r, i, v, b = _system(2, 24)
+    kw = dict(m2=4, m3=2, m4=1, c=8)
+    o = O.f3r_solve(O.Mat.from_csr(r, i, v), *O.ilu0_bj(O.Mat.from_csr(r, i, v), blocks), b,
+                    O.params(precond=O.PRECOND_ILU0_JACOBI, tol=1e-10, trsv_iters=iters, trsv_omega=omega, **kw))
+    S = F.Solver(ctx, F.HostMatrix.from_csr(r, i, v), rel_tol=1e-10, precond=F.PRECOND_ILU0_JACOBI,
+                 ilu_blocks=blocks, trsv_iters=iters, trsv_omega=omega, **kw)
+    res = S.solve(b, np.zeros(len(b)))
+    assert res.is_solved and res.expl_rel_res < 1e-10
+    assert o["solved"] and abs(res.res_iter - o["iters"]) <= 1, (res.res_iter, o["iters"])
+
+
+def test_solver_with_baj_ilu(ctx):
+    r, i, v, b = _system(2, 24, 1)
+    S = F.Solver(ctx, F.HostMatrix.from_csr(r, i, v), rel_tol=1e-10, precond=F.PRECOND_ILU0_BAJ, ilu_blocks=1,
+                 trsv_iters=3, m2=4, m3=2, m4=1, c=8)
+    res = S.solve(b, np.zeros(len(b)))
+    assert res.is_solved and res.expl_rel_res < 1e-10

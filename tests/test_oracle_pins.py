@@ -177,3 +177,41 @@ def test_oracle_variants_match_reference(name):
     ref_iters = int(sol[name + "_iters"])
     assert o["solved"]
     assert abs(o["iters"] - ref_iters) <= max(1, round(0.1 * ref_iters)), (o["iters"], ref_iters)
+
+
+def trsv_matrices():
+    """(name -> (rptr, idx, val, form)) of the Jacobi-trsv fixtures"""
+    s = load("setup.npz")
+    t = load("trsv.npz")
+    key = "hpcg8_ilu16"
+    return {"L": (s[key + "_L_rptr"], s[key + "_L_idx"], s[key + "_L_val"], O.FORM_LOWER),
+            "Tl": (t["tl_rptr"], t["tl_idx"], t["tl_val"], O.FORM_LOWER_D),
+            "U": (s[key + "_U_rptr"], s[key + "_U_idx"], s[key + "_U_val"], O.FORM_D_UPPER)}
+
+
+def test_jacobi_trsv_matches_reference():
+    """Jacobi / BAJ triangular solves (trsv/jacobi.hpp, trsv/baj.hpp), SELL and
+    CSR forms, all three triangle forms: the oracle's reference-arithmetic
+    mode reproduces the reference bit for bit; the product arithmetic (fp32
+    accumulation) stays within a few fp16 ulps (of the vector's largest
+    entry) of it"""
+    s = load("setup.npz")
+    t = load("trsv.npz")
+    x = s["bj_in"]
+    mats = trsv_matrices()
+    seen = 0
+    for key, want in t.items():
+        if key.startswith("tl_"):
+            continue
+        name, kind, iters, om = key.split("_")
+        r, i, v, form = mats[name]
+        M = O.Mat.from_csr(r, i, v)
+        baj = kind.startswith("baj")
+        got = O.jacobi_trsv(M, form, x, int(iters), float(om), baj, O.ARITH_REF)
+        assert same(got, want), key
+        prod = O.jacobi_trsv(M, form, x, int(iters), float(om), baj, O.ARITH_PRODUCT).astype(np.float64)
+        w = want.astype(np.float64)
+        # cancellation makes a per-entry relative bound meaningless: compare on the vector's scale
+        assert np.max(np.abs(prod - w)) <= 4 * 2.0 ** -11 * np.max(np.abs(w)), key
+        seen += 1
+    assert seen == 32
