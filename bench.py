@@ -16,6 +16,12 @@ N GPUs every rank solves its own system (replicas, no collective on the data
 path); the time is the max over ranks.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Other preconditioners on the same workload (not the headline configuration):
+  --precond ilu-bj      block-Jacobi ILU(0), exact level-scheduled solves
+  --precond ilu-jacobi  ILU(0) solved by --trsv-iters Jacobi sweeps (trsv/jacobi.hpp)
+  --precond ilu-baj     ILU(0) solved by --trsv-iters BAJ sweeps (trsv/baj.hpp)
+with --ilu-blocks B (112, the reference's; 1 = one global ILU(0)).
 """
 from __future__ import annotations
 
@@ -43,6 +49,10 @@ METRIC = "time to 1e-10 FP64 relative residual, plain F3R (fp64/fp32/fp16 nested
 WORKLOAD = "F3R-SDAINV-SELL32s256 stencil27-halfspace beta0.5 192^3 (n=7077888, nnz=189119224), tol 1e-10"
 
 
+PRECONDS = {"sdainv": 0, "ilu-bj": 1, "ilu-jacobi": 2, "ilu-baj": 3}
+PRECOND_DESC = "SDAINV(tol=0.1, acc=1.0)"
+
+
 def set_size(nx):
     global NX, WORKLOAD
     NX = nx
@@ -50,10 +60,24 @@ def set_size(nx):
     WORKLOAD = (f"F3R-SDAINV-SELL32s256 stencil27-halfspace beta0.5 {nx}^3 (n={nx ** 3}, nnz={nnz}), tol 1e-10")
 
 
+def set_precond(name, blocks, iters):
+    """Switches the innermost preconditioner (PARAMS, workload name, config)."""
+    global WORKLOAD, PRECOND_DESC
+    if name == "sdainv":
+        return
+    PARAMS.update(precond=PRECONDS[name], ilu_blocks=blocks, trsv_iters=iters)
+    label = {"ilu-bj": f"BJILU0x{blocks}-levels", "ilu-jacobi": f"ILU0x{blocks}-jacobi{iters}",
+             "ilu-baj": f"ILU0x{blocks}-baj{iters}"}[name]
+    WORKLOAD = WORKLOAD.replace("F3R-SDAINV", "F3R-" + label)
+    PRECOND_DESC = {"ilu-bj": f"block-Jacobi ILU(0), {blocks} blocks, exact level-scheduled triangular solves",
+                    "ilu-jacobi": f"ILU(0) over {blocks} block(s), {iters} Jacobi sweeps per triangular solve",
+                    "ilu-baj": f"ILU(0) over {blocks} block(s), BAJ max_iter {iters}"}[name]
+
+
 def config_dict(extra=None):
     d = {"workload": WORKLOAD, "grid": [NX, NX, NX], "n": NX ** 3, "nnz": 27 * NX ** 3 - 54 * NX ** 2 + 36 * NX - 8, "sell": {"C": 32, "sigma": SIGMA},
          "f3r": {"m_outer": 100, "m2": 8, "m3": 4, "m4": 2, "c": 64, "restarts": 20},
-         "precond": "SDAINV(tol=0.1, acc=1.0)", "rhs": "b = A x*, x* ~ U(-1,1) mt19937_64(rank)",
+         "precond": PRECOND_DESC, "rhs": "b = A x*, x* ~ U(-1,1) mt19937_64(rank)",
          "l2": "inputs larger than L2 (fp16+fp32+fp64 matrix copies 4.6 GB, vectors 12 GB)",
          "parallelism": "replicas (one independent system per GPU)"}
     if extra:
@@ -200,12 +224,16 @@ def cpu_baseline(A, b, iters_gpu, sample_steps=2):
     except FileNotFoundError as e:
         return {"value": None, "unit": "ms", "cores": cores, "kind": "reference", "sample": f"unavailable: {e}"}
     rptr, idx, val = A.arrays()
-    r = ref.f3r_solve(0, rptr, idx, val, b, tol=TOL, stop_after=sample_steps)
+    # the reference's SDAINV + SELL-32 method (f3r-gpu.cpp) or, for the ILU
+    # preconditioners, its block-Jacobi ILU(0) + CSR method (f3r.cpp)
+    config = 0 if PARAMS.get("precond", 0) == 0 else 1
+    r = ref.f3r_solve(config, rptr, idx, val, b, tol=TOL, stop_after=sample_steps)
     per_step = r["time_s"] / max(r["iters"], 1)
     return {"value": round(per_step * iters_gpu * 1e3, 1), "unit": "ms", "cores": int(os.environ["OMP_NUM_THREADS"]),
             "kind": "reference",
-            "sample": f"{r['iters']} outer FGMRES steps of the same 192^3 solve on the host "
-                      f"({ref.name}, SELL-32 + SDAINV, fp16 as _Float16; {per_step:.2f} s/step), "
+            "sample": f"{r['iters']} outer FGMRES steps of the same {NX}^3 solve on the host "
+                      f"({ref.name}, {'SELL-32 + SDAINV' if config == 0 else 'CSR + BJ-ILU(0) x112'}, fp16 as "
+                      f"_Float16; {per_step:.2f} s/step), "
                       f"scaled by the GPU solve's {iters_gpu} outer steps"}
 
 
@@ -353,8 +381,14 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--nx", type=int, default=NX, help="grid edge (the benchmark is 192; smaller sizes for profiling)")
+    ap.add_argument("--precond", default="sdainv", choices=sorted(PRECONDS),
+                    help="innermost preconditioner of our arm (the headline is sdainv)")
+    ap.add_argument("--ilu-blocks", type=int, default=112)
+    ap.add_argument("--trsv-iters", type=int, default=2)
     args = ap.parse_args()
     set_size(args.nx)
+    if args.impl == "ours":
+        set_precond(args.precond, args.ilu_blocks, args.trsv_iters)
     if args.impl == "reference":
         run_reference(args)
     else:
