@@ -38,7 +38,8 @@ class Params(C.Structure):
                 ("sdainv_tol", C.c_double), ("acc", C.c_double), ("sell_c", C.c_int32), ("sell_sigma", C.c_int32),
                 ("rel_tol", C.c_double), ("half_scale_log2", C.c_int32), ("use_graphs", C.c_int32),
                 ("sell_index16", C.c_int32), ("static_weight", C.c_double), ("trsv_iters", C.c_int32),
-                ("reserved0", C.c_int32), ("trsv_omega", C.c_double), ("reserved", C.c_int32 * 8)]
+                ("reserved0", C.c_int32), ("trsv_omega", C.c_double), ("inner_sstep", C.c_int32),
+                ("reserved1", C.c_int32), ("reserved", C.c_int32 * 8)]
 
 
 class Result(C.Structure):

@@ -362,24 +362,46 @@ struct Solver {
   // the fp16 level uses the separate pass; the fp32 level keeps the fusion
   // for up to 4 dots (its product streams more bytes per slice and hides the
   // epilogue: 244 us fused against 228 + ~20 us) and separates wider ones.
+  // H(j, 0..nv-1) = <w, V(k)>, one vectorised pass
+  void dots(const float *w, const Cols<float> &Vc, int nv, float *hcol) {
+    const int gv = C().ew_grid(cdiv(n, 4));
+    if (nv <= 4)
+      launch_k(C(), k_multidot_f32<4, 8>, gv, 256, 0, C().stream, w, Vc, nv, (int64_t)n, C().gred(), hcol);
+    else if (nv <= 8)
+      launch_k(C(), k_multidot_f32<8, 8>, gv, 256, 0, C().stream, w, Vc, nv, (int64_t)n, C().gred(), hcol);
+    else
+      launch_k(C(), k_multidot_chunked<float, 8>, C().ew_grid(n), 256, 0, C().stream, w, Vc, nv, (int64_t)n,
+               C().gred(), hcol);
+  }
+
   template <typename V>
   Status spmv_dots(const V *vals, const float *z, float *w, const Cols<float> &Vc, int nv, float *hcol) {
     if (sizeof(V) == 2 || nv > 4) {
       F3R_TRY(launch_sell(C(), vals, A.view(), z, EpiStore<float>{w, nullptr}));
-      const int gv = C().ew_grid(cdiv(n, 4));
-      if (nv <= 4)
-        launch_k(C(), k_multidot_f32<4, 8>, gv, 256, 0, C().stream, (const float *)w, Vc, nv, (int64_t)n, C().gred(),
-                 hcol);
-      else if (nv <= 8)
-        launch_k(C(), k_multidot_f32<8, 8>, gv, 256, 0, C().stream, (const float *)w, Vc, nv, (int64_t)n, C().gred(),
-                 hcol);
-      else
-        launch_k(C(), k_multidot_chunked<float, 8>, C().ew_grid(n), 256, 0, C().stream, (const float *)w, Vc, nv,
-                 (int64_t)n, C().gred(), hcol);
+      dots(w, Vc, nv, hcol);
       return F3R_SUCCESS;
     }
     if (nv <= 4) return launch_sell(C(), vals, A.view(), z, EpiStoreDots<4>{w, Vc, nv, C().gred(), hcol});
     return launch_sell(C(), vals, A.view(), z, EpiStoreDots<8>{w, Vc, nv, C().gred(), hcol});
+  }
+
+  // sFGMRES's second and third loops (gmres2.hpp:181-193): classical
+  // Gram-Schmidt of the stored raw vectors W(1..m) against the basis built so
+  // far, with each Givens rotation fused into its step as in FGMRES (the
+  // rotation of column j needs only column j).  The next step reads V(j+1)
+  // through the dots and the update, so it is normalised explicitly here.
+  Status sstep_orthogonalise(Level<float> &L, float *const *Vp, const Cols<float> &V) {
+    const int64_t N = n;
+    const int gv = C().ew_grid(cdiv(N, 4));
+    for (int j = 0; j < L.m; j++) {
+      float *w = Vp[j + 1];
+      dots(w, V, j + 1, L.H + (size_t)j * (L.m + 1));
+      GivensCtl<float> g{L.H, L.cs, L.sn, L.e, L.y, L.inv, nullptr, L.m + 1, j, j == L.m - 1, C().err};
+      launch_k(C(), k_cgs_update<float, 8>, gv, 256, 0, C().stream, w, V, j + 1, N, C().gred(), g);
+      if (j + 1 < L.m) launch_k(C(), k_scale<float>, gv, kEwThreads, 0, C().stream, w, (const float *)L.inv, N);
+    }
+    CUDA_TRY(cudaGetLastError());
+    return F3R_SUCCESS;
   }
 
   // ---- level 3: FGMRES<float>(A16, R, m3), input V2 column, output Z2 col ----
@@ -397,13 +419,23 @@ struct Solver {
     for (int k = 1; k <= L.m; k++) Vp[k] = L.V + (size_t)(k - 1) * ldn;
     for (int k = 0; k <= L.m; k++) V.p[k] = Vp[k];
     for (int k = 0; k < L.m; k++) Zc.p[k] = L.Z + (size_t)k * ldn;
-    for (int j = 0; j < L.m; j++) {
-      float *zj = L.Z + (size_t)j * ldn;
-      float *w = Vp[j + 1];
-      F3R_TRY(rich_apply(Vp[j], zj, j == 0 ? L.e : nullptr, j == 0 ? in_inv : L.inv));
-      F3R_TRY(spmv_dots(A.v16, zj, w, V, j + 1, L.H + (size_t)j * (L.m + 1)));
-      GivensCtl<float> g{L.H, L.cs, L.sn, L.e, L.y, L.inv, nullptr, L.m + 1, j, j == L.m - 1, C().err};
-      launch_k(C(), k_cgs_update<float, 8>, gv, 256, 0, C().stream, w, V, j + 1, N, C().gred(), g);
+    if (p.inner_sstep & 2) {
+      // sFGMRES (gmres2.hpp:176-180): W(j+1) = A16 R W(j) on the raw vectors
+      for (int j = 0; j < L.m; j++) {
+        float *zj = L.Z + (size_t)j * ldn;
+        F3R_TRY(rich_apply(Vp[j], zj, j == 0 ? L.e : nullptr, j == 0 ? in_inv : nullptr));
+        F3R_TRY(launch_sell(C(), A.v16, A.view(), (const float *)zj, EpiStore<float>{Vp[j + 1], nullptr}));
+      }
+      F3R_TRY(sstep_orthogonalise(L, Vp, V));
+    } else {
+      for (int j = 0; j < L.m; j++) {
+        float *zj = L.Z + (size_t)j * ldn;
+        float *w = Vp[j + 1];
+        F3R_TRY(rich_apply(Vp[j], zj, j == 0 ? L.e : nullptr, j == 0 ? in_inv : L.inv));
+        F3R_TRY(spmv_dots(A.v16, zj, w, V, j + 1, L.H + (size_t)j * (L.m + 1)));
+        GivensCtl<float> g{L.H, L.cs, L.sn, L.e, L.y, L.inv, nullptr, L.m + 1, j, j == L.m - 1, C().err};
+        launch_k(C(), k_cgs_update<float, 8>, gv, 256, 0, C().stream, w, V, j + 1, N, C().gred(), g);
+      }
     }
     launch_k(C(), k_zy<float, float, false>, gv, kEwThreads, 0, C().stream, Zc, L.y, L.m, out, nullptr, N);
     CUDA_TRY(cudaGetLastError());
@@ -422,14 +454,25 @@ struct Solver {
     // normalises the outer basis vector in place (its 1/h is L1.inv) and casts it
     launch_k(C(), k_level2_enter, gv, kEwThreads, 0, C().stream, (double *const *)in_slot, (const double *)L1.inv, L.V,
              L.e, N);
-    for (int j = 0; j < L.m; j++) {
-      float *zj = L.Z + (size_t)j * ldn;
-      float *w = Vp[j + 1];
-      if (p.m3 > 0) F3R_TRY(level3(Vp[j], zj, j == 0 ? nullptr : L.inv));
-      else F3R_TRY(rich_apply(Vp[j], zj, nullptr, j == 0 ? nullptr : L.inv));  // depth 2: R directly
-      F3R_TRY(spmv_dots(A.v32, zj, w, V, j + 1, L.H + (size_t)j * (L.m + 1)));
-      GivensCtl<float> g{L.H, L.cs, L.sn, L.e, L.y, L.inv, nullptr, L.m + 1, j, j == L.m - 1, C().err};
-      launch_k(C(), k_cgs_update<float, 8>, gv, 256, 0, C().stream, w, V, j + 1, N, C().gred(), g);
+    if (p.inner_sstep & 1) {
+      // sFGMRES (gmres2.hpp:176-180): W(j+1) = A32 M W(j) on the raw vectors
+      for (int j = 0; j < L.m; j++) {
+        float *zj = L.Z + (size_t)j * ldn;
+        if (p.m3 > 0) F3R_TRY(level3(Vp[j], zj, nullptr));
+        else F3R_TRY(rich_apply(Vp[j], zj, nullptr, nullptr));
+        F3R_TRY(launch_sell(C(), A.v32, A.view(), (const float *)zj, EpiStore<float>{Vp[j + 1], nullptr}));
+      }
+      F3R_TRY(sstep_orthogonalise(L, Vp, V));
+    } else {
+      for (int j = 0; j < L.m; j++) {
+        float *zj = L.Z + (size_t)j * ldn;
+        float *w = Vp[j + 1];
+        if (p.m3 > 0) F3R_TRY(level3(Vp[j], zj, j == 0 ? nullptr : L.inv));
+        else F3R_TRY(rich_apply(Vp[j], zj, nullptr, j == 0 ? nullptr : L.inv));  // depth 2: R directly
+        F3R_TRY(spmv_dots(A.v32, zj, w, V, j + 1, L.H + (size_t)j * (L.m + 1)));
+        GivensCtl<float> g{L.H, L.cs, L.sn, L.e, L.y, L.inv, nullptr, L.m + 1, j, j == L.m - 1, C().err};
+        launch_k(C(), k_cgs_update<float, 8>, gv, 256, 0, C().stream, w, V, j + 1, N, C().gred(), g);
+      }
     }
     launch_k(C(), k_zy<float, double, false>, gv, kEwThreads, 0, C().stream, Zc, L.y, L.m, nullptr, out_slot, N);
     CUDA_TRY(cudaGetLastError());
@@ -637,6 +680,7 @@ static Status make_solver(f3r_context *ctx, const f3r_csr *a, const f3r_params *
   if (p.precond < F3R_PRECOND_SDAINV || p.precond > F3R_PRECOND_ILU0_BAJ)
     return fail(F3R_ERROR_INVALID_VALUE, "unknown preconditioner");
   if (p.half_scale_log2 < 0 || p.half_scale_log2 > 20) return fail(F3R_ERROR_INVALID_VALUE, "half_scale_log2 in [0, 20]");
+  if (p.inner_sstep < 0 || p.inner_sstep > 3) return fail(F3R_ERROR_INVALID_VALUE, "inner_sstep is a 2-bit mask");
   auto s = std::make_unique<Solver>();
   s->ctx = ctx;
   s->p = p;

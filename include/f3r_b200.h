@@ -99,6 +99,10 @@ typedef struct f3r_params {
                               ILU0_BAJ: BAJ max_iter (the first is the diagonal scaling) */
   int32_t reserved0;
   double trsv_omega;       /* ILU0_JACOBI: damping omega in (0, 2], 1.0 */
+  int32_t inner_sstep;     /* bit 0: level 2, bit 1: level 3 run as sFGMRES (solver/gmres2.hpp:
+                              137-221): all m preconditioner + matrix applications first, on the
+                              raw vectors W(j+1) = A M W(j), then the Gram-Schmidt steps.  0 */
+  int32_t reserved1;
   int32_t reserved[8];
 } f3r_params;
 

@@ -701,6 +701,8 @@ typedef struct {
   int32_t trsv_iters;  /* PRECOND_ILU0_JACOBI / _BAJ: sweeps (max_ier / max_iter) */
   int32_t pad_;
   double trsv_omega;   /* PRECOND_ILU0_JACOBI: damping omega */
+  int32_t sstep;       /* bit 0: level 2 is sFGMRES, bit 1: level 3 (solver/gmres2.hpp:137-221) */
+  int32_t pad2_;
 } or_f3r_params;
 
 #define MAXM4 16
@@ -876,17 +878,25 @@ static void level_inner(f3r_ctx *c, int level, const float *in, float *out) {
   e[0] = 1.0f;
   memcpy(V, in, sizeof(float) * (size_t)n);
   const or_mat *A = c->A;
+  /* sFGMRES (gmres2.hpp:176-192): every M and A application first, on the
+   * raw vectors W(j+1) = A M W(j); then the same classical Gram-Schmidt,
+   * norms and Givens rotations over the stored W, step by step.           */
+  const int sstep = (c->p.sstep >> (level - 2)) & 1;
+  for (int pass = 0; pass < (sstep ? 2 : 1); pass++)
   for (int j = 0; j < m; j++) {
     float *vj = V + (size_t)n * j, *zj = Z + (size_t)n * j, *w = V + (size_t)n * (j + 1);
-    if (level == 2 && c->p.m3 > 0) level_inner(c, 3, vj, zj);
-    else level4(c, vj, zj);  /* level 3, or level 2 of the depth-2 form (work/src/depth.cpp:157-162) */
-    for (int32_t i = 0; i < n; i++) {
-      float t = 0.0f;
-      if (level == 2)
-        for (int32_t q = A->rptr[i]; q < A->rptr[i + 1]; q++) t = fmaf(c->v32[q], zj[A->idx[q]], t);
-      else
-        for (int32_t q = A->rptr[i]; q < A->rptr[i + 1]; q++) t = fmaf((float)c->v16[q], zj[A->idx[q]], t);
-      w[i] = t;
+    if (!sstep || pass == 0) {
+      if (level == 2 && c->p.m3 > 0) level_inner(c, 3, vj, zj);
+      else level4(c, vj, zj);  /* level 3, or level 2 of the depth-2 form (work/src/depth.cpp:157-162) */
+      for (int32_t i = 0; i < n; i++) {
+        float t = 0.0f;
+        if (level == 2)
+          for (int32_t q = A->rptr[i]; q < A->rptr[i + 1]; q++) t = fmaf(c->v32[q], zj[A->idx[q]], t);
+        else
+          for (int32_t q = A->rptr[i]; q < A->rptr[i + 1]; q++) t = fmaf((float)c->v16[q], zj[A->idx[q]], t);
+        w[i] = t;
+      }
+      if (sstep) continue;
     }
     float *Hj = H + (size_t)(m + 1) * j;
     for (int k = 0; k <= j; k++) Hj[k] = dotf(n, w, V + (size_t)n * k);

@@ -94,13 +94,14 @@ class F3RParams(C.Structure):
     _fields_ = [("m1", C.c_int32), ("restarts", C.c_int32), ("m2", C.c_int32), ("m3", C.c_int32),
                 ("m4", C.c_int32), ("c", C.c_int32), ("precond", C.c_int32), ("arith", C.c_int32),
                 ("half_scale_log2", C.c_int32), ("tol", C.c_double), ("static_weight", C.c_double),
-                ("trsv_iters", C.c_int32), ("pad_", C.c_int32), ("trsv_omega", C.c_double)]
+                ("trsv_iters", C.c_int32), ("pad_", C.c_int32), ("trsv_omega", C.c_double),
+                ("sstep", C.c_int32), ("pad2_", C.c_int32)]
 
 
 def params(m1=100, restarts=20, m2=8, m3=4, m4=2, c=64, precond=PRECOND_SDAINV, arith=ARITH_PRODUCT,
-           half_scale_log2=0, tol=1e-10, static_weight=0.0, trsv_iters=3, trsv_omega=1.0) -> F3RParams:
+           half_scale_log2=0, tol=1e-10, static_weight=0.0, trsv_iters=2, trsv_omega=1.0, sstep=0) -> F3RParams:
     return F3RParams(m1, restarts, m2, m3, m4, c, precond, arith, half_scale_log2, tol, static_weight, trsv_iters,
-                     0, trsv_omega)
+                     0, trsv_omega, sstep, 0)
 
 
 class Mat:
@@ -452,5 +453,29 @@ class Ref:
         nh = self.L.ref_f3r_solve(config, n, len(idx), rptr, idx, np.ascontiguousarray(val, np.float64),
                                   np.ascontiguousarray(b, np.float64), x, m2, m3, m4, c, restarts, tol, acc,
                                   sdainv_tol, blocks, out, hist, hist_cap, stop_after, weight)
+        return dict(x=x, time_s=out[0], iters=int(out[1]), impl_res=out[2], expl_res=out[3],
+                    solved=bool(out[4]), hist=hist[:min(nh, hist_cap)].copy())
+
+    def f3r_solve_sstep(self, mask, rptr, idx, val, b, m2=8, m3=4, m4=2, c=64, restarts=20, tol=1e-10, acc=1.0,
+                        sdainv_tol=0.1, hist_cap=4096):
+        """the SDAINV + SELL-32 F3R solve with sFGMRES (gmres2.hpp:137-221) at
+        level 2 (mask bit 0) and / or level 3 (mask bit 1)"""
+        if getattr(self, "S", None) is None:
+            path = os.path.join(REF_DIR, "libf3r_ref_sstep.so")
+            if not os.path.exists(path):
+                raise FileNotFoundError(f"{path} missing: run `make -C oracle ref` where the reference tree exists")
+            self.S = C.CDLL(path)
+            self.S.ref_f3r_solve_sstep.restype = C.c_int
+            self.S.ref_f3r_solve_sstep.argtypes = [C.c_int, C.c_int32, C.c_int32, _i32p, _i32p, _f64p, _f64p, _f64p,
+                                                   C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
+                                                   C.c_double, C.c_double, _f64p, _f64p, C.c_int]
+        n = len(rptr) - 1
+        x = np.zeros(n)
+        out = np.zeros(5)
+        hist = np.zeros(hist_cap)
+        nh = self.S.ref_f3r_solve_sstep(mask, n, len(idx), np.ascontiguousarray(rptr, np.int32),
+                                        np.ascontiguousarray(idx, np.int32), np.ascontiguousarray(val, np.float64),
+                                        np.ascontiguousarray(b, np.float64), x, m2, m3, m4, c, restarts, tol, acc,
+                                        sdainv_tol, out, hist, hist_cap)
         return dict(x=x, time_s=out[0], iters=int(out[1]), impl_res=out[2], expl_res=out[3],
                     solved=bool(out[4]), hist=hist[:min(nh, hist_cap)].copy())

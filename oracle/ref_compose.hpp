@@ -95,9 +95,13 @@ solve_out run_solve(const Solver &solver, const Mat &A, const double *b_in, doub
 }
 
 // f3r-gpu.cpp:210-265 on the host.  `data` is the already scaled matrix.
-inline solve_out f3r_sdainv_sell(const CSR<double, host> &data, const double *b, double *x,
-                                 int m2, int m3, int m4, int c, int restarts, double tol,
-                                 double acc, double sdainv_tol, double *hist, int hist_cap) {
+// Level2 / Level3 are the solver class templates of the two inner levels
+// (FGMRES as the driver; sFGMRES of solver/gmres2.hpp:137-221 in
+// ref_sstep.cpp).
+template <template <class, class> class Level2, template <class, class> class Level3>
+solve_out f3r_sdainv_sell_t(const CSR<double, host> &data, const double *b, double *x,
+                            int m2, int m3, int m4, int c, int restarts, double tol,
+                            double acc, double sdainv_tol, double *hist, int hist_cap) {
   using tag = host;
   const int32_t n = data.nrows();
   auto A = SELL<32, double, tag>(data);
@@ -154,8 +158,8 @@ inline solve_out f3r_sdainv_sell(const CSR<double, host> &data, const double *b,
     out.copy(hout);
   });
   auto A32 = SELL<32, float, tag>(A);
-  auto MM = FGMRES<float, tag>(A16, R, {m3, false});
-  auto MMM = FGMRES<float, tag>(A32, MM, {m2, false});
+  auto MM = Level3<float, tag>(A16, R, {m3, false});
+  auto MMM = Level2<float, tag>(A32, MM, {m2, false});
   auto inner = Solver<tag>(FGMRES<double, tag>(A, MMM, {100, true}));
   auto solver = Restarted<double, tag>(A, inner, {restarts});
   cnt = c;
@@ -164,6 +168,13 @@ inline solve_out f3r_sdainv_sell(const CSR<double, host> &data, const double *b,
     ome[k] = 1.0;
   }
   return run_solve(solver, A, b, x, n, tol, hist, hist_cap);
+}
+
+inline solve_out f3r_sdainv_sell(const CSR<double, host> &data, const double *b, double *x,
+                                 int m2, int m3, int m4, int c, int restarts, double tol,
+                                 double acc, double sdainv_tol, double *hist, int hist_cap) {
+  return f3r_sdainv_sell_t<FGMRES, FGMRES>(data, b, x, m2, m3, m4, c, restarts, tol, acc, sdainv_tol,
+                                           hist, hist_cap);
 }
 
 // f3r.cpp:195-248 (HALF) on the host: CSR, block-Jacobi ILU(0).

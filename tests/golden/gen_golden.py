@@ -235,6 +235,8 @@ def main(big: bool):
                 "depth3_hpgmp16": dict(config=3, m2=8, m3=8, m4=1, weight=1.0),
                 "depth2_hpgmp16": dict(config=4, m2=64, m3=0, m4=1, weight=1.0)}
     cases += [(k, v["config"], (16, 16, 16, 1), 6 + j) for j, (k, v) in enumerate(variants.items())]
+    # sFGMRES inner levels (solver/gmres2.hpp:137-221): mask bit 0 level 2, bit 1 level 3
+    cases += [(f"sstep{mask}_hpgmp16", 10 + mask, (16, 16, 16, 1), 12 + mask) for mask in (1, 2, 3)]
     for name, config, spec, seed in cases:
         if spec is None:
             D = F.diffusion7(12, 12, 12, 1.5, 3.0, 9)
@@ -245,8 +247,11 @@ def main(big: bool):
         xs, b = rhs_for(ref, rr, ii, vv, seed)
         blocks = 16 if spec is not None and spec[0] == 16 else 112
         extra = {k: v for k, v in variants.get(name, {}).items() if k != "config"}
-        res = ref.f3r_solve(config, rr, ii, vv, b, tol=1e-10, c=64 if spec and spec[0] >= 64 else 8,
-                            blocks=blocks, **extra)
+        if config >= 10:
+            res = ref.f3r_solve_sstep(config - 10, rr, ii, vv, b, tol=1e-10, c=8)
+        else:
+            res = ref.f3r_solve(config, rr, ii, vv, b, tol=1e-10, c=64 if spec and spec[0] >= 64 else 8,
+                                blocks=blocks, **extra)
         print(name, res["iters"], res["impl_res"], res["expl_res"], res["time_s"])
         sol[name + "_iters"] = np.array(res["iters"])
         sol[name + "_hist"] = res["hist"]

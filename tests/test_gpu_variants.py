@@ -42,3 +42,36 @@ def test_static_weight_never_updates(ctx):
         S.solve(b, x)
         xs.append(x)
     assert np.array_equal(xs[0], xs[1])
+
+
+@pytest.mark.parametrize("name", ["sstep1_hpgmp16", "sstep2_hpgmp16", "sstep3_hpgmp16"])
+def test_sstep_matches_reference_and_oracle(ctx, name):
+    """sFGMRES inner levels (solver/gmres2.hpp:137-221) against the
+    reference's solve and the oracle's product arithmetic"""
+    from oracle import oracle as O
+    from test_oracle_pins import SSTEP
+    r, i, v, b, xs, sol = golden_system(name)
+    S = F.Solver(ctx, F.HostMatrix.from_csr(r, i, v), rel_tol=1e-10, c=8, inner_sstep=SSTEP[name])
+    res = S.solve(b, np.zeros(len(b)))
+    A = O.Mat.from_csr(r, i, v)
+    Z, W = O.sdainv(A)
+    o = O.f3r_solve(A, W, Z, b, O.params(c=8, tol=1e-10, sstep=SSTEP[name]))
+    ref_iters = int(sol[name + "_iters"])
+    assert res.is_solved and res.expl_rel_res < 1e-10
+    assert abs(res.res_iter - ref_iters) <= 1, (res.res_iter, ref_iters)
+    assert abs(res.res_iter - o["iters"]) <= 1, (res.res_iter, o["iters"])
+
+
+def test_sstep_large_level_and_graphs(ctx):
+    """both levels s-step with a wide level 2 (16 raw vectors, chunked dots),
+    graphs on and off give the same iterate"""
+    A = F.stencil27(20, 20, 20, 2, 0.5).scale()
+    b = A.spmv(F.random_uniform(3, -1, 1, A.shape[0]))
+    xs = []
+    for graphs in (1, 0):
+        S = F.Solver(ctx, A, rel_tol=1e-10, c=8, m2=16, m3=3, inner_sstep=3, use_graphs=graphs)
+        x = np.zeros(len(b))
+        res = S.solve(b, x)
+        assert res.is_solved and res.expl_rel_res < 1e-10
+        xs.append(x)
+    assert np.array_equal(xs[0], xs[1])

@@ -122,6 +122,7 @@ def _problem(name):
         return D.arrays()
     spec = {"sdainv_hpgmp16": (16, 16, 16, 1), "sdainv_half16": (16, 16, 16, 2), "bjilu_hpcg16": (16, 16, 16, 0),
             "static_hpgmp16": (16, 16, 16, 1), "depth3_hpgmp16": (16, 16, 16, 1), "depth2_hpgmp16": (16, 16, 16, 1),
+            "sstep1_hpgmp16": (16, 16, 16, 1), "sstep2_hpgmp16": (16, 16, 16, 1), "sstep3_hpgmp16": (16, 16, 16, 1),
             "bjilu_hpcg64": (64, 64, 64, 0), "sdainv_half192": (192, 192, 192, 2)}[name]
     return O.stencil27(*spec[:3], variant=spec[3], beta=0.5)
 
@@ -215,3 +216,20 @@ def test_jacobi_trsv_matches_reference():
         assert np.max(np.abs(prod - w)) <= 4 * 2.0 ** -11 * np.max(np.abs(w)), key
         seen += 1
     assert seen == 32
+
+
+# sFGMRES at the inner levels (solver/gmres2.hpp:137-221): mask bit 0 level 2, bit 1 level 3
+SSTEP = {"sstep1_hpgmp16": 1, "sstep2_hpgmp16": 2, "sstep3_hpgmp16": 3}
+
+
+@pytest.mark.parametrize("name", sorted(SSTEP))
+def test_oracle_sstep_matches_reference(name):
+    """the raw-vector s-step basis is sensitive to rounding: +-1 outer step"""
+    r, i, v, b, xs, sol = golden_system(name)
+    A = O.Mat.from_csr(r, i, v)
+    Z, W = O.sdainv(A)
+    ref_iters = int(sol[name + "_iters"])
+    for arith in (O.ARITH_PRODUCT, O.ARITH_REF):
+        o = O.f3r_solve(A, W, Z, b, O.params(c=8, tol=1e-10, sstep=SSTEP[name], arith=arith))
+        assert o["solved"]
+        assert abs(o["iters"] - ref_iters) <= 1, (name, arith, o["iters"], ref_iters)
