@@ -217,8 +217,9 @@ class Sell:
     """Device SELL-32-sigma matrix (f3r_sell) -- CoefficientMatrix::operate /
     compute_residual on device tensors."""
 
-    def __init__(self, ctx: Context, A: HostMatrix, sigma: int = 1, dtypes=(F64, F32, F16), index16: bool = False):
-        mask = _capi.SELL_INDEX16 if index16 else 0
+    def __init__(self, ctx: Context, A: HostMatrix, sigma: int = 1, dtypes=(F64, F32, F16), index16: bool = False,
+                 aligned: bool = False):
+        mask = (_capi.SELL_INDEX16 if index16 else 0) | (_capi.SELL_ALIGNED if aligned else 0)
         for d in dtypes:
             mask |= 1 << d
         h = C.c_void_p()

@@ -75,55 +75,69 @@ struct DeviceSell {
   int32_t n = 0, ncols = 0, nslices = 0, max_width = 0, sigma = 1;
   int64_t nnz = 0, nnz_pad = 0;
   int32_t *col = nullptr, *sptr = nullptr, *perm = nullptr, *cbase = nullptr, *cbptr = nullptr;
+  int32_t *xoff = nullptr;  // mixed aligned form: per slice, -1 or the explicit indices' offset
   uint16_t *dcol = nullptr;
   double *v64 = nullptr;
   float *v32 = nullptr;
   __half *v16 = nullptr;
   int dtypes = 0;
-  int index_bits() const { return dcol ? 16 : 32; }
-  DevSell view() const { return DevSell{col, dcol, cbase, cbptr, sptr, perm, n, nslices}; }
+  // 32, 16, or 0 (offset-aligned slices, mixed with explicit ones or not)
+  int index_bits() const { return (xoff || (cbase && !dcol)) ? 0 : dcol ? 16 : 32; }
+  DevSell view() const { return DevSell{col, dcol, cbase, cbptr, xoff, sptr, perm, n, ncols, nslices}; }
   void release() {
     cudaFree(col); cudaFree(sptr); cudaFree(perm); cudaFree(cbase); cudaFree(cbptr); cudaFree(dcol);
+    cudaFree(xoff);
     cbptr = nullptr;
+    xoff = nullptr;
     cudaFree(v64); cudaFree(v32); cudaFree(v16);
     col = sptr = perm = cbase = nullptr; dcol = nullptr; v64 = nullptr; v32 = nullptr; v16 = nullptr;
   }
 };
 
 
-// Raises the kernel's dynamic shared memory limit once per device.  Called
-// before any graph capture for every instantiation the solver uses.
+template <typename V, typename X, typename Epi, typename CI>
+inline Status sell_attr_one() {
+  using Cfg = SellCfg<V, CI>;
+  CUDA_TRY(cudaFuncSetAttribute(k_sell_cfg<V, X, Epi, Cfg::WARPS, Cfg::STAGES, Cfg::KC, CI>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sell_smem_bytes<V, CI>()));
+  return F3R_SUCCESS;
+}
+
+// Raises the kernel's dynamic shared memory limit once per device, for every
+// index form.  Called before any graph capture for every instantiation the
+// solver uses.
 template <typename V, typename X, typename Epi>
 inline Status sell_attr(Context &c) {
   static int attr_done[64] = {0};
   if (!attr_done[c.device & 63]) {
-    CUDA_TRY(cudaFuncSetAttribute(
-        k_sell_cfg<V, X, Epi, SellCfg<V>::WARPS, SellCfg<V>::STAGES, SellCfg<V>::KC, int32_t>,
-        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sell_smem_bytes<V, int32_t>()));
-    CUDA_TRY(cudaFuncSetAttribute(
-        k_sell_cfg<V, X, Epi, SellCfg<V>::WARPS, SellCfg<V>::STAGES, SellCfg<V>::KC, uint16_t>,
-        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sell_smem_bytes<V, uint16_t>()));
+    F3R_TRY((sell_attr_one<V, X, Epi, int32_t>()));
+    F3R_TRY((sell_attr_one<V, X, Epi, uint16_t>()));
+    F3R_TRY((sell_attr_one<V, X, Epi, AlignedIdx>()));
+    F3R_TRY((sell_attr_one<V, X, Epi, AllAlignedIdx>()));
     attr_done[c.device & 63] = 1;
   }
   return F3R_SUCCESS;
 }
 
+template <typename V, typename X, typename Epi, typename CI>
+inline void launch_sell_one(Context &c, const V *val, const DevSell &A, const X *x, const Epi &epi) {
+  using Cfg = SellCfg<V, CI>;
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(cdiv(A.nslices, Cfg::WARPS), c.sm_count));
+  launch_k(c, k_sell_cfg<V, X, Epi, Cfg::WARPS, Cfg::STAGES, Cfg::KC, CI>, grid, Cfg::WARPS * 32,
+           sell_smem_bytes<V, CI>(), c.stream, val, A, x, epi, c.err);
+}
+
 template <typename V, typename X, typename Epi>
 inline Status launch_sell(Context &c, const V *val, const DevSell &A, const X *x, const Epi &epi) {
   if (A.nslices == 0) return F3R_SUCCESS;
-  constexpr int WARPS = SellCfg<V>::WARPS;
   F3R_TRY((sell_attr<V, X, Epi>(c)));
-  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(cdiv(A.nslices, WARPS), c.sm_count));
-  if (A.dcol)
-    launch_k(c, k_sell_cfg<V, X, Epi, WARPS, SellCfg<V>::STAGES, SellCfg<V>::KC, uint16_t>, grid, WARPS * 32,
-             sell_smem_bytes<V, uint16_t>(), c.stream, val, A, x, epi, c.err);
-  else
-    launch_k(c, k_sell_cfg<V, X, Epi, WARPS, SellCfg<V>::STAGES, SellCfg<V>::KC, int32_t>, grid, WARPS * 32,
-             sell_smem_bytes<V, int32_t>(), c.stream, val, A, x, epi, c.err);
+  if (A.xoff) launch_sell_one<V, X, Epi, AlignedIdx>(c, val, A, x, epi);
+  else if (A.cbase && !A.dcol) launch_sell_one<V, X, Epi, AllAlignedIdx>(c, val, A, x, epi);
+  else if (A.dcol) launch_sell_one<V, X, Epi, uint16_t>(c, val, A, x, epi);
+  else launch_sell_one<V, X, Epi, int32_t>(c, val, A, x, epi);
   CUDA_TRY(cudaGetLastError());
   return F3R_SUCCESS;
 }
-
 
 // ---------------------------------------------------------------------------
 // SELL-32 construction on the host (solver.cu)
@@ -135,7 +149,9 @@ struct SellHost {
   std::vector<double> val;
   std::vector<uint16_t> dcol;            // 16-bit offsets (when they fit)
   std::vector<int32_t> cbase;            // base of each slice column, slice s from cbptr[s]
-  std::vector<int32_t> cbptr;            // nslices + 1, multiples of 4
+  std::vector<int32_t> cbptr;            // nslices + 1, multiples of 4 (aligned forms: bit 0 = clamp)
+  std::vector<int32_t> xoff;             // mixed aligned form: per slice, -1 or explicit offset
+  bool aligned_all = false;              // fully aligned form (no explicit index at all)
 };
 
 // Rows sorted by decreasing length in windows of sigma (renumber: columns
@@ -144,6 +160,11 @@ Status build_sell(const f3r_csr &a, int32_t sigma, bool renumber, SellHost &s,
                   const std::vector<int32_t> *given_perm = nullptr);
 // 16-bit column offsets when every slice column fits a 65536 window
 bool compress_index16(SellHost &s);
+// Re-lays a packed SellHost out offset-aligned: the fully aligned form when
+// every slice's rows share their column offsets (offset set at most 5/4 of
+// the slice's width), otherwise the mixed form.  Returns the fraction of
+// slices aligned, or -1 when the padded matrix would exceed 2^31 entries.
+double align_offsets(const f3r_csr &a, bool renumber, SellHost &s);
 // Uploads the value copies selected by dtype_mask (bit 1 << f3r_dtype).
 Status upload_sell(Context &c, const SellHost &h, int dtype_mask, bool scatter_perm, DeviceSell &d);
 

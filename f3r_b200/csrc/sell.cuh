@@ -24,58 +24,135 @@
 // dot-product work.
 #pragma once
 
+#include <type_traits>
+
 #include "device.cuh"
 
 namespace f3r {
 
-// Column indices come in one of two forms:
+// Column indices come in one of four forms:
 //  * col:   int32 per entry;
 //  * dcol + cbase: a uint16 offset per entry from an int32 base per slice
 //    column, used when every slice column's indices fit in a 65536 window --
 //    2 + 4/32 bytes per entry instead of 4.  The bases of slice s start at
 //    cbptr[s], a multiple of 4, so a chunk's bases are one 16-byte aligned
 //    bulk copy like its values and offsets.
+//  * offset-aligned: in a slice whose rows share a small set of column
+//    offsets d = column - row (a stencil, a banded or block-structured
+//    matrix), slice column k holds every row's entry at offset D_k, so its
+//    column is cbase[k] + lane with cbase[k] = first row + D_k; rows without
+//    that offset hold a zero there.  Such a slice stores no index at all,
+//    4/32 bytes per entry.  In the mixed form (xoff set) a slice that does
+//    not fit, or whose columns base + lane would leave [0, ncols), keeps
+//    explicit int32 indices in col from entry xoff[s] (xoff[s] < 0 marks an
+//    aligned slice); chunks of kAlignedChunk columns.
+//  * fully aligned (cbase set, no xoff, no dcol): every slice is aligned,
+//    chunks of kAllAlignedChunk columns.  Bit 0 of cbptr[s] flags a slice
+//    whose columns base + lane can leave [0, ncols) -- only zero entries of
+//    the matrix's first and last rows do -- and the kernel clamps those.
+//  In both aligned forms the values of a chunk are stored lane-major (a lane's
+//  values contiguous) and slice widths are padded to a multiple of 4, so a
+//  lane reads 4 values with one vector load; explicit indices stay
+//  column-major (entry (k, lane) at k * 32 + lane of the slice).
 struct DevSell {
-  const int32_t *col;     // (sptr[nslices]) * 32, or nullptr
+  const int32_t *col;     // explicit indices (packed layout, or the mixed form's explicit slices)
   const uint16_t *dcol;   // (sptr[nslices]) * 32, or nullptr
-  const int32_t *cbase;   // cbptr[nslices] (+ padding), with dcol
-  const int32_t *cbptr;   // nslices + 1, with dcol
+  const int32_t *cbase;   // per slice column: 16-bit bases, or aligned bases
+  const int32_t *cbptr;   // nslices + 1 (aligned forms: slice s's bases start at cbptr[s] & ~3)
+  const int32_t *xoff;    // nslices, mixed aligned form only
   const int32_t *sptr;    // nslices + 1, in units of 32 entries
   const int32_t *perm;    // storage row -> output row, or nullptr (identity)
   int32_t n;              // rows (outputs written only for storage rows < n)
+  int32_t ncols;
   int32_t nslices;
 };
 
-// Launch shape per value type: WARPS warps per CTA, STAGES buffers per warp,
-// KC columns per chunk.  One CTA per SM (the rings take most of the 227 KB).
-// Chosen by a sweep on the 192^3 27-point matrix (n = 7.08M, nnz = 189M):
-// fp16 values x fp32 vector 24/2/16 -> 187 us (6.5 TB/s), versus 8/4/32 ->
-// 345 us; the bound is how many slices are being consumed at once, not how
-// many bytes are in flight.
-template <typename V> struct SellCfg;
-template <> struct SellCfg<__half> { static constexpr int WARPS = 24, STAGES = 2, KC = 16; };
-template <> struct SellCfg<float> { static constexpr int WARPS = 24, STAGES = 2, KC = 16; };
-template <> struct SellCfg<double> { static constexpr int WARPS = 16, STAGES = 2, KC = 16; };
+// Index form of a kernel instantiation.
+struct AlignedIdx {};     // mixed offset-aligned / explicit slices
+struct AllAlignedIdx {};  // every slice offset-aligned
+template <typename CI> struct IdxForm {
+  static constexpr int mode = 0;                // explicit int32
+  static constexpr uint32_t bytes = 4;          // stored index bytes per entry in a stage
+};
+template <> struct IdxForm<uint16_t> {
+  static constexpr int mode = 1;
+  static constexpr uint32_t bytes = 2;
+};
+template <> struct IdxForm<AlignedIdx> {
+  static constexpr int mode = 2;
+  static constexpr uint32_t bytes = 4;          // room for an explicit slice's chunk
+};
+template <> struct IdxForm<AllAlignedIdx> {
+  static constexpr int mode = 3;
+  static constexpr uint32_t bytes = 0;          // no index in a stage
+};
+// Chunk widths of the aligned forms' lane-major value layouts (the builder
+// and the kernel's KC must agree).
+constexpr int kAlignedChunk = 16;
+constexpr int kAllAlignedChunk = 32;
+
+// 4 consecutive values of one lane (aligned forms), one or two vector loads
+template <typename V> struct Vec4Load;
+template <> struct Vec4Load<__half> {
+  static __device__ __forceinline__ void ld(const __half *p, __half (&o)[4]) {
+    const uint2 u = *reinterpret_cast<const uint2 *>(p);
+    const __half2 a = *reinterpret_cast<const __half2 *>(&u.x), b = *reinterpret_cast<const __half2 *>(&u.y);
+    o[0] = __low2half(a); o[1] = __high2half(a); o[2] = __low2half(b); o[3] = __high2half(b);
+  }
+};
+template <> struct Vec4Load<float> {
+  static __device__ __forceinline__ void ld(const float *p, float (&o)[4]) {
+    const float4 u = *reinterpret_cast<const float4 *>(p);
+    o[0] = u.x; o[1] = u.y; o[2] = u.z; o[3] = u.w;
+  }
+};
+template <> struct Vec4Load<double> {
+  static __device__ __forceinline__ void ld(const double *p, double (&o)[4]) {
+    const double2 a = *reinterpret_cast<const double2 *>(p), b = *reinterpret_cast<const double2 *>(p + 2);
+    o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
+  }
+};
+
+// Launch shape per value type and index form: WARPS warps per CTA, STAGES
+// buffers per warp, KC columns per chunk; one CTA per SM.  Chosen by sweeps
+// (f3r_sell_tune) on the 192^3 27-point matrix (n = 7.08M, nnz = 189M).  The
+// packed forms are bound by the bytes in flight per SM; the fully aligned
+// form streams 2 bytes per fp16 entry and is bound by registers: a 32-column
+// chunk worked in two halves fits 80 registers at 24 warps.
+template <typename V, typename CI = int32_t> struct SellCfg;
+template <typename CI> struct SellCfg<__half, CI> { static constexpr int WARPS = 24, STAGES = 2, KC = 16; };
+template <typename CI> struct SellCfg<float, CI> { static constexpr int WARPS = 24, STAGES = 2, KC = 16; };
+template <typename CI> struct SellCfg<double, CI> { static constexpr int WARPS = 16, STAGES = 2, KC = 16; };
+template <> struct SellCfg<__half, AllAlignedIdx> { static constexpr int WARPS = 24, STAGES = 2, KC = 32; };
+template <> struct SellCfg<float, AllAlignedIdx> { static constexpr int WARPS = 24, STAGES = 2, KC = 32; };
+template <> struct SellCfg<double, AllAlignedIdx> { static constexpr int WARPS = 12, STAGES = 2, KC = 32; };
 
 template <typename V, typename CI, int WARPS, int STAGES, int KC>
 constexpr size_t sell_smem_bytes_cfg() {
-  return (size_t)WARPS * STAGES * ((size_t)KC * 32 * (sizeof(V) + sizeof(CI)) + (sizeof(CI) == 2 ? KC * 4 : 0)) +
+  return (size_t)WARPS * STAGES *
+             ((size_t)KC * 32 * (sizeof(V) + IdxForm<CI>::bytes) + (IdxForm<CI>::mode != 0 ? KC * 4 : 0)) +
          (size_t)WARPS * STAGES * sizeof(uint64_t);
 }
 template <typename V, typename CI>
 constexpr size_t sell_smem_bytes() {
-  return sell_smem_bytes_cfg<V, CI, SellCfg<V>::WARPS, SellCfg<V>::STAGES, SellCfg<V>::KC>();
+  return sell_smem_bytes_cfg<V, CI, SellCfg<V, CI>::WARPS, SellCfg<V, CI>::STAGES, SellCfg<V, CI>::KC>();
 }
 
-// CI: the stored index type, int32_t (col) or uint16_t (dcol + cbase).
+// CI: the index form -- int32_t (col), uint16_t (dcol + cbase), AlignedIdx
+// (cbase for aligned slices, col from xoff for the others) or AllAlignedIdx.
 template <typename V, typename X, typename Epi, int WARPS, int STAGES, int KC, typename CI = int32_t>
 __global__ void __launch_bounds__(WARPS * 32, 1)
     k_sell_cfg(const V *__restrict__ val, DevSell A, const X *__restrict__ x, Epi epi, int *err) {
   using Acc = typename acc_of<V>::type;
-  constexpr bool C16 = sizeof(CI) == 2;
+  constexpr int MODE = IdxForm<CI>::mode;
+  constexpr bool C16 = MODE == 1;
+  using SI = typename std::conditional<C16, uint16_t, int32_t>::type;  // stored index type
   static_assert(KC % 4 == 0, "chunk width must keep the bases 16-byte aligned");
-  constexpr uint32_t VB = KC * 32 * sizeof(V), CB = KC * 32 * sizeof(CI), BB = C16 ? KC * 4 : 0, SB = VB + CB + BB;
-  const CI *cidx = C16 ? reinterpret_cast<const CI *>(A.dcol) : reinterpret_cast<const CI *>(A.col);
+  static_assert(MODE != 2 || KC == kAlignedChunk, "aligned layout is built for kAlignedChunk columns");
+  static_assert(MODE != 3 || KC == kAllAlignedChunk, "fully aligned layout is built for kAllAlignedChunk columns");
+  constexpr uint32_t VB = KC * 32 * sizeof(V), CB = KC * 32 * IdxForm<CI>::bytes, BB = MODE != 0 ? KC * 4 : 0,
+                     SB = VB + CB + BB;
+  const SI *cidx = C16 ? reinterpret_cast<const SI *>(A.dcol) : reinterpret_cast<const SI *>(A.col);
   extern __shared__ __align__(128) unsigned char smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   unsigned char *buf = smem + (size_t)warp * STAGES * SB;
@@ -89,34 +166,52 @@ __global__ void __launch_bounds__(WARPS * 32, 1)
   const uint64_t pol = l2_evict_first_policy();
   const int TW = gridDim.x * WARPS;
 
-  // fetch cursor (warp-uniform)
+  // fetch cursor (warp-uniform); the current slice's metadata is read once,
+  // when the cursor enters it
   int fs = blockIdx.x * WARPS + warp, fk = 0, fst = 0, inflight = 0;
+  int fs0 = 0, fw = 0, fxo = 0, fcb = 0;
   auto fetch = [&]() {
     while (inflight < STAGES && fs < A.nslices) {
-      const int s0 = A.sptr[fs], w = A.sptr[fs + 1] - s0;
-      if (w == 0) {
+      if (fk == 0) {
+        fs0 = A.sptr[fs];
+        fw = A.sptr[fs + 1] - fs0;
+        if (MODE == 2) fxo = A.xoff[fs];
+        if (MODE != 0) fcb = A.cbptr[fs] & ~3;
+      }
+      if (fw == 0) {
         fs += TW;
         fk = 0;
         continue;
       }
-      const int kc = min(KC, w - fk);
+      const int kc = min(KC, fw - fk);
       if (lane == 0) {
-        const size_t off = ((size_t)s0 + fk) * 32;
+        const size_t off = ((size_t)fs0 + fk) * 32;
+        // aligned forms: a slice carries either bases (aligned) or explicit indices
+        const bool want_idx = MODE == 0 || MODE == 1 || (MODE == 2 && fxo >= 0);
+        const bool want_base = MODE == 1 || MODE == 3 || (MODE == 2 && fxo < 0);
+        const SI *isrc = MODE == 2 ? cidx + (size_t)fxo + (size_t)fk * 32 : cidx + off;
         fence_proxy_async_smem();
-        const uint32_t bb = C16 ? (uint32_t)((kc + 3) & ~3) * 4u : 0u;
-        mbar_arrive_expect_tx(&bars[fst], (uint32_t)kc * 32u * (uint32_t)(sizeof(V) + sizeof(CI)) + bb);
+        const uint32_t ib = want_idx ? (uint32_t)kc * 32u * (uint32_t)sizeof(SI) : 0u;
+        const uint32_t bb = want_base ? (uint32_t)((kc + 3) & ~3) * 4u : 0u;
+        mbar_arrive_expect_tx(&bars[fst], (uint32_t)kc * 32u * (uint32_t)sizeof(V) + ib + bb);
         bulk_g2s(buf + (size_t)fst * SB, val + off, (uint32_t)kc * 32u * (uint32_t)sizeof(V), &bars[fst], pol);
-        bulk_g2s(buf + (size_t)fst * SB + VB, cidx + off, (uint32_t)kc * 32u * (uint32_t)sizeof(CI), &bars[fst], pol);
-        if (C16) bulk_g2s(buf + (size_t)fst * SB + VB + CB, A.cbase + A.cbptr[fs] + fk, bb, &bars[fst], pol);
+        if (want_idx) bulk_g2s(buf + (size_t)fst * SB + VB, isrc, ib, &bars[fst], pol);
+        if (want_base) bulk_g2s(buf + (size_t)fst * SB + VB + CB, A.cbase + fcb + fk, bb, &bars[fst], pol);
       }
       fst = (fst + 1 == STAGES) ? 0 : fst + 1;
       inflight++;
       fk += kc;
-      if (fk >= w) {
+      if (fk >= fw) {
         fk = 0;
         fs += TW;
       }
     }
+  };
+  // hands the stage just read back to the copy engine and refills the ring
+  auto release = [&]() {
+    __syncwarp();
+    inflight--;
+    fetch();
   };
   fetch();
 
@@ -128,8 +223,15 @@ __global__ void __launch_bounds__(WARPS * 32, 1)
   bool ok = true;
   Acc acc = 0;
   typename Epi::Pre pre{};
+  int w = 0;                  // width of the consumer's current slice
+  bool aligned = MODE == 3;   // the current slice is offset-aligned
+  bool clampc = false;        // fully aligned form: its columns need clamping
   while (cs < A.nslices) {
-    const int s0 = A.sptr[cs], w = A.sptr[cs + 1] - s0;
+    if (ck == 0) {
+      w = A.sptr[cs + 1] - A.sptr[cs];
+      if (MODE == 2) aligned = A.xoff[cs] < 0;
+      if (MODE == 3) clampc = (A.cbptr[cs] & 1) != 0;
+    }
     const int64_t r = (int64_t)cs * 32 + lane;
     const bool live = r < A.n;
     if (w == 0) {
@@ -148,30 +250,115 @@ __global__ void __launch_bounds__(WARPS * 32, 1)
     }
     phase ^= 1u << cst;
     const V *sv = reinterpret_cast<const V *>(buf + (size_t)cst * SB);
-    const CI *sc = reinterpret_cast<const CI *>(buf + (size_t)cst * SB + VB);
+    const SI *sc = reinterpret_cast<const SI *>(buf + (size_t)cst * SB + VB);
     const int32_t *sb = reinterpret_cast<const int32_t *>(buf + (size_t)cst * SB + VB + CB);
-    V vv[KC];
-    int32_t cc[KC];
+    cst = (cst + 1 == STAGES) ? 0 : cst + 1;  // the stage read now is released below
+    const bool full = kc == KC;
+    if constexpr (MODE == 3) {
+      // fully aligned: the 32-column chunk is worked in two halves of 16 (so
+      // 24 warps fit at 80 registers); the stage is released after the last
+      // half's loads
+      const V *lv = sv + lane * kc;  // lane-major values (kc a multiple of 4)
+      const int hlast = (kc - 1) >> 4;
 #pragma unroll
-    for (int k = 0; k < KC; k++) {
-      if (k < kc) {
-        vv[k] = sv[k * 32 + lane];
-        if (C16) cc[k] = sb[k] + (int32_t)sc[k * 32 + lane];
-        else cc[k] = (int32_t)sc[k * 32 + lane];
+      for (int h = 0; h < KC / 16; h++) {
+        if (h <= hlast) {
+          V vh[16];
+          int32_t ch[16];
+#pragma unroll
+          for (int g = 0; g < 4; g++) {
+            const int k0 = h * 16 + g * 4;
+            if (full || k0 < kc) {
+              V t[4];
+              Vec4Load<V>::ld(lv + k0, t);
+              const int4 q = *reinterpret_cast<const int4 *>(sb + k0);
+              int32_t b[4] = {q.x + lane, q.y + lane, q.z + lane, q.w + lane};
+              if (clampc) {
+#pragma unroll
+                for (int e = 0; e < 4; e++) b[e] = min(max(b[e], 0), A.ncols - 1);
+              }
+#pragma unroll
+              for (int e = 0; e < 4; e++) {
+                vh[g * 4 + e] = t[e];
+                ch[g * 4 + e] = b[e];
+              }
+            }
+          }
+          if (h == hlast) release();
+          Acc xh[16];
+#pragma unroll
+          for (int g = 0; g < 4; g++)
+            if (full || h * 16 + g * 4 < kc) {
+#pragma unroll
+              for (int e = 0; e < 4; e++) xh[g * 4 + e] = to_acc<Acc>(__ldg(x + ch[g * 4 + e]));
+            }
+#pragma unroll
+          for (int g = 0; g < 4; g++)
+            if (full || h * 16 + g * 4 < kc) {
+#pragma unroll
+              for (int e = 0; e < 4; e++) acc = fmaT(to_acc<Acc>(vh[g * 4 + e]), xh[g * 4 + e], acc);
+            }
+        }
+      }
+    } else {
+      V vv[KC];
+      int32_t cc[KC];
+      // Straight-line code for a full chunk, guarded code for a slice's last,
+      // partial one; the index form is decided once per chunk, outside the
+      // unrolled loops (warp-uniform).
+      if constexpr (MODE == 2) {
+        const V *lv = sv + lane * kc;  // lane-major values (kc a multiple of 4)
+#pragma unroll
+        for (int g = 0; g < KC / 4; g++) {
+          if (full || g * 4 < kc) {
+            V t[4];
+            Vec4Load<V>::ld(lv + g * 4, t);
+            int32_t b[4];
+            if (aligned) {
+              const int4 q = *reinterpret_cast<const int4 *>(sb + g * 4);
+              b[0] = q.x + lane; b[1] = q.y + lane; b[2] = q.z + lane; b[3] = q.w + lane;
+            } else {
+#pragma unroll
+              for (int e = 0; e < 4; e++) b[e] = (int32_t)sc[(g * 4 + e) * 32 + lane];
+            }
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+              vv[g * 4 + e] = t[e];
+              cc[g * 4 + e] = b[e];
+            }
+          }
+        }
+      } else if (full) {
+#pragma unroll
+        for (int k = 0; k < KC; k++) {
+          vv[k] = sv[k * 32 + lane];
+          cc[k] = C16 ? sb[k] + (int32_t)sc[k * 32 + lane] : (int32_t)sc[k * 32 + lane];
+        }
+      } else {
+#pragma unroll
+        for (int k = 0; k < KC; k++)
+          if (k < kc) {
+            vv[k] = sv[k * 32 + lane];
+            cc[k] = C16 ? sb[k] + (int32_t)sc[k * 32 + lane] : (int32_t)sc[k * 32 + lane];
+          }
+      }
+      // the chunk is in registers: release the stage to the copy engine now
+      release();
+      Acc xv[KC];
+      if (full) {
+#pragma unroll
+        for (int k = 0; k < KC; k++) xv[k] = to_acc<Acc>(__ldg(x + cc[k]));
+#pragma unroll
+        for (int k = 0; k < KC; k++) acc = fmaT(to_acc<Acc>(vv[k]), xv[k], acc);
+      } else {
+#pragma unroll
+        for (int k = 0; k < KC; k++)
+          if (k < kc) xv[k] = to_acc<Acc>(__ldg(x + cc[k]));
+#pragma unroll
+        for (int k = 0; k < KC; k++)
+          if (k < kc) acc = fmaT(to_acc<Acc>(vv[k]), xv[k], acc);
       }
     }
-    // the chunk is in registers: release the stage to the copy engine now
-    __syncwarp();
-    inflight--;
-    cst = (cst + 1 == STAGES) ? 0 : cst + 1;
-    fetch();
-    Acc xv[KC];
-#pragma unroll
-    for (int k = 0; k < KC; k++)
-      if (k < kc) xv[k] = to_acc<Acc>(__ldg(x + cc[k]));
-#pragma unroll
-    for (int k = 0; k < KC; k++)
-      if (k < kc) acc = fmaT(to_acc<Acc>(vv[k]), xv[k], acc);
     ck += kc;
     if (ck >= w) {
       if (live) epi.row(r, acc, pre, dots);

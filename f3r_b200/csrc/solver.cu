@@ -72,6 +72,128 @@ bool compress_index16(SellHost &s) {
 
 // renumber = true builds P A P^T (columns mapped to storage order) for the
 // solver's permuted system; false keeps original columns and scatters rows.
+// Offset-aligned slices.  Per slice, D = the sorted set of offsets
+// column - row over its rows (storage numbering).  A slice can be aligned when
+// |D| is at most 5/4 of its packed width: slice column k then becomes offset
+// D_k for every row (a zero where the row has no entry at that offset) and no
+// index is stored.  Within a row the entries stay in increasing column order,
+// so the product's sums are unchanged (a zero entry adds 0 x to the chain).
+//  * Every slice alignable (stencil-like matrices): the fully aligned form,
+//    kAllAlignedChunk-column chunks; a slice whose columns first row + D_k +
+//    lane can leave [0, ncols) is flagged in bit 0 of cbptr and clamped.
+//  * Otherwise the mixed form: slices that are alignable and in range are
+//    aligned, the rest keep explicit indices (compact, from xoff);
+//    kAlignedChunk-column chunks.
+// Slice widths are padded to a multiple of 4 and each chunk stores its values
+// lane-major (a lane's values contiguous), so the kernel reads them with
+// vector loads.
+double align_offsets(const f3r_csr &a, bool renumber, SellHost &s) {
+  const int32_t n = s.n, ns = s.nslices, nc = s.ncols;
+  std::vector<int32_t> iperm;
+  if (renumber) {
+    iperm.resize(n);
+    for (int32_t i = 0; i < n; i++) iperm[s.perm[i]] = i;
+  }
+  auto colof = [&](int32_t q) { return renumber ? iperm[a.idx[q]] : a.idx[q]; };
+  std::vector<std::vector<int32_t>> D(ns);
+  std::vector<char> shape_ok(ns, 1), in_range(ns, 1);
+  int64_t not_ok = 0;
+#pragma omp parallel for schedule(dynamic, 256) reduction(+ : not_ok)
+  for (int32_t sl = 0; sl < ns; sl++) {
+    const int32_t wstd = s.sptr[sl + 1] - s.sptr[sl];
+    if (wstd == 0) continue;
+    std::vector<int32_t> d;
+    d.reserve((size_t)wstd * 2);
+    for (int32_t l = 0; l < 32; l++) {
+      const int64_t r = (int64_t)sl * 32 + l;
+      if (r >= n) break;
+      const int32_t o = s.perm[r];
+      for (int32_t q = a.rptr[o]; q < a.rptr[o + 1]; q++) d.push_back(colof(q) - (int32_t)r);
+    }
+    std::sort(d.begin(), d.end());
+    d.erase(std::unique(d.begin(), d.end()), d.end());
+    const int64_t lo = (int64_t)sl * 32 + d.front(), hi = (int64_t)sl * 32 + d.back() + 31;
+    in_range[sl] = lo >= 0 && hi < nc;
+    shape_ok[sl] = (int64_t)d.size() * 4 <= (int64_t)wstd * 5;
+    if (!shape_ok[sl]) not_ok++;
+    D[sl] = std::move(d);
+  }
+  const bool all = not_ok == 0;
+  const int32_t chunk = all ? kAllAlignedChunk : kAlignedChunk;
+  std::vector<char> al(ns, 0);
+  std::vector<int32_t> width(ns);
+  for (int32_t sl = 0; sl < ns; sl++) {
+    const int32_t wstd = s.sptr[sl + 1] - s.sptr[sl];
+    al[sl] = wstd > 0 && shape_ok[sl] && (all || in_range[sl]);
+    width[sl] = ((al[sl] ? (int32_t)D[sl].size() : wstd) + 3) & ~3;
+  }
+  std::vector<int32_t> sptr(ns + 1, 0), cbptr(ns + 1, 0), xoff(all ? 0 : ns, -1);
+  int64_t nx = 0, na = 0;
+  for (int32_t sl = 0; sl < ns; sl++) {
+    if ((int64_t)sptr[sl] + width[sl] > INT32_MAX / 32) return -1.0;
+    sptr[sl + 1] = sptr[sl] + width[sl];
+    cbptr[sl + 1] = cbptr[sl] + (al[sl] ? width[sl] : 0);
+    if (al[sl]) {
+      na++;
+    } else if (!all) {
+      xoff[sl] = (int32_t)nx;
+      nx += (int64_t)width[sl] * 32;
+    }
+  }
+  const int64_t np = (int64_t)sptr[ns] * 32;
+  std::vector<double> val(np, 0.0);
+  std::vector<int32_t> col(std::max<int64_t>(nx, 1), 0), cbase((size_t)cbptr[ns] + 4, 0);
+#pragma omp parallel for schedule(dynamic, 256)
+  for (int32_t sl = 0; sl < ns; sl++) {
+    const int32_t wp = width[sl];
+    const int64_t nb = (int64_t)sptr[sl] * 32, ob = (int64_t)s.sptr[sl] * 32;
+    // lane-major position of entry (k, lane) inside the slice
+    auto at = [&](int32_t k, int32_t l) {
+      const int32_t k0 = k / chunk * chunk, kw = std::min(chunk, wp - k0);
+      return nb + (int64_t)k0 * 32 + (int64_t)l * kw + (k - k0);
+    };
+    if (al[sl]) {
+      const std::vector<int32_t> &d = D[sl];
+      // padding slots repeat the last offset (their values are zero)
+      for (int32_t k = 0; k < wp; k++) cbase[cbptr[sl] + k] = sl * 32 + d[std::min<size_t>(k, d.size() - 1)];
+      for (int32_t l = 0; l < 32; l++) {
+        const int64_t r = (int64_t)sl * 32 + l;
+        if (r >= n) break;
+        const int32_t o = s.perm[r];
+        for (int32_t q = a.rptr[o]; q < a.rptr[o + 1]; q++) {
+          const int32_t k = (int32_t)(std::lower_bound(d.begin(), d.end(), colof(q) - (int32_t)r) - d.begin());
+          val[at(k, l)] = a.val[q];
+        }
+      }
+    } else if (wp > 0) {
+      const int32_t wstd = s.sptr[sl + 1] - s.sptr[sl];
+      for (int32_t k = 0; k < wp; k++)
+        for (int32_t l = 0; l < 32; l++) {
+          const int32_t ks = std::min(k, wstd - 1);
+          col[xoff[sl] + (int64_t)k * 32 + l] = s.col[ob + (int64_t)ks * 32 + l];
+          if (k < wstd) val[at(k, l)] = s.val[ob + (int64_t)k * 32 + l];
+        }
+    }
+  }
+  // the fully aligned form flags the slices to clamp in bit 0 of cbptr
+  if (all)
+    for (int32_t sl = 0; sl < ns; sl++)
+      if (al[sl] && !in_range[sl]) cbptr[sl] |= 1;
+  int32_t mw = 0;
+  for (int32_t sl = 0; sl < ns; sl++) mw = std::max(mw, width[sl]);
+  s.sptr = std::move(sptr);
+  s.val = std::move(val);
+  s.col = all ? std::vector<int32_t>() : std::move(col);
+  s.cbase = std::move(cbase);
+  s.cbptr = std::move(cbptr);
+  s.xoff = std::move(xoff);
+  s.aligned_all = all;
+  s.dcol.clear();
+  s.nnz_pad = np;
+  s.max_width = mw;
+  return ns ? (double)na / ns : 0.0;
+}
+
 Status build_sell(const f3r_csr &a, int32_t sigma, bool renumber, SellHost &s,
                   const std::vector<int32_t> *given_perm) {
   if (sigma < 1) return fail(F3R_ERROR_INVALID_VALUE, "sigma must be >= 1");
@@ -142,7 +264,19 @@ Status upload_sell(Context &c, const SellHost &h, int dtype_mask, bool scatter_p
   d.n = h.n; d.ncols = h.ncols; d.nslices = h.nslices; d.max_width = h.max_width; d.sigma = h.sigma;
   d.nnz = h.nnz; d.nnz_pad = h.nnz_pad; d.dtypes = dtype_mask;
   const size_t np = (size_t)h.nnz_pad;
-  if (!h.dcol.empty()) {
+  if (!h.xoff.empty() || h.aligned_all) {
+    const size_t nc = h.cbase.size(), nx = h.col.size();
+    F3R_TRY(c.alloc((void **)&d.cbase, nc * 4));
+    F3R_TRY(c.alloc((void **)&d.cbptr, (size_t)(h.nslices + 1) * 4));
+    CUDA_TRY(cudaMemcpyAsync(d.cbase, h.cbase.data(), nc * 4, cudaMemcpyHostToDevice, c.stream));
+    CUDA_TRY(cudaMemcpyAsync(d.cbptr, h.cbptr.data(), (size_t)(h.nslices + 1) * 4, cudaMemcpyHostToDevice, c.stream));
+    if (!h.aligned_all) {  // mixed form: the explicit slices' indices
+      F3R_TRY(c.alloc((void **)&d.col, nx * 4));
+      F3R_TRY(c.alloc((void **)&d.xoff, (size_t)std::max(h.nslices, 1) * 4));
+      CUDA_TRY(cudaMemcpyAsync(d.col, h.col.data(), nx * 4, cudaMemcpyHostToDevice, c.stream));
+      CUDA_TRY(cudaMemcpyAsync(d.xoff, h.xoff.data(), (size_t)h.nslices * 4, cudaMemcpyHostToDevice, c.stream));
+    }
+  } else if (!h.dcol.empty()) {
     const size_t nc = h.cbase.size();
     F3R_TRY(c.alloc((void **)&d.dcol, np * 2));
     F3R_TRY(c.alloc((void **)&d.cbase, nc * 4));
@@ -692,7 +826,11 @@ static Status make_solver(f3r_context *ctx, const f3r_csr *a, const f3r_params *
   SellHost h;
   F3R_TRY(build_sell(*a, p.sell_sigma, true, h));
   const std::vector<int32_t> hperm = h.perm;
-  if (p.sell_index16) compress_index16(h);
+  if (p.sell_align) {
+    if (align_offsets(*a, true, h) < 0) return fail(F3R_ERROR_UNSUPPORTED, "padded matrix exceeds 2^31 entries");
+  } else if (p.sell_index16) {
+    compress_index16(h);
+  }
   F3R_TRY(upload_sell(*ctx, h, (1 << F3R_F64) | (1 << F3R_F32) | (1 << F3R_F16), false, s->A));
   h = SellHost();  // release the host copy (up to several GB)
   s->perm = hperm;
@@ -738,7 +876,10 @@ static Status make_solver(f3r_context *ctx, const f3r_csr *a, const f3r_params *
       f3r_csr wv = Wh->view(), zv = Zh->view();
       F3R_TRY(build_sell(wv, p.sell_sigma, true, hw, &hperm));
       F3R_TRY(build_sell(zv, p.sell_sigma, true, hz, &hperm));
-      if (p.sell_index16) {
+      if (p.sell_align) {
+        if (align_offsets(wv, true, hw) < 0 || align_offsets(zv, true, hz) < 0)
+          return fail(F3R_ERROR_UNSUPPORTED, "padded matrix exceeds 2^31 entries");
+      } else if (p.sell_index16) {
         compress_index16(hw);
         compress_index16(hz);
       }
@@ -986,13 +1127,18 @@ f3r_status f3r_sell_create(f3r_context *ctx, const f3r_csr *a, int32_t slice_hei
                            int32_t dtype_mask, f3r_sell **out) {
   if (!ctx || !out) return fail(F3R_ERROR_INVALID_VALUE, "null argument");
   if (slice_height != 32) return fail(F3R_ERROR_UNSUPPORTED, "only slice height 32 is implemented");
-  if ((dtype_mask & 7) == 0 || (dtype_mask & ~(7 | F3R_SELL_INDEX16)))
-    return fail(F3R_ERROR_INVALID_VALUE, "dtype_mask must select f64/f32/f16 (plus F3R_SELL_INDEX16)");
+  if ((dtype_mask & 7) == 0 || (dtype_mask & ~(7 | F3R_SELL_INDEX16 | F3R_SELL_ALIGNED)))
+    return fail(F3R_ERROR_INVALID_VALUE,
+                "dtype_mask must select f64/f32/f16 (plus F3R_SELL_INDEX16 or F3R_SELL_ALIGNED)");
   F3R_TRY(check_csr(a));
   CUDA_TRY(cudaSetDevice(ctx->device));
   SellHost h;
   F3R_TRY(build_sell(*a, sigma, false, h));
-  if (dtype_mask & F3R_SELL_INDEX16) compress_index16(h);
+  if (dtype_mask & F3R_SELL_ALIGNED) {
+    if (align_offsets(*a, false, h) < 0) return fail(F3R_ERROR_UNSUPPORTED, "padded matrix exceeds 2^31 entries");
+  } else if (dtype_mask & F3R_SELL_INDEX16) {
+    compress_index16(h);
+  }
   auto m = std::make_unique<f3r_sell>();
   m->ctx = ctx;
   Status s = upload_sell(*ctx, h, dtype_mask & 7, true, m->d);

@@ -16,8 +16,8 @@ namespace f3r {
 namespace {
 
 template <typename V, typename X, typename Y, int W, int S, int KC, typename CI>
-void time_shape(Context &c, const DeviceSell &d, const V *val, const X *x, Y *y, int reps,
-                std::vector<f3r_tune_entry> &out) {
+void time_shape_run(Context &c, const DeviceSell &d, const V *val, const X *x, Y *y, int reps,
+                    std::vector<f3r_tune_entry> &out) {
   auto k = k_sell_cfg<V, X, EpiStore<Y>, W, S, KC, CI>;
   const size_t smem = sell_smem_bytes_cfg<V, CI, W, S, KC>();
   int optin = 0;
@@ -45,25 +45,49 @@ void time_shape(Context &c, const DeviceSell &d, const V *val, const X *x, Y *y,
   t.warps = W;
   t.stages = S;
   t.kc = KC;
-  t.index_bits = sizeof(CI) * 8;
-  t.is_default = (W == SellCfg<V>::WARPS && S == SellCfg<V>::STAGES && KC == SellCfg<V>::KC) ? 1 : 0;
+  t.index_bits = IdxForm<CI>::mode >= 2 ? 0 : IdxForm<CI>::mode == 1 ? 16 : 32;
+  t.is_default = (W == SellCfg<V, CI>::WARPS && S == SellCfg<V, CI>::STAGES && KC == SellCfg<V, CI>::KC) ? 1 : 0;
   t.microseconds = ms * 1e3 / reps;
   const double nnz = (double)d.nnz, n = (double)d.n;
   t.gbs_algorithmic = (nnz * (sizeof(V) + 4) + 4 * (n + 1) + n * sizeof(X) + n * sizeof(Y)) / (t.microseconds * 1e3);
   out.push_back(t);
 }
 
+// the aligned forms' value layouts are built for one chunk width each
+template <typename V, typename X, typename Y, int W, int S, int KC, typename CI>
+void time_shape(Context &c, const DeviceSell &d, const V *val, const X *x, Y *y, int reps,
+                std::vector<f3r_tune_entry> &out) {
+  if constexpr ((IdxForm<CI>::mode == 2 && KC != kAlignedChunk) || (IdxForm<CI>::mode == 3 && KC != kAllAlignedChunk))
+    return;
+  else
+    time_shape_run<V, X, Y, W, S, KC, CI>(c, d, val, x, y, reps, out);
+}
+
 template <typename V, typename X, typename Y, typename CI>
 void sweep(Context &c, const DeviceSell &d, const V *val, const X *x, Y *y, int reps, std::vector<f3r_tune_entry> &out) {
-  time_shape<V, X, Y, 24, 2, 16, CI>(c, d, val, x, y, reps, out);
-  time_shape<V, X, Y, 20, 2, 16, CI>(c, d, val, x, y, reps, out);
-  time_shape<V, X, Y, 20, 3, 16, CI>(c, d, val, x, y, reps, out);
-  time_shape<V, X, Y, 16, 2, 16, CI>(c, d, val, x, y, reps, out);
-  time_shape<V, X, Y, 16, 3, 16, CI>(c, d, val, x, y, reps, out);
-  time_shape<V, X, Y, 12, 4, 16, CI>(c, d, val, x, y, reps, out);
-  time_shape<V, X, Y, 32, 2, 8, CI>(c, d, val, x, y, reps, out);
-  time_shape<V, X, Y, 24, 3, 8, CI>(c, d, val, x, y, reps, out);
-  time_shape<V, X, Y, 8, 4, 16, CI>(c, d, val, x, y, reps, out);
+  if constexpr (IdxForm<CI>::mode == 3) {
+    time_shape<V, X, Y, 32, 2, 32, CI>(c, d, val, x, y, reps, out);
+    time_shape<V, X, Y, 24, 4, 32, CI>(c, d, val, x, y, reps, out);
+    time_shape<V, X, Y, 24, 3, 32, CI>(c, d, val, x, y, reps, out);
+    time_shape<V, X, Y, 24, 2, 32, CI>(c, d, val, x, y, reps, out);
+    time_shape<V, X, Y, 20, 2, 32, CI>(c, d, val, x, y, reps, out);
+    time_shape<V, X, Y, 16, 4, 32, CI>(c, d, val, x, y, reps, out);
+    time_shape<V, X, Y, 16, 2, 32, CI>(c, d, val, x, y, reps, out);
+    time_shape<V, X, Y, 12, 3, 32, CI>(c, d, val, x, y, reps, out);
+    time_shape<V, X, Y, 12, 2, 32, CI>(c, d, val, x, y, reps, out);
+    time_shape<V, X, Y, 8, 4, 32, CI>(c, d, val, x, y, reps, out);
+    time_shape<V, X, Y, 8, 2, 32, CI>(c, d, val, x, y, reps, out);
+  } else {
+    time_shape<V, X, Y, 24, 2, 16, CI>(c, d, val, x, y, reps, out);
+    time_shape<V, X, Y, 20, 2, 16, CI>(c, d, val, x, y, reps, out);
+    time_shape<V, X, Y, 20, 3, 16, CI>(c, d, val, x, y, reps, out);
+    time_shape<V, X, Y, 16, 2, 16, CI>(c, d, val, x, y, reps, out);
+    time_shape<V, X, Y, 16, 3, 16, CI>(c, d, val, x, y, reps, out);
+    time_shape<V, X, Y, 12, 4, 16, CI>(c, d, val, x, y, reps, out);
+    time_shape<V, X, Y, 32, 2, 8, CI>(c, d, val, x, y, reps, out);
+    time_shape<V, X, Y, 24, 3, 8, CI>(c, d, val, x, y, reps, out);
+    time_shape<V, X, Y, 8, 4, 16, CI>(c, d, val, x, y, reps, out);
+  }
 }
 
 template <typename V, typename X, typename Y>
@@ -77,7 +101,9 @@ Status run(Context &c, const DeviceSell &d, const V *val, int reps, std::vector<
     return s;
   }
   cudaMemsetAsync(x, 0, sizeof(X) * d.ncols, c.stream);
-  if (d.dcol) sweep<V, X, Y, uint16_t>(c, d, val, x, y, reps, out);
+  if (d.xoff) sweep<V, X, Y, AlignedIdx>(c, d, val, x, y, reps, out);
+  else if (d.cbase && !d.dcol) sweep<V, X, Y, AllAlignedIdx>(c, d, val, x, y, reps, out);
+  else if (d.dcol) sweep<V, X, Y, uint16_t>(c, d, val, x, y, reps, out);
   else sweep<V, X, Y, int32_t>(c, d, val, x, y, reps, out);
   cudaStreamSynchronize(c.stream);
   cudaFree(x);

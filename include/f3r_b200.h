@@ -102,7 +102,11 @@ typedef struct f3r_params {
   int32_t inner_sstep;     /* bit 0: level 2, bit 1: level 3 run as sFGMRES (solver/gmres2.hpp:
                               137-221): all m preconditioner + matrix applications first, on the
                               raw vectors W(j+1) = A M W(j), then the Gram-Schmidt steps.  0 */
-  int32_t reserved1;
+  int32_t sell_align;      /* 1: offset-aligned SELL slices where the rows of a slice share their
+                              column offsets (stencil, banded structure): no column index is
+                              stored there, so an fp16 entry streams 2 bytes instead of 6.  With
+                              sell_sigma = 1 a stencil aligns every slice.  Same sums in the same
+                              order as the packed layout.  0 */
   int32_t reserved[8];
 } f3r_params;
 
@@ -137,12 +141,16 @@ typedef struct f3r_sell_info {
   int64_t nnz_padded;       /* stored entries including slice padding */
   int32_t max_width;        /* widest slice (entries per row) */
   int32_t dtypes;           /* bit (1 << f3r_dtype) set for each value copy held */
-  int32_t index_bits;       /* 16 (offsets from per-slice-column bases) or 32 */
+  int32_t index_bits;       /* 32, 16 (offsets from per-slice-column bases) or 0 (offset-aligned
+                               slices, with or without explicit 32-bit slices among them) */
 } f3r_sell_info;
 
 /* f3r_sell_create dtype_mask flag: store the column indices as 16-bit offsets
  * when they fit (see f3r_params.sell_index16). */
 #define F3R_SELL_INDEX16 (1 << 8)
+/* f3r_sell_create dtype_mask flag: offset-aligned slices where they fit (see
+ * f3r_params.sell_align). */
+#define F3R_SELL_ALIGNED (1 << 9)
 
 /* ---------------------------------------------------------------- errors */
 const char *f3r_last_error_string(void);

@@ -141,3 +141,18 @@ def test_invalid_params(ctx):
             F.Solver(ctx, A, **bad)
     with pytest.raises(F.F3RError):
         F.Solver(ctx, A, precond=F.PRECOND_ILU0_BJ, ilu_blocks=112)
+
+
+def test_aligned_sell_solve_is_identical(ctx):
+    """the offset-aligned layout changes no sum: the solve's iterate is the
+    packed layout's bit for bit (sigma 1, SDAINV factors aligned too)"""
+    A = F.stencil27(20, 20, 20, 2, 0.5).scale()
+    b = A.spmv(F.random_uniform(2, -1, 1, A.shape[0]))
+    xs = []
+    for align in (0, 1):
+        S = F.Solver(ctx, A, rel_tol=1e-10, c=8, sell_align=align)
+        x = np.zeros(len(b))
+        r = S.solve(b, x)
+        assert r.is_solved and r.expl_rel_res < 1e-10
+        xs.append(x)
+    assert np.array_equal(xs[0], xs[1])

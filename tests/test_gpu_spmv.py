@@ -46,13 +46,25 @@ def matrices():
     yield "diffusion7", F.diffusion7(10, 9, 8, 2.5, 3.0, 1).scale()
 
 
-@pytest.mark.parametrize("sigma,index16", [(1, False), (256, False), (1, True), (256, True)])
-def test_operate_bitexact(ctx, sigma, index16):
+FORM_BITS = {"int32": 32, "index16": 16, "aligned": 0}
+
+
+def make_sell(ctx, A, sigma, form):
+    return F.Sell(ctx, A, sigma=sigma, index16=form == "index16", aligned=form == "aligned")
+
+
+@pytest.mark.parametrize("sigma,form", [(1, "int32"), (256, "int32"), (1, "index16"), (256, "index16"),
+                                        (1, "aligned"), (256, "aligned"), (32, "aligned")])
+def test_operate_bitexact(ctx, sigma, form):
+    """every index form gives the oracle's sums bit for bit.  The aligned
+    cases cover the fully aligned form (stencils in natural order, clamped
+    edge slices), the mixed form (ragged matrices, sorted rows) and its
+    explicit slices"""
     for name, A in matrices():
         rptr, idx, val = A.arrays()
         n = A.shape[0]
-        S = F.Sell(ctx, A, sigma=sigma, index16=index16)
-        assert S.info().index_bits == (16 if index16 else 32)
+        S = make_sell(ctx, A, sigma, form)
+        assert S.info().index_bits == FORM_BITS[form]
         rng = np.random.default_rng(1)
         x64 = rng.standard_normal(n)
         x32 = x64.astype(np.float32)
@@ -82,12 +94,13 @@ def test_operate_bitexact(ctx, sigma, index16):
         S.close()
 
 
-@pytest.mark.parametrize("sigma,index16", [(1, False), (32, False), (32, True)])
-def test_residual_bitexact(ctx, sigma, index16):
+@pytest.mark.parametrize("sigma,form", [(1, "int32"), (32, "int32"), (32, "index16"), (1, "aligned"),
+                                        (32, "aligned")])
+def test_residual_bitexact(ctx, sigma, form):
     for name, A in matrices():
         rptr, idx, val = A.arrays()
         n = A.shape[0]
-        S = F.Sell(ctx, A, sigma=sigma, index16=index16)
+        S = make_sell(ctx, A, sigma, form)
         rng = np.random.default_rng(2)
         for dt, odt in ((np.float64, O.DT_F64), (np.float32, O.DT_F32), (np.float16, O.DT_F16)):
             x = (rng.standard_normal(n) * 0.1).astype(dt)
@@ -115,6 +128,28 @@ def test_wide_columns_fall_back_to_32bit(ctx):
     torch.cuda.synchronize()
     ref = O.spmv(rptr, idx, val, x, O.DT_F64, O.DT_F64, O.DT_F64)
     assert np.array_equal(y.cpu().numpy(), ref)
+
+
+@pytest.mark.parametrize("dims", [(32, 20, 9), (16, 16, 16), (33, 7, 5)])
+def test_aligned_stencil_matches_packed(ctx, dims):
+    """a 27-point stencil in natural order takes the fully aligned form (no
+    index stored, widths padded from 27 to 28): every value type's product
+    equals the packed int32 form's bit for bit, including the clamped slices
+    at the matrix's first and last rows"""
+    A = F.stencil27(*dims, 2, 0.5).scale()
+    n = A.shape[0]
+    S32, SA = F.Sell(ctx, A), F.Sell(ctx, A, aligned=True)
+    assert SA.info().index_bits == 0
+    assert S32.info().nnz_padded < SA.info().nnz_padded <= S32.info().nnz_padded * 1.2  # widths to a multiple of 4
+    rng = np.random.default_rng(9)
+    for vt, dt in ((F.F16, torch.float32), (F.F32, torch.float32), (F.F64, torch.float64), (F.F16, torch.float16)):
+        x = torch.from_numpy(rng.standard_normal(n)).to(dt).cuda()
+        y1 = torch.zeros(n, dtype=dt, device="cuda")
+        y2 = torch.zeros_like(y1)
+        S32.operate(x, y1, val_t=vt)
+        SA.operate(x, y2, val_t=vt)
+        torch.cuda.synchronize()
+        assert np.array_equal(y1.cpu().numpy().view(np.uint8), y2.cpu().numpy().view(np.uint8)), (vt, dt)
 
 
 def test_fp16_within_reference_bound(ctx):
@@ -160,12 +195,15 @@ def test_empty_and_bad_inputs(ctx):
         F.Sell(ctx, F.stencil27(4, 4, 4), sigma=0)
 
 
-def test_tune_times_every_shape(ctx):
+@pytest.mark.parametrize("aligned", [False, True])
+def test_tune_times_every_shape(ctx, aligned):
     A = F.stencil27(24, 24, 24, 2, 0.5).scale()
-    S = F.Sell(ctx, A)
+    S = F.Sell(ctx, A, aligned=aligned)
     for vt in (F.F16, F.F32, F.F64):
         rows = S.tune(vt, reps=3)
-        assert len(rows) >= 3  # shapes whose rings exceed the shared memory are skipped
+        # shapes whose rings exceed the shared memory are skipped; the aligned
+        # forms are laid out for one chunk width
+        assert len(rows) >= (2 if aligned else 3)
         assert sum(r["default"] for r in rows) == 1
         assert all(r["us"] > 0 for r in rows)
         assert rows == sorted(rows, key=lambda r: r["us"])
