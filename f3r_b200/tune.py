@@ -3,9 +3,11 @@
     python -m f3r_b200.tune [--nx 192] [--reps 20]
 
 Builds the nonsymmetric 27-point matrix of the benchmark (scaled), stores it
-as SELL-32 with sigma in {1, 256} and 32- or 16-bit column indices, and times
-out = A x for fp16 values (fp32 vectors), fp32 and fp64 at every launch shape
-the library carries (f3r_sell_tune).  Prints one markdown table per case.
+as SELL-32 with sigma in {1, 256} and 32- or 16-bit column indices, and with
+sigma = 1 also offset-aligned (no stored column index), and times out = A x
+for fp16 values (fp32 vectors), fp32 and fp64 at every launch shape the
+library carries for that layout (f3r_sell_tune).  Prints one markdown table
+per case.
 """
 from __future__ import annotations
 
@@ -22,20 +24,20 @@ def main():
     A = F.stencil27(args.nx, args.nx, args.nx, 2, 0.5).scale()
     ctx = F.Context(0)
     print(f"# SELL SpMV launch-shape sweep, {args.nx}^3 27-point (n={A.shape[0]}, nnz={A.nnz})\n")
-    for sigma in (1, 256):
-        for index16 in (False, True):
-            S = F.Sell(ctx, A, sigma=sigma, index16=index16)
-            bits = S.info().index_bits
-            for vt, name in ((F.F16, "fp16 values x fp32 vectors"), (F.F32, "fp32"), (F.F64, "fp64")):
-                rows = S.tune(vt, args.reps)
-                print(f"## sigma={sigma}, {bits}-bit indices, {name}\n")
-                print("| warps | stages | cols/copy | us | GB/s (algorithmic) | default |")
-                print("|---|---|---|---|---|---|")
-                for r in rows:
-                    print(f"| {r['warps']} | {r['stages']} | {r['kc']} | {r['us']:.1f} | {r['gbs']:.0f} | "
-                          f"{'yes' if r['default'] else ''} |")
-                print()
-            S.close()
+    for sigma, form in ((1, "aligned"), (1, "int32"), (1, "index16"), (256, "int32"), (256, "index16")):
+        S = F.Sell(ctx, A, sigma=sigma, index16=form == "index16", aligned=form == "aligned")
+        bits = S.info().index_bits
+        label = "offset-aligned (no stored index)" if bits == 0 else f"{bits}-bit indices"
+        for vt, name in ((F.F16, "fp16 values x fp32 vectors"), (F.F32, "fp32"), (F.F64, "fp64")):
+            rows = S.tune(vt, args.reps)
+            print(f"## sigma={sigma}, {label}, {name}\n")
+            print("| warps | stages | cols/copy | us | GB/s (algorithmic) | default |")
+            print("|---|---|---|---|---|---|")
+            for r in rows:
+                print(f"| {r['warps']} | {r['stages']} | {r['kc']} | {r['us']:.1f} | {r['gbs']:.0f} | "
+                      f"{'yes' if r['default'] else ''} |")
+            print()
+        S.close()
     ctx.close()
 
 
