@@ -255,48 +255,53 @@ __global__ void __launch_bounds__(WARPS * 32, 1)
     cst = (cst + 1 == STAGES) ? 0 : cst + 1;  // the stage read now is released below
     const bool full = kc == KC;
     if constexpr (MODE == 3) {
-      // fully aligned: the 32-column chunk is worked in two halves of 16 (so
-      // 24 warps fit at 80 registers); the stage is released after the last
-      // half's loads
+      // Fully aligned: the 32-column chunk is worked in sub-blocks of SUB
+      // columns, software-pipelined: the gathers of sub-block h + 1 are issued
+      // before the multiply-adds of sub-block h, so two sub-blocks of loads
+      // are in flight per warp.  SUB keeps the registers within the launch
+      // bound (16 columns for fp16 at up to 24 warps and for fp32 / fp64 at up
+      // to 16, 8 beyond).  The stage is
+      // released after the last sub-block's shared-memory loads.
+      constexpr int SUB = (WARPS > 24 || (sizeof(V) >= 4 && WARPS > 16)) ? 8 : 16, NS = KC / SUB;
       const V *lv = sv + lane * kc;  // lane-major values (kc a multiple of 4)
-      const int hlast = (kc - 1) >> 4;
+      const int nsub = (kc + SUB - 1) / SUB;
+      V vb[2][SUB];
+      Acc xb[2][SUB];
+      auto load_sub = [&](int h, V (&v)[SUB], Acc (&xg)[SUB]) {
 #pragma unroll
-      for (int h = 0; h < KC / 16; h++) {
-        if (h <= hlast) {
-          V vh[16];
-          int32_t ch[16];
+        for (int g = 0; g < SUB / 4; g++) {
+          const int k0 = h * SUB + g * 4;
+          if (full || k0 < kc) {
+            V t[4];
+            Vec4Load<V>::ld(lv + k0, t);
+            const int4 q = *reinterpret_cast<const int4 *>(sb + k0);
+            int32_t b[4] = {q.x + lane, q.y + lane, q.z + lane, q.w + lane};
+            if (clampc) {
 #pragma unroll
-          for (int g = 0; g < 4; g++) {
-            const int k0 = h * 16 + g * 4;
-            if (full || k0 < kc) {
-              V t[4];
-              Vec4Load<V>::ld(lv + k0, t);
-              const int4 q = *reinterpret_cast<const int4 *>(sb + k0);
-              int32_t b[4] = {q.x + lane, q.y + lane, q.z + lane, q.w + lane};
-              if (clampc) {
+              for (int e = 0; e < 4; e++) b[e] = min(max(b[e], 0), A.ncols - 1);
+            }
 #pragma unroll
-                for (int e = 0; e < 4; e++) b[e] = min(max(b[e], 0), A.ncols - 1);
-              }
-#pragma unroll
-              for (int e = 0; e < 4; e++) {
-                vh[g * 4 + e] = t[e];
-                ch[g * 4 + e] = b[e];
-              }
+            for (int e = 0; e < 4; e++) {
+              v[g * 4 + e] = t[e];
+              xg[g * 4 + e] = to_acc<Acc>(__ldg(x + b[e]));
             }
           }
-          if (h == hlast) release();
-          Acc xh[16];
+        }
+      };
+      load_sub(0, vb[0], xb[0]);
+      if (nsub == 1) release();
 #pragma unroll
-          for (int g = 0; g < 4; g++)
-            if (full || h * 16 + g * 4 < kc) {
+      for (int h = 0; h < NS; h++) {
+        if (h < nsub) {
+          if (h + 1 < NS && h + 1 < nsub) {
+            load_sub(h + 1, vb[(h + 1) & 1], xb[(h + 1) & 1]);
+            if (h + 2 == nsub) release();
+          }
 #pragma unroll
-              for (int e = 0; e < 4; e++) xh[g * 4 + e] = to_acc<Acc>(__ldg(x + ch[g * 4 + e]));
-            }
+          for (int g = 0; g < SUB / 4; g++)
+            if (full || h * SUB + g * 4 < kc) {
 #pragma unroll
-          for (int g = 0; g < 4; g++)
-            if (full || h * 16 + g * 4 < kc) {
-#pragma unroll
-              for (int e = 0; e < 4; e++) acc = fmaT(to_acc<Acc>(vh[g * 4 + e]), xh[g * 4 + e], acc);
+              for (int e = 0; e < 4; e++) acc = fmaT(to_acc<Acc>(vb[h & 1][g * 4 + e]), xb[h & 1][g * 4 + e], acc);
             }
         }
       }
