@@ -117,14 +117,15 @@ template <> struct Vec4Load<double> {
 // buffers per warp, KC columns per chunk; one CTA per SM.  Chosen by sweeps
 // (f3r_sell_tune) on the 192^3 27-point matrix (n = 7.08M, nnz = 189M).  The
 // packed forms are bound by the bytes in flight per SM; the fully aligned
-// form streams 2 bytes per fp16 entry and is bound by registers: a 32-column
-// chunk worked in two halves fits 80 registers at 24 warps.
+// form streams 2 bytes per fp16 entry and is bound by the latency of its
+// gathers: a 32-column chunk worked in pipelined sub-blocks fits 80 registers
+// at 24 warps (fp16); fp32 is fastest at 16 warps with 16-column sub-blocks.
 template <typename V, typename CI = int32_t> struct SellCfg;
 template <typename CI> struct SellCfg<__half, CI> { static constexpr int WARPS = 24, STAGES = 2, KC = 16; };
 template <typename CI> struct SellCfg<float, CI> { static constexpr int WARPS = 24, STAGES = 2, KC = 16; };
 template <typename CI> struct SellCfg<double, CI> { static constexpr int WARPS = 16, STAGES = 2, KC = 16; };
 template <> struct SellCfg<__half, AllAlignedIdx> { static constexpr int WARPS = 24, STAGES = 2, KC = 32; };
-template <> struct SellCfg<float, AllAlignedIdx> { static constexpr int WARPS = 24, STAGES = 2, KC = 32; };
+template <> struct SellCfg<float, AllAlignedIdx> { static constexpr int WARPS = 16, STAGES = 2, KC = 32; };
 template <> struct SellCfg<double, AllAlignedIdx> { static constexpr int WARPS = 12, STAGES = 2, KC = 32; };
 
 template <typename V, typename CI, int WARPS, int STAGES, int KC>
