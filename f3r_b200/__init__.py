@@ -24,9 +24,27 @@ from ._capi import (F16, F32, F64, PRECOND_ILU0_BAJ, PRECOND_ILU0_BJ, PRECOND_IL
 __all__ = ["HostMatrix", "Context", "Sell", "Solver", "Params", "solve_res_t", "F3RError", "F64", "F32", "F16",
            "PRECOND_SDAINV", "PRECOND_ILU0_BJ", "PRECOND_ILU0_JACOBI", "PRECOND_ILU0_BAJ", "Trsv", "TRSV_LOWER",
            "TRSV_LOWER_D", "TRSV_D_UPPER", "TRSV_JACOBI", "TRSV_BAJ", "stencil27", "diffusion7", "random_uniform", "host_spmv",
-           "read_matrix", "read_system", "read_vector", "write_vector", "CSV_HEADER", "csv_row"]
+           "read_matrix", "read_system", "read_vector", "write_vector", "CSV_HEADER", "csv_row", "solve_batch"]
 
 _NP2DT = {np.dtype(np.float64): F64, np.dtype(np.float32): F32, np.dtype(np.float16): F16}
+
+# Live device objects, closed at interpreter exit in dependency order (solvers,
+# matrices and triangular solves before the contexts they run on), before the
+# CUDA runtime itself shuts down.
+import atexit
+import weakref
+
+_LIVE = {k: weakref.WeakSet() for k in ("solver", "sell", "trsv", "context")}
+
+
+@atexit.register
+def _close_all():
+    for kind in ("solver", "sell", "trsv", "context"):
+        for obj in list(_LIVE[kind]):
+            try:
+                obj.close()
+            except Exception:
+                pass
 
 
 class HostMatrix:
@@ -184,6 +202,7 @@ class Context:
         h = C.c_void_p()
         check(lib().f3r_context_create(device, C.byref(h)))
         self._h = h
+        _LIVE["context"].add(self)
         self.device = device
 
     def set_stream(self, stream_ptr: Optional[int]) -> None:
@@ -226,6 +245,7 @@ class Sell:
         v = A.view()
         check(lib().f3r_sell_create(ctx._h, C.byref(v), 32, sigma, mask, C.byref(h)))
         self._h = h
+        _LIVE["sell"].add(self)
         self.ctx = ctx
 
     def info(self) -> _capi.SellInfo:
@@ -274,6 +294,7 @@ class Trsv:
         v = M.view()
         check(lib().f3r_trsv_create(ctx._h, C.byref(v), form, kind, iters, omega, C.byref(h)))
         self._h = h
+        _LIVE["trsv"].add(self)
         self.ctx = ctx
 
     def solve(self, x, y) -> None:
@@ -324,6 +345,7 @@ class Solver:
         v = A.view()
         check(lib().f3r_solver_create(ctx._h, C.byref(v), C.byref(p), C.byref(h)))
         self._h = h
+        _LIVE["solver"].add(self)
         self.ctx = ctx
         self.params = p
         self.n = v.nrows
@@ -343,17 +365,22 @@ class Solver:
     def solve(self, b, x, cond: Optional[Callable[[int, float], bool]] = None) -> solve_res_t:
         """Solve A x = b.  b, x: numpy float64 arrays (x is updated in place and
         holds the initial guess) or torch CUDA float64 tensors."""
-        def ptr(a):
-            if isinstance(a, np.ndarray):
-                if a.dtype != np.float64 or not a.flags.c_contiguous:
-                    raise TypeError("numpy vectors must be contiguous float64")
-                return a.ctypes.data
-            return a.data_ptr()
         res = _capi.Result()
         cb = COND_NONE if cond is None else _capi.COND_FN(lambda i, e, u: 1 if cond(i, e) else 0)
-        check(lib().f3r_solver_solve(self._h, C.c_void_p(ptr(b)), C.c_void_p(ptr(x)), cb, None, C.byref(res)))
-        return solve_res_t(bool(res.is_solved), res.res_iter, res.res_nrm2, res.impl_rel_res, res.expl_rel_res,
-                           res.restarts, res.inner_applications, res.solve_seconds, res.kernel_launches)
+        check(lib().f3r_solver_solve(self._h, C.c_void_p(_ptr(b)), C.c_void_p(_ptr(x)), cb, None, C.byref(res)))
+        return _res(res)
+
+    def solve_multi(self, B, X, cond: Optional[Callable[[int, float], bool]] = None):
+        """Solve A X = B for several right-hand sides: B and X of shape
+        (nrhs, n), row k one system (numpy float64 C-contiguous, or torch CUDA
+        float64); X is updated in place.  Returns one solve_res_t per row."""
+        nrhs, ld = _rows(B, self.n)
+        _rows(X, self.n)
+        res = (_capi.Result * max(nrhs, 1))()
+        cb = COND_NONE if cond is None else _capi.COND_FN(lambda i, e, u: 1 if cond(i, e) else 0)
+        check(lib().f3r_solver_solve_multi(self._h, nrhs, C.c_void_p(_ptr(B)), ld, C.c_void_p(_ptr(X)), ld, cb,
+                                           None, res))
+        return [_res(r) for r in res[:nrhs]]
 
     def close(self):
         if getattr(self, "_h", None) is not None and _capi is not None and _capi._lib is not None:
@@ -365,3 +392,52 @@ class Solver:
 
 
 COND_NONE = _capi.COND_FN()
+
+
+def _ptr(a) -> int:
+    if isinstance(a, np.ndarray):
+        if a.dtype != np.float64 or not a.flags.c_contiguous:
+            raise TypeError("numpy vectors must be contiguous float64")
+        return a.ctypes.data
+    if a.dtype != __import__("torch").float64 or not a.is_contiguous():
+        raise TypeError("torch vectors must be contiguous float64")
+    return a.data_ptr()
+
+
+def _rows(M, n: int):
+    """(nrhs, leading dimension) of a (nrhs, n) block of right-hand sides"""
+    shape = tuple(M.shape)
+    if len(shape) != 2 or shape[1] != n:
+        raise ValueError(f"expected shape (nrhs, {n}), got {shape}")
+    return shape[0], n
+
+
+def _res(res) -> solve_res_t:
+    return solve_res_t(bool(res.is_solved), res.res_iter, res.res_nrm2, res.impl_rel_res, res.expl_rel_res,
+                       res.restarts, res.inner_applications, res.solve_seconds, res.kernel_launches)
+
+
+def solve_batch(systems, cond: Optional[Callable[[int, float], bool]] = None):
+    """Independent systems at once (f3r_solve_batch): systems is a list of
+    (solver, B, X) with B, X of shape (nrhs, n) as in Solver.solve_multi.
+    Solvers on different contexts run concurrently.  Returns, per system, the
+    list of its solve_res_t."""
+    count = len(systems)
+    S = (C.c_void_p * max(count, 1))()
+    nr = (C.c_int32 * max(count, 1))()
+    bp = (C.c_void_p * max(count, 1))()
+    xp = (C.c_void_p * max(count, 1))()
+    ld = (C.c_int64 * max(count, 1))()
+    for i, (solver, B, X) in enumerate(systems):
+        k, n = _rows(B, solver.n)
+        _rows(X, solver.n)
+        S[i], nr[i], bp[i], xp[i], ld[i] = solver._h.value, k, _ptr(B), _ptr(X), n
+    total = sum(nr[i] for i in range(count))
+    res = (_capi.Result * max(total, 1))()
+    cb = COND_NONE if cond is None else _capi.COND_FN(lambda i, e, u: 1 if cond(i, e) else 0)
+    check(lib().f3r_solve_batch(count, S, nr, bp, ld, xp, ld, cb, None, res))
+    out, at = [], 0
+    for i in range(count):
+        out.append([_res(r) for r in res[at:at + nr[i]]])
+        at += nr[i]
+    return out

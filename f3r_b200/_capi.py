@@ -104,6 +104,11 @@ SIGNATURES = {
     "f3r_params_default": (None, [C.POINTER(Params)]),
     "f3r_solver_create": (C.c_int, [_vp, C.POINTER(CSR), C.POINTER(Params), _pp]),
     "f3r_solver_solve": (C.c_int, [_vp, _vp, _vp, COND_FN, _vp, C.POINTER(Result)]),
+    "f3r_solver_solve_multi": (C.c_int, [_vp, C.c_int32, _vp, C.c_int64, _vp, C.c_int64, COND_FN, _vp,
+                                         C.POINTER(Result)]),
+    "f3r_solve_batch": (C.c_int, [C.c_int32, C.POINTER(_vp), C.POINTER(C.c_int32), C.POINTER(_vp),
+                                  C.POINTER(C.c_int64), C.POINTER(_vp), C.POINTER(C.c_int64), COND_FN, _vp,
+                                  C.POINTER(Result)]),
     "f3r_solver_info": (C.c_int, [_vp, C.POINTER(SellInfo), C.POINTER(C.c_int32)]),
     "f3r_solver_operate": (C.c_int, [_vp, C.c_int, C.c_int, _vp, C.c_int, _vp]),
     "f3r_solver_destroy": (None, [_vp]),

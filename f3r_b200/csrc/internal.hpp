@@ -42,6 +42,11 @@ Status sdainv(const HostCSR &A, double tol, double acc, HostCSR **Z, HostCSR **W
 Status ilu0_bj(const HostCSR &A, int32_t blocks, double acc, HostCSR **L, HostCSR **U,
                std::vector<int32_t> *bptr);
 
+// The context a solver runs on (solves sharing one must not overlap) and its
+// row count (solver.cu).
+const void *solver_context(const f3r_solver *s);
+int32_t solver_rows(const f3r_solver *s);
+
 }  // namespace f3r
 
 struct f3r_host_matrix {

@@ -49,12 +49,17 @@ struct Context {
   // grid for the elementwise / reduction kernels: up to 8 blocks of 256 per SM
   // (full thread occupancy); partial-sum buffers are sized for this bound
   int ew_grid(int64_t n) const { return (int)std::max<int64_t>(1, std::min<int64_t>(cdiv(n, kEwThreads), (int64_t)sm_count * 8)); }
-  // checks the device error word (after a synchronisation)
+  // checks the device error word.  Stream-ordered on this context's stream
+  // (no legacy-stream call), so it may run while another thread captures a
+  // graph on its own context.
   Status check_device_error() {
-    int e = 0;
-    CUDA_TRY(cudaMemcpy(&e, err, sizeof(int), cudaMemcpyDeviceToHost));
+    int *e_h = reinterpret_cast<int *>(pinned + 7);
+    CUDA_TRY(cudaMemcpyAsync(e_h, err, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    CUDA_TRY(cudaStreamSynchronize(stream));
+    const int e = *e_h;
     if (e == DEV_OK) return F3R_SUCCESS;
-    CUDA_TRY(cudaMemset(err, 0, sizeof(int)));
+    CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(int), stream));
+    CUDA_TRY(cudaStreamSynchronize(stream));
     if (e == DEV_TIMEOUT_SPMV) return fail(F3R_ERROR_TIMEOUT, "a bulk-copy wait in the SpMV kernel exceeded its bound");
     return fail(F3R_ERROR_BREAKDOWN, "zero or non-finite norm in an Arnoldi step");
   }

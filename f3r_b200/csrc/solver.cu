@@ -956,6 +956,11 @@ struct f3r_solver {
   f3r::Solver *s = nullptr;
 };
 
+namespace f3r {
+const void *solver_context(const f3r_solver *s) { return s && s->s ? (const void *)s->s->ctx : nullptr; }
+int32_t solver_rows(const f3r_solver *s) { return s && s->s ? s->s->n : 0; }
+}  // namespace f3r
+
 // ===========================================================================
 // C ABI
 // ===========================================================================
@@ -1101,7 +1106,9 @@ f3r_status f3r_context_create(int32_t device, f3r_context **out) {
 }
 void f3r_context_destroy(f3r_context *ctx) {
   if (!ctx) return;
-  cudaSetDevice(ctx->device);
+  // while the CUDA runtime shuts down (process exit) nothing can be released
+  // any more: the object is left to the exit
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return;
   cudaStreamSynchronize(ctx->stream);
   cudaFree(ctx->err);
   cudaFree(ctx->partials);
@@ -1165,7 +1172,7 @@ f3r_status f3r_sell_info_get(const f3r_sell *m, f3r_sell_info *info) {
 }
 void f3r_sell_destroy(f3r_sell *m) {
   if (!m) return;
-  cudaSetDevice(m->ctx->device);
+  if (cudaSetDevice(m->ctx->device) != cudaSuccess) return;  // runtime shutting down: left to the exit
   cudaStreamSynchronize(m->ctx->stream);
   m->d.release();
   delete m;
@@ -1304,7 +1311,7 @@ f3r_status f3r_solver_operate(f3r_solver *s, f3r_dtype val_t, f3r_dtype in_t, co
 
 void f3r_solver_destroy(f3r_solver *s) {
   if (!s) return;
-  cudaSetDevice(s->s->ctx->device);
+  if (cudaSetDevice(s->s->ctx->device) != cudaSuccess) return;  // runtime shutting down: left to the exit
   cudaStreamSynchronize(s->s->ctx->stream);
   delete s->s;
   delete s;

@@ -239,7 +239,7 @@ f3r_status f3r_trsv_solve(f3r_trsv *t, const void *in, void *out) {
 
 void f3r_trsv_destroy(f3r_trsv *t) {
   if (!t) return;
-  cudaSetDevice(t->ctx->device);
+  if (cudaSetDevice(t->ctx->device) != cudaSuccess) return;  // runtime shutting down: left to the exit
   t->t.release();
   delete t;
 }

@@ -335,6 +335,26 @@ f3r_status f3r_solver_create(f3r_context *ctx, const f3r_csr *a, const f3r_param
 f3r_status f3r_solver_solve(f3r_solver *s, const double *b, double *x, f3r_cond_fn cond,
                             void *user, f3r_result *result);
 f3r_status f3r_solver_info(const f3r_solver *s, f3r_sell_info *a_info, int32_t *precond_diagonal);
+/* Several right-hand sides: column k of B (b + k * ldb) is solved into
+ * column k of X (x + k * ldx), x holding the initial guesses; ldb, ldx >= n;
+ * host or device pointers.  Each column is its own F3R solve on this
+ * solver's device objects (matrix, preconditioner, captured graphs), in
+ * column order; results (may be NULL) gets one entry per column.  The
+ * nrhs argument of the planned boundary's solve call. */
+f3r_status f3r_solver_solve_multi(f3r_solver *s, int32_t nrhs, const double *b, int64_t ldb, double *x, int64_t ldx,
+                                  f3r_cond_fn cond, void *user, f3r_result *results);
+/* Independent systems at once: system i is f3r_solver_solve_multi(solvers[i],
+ * nrhs[i], b[i], ldb[i], x[i], ldx[i], ...).  Solvers on different contexts
+ * (streams) run concurrently, one host thread per context (at most 128),
+ * solvers sharing a context one after another; so cond may be called from
+ * several threads at once.  results holds sum(nrhs) entries, system by
+ * system.  Every system is attempted; the first failing one (in index order)
+ * gives the status.  The batched solve of the planned boundary
+ * (f3r_solve_batch(handles[], ...)); the reference has no counterpart. */
+f3r_status f3r_solve_batch(int32_t count, f3r_solver *const *solvers, const int32_t *nrhs, const double *const *b,
+                           const int64_t *ldb, double *const *x, const int64_t *ldx, f3r_cond_fn cond, void *user,
+                           f3r_result *results);
+
 /* out = A in with the solver's own device copy of A (the matrix its levels
  * use: SELL-C-sigma, rows and columns in the solver's storage order P A P^T,
  * so with sigma > 1 `in` and `out` are in that order too).  Same type

@@ -196,6 +196,13 @@ class F3R {
   }
   // Solver::solve(in, out) without a stop test: the params' rel_tol applies
   void solve(const double *b, double *x) const { solve(b, x, nullptr); }
+  // nrhs systems: column k of B (b + k * ld) into column k of X (x + k * ld)
+  std::vector<f3r_result> solve_multi(int32_t nrhs, const double *b, double *x, int64_t ld) const {
+    std::vector<f3r_result> r(nrhs > 0 ? nrhs : 0);
+    check(f3r_solver_solve_multi(s_.get(), nrhs, b, ld, x, ld, nullptr, nullptr, r.data()));
+    return r;
+  }
+  f3r_solver *handle() const { return s_.get(); }
 
  private:
   std::shared_ptr<f3r_solver> s_;
