@@ -516,6 +516,83 @@ def run_c4(args):
     print(json.dumps(line), flush=True)
 
 
+def level_errors(F, torch, solver, A_unscaled_range, A, xs):
+    """Error of every precision level against fp64, on the solved (scaled)
+    system: the value copies' rounding (max relative entry error) and the
+    products w = A z at each level's types against the fp64 product, all on
+    z = x* (the exact solution)."""
+    rptr, idx, val = A.arrays()
+    e16 = np.abs(val.astype(np.float16).astype(np.float64) - val) / np.abs(val)
+    e32 = np.abs(val.astype(np.float32).astype(np.float64) - val) / np.abs(val)
+    n = A.shape[0]
+    z64 = torch.from_numpy(xs).cuda()
+    y64 = torch.empty_like(z64)
+    solver.operate(z64, y64, val_t=F.F64)
+    z32 = z64.float()
+    y32 = torch.empty_like(z32)
+    solver.operate(z32, y32, val_t=F.F32)
+    y16 = torch.empty_like(z32)
+    solver.operate(z32, y16, val_t=F.F16)           # level 3: fp16 matrix, fp32 vectors
+    z16 = z64.half()
+    y16h = torch.empty(n, dtype=torch.float16, device="cuda")
+    solver.operate(z16, y16h, val_t=F.F16)           # level 4: fp16 matrix, fp16 vectors
+    torch.cuda.synchronize()
+    ref = y64.double()
+    nr = float(torch.linalg.norm(ref))
+    rel = lambda y: float(torch.linalg.norm(y.double() - ref)) / nr
+    return {"raw_entry_range": A_unscaled_range,
+            "scaled_entry_range": [float(np.abs(val).min()), float(np.abs(val).max())],
+            "value_rounding_max_rel": {"fp32": float(e32.max()), "fp16": float(e16.max())},
+            "spmv_rel_err_vs_fp64": {"level2_fp32": rel(y32), "level3_fp16A_fp32x": rel(y16),
+                                     "level4_fp16A_fp16x": rel(y16h)}}
+
+
+def run_c3(args):
+    """C3, precision stress: 7-point diffusion with coefficients exp(g) (g a
+    seeded Gaussian field, sigma 2.5, correlation length 8 cells) on an
+    nx^3 grid (256 by default), diagonally scaled into fp16 range; time to
+    1e-10 and the error of every precision level against fp64."""
+    import torch
+    import f3r_b200 as F
+    torch.cuda.set_device(0)
+    nx = args.nx if args.nx != NX else 256
+    A = F.diffusion7(nx, nx, nx, 2.5, 8.0, 3)
+    raw = np.abs(A.arrays()[2])
+    raw_range = [float(raw.min()), float(raw.max())]
+    A.scale()
+    n = A.shape[0]
+    xs = F.random_uniform(0, -1.0, 1.0, n)
+    b = A.spmv(xs)
+    ctx = F.Context(0)
+    t0 = time.perf_counter()
+    S = F.Solver(ctx, A, **PARAMS)
+    setup = time.perf_counter() - t0
+    b_d = torch.from_numpy(b).cuda()
+    x_d = torch.zeros_like(b_d)
+    for _ in range(max(args.warmup, 1)):
+        x_d.zero_()
+        S.solve(b_d, x_d)
+    torch.cuda.synchronize()
+    times, r = [], None
+    for _ in range(args.steps):
+        x_d.zero_()
+        r = S.solve(b_d, x_d)
+        times.append(r.solve_seconds)
+    err = float(torch.linalg.norm(x_d.cpu() - torch.from_numpy(xs)) / np.linalg.norm(xs))
+    lv = level_errors(F, torch, S, raw_range, A, xs)
+    line = {"metric": "time to 1e-10 FP64 relative residual, plain F3R, C3 precision stress", "value":
+            round(min(times) * 1e3, 2), "unit": "ms", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": False, "dtype": "mixed: f16 storage/f32 accumulate, f32, f64",
+            "data": "synthetic (seeded log-normal coefficient field)",
+            "config": {"workload": f"C3: 7-pt diffusion exp(g), sigma 2.5, corr 8, {nx}^3 (n={n}, nnz={A.nnz}), "
+                                   "SDAINV, tol 1e-10", "sell": layout_desc(), "setup_s": round(setup, 1)},
+            "solve": {"outer_iters": r.res_iter, "inner_applications": r.inner_applications,
+                      "impl_rel_res": r.impl_rel_res, "expl_rel_res": r.expl_rel_res,
+                      "x_rel_err_vs_exact": err, "solved": r.is_solved},
+            "levels": lv}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -531,8 +608,9 @@ def main():
     ap.add_argument("--layout", default="aligned", choices=sorted(LAYOUTS),
                     help="SELL layout of our arm: offset-aligned sigma=1 (default) or packed sigma=256")
     ap.add_argument("--no-alt-layout", action="store_true", help="skip timing the other layout")
-    ap.add_argument("--config", default="c2", choices=["c2", "c4"],
-                    help="c2: the headline solve; c4: the batched configuration (96 systems, 1-16 RHS each)")
+    ap.add_argument("--config", default="c2", choices=["c2", "c3", "c4"],
+                    help="c2: the headline solve; c3: the precision stress (256^3 diffusion, per-level errors); "
+                         "c4: the batched configuration (96 systems, 1-16 RHS each)")
     args = ap.parse_args()
     if args.impl == "ours":
         set_layout(args.layout)
@@ -541,6 +619,8 @@ def main():
         set_precond(args.precond, args.ilu_blocks, args.trsv_iters)
     if args.config == "c4":
         run_c4(args)
+    elif args.config == "c3":
+        run_c3(args)
     elif args.impl == "reference":
         run_reference(args)
     else:

@@ -87,9 +87,11 @@ HostCSR *stencil27(int32_t nx, int32_t ny, int32_t nz, int32_t variant, double b
 // ---------------------------------------------------------------------------
 // 7-point variable-coefficient diffusion with log-normal coefficients.  The
 // field g is white noise smoothed by a separable Gaussian of standard
-// deviation corr_len cells (clamped at the box edges), normalised to zero mean
-// and unit variance, times sigma; k = exp(g).  Face coefficients are the
-// harmonic mean of the two cells; a boundary face uses the cell's own k.
+// deviation corr_len cells, applied periodically (the circular convolution an
+// FFT filter computes, so g is stationary: every cell has the same variance),
+// normalised to zero mean and unit variance, times sigma; k = exp(g).  Face
+// coefficients are the harmonic mean of the two cells; a boundary face uses
+// the cell's own k.
 // ---------------------------------------------------------------------------
 HostCSR *diffusion7(int32_t nx, int32_t ny, int32_t nz, double sigma, double corr_len, uint64_t seed) {
   const int64_t n = (int64_t)nx * ny * nz;
@@ -113,7 +115,8 @@ HostCSR *diffusion7(int32_t nx, int32_t ny, int32_t nz, double sigma, double cor
         int32_t c = (int32_t)((r / stride[axis]) % ext[axis]);
         double s = 0;
         for (int q = -R; q <= R; q++) {
-          int32_t cc = std::min(std::max(c + q, 0), ext[axis] - 1);
+          int32_t cc = (c + q) % ext[axis];
+          if (cc < 0) cc += ext[axis];
           s += w[q + R] * g[r + (int64_t)(cc - c) * stride[axis]];
         }
         t[r] = s;

@@ -171,9 +171,10 @@ f3r_status f3r_problem_stencil27(int32_t nx, int32_t ny, int32_t nz, int32_t var
                                  double beta, f3r_host_matrix **out);
 
 /* 7-point variable-coefficient diffusion: face coefficient = harmonic mean of
- * exp(g) of the two cells, g a seeded Gaussian random field (std sigma,
- * correlation length corr_len cells), Dirichlet boundary folded into the
- * diagonal.  No reference counterpart (a synthetic stress matrix). */
+ * exp(g) of the two cells, g a seeded stationary Gaussian random field (std
+ * sigma, periodic Gaussian filter of correlation length corr_len cells),
+ * Dirichlet boundary folded into the diagonal.  No reference counterpart (a
+ * synthetic stress matrix). */
 f3r_status f3r_problem_diffusion7(int32_t nx, int32_t ny, int32_t nz, double sigma,
                                   double corr_len, uint64_t seed, f3r_host_matrix **out);
 
