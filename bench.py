@@ -593,6 +593,121 @@ def run_c3(args):
     print(json.dumps(line), flush=True)
 
 
+def run_c5(args):
+    """C5, the learned preconditioner: the network trained on the GPU on
+    residual / error pairs of 256 seeded 7-point log-normal fields (sigma
+    1.5, correlation length 6; 24^3 each, stacked), then held-out 128^3
+    fields solved to 1e-10 with plain SDAINV and with the learned correction
+    (BF16 tensor-core inference), one after another and batched
+    (f3r_solve_batch over one context per system)."""
+    import torch
+    import f3r_b200 as F
+    from f3r_b200.learned import Learned, training_set
+    torch.cuda.set_device(0)
+    nx = args.nx if args.nx != NX else 128
+    ctx = F.Context(0)
+    t0 = time.perf_counter()
+    ts = training_set(ctx, range(args.c5_train), nt=24, **PARAMS)
+    t_data = time.perf_counter() - t0
+    L = Learned(ctx, seed=0)
+    L.set_data(**ts.data())
+    t0 = time.perf_counter()
+    losses = L.train(args.c5_steps, 2e-3)
+    t_train = time.perf_counter() - t0
+    final_loss = L.evaluate()
+    n_train, n_pairs = ts.A.shape[0], ts.r.shape[0]
+    del ts
+    rows, solvers_l, solvers_p, ctxs, bs, xs_d = [], [], [], [], [], []
+    probe_k = []
+    for s in range(10000, 10000 + args.c5_eval):
+        A = F.diffusion7(nx, nx, nx, 1.5, 6.0, s).scale()
+        n = A.shape[0]
+        Z, Wt = A.sdainv()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        Zc, Wc = L.correct(A, nx, nx, Z, Wt)
+        t_inf = time.perf_counter() - t0
+        b = A.spmv(F.random_uniform(s, -1.0, 1.0, n))
+        c = F.Context(0)
+        Sp = F.Solver(c, A, factors=(Z, Wt), **PARAMS)
+        Sl = F.Solver(c, A, factors=(Zc, Wc), **PARAMS)
+        b_d = torch.from_numpy(b).cuda()
+        x_d = torch.zeros_like(b_d)
+        rec = {"seed": s, "correct_call_ms": round(t_inf * 1e3, 1)}
+        for name, S in (("plain", Sp), ("learned", Sl)):
+            for _ in range(max(args.warmup, 1)):
+                x_d.zero_()
+                S.solve(b_d, x_d)
+            best = None
+            for _ in range(args.steps):
+                x_d.zero_()
+                r = S.solve(b_d, x_d)
+                best = r if best is None or r.solve_seconds < best.solve_seconds else best
+            rec[name] = {"ms": round(best.solve_seconds * 1e3, 2), "outer_iters": best.res_iter,
+                         "expl_rel_res": best.expl_rel_res, "solved": bool(best.is_solved)}
+        # residual after a fixed number of outer steps (one fewer than plain needs): the
+        # convergence gain that the whole-iteration count can hide
+        k = max(1, rec["plain"]["outer_iters"] - 1)
+        for name, S in (("plain", Sp), ("learned", Sl)):
+            x_d.zero_()
+            r = S.solve(b_d, x_d, cond=lambda i, e, k=k: i >= k)
+            rec[name][f"expl_rel_res_after_{k}"] = r.expl_rel_res
+        rows.append(rec)
+        ctxs.append(c)
+        solvers_p.append(Sp)
+        solvers_l.append(Sl)
+        bs.append(b_d)
+        xs_d.append(torch.zeros_like(b_d))
+
+    def run(solvers, batched):
+        for x in xs_d:
+            x.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        if batched:
+            res = [r[0] for r in F.solve_batch([(S, b.view(1, -1), x.view(1, -1))
+                                                 for S, b, x in zip(solvers, bs, xs_d)])]
+        else:
+            res = [S.solve(b, x) for S, b, x in zip(solvers, bs, xs_d)]
+        torch.cuda.synchronize()
+        return time.perf_counter() - t0, res
+
+    for _ in range(max(args.warmup, 1)):
+        run(solvers_p, False)
+        run(solvers_l, True)
+    tp, resp = min((run(solvers_p, False) for _ in range(args.steps)), key=lambda t: t[0])
+    tl, resl = min((run(solvers_l, False) for _ in range(args.steps)), key=lambda t: t[0])
+    tlb, reslb = min((run(solvers_l, True) for _ in range(args.steps)), key=lambda t: t[0])
+    tpb, _ = min((run(solvers_p, True) for _ in range(args.steps)), key=lambda t: t[0])
+    mean = lambda key, f: float(np.mean([f(r[key]) for r in rows]))
+    gains = [r["plain"][k] / r["learned"][k] for r in rows for k in r["plain"] if k.startswith("expl_rel_res_after")]
+    line = {"metric": "time to 1e-10 FP64 relative residual, learned vs plain SDAINV (C5)",
+            "value": round(mean("learned", lambda d: d["ms"]), 2), "unit": "ms", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": False,
+            "dtype": "mixed: f16 storage/f32 accumulate, f32, f64; MLP bf16 inference, f32 training",
+            "data": "synthetic (seeded log-normal coefficient fields)",
+            "config": {"workload": f"C5: 7-pt diffusion, log-normal sigma 1.5, corr 6, {nx}^3 held-out "
+                                   f"(n={nx ** 3}), SDAINV vs learned SDAINV, tol 1e-10",
+                       "train_fields": args.c5_train, "train_grid": "24^3 each, stacked", "train_rows": n_train,
+                       "eval_fields": args.c5_eval, "sell": layout_desc(),
+                       "timing": "per system: device solve time (CUDA events), best of steps; "
+                                 "whole set: host wall clock, device synchronised on both sides"},
+            "plain_ms": round(mean("plain", lambda d: d["ms"]), 2),
+            "learned_over_plain_time": round(mean("learned", lambda d: d["ms"]) / mean("plain", lambda d: d["ms"]), 3),
+            "outer_iters": {"plain": [r["plain"]["outer_iters"] for r in rows],
+                            "learned": [r["learned"]["outer_iters"] for r in rows]},
+            "residual_gain_at_fixed_outer_steps": {"min": round(min(gains), 2), "max": round(max(gains), 2),
+                                                   "geomean": round(float(np.exp(np.mean(np.log(gains)))), 2)},
+            "set_wall_ms": {"plain_sequential": round(tp * 1e3, 1), "learned_sequential": round(tl * 1e3, 1),
+                            "plain_batched": round(tpb * 1e3, 1), "learned_batched": round(tlb * 1e3, 1)},
+            "speedup_learned_batched_vs_plain_sequential": round(tp / tlb, 3),
+            "all_solved": all(r.is_solved for r in resl + reslb + resp),
+            "training": {"pairs": n_pairs, "steps": args.c5_steps, "train_s": round(t_train, 2),
+                         "data_s": round(t_data, 1), "loss_first": float(losses[0]), "loss_final": final_loss},
+            "systems": rows}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -608,16 +723,22 @@ def main():
     ap.add_argument("--layout", default="aligned", choices=sorted(LAYOUTS),
                     help="SELL layout of our arm: offset-aligned sigma=1 (default) or packed sigma=256")
     ap.add_argument("--no-alt-layout", action="store_true", help="skip timing the other layout")
-    ap.add_argument("--config", default="c2", choices=["c2", "c3", "c4"],
+    ap.add_argument("--config", default="c2", choices=["c2", "c3", "c4", "c5"],
                     help="c2: the headline solve; c3: the precision stress (256^3 diffusion, per-level errors); "
-                         "c4: the batched configuration (96 systems, 1-16 RHS each)")
+                         "c4: the batched configuration (96 systems, 1-16 RHS each); "
+                         "c5: the learned preconditioner (training, then held-out 128^3 solves)")
+    ap.add_argument("--c5-train", type=int, default=256, help="C5 training fields")
+    ap.add_argument("--c5-eval", type=int, default=4, help="C5 held-out fields solved (32 for the full set)")
+    ap.add_argument("--c5-steps", type=int, default=500, help="C5 Adam steps")
     args = ap.parse_args()
     if args.impl == "ours":
         set_layout(args.layout)
     set_size(args.nx)
     if args.impl == "ours":
         set_precond(args.precond, args.ilu_blocks, args.trsv_iters)
-    if args.config == "c4":
+    if args.config == "c5":
+        run_c5(args)
+    elif args.config == "c4":
         run_c4(args)
     elif args.config == "c3":
         run_c3(args)

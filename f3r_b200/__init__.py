@@ -34,12 +34,12 @@ _NP2DT = {np.dtype(np.float64): F64, np.dtype(np.float32): F32, np.dtype(np.floa
 import atexit
 import weakref
 
-_LIVE = {k: weakref.WeakSet() for k in ("solver", "sell", "trsv", "context")}
+_LIVE = {k: weakref.WeakSet() for k in ("solver", "sell", "trsv", "learned", "context")}
 
 
 @atexit.register
 def _close_all():
-    for kind in ("solver", "sell", "trsv", "context"):
+    for kind in ("solver", "sell", "trsv", "learned", "context"):
         for obj in list(_LIVE[kind]):
             try:
                 obj.close()
@@ -339,11 +339,18 @@ class Solver:
     FGMRES<float>(A32, FGMRES<float>(A16, R)))) with R the adaptive fp16
     Richardson over SDAINV or block-Jacobi ILU(0)."""
 
-    def __init__(self, ctx: Context, A: HostMatrix, params: Optional[_capi.Params] = None, **kw):
+    def __init__(self, ctx: Context, A: HostMatrix, params: Optional[_capi.Params] = None, factors=None, **kw):
+        """factors: optional (Z, W^T) HostMatrix pair used as the SDAINV
+        factors instead of computing them (f3r_solver_create_factors)."""
         p = params if params is not None else Params(**kw)
         h = C.c_void_p()
         v = A.view()
-        check(lib().f3r_solver_create(ctx._h, C.byref(v), C.byref(p), C.byref(h)))
+        if factors is None:
+            check(lib().f3r_solver_create(ctx._h, C.byref(v), C.byref(p), C.byref(h)))
+        else:
+            zv, wv = factors[0].view(), factors[1].view()
+            check(lib().f3r_solver_create_factors(ctx._h, C.byref(v), C.byref(p), C.byref(zv), C.byref(wv),
+                                                  C.byref(h)))
         self._h = h
         _LIVE["solver"].add(self)
         self.ctx = ctx

@@ -112,6 +112,17 @@ SIGNATURES = {
     "f3r_solver_info": (C.c_int, [_vp, C.POINTER(SellInfo), C.POINTER(C.c_int32)]),
     "f3r_solver_operate": (C.c_int, [_vp, C.c_int, C.c_int, _vp, C.c_int, _vp]),
     "f3r_solver_destroy": (None, [_vp]),
+    "f3r_solver_create_factors": (C.c_int, [_vp, C.POINTER(CSR), C.POINTER(Params), C.POINTER(CSR), C.POINTER(CSR),
+                                            _pp]),
+    "f3r_learned_create": (C.c_int, [_vp, C.c_int32, C.c_uint64, _pp]),
+    "f3r_learned_destroy": (None, [_vp]),
+    "f3r_learned_params": (C.c_int, [_vp, _vp, C.c_int32, C.POINTER(C.c_int64)]),
+    "f3r_learned_set_data": (C.c_int, [_vp, C.POINTER(CSR), C.c_int32, C.c_int32, C.POINTER(CSR), C.POINTER(CSR),
+                                       C.c_int32, _vp, _vp]),
+    "f3r_learned_evaluate": (C.c_int, [_vp, C.POINTER(C.c_double), _vp]),
+    "f3r_learned_train": (C.c_int, [_vp, C.c_int32, C.c_double, _vp]),
+    "f3r_learned_correct": (C.c_int, [_vp, C.POINTER(CSR), C.c_int32, C.c_int32, C.POINTER(CSR), C.POINTER(CSR),
+                                      C.c_int32, _vp, _vp, _vp]),
 }
 
 _lib = None

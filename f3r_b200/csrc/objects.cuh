@@ -69,7 +69,7 @@ struct Context {
 // Launches a kernel on the context's bookkeeping (every launch is counted,
 // so a solve can report how many kernels of this library it ran).
 template <typename... KP, typename... A>
-inline void launch_k(Context &c, void (*k)(KP...), int grid, int block, size_t smem, cudaStream_t st,
+inline void launch_k(Context &c, void (*k)(KP...), dim3 grid, int block, size_t smem, cudaStream_t st,
                             A &&...args) {
   k<<<grid, block, smem, st>>>(std::forward<A>(args)...);
   c.launches++;

@@ -801,9 +801,20 @@ struct Solver {
   }
 };
 
-static Status make_solver(f3r_context *ctx, const f3r_csr *a, const f3r_params *pp, Solver **out) {
+// zf / wf: given SDAINV factors (both or neither; precond SDAINV only)
+static Status make_solver(f3r_context *ctx, const f3r_csr *a, const f3r_params *pp, Solver **out,
+                          const f3r_csr *zf = nullptr, const f3r_csr *wf = nullptr) {
   F3R_TRY(check_csr(a));
   if (a->nrows != a->ncols) return fail(F3R_ERROR_INVALID_VALUE, "the system matrix must be square");
+  if ((zf != nullptr) != (wf != nullptr)) return fail(F3R_ERROR_INVALID_VALUE, "give both factors or neither");
+  if (zf) {
+    if (pp->precond != F3R_PRECOND_SDAINV)
+      return fail(F3R_ERROR_INVALID_VALUE, "given factors need precond F3R_PRECOND_SDAINV");
+    F3R_TRY(check_csr(zf));
+    F3R_TRY(check_csr(wf));
+    if (zf->nrows != a->nrows || zf->ncols != a->nrows || wf->nrows != a->nrows || wf->ncols != a->nrows)
+      return fail(F3R_ERROR_INVALID_VALUE, "the factors must be square and of the matrix's size");
+  }
   f3r_params p = *pp;
   if (p.m_outer < 1 || p.m_outer + 1 > kMaxCols || p.m2 < 1 || p.m2 + 1 > kMaxCols || p.m3 < 0 ||
       p.m3 + 1 > kMaxCols || p.m4 < 1 || p.m4 > kMaxM4 || p.c < 1 || p.max_restarts < 1 || p.static_weight < 0)
@@ -845,7 +856,19 @@ static Status make_solver(f3r_context *ctx, const f3r_csr *a, const f3r_params *
   std::memcpy(Ah.val.data(), a->val, sizeof(double) * a->nnz);
   if (p.precond == F3R_PRECOND_SDAINV) {
     HostCSR *zr = nullptr, *wr = nullptr;
-    F3R_TRY(sdainv(Ah, p.sdainv_tol, p.acc, &zr, &wr));
+    if (zf) {
+      auto copy = [](const f3r_csr &m) {
+        HostCSR *h = new HostCSR(m.nrows, m.ncols, m.nnz);
+        std::memcpy(h->rptr.data(), m.rptr, sizeof(int32_t) * (m.nrows + 1));
+        std::memcpy(h->idx.data(), m.idx, sizeof(int32_t) * m.nnz);
+        std::memcpy(h->val.data(), m.val, sizeof(double) * m.nnz);
+        return h;
+      };
+      zr = copy(*zf);
+      wr = copy(*wf);
+    } else {
+      F3R_TRY(sdainv(Ah, p.sdainv_tol, p.acc, &zr, &wr));
+    }
     std::unique_ptr<HostCSR> Zh(zr), Wh(wr);
     bool diag = true;
     for (int32_t i = 0; i < n && diag; i++) {
@@ -1263,6 +1286,14 @@ f3r_status f3r_solver_create(f3r_context *ctx, const f3r_csr *a, const f3r_param
   if (!ctx || !a || !p || !out) return fail(F3R_ERROR_INVALID_VALUE, "null argument");
   Solver *s = nullptr;
   F3R_TRY(make_solver(ctx, a, p, &s));
+  *out = new f3r_solver{s};
+  return F3R_SUCCESS;
+}
+f3r_status f3r_solver_create_factors(f3r_context *ctx, const f3r_csr *a, const f3r_params *p, const f3r_csr *z,
+                                     const f3r_csr *wt, f3r_solver **out) {
+  if (!ctx || !a || !p || !z || !wt || !out) return fail(F3R_ERROR_INVALID_VALUE, "null argument");
+  Solver *s = nullptr;
+  F3R_TRY(make_solver(ctx, a, p, &s, z, wt));
   *out = new f3r_solver{s};
   return F3R_SUCCESS;
 }

@@ -365,6 +365,51 @@ f3r_status f3r_solver_operate(f3r_solver *s, f3r_dtype val_t, f3r_dtype in_t, co
                               void *out);
 void f3r_solver_destroy(f3r_solver *s);
 
+/* As f3r_solver_create with precond F3R_PRECOND_SDAINV, but the SDAINV
+ * factors are given instead of computed: M r = Z (W^T r), Z and W^T square
+ * CSR of a's size (for example f3r_host_sdainv's factors with their values
+ * corrected by f3r_learned_correct).  The reference builds them itself
+ * (work/src/f3r-gpu.cpp:74). */
+f3r_status f3r_solver_create_factors(f3r_context *ctx, const f3r_csr *a, const f3r_params *p, const f3r_csr *z,
+                                     const f3r_csr *wt, f3r_solver **out);
+
+/* ---- learned correction of the SDAINV values ---------------------------
+ * No reference counterpart.  A network 7 -> 64 -> 64 -> 8 (ReLU) maps the
+ * seven coefficients of row i of a 7-point matrix in natural order (column
+ * offsets 0, -1, +1, -nx, +nx, -nx*ny, +nx*ny) to corrections delta of that
+ * row's SDAINV entries on their fixed pattern: Z entries at offsets
+ * {0, +1, +nx, +nx*ny} and W^T entries at {0, -1, -nx, -nx*ny} become
+ * v (1 + delta); entries at other offsets keep their values.  The output
+ * layer starts at zero (an untrained network is plain SDAINV).  Training
+ * (fp32 weights, hand-written forward / backward kernels, Adam) minimises
+ * 1/P sum_p ||Z' W'^T r_p - e_p||^2 / ||e_p||^2 over residual / error pairs;
+ * inference runs in BF16 on tensor cores with fp32 accumulation.
+ * Parameters, flat fp32: W1 (64 x 7), b1 (64), W2 (64 x 64), b2 (64),
+ * W3 (8 x 64), b3 (8); W row-major (outputs x inputs); 5192 in all. */
+typedef struct f3r_learned f3r_learned;
+/* hidden must be 64; seed draws the He-normal hidden layers */
+f3r_status f3r_learned_create(f3r_context *ctx, int32_t hidden, uint64_t seed, f3r_learned **out);
+void f3r_learned_destroy(f3r_learned *l);
+/* count (may be NULL) receives the parameter count; params (may be NULL)
+ * is read from the network (set = 0) or written to it (set != 0) */
+f3r_status f3r_learned_params(f3r_learned *l, float *params, int32_t set, int64_t *count);
+/* The training data: a 7-point matrix (several systems of one grid shape
+ * may be stacked block-diagonally), its grid strides nx and nx*ny, its
+ * SDAINV factors, and npairs (1..1024) pairs, r and e each npairs x n
+ * (pair-major, host memory), A e_p = r_p up to the solver's error. */
+f3r_status f3r_learned_set_data(f3r_learned *l, const f3r_csr *a, int32_t nx, int32_t ny, const f3r_csr *z,
+                                const f3r_csr *wt, int32_t npairs, const double *r, const double *e);
+/* loss at the current parameters; grad (may be NULL; 5192 floats) its gradient */
+f3r_status f3r_learned_evaluate(f3r_learned *l, double *loss, float *grad);
+/* steps full-batch Adam steps (beta 0.9 / 0.999); losses (may be NULL)
+ * receives the loss before each step */
+f3r_status f3r_learned_train(f3r_learned *l, int32_t steps, double lr, double *losses);
+/* Corrected factor values of a system: z_val / wt_val (nnz of z / wt) and,
+ * when delta is not NULL, the raw network outputs (n x 8).  bf16 != 0 runs
+ * the BF16 tensor-core inference, else the fp32 training forward pass. */
+f3r_status f3r_learned_correct(f3r_learned *l, const f3r_csr *a, int32_t nx, int32_t ny, const f3r_csr *z,
+                               const f3r_csr *wt, int32_t bf16, double *z_val, double *wt_val, float *delta);
+
 #ifdef __cplusplus
 }
 #endif
