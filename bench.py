@@ -50,10 +50,11 @@ NX = 192
 BETA = 0.5
 SIGMA = 1
 ALIGN = 1
-LAYOUTS = {"aligned": dict(sell_sigma=1, sell_align=1), "sigma256": dict(sell_sigma=256, sell_align=0)}
+LAYOUTS = {"aligned": dict(sell_sigma=1, sell_align=1, format=0), "sigma256": dict(sell_sigma=256, sell_align=0, format=0),
+           "csr": dict(sell_sigma=1, sell_align=0, format=1)}
 TOL = 1e-10
 PARAMS = dict(m_outer=100, max_restarts=20, m2=8, m3=4, m4=2, c=64, sdainv_tol=0.1, acc=1.0, sell_sigma=SIGMA,
-              sell_align=ALIGN,
+              sell_align=ALIGN, format=0,
               rel_tol=TOL, use_graphs=1)
 METRIC = "time to 1e-10 FP64 relative residual, plain F3R (fp64/fp32/fp16 nested FGMRES), 192^3 27-pt nonsymmetric"
 WORKLOAD = "F3R-SDAINV-SELL32al stencil27-halfspace beta0.5 192^3 (n=7077888, nnz=189119224), tol 1e-10"
@@ -71,6 +72,8 @@ def set_size(nx):
 
 
 def layout_tag():
+    if PARAMS.get("format"):
+        return "CSR"
     return "SELL32al" if PARAMS["sell_align"] else f"SELL32s{PARAMS['sell_sigma']}"
 
 
@@ -80,6 +83,8 @@ def set_layout(name):
 
 def layout_desc(p=None):
     p = PARAMS if p is None else p
+    if p.get("format"):
+        return {"format": "CSR", "index": "explicit int32"}
     return {"C": 32, "sigma": p["sell_sigma"],
             "index": "offset-aligned (no stored column index)" if p["sell_align"] else "explicit int32"}
 
@@ -235,16 +240,21 @@ def spmv_roofline(solver, A, torch, F):
     dt = e0.elapsed_time(e1) * 1e-3 / reps
     alg = nnz * (2 + 4) + 4 * (n + 1) + n * 4 + n * 4
     aligned = info.index_bits == 0
+    csr = info.slice_height == 0
     nslices = (n + 31) // 32
     idx_bytes = (info.nnz_padded // 32) * 4 if aligned else info.nnz_padded * 4
-    stored = info.nnz_padded * 2 + idx_bytes + 4 * (nslices + 1) + n * 4 + n * 4
+    stored = alg if csr else info.nnz_padded * 2 + idx_bytes + 4 * (nslices + 1) + n * 4 + n * 4
     peak, src = measured_peak()
     achieved = alg / dt / 1e9
-    kern = ("k_sell_cfg<__half,float,EpiStore<float>,24,2,32,AllAlignedIdx> (SELL-32 sigma=1, offset-aligned, "
-            "fp16 A, fp32 x, fp32 y)" if aligned else
-            f"k_sell_cfg<__half,float,EpiStore<float>,24,2,16,int> (SELL-32 sigma={info.sigma}, fp16 A, fp32 x, fp32 y)")
+    if csr:
+        kern = "k_csr_cfg<__half,float,EpiStore<float>,24> (CSR, fp16 A, fp32 x, fp32 y)"
+    elif aligned:
+        kern = ("k_sell_cfg<__half,float,EpiStore<float>,24,2,32,AllAlignedIdx> (SELL-32 sigma=1, offset-aligned, "
+                "fp16 A, fp32 x, fp32 y)")
+    else:
+        kern = f"k_sell_cfg<__half,float,EpiStore<float>,24,2,16,int> (SELL-32 sigma={info.sigma}, fp16 A, fp32 x, fp32 y)"
     return {"kernel": kern, "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "peak_source": src,
-            "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": profiled_traffic(aligned),
+            "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None if csr else profiled_traffic(aligned),
             "algorithmic_bytes": alg, "effective_rate": aligned, "stored_bytes": stored,
             "stored_achieved": round(stored / dt / 1e9, 1), "stored_frac": round(stored / dt / 1e9 / peak, 4),
             "launch_us": round(dt * 1e6, 2)}
@@ -721,7 +731,7 @@ def main():
     ap.add_argument("--ilu-blocks", type=int, default=112)
     ap.add_argument("--trsv-iters", type=int, default=2)
     ap.add_argument("--layout", default="aligned", choices=sorted(LAYOUTS),
-                    help="SELL layout of our arm: offset-aligned sigma=1 (default) or packed sigma=256")
+                    help="matrix layout of our arm: offset-aligned SELL sigma=1 (default), packed SELL sigma=256, or CSR")
     ap.add_argument("--no-alt-layout", action="store_true", help="skip timing the other layout")
     ap.add_argument("--config", default="c2", choices=["c2", "c3", "c4", "c5"],
                     help="c2: the headline solve; c3: the precision stress (256^3 diffusion, per-level errors); "

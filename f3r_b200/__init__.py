@@ -18,10 +18,11 @@ from typing import Callable, Optional
 import numpy as np
 
 from . import _capi
-from ._capi import (F16, F32, F64, PRECOND_ILU0_BAJ, PRECOND_ILU0_BJ, PRECOND_ILU0_JACOBI, PRECOND_SDAINV, TRSV_BAJ,
-                    TRSV_D_UPPER, TRSV_JACOBI, TRSV_LOWER, TRSV_LOWER_D, F3RError, check, lib)
+from ._capi import (F16, F32, F64, FORMAT_CSR, FORMAT_SELL, PRECOND_ILU0_BAJ, PRECOND_ILU0_BJ, PRECOND_ILU0_JACOBI,
+                    PRECOND_ILU0_LEVEL, PRECOND_SDAINV, TRSV_BAJ, TRSV_D_UPPER, TRSV_JACOBI, TRSV_LOWER, TRSV_LOWER_D, F3RError, check, lib)
 
 __all__ = ["HostMatrix", "Context", "Sell", "Solver", "Params", "solve_res_t", "F3RError", "F64", "F32", "F16",
+           "FORMAT_SELL", "FORMAT_CSR", "PRECOND_ILU0_LEVEL",
            "PRECOND_SDAINV", "PRECOND_ILU0_BJ", "PRECOND_ILU0_JACOBI", "PRECOND_ILU0_BAJ", "Trsv", "TRSV_LOWER",
            "TRSV_LOWER_D", "TRSV_D_UPPER", "TRSV_JACOBI", "TRSV_BAJ", "stencil27", "diffusion7", "random_uniform", "host_spmv",
            "read_matrix", "read_system", "read_vector", "write_vector", "CSV_HEADER", "csv_row", "solve_batch"]
@@ -237,8 +238,10 @@ class Sell:
     compute_residual on device tensors."""
 
     def __init__(self, ctx: Context, A: HostMatrix, sigma: int = 1, dtypes=(F64, F32, F16), index16: bool = False,
-                 aligned: bool = False):
-        mask = (_capi.SELL_INDEX16 if index16 else 0) | (_capi.SELL_ALIGNED if aligned else 0)
+                 aligned: bool = False, csr: bool = False):
+        """csr: keep the matrix in CSR (F3R_SELL_CSR) instead of SELL-32"""
+        mask = ((_capi.SELL_INDEX16 if index16 else 0) | (_capi.SELL_ALIGNED if aligned else 0) |
+                (_capi.SELL_CSR if csr else 0))
         for d in dtypes:
             mask |= 1 << d
         h = C.c_void_p()

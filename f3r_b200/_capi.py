@@ -16,8 +16,10 @@ STATUS = {0: "SUCCESS", 1: "INVALID_VALUE", 2: "CUDA", 3: "OUT_OF_MEMORY", 5: "B
           8: "UNSUPPORTED", 9: "NO_DEVICE"}
 F64, F32, F16 = 0, 1, 2
 SELL_INDEX16 = 1 << 8
+SELL_CSR = 1 << 10
+FORMAT_SELL, FORMAT_CSR = 0, 1
 SELL_ALIGNED = 1 << 9
-PRECOND_SDAINV, PRECOND_ILU0_BJ, PRECOND_ILU0_JACOBI, PRECOND_ILU0_BAJ = 0, 1, 2, 3
+PRECOND_SDAINV, PRECOND_ILU0_BJ, PRECOND_ILU0_JACOBI, PRECOND_ILU0_BAJ, PRECOND_ILU0_LEVEL = 0, 1, 2, 3, 4
 TRSV_LOWER, TRSV_LOWER_D, TRSV_D_UPPER = 0, 1, 2
 TRSV_JACOBI, TRSV_BAJ = 0, 1
 
@@ -39,7 +41,7 @@ class Params(C.Structure):
                 ("sdainv_tol", C.c_double), ("acc", C.c_double), ("sell_c", C.c_int32), ("sell_sigma", C.c_int32),
                 ("rel_tol", C.c_double), ("half_scale_log2", C.c_int32), ("use_graphs", C.c_int32),
                 ("sell_index16", C.c_int32), ("static_weight", C.c_double), ("trsv_iters", C.c_int32),
-                ("reserved0", C.c_int32), ("trsv_omega", C.c_double), ("inner_sstep", C.c_int32),
+                ("format", C.c_int32), ("trsv_omega", C.c_double), ("inner_sstep", C.c_int32),
                 ("sell_align", C.c_int32), ("reserved", C.c_int32 * 8)]
 
 

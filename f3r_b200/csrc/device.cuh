@@ -9,7 +9,7 @@
 namespace f3r {
 
 // Device-side error codes written to the context's error word.
-enum DevError : int { DEV_OK = 0, DEV_TIMEOUT_SPMV = 1, DEV_BREAKDOWN = 2 };
+enum DevError : int { DEV_OK = 0, DEV_TIMEOUT_SPMV = 1, DEV_BREAKDOWN = 2, DEV_TIMEOUT_TRSV = 3 };
 
 // Threads per block of the elementwise / reduction kernels.
 constexpr int kEwThreads = 256;

@@ -168,4 +168,184 @@ struct IluDevice {
   }
 };
 
+// ---------------------------------------------------------------------------
+// Global ILU(0), level-scheduled over the whole GPU (F3R_PRECOND_ILU0_LEVEL).
+//
+// One factor of the global (single-block) ILU(0) is solved by one kernel
+// without grid barriers.  The rows are listed level by level, every level
+// padded with -1 to whole 32-row chunks, so the 32 rows of a chunk never read
+// each other.  Warps take chunks in list order from an atomic counter; a row
+// waits until each row it reads carries this launch's generation in its flag
+// (acquire load), then computes exactly as k_trsv_bj does (same order of
+// terms, same roundings) and publishes value then flag (release store).  A
+// warp waits only on chunks taken before its own by running warps, and the
+// lowest unfinished chunk never waits, so the solve always completes.  Every
+// wait is bounded (kWaitLimitNs); the first timeout sets the device error
+// word, which ends every other wait of the launch at once.  The last block to
+// finish resets the counter and advances the generation, so back-to-back
+// launches (and graph replays) need no host work.
+struct IluLevelTri {
+  int32_t *rptr = nullptr, *idx = nullptr;  // idx mapped to vector positions
+  __half *val = nullptr;
+  __half *dinv = nullptr;                   // upper only
+  int32_t *order = nullptr;                 // rows level by level, -1 padded to 32-row chunks
+  int32_t nchunks = 0;
+  int32_t nlevels = 0;
+  int32_t *flag = nullptr;                  // per vector position: generation of its last write
+  unsigned int *state = nullptr;            // chunk counter, finished-block ticket, generation
+};
+
+__device__ __forceinline__ unsigned int ld_acquire_u32(const int32_t *p) {
+  unsigned int v;
+  asm volatile("ld.acquire.gpu.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_u32(int32_t *p, unsigned int v) {
+  asm volatile("st.release.gpu.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+template <bool UPPER>
+__global__ void __launch_bounds__(256) k_trsv_level(IluLevelTri T, const int32_t *__restrict__ rowpos,
+                                                    const __half *__restrict__ in, __half *out,
+                                                    const __half *__restrict__ ome, int *err) {
+  __shared__ unsigned int gen_s;
+  if (threadIdx.x == 0) gen_s = *(volatile unsigned int *)&T.state[2] + 1u;
+  __syncthreads();
+  const unsigned int gen = gen_s;
+  const int lane = threadIdx.x & 31;
+  const float om = ome ? __half2float(*ome) : 1.0f;
+  volatile int *verr = err;
+  bool abort = false;
+  while (true) {
+    unsigned int c = 0;
+    if (lane == 0) c = atomicAdd(&T.state[0], 1u);
+    c = __shfl_sync(0xffffffffu, c, 0);
+    if (c >= (unsigned int)T.nchunks) break;
+    const int32_t i = T.order[(size_t)c * 32 + lane];
+    if (i >= 0) {
+      const int32_t p = rowpos[i];
+      float t = __half2float(in[p]);
+      const int32_t b = T.rptr[i], e = T.rptr[i + 1];
+      // lower: off-diagonals by increasing column (last entry = unit diagonal);
+      // upper: by decreasing column (first entry = diagonal)
+      const int32_t j0 = UPPER ? e - 1 : b, j1 = UPPER ? b : e - 1, dj = UPPER ? -1 : 1;
+      for (int32_t j = j0; j != j1; j += dj) {
+        const int32_t q = T.idx[j];
+        if (!abort && ld_acquire_u32(T.flag + q) != gen) {
+          const unsigned long long t0 = global_ns();
+          int polls = 0;
+          while (ld_acquire_u32(T.flag + q) != gen) {
+            if (*verr != 0) {
+              abort = true;
+              break;
+            }
+            if (++polls > 8) __nanosleep(64);
+            if (global_ns() - t0 > kWaitLimitNs) {
+              atomicCAS(err, 0, (int)DEV_TIMEOUT_TRSV);
+              abort = true;
+              break;
+            }
+          }
+        }
+        t = __fmaf_rn(-__half2float(T.val[j]), __half2float(__ldcg(out + q)), t);
+      }
+      __half h;
+      if (!UPPER) {
+        h = __float2half_rn(t);
+      } else {
+        h = __float2half_rn(t * __half2float(T.dinv[i]));
+        if (ome) h = __float2half_rn(__half2float(h) * om);
+      }
+      out[p] = h;
+      __threadfence();
+      st_release_u32(T.flag + p, gen);
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const unsigned int tk = atomicAdd(&T.state[1], 1u);
+    if (tk == gridDim.x - 1) {
+      T.state[0] = 0;
+      T.state[1] = 0;
+      __threadfence();
+      atomicAdd(&T.state[2], 1u);
+    }
+  }
+}
+
+struct IluLevel {
+  IluLevelTri L, U;
+  int32_t *rowpos = nullptr;
+  int grid = 0;
+  std::vector<void *> allocs;
+
+  template <typename T> cudaError_t up(T **d, const std::vector<T> &h) {
+    cudaError_t e = cudaMalloc((void **)d, sizeof(T) * std::max<size_t>(h.size(), 1));
+    if (e != cudaSuccess) return e;
+    allocs.push_back((void *)*d);
+    return cudaMemcpy(*d, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice);
+  }
+  void release() {
+    for (void *p : allocs) cudaFree(p);
+    allocs.clear();
+  }
+
+  Status build_tri(IluLevelTri &T, const HostCSR &M, bool upper, const std::vector<int32_t> &pos) {
+    const int32_t n = M.n;
+    std::vector<int32_t> order, lvl_off, blk_lvl, idx(M.idx.size());
+    int32_t nl = 0;
+    IluDevice::levels(M, upper, std::vector<int32_t>{0, n}, order, lvl_off, blk_lvl, nl);
+    std::vector<int32_t> padded;
+    padded.reserve(order.size() + (size_t)nl * 32);
+    for (int32_t l = 0; l + 1 < (int32_t)lvl_off.size(); l++) {
+      for (int32_t q = lvl_off[l]; q < lvl_off[l + 1]; q++) padded.push_back(order[q]);
+      while (padded.size() % 32) padded.push_back(-1);
+    }
+    T.nchunks = (int32_t)(padded.size() / 32);
+    T.nlevels = nl;
+    for (size_t j = 0; j < M.idx.size(); j++) idx[j] = pos[M.idx[j]];
+    std::vector<double> v(M.val.begin(), M.val.end()), dinv;
+    if (upper) {
+      dinv.resize(n);
+      for (int32_t i = 0; i < n; i++) dinv[i] = 1.0 / M.val[M.rptr[i]];
+    }
+    const std::vector<int32_t> zeros(std::max(n, 1), 0);
+    const std::vector<unsigned int> st(3, 0u);
+    if (up(&T.rptr, M.rptr) != cudaSuccess || up(&T.idx, idx) != cudaSuccess ||
+        up(&T.order, padded) != cudaSuccess || up(&T.flag, zeros) != cudaSuccess || up(&T.state, st) != cudaSuccess)
+      return fail(F3R_ERROR_CUDA, "ILU upload failed");
+    F3R_TRY(half_copy(&T.val, v));
+    if (upper) F3R_TRY(half_copy(&T.dinv, dinv));
+    return F3R_SUCCESS;
+  }
+
+  Status half_copy(__half **d, const std::vector<double> &v);
+
+  Status build(int sm_count, const HostCSR &Lh, const HostCSR &Uh, const std::vector<int32_t> &perm, bool permuted) {
+    const int32_t n = Lh.n;
+    std::vector<int32_t> pos(n);
+    for (int32_t i = 0; i < n; i++) pos[i] = i;
+    if (permuted)
+      for (int32_t s = 0; s < n; s++) pos[perm[s]] = s;
+    if (up(&rowpos, pos) != cudaSuccess) return fail(F3R_ERROR_CUDA, "ILU upload failed");
+    F3R_TRY(build_tri(L, Lh, false, pos));
+    F3R_TRY(build_tri(U, Uh, true, pos));
+    // enough warps to work several levels ahead, few enough that the spinning
+    // ones leave the L2 to the rows being computed
+    const int32_t chunks = std::max(L.nchunks, U.nchunks);
+    grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)sm_count * 4, (chunks + 7) / 8));
+    return F3R_SUCCESS;
+  }
+
+  // out = U^-1 L^-1 x (tmp holds L^-1 x); ome (nullable) scales the result
+  Status apply(cudaStream_t st, const __half *x, __half *tmp, __half *out, const __half *ome, int *err) const {
+    k_trsv_level<false><<<grid, 256, 0, st>>>(L, rowpos, x, tmp, nullptr, err);
+    k_trsv_level<true><<<grid, 256, 0, st>>>(U, rowpos, tmp, out, ome, err);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(F3R_ERROR_CUDA, std::string("ILU trsv launch: ") + cudaGetErrorString(e));
+    return F3R_SUCCESS;
+  }
+};
+
 }  // namespace f3r

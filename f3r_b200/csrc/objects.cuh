@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "internal.hpp"
+#include "csr.cuh"
 #include "sell.cuh"
 
 namespace f3r {
@@ -61,6 +62,8 @@ struct Context {
     CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(int), stream));
     CUDA_TRY(cudaStreamSynchronize(stream));
     if (e == DEV_TIMEOUT_SPMV) return fail(F3R_ERROR_TIMEOUT, "a bulk-copy wait in the SpMV kernel exceeded its bound");
+    if (e == DEV_TIMEOUT_TRSV)
+      return fail(F3R_ERROR_TIMEOUT, "a dependency wait in the level-scheduled ILU solve exceeded its bound");
     return fail(F3R_ERROR_BREAKDOWN, "zero or non-finite norm in an Arnoldi step");
   }
 };
@@ -81,6 +84,7 @@ struct DeviceSell {
   int64_t nnz = 0, nnz_pad = 0;
   int32_t *col = nullptr, *sptr = nullptr, *perm = nullptr, *cbase = nullptr, *cbptr = nullptr;
   int32_t *xoff = nullptr;  // mixed aligned form: per slice, -1 or the explicit indices' offset
+  int32_t *rptr = nullptr;  // CSR storage (col = CSR indices, values unpadded), else nullptr
   uint16_t *dcol = nullptr;
   double *v64 = nullptr;
   float *v32 = nullptr;
@@ -88,12 +92,14 @@ struct DeviceSell {
   int dtypes = 0;
   // 32, 16, or 0 (offset-aligned slices, mixed with explicit ones or not)
   int index_bits() const { return (xoff || (cbase && !dcol)) ? 0 : dcol ? 16 : 32; }
-  DevSell view() const { return DevSell{col, dcol, cbase, cbptr, xoff, sptr, perm, n, ncols, nslices}; }
+  DevSell view() const { return DevSell{col, dcol, cbase, cbptr, xoff, sptr, perm, n, ncols, nslices, rptr}; }
   void release() {
     cudaFree(col); cudaFree(sptr); cudaFree(perm); cudaFree(cbase); cudaFree(cbptr); cudaFree(dcol);
     cudaFree(xoff);
+    cudaFree(rptr);
     cbptr = nullptr;
     xoff = nullptr;
+    rptr = nullptr;
     cudaFree(v64); cudaFree(v32); cudaFree(v16);
     col = sptr = perm = cbase = nullptr; dcol = nullptr; v64 = nullptr; v32 = nullptr; v16 = nullptr;
   }
@@ -119,6 +125,8 @@ inline Status sell_attr(Context &c) {
     F3R_TRY((sell_attr_one<V, X, Epi, uint16_t>()));
     F3R_TRY((sell_attr_one<V, X, Epi, AlignedIdx>()));
     F3R_TRY((sell_attr_one<V, X, Epi, AllAlignedIdx>()));
+    CUDA_TRY(cudaFuncSetAttribute(k_csr_cfg<V, X, Epi, SellCfg<V, int32_t>::WARPS>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csr_smem_bytes<V>()));
     attr_done[c.device & 63] = 1;
   }
   return F3R_SUCCESS;
@@ -136,7 +144,12 @@ template <typename V, typename X, typename Epi>
 inline Status launch_sell(Context &c, const V *val, const DevSell &A, const X *x, const Epi &epi) {
   if (A.nslices == 0) return F3R_SUCCESS;
   F3R_TRY((sell_attr<V, X, Epi>(c)));
-  if (A.xoff) launch_sell_one<V, X, Epi, AlignedIdx>(c, val, A, x, epi);
+  if (A.rptr) {
+    // the packed kernel's geometry (rows per thread, CTAs), so sums and partials match it
+    constexpr int W = SellCfg<V, int32_t>::WARPS;
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(cdiv(A.nslices, W), c.sm_count));
+    launch_k(c, k_csr_cfg<V, X, Epi, W>, grid, W * 32, csr_smem_bytes<V>(), c.stream, val, A, x, epi, c.err);
+  } else if (A.xoff) launch_sell_one<V, X, Epi, AlignedIdx>(c, val, A, x, epi);
   else if (A.cbase && !A.dcol) launch_sell_one<V, X, Epi, AllAlignedIdx>(c, val, A, x, epi);
   else if (A.dcol) launch_sell_one<V, X, Epi, uint16_t>(c, val, A, x, epi);
   else launch_sell_one<V, X, Epi, int32_t>(c, val, A, x, epi);
@@ -172,6 +185,8 @@ bool compress_index16(SellHost &s);
 double align_offsets(const f3r_csr &a, bool renumber, SellHost &s);
 // Uploads the value copies selected by dtype_mask (bit 1 << f3r_dtype).
 Status upload_sell(Context &c, const SellHost &h, int dtype_mask, bool scatter_perm, DeviceSell &d);
+// CSR storage with the same value copies (the kernels' CSR path; sigma 1)
+Status upload_csr(Context &c, const f3r_csr &a, int dtype_mask, DeviceSell &d);
 
 }  // namespace f3r
 

@@ -65,6 +65,7 @@ struct DevSell {
   int32_t n;              // rows (outputs written only for storage rows < n)
   int32_t ncols;
   int32_t nslices;
+  const int32_t *rptr;    // CSR storage: row pointers (col holds the CSR indices), else nullptr
 };
 
 // Index form of a kernel instantiation.

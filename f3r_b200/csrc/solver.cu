@@ -320,7 +320,44 @@ Status upload_sell(Context &c, const SellHost &h, int dtype_mask, bool scatter_p
 // ---------------------------------------------------------------------------
 // SpMV launcher
 // ---------------------------------------------------------------------------
-Status IluDevice::to_half(__half **d, const std::vector<double> &v) {
+Status upload_csr(Context &c, const f3r_csr &a, int dtype_mask, DeviceSell &d) {
+  const int32_t n = a.nrows;
+  const size_t nz = (size_t)a.nnz;
+  d.n = n;
+  d.ncols = a.ncols;
+  d.nslices = (int32_t)cdiv(n, 32);
+  d.sigma = 1;
+  d.nnz = a.nnz;
+  d.nnz_pad = a.nnz;
+  d.dtypes = dtype_mask;
+  int32_t mw = 0;
+  for (int32_t i = 0; i < n; i++) mw = std::max(mw, a.rptr[i + 1] - a.rptr[i]);
+  d.max_width = mw;
+  F3R_TRY(c.alloc((void **)&d.rptr, ((size_t)n + 1) * 4));
+  F3R_TRY(c.alloc((void **)&d.col, std::max<size_t>(nz, 1) * 4));
+  CUDA_TRY(cudaMemcpyAsync(d.rptr, a.rptr, ((size_t)n + 1) * 4, cudaMemcpyHostToDevice, c.stream));
+  if (nz) CUDA_TRY(cudaMemcpyAsync(d.col, a.idx, nz * 4, cudaMemcpyHostToDevice, c.stream));
+  double *tmp64 = nullptr;
+  F3R_TRY(c.alloc((void **)&tmp64, std::max<size_t>(nz, 1) * 8));
+  if (nz) CUDA_TRY(cudaMemcpyAsync(tmp64, a.val, nz * 8, cudaMemcpyHostToDevice, c.stream));
+  const int g = c.ew_grid((int64_t)nz);
+  if (dtype_mask & (1 << F3R_F32)) {
+    F3R_TRY(c.alloc((void **)&d.v32, std::max<size_t>(nz, 1) * 4));
+    launch_k(c, k_convert_vals<float>, g, kEwThreads, 0, c.stream, tmp64, d.v32, (int64_t)nz);
+  }
+  if (dtype_mask & (1 << F3R_F16)) {
+    F3R_TRY(c.alloc((void **)&d.v16, std::max<size_t>(nz, 1) * 2));
+    launch_k(c, k_convert_vals<__half>, g, kEwThreads, 0, c.stream, tmp64, d.v16, (int64_t)nz);
+  }
+  CUDA_TRY(cudaGetLastError());
+  CUDA_TRY(cudaStreamSynchronize(c.stream));
+  if (dtype_mask & (1 << F3R_F64)) d.v64 = tmp64;
+  else cudaFree(tmp64);
+  return F3R_SUCCESS;
+}
+
+// fp16 copy of fp64 values (rounded once on the device), recorded in allocs
+static Status half_upload(std::vector<void *> &allocs, __half **d, const std::vector<double> &v) {
   double *tmp = nullptr;
   const size_t nb = std::max<size_t>(v.size(), 1);
   CUDA_TRY(cudaMalloc((void **)&tmp, nb * sizeof(double)));
@@ -338,6 +375,8 @@ Status IluDevice::to_half(__half **d, const std::vector<double> &v) {
   cudaFree(tmp);
   return F3R_SUCCESS;
 }
+Status IluDevice::to_half(__half **d, const std::vector<double> &v) { return half_upload(allocs, d, v); }
+Status IluLevel::half_copy(__half **d, const std::vector<double> &v) { return half_upload(allocs, d, v); }
 
 }  // namespace f3r
 
@@ -367,6 +406,7 @@ struct Solver {
   __half *wd = nullptr, *zd = nullptr;
   DeviceSell W, Z;    // general SDAINV factors (permuted system)
   IluDevice ilu;      // block-Jacobi ILU(0), level scheduled
+  IluLevel ilul;      // global ILU(0), level scheduled over the whole GPU
   JacobiTrsv jl, ju;  // the same factors solved by Jacobi / BAJ sweeps
   // levels
   Level<double> L1;
@@ -392,7 +432,7 @@ struct Solver {
   ~Solver() {
     for (auto &kv : graphs) cudaGraphExecDestroy(kv.second.first);
     for (void *q : allocs) cudaFree(q);
-    A.release(); W.release(); Z.release(); ilu.release(); jl.release(); ju.release();
+    A.release(); W.release(); Z.release(); ilu.release(); ilul.release(); jl.release(); ju.release();
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
   }
@@ -478,6 +518,9 @@ struct Solver {
       F3R_TRY(launch_sell(C(), Z.v16, Z.view(), (const __half *)tmp, EpiZScale{out, rs, scale_ome ? 1 : 0}));
     } else if (p.precond == F3R_PRECOND_ILU0_BJ) {
       F3R_TRY(ilu.apply(C().stream, x, tmp, out, scale_ome ? &rs->ome[0] : nullptr));
+      C().launches += 2;
+    } else if (p.precond == F3R_PRECOND_ILU0_LEVEL) {
+      F3R_TRY(ilul.apply(C().stream, x, tmp, out, scale_ome ? &rs->ome[0] : nullptr, C().err));
       C().launches += 2;
     } else {
       F3R_TRY(jl.apply(C(), x, tmp, nullptr));
@@ -822,7 +865,10 @@ static Status make_solver(f3r_context *ctx, const f3r_csr *a, const f3r_params *
                 "need 1 <= m_outer, m2 <= 127, 0 <= m3 <= 127, 1 <= m4 <= 16, c >= 1, max_restarts >= 1, "
                 "static_weight >= 0");
   if (p.sell_c != 32) return fail(F3R_ERROR_UNSUPPORTED, "only SELL slice height 32 is implemented");
-  if (p.precond < F3R_PRECOND_SDAINV || p.precond > F3R_PRECOND_ILU0_BAJ)
+  if (p.format != F3R_FORMAT_SELL && p.format != F3R_FORMAT_CSR) return fail(F3R_ERROR_INVALID_VALUE, "unknown format");
+  if (p.format == F3R_FORMAT_CSR && (p.sell_sigma != 1 || p.sell_align || p.sell_index16))
+    return fail(F3R_ERROR_INVALID_VALUE, "format CSR takes no SELL options (sigma 1, no alignment, 32-bit indices)");
+  if (p.precond < F3R_PRECOND_SDAINV || p.precond > F3R_PRECOND_ILU0_LEVEL)
     return fail(F3R_ERROR_INVALID_VALUE, "unknown preconditioner");
   if (p.half_scale_log2 < 0 || p.half_scale_log2 > 20) return fail(F3R_ERROR_INVALID_VALUE, "half_scale_log2 in [0, 20]");
   if (p.inner_sstep < 0 || p.inner_sstep > 3) return fail(F3R_ERROR_INVALID_VALUE, "inner_sstep is a 2-bit mask");
@@ -834,16 +880,24 @@ static Status make_solver(f3r_context *ctx, const f3r_csr *a, const f3r_params *
   const int32_t n = a->nrows;
   CUDA_TRY(cudaSetDevice(ctx->device));
   // system matrix in SELL-C-sigma order with all three value copies
-  SellHost h;
-  F3R_TRY(build_sell(*a, p.sell_sigma, true, h));
-  const std::vector<int32_t> hperm = h.perm;
-  if (p.sell_align) {
-    if (align_offsets(*a, true, h) < 0) return fail(F3R_ERROR_UNSUPPORTED, "padded matrix exceeds 2^31 entries");
-  } else if (p.sell_index16) {
-    compress_index16(h);
-  }
-  F3R_TRY(upload_sell(*ctx, h, (1 << F3R_F64) | (1 << F3R_F32) | (1 << F3R_F16), false, s->A));
-  h = SellHost();  // release the host copy (up to several GB)
+  const bool csr = p.format == F3R_FORMAT_CSR;
+  const int all_types = (1 << F3R_F64) | (1 << F3R_F32) | (1 << F3R_F16);
+  std::vector<int32_t> hperm;
+  if (csr) {
+    hperm.resize(n);
+    for (int32_t i = 0; i < n; i++) hperm[i] = i;
+    F3R_TRY(upload_csr(*ctx, *a, all_types, s->A));
+  } else {
+    SellHost h;
+    F3R_TRY(build_sell(*a, p.sell_sigma, true, h));
+    hperm = h.perm;
+    if (p.sell_align) {
+      if (align_offsets(*a, true, h) < 0) return fail(F3R_ERROR_UNSUPPORTED, "padded matrix exceeds 2^31 entries");
+    } else if (p.sell_index16) {
+      compress_index16(h);
+    }
+    F3R_TRY(upload_sell(*ctx, h, all_types, false, s->A));
+  }  // the host copy (up to several GB) is released here
   s->perm = hperm;
   if (p.sell_sigma > 1) {
     F3R_TRY(s->alloc(&s->perm_d, (size_t)std::max(n, 1)));
@@ -894,9 +948,13 @@ static Status make_solver(f3r_context *ctx, const f3r_csr *a, const f3r_params *
       CUDA_TRY(cudaStreamSynchronize(ctx->stream));
       cudaFree(tmp);
     } else {
-      // W^T and Z as SELL matrices of the permuted system (same sigma order)
+      // W^T and Z as SELL matrices of the permuted system (same sigma order), or CSR
       SellHost hw, hz;
       f3r_csr wv = Wh->view(), zv = Zh->view();
+      if (csr) {
+        F3R_TRY(upload_csr(*ctx, wv, 1 << F3R_F16, s->W));
+        F3R_TRY(upload_csr(*ctx, zv, 1 << F3R_F16, s->Z));
+      } else {
       F3R_TRY(build_sell(wv, p.sell_sigma, true, hw, &hperm));
       F3R_TRY(build_sell(zv, p.sell_sigma, true, hz, &hperm));
       if (p.sell_align) {
@@ -908,14 +966,18 @@ static Status make_solver(f3r_context *ctx, const f3r_csr *a, const f3r_params *
       }
       F3R_TRY(upload_sell(*ctx, hw, 1 << F3R_F16, false, s->W));
       F3R_TRY(upload_sell(*ctx, hz, 1 << F3R_F16, false, s->Z));
+      }
     }
   } else {
     HostCSR *lr = nullptr, *ur = nullptr;
     std::vector<int32_t> bptr;
-    F3R_TRY(ilu0_bj(Ah, p.ilu_blocks, p.acc, &lr, &ur, &bptr));
+    const bool global = p.precond == F3R_PRECOND_ILU0_LEVEL;
+    F3R_TRY(ilu0_bj(Ah, global ? 1 : p.ilu_blocks, p.acc, &lr, &ur, &bptr));
     std::unique_ptr<HostCSR> Lh(lr), Uh(ur);
     if (p.precond == F3R_PRECOND_ILU0_BJ) {
       F3R_TRY(s->ilu.build(ctx->stream, *Lh, *Uh, hperm, p.sell_sigma > 1, bptr));
+    } else if (global) {
+      F3R_TRY(s->ilul.build(ctx->sm_count, *Lh, *Uh, hperm, p.sell_sigma > 1));
     } else {
       const int kind = p.precond == F3R_PRECOND_ILU0_BAJ ? TRSV_BAJ : TRSV_JACOBI;
       F3R_TRY(jacobi_trsv_prepare(*ctx));
@@ -1157,11 +1219,24 @@ f3r_status f3r_sell_create(f3r_context *ctx, const f3r_csr *a, int32_t slice_hei
                            int32_t dtype_mask, f3r_sell **out) {
   if (!ctx || !out) return fail(F3R_ERROR_INVALID_VALUE, "null argument");
   if (slice_height != 32) return fail(F3R_ERROR_UNSUPPORTED, "only slice height 32 is implemented");
-  if ((dtype_mask & 7) == 0 || (dtype_mask & ~(7 | F3R_SELL_INDEX16 | F3R_SELL_ALIGNED)))
+  if ((dtype_mask & 7) == 0 || (dtype_mask & ~(7 | F3R_SELL_INDEX16 | F3R_SELL_ALIGNED | F3R_SELL_CSR)))
     return fail(F3R_ERROR_INVALID_VALUE,
-                "dtype_mask must select f64/f32/f16 (plus F3R_SELL_INDEX16 or F3R_SELL_ALIGNED)");
+                "dtype_mask must select f64/f32/f16 (plus F3R_SELL_INDEX16, F3R_SELL_ALIGNED or F3R_SELL_CSR)");
   F3R_TRY(check_csr(a));
   CUDA_TRY(cudaSetDevice(ctx->device));
+  if (dtype_mask & F3R_SELL_CSR) {
+    if (sigma != 1 || (dtype_mask & (F3R_SELL_INDEX16 | F3R_SELL_ALIGNED)))
+      return fail(F3R_ERROR_INVALID_VALUE, "F3R_SELL_CSR takes sigma 1 and no other layout flag");
+    auto m = std::make_unique<f3r_sell>();
+    m->ctx = ctx;
+    Status s = upload_csr(*ctx, *a, dtype_mask & 7, m->d);
+    if (s != F3R_SUCCESS) {
+      m->d.release();
+      return s;
+    }
+    *out = m.release();
+    return F3R_SUCCESS;
+  }
   SellHost h;
   F3R_TRY(build_sell(*a, sigma, false, h));
   if (dtype_mask & F3R_SELL_ALIGNED) {
@@ -1184,7 +1259,7 @@ f3r_status f3r_sell_info_get(const f3r_sell *m, f3r_sell_info *info) {
   info->nrows = m->d.n;
   info->ncols = m->d.ncols;
   info->nnz = (int32_t)m->d.nnz;
-  info->slice_height = 32;
+  info->slice_height = m->d.rptr ? 0 : 32;
   info->sigma = m->d.sigma;
   info->nslices = m->d.nslices;
   info->nnz_padded = m->d.nnz_pad;
@@ -1310,7 +1385,7 @@ f3r_status f3r_solver_info(const f3r_solver *s, f3r_sell_info *a_info, int32_t *
     a_info->nrows = d.n;
     a_info->ncols = d.ncols;
     a_info->nnz = (int32_t)d.nnz;
-    a_info->slice_height = 32;
+    a_info->slice_height = d.rptr ? 0 : 32;
     a_info->sigma = d.sigma;
     a_info->nslices = d.nslices;
     a_info->nnz_padded = d.nnz_pad;

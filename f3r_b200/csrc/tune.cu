@@ -121,6 +121,7 @@ extern "C" f3r_status f3r_sell_tune(f3r_sell *m, f3r_dtype val_t, int32_t reps, 
   if (!m || !out || !count || cap < 1 || reps < 1) return fail(F3R_ERROR_INVALID_VALUE, "bad argument");
   const DeviceSell &d = m->d;
   if (!(d.dtypes & (1 << val_t))) return fail(F3R_ERROR_INVALID_VALUE, "matrix holds no copy of that value type");
+  if (d.rptr) return fail(F3R_ERROR_UNSUPPORTED, "the launch shapes tuned are the SELL kernel's; this matrix is CSR");
   std::vector<f3r_tune_entry> res;
   Context &c = *m->ctx;
   if (val_t == F3R_F16) F3R_TRY((run<__half, float, float>(c, d, d.v16, reps, res)));

@@ -53,8 +53,11 @@ typedef enum f3r_precond {
                                   work/src/f3r.cpp:57-58,200-201 */
   F3R_PRECOND_ILU0_JACOBI = 2, /* the same ILU(0) factors, triangular solves by trsv_iters
                                   Jacobi sweeps (trsv/jacobi.hpp:290-505) */
-  F3R_PRECOND_ILU0_BAJ = 3     /* ... by trsv_iters in-place BAJ sweeps (trsv/baj.hpp:95-190);
+  F3R_PRECOND_ILU0_BAJ = 3,    /* ... by trsv_iters in-place BAJ sweeps (trsv/baj.hpp:95-190);
                                   results depend on scheduling before convergence */
+  F3R_PRECOND_ILU0_LEVEL = 4   /* one global ILU(0) (ilu_blocks ignored: ilu.hpp:128-164 with
+                                  one block), exact triangular solves level-scheduled over the
+                                  whole GPU; the same values as ILU0_BJ with ilu_blocks = 1 */
 } f3r_precond;
 
 /* Host CSR matrix, borrowed for the duration of a call.  Rows sorted by
@@ -97,7 +100,9 @@ typedef struct f3r_params {
                               work/src/static.cpp:99-114) */
   int32_t trsv_iters;      /* ILU0_JACOBI: sweeps per triangular solve (Jacobi max_ier, 2);
                               ILU0_BAJ: BAJ max_iter (the first is the diagonal scaling) */
-  int32_t reserved0;
+  int32_t format;          /* f3r_format: F3R_FORMAT_SELL (0, SELL-C-sigma as the GPU drivers,
+                              f3r-gpu.cpp:66) or F3R_FORMAT_CSR (CSR as the CPU driver, f3r.cpp:50;
+                              sigma 1, no SELL options).  Both give the same sums */
   double trsv_omega;       /* ILU0_JACOBI: damping omega in (0, 2], 1.0 */
   int32_t inner_sstep;     /* bit 0: level 2, bit 1: level 3 run as sFGMRES (solver/gmres2.hpp:
                               137-221): all m preconditioner + matrix applications first, on the
@@ -151,6 +156,13 @@ typedef struct f3r_sell_info {
 /* f3r_sell_create dtype_mask flag: offset-aligned slices where they fit (see
  * f3r_params.sell_align). */
 #define F3R_SELL_ALIGNED (1 << 9)
+/* f3r_sell_create dtype_mask flag: keep the matrix in CSR (sigma must be 1;
+ * f3r_sell_info reports slice_height 0).  The kernels sum each row in column
+ * order as the packed SELL kernel does, so the results are the same. */
+#define F3R_SELL_CSR (1 << 10)
+
+/* f3r_params.format */
+typedef enum f3r_format { F3R_FORMAT_SELL = 0, F3R_FORMAT_CSR = 1 } f3r_format;
 
 /* ---------------------------------------------------------------- errors */
 const char *f3r_last_error_string(void);

@@ -143,6 +143,32 @@ def test_invalid_params(ctx):
         F.Solver(ctx, A, precond=F.PRECOND_ILU0_BJ, ilu_blocks=112)
 
 
+@pytest.mark.parametrize("kind", ["stencil27", "diffusion7"])
+def test_csr_format_solve_is_identical(ctx, kind):
+    """format CSR runs every product through the CSR kernel, in the packed
+    SELL kernel's launch geometry and column order: the solve is the packed
+    sigma = 1 layout's bit for bit (the diffusion matrix has non-diagonal
+    SDAINV factors, so W^T and Z are CSR too)"""
+    A = (F.stencil27(20, 20, 20, 2, 0.5) if kind == "stencil27" else F.diffusion7(18, 18, 18, 1.5, 6.0, 2)).scale()
+    b = A.spmv(F.random_uniform(5, -1, 1, A.shape[0]))
+    xs, its = [], []
+    for fmt in (F.FORMAT_SELL, F.FORMAT_CSR):
+        S = F.Solver(ctx, A, rel_tol=1e-10, c=8, format=fmt)
+        info, diag = S.info()
+        assert info.slice_height == (0 if fmt == F.FORMAT_CSR else 32)
+        assert diag == (kind == "stencil27")
+        x = np.zeros(len(b))
+        r = S.solve(b, x)
+        assert r.is_solved and r.expl_rel_res < 1e-10
+        xs.append(x)
+        its.append(r.res_iter)
+    assert its[0] == its[1] and np.array_equal(xs[0], xs[1])
+    with pytest.raises(F.F3RError, match="CSR"):
+        F.Solver(ctx, A, format=F.FORMAT_CSR, sell_sigma=256)
+    with pytest.raises(F.F3RError, match="format"):
+        F.Solver(ctx, A, format=7)
+
+
 def test_aligned_sell_solve_is_identical(ctx):
     """the offset-aligned layout changes no sum: the solve's iterate is the
     packed layout's bit for bit (sigma 1, SDAINV factors aligned too)"""

@@ -46,15 +46,15 @@ def matrices():
     yield "diffusion7", F.diffusion7(10, 9, 8, 2.5, 3.0, 1).scale()
 
 
-FORM_BITS = {"int32": 32, "index16": 16, "aligned": 0}
+FORM_BITS = {"int32": 32, "index16": 16, "aligned": 0, "csr": 32}
 
 
 def make_sell(ctx, A, sigma, form):
-    return F.Sell(ctx, A, sigma=sigma, index16=form == "index16", aligned=form == "aligned")
+    return F.Sell(ctx, A, sigma=sigma, index16=form == "index16", aligned=form == "aligned", csr=form == "csr")
 
 
 @pytest.mark.parametrize("sigma,form", [(1, "int32"), (256, "int32"), (1, "index16"), (256, "index16"),
-                                        (1, "aligned"), (256, "aligned"), (32, "aligned")])
+                                        (1, "aligned"), (256, "aligned"), (32, "aligned"), (1, "csr")])
 def test_operate_bitexact(ctx, sigma, form):
     """every index form gives the oracle's sums bit for bit.  The aligned
     cases cover the fully aligned form (stencils in natural order, clamped
@@ -95,7 +95,7 @@ def test_operate_bitexact(ctx, sigma, form):
 
 
 @pytest.mark.parametrize("sigma,form", [(1, "int32"), (32, "int32"), (32, "index16"), (1, "aligned"),
-                                        (32, "aligned")])
+                                        (32, "aligned"), (1, "csr")])
 def test_residual_bitexact(ctx, sigma, form):
     for name, A in matrices():
         rptr, idx, val = A.arrays()
@@ -182,6 +182,27 @@ def test_dot(ctx):
         assert abs(got - float(a32.astype(np.float64) @ b32)) <= 1e-5 * (np.abs(a) @ np.abs(b) + 1)
 
 
+def test_csr_rows_across_tiles(ctx):
+    """CSR rows longer than a staging tile (512 entries) and groups whose
+    range starts mid-tile: the sums stay the oracle's"""
+    n = 300
+    rng = np.random.default_rng(6)
+    lens = rng.integers(0, 40, n)
+    lens[[5, 33, 34, 200]] = [700, 1300, 513, 2048]
+    rptr = np.concatenate([[0], np.cumsum(lens)]).astype(np.int32)
+    idx = np.concatenate([np.sort(rng.choice(4096, size=k, replace=False)) for k in lens]).astype(np.int32)
+    val = rng.standard_normal(len(idx))
+    A = F.HostMatrix.from_csr(rptr, idx, val, ncols=4096)
+    S = F.Sell(ctx, A, csr=True)
+    assert S.info().slice_height == 0 and S.info().max_width == 2048
+    x = rng.standard_normal(4096)
+    for vt, xd, ov in ((F.F64, x, O.DT_F64), (F.F32, x.astype(np.float32), O.DT_F32)):
+        y = torch.zeros(n, dtype=torch.float64 if vt == F.F64 else torch.float32, device="cuda")
+        S.operate(torch.from_numpy(xd).cuda(), y, val_t=vt)
+        torch.cuda.synchronize()
+        assert np.array_equal(y.cpu().numpy(), O.spmv(rptr, idx, val, xd, ov, ov, ov))
+
+
 def test_empty_and_bad_inputs(ctx):
     A = F.HostMatrix.from_csr(np.zeros(5, np.int32), np.zeros(0, np.int32), np.zeros(0))
     S = F.Sell(ctx, A)
@@ -193,6 +214,18 @@ def test_empty_and_bad_inputs(ctx):
         F.HostMatrix.from_csr(np.array([0, 2], np.int32), np.array([1, 0], np.int32), np.ones(2))
     with pytest.raises(F.F3RError):
         F.Sell(ctx, F.stencil27(4, 4, 4), sigma=0)
+    # an empty CSR matrix, CSR with sorting or another layout flag, tuning a CSR matrix
+    S = F.Sell(ctx, A, csr=True)
+    y = torch.ones(4, dtype=torch.float64, device="cuda")
+    S.operate(torch.ones(4, dtype=torch.float64, device="cuda"), y)
+    torch.cuda.synchronize()
+    assert torch.all(y == 0)
+    with pytest.raises(F.F3RError, match="sigma 1"):
+        F.Sell(ctx, F.stencil27(4, 4, 4), sigma=32, csr=True)
+    with pytest.raises(F.F3RError, match="sigma 1"):
+        F.Sell(ctx, F.stencil27(4, 4, 4), aligned=True, csr=True)
+    with pytest.raises(F.F3RError, match="CSR"):
+        F.Sell(ctx, F.stencil27(8, 8, 8), csr=True).tune(F.F16, reps=1)
 
 
 @pytest.mark.parametrize("aligned", [False, True])

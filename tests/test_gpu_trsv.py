@@ -131,3 +131,47 @@ def test_solver_with_baj_ilu(ctx):
                  trsv_iters=3, m2=4, m3=2, m4=1, c=8)
     res = S.solve(b, np.zeros(len(b)))
     assert res.is_solved and res.expl_rel_res < 1e-10
+
+
+@pytest.mark.parametrize("kind,sigma", [("stencil27", 1), ("stencil27", 256), ("diffusion7", 1)])
+def test_global_level_scheduled_ilu(ctx, kind, sigma):
+    """PRECOND_ILU0_LEVEL: one global ILU(0), its triangular solves spread
+    over the whole GPU (dependency flags, no grid barrier).  Every row is
+    computed as the single-block block-Jacobi kernel computes it, so the
+    solve is ILU0_BJ with one block bit for bit, and it matches the oracle's
+    single-block ILU(0) solve"""
+    if kind == "stencil27":
+        A = F.stencil27(24, 24, 24, 2, 0.5).scale()
+    else:
+        A = F.diffusion7(24, 22, 20, 1.5, 6.0, 3).scale()
+    b = A.spmv(F.random_uniform(7, -1, 1, A.shape[0]))
+    kw = dict(rel_tol=1e-10, m2=4, m3=2, m4=1, c=8, sell_sigma=sigma)
+    xs, its = [], []
+    for prec, blocks in ((F.PRECOND_ILU0_LEVEL, 112), (F.PRECOND_ILU0_BJ, 1)):
+        S = F.Solver(ctx, F.HostMatrix.from_csr(*A.arrays()), precond=prec, ilu_blocks=blocks, **kw)
+        x = np.zeros(len(b))
+        r = S.solve(b, x)
+        assert r.is_solved and r.expl_rel_res < 1e-10
+        xs.append(x)
+        its.append(r.res_iter)
+        S.close()
+    assert its[0] == its[1] and np.array_equal(xs[0], xs[1])
+    rptr, idx, val = A.arrays()
+    M = O.Mat.from_csr(rptr, idx, val)
+    o = O.f3r_solve(M, *O.ilu0_bj(M, 1), b, O.params(precond=O.PRECOND_ILU0_BJ, tol=1e-10, m2=4, m3=2, m4=1, c=8))
+    assert o["solved"] and abs(its[0] - o["iters"]) <= 1, (its[0], o["iters"])
+
+
+def test_global_level_ilu_many_levels(ctx):
+    """a 64^3 27-point matrix: 262,144 rows in several hundred levels, warps
+    far ahead of the frontier; repeated solves reuse the device-side
+    generation counter (graph replays)"""
+    A = F.stencil27(64, 64, 64, 1, 0.5).scale()
+    b = A.spmv(F.random_uniform(8, -1, 1, A.shape[0]))
+    kw = dict(rel_tol=1e-10, m2=4, m3=2, m4=1, c=8)
+    S = F.Solver(ctx, A, precond=F.PRECOND_ILU0_LEVEL, **kw)
+    x1 = np.zeros(len(b))
+    r1 = S.solve(b, x1)
+    x2 = np.zeros(len(b))
+    r2 = S.solve(b, x2)
+    assert r1.is_solved and r1.expl_rel_res < 1e-10 and np.array_equal(x1, x2) and r1.res_iter == r2.res_iter
