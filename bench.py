@@ -60,7 +60,7 @@ METRIC = "time to 1e-10 FP64 relative residual, plain F3R (fp64/fp32/fp16 nested
 WORKLOAD = "F3R-SDAINV-SELL32al stencil27-halfspace beta0.5 192^3 (n=7077888, nnz=189119224), tol 1e-10"
 
 
-PRECONDS = {"sdainv": 0, "ilu-bj": 1, "ilu-jacobi": 2, "ilu-baj": 3}
+PRECONDS = {"sdainv": 0, "ilu-bj": 1, "ilu-jacobi": 2, "ilu-baj": 3, "ilu-level": 4}
 PRECOND_DESC = "SDAINV(tol=0.1, acc=1.0)"
 
 
@@ -96,11 +96,12 @@ def set_precond(name, blocks, iters):
         return
     PARAMS.update(precond=PRECONDS[name], ilu_blocks=blocks, trsv_iters=iters)
     label = {"ilu-bj": f"BJILU0x{blocks}-levels", "ilu-jacobi": f"ILU0x{blocks}-jacobi{iters}",
-             "ilu-baj": f"ILU0x{blocks}-baj{iters}"}[name]
+             "ilu-baj": f"ILU0x{blocks}-baj{iters}", "ilu-level": "ILU0-global-levels"}[name]
     WORKLOAD = WORKLOAD.replace("F3R-SDAINV", "F3R-" + label)
     PRECOND_DESC = {"ilu-bj": f"block-Jacobi ILU(0), {blocks} blocks, exact level-scheduled triangular solves",
                     "ilu-jacobi": f"ILU(0) over {blocks} block(s), {iters} Jacobi sweeps per triangular solve",
-                    "ilu-baj": f"ILU(0) over {blocks} block(s), BAJ max_iter {iters}"}[name]
+                    "ilu-baj": f"ILU(0) over {blocks} block(s), BAJ max_iter {iters}",
+                    "ilu-level": "one global ILU(0), exact triangular solves level-scheduled over the whole GPU"}[name]
 
 
 def config_dict(extra=None):

@@ -195,14 +195,16 @@ struct IluLevelTri {
   unsigned int *state = nullptr;            // chunk counter, finished-block ticket, generation
 };
 
-__device__ __forceinline__ unsigned int ld_acquire_u32(const int32_t *p) {
+__device__ __forceinline__ unsigned int ld_relaxed_u32(const int32_t *p) {
   unsigned int v;
-  asm volatile("ld.acquire.gpu.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  asm volatile("ld.relaxed.gpu.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
   return v;
 }
 __device__ __forceinline__ void st_release_u32(int32_t *p, unsigned int v) {
   asm volatile("st.release.gpu.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
+
+constexpr int kLevelBatch = 16;  // dependencies polled, then read, together
 
 template <bool UPPER>
 __global__ void __launch_bounds__(256) k_trsv_level(IluLevelTri T, const int32_t *__restrict__ rowpos,
@@ -228,26 +230,50 @@ __global__ void __launch_bounds__(256) k_trsv_level(IluLevelTri T, const int32_t
       const int32_t b = T.rptr[i], e = T.rptr[i + 1];
       // lower: off-diagonals by increasing column (last entry = unit diagonal);
       // upper: by decreasing column (first entry = diagonal)
-      const int32_t j0 = UPPER ? e - 1 : b, j1 = UPPER ? b : e - 1, dj = UPPER ? -1 : 1;
-      for (int32_t j = j0; j != j1; j += dj) {
-        const int32_t q = T.idx[j];
-        if (!abort && ld_acquire_u32(T.flag + q) != gen) {
-          const unsigned long long t0 = global_ns();
+      const int32_t ndep = e - b - 1;
+      for (int32_t base = 0; base < ndep; base += kLevelBatch) {
+        const int cnt = min(kLevelBatch, ndep - base);
+        int32_t q[kLevelBatch];
+        float lv[kLevelBatch];
+#pragma unroll
+        for (int u = 0; u < kLevelBatch; u++)
+          if (u < cnt) {
+            const int32_t j = UPPER ? e - 1 - (base + u) : b + base + u;
+            q[u] = T.idx[j];
+            lv[u] = __half2float(T.val[j]);
+          }
+        // every flag of the batch polled at once; one fence orders the value loads after them
+        if (!abort) {
+          uint32_t waiting = cnt == 32 ? 0xffffffffu : ((1u << cnt) - 1u);
+          unsigned long long t0 = 0;
           int polls = 0;
-          while (ld_acquire_u32(T.flag + q) != gen) {
+          while (true) {
+#pragma unroll
+            for (int u = 0; u < kLevelBatch; u++)
+              if ((waiting >> u) & 1u)
+                if (ld_relaxed_u32(T.flag + q[u]) == gen) waiting &= ~(1u << u);
+            if (waiting == 0) break;
             if (*verr != 0) {
               abort = true;
               break;
             }
-            if (++polls > 8) __nanosleep(64);
-            if (global_ns() - t0 > kWaitLimitNs) {
+            if (polls++ == 0) t0 = global_ns();
+            else if (global_ns() - t0 > kWaitLimitNs) {
               atomicCAS(err, 0, (int)DEV_TIMEOUT_TRSV);
               abort = true;
               break;
             }
+            if (polls > 4) __nanosleep(32);
           }
+          __threadfence();
         }
-        t = __fmaf_rn(-__half2float(T.val[j]), __half2float(__ldcg(out + q)), t);
+        float y[kLevelBatch];
+#pragma unroll
+        for (int u = 0; u < kLevelBatch; u++)
+          if (u < cnt) y[u] = __half2float(__ldcg(out + q[u]));
+#pragma unroll
+        for (int u = 0; u < kLevelBatch; u++)
+          if (u < cnt) t = __fmaf_rn(-lv[u], y[u], t);
       }
       __half h;
       if (!UPPER) {
@@ -331,10 +357,11 @@ struct IluLevel {
     if (up(&rowpos, pos) != cudaSuccess) return fail(F3R_ERROR_CUDA, "ILU upload failed");
     F3R_TRY(build_tri(L, Lh, false, pos));
     F3R_TRY(build_tri(U, Uh, true, pos));
-    // enough warps to work several levels ahead, few enough that the spinning
-    // ones leave the L2 to the rows being computed
-    const int32_t chunks = std::max(L.nchunks, U.nchunks);
-    grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)sm_count * 4, (chunks + 7) / 8));
+    // warps for about four levels' chunks at a time: the frontier has work for
+    // them, and few enough are left spinning ahead of it
+    const int64_t chunks = std::max(L.nchunks, U.nchunks), levels = std::max(1, std::max(L.nlevels, U.nlevels));
+    const int64_t warps = 4 * ((chunks + levels - 1) / levels);
+    grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)sm_count * 2, (warps + 7) / 8));
     return F3R_SUCCESS;
   }
 

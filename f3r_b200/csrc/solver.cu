@@ -333,20 +333,22 @@ Status upload_csr(Context &c, const f3r_csr &a, int dtype_mask, DeviceSell &d) {
   int32_t mw = 0;
   for (int32_t i = 0; i < n; i++) mw = std::max(mw, a.rptr[i + 1] - a.rptr[i]);
   d.max_width = mw;
+  // the kernel's 16-byte copies may read up to 15 bytes past the last entry: kCsrPad elements of padding
+  const size_t na = nz + kCsrPad;
   F3R_TRY(c.alloc((void **)&d.rptr, ((size_t)n + 1) * 4));
-  F3R_TRY(c.alloc((void **)&d.col, std::max<size_t>(nz, 1) * 4));
+  F3R_TRY(c.alloc((void **)&d.col, na * 4));
   CUDA_TRY(cudaMemcpyAsync(d.rptr, a.rptr, ((size_t)n + 1) * 4, cudaMemcpyHostToDevice, c.stream));
   if (nz) CUDA_TRY(cudaMemcpyAsync(d.col, a.idx, nz * 4, cudaMemcpyHostToDevice, c.stream));
   double *tmp64 = nullptr;
-  F3R_TRY(c.alloc((void **)&tmp64, std::max<size_t>(nz, 1) * 8));
+  F3R_TRY(c.alloc((void **)&tmp64, na * 8));
   if (nz) CUDA_TRY(cudaMemcpyAsync(tmp64, a.val, nz * 8, cudaMemcpyHostToDevice, c.stream));
   const int g = c.ew_grid((int64_t)nz);
   if (dtype_mask & (1 << F3R_F32)) {
-    F3R_TRY(c.alloc((void **)&d.v32, std::max<size_t>(nz, 1) * 4));
+    F3R_TRY(c.alloc((void **)&d.v32, na * 4));
     launch_k(c, k_convert_vals<float>, g, kEwThreads, 0, c.stream, tmp64, d.v32, (int64_t)nz);
   }
   if (dtype_mask & (1 << F3R_F16)) {
-    F3R_TRY(c.alloc((void **)&d.v16, std::max<size_t>(nz, 1) * 2));
+    F3R_TRY(c.alloc((void **)&d.v16, na * 2));
     launch_k(c, k_convert_vals<__half>, g, kEwThreads, 0, c.stream, tmp64, d.v16, (int64_t)nz);
   }
   CUDA_TRY(cudaGetLastError());
