@@ -51,7 +51,8 @@ BETA = 0.5
 SIGMA = 1
 ALIGN = 1
 LAYOUTS = {"aligned": dict(sell_sigma=1, sell_align=1, format=0), "sigma256": dict(sell_sigma=256, sell_align=0, format=0),
-           "csr": dict(sell_sigma=1, sell_align=0, format=1)}
+           "csr": dict(sell_sigma=1, sell_align=0, format=1),
+           "auto": dict(sell_sigma=1, sell_align=0, format=0, sell_autotune=1)}
 TOL = 1e-10
 PARAMS = dict(m_outer=100, max_restarts=20, m2=8, m3=4, m4=2, c=64, sdainv_tol=0.1, acc=1.0, sell_sigma=SIGMA,
               sell_align=ALIGN, format=0,
@@ -81,8 +82,15 @@ def set_layout(name):
     PARAMS.update(LAYOUTS[name])
 
 
+AUTOTUNED = {}
+
+
 def layout_desc(p=None):
     p = PARAMS if p is None else p
+    if p.get("sell_autotune"):
+        return {"autotuned": True}
+    if AUTOTUNED and p is PARAMS:
+        return dict(AUTOTUNED["chosen"], autotuned=True)
     if p.get("format"):
         return {"format": "CSR", "index": "explicit int32"}
     return {"C": 32, "sigma": p["sell_sigma"],
@@ -332,6 +340,12 @@ def run_ours(args):
     torch.cuda.set_stream(stream)
     ctx.set_stream(stream.cuda_stream)
     solver = F.Solver(ctx, A, **PARAMS)
+    if PARAMS.get("sell_autotune"):
+        # the layout the autotuner chose, in the config's terms
+        info, _ = solver.info()
+        PARAMS.update(format=1 if info.slice_height == 0 else 0, sell_sigma=info.sigma,
+                      sell_align=1 if info.index_bits == 0 else 0, sell_autotune=0)
+        AUTOTUNED["chosen"] = layout_desc()
     b_d = torch.from_numpy(b).cuda()
     x_d = torch.zeros_like(b_d)
 
@@ -732,7 +746,8 @@ def main():
     ap.add_argument("--ilu-blocks", type=int, default=112)
     ap.add_argument("--trsv-iters", type=int, default=2)
     ap.add_argument("--layout", default="aligned", choices=sorted(LAYOUTS),
-                    help="matrix layout of our arm: offset-aligned SELL sigma=1 (default), packed SELL sigma=256, or CSR")
+                    help="matrix layout of our arm: offset-aligned SELL sigma=1 (default), packed SELL sigma=256, CSR, or "
+                         "auto (the library's layout autotuner picks at set-up)")
     ap.add_argument("--no-alt-layout", action="store_true", help="skip timing the other layout")
     ap.add_argument("--config", default="c2", choices=["c2", "c3", "c4", "c5"],
                     help="c2: the headline solve; c3: the precision stress (256^3 diffusion, per-level errors); "

@@ -846,6 +846,82 @@ struct Solver {
   }
 };
 
+// Layout autotuner (f3r_params.sell_autotune): the fp16 copy of A is built in
+// every candidate layout and its fp16 x fp32 product timed on the context's
+// stream (2 warm-up launches, best of 3 runs of 5, CUDA events); p takes the
+// fastest layout.  Candidates that cannot be built (padding beyond 2^31
+// entries) are skipped.
+static Status autotune_layout(f3r_context *ctx, const f3r_csr *a, f3r_params &p) {
+  struct Cand {
+    int32_t format, sigma, align, index16;
+  };
+  const Cand cands[] = {{F3R_FORMAT_SELL, 1, 1, 0},   {F3R_FORMAT_SELL, 1, 0, 0}, {F3R_FORMAT_SELL, 1, 0, 1},
+                        {F3R_FORMAT_SELL, 256, 0, 0}, {F3R_FORMAT_SELL, 256, 1, 0}, {F3R_FORMAT_CSR, 1, 0, 0}};
+  Context &c = *ctx;
+  const int32_t n = a->nrows;
+  float *xy = nullptr;
+  F3R_TRY(c.alloc((void **)&xy, sizeof(float) * 2 * (size_t)std::max(n, 1)));
+  CUDA_TRY(cudaMemsetAsync(xy, 0, sizeof(float) * 2 * (size_t)std::max(n, 1), c.stream));
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float best = 0;
+  int besti = -1;
+  Status st = F3R_SUCCESS;
+  for (int i = 0; i < (int)(sizeof(cands) / sizeof(cands[0])) && st == F3R_SUCCESS; i++) {
+    const Cand &k = cands[i];
+    DeviceSell d;
+    if (k.format == F3R_FORMAT_CSR) {
+      st = upload_csr(c, *a, 1 << F3R_F16, d);
+    } else {
+      SellHost h;
+      st = build_sell(*a, k.sigma, true, h);
+      if (st != F3R_SUCCESS) break;
+      if (k.align) {
+        if (align_offsets(*a, true, h) < 0) continue;  // too large padded: not a candidate
+      } else if (k.index16) {
+        compress_index16(h);
+      }
+      st = upload_sell(c, h, 1 << F3R_F16, false, d);
+    }
+    float ms = 0;
+    if (st == F3R_SUCCESS) {
+      const DevSell v = d.view();
+      float run_best = 0;
+      for (int w = 0; w < 2 && st == F3R_SUCCESS; w++)
+        st = launch_sell(c, d.v16, v, (const float *)xy, EpiStore<float>{xy + n, nullptr});
+      for (int r = 0; r < 3 && st == F3R_SUCCESS; r++) {
+        cudaEventRecord(e0, c.stream);
+        for (int w = 0; w < 5 && st == F3R_SUCCESS; w++)
+          st = launch_sell(c, d.v16, v, (const float *)xy, EpiStore<float>{xy + n, nullptr});
+        cudaEventRecord(e1, c.stream);
+        if (cudaEventSynchronize(e1) != cudaSuccess) st = fail(F3R_ERROR_CUDA, "autotune timing failed");
+        float t = 0;
+        cudaEventElapsedTime(&t, e0, e1);
+        if (r == 0 || t < run_best) run_best = t;
+      }
+      ms = run_best;
+    }
+    cudaStreamSynchronize(c.stream);
+    d.release();
+    if (st == F3R_SUCCESS && (besti < 0 || ms < best)) {
+      best = ms;
+      besti = i;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(xy);
+  F3R_TRY(st);
+  F3R_TRY(c.check_device_error());
+  if (besti < 0) return fail(F3R_ERROR_UNSUPPORTED, "no candidate layout could be built");
+  p.format = cands[besti].format;
+  p.sell_sigma = cands[besti].sigma;
+  p.sell_align = cands[besti].align;
+  p.sell_index16 = cands[besti].index16;
+  return F3R_SUCCESS;
+}
+
 // zf / wf: given SDAINV factors (both or neither; precond SDAINV only)
 static Status make_solver(f3r_context *ctx, const f3r_csr *a, const f3r_params *pp, Solver **out,
                           const f3r_csr *zf = nullptr, const f3r_csr *wf = nullptr) {
@@ -874,6 +950,10 @@ static Status make_solver(f3r_context *ctx, const f3r_csr *a, const f3r_params *
     return fail(F3R_ERROR_INVALID_VALUE, "unknown preconditioner");
   if (p.half_scale_log2 < 0 || p.half_scale_log2 > 20) return fail(F3R_ERROR_INVALID_VALUE, "half_scale_log2 in [0, 20]");
   if (p.inner_sstep < 0 || p.inner_sstep > 3) return fail(F3R_ERROR_INVALID_VALUE, "inner_sstep is a 2-bit mask");
+  if (p.sell_autotune) {
+    CUDA_TRY(cudaSetDevice(ctx->device));
+    F3R_TRY(autotune_layout(ctx, a, p));
+  }
   auto s = std::make_unique<Solver>();
   s->ctx = ctx;
   s->p = p;

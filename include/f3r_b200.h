@@ -112,7 +112,13 @@ typedef struct f3r_params {
                               stored there, so an fp16 entry streams 2 bytes instead of 6.  With
                               sell_sigma = 1 a stencil aligns every slice.  Same sums in the same
                               order as the packed layout.  0 */
-  int32_t reserved[8];
+  int32_t sell_autotune;   /* 1: at set-up, build the fp16 copy of the matrix in each candidate
+                              layout (offset-aligned SELL sigma 1; packed SELL sigma 1 with 32- and
+                              16-bit indices; packed and aligned SELL sigma 256; CSR), time the fp16
+                              product on it, and solve in the fastest; the layout fields above are
+                              then ignored (f3r_solver_info reports the choice).  All give the same
+                              sums at sigma 1; sigma 256 permutes the rows.  0 */
+  int32_t reserved[7];
 } f3r_params;
 
 /* Solve outcome.  The first three fields are solve_res_t

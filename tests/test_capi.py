@@ -47,7 +47,7 @@ def test_params_default_match_drivers():
     assert (p.sdainv_tol, p.acc, p.rel_tol, p.ilu_blocks, p.sell_c, p.sell_sigma) == (0.1, 1.0, 1e-8, 112, 32, 1)
     assert p.half_scale_log2 == 0 and p.use_graphs == 1 and p.sell_index16 == 0
     assert p.static_weight == 0.0 and (p.trsv_iters, p.trsv_omega) == (2, 1.0) and p.inner_sstep == 0
-    assert p.sell_align == 0 and p.format == 0
+    assert p.sell_align == 0 and p.format == 0 and p.sell_autotune == 0
     # the ctypes mirror has the C struct's size
     assert C.sizeof(p) == 144
 

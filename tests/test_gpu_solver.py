@@ -169,6 +169,33 @@ def test_csr_format_solve_is_identical(ctx, kind):
         F.Solver(ctx, A, format=7)
 
 
+@pytest.mark.parametrize("kind", ["stencil27", "ragged"])
+def test_layout_autotuner(ctx, kind):
+    """sell_autotune times every candidate layout's fp16 product at set-up and
+    solves in the fastest: the solve is the one made with that layout given
+    explicitly, bit for bit"""
+    if kind == "stencil27":
+        A = F.stencil27(24, 24, 24, 2, 0.5).scale()
+    else:
+        A = F.diffusion7(20, 17, 13, 1.0, 3.0, 9).scale()
+    b = A.spmv(F.random_uniform(3, -1, 1, A.shape[0]))
+    S = F.Solver(ctx, A, rel_tol=1e-10, c=8, sell_autotune=1)
+    info, _ = S.info()
+    fmt = F.FORMAT_CSR if info.slice_height == 0 else F.FORMAT_SELL
+    assert info.sigma in (1, 256)
+    x1 = np.zeros(len(b))
+    r1 = S.solve(b, x1)
+    assert r1.is_solved and r1.expl_rel_res < 1e-10
+    kw = dict(format=fmt, sell_sigma=info.sigma, sell_align=1 if info.index_bits == 0 else 0,
+              sell_index16=1 if info.index_bits == 16 else 0)
+    S2 = F.Solver(ctx, A, rel_tol=1e-10, c=8, **kw)
+    i2, _ = S2.info()
+    assert (i2.sigma, i2.index_bits, i2.slice_height) == (info.sigma, info.index_bits, info.slice_height)
+    x2 = np.zeros(len(b))
+    r2 = S2.solve(b, x2)
+    assert r2.res_iter == r1.res_iter and np.array_equal(x1, x2)
+
+
 def test_aligned_sell_solve_is_identical(ctx):
     """the offset-aligned layout changes no sum: the solve's iterate is the
     packed layout's bit for bit (sigma 1, SDAINV factors aligned too)"""
