@@ -125,8 +125,8 @@ template <typename V, typename CI = int32_t> struct SellCfg;
 template <typename CI> struct SellCfg<__half, CI> { static constexpr int WARPS = 24, STAGES = 2, KC = 16; };
 template <typename CI> struct SellCfg<float, CI> { static constexpr int WARPS = 24, STAGES = 2, KC = 16; };
 template <typename CI> struct SellCfg<double, CI> { static constexpr int WARPS = 16, STAGES = 2, KC = 16; };
-template <> struct SellCfg<__half, AllAlignedIdx> { static constexpr int WARPS = 24, STAGES = 2, KC = 32; };
-template <> struct SellCfg<float, AllAlignedIdx> { static constexpr int WARPS = 16, STAGES = 2, KC = 32; };
+template <> struct SellCfg<__half, AllAlignedIdx> { static constexpr int WARPS = 32, STAGES = 2, KC = 32; };
+template <> struct SellCfg<float, AllAlignedIdx> { static constexpr int WARPS = 24, STAGES = 2, KC = 32; };
 template <> struct SellCfg<double, AllAlignedIdx> { static constexpr int WARPS = 12, STAGES = 2, KC = 32; };
 
 template <typename V, typename CI, int WARPS, int STAGES, int KC>
@@ -269,6 +269,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1)
       const int nsub = (kc + SUB - 1) / SUB;
       V vb[2][SUB];
       Acc xb[2][SUB];
+      const X *xl = x + lane;  // this lane's column is base + lane
       auto load_sub = [&](int h, V (&v)[SUB], Acc (&xg)[SUB]) {
 #pragma unroll
         for (int g = 0; g < SUB / 4; g++) {
@@ -277,15 +278,15 @@ __global__ void __launch_bounds__(WARPS * 32, 1)
             V t[4];
             Vec4Load<V>::ld(lv + k0, t);
             const int4 q = *reinterpret_cast<const int4 *>(sb + k0);
-            int32_t b[4] = {q.x + lane, q.y + lane, q.z + lane, q.w + lane};
-            if (clampc) {
+            const int32_t b[4] = {q.x, q.y, q.z, q.w};
 #pragma unroll
-              for (int e = 0; e < 4; e++) b[e] = min(max(b[e], 0), A.ncols - 1);
-            }
+            for (int e = 0; e < 4; e++) v[g * 4 + e] = t[e];
+            if (!clampc) {
 #pragma unroll
-            for (int e = 0; e < 4; e++) {
-              v[g * 4 + e] = t[e];
-              xg[g * 4 + e] = to_acc<Acc>(__ldg(x + b[e]));
+              for (int e = 0; e < 4; e++) xg[g * 4 + e] = to_acc<Acc>(__ldg(xl + b[e]));
+            } else {
+#pragma unroll
+              for (int e = 0; e < 4; e++) xg[g * 4 + e] = to_acc<Acc>(__ldg(x + min(max(b[e] + lane, 0), A.ncols - 1)));
             }
           }
         }
