@@ -66,7 +66,10 @@ void time_shape(Context &c, const DeviceSell &d, const V *val, const X *x, Y *y,
 template <typename V, typename X, typename Y, typename CI>
 void sweep(Context &c, const DeviceSell &d, const V *val, const X *x, Y *y, int reps, std::vector<f3r_tune_entry> &out) {
   if constexpr (IdxForm<CI>::mode == 3) {
+    time_shape<V, X, Y, 32, 3, 32, CI>(c, d, val, x, y, reps, out);
     time_shape<V, X, Y, 32, 2, 32, CI>(c, d, val, x, y, reps, out);
+    time_shape<V, X, Y, 28, 3, 32, CI>(c, d, val, x, y, reps, out);
+    time_shape<V, X, Y, 28, 2, 32, CI>(c, d, val, x, y, reps, out);
     time_shape<V, X, Y, 24, 4, 32, CI>(c, d, val, x, y, reps, out);
     time_shape<V, X, Y, 24, 3, 32, CI>(c, d, val, x, y, reps, out);
     time_shape<V, X, Y, 24, 2, 32, CI>(c, d, val, x, y, reps, out);
