@@ -212,6 +212,12 @@ class Context:
     def synchronize(self) -> None:
         check(lib().f3r_context_synchronize(self._h))
 
+    def wait_probe(self, set_flag: bool, limit_ms: int) -> None:
+        """The library's bounded device wait on a flag that is set or that
+        nothing sets (f3r_context_wait_probe); raises F3RError (TIMEOUT) when
+        the limit passes."""
+        check(lib().f3r_context_wait_probe(self._h, 1 if set_flag else 0, limit_ms))
+
     def dot(self, x, y) -> float:
         """<x, y> of two device tensors (torch) of the same dtype."""
         dt = _torch_dt(x)

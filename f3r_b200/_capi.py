@@ -101,6 +101,7 @@ SIGNATURES = {
     "f3r_sell_tune": (C.c_int, [_vp, C.c_int, C.c_int32, C.POINTER(TuneEntry), C.c_int32, C.POINTER(C.c_int32)]),
     "f3r_sell_operate": (C.c_int, [_vp, C.c_int, C.c_int, _vp, C.c_int, _vp]),
     "f3r_sell_compute_residual": (C.c_int, [_vp, C.c_int, C.c_int, _vp, C.c_int, _vp, C.c_int, _vp]),
+    "f3r_context_wait_probe": (C.c_int, [_vp, C.c_int32, C.c_int32]),
     "f3r_dot": (C.c_int, [_vp, C.c_int, C.c_int64, _vp, _vp, C.POINTER(C.c_double)]),
     "f3r_dot_noalloc": (C.c_int, [C.c_int, C.c_int64, _vp, _vp, _vp, _vp]),
     "f3r_params_default": (None, [C.POINTER(Params)]),

@@ -206,6 +206,41 @@ __device__ __forceinline__ void st_release_u32(int32_t *p, unsigned int v) {
 
 constexpr int kLevelBatch = 16;  // dependencies polled, then read, together
 
+// Waits until flag[q[u]] == gen for every u < cnt (relaxed polls, then one
+// fence orders the caller's later loads after them).  Bounded: after
+// limit_ns of %globaltimer it records DEV_TIMEOUT_TRSV in *err and returns
+// false; it also returns false at once when *err is already set (another
+// wait of the launch gave up, or the solve broke down), so no wait outlives
+// the first failure by more than one bound.
+__device__ __forceinline__ bool wait_flags(const int32_t *flag, const int32_t (&q)[kLevelBatch], int cnt,
+                                           unsigned int gen, int *err, unsigned long long limit_ns) {
+  volatile int *verr = err;
+  uint32_t waiting = (1u << cnt) - 1u;
+  unsigned long long t0 = 0;
+  int polls = 0;
+  bool ok = true;
+  while (true) {
+#pragma unroll
+    for (int u = 0; u < kLevelBatch; u++)
+      if ((waiting >> u) & 1u)
+        if (ld_relaxed_u32(flag + q[u]) == gen) waiting &= ~(1u << u);
+    if (waiting == 0) break;
+    if (*verr != 0) {
+      ok = false;
+      break;
+    }
+    if (polls++ == 0) t0 = global_ns();
+    else if (global_ns() - t0 > limit_ns) {
+      atomicCAS(err, 0, (int)DEV_TIMEOUT_TRSV);
+      ok = false;
+      break;
+    }
+    if (polls > 4) __nanosleep(32);
+  }
+  __threadfence();
+  return ok;
+}
+
 template <bool UPPER>
 __global__ void __launch_bounds__(256) k_trsv_level(IluLevelTri T, const int32_t *__restrict__ rowpos,
                                                     const __half *__restrict__ in, __half *out,
@@ -216,7 +251,6 @@ __global__ void __launch_bounds__(256) k_trsv_level(IluLevelTri T, const int32_t
   const unsigned int gen = gen_s;
   const int lane = threadIdx.x & 31;
   const float om = ome ? __half2float(*ome) : 1.0f;
-  volatile int *verr = err;
   bool abort = false;
   while (true) {
     unsigned int c = 0;
@@ -243,30 +277,7 @@ __global__ void __launch_bounds__(256) k_trsv_level(IluLevelTri T, const int32_t
             lv[u] = __half2float(T.val[j]);
           }
         // every flag of the batch polled at once; one fence orders the value loads after them
-        if (!abort) {
-          uint32_t waiting = cnt == 32 ? 0xffffffffu : ((1u << cnt) - 1u);
-          unsigned long long t0 = 0;
-          int polls = 0;
-          while (true) {
-#pragma unroll
-            for (int u = 0; u < kLevelBatch; u++)
-              if ((waiting >> u) & 1u)
-                if (ld_relaxed_u32(T.flag + q[u]) == gen) waiting &= ~(1u << u);
-            if (waiting == 0) break;
-            if (*verr != 0) {
-              abort = true;
-              break;
-            }
-            if (polls++ == 0) t0 = global_ns();
-            else if (global_ns() - t0 > kWaitLimitNs) {
-              atomicCAS(err, 0, (int)DEV_TIMEOUT_TRSV);
-              abort = true;
-              break;
-            }
-            if (polls > 4) __nanosleep(32);
-          }
-          __threadfence();
-        }
+        if (!abort) abort = !wait_flags(T.flag, q, cnt, gen, err, kWaitLimitNs);
         float y[kLevelBatch];
 #pragma unroll
         for (int u = 0; u < kLevelBatch; u++)
@@ -374,5 +385,13 @@ struct IluLevel {
     return F3R_SUCCESS;
   }
 };
+
+// The level solve's flag wait on one flag (f3r_context_wait_probe): the
+// flag holds gen when set, 0 otherwise.
+__global__ void k_wait_probe(const int32_t *flag, unsigned int gen, int *err, unsigned long long limit_ns) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  int32_t q[kLevelBatch] = {0};
+  wait_flags(flag, q, 1, gen, err, limit_ns);
+}
 
 }  // namespace f3r

@@ -1393,6 +1393,20 @@ f3r_status f3r_sell_compute_residual(f3r_sell *m, f3r_dtype val_t, f3r_dtype rhs
   return fail(F3R_ERROR_UNSUPPORTED, "unsupported (val, rhs, in, res) type combination");
 }
 
+f3r_status f3r_context_wait_probe(f3r_context *ctx, int32_t set, int32_t limit_ms) {
+  if (!ctx || limit_ms < 1 || limit_ms > 10000) return fail(F3R_ERROR_INVALID_VALUE, "need 1 <= limit_ms <= 10000");
+  Context &c = *ctx;
+  CUDA_TRY(cudaSetDevice(c.device));
+  const int32_t gen = 7;
+  int32_t *flag = reinterpret_cast<int32_t *>(c.dscratch);  // the context's device scalars
+  CUDA_TRY(cudaMemsetAsync(flag, 0, sizeof(int32_t), c.stream));
+  if (set) CUDA_TRY(cudaMemcpyAsync(flag, &gen, sizeof(int32_t), cudaMemcpyHostToDevice, c.stream));
+  launch_k(c, k_wait_probe, 1, 32, 0, c.stream, (const int32_t *)flag, (unsigned int)gen, c.err,
+           (unsigned long long)limit_ms * 1000000ull);
+  CUDA_TRY(cudaGetLastError());
+  return c.check_device_error();
+}
+
 f3r_status f3r_dot(f3r_context *ctx, f3r_dtype t, int64_t n, const void *x, const void *y, double *result) {
   if (!ctx || !result || n < 0 || (n > 0 && (!x || !y))) return fail(F3R_ERROR_INVALID_VALUE, "bad argument");
   Context &c = *ctx;

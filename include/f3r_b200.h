@@ -317,6 +317,15 @@ typedef struct f3r_tune_entry {
 f3r_status f3r_sell_tune(f3r_sell *m, f3r_dtype val_t, int32_t reps, f3r_tune_entry *out, int32_t cap,
                          int32_t *count);
 
+/* Runs the level-scheduled ILU solve's bounded dependency wait on one device
+ * flag that is already set (set != 0) or that nothing sets (set = 0), with a
+ * limit of limit_ms (1..10000) instead of the kernels' 2 s.  Returns
+ * F3R_SUCCESS, or F3R_ERROR_TIMEOUT once the limit has passed; either way the
+ * context's device error word is clear again and the context stays usable.
+ * A check of the failure path for callers and tests; no reference
+ * counterpart (the reference never waits on the device). */
+f3r_status f3r_context_wait_probe(f3r_context *ctx, int32_t set, int32_t limit_ms);
+
 /* *result = <x, y> over n entries (fp64 for F64, fp32 accumulation otherwise;
  * F16 inputs are widened to fp32 as the reference's wildcard(., tof32),
  * f3r-gpu.cpp:236).  Replaces kmm::dot (core/tensor.hpp:509-537, 686-688).
