@@ -258,7 +258,7 @@ def spmv_roofline(solver, A, torch, F):
     if csr:
         kern = "k_csr_cfg<__half,float,EpiStore<float>,24> (CSR, fp16 A, fp32 x, fp32 y)"
     elif aligned:
-        kern = ("k_sell_cfg<__half,float,EpiStore<float>,24,2,32,AllAlignedIdx> (SELL-32 sigma=1, offset-aligned, "
+        kern = ("k_sell_cfg<__half,float,EpiStore<float>,32,2,32,AllAlignedIdx> (SELL-32 sigma=1, offset-aligned, "
                 "fp16 A, fp32 x, fp32 y)")
     else:
         kern = f"k_sell_cfg<__half,float,EpiStore<float>,24,2,16,int> (SELL-32 sigma={info.sigma}, fp16 A, fp32 x, fp32 y)"
