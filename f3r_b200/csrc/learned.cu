@@ -28,7 +28,7 @@
 //              accumulator, and adds that to the global gradient once
 //   Adam       one thread per parameter
 // Inference runs the same network in BF16 on tensor cores (mma.sync
-// m16n8k16, fp32 accumulation), one warp per 16 rows.
+// m16n8k16, fp32 accumulation), one warp per 16-row tile, persistent CTAs.
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -403,8 +403,10 @@ __global__ void __launch_bounds__(128) k_mlp_infer_bf16(int32_t n, const float *
   if (threadIdx.x < kOut) b3s[threadIdx.x] = p[oB3 + threadIdx.x];
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, c = lane & 3;
-  const int64_t r0 = ((int64_t)blockIdx.x * 4 + warp) * 16;
-  if (r0 >= n) return;
+  // persistent grid: the weights above are staged once per CTA, then each
+  // warp walks 16-row tiles
+#pragma unroll 1
+  for (int64_t r0 = ((int64_t)blockIdx.x * 4 + warp) * 16; r0 < n; r0 += (int64_t)gridDim.x * 64) {
   const int64_t ra = r0 + g, rb = r0 + g + 8;
   auto fx = [&](int64_t r, int col) { return (r < n && col < kIn) ? f[r * kIn + col] : 0.f; };
   // layer 1: [16 x 16 (7 inputs, zero-padded)] x [16 x 64]
@@ -445,6 +447,7 @@ __global__ void __launch_bounds__(128) k_mlp_infer_bf16(int32_t n, const float *
   if (rb < n) {
     o[rb * kOut + 2 * c] = y[2];
     o[rb * kOut + 2 * c + 1] = y[3];
+  }
   }
 }
 
@@ -538,8 +541,10 @@ namespace {
 // forward pass and corrected factors of a loaded system
 Status forward(Context &c, const float *params, SysDev &s, bool bf16) {
   if (s.n == 0) return F3R_SUCCESS;
+  // inference: a persistent grid, each CTA staging the weights once
   if (bf16)
-    launch_k(c, k_mlp_infer_bf16, (int)cdiv(s.n, 64), 128, 0, c.stream, s.n, (const float *)s.feat, params, s.out);
+    launch_k(c, k_mlp_infer_bf16, (int)std::min<int64_t>(cdiv(s.n, 64), (int64_t)c.sm_count * 8), 128, 0, c.stream,
+             s.n, (const float *)s.feat, params, s.out);
   else
     launch_k(c, k_mlp_forward, (int)cdiv(s.n, kRows), kRows, 0, c.stream, s.n, (const float *)s.feat, params, s.out);
   const int g = (int)cdiv(s.n, 256);
