@@ -491,10 +491,14 @@ template <bool PREFETCH = true> struct EpiRichStepT {
   }
   template <typename Acc> __device__ __forceinline__ void row(int64_t r, Acc acc, const Pre &pp, Red (&)[1]) const {
     const Pre p = PREFETCH ? pp : Pre{hin[r], hout[r], M.w[r], M.z[r], rs->ome[k]};
-    const float hr = h2f(f2h(h2f(p.hin) - (float)acc));
-    const float t = h2f(f2h(h2f(p.w) * hr));
-    const float t2 = h2f(f2h(h2f(p.z) * t));
-    const float hn = h2f(f2h(__fmaf_rn(h2f(p.ome), t2, h2f(p.hout))));
+    // The product of two fp16 values is exact in fp32, so the fp16 multiply
+    // (one correctly rounded result) gives the bits of fp16(float(a) * float(b))
+    // in one instruction; the subtraction (fp32 acc) and the fused update keep
+    // their fp32 arithmetic.
+    const __half hr = f2h(h2f(p.hin) - (float)acc);
+    const __half t = __hmul(p.w, hr);
+    const __half t2 = __hmul(p.z, t);
+    const float hn = h2f(f2h(__fmaf_rn(h2f(p.ome), h2f(t2), h2f(p.hout))));
     if (out) out[r] = hn * isc;
     else hnext[r] = f2h(hn);
   }

@@ -117,6 +117,13 @@ inline void write_vector(const std::string &path, const std::vector<double> &x) 
 namespace algorithm {
 // kmm::algorithm::scaling (algorithm.hpp:45-59)
 inline void scaling(CSR &a) { check(f3r_host_scaling(a.handle())); }
+// kmm::algorithm::sdainv (preconditioner/ainv.hpp:27-65): {Z, W^T}, M r = Z (W^T r)
+inline std::pair<CSR, CSR> sdainv(const CSR &a, double tol = 0.1, double acc = 1.0) {
+  f3r_csr v = a.view();
+  f3r_host_matrix *z = nullptr, *wt = nullptr;
+  check(f3r_host_sdainv(&v, tol, acc, &z, &wt));
+  return {CSR::adopt(z), CSR::adopt(wt)};
+}
 }  // namespace algorithm
 
 class Context {
@@ -174,6 +181,14 @@ class F3R {
     f3r_csr v = a.view();
     f3r_solver *s = nullptr;
     check(f3r_solver_create(ctx.handle(), &v, &p, &s));
+    s_.reset(s, f3r_solver_destroy);
+  }
+  // SDAINV factors given instead of computed (f3r_solver_create_factors), e.g.
+  // algorithm::sdainv's with values corrected by f3r_learned_correct
+  F3R(Context &ctx, const CSR &a, const params &p, const CSR &z, const CSR &wt) {
+    f3r_csr v = a.view(), zv = z.view(), wv = wt.view();
+    f3r_solver *s = nullptr;
+    check(f3r_solver_create_factors(ctx.handle(), &v, &p, &zv, &wv, &s));
     s_.reset(s, f3r_solver_destroy);
   }
   solve_res_t solve(const double *b, double *x, const std::function<bool(int, double)> &cond,

@@ -38,5 +38,14 @@ int main(int argc, char **argv) {
   }
   std::printf("solved %d iters %d calls %d expl %.3e err %.3e\n", flag.is_solved ? 1 : 0, flag.res_iter, calls,
               detail.expl_rel_res, std::sqrt(err / nx2));
-  return (flag.is_solved && detail.expl_rel_res < eps) ? 0 : 1;
+  // the same solve with the SDAINV factors computed here and handed over
+  auto zw = f3r::algorithm::sdainv(data, 0.1, 1.0);
+  f3r::F3R given(ctx, data, p, zw.first, zw.second);
+  std::vector<double> x2(n, 0.0);
+  f3r_result d2{};
+  const f3r::solve_res_t f2 = given.solve(b.data(), x2.data(), cond, &d2);
+  bool same = f2.res_iter == flag.res_iter;
+  for (int i = 0; i < n && same; i++) same = x2[i] == x[i];
+  std::printf("given_factors_identical %d\n", same ? 1 : 0);
+  return (flag.is_solved && detail.expl_rel_res < eps && same) ? 0 : 1;
 }
