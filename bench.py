@@ -618,6 +618,78 @@ def run_c3(args):
     print(json.dumps(line), flush=True)
 
 
+def run_c1(args):
+    """C1, the reference's own CPU configuration (work/src/f3r.cpp:44-58,
+    195-248): the hpcg 27-point matrix on a 64^3 grid (diagonal 26,
+    neighbours -1), scaled, b = A_s 1, x0 = 0, tol 1e-10, F3R(8, 4, 2, c 64)
+    with a restart cap of 3, acc 1.0, block-Jacobi ILU(0) over 112 blocks,
+    CSR storage.  Our GPU solve in exactly that configuration (format CSR,
+    exact level-scheduled block solves), the same preconditioner in the
+    offset-aligned SELL layout, and the reference's compiled CPU solve on all
+    host cores (oracle/_ref, config 1 = f3r.cpp's solver)."""
+    import torch
+    import f3r_b200 as F
+    torch.cuda.set_device(0)
+    nx = args.nx if args.nx != NX else 64
+    A = F.stencil27(nx, nx, nx, 0, 0.0).scale()
+    n = A.shape[0]
+    b = A.spmv(np.ones(n))
+    kw = dict(m_outer=100, max_restarts=3, m2=8, m3=4, m4=2, c=64, precond=F.PRECOND_ILU0_BJ, ilu_blocks=112,
+              acc=1.0, rel_tol=TOL, use_graphs=1)
+    ctx = F.Context(0)
+
+    def gpu(layout):
+        S = F.Solver(ctx, A, **kw, **layout)
+        x = np.zeros(n)
+        for _ in range(max(args.warmup, 1)):
+            x[:] = 0
+            S.solve(b, x)
+        best, wall = None, []
+        for _ in range(args.steps):
+            x[:] = 0
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            r = S.solve(b, x)
+            wall.append(time.perf_counter() - t0)
+            best = r if best is None or r.solve_seconds < best.solve_seconds else best
+        S.close()
+        return best, min(wall), float(np.max(np.abs(x - 1.0)))
+
+    r_csr, w_csr, e_csr = gpu(dict(format=1, sell_sigma=1, sell_align=0))
+    r_al, w_al, _ = gpu(dict(format=0, sell_sigma=1, sell_align=1))
+    cores = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    ref_line = None
+    try:
+        from oracle import oracle as O
+        ref = O.Ref("fast")
+        rptr, idx, val = A.arrays()
+        runs = [ref.f3r_solve(1, rptr, idx, val, b, m2=8, m3=4, m4=2, c=64, restarts=3, tol=TOL, acc=1.0, blocks=112)
+                for _ in range(2)]
+        rr = min(runs, key=lambda d: d["time_s"])
+        ref_line = {"ms": round(rr["time_s"] * 1e3, 1), "outer_iters": rr["iters"], "expl_rel_res": rr["expl_res"],
+                    "solved": rr["solved"], "cores": int(os.environ["OMP_NUM_THREADS"]), "build": ref.name}
+    except FileNotFoundError as e:
+        ref_line = {"unavailable": str(e)}
+    line = {"metric": "time to 1e-10 FP64 relative residual, F3R in the reference's CPU configuration (C1)",
+            "value": round(r_csr.solve_seconds * 1e3, 2), "unit": "ms", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": False, "dtype": "mixed: f16 storage/f32 accumulate, f32, f64",
+            "data": "synthetic (hpcg 27-point matrix, b = A 1)",
+            "config": {"workload": f"C1: hpcg 27-pt {nx}^3 (n={n}, nnz={A.nnz}), BJ-ILU(0) x112 exact, CSR, "
+                                   "F3R(8,4,2,c=64), restart cap 3, tol 1e-10",
+                       "timing": "device solve time (CUDA events), best of steps"},
+            "e2e": {"value": round(w_csr * 1e3, 2), "unit": "ms", "h2d_bytes_per_step": 16 * n,
+                    "d2h_bytes_per_step": 8 * n},
+            "solve": {"outer_iters": r_csr.res_iter, "expl_rel_res": r_csr.expl_rel_res, "solved": r_csr.is_solved,
+                      "max_abs_err_vs_ones": e_csr},
+            "aligned_sell_same_precond": {"ms": round(r_al.solve_seconds * 1e3, 2), "outer_iters": r_al.res_iter,
+                                          "e2e_ms": round(w_al * 1e3, 2)},
+            "reference_cpu": ref_line}
+    if ref_line and "ms" in ref_line:
+        line["reference_cpu_over_gpu_e2e"] = round(ref_line["ms"] / (w_csr * 1e3), 1)
+    print(json.dumps(line), flush=True)
+
+
 C5_BATCH = 8  # held-out systems kept for the batched comparison (two solvers each)
 
 
@@ -758,10 +830,12 @@ def main():
                     help="matrix layout of our arm: offset-aligned SELL sigma=1 (default), packed SELL sigma=256, CSR, or "
                          "auto (the library's layout autotuner picks at set-up)")
     ap.add_argument("--no-alt-layout", action="store_true", help="skip timing the other layout")
-    ap.add_argument("--config", default="c2", choices=["c2", "c3", "c4", "c5"],
+    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c4", "c5"],
                     help="c2: the headline solve; c3: the precision stress (256^3 diffusion, per-level errors); "
                          "c4: the batched configuration (96 systems, 1-16 RHS each); "
-                         "c5: the learned preconditioner (training, then held-out 128^3 solves)")
+                         "c5: the learned preconditioner (training, then held-out 128^3 solves); "
+                         "c1: the reference's CPU configuration (64^3 hpcg, BJ-ILU(0) x112, CSR) on the GPU and, "
+                         "beside it, the reference's CPU solve")
     ap.add_argument("--c5-train", type=int, default=256, help="C5 training fields")
     ap.add_argument("--c5-eval", type=int, default=4, help="C5 held-out fields solved (32 for the full set)")
     ap.add_argument("--c5-steps", type=int, default=500, help="C5 Adam steps")
@@ -771,7 +845,9 @@ def main():
     set_size(args.nx)
     if args.impl == "ours":
         set_precond(args.precond, args.ilu_blocks, args.trsv_iters)
-    if args.config == "c5":
+    if args.config == "c1":
+        run_c1(args)
+    elif args.config == "c5":
         run_c5(args)
     elif args.config == "c4":
         run_c4(args)

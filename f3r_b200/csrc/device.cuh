@@ -77,6 +77,16 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
       : "memory");
 }
 
+namespace {
+// y = fp16(y * ome): the scaling the reference applies after a whole
+// preconditioner solve (hout *= ome[0], work/src/f3r.cpp:216, 229)
+__global__ void k_half_scale(__half *__restrict__ y, const __half *__restrict__ ome, int64_t n) {
+  const float om = __half2float(*ome);
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    y[i] = __float2half_rn(__half2float(y[i]) * om);
+}
+}  // namespace
+
 template <typename T>
 __device__ __forceinline__ T warp_sum(T v) {
 #pragma unroll

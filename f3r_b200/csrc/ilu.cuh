@@ -29,15 +29,25 @@ struct IluTri {
   int32_t *order = nullptr;                 // rows in (block, level) order
   int32_t *lvl_off = nullptr;               // row ranges of the levels, all blocks
   int32_t *blk_lvl = nullptr;               // per block: first level index (nblocks + 1)
+  int32_t *blk_pos = nullptr;               // per block: first vector position (nblocks + 1)
   int32_t nlevels_max = 0;
+  int32_t smem_rows = 0;  // > 0: blocks occupy contiguous positions, each at most this many rows
 };
 
+// One CTA per block-Jacobi block.  When the blocks occupy contiguous vector
+// positions (T.smem_rows > 0) the block's results are also kept in shared
+// memory, so a row reads the rows it depends on (all in its block, written
+// at earlier levels) from there instead of from L2: the same values in the
+// same order, a shorter wait per level.
 template <bool UPPER>
 __global__ void k_trsv_bj(IluTri T, const int32_t *__restrict__ rowpos, const __half *__restrict__ in,
                           __half *__restrict__ out, const __half *__restrict__ ome) {
+  extern __shared__ __half sy[];
   const int b = blockIdx.x;
   const int l0 = T.blk_lvl[b], l1 = T.blk_lvl[b + 1];
   const float om = ome ? __half2float(*ome) : 1.0f;
+  const bool sm = T.smem_rows > 0;
+  const int32_t p0 = sm ? T.blk_pos[b] : 0;
   for (int l = l0; l < l1; l++) {
     const int r0 = T.lvl_off[l], r1 = T.lvl_off[l + 1];
     for (int q = r0 + threadIdx.x; q < r1; q += blockDim.x) {
@@ -47,20 +57,31 @@ __global__ void k_trsv_bj(IluTri T, const int32_t *__restrict__ rowpos, const __
       if (!UPPER) {
         const int32_t e = T.rptr[i + 1] - 1;  // last entry is the unit diagonal
         for (int32_t j = T.rptr[i]; j < e; j++)
-          t = __fmaf_rn(-__half2float(T.val[j]), __half2float(out[T.idx[j]]), t);
-        out[p] = __float2half_rn(t);
+          t = __fmaf_rn(-__half2float(T.val[j]), __half2float(sm ? sy[T.idx[j] - p0] : out[T.idx[j]]), t);
+        const __half h = __float2half_rn(t);
+        out[p] = h;
+        if (sm) sy[p - p0] = h;
       } else {
         const int32_t d = T.rptr[i];  // first entry is the diagonal
         for (int32_t j = T.rptr[i + 1] - 1; j > d; j--)
-          t = __fmaf_rn(-__half2float(T.val[j]), __half2float(out[T.idx[j]]), t);
-        __half h = __float2half_rn(t * __half2float(T.dinv[i]));
-        if (ome) h = __float2half_rn(__half2float(h) * om);
+          t = __fmaf_rn(-__half2float(T.val[j]), __half2float(sm ? sy[T.idx[j] - p0] : out[T.idx[j]]), t);
+        const __half h = __float2half_rn(t * __half2float(T.dinv[i]));
         out[p] = h;
+        if (sm) sy[p - p0] = h;
       }
     }
     __syncthreads();
   }
+  // the reference solves, then scales: hout *= ome[0] (work/src/f3r.cpp:216, 229)
+  if (UPPER && ome) {
+    for (int q = T.lvl_off[l0] + threadIdx.x; q < T.lvl_off[l1]; q += blockDim.x) {
+      const int32_t p = rowpos[T.order[q]];
+      out[p] = __float2half_rn(__half2float(sm ? sy[p - p0] : out[p]) * om);
+    }
+  }
 }
+
+constexpr int32_t kIluSmemRows = 48 * 1024;  // fp16 results of one block in shared memory: 96 KB at most
 
 struct IluDevice {
   IluTri L, U;
@@ -125,6 +146,19 @@ struct IluDevice {
                    const std::vector<int32_t> &pos) {
     std::vector<int32_t> order, lvl_off, blk_lvl, idx(M.idx.size());
     levels(M, upper, bptr, order, lvl_off, blk_lvl, T.nlevels_max);
+    // blocks on contiguous positions (natural order) and of at most
+    // kIluSmemRows rows keep their results in shared memory
+    const int32_t nb = (int32_t)bptr.size() - 1;
+    std::vector<int32_t> bpos(nb + 1, 0);
+    bool contiguous = true;
+    int32_t maxlen = 0;
+    for (int32_t b = 0; b < nb; b++) {
+      bpos[b] = bptr[b] < bptr[b + 1] ? pos[bptr[b]] : 0;
+      maxlen = std::max(maxlen, bptr[b + 1] - bptr[b]);
+      for (int32_t i = bptr[b]; i < bptr[b + 1] && contiguous; i++) contiguous = pos[i] == bpos[b] + (i - bptr[b]);
+    }
+    T.smem_rows = (contiguous && maxlen <= kIluSmemRows) ? std::max(maxlen, 1) : 0;
+    if (up(&T.blk_pos, bpos) != cudaSuccess) return fail(F3R_ERROR_CUDA, "ILU upload failed");
     for (size_t j = 0; j < M.idx.size(); j++) idx[j] = pos[M.idx[j]];
     // fp16 values rounded once from fp64 (the reference casts CSR<double> to
     // CSR<__half>, csr.hpp:23-25)
@@ -155,13 +189,18 @@ struct IluDevice {
     if (up(&rowpos, pos) != cudaSuccess) return fail(F3R_ERROR_CUDA, "ILU upload failed");
     F3R_TRY(build_tri(L, Lh, false, bptr, pos));
     F3R_TRY(build_tri(U, Uh, true, bptr, pos));
+    // the attribute is the kernel's, shared by every solver: always the cap
+    const int cap = (int)(kIluSmemRows * sizeof(__half));
+    if (cudaFuncSetAttribute(k_trsv_bj<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, cap) != cudaSuccess ||
+        cudaFuncSetAttribute(k_trsv_bj<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, cap) != cudaSuccess)
+      return fail(F3R_ERROR_CUDA, "ILU shared-memory attribute");
     return F3R_SUCCESS;
   }
 
   // out = U^-1 L^-1 x (tmp holds L^-1 x); ome (nullable) scales the result
   Status apply(cudaStream_t st, const __half *x, __half *tmp, __half *out, const __half *ome) const {
-    k_trsv_bj<false><<<nblocks, 256, 0, st>>>(L, rowpos, x, tmp, nullptr);
-    k_trsv_bj<true><<<nblocks, 256, 0, st>>>(U, rowpos, tmp, out, ome);
+    k_trsv_bj<false><<<nblocks, 256, (size_t)L.smem_rows * sizeof(__half), st>>>(L, rowpos, x, tmp, nullptr);
+    k_trsv_bj<true><<<nblocks, 256, (size_t)U.smem_rows * sizeof(__half), st>>>(U, rowpos, tmp, out, ome);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return fail(F3R_ERROR_CUDA, std::string("ILU trsv launch: ") + cudaGetErrorString(e));
     return F3R_SUCCESS;
@@ -243,14 +282,12 @@ __device__ __forceinline__ bool wait_flags(const int32_t *flag, const int32_t (&
 
 template <bool UPPER>
 __global__ void __launch_bounds__(256) k_trsv_level(IluLevelTri T, const int32_t *__restrict__ rowpos,
-                                                    const __half *__restrict__ in, __half *out,
-                                                    const __half *__restrict__ ome, int *err) {
+                                                    const __half *__restrict__ in, __half *out, int *err) {
   __shared__ unsigned int gen_s;
   if (threadIdx.x == 0) gen_s = *(volatile unsigned int *)&T.state[2] + 1u;
   __syncthreads();
   const unsigned int gen = gen_s;
   const int lane = threadIdx.x & 31;
-  const float om = ome ? __half2float(*ome) : 1.0f;
   bool abort = false;
   while (true) {
     unsigned int c = 0;
@@ -286,13 +323,7 @@ __global__ void __launch_bounds__(256) k_trsv_level(IluLevelTri T, const int32_t
         for (int u = 0; u < kLevelBatch; u++)
           if (u < cnt) t = __fmaf_rn(-lv[u], y[u], t);
       }
-      __half h;
-      if (!UPPER) {
-        h = __float2half_rn(t);
-      } else {
-        h = __float2half_rn(t * __half2float(T.dinv[i]));
-        if (ome) h = __float2half_rn(__half2float(h) * om);
-      }
+      const __half h = UPPER ? __float2half_rn(t * __half2float(T.dinv[i])) : __float2half_rn(t);
       out[p] = h;
       __threadfence();
       st_release_u32(T.flag + p, gen);
@@ -314,7 +345,8 @@ __global__ void __launch_bounds__(256) k_trsv_level(IluLevelTri T, const int32_t
 struct IluLevel {
   IluLevelTri L, U;
   int32_t *rowpos = nullptr;
-  int grid = 0;
+  int grid = 0, scale_grid = 1;
+  int64_t n = 0;
   std::vector<void *> allocs;
 
   template <typename T> cudaError_t up(T **d, const std::vector<T> &h) {
@@ -361,6 +393,8 @@ struct IluLevel {
 
   Status build(int sm_count, const HostCSR &Lh, const HostCSR &Uh, const std::vector<int32_t> &perm, bool permuted) {
     const int32_t n = Lh.n;
+    this->n = n;
+    scale_grid = (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)sm_count * 8));
     std::vector<int32_t> pos(n);
     for (int32_t i = 0; i < n; i++) pos[i] = i;
     if (permuted)
@@ -378,8 +412,10 @@ struct IluLevel {
 
   // out = U^-1 L^-1 x (tmp holds L^-1 x); ome (nullable) scales the result
   Status apply(cudaStream_t st, const __half *x, __half *tmp, __half *out, const __half *ome, int *err) const {
-    k_trsv_level<false><<<grid, 256, 0, st>>>(L, rowpos, x, tmp, nullptr, err);
-    k_trsv_level<true><<<grid, 256, 0, st>>>(U, rowpos, tmp, out, ome, err);
+    k_trsv_level<false><<<grid, 256, 0, st>>>(L, rowpos, x, tmp, err);
+    k_trsv_level<true><<<grid, 256, 0, st>>>(U, rowpos, tmp, out, err);
+    // then the scaling, as the reference: hout *= ome[0] (work/src/f3r.cpp:216, 229)
+    if (ome) k_half_scale<<<scale_grid, 256, 0, st>>>(out, ome, n);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return fail(F3R_ERROR_CUDA, std::string("ILU trsv launch: ") + cudaGetErrorString(e));
     return F3R_SUCCESS;

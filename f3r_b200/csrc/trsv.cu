@@ -188,7 +188,10 @@ Status JacobiTrsv::apply(Context &c, const __half *in, __half *out, const __half
     for (int k = 1; k < iters; k++)
       launch_k(c, k_baj_sweep, gb, kBajWarps * 32, 0, c.stream, (const __half *)off.v16, (const int32_t *)off.col,
                (const int32_t *)off.sptr, off.nslices, (int64_t)n, in, (const __half *)dinv, out,
-               k == iters - 1 ? ome : nullptr, reverse ? 1 : 0);
+               (const __half *)nullptr, reverse ? 1 : 0);
+    // the in-place sweeps read rows that other warps rewrite, so the scaling
+    // follows the solve, as in the reference (hout *= ome[0], f3r.cpp:216, 229)
+    if (ome && iters > 1) launch_k(c, k_half_scale, g, kEwThreads, 0, c.stream, out, ome, (int64_t)n);
   } else {
     const float om = (float)omega, omc = 1.0f - om;
     __half *a = (iters % 2 == 0) ? out : tmp, *b = (iters % 2 == 0) ? tmp : out;
