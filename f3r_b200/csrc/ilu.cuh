@@ -23,25 +23,30 @@ namespace f3r {
 struct RichState;
 
 struct IluTri {
-  int32_t *rptr = nullptr, *idx = nullptr;  // idx mapped to vector positions
-  __half *val = nullptr;
-  __half *dinv = nullptr;                   // upper only: fp16(1 / u_ii), by row
-  int32_t *order = nullptr;                 // rows in (block, level) order
-  int32_t *lvl_off = nullptr;               // row ranges of the levels, all blocks
-  int32_t *blk_lvl = nullptr;               // per block: first level index (nblocks + 1)
-  int32_t *blk_pos = nullptr;               // per block: first vector position (nblocks + 1)
+  // the factor laid out in (block, level) row order q, as the kernel visits it
+  int4 *meta = nullptr;    // per q: vector position, first and end entry, unused
+  __half *val = nullptr;   // entries of every row in processing order (diagonal excluded)
+  int32_t *idx = nullptr;  // their columns, mapped to vector positions
+  __half *dinv = nullptr;  // upper only: fp16(1 / u_ii), per q
+  int32_t *lvl_off = nullptr;  // row ranges (in q) of the levels, all blocks
+  int32_t *blk_lvl = nullptr;  // per block: first level index (nblocks + 1)
+  int32_t *blk_pos = nullptr;  // per block: first vector position (nblocks + 1)
   int32_t nlevels_max = 0;
   int32_t smem_rows = 0;  // > 0: blocks occupy contiguous positions, each at most this many rows
 };
 
-// One CTA per block-Jacobi block.  When the blocks occupy contiguous vector
-// positions (T.smem_rows > 0) the block's results are also kept in shared
-// memory, so a row reads the rows it depends on (all in its block, written
-// at earlier levels) from there instead of from L2: the same values in the
-// same order, a shorter wait per level.
+// One CTA per block-Jacobi block.  The factor is stored in the order the
+// kernel visits rows (level by level within a block), so a row's data is one
+// int4 of metadata and a contiguous run of entries: two dependent loads,
+// coalesced across the threads of a level.  When the blocks occupy
+// contiguous vector positions (T.smem_rows > 0) the block's results are also
+// kept in shared memory, so a row reads the rows it depends on (all in its
+// block, written at earlier levels) from there instead of from L2.  The
+// terms are the reference's, in its order: the forward sweep by increasing
+// column, the backward sweep by decreasing column.
 template <bool UPPER>
-__global__ void k_trsv_bj(IluTri T, const int32_t *__restrict__ rowpos, const __half *__restrict__ in,
-                          __half *__restrict__ out, const __half *__restrict__ ome) {
+__global__ void k_trsv_bj(IluTri T, const __half *__restrict__ in, __half *__restrict__ out,
+                          const __half *__restrict__ ome) {
   extern __shared__ __half sy[];
   const int b = blockIdx.x;
   const int l0 = T.blk_lvl[b], l1 = T.blk_lvl[b + 1];
@@ -51,31 +56,20 @@ __global__ void k_trsv_bj(IluTri T, const int32_t *__restrict__ rowpos, const __
   for (int l = l0; l < l1; l++) {
     const int r0 = T.lvl_off[l], r1 = T.lvl_off[l + 1];
     for (int q = r0 + threadIdx.x; q < r1; q += blockDim.x) {
-      const int32_t i = T.order[q];
-      const int32_t p = rowpos[i];
-      float t = __half2float(in[p]);
-      if (!UPPER) {
-        const int32_t e = T.rptr[i + 1] - 1;  // last entry is the unit diagonal
-        for (int32_t j = T.rptr[i]; j < e; j++)
-          t = __fmaf_rn(-__half2float(T.val[j]), __half2float(sm ? sy[T.idx[j] - p0] : out[T.idx[j]]), t);
-        const __half h = __float2half_rn(t);
-        out[p] = h;
-        if (sm) sy[p - p0] = h;
-      } else {
-        const int32_t d = T.rptr[i];  // first entry is the diagonal
-        for (int32_t j = T.rptr[i + 1] - 1; j > d; j--)
-          t = __fmaf_rn(-__half2float(T.val[j]), __half2float(sm ? sy[T.idx[j] - p0] : out[T.idx[j]]), t);
-        const __half h = __float2half_rn(t * __half2float(T.dinv[i]));
-        out[p] = h;
-        if (sm) sy[p - p0] = h;
-      }
+      const int4 m = T.meta[q];
+      float t = __half2float(in[m.x]);
+      for (int32_t j = m.y; j < m.z; j++)
+        t = __fmaf_rn(-__half2float(T.val[j]), __half2float(sm ? sy[T.idx[j] - p0] : out[T.idx[j]]), t);
+      const __half h = UPPER ? __float2half_rn(t * __half2float(T.dinv[q])) : __float2half_rn(t);
+      out[m.x] = h;
+      if (sm) sy[m.x - p0] = h;
     }
     __syncthreads();
   }
   // the reference solves, then scales: hout *= ome[0] (work/src/f3r.cpp:216, 229)
   if (UPPER && ome) {
     for (int q = T.lvl_off[l0] + threadIdx.x; q < T.lvl_off[l1]; q += blockDim.x) {
-      const int32_t p = rowpos[T.order[q]];
+      const int32_t p = T.meta[q].x;
       out[p] = __float2half_rn(__half2float(sm ? sy[p - p0] : out[p]) * om);
     }
   }
@@ -85,7 +79,6 @@ constexpr int32_t kIluSmemRows = 48 * 1024;  // fp16 results of one block in sha
 
 struct IluDevice {
   IluTri L, U;
-  int32_t *rowpos = nullptr;  // original row -> vector position
   int32_t nblocks = 0;
   std::vector<void *> allocs;
 
@@ -144,7 +137,7 @@ struct IluDevice {
 
   Status build_tri(IluTri &T, const HostCSR &M, bool upper, const std::vector<int32_t> &bptr,
                    const std::vector<int32_t> &pos) {
-    std::vector<int32_t> order, lvl_off, blk_lvl, idx(M.idx.size());
+    std::vector<int32_t> order, lvl_off, blk_lvl;
     levels(M, upper, bptr, order, lvl_off, blk_lvl, T.nlevels_max);
     // blocks on contiguous positions (natural order) and of at most
     // kIluSmemRows rows keep their results in shared memory
@@ -158,18 +151,36 @@ struct IluDevice {
       for (int32_t i = bptr[b]; i < bptr[b + 1] && contiguous; i++) contiguous = pos[i] == bpos[b] + (i - bptr[b]);
     }
     T.smem_rows = (contiguous && maxlen <= kIluSmemRows) ? std::max(maxlen, 1) : 0;
-    if (up(&T.blk_pos, bpos) != cudaSuccess) return fail(F3R_ERROR_CUDA, "ILU upload failed");
-    for (size_t j = 0; j < M.idx.size(); j++) idx[j] = pos[M.idx[j]];
-    // fp16 values rounded once from fp64 (the reference casts CSR<double> to
-    // CSR<__half>, csr.hpp:23-25)
-    std::vector<double> v(M.val.begin(), M.val.end());
-    std::vector<double> dinv;
-    if (upper) {
-      dinv.resize(M.n);
-      for (int32_t i = 0; i < M.n; i++) dinv[i] = 1.0 / M.val[M.rptr[i]];
+    // the factor in visiting order: fp16 values rounded once from fp64 (the
+    // reference casts CSR<double> to CSR<__half>, csr.hpp:23-25)
+    const size_t nq = order.size();
+    std::vector<int4> meta(nq);
+    std::vector<double> v, dinv;
+    std::vector<int32_t> idx;
+    v.reserve(M.val.size());
+    idx.reserve(M.idx.size());
+    if (upper) dinv.resize(nq);
+    for (size_t q = 0; q < nq; q++) {
+      const int32_t i = order[q], r0 = M.rptr[i], r1 = M.rptr[i + 1];
+      meta[q].x = pos[i];
+      meta[q].y = (int32_t)idx.size();
+      if (!upper) {
+        for (int32_t j = r0; j < r1 - 1; j++) {  // last entry is the unit diagonal
+          v.push_back(M.val[j]);
+          idx.push_back(pos[M.idx[j]]);
+        }
+      } else {
+        for (int32_t j = r1 - 1; j > r0; j--) {  // first entry is the diagonal
+          v.push_back(M.val[j]);
+          idx.push_back(pos[M.idx[j]]);
+        }
+        dinv[q] = 1.0 / M.val[r0];
+      }
+      meta[q].z = (int32_t)idx.size();
+      meta[q].w = 0;
     }
-    if (up(&T.rptr, M.rptr) != cudaSuccess || up(&T.idx, idx) != cudaSuccess || up(&T.order, order) != cudaSuccess ||
-        up(&T.lvl_off, lvl_off) != cudaSuccess || up(&T.blk_lvl, blk_lvl) != cudaSuccess)
+    if (up(&T.meta, meta) != cudaSuccess || up(&T.idx, idx) != cudaSuccess || up(&T.lvl_off, lvl_off) != cudaSuccess ||
+        up(&T.blk_lvl, blk_lvl) != cudaSuccess || up(&T.blk_pos, bpos) != cudaSuccess)
       return fail(F3R_ERROR_CUDA, "ILU upload failed");
     F3R_TRY(to_half(&T.val, v));
     if (upper) F3R_TRY(to_half(&T.dinv, dinv));
@@ -186,7 +197,6 @@ struct IluDevice {
     if (permuted)
       for (int32_t s = 0; s < n; s++) pos[perm[s]] = s;
     nblocks = (int32_t)bptr.size() - 1;
-    if (up(&rowpos, pos) != cudaSuccess) return fail(F3R_ERROR_CUDA, "ILU upload failed");
     F3R_TRY(build_tri(L, Lh, false, bptr, pos));
     F3R_TRY(build_tri(U, Uh, true, bptr, pos));
     // the attribute is the kernel's, shared by every solver: always the cap
@@ -199,8 +209,8 @@ struct IluDevice {
 
   // out = U^-1 L^-1 x (tmp holds L^-1 x); ome (nullable) scales the result
   Status apply(cudaStream_t st, const __half *x, __half *tmp, __half *out, const __half *ome) const {
-    k_trsv_bj<false><<<nblocks, 256, (size_t)L.smem_rows * sizeof(__half), st>>>(L, rowpos, x, tmp, nullptr);
-    k_trsv_bj<true><<<nblocks, 256, (size_t)U.smem_rows * sizeof(__half), st>>>(U, rowpos, tmp, out, ome);
+    k_trsv_bj<false><<<nblocks, 256, (size_t)L.smem_rows * sizeof(__half), st>>>(L, x, tmp, nullptr);
+    k_trsv_bj<true><<<nblocks, 256, (size_t)U.smem_rows * sizeof(__half), st>>>(U, tmp, out, ome);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return fail(F3R_ERROR_CUDA, std::string("ILU trsv launch: ") + cudaGetErrorString(e));
     return F3R_SUCCESS;
