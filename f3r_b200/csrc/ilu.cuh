@@ -234,10 +234,11 @@ struct IluDevice {
 // finish resets the counter and advances the generation, so back-to-back
 // launches (and graph replays) need no host work.
 struct IluLevelTri {
-  int32_t *rptr = nullptr, *idx = nullptr;  // idx mapped to vector positions
-  __half *val = nullptr;
-  __half *dinv = nullptr;                   // upper only
-  int32_t *order = nullptr;                 // rows level by level, -1 padded to 32-row chunks
+  // rows level by level, padded to 32-row chunks, in the order warps take them
+  int4 *meta = nullptr;     // per slot: vector position (-1: padding), first and end entry
+  __half *val = nullptr;    // entries in processing order (diagonal excluded)
+  int32_t *idx = nullptr;   // their columns, mapped to vector positions
+  __half *dinv = nullptr;   // upper only: per slot
   int32_t nchunks = 0;
   int32_t nlevels = 0;
   int32_t *flag = nullptr;                  // per vector position: generation of its last write
@@ -291,8 +292,8 @@ __device__ __forceinline__ bool wait_flags(const int32_t *flag, const int32_t (&
 }
 
 template <bool UPPER>
-__global__ void __launch_bounds__(256) k_trsv_level(IluLevelTri T, const int32_t *__restrict__ rowpos,
-                                                    const __half *__restrict__ in, __half *out, int *err) {
+__global__ void __launch_bounds__(256, 2) k_trsv_level(IluLevelTri T, const __half *__restrict__ in, __half *out,
+                                                    int *err) {
   __shared__ unsigned int gen_s;
   if (threadIdx.x == 0) gen_s = *(volatile unsigned int *)&T.state[2] + 1u;
   __syncthreads();
@@ -304,14 +305,13 @@ __global__ void __launch_bounds__(256) k_trsv_level(IluLevelTri T, const int32_t
     if (lane == 0) c = atomicAdd(&T.state[0], 1u);
     c = __shfl_sync(0xffffffffu, c, 0);
     if (c >= (unsigned int)T.nchunks) break;
-    const int32_t i = T.order[(size_t)c * 32 + lane];
-    if (i >= 0) {
-      const int32_t p = rowpos[i];
+    const size_t slot = (size_t)c * 32 + lane;
+    const int4 m = T.meta[slot];
+    if (m.x >= 0) {
+      const int32_t p = m.x;
       float t = __half2float(in[p]);
-      const int32_t b = T.rptr[i], e = T.rptr[i + 1];
-      // lower: off-diagonals by increasing column (last entry = unit diagonal);
-      // upper: by decreasing column (first entry = diagonal)
-      const int32_t ndep = e - b - 1;
+      // the entries in processing order: lower by increasing, upper by decreasing column
+      const int32_t b = m.y, ndep = m.z - m.y;
       for (int32_t base = 0; base < ndep; base += kLevelBatch) {
         const int cnt = min(kLevelBatch, ndep - base);
         int32_t q[kLevelBatch];
@@ -319,7 +319,7 @@ __global__ void __launch_bounds__(256) k_trsv_level(IluLevelTri T, const int32_t
 #pragma unroll
         for (int u = 0; u < kLevelBatch; u++)
           if (u < cnt) {
-            const int32_t j = UPPER ? e - 1 - (base + u) : b + base + u;
+            const int32_t j = b + base + u;
             q[u] = T.idx[j];
             lv[u] = __half2float(T.val[j]);
           }
@@ -333,7 +333,7 @@ __global__ void __launch_bounds__(256) k_trsv_level(IluLevelTri T, const int32_t
         for (int u = 0; u < kLevelBatch; u++)
           if (u < cnt) t = __fmaf_rn(-lv[u], y[u], t);
       }
-      const __half h = UPPER ? __float2half_rn(t * __half2float(T.dinv[i])) : __float2half_rn(t);
+      const __half h = UPPER ? __float2half_rn(t * __half2float(T.dinv[slot])) : __float2half_rn(t);
       out[p] = h;
       __threadfence();
       st_release_u32(T.flag + p, gen);
@@ -354,7 +354,6 @@ __global__ void __launch_bounds__(256) k_trsv_level(IluLevelTri T, const int32_t
 
 struct IluLevel {
   IluLevelTri L, U;
-  int32_t *rowpos = nullptr;
   int grid = 0, scale_grid = 1;
   int64_t n = 0;
   std::vector<void *> allocs;
@@ -372,7 +371,7 @@ struct IluLevel {
 
   Status build_tri(IluLevelTri &T, const HostCSR &M, bool upper, const std::vector<int32_t> &pos) {
     const int32_t n = M.n;
-    std::vector<int32_t> order, lvl_off, blk_lvl, idx(M.idx.size());
+    std::vector<int32_t> order, lvl_off, blk_lvl;
     int32_t nl = 0;
     IluDevice::levels(M, upper, std::vector<int32_t>{0, n}, order, lvl_off, blk_lvl, nl);
     std::vector<int32_t> padded;
@@ -383,16 +382,37 @@ struct IluLevel {
     }
     T.nchunks = (int32_t)(padded.size() / 32);
     T.nlevels = nl;
-    for (size_t j = 0; j < M.idx.size(); j++) idx[j] = pos[M.idx[j]];
-    std::vector<double> v(M.val.begin(), M.val.end()), dinv;
-    if (upper) {
-      dinv.resize(n);
-      for (int32_t i = 0; i < n; i++) dinv[i] = 1.0 / M.val[M.rptr[i]];
+    // the factor in slot order; fp16 values rounded once from fp64
+    std::vector<int4> meta(padded.size());
+    std::vector<double> v, dinv(upper ? padded.size() : 0, 1.0);
+    std::vector<int32_t> idx;
+    v.reserve(M.val.size());
+    idx.reserve(M.idx.size());
+    for (size_t q = 0; q < padded.size(); q++) {
+      const int32_t i = padded[q];
+      meta[q] = make_int4(-1, 0, 0, 0);
+      if (i < 0) continue;
+      const int32_t r0 = M.rptr[i], r1 = M.rptr[i + 1];
+      meta[q].x = pos[i];
+      meta[q].y = (int32_t)idx.size();
+      if (!upper) {
+        for (int32_t j = r0; j < r1 - 1; j++) {  // last entry is the unit diagonal
+          v.push_back(M.val[j]);
+          idx.push_back(pos[M.idx[j]]);
+        }
+      } else {
+        for (int32_t j = r1 - 1; j > r0; j--) {  // first entry is the diagonal
+          v.push_back(M.val[j]);
+          idx.push_back(pos[M.idx[j]]);
+        }
+        dinv[q] = 1.0 / M.val[r0];
+      }
+      meta[q].z = (int32_t)idx.size();
     }
     const std::vector<int32_t> zeros(std::max(n, 1), 0);
     const std::vector<unsigned int> st(3, 0u);
-    if (up(&T.rptr, M.rptr) != cudaSuccess || up(&T.idx, idx) != cudaSuccess ||
-        up(&T.order, padded) != cudaSuccess || up(&T.flag, zeros) != cudaSuccess || up(&T.state, st) != cudaSuccess)
+    if (up(&T.meta, meta) != cudaSuccess || up(&T.idx, idx) != cudaSuccess || up(&T.flag, zeros) != cudaSuccess ||
+        up(&T.state, st) != cudaSuccess)
       return fail(F3R_ERROR_CUDA, "ILU upload failed");
     F3R_TRY(half_copy(&T.val, v));
     if (upper) F3R_TRY(half_copy(&T.dinv, dinv));
@@ -409,7 +429,6 @@ struct IluLevel {
     for (int32_t i = 0; i < n; i++) pos[i] = i;
     if (permuted)
       for (int32_t s = 0; s < n; s++) pos[perm[s]] = s;
-    if (up(&rowpos, pos) != cudaSuccess) return fail(F3R_ERROR_CUDA, "ILU upload failed");
     F3R_TRY(build_tri(L, Lh, false, pos));
     F3R_TRY(build_tri(U, Uh, true, pos));
     // warps for about four levels' chunks at a time: the frontier has work for
@@ -422,8 +441,8 @@ struct IluLevel {
 
   // out = U^-1 L^-1 x (tmp holds L^-1 x); ome (nullable) scales the result
   Status apply(cudaStream_t st, const __half *x, __half *tmp, __half *out, const __half *ome, int *err) const {
-    k_trsv_level<false><<<grid, 256, 0, st>>>(L, rowpos, x, tmp, err);
-    k_trsv_level<true><<<grid, 256, 0, st>>>(U, rowpos, tmp, out, err);
+    k_trsv_level<false><<<grid, 256, 0, st>>>(L, x, tmp, err);
+    k_trsv_level<true><<<grid, 256, 0, st>>>(U, tmp, out, err);
     // then the scaling, as the reference: hout *= ome[0] (work/src/f3r.cpp:216, 229)
     if (ome) k_half_scale<<<scale_grid, 256, 0, st>>>(out, ome, n);
     cudaError_t e = cudaGetLastError();
