@@ -25,6 +25,9 @@
 //   --precond SDAINV|BJILU0         default SDAINV for F3R (f3r-gpu.cpp:74),
 //                                   BJILU0 for the others (static.cpp:57-58)
 //   --blocks N                      block-Jacobi blocks, default 112
+//   --format SELL|CSR|AUTO          matrix storage on the GPU: SELL-32 (default), CSR as the CPU
+//                                   drivers store it (f3r.cpp:50; the same sums), or the layout
+//                                   autotuner's choice
 //   --tol EPS                       stop at ||r|| / ||b|| < EPS, default 1e-8
 //   --header                        print the CSV header line first
 //
@@ -51,7 +54,8 @@ namespace {
 int usage(const char *msg) {
   std::fprintf(stderr,
                "%s\nusage: f3r-run [--method F3R|F3R-Static|F3|F2] [--precond SDAINV|BJILU0] [--blocks N] "
-               "[--tol EPS] [--header] <matrix.mtx> <acc> <suite_iter> <m2> <m3> <m4> <c> <restart> [weight]\n",
+               "[--format SELL|CSR|AUTO] [--tol EPS] [--header] <matrix.mtx> <acc> <suite_iter> <m2> <m3> <m4> <c> "
+               "<restart> [weight]\n",
                msg);
   return 2;
 }
@@ -74,7 +78,7 @@ bool exists(const std::string &p) {
 }  // namespace
 
 int main(int argc, char **argv) {
-  std::string method = "F3R", precond;
+  std::string method = "F3R", precond, format = "SELL";
   int blocks = 112;
   double eps = 1e-8;
   bool header = false;
@@ -94,6 +98,11 @@ int main(int argc, char **argv) {
       const char *v = val();
       if (!v) return usage("--blocks needs a value");
       blocks = std::atoi(v);
+    } else if (a == "--format") {
+      const char *v = val();
+      if (!v) return usage("--format needs a value");
+      format = v;
+      if (format != "SELL" && format != "CSR" && format != "AUTO") return usage("--format is SELL, CSR or AUTO");
     } else if (a == "--tol") {
       const char *v = val();
       if (!v) return usage("--tol needs a value");
@@ -139,6 +148,8 @@ int main(int argc, char **argv) {
     p.c = c;
     p.precond = precond == "SDAINV" ? F3R_PRECOND_SDAINV : F3R_PRECOND_ILU0_BJ;
     p.ilu_blocks = blocks;
+    if (format == "CSR") p.format = F3R_FORMAT_CSR;
+    if (format == "AUTO") p.sell_autotune = 1;
     const bool gpu_build = method == "F3R" && precond == "SDAINV";  // the f3r16-gpu.exe configuration
     p.max_restarts = gpu_build ? 20 : restart;
     if (method == "F3" || method == "F2") {

@@ -59,6 +59,10 @@ def test_static_and_depth_lines(suite_dirs):
     r = python_solve(str(suite_dirs / "matrix" / "hpgmp_4_4_4.mtx"), m2=8, m3=4, m4=2, static_weight=1.2,
                      precond=F.PRECOND_ILU0_BJ, ilu_blocks=16, max_restarts=3)
     assert int(f[10]) == r.res_iter * 64 and float(f[12]) < 1e-7
+    # the CPU driver's CSR storage: the same sums, so the same line but for the time
+    fc = run(["--method", "F3R-Static", "--blocks", "16", "--format", "CSR", "hpgmp_4_4_4.mtx", "1.0", "1", "8", "4",
+              "2", "8", "3", "1.2"], cwd)[0].split(",")
+    assert fc[:9] == f[:9] and fc[10:] == f[10:]
     for method in ("F3", "F2"):
         f = run(["--method", method, "--blocks", "16", "hpgmp_4_4_4.mtx", "1.0", "1", "8", "4", "2", "8", "3"],
                 cwd)[0].split(",")
