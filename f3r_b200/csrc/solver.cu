@@ -389,6 +389,11 @@ using namespace f3r;
 // ---------------------------------------------------------------------------
 namespace f3r {
 
+__global__ void k_set_slots(double **in_slot, double **out_slot, double *in, double *out) {
+  *in_slot = in;
+  *out_slot = out;
+}
+
 template <typename T> struct Level {
   int m = 0;
   T *V = nullptr, *Z = nullptr;  // column-major n x (m+1), n x m (level 3 V column 0 is an alias)
@@ -661,8 +666,9 @@ struct Solver {
   // One call into level 2 for outer column j, replayed from a CUDA graph
   // keyed by which Richardson calls inside it update their weights.
   Status level2_call(double *in, double *out) {
-    CUDA_TRY(cudaMemcpyAsync((void *)in_slot, &in, sizeof(in), cudaMemcpyHostToDevice, C().stream));
-    CUDA_TRY(cudaMemcpyAsync((void *)out_slot, &out, sizeof(out), cudaMemcpyHostToDevice, C().stream));
+    // the graph reads its input and output columns from two device slots,
+    // set stream-ordered by a one-thread kernel (no host staging copy)
+    launch_k(C(), k_set_slots, 1, 1, 0, C().stream, in_slot, out_slot, in, out);
     // the legacy / per-thread default streams cannot be captured
     const cudaStream_t cs = C().stream;
     if (!p.use_graphs || cs == 0 || cs == cudaStreamLegacy || cs == cudaStreamPerThread) return level2();
@@ -697,10 +703,13 @@ struct Solver {
     return F3R_SUCCESS;
   }
 
+  // |e| and the device error word come back together, one synchronisation per outer step
   Status read_abs_e(double *v) {
+    int *e_h = reinterpret_cast<int *>(C().pinned + 7);
     CUDA_TRY(cudaMemcpyAsync(C().pinned, abs_e, sizeof(double), cudaMemcpyDeviceToHost, C().stream));
+    CUDA_TRY(cudaMemcpyAsync(e_h, C().err, sizeof(int), cudaMemcpyDeviceToHost, C().stream));
     CUDA_TRY(cudaStreamSynchronize(C().stream));
-    F3R_TRY(C().check_device_error());
+    if (*e_h != DEV_OK) return C().check_device_error();  // maps the word to a status and clears it
     *v = C().pinned[0];
     return F3R_SUCCESS;
   }
