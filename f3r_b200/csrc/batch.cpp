@@ -3,8 +3,10 @@
 //
 // The reference solves one system per driver run (work/src/f3r-gpu.cpp:88).
 // Here a solver's device objects (matrix copies, preconditioner, captured
-// inner-level graphs) serve every right-hand side given to it, one Krylov
-// solve per column; and independent solvers run concurrently, one host thread
+// inner-level graphs) serve every right-hand side given to it: up to 16
+// columns at once in lockstep, one block product per matrix pass
+// (Solver::solve_multi, solver.cu), or column by column where the nest has
+// no block form; and independent solvers run concurrently, one host thread
 // per context, so that their streams overlap on the GPU while each thread
 // waits for its own solves' residual checks.
 #include <algorithm>
@@ -24,12 +26,7 @@ f3r_status f3r_solver_solve_multi(f3r_solver *s, int32_t nrhs, const double *b, 
   if (!s || nrhs < 0 || (nrhs > 0 && (!b || !x))) return fail(F3R_ERROR_INVALID_VALUE, "bad argument");
   const int32_t n = solver_rows(s);
   if (ldb < n || ldx < n) return fail(F3R_ERROR_INVALID_VALUE, "leading dimension below the row count");
-  for (int32_t k = 0; k < nrhs; k++) {
-    f3r_result r{};
-    F3R_TRY(f3r_solver_solve(s, b + (size_t)k * ldb, x + (size_t)k * ldx, cond, user, &r));
-    if (results) results[k] = r;
-  }
-  return F3R_SUCCESS;
+  return solver_solve_multi(s, nrhs, b, ldb, x, ldx, cond, user, results);
 }
 
 f3r_status f3r_solve_batch(int32_t count, f3r_solver *const *solvers, const int32_t *nrhs, const double *const *b,

@@ -1,0 +1,914 @@
+// block.cuh -- K right-hand sides at once: the SELL product of K vectors
+// (block SpMM), and the Gram-Schmidt, Givens, Richardson and level kernels of
+// the nested solver over K columns.
+//
+// A block vector holds K columns interleaved by row, v[row * K + c], so the
+// K values a matrix entry multiplies are one contiguous 8..64-byte run: one
+// gather instruction feeds several columns, and the matrix (values and
+// slice metadata) is streamed once for all K.
+//
+// Every reduction kernel here splits rows over threads exactly as the
+// single-column kernel it generalises does (same grid, same rows per thread
+// and order, same warp / block / grid summation tree), and every product sums
+// a row in stored column order: column c of a K-column solve is therefore the
+// single-column solve of that right-hand side, bit for bit.  `active` is a
+// device word with bit c set for the columns still iterating; columns whose
+// bit is clear are finished (their results are final and no longer written
+// where that matters: Givens breakdown flags, the outer update x += Z y).
+#pragma once
+
+#include "kernels.cuh"
+
+namespace f3r {
+
+constexpr int kMaxBlock = 16;  // widest block of right-hand sides
+
+// a VecN (an aggregate of at most 16 bytes) through the read-only path
+template <typename T, int N> __device__ __forceinline__ VecN<T, N> ldg_vec(const VecN<T, N> *p) {
+  if constexpr (sizeof(VecN<T, N>) == 16) {
+    const int4 u = ::__ldg(reinterpret_cast<const int4 *>(p));
+    return *reinterpret_cast<const VecN<T, N> *>(&u);
+  } else if constexpr (sizeof(VecN<T, N>) == 8) {
+    const int2 u = ::__ldg(reinterpret_cast<const int2 *>(p));
+    return *reinterpret_cast<const VecN<T, N> *>(&u);
+  } else if constexpr (sizeof(VecN<T, N>) == 4) {
+    const int u = ::__ldg(reinterpret_cast<const int *>(p));
+    return *reinterpret_cast<const VecN<T, N> *>(&u);
+  } else {
+    const short u = ::__ldg(reinterpret_cast<const short *>(p));
+    return *reinterpret_cast<const VecN<T, N> *>(&u);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// K contiguous values of one row, 16-byte accesses where K allows
+// ---------------------------------------------------------------------------
+template <typename T, int K> struct RowK {
+  static constexpr int BYTES = (int)sizeof(T) * K;
+  static constexpr int VEC = BYTES >= 16 ? 16 / (int)sizeof(T) : K;  // elements per access
+  template <typename Acc> static __device__ __forceinline__ void load(const T *p, Acc (&o)[K]) {
+#pragma unroll
+    for (int q = 0; q < K / VEC; q++) {
+      const VecN<T, VEC> a = *reinterpret_cast<const VecN<T, VEC> *>(p + q * VEC);
+#pragma unroll
+      for (int e = 0; e < VEC; e++) o[q * VEC + e] = to_acc<Acc>(a.v[e]);
+    }
+  }
+  template <typename Acc> static __device__ __forceinline__ void ldg(const T *p, Acc (&o)[K]) {
+#pragma unroll
+    for (int q = 0; q < K / VEC; q++) {
+      const VecN<T, VEC> a = ldg_vec(reinterpret_cast<const VecN<T, VEC> *>(p + q * VEC));
+#pragma unroll
+      for (int e = 0; e < VEC; e++) o[q * VEC + e] = to_acc<Acc>(a.v[e]);
+    }
+  }
+  template <typename Acc> static __device__ __forceinline__ void store(T *p, const Acc (&v)[K]) {
+#pragma unroll
+    for (int q = 0; q < K / VEC; q++) {
+      VecN<T, VEC> a;
+#pragma unroll
+      for (int e = 0; e < VEC; e++) a.v[e] = cvt<T>(v[q * VEC + e]);
+      *reinterpret_cast<VecN<T, VEC> *>(p + q * VEC) = a;
+    }
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Block SELL product: out(:, c) = A x(:, c) for c < K, one pass over A.
+// Same layouts and bulk-copy ring as k_sell_cfg (sell.cuh); the index forms
+// are the packed int32 one (MODE 0) and the fully offset-aligned one (MODE 3).
+// Each lane owns one row of a slice and K accumulators, summing the row's
+// entries in stored order with one FMA per column.
+// ---------------------------------------------------------------------------
+template <typename V, int K, typename CI> struct BlockCfg;
+template <int K> struct BlockCfg<__half, K, int32_t> { static constexpr int WARPS = 16, STAGES = 2, KC = 16; };
+template <int K> struct BlockCfg<float, K, int32_t> { static constexpr int WARPS = 16, STAGES = 2, KC = 16; };
+template <int K> struct BlockCfg<double, K, int32_t> { static constexpr int WARPS = 12, STAGES = 2, KC = 16; };
+template <int K> struct BlockCfg<__half, K, AllAlignedIdx> { static constexpr int WARPS = 16, STAGES = 2, KC = 32; };
+template <int K> struct BlockCfg<float, K, AllAlignedIdx> { static constexpr int WARPS = 16, STAGES = 2, KC = 32; };
+template <int K> struct BlockCfg<double, K, AllAlignedIdx> { static constexpr int WARPS = 12, STAGES = 2, KC = 32; };
+
+template <typename V, int K, typename CI> constexpr size_t block_smem_bytes() {
+  using Cfg = BlockCfg<V, K, CI>;
+  return sell_smem_bytes_cfg<V, CI, Cfg::WARPS, Cfg::STAGES, Cfg::KC>();
+}
+
+template <typename V, typename X, typename Epi, int K, int WARPS, int STAGES, int KC, typename CI>
+__global__ void __launch_bounds__(WARPS * 32, 1)
+    k_sell_block(const V *__restrict__ val, DevSell A, const X *__restrict__ x, Epi epi, int *err) {
+  using Acc = typename acc_of<V>::type;
+  constexpr int MODE = IdxForm<CI>::mode;
+  static_assert(MODE == 0 || MODE == 3, "block product: packed int32 or fully aligned slices");
+  static_assert(MODE != 3 || KC == kAllAlignedChunk, "fully aligned layout is built for kAllAlignedChunk columns");
+  constexpr uint32_t VB = KC * 32 * sizeof(V), CB = KC * 32 * IdxForm<CI>::bytes, BB = MODE != 0 ? KC * 4 : 0,
+                     SB = VB + CB + BB;
+  // entries gathered per pipelined sub-block: about 64 gathered values per lane
+  constexpr int SUB = K >= 16 ? 4 : K >= 8 ? 8 : 16;
+  extern __shared__ __align__(128) unsigned char smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  unsigned char *buf = smem + (size_t)warp * STAGES * SB;
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem + (size_t)WARPS * STAGES * SB) + warp * STAGES;
+  if (lane == 0) {
+#pragma unroll
+    for (int s = 0; s < STAGES; s++) mbar_init(&bars[s], 1);
+    fence_mbar_init();
+  }
+  __syncwarp();
+  const uint64_t pol = l2_evict_first_policy();
+  const int TW = gridDim.x * WARPS;
+  int fs = blockIdx.x * WARPS + warp, fk = 0, fst = 0, inflight = 0;
+  int fs0 = 0, fw = 0, fcb = 0;
+  auto fetch = [&]() {
+    while (inflight < STAGES && fs < A.nslices) {
+      if (fk == 0) {
+        fs0 = A.sptr[fs];
+        fw = A.sptr[fs + 1] - fs0;
+        if (MODE == 3) fcb = A.cbptr[fs] & ~3;
+      }
+      if (fw == 0) {
+        fs += TW;
+        fk = 0;
+        continue;
+      }
+      const int kc = min(KC, fw - fk);
+      if (lane == 0) {
+        const size_t off = ((size_t)fs0 + fk) * 32;
+        fence_proxy_async_smem();
+        const uint32_t ib = MODE == 0 ? (uint32_t)kc * 32u * 4u : 0u;
+        const uint32_t bb = MODE == 3 ? (uint32_t)((kc + 3) & ~3) * 4u : 0u;
+        mbar_arrive_expect_tx(&bars[fst], (uint32_t)kc * 32u * (uint32_t)sizeof(V) + ib + bb);
+        bulk_g2s(buf + (size_t)fst * SB, val + off, (uint32_t)kc * 32u * (uint32_t)sizeof(V), &bars[fst], pol);
+        if (MODE == 0) bulk_g2s(buf + (size_t)fst * SB + VB, A.col + off, ib, &bars[fst], pol);
+        if (MODE == 3) bulk_g2s(buf + (size_t)fst * SB + VB + CB, A.cbase + fcb + fk, bb, &bars[fst], pol);
+      }
+      fst = (fst + 1 == STAGES) ? 0 : fst + 1;
+      inflight++;
+      fk += kc;
+      if (fk >= fw) {
+        fk = 0;
+        fs += TW;
+      }
+    }
+  };
+  auto release = [&]() {
+    __syncwarp();
+    inflight--;
+    fetch();
+  };
+  fetch();
+
+  int cs = blockIdx.x * WARPS + warp, ck = 0, cst = 0;
+  uint32_t phase = 0;
+  bool ok = true;
+  Acc acc[K];
+#pragma unroll
+  for (int c = 0; c < K; c++) acc[c] = 0;
+  int w = 0;
+  bool clampc = false;
+  while (cs < A.nslices) {
+    if (ck == 0) {
+      w = A.sptr[cs + 1] - A.sptr[cs];
+      if (MODE == 3) clampc = (A.cbptr[cs] & 1) != 0;
+    }
+    const int64_t r = (int64_t)cs * 32 + lane;
+    const bool live = r < A.n;
+    if (w == 0) {
+      if (live) epi.row(r, acc);
+      cs += TW;
+      continue;
+    }
+    const int kc = min(KC, w - ck);
+    if (!mbar_wait_bounded(&bars[cst], (phase >> cst) & 1u)) {
+      ok = false;
+      break;
+    }
+    phase ^= 1u << cst;
+    const V *sv = reinterpret_cast<const V *>(buf + (size_t)cst * SB);
+    const int32_t *sc = reinterpret_cast<const int32_t *>(buf + (size_t)cst * SB + VB);
+    const int32_t *sb = reinterpret_cast<const int32_t *>(buf + (size_t)cst * SB + VB + CB);
+    cst = (cst + 1 == STAGES) ? 0 : cst + 1;
+    // the chunk is worked in sub-blocks of SUB entries: values and columns
+    // first (then the stage goes back to the copy engine), then the gathers
+    // of the sub-block, then its multiply-adds
+    constexpr int NSUB = (KC + SUB - 1) / SUB;
+    V vv[SUB];
+    int32_t cc[SUB];
+    const V *lv = sv + lane * kc;  // aligned form: lane-major values
+    for (int h = 0; h < NSUB; h++) {
+      const int k0 = h * SUB;
+      if (k0 >= kc) break;
+#pragma unroll
+      for (int e = 0; e < SUB; e++) {
+        const int k = k0 + e;
+        if (k < kc) {
+          if (MODE == 3) {
+            vv[e] = lv[k];
+            const int32_t b = sb[k] + lane;
+            cc[e] = clampc ? min(max(b, 0), A.ncols - 1) : b;
+          } else {
+            vv[e] = sv[k * 32 + lane];
+            cc[e] = sc[k * 32 + lane];
+          }
+        }
+      }
+      if (k0 + SUB >= kc) release();  // last sub-block of the chunk: its shared data is in registers
+      Acc xg[SUB][K];
+#pragma unroll
+      for (int e = 0; e < SUB; e++)
+        if (k0 + e < kc) RowK<X, K>::ldg(x + (size_t)cc[e] * K, xg[e]);
+#pragma unroll
+      for (int e = 0; e < SUB; e++)
+        if (k0 + e < kc) {
+          const Acc v = to_acc<Acc>(vv[e]);
+#pragma unroll
+          for (int c = 0; c < K; c++) acc[c] = fmaT(v, xg[e][c], acc[c]);
+        }
+    }
+    ck += kc;
+    if (ck >= w) {
+      if (live) epi.row(r, acc);
+#pragma unroll
+      for (int c = 0; c < K; c++) acc[c] = 0;
+      ck = 0;
+      cs += TW;
+    }
+  }
+  if (!ok) {
+    if (lane == 0) atomicExch(err, (int)DEV_TIMEOUT_SPMV);
+    for (int i = 0; i < inflight; i++) {
+      mbar_wait_bounded(&bars[cst], (phase >> cst) & 1u);
+      phase ^= 1u << cst;
+      cst = (cst + 1 == STAGES) ? 0 : cst + 1;
+    }
+  }
+}
+
+// ---- epilogues of the block product (one row, K columns) --------------------
+// y(:, c) = A x(:, c)
+template <typename Out, int K> struct EpiStoreK {
+  Out *y;
+  template <typename Acc> __device__ __forceinline__ void row(int64_t r, const Acc (&acc)[K]) const {
+    RowK<Out, K>::store(y + r * K, acc);
+  }
+};
+// y(:, c) = b(:, c) - A x(:, c), the subtraction in the accumulator type
+template <typename B, typename Out, int K> struct EpiResidualK {
+  const B *b;
+  Out *y;
+  template <typename Acc> __device__ __forceinline__ void row(int64_t r, const Acc (&acc)[K]) const {
+    Acc bv[K], o[K];
+    RowK<B, K>::load(b + r * K, bv);
+#pragma unroll
+    for (int c = 0; c < K; c++) o[c] = bv[c] - acc[c];
+    RowK<Out, K>::store(y + r * K, o);
+  }
+};
+
+// Richardson step without a weight update, diagonal preconditioner fused
+// (EpiRichStepT, kernels.cuh, per column with the column's own weight):
+// hr = fp16(hin - A hout); t2 = z (w hr); hnew = fp16(hout + ome_c[k] t2); the
+// last step writes out = fp32(hnew) / sc instead.
+template <int K> struct EpiRichStepK {
+  const __half *hin, *hout;
+  DiagPre M;
+  const RichState *rs;  // K states
+  int k;
+  __half *hnext;
+  float *out;
+  float isc;
+  template <typename Acc> __device__ __forceinline__ void row(int64_t r, const Acc (&acc)[K]) const {
+    float hi[K], ho[K], res[K];
+    RowK<__half, K>::load(hin + r * K, hi);
+    RowK<__half, K>::load(hout + r * K, ho);
+    const __half w = M.w[r], z = M.z[r];
+#pragma unroll
+    for (int c = 0; c < K; c++) {
+      const __half hr = f2h(hi[c] - (float)acc[c]);
+      const __half t2 = __hmul(z, __hmul(w, hr));
+      res[c] = h2f(f2h(__fmaf_rn(h2f(rs[c].ome[k]), h2f(t2), ho[c])));
+    }
+    if (out) {
+#pragma unroll
+      for (int c = 0; c < K; c++) res[c] *= isc;
+      RowK<float, K>::store(out + r * K, res);
+    } else {
+      RowK<__half, K>::store(hnext + r * K, res);
+    }
+  }
+};
+
+// Residual step of an update call (diagonal M): hr and t2 = M hr stored
+template <int K> struct EpiRichResPreK {
+  const __half *hin;
+  DiagPre M;
+  __half *hr, *t2;
+  template <typename Acc> __device__ __forceinline__ void row(int64_t r, const Acc (&acc)[K]) const {
+    float hi[K], h[K], t[K];
+    RowK<__half, K>::load(hin + r * K, hi);
+    const float w = h2f(M.w[r]), z = h2f(M.z[r]);
+#pragma unroll
+    for (int c = 0; c < K; c++) {
+      h[c] = h2f(f2h(hi[c] - (float)acc[c]));
+      t[c] = z * h2f(f2h(w * h[c]));
+    }
+    RowK<__half, K>::store(hr + r * K, h);
+    RowK<__half, K>::store(t2 + r * K, t);
+  }
+};
+
+// General M, Z apply: hout = fp16(Z tmp), then on a call without a weight
+// update hout *= ome_c[0] (EpiZScale, per column)
+template <int K> struct EpiZScaleK {
+  __half *hout;
+  const RichState *rs;
+  int scale;
+  template <typename Acc> __device__ __forceinline__ void row(int64_t r, const Acc (&acc)[K]) const {
+    float o[K];
+#pragma unroll
+    for (int c = 0; c < K; c++) {
+      float h = h2f(f2h((float)acc[c]));
+      if (scale) h = h2f(rs[c].ome[0]) * h;
+      o[c] = h;
+    }
+    RowK<__half, K>::store(hout + r * K, o);
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Reductions over K columns.  Two final stages exist, each reproducing one of
+// the single-column kernels' trees exactly:
+//  * "block-strided" (grid_reduce, device.cuh): each thread adds the partial
+//    sums of blocks t, t + blockDim, ... ; a warp shuffle tree; thread 0 adds
+//    the warps in order;
+//  * "lane-strided" (k_multidot_chunked, kernels.cuh): one warp per value,
+//    lanes add blocks l, l + 32, ... ; a warp shuffle tree.
+// The block stage is the same in both: warp shuffle trees, then the warps of
+// the block added in order.  Partial sums are laid out [block][value].
+// ---------------------------------------------------------------------------
+
+// Per-column scalars of one FGMRES level: column c's H at H + c * hs
+// (column-major (m+1) x m), its cs, sn, e, y at + c * vs, its 1/h at inv[c].
+template <typename T> struct LevelK {
+  T *H, *cs, *sn, *e, *y, *inv;
+  int64_t hs, vs;
+  int ldh;  // m + 1
+  __device__ __forceinline__ GivensCtl<T> col(int c, int j, int compute_y, double *abs_e, int *err) const {
+    return GivensCtl<T>{H + c * hs, cs + c * vs, sn + c * vs, e + c * vs, y + c * vs, inv + c, abs_e, ldh, j,
+                        compute_y, err};
+  }
+};
+
+// block stage: v[q] (q < NQ, this thread's values) -> part[blockIdx.x * nq + q]
+template <typename T, int NQ, int WARPS>
+__device__ __forceinline__ void block_partials(T (&v)[NQ], int nq, int q0, int ntot, T *part, T (&sred)[WARPS][NQ]) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < NQ; q++) {
+    if (q < nq) {
+      const T s = warp_sum(v[q]);
+      if (lane == 0) sred[warp][q] = s;
+    }
+  }
+  __syncthreads();
+  if ((int)threadIdx.x < nq) {
+    T s = 0;
+    for (int w = 0; w < WARPS; w++) s += sred[w][threadIdx.x];
+    part[(size_t)blockIdx.x * ntot + q0 + threadIdx.x] = s;
+  }
+  __syncthreads();
+}
+
+// true in the last block to arrive (after every block wrote its partials)
+__device__ __forceinline__ bool last_block(unsigned int *ticket) {
+  __shared__ bool last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = (atomicAdd(ticket, 1u) == gridDim.x - 1);
+  __syncthreads();
+  if (last) __threadfence();
+  return last;
+}
+
+// final stage, block-strided: value q of ntot -> returned on thread 0
+template <typename T, int WARPS> __device__ __forceinline__ T final_block_strided(const T *part, int q, int ntot) {
+  __shared__ T sw[WARPS];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  T s = 0;
+  for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) s += __ldcg(&part[(size_t)b * ntot + q]);
+  s = warp_sum(s);
+  if (lane == 0) sw[warp] = s;
+  __syncthreads();
+  T t = 0;
+  if (threadIdx.x == 0)
+    for (int w = 0; w < WARPS; w++) t += sw[w];
+  __syncthreads();
+  return t;
+}
+
+// <x(:, c), y(:, c)> for c < K (kmm::dot; k_dot of kernels.cuh): one element
+// per thread and grid stride, block-strided final stage
+template <typename T, typename Acc, int WARPS, int K>
+__global__ void __launch_bounds__(WARPS * 32) k_dotK(const T *__restrict__ x, const T *__restrict__ y, int64_t n,
+                                                     GridRed gr, Acc *out) {
+  __shared__ Acc sred[WARPS][K];
+  Acc a[K];
+#pragma unroll
+  for (int c = 0; c < K; c++) a[c] = 0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    Acc xv[K], yv[K];
+    RowK<T, K>::load(x + i * K, xv);
+    RowK<T, K>::load(y + i * K, yv);
+#pragma unroll
+    for (int c = 0; c < K; c++) a[c] = fmaT(xv[c], yv[c], a[c]);
+  }
+  Acc *part = static_cast<Acc *>(gr.partials);
+  block_partials<Acc, K, WARPS>(a, K, 0, K, part, sred);
+  if (!last_block(gr.ticket)) return;
+  for (int c = 0; c < K; c++) {
+    const Acc t = final_block_strided<Acc, WARPS>(part, c, K);
+    if (threadIdx.x == 0) out[c] = t;
+  }
+  if (threadIdx.x == 0) *gr.ticket = 0;
+}
+
+// H(j, k)(c) = <w(:, c), V(k)(:, c)>, k < nv, one element per thread and
+// grid stride, lane-strided final stage (k_multidot_chunked): the outer fp64
+// level and inner fp32 levels with more than 8 basis vectors.  Column c's
+// values go to hcol + c * hstride.
+template <typename T, int WARPS, int K>
+__global__ void __launch_bounds__(WARPS * 32) k_multidot_chunkedK(const T *__restrict__ w, Cols<T> V, int nv,
+                                                                  int64_t n, GridRed gr, T *hcol, int64_t hstride) {
+  constexpr int CH = K >= 8 ? 1 : 8 / K;  // basis vectors per pass over w
+  constexpr int NQ = CH * K;
+  __shared__ T sred[WARPS][NQ];
+  T *part = static_cast<T *>(gr.partials);
+  const int ntot = nv * K;
+  for (int k0 = 0; k0 < nv; k0 += CH) {
+    T a[NQ];
+#pragma unroll
+    for (int q = 0; q < NQ; q++) a[q] = 0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+      T wv[K];
+      RowK<T, K>::load(w + i * K, wv);
+#pragma unroll
+      for (int v = 0; v < CH; v++) {
+        if (k0 + v < nv) {
+          T vv[K];
+          RowK<T, K>::load(V.p[k0 + v] + i * K, vv);
+#pragma unroll
+          for (int c = 0; c < K; c++) a[v * K + c] = fmaT(wv[c], vv[c], a[v * K + c]);
+        }
+      }
+    }
+    const int nq = min(CH, nv - k0) * K;
+    block_partials<T, NQ, WARPS>(a, nq, k0 * K, ntot, part, sred);
+  }
+  if (!last_block(gr.ticket)) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int q = warp; q < ntot; q += WARPS) {
+    T t = 0;
+    for (int b = lane; b < (int)gridDim.x; b += 32) t += __ldcg(&part[(size_t)b * ntot + q]);
+    t = warp_sum(t);
+    if (lane == 0) hcol[(q % K) * hstride + q / K] = t;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) *gr.ticket = 0;
+}
+
+// H(j, k)(c) = <w(:, c), V(k)(:, c)> for nv <= MAXV basis vectors in fp32
+// (k_multidot_f32): rows in groups of 4 per thread, block-strided final stage
+template <int MAXV, int WARPS, int K>
+__global__ void __launch_bounds__(WARPS * 32) k_multidot_f32K(const float *__restrict__ w, Cols<float> V, int nv,
+                                                              int64_t n, GridRed gr, float *hcol, int64_t hstride) {
+  constexpr int CV = (MAXV * K > 32) ? (32 / K > 0 ? 32 / K : 1) : MAXV;  // basis vectors per pass
+  constexpr int NQ = CV * K;
+  __shared__ float sred[WARPS][NQ];
+  float *part = static_cast<float *>(gr.partials);
+  const int ntot = nv * K;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x, tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t nq4 = n / 4;
+  for (int k0 = 0; k0 < nv; k0 += CV) {
+    float a[NQ];
+#pragma unroll
+    for (int q = 0; q < NQ; q++) a[q] = 0.0f;
+    for (int64_t q4 = tid; q4 < nq4; q4 += stride) {
+#pragma unroll
+      for (int e = 0; e < 4; e++) {
+        float wv[K];
+        RowK<float, K>::load(w + (4 * q4 + e) * K, wv);
+#pragma unroll
+        for (int v = 0; v < CV; v++) {
+          if (k0 + v < nv) {
+            float vv[K];
+            RowK<float, K>::load(V.p[k0 + v] + (4 * q4 + e) * K, vv);
+#pragma unroll
+            for (int c = 0; c < K; c++) a[v * K + c] = __fmaf_rn(wv[c], vv[c], a[v * K + c]);
+          }
+        }
+      }
+    }
+    for (int64_t i = nq4 * 4 + tid; i < n; i += stride) {
+      float wv[K];
+      RowK<float, K>::load(w + i * K, wv);
+#pragma unroll
+      for (int v = 0; v < CV; v++) {
+        if (k0 + v < nv) {
+          float vv[K];
+          RowK<float, K>::load(V.p[k0 + v] + i * K, vv);
+#pragma unroll
+          for (int c = 0; c < K; c++) a[v * K + c] = __fmaf_rn(wv[c], vv[c], a[v * K + c]);
+        }
+      }
+    }
+    const int nq = min(CV, nv - k0) * K;
+    block_partials<float, NQ, WARPS>(a, nq, k0 * K, ntot, part, sred);
+  }
+  if (!last_block(gr.ticket)) return;
+  for (int q = 0; q < ntot; q++) {
+    const float t = final_block_strided<float, WARPS>(part, q, ntot);
+    if (threadIdx.x == 0) hcol[(q % K) * hstride + q / K] = t;
+  }
+  if (threadIdx.x == 0) *gr.ticket = 0;
+}
+
+// w(:, c) -= sum_k H(j, k)(c) V(k)(:, c) (MULMV order), then ||w(:, c)||^2 ->
+// Givens of column c for the columns in *active (k_cgs_update): N elements
+// per thread (16 bytes of one column), block-strided final stage.
+template <typename T, int WARPS, int K>
+__global__ void __launch_bounds__(WARPS * 32) k_cgs_updateK(T *__restrict__ w, Cols<T> V, int nv, int64_t n,
+                                                            GridRed gr, LevelK<T> L, int j, int compute_y,
+                                                            double *abs_e, const uint32_t *active, int *err) {
+  constexpr int N = 16 / sizeof(T);
+  __shared__ T sh[K][kMaxCols];
+  __shared__ T sred[WARPS][K];
+  for (int t = threadIdx.x; t < nv * K; t += blockDim.x) {
+    const int c = t / nv, k = t % nv;
+    sh[c][k] = L.H[c * L.hs + (int64_t)j * L.ldh + k];
+  }
+  __syncthreads();
+  T part[K];
+#pragma unroll
+  for (int c = 0; c < K; c++) part[c] = 0;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x, tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t nq = n / N;
+  for (int64_t q = tid; q < nq; q += stride) {
+#pragma unroll
+    for (int e = 0; e < N; e++) {
+      const int64_t i = q * N + e;
+      T a[K], r[K], wv[K];
+      RowK<T, K>::load(V.p[0] + i * K, a);
+#pragma unroll
+      for (int c = 0; c < K; c++) r[c] = mul_rn(a[c], sh[c][0]);
+      for (int k = 1; k < nv; k++) {
+        T b[K];
+        RowK<T, K>::load(V.p[k] + i * K, b);
+#pragma unroll
+        for (int c = 0; c < K; c++) r[c] = fmaT(b[c], sh[c][k], r[c]);
+      }
+      RowK<T, K>::load(w + i * K, wv);
+#pragma unroll
+      for (int c = 0; c < K; c++) wv[c] = sub_rn(wv[c], r[c]);
+      RowK<T, K>::store(w + i * K, wv);
+    }
+    // the norm in the single-column kernel's order: element by element
+#pragma unroll
+    for (int e = 0; e < N; e++) {
+      T wv[K];
+      RowK<T, K>::load(w + (q * N + e) * K, wv);
+#pragma unroll
+      for (int c = 0; c < K; c++) part[c] = fmaT(wv[c], wv[c], part[c]);
+    }
+  }
+  for (int64_t i = nq * N + tid; i < n; i += stride) {
+    T a[K], r[K], wv[K];
+    RowK<T, K>::load(V.p[0] + i * K, a);
+#pragma unroll
+    for (int c = 0; c < K; c++) r[c] = mul_rn(a[c], sh[c][0]);
+    for (int k = 1; k < nv; k++) {
+      T b[K];
+      RowK<T, K>::load(V.p[k] + i * K, b);
+#pragma unroll
+      for (int c = 0; c < K; c++) r[c] = fmaT(b[c], sh[c][k], r[c]);
+    }
+    RowK<T, K>::load(w + i * K, wv);
+#pragma unroll
+    for (int c = 0; c < K; c++) {
+      wv[c] = sub_rn(wv[c], r[c]);
+      part[c] = fmaT(wv[c], wv[c], part[c]);
+    }
+    RowK<T, K>::store(w + i * K, wv);
+  }
+  T *parts = static_cast<T *>(gr.partials);
+  block_partials<T, K, WARPS>(part, K, 0, K, parts, sred);
+  if (!last_block(gr.ticket)) return;
+  const uint32_t act = *active;
+  for (int c = 0; c < K; c++) {
+    const T t = final_block_strided<T, WARPS>(parts, c, K);
+    if (threadIdx.x == 0 && ((act >> c) & 1u)) givens_step<T>(L.col(c, j, compute_y, abs_e ? abs_e + c : nullptr, err), t);
+  }
+  if (threadIdx.x == 0) *gr.ticket = 0;
+}
+
+// ||r(:, c)|| of the outer residual (V(0) = b - A x, stored by the product):
+// e(0) = ||r||, 1/||r|| and |e(0)| for the host, per column (gmres.hpp:87,
+// 100-103).  Two elements per thread (16 bytes of one column).
+template <int WARPS, int K>
+__global__ void __launch_bounds__(WARPS * 32) k_resnormK(const double *__restrict__ r, int64_t n, GridRed gr,
+                                                         LevelK<double> L, double *abs_e, const uint32_t *active) {
+  __shared__ double sred[WARPS][K];
+  double part[K];
+#pragma unroll
+  for (int c = 0; c < K; c++) part[c] = 0;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x, tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  for (int64_t i = tid; i < n; i += stride) {
+    double v[K];
+    RowK<double, K>::load(r + i * K, v);
+#pragma unroll
+    for (int c = 0; c < K; c++) part[c] = __fma_rn(v[c], v[c], part[c]);
+  }
+  double *parts = static_cast<double *>(gr.partials);
+  block_partials<double, K, WARPS>(part, K, 0, K, parts, sred);
+  if (!last_block(gr.ticket)) return;
+  const uint32_t act = *active;
+  for (int c = 0; c < K; c++) {
+    const double t = final_block_strided<double, WARPS>(parts, c, K);
+    if (threadIdx.x == 0 && ((act >> c) & 1u)) {
+      const double h = sqrt(t);
+      L.e[c * L.vs] = h;
+      L.inv[c] = 1.0 / h;
+      abs_e[c] = fabs(h);
+    }
+  }
+  if (threadIdx.x == 0) *gr.ticket = 0;
+}
+
+// The Richardson weight of an update call, per column: with t = tmp(:, c)
+// (fp16(A v), stored by the product) and o = other(:, c), om = <t, o> / <t, t>
+// in fp32 (wildcard(., tof32), f3r-gpu.cpp:235-240 / 249-254), then the
+// running mean ome[k] = fp16(sum[k] / den); k = 0 also advances den.  Rows
+// in groups of 4 per thread, block-strided final stage.
+template <int WARPS, int K>
+__global__ void __launch_bounds__(WARPS * 32) k_rich_weightK(const __half *__restrict__ tmp,
+                                                             const __half *__restrict__ other, int64_t n,
+                                                             GridRed gr, RichState *rs, int k) {
+  __shared__ float sred[WARPS][2 * K];
+  float d[2 * K];
+#pragma unroll
+  for (int q = 0; q < 2 * K; q++) d[q] = 0.0f;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x, tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  for (int64_t i = tid; i < n; i += stride) {
+    float t[K], o[K];
+    RowK<__half, K>::load(tmp + i * K, t);
+    RowK<__half, K>::load(other + i * K, o);
+#pragma unroll
+    for (int c = 0; c < K; c++) {
+      d[c] = __fmaf_rn(t[c], t[c], d[c]);
+      d[K + c] = __fmaf_rn(t[c], o[c], d[K + c]);
+    }
+  }
+  float *parts = static_cast<float *>(gr.partials);
+  block_partials<float, 2 * K, WARPS>(d, 2 * K, 0, 2 * K, parts, sred);
+  if (!last_block(gr.ticket)) return;
+  for (int c = 0; c < K; c++) {
+    const float tt = final_block_strided<float, WARPS>(parts, c, 2 * K);
+    const float to = final_block_strided<float, WARPS>(parts, K + c, 2 * K);
+    if (threadIdx.x == 0) {
+      RichState *s = rs + c;
+      const float om = to / tt;
+      s->om[k] = om;
+      s->sum[k] += om;
+      if (k == 0) s->den += 1;
+      s->ome[k] = __float2half_rn(s->sum[k] / (float)s->den);
+    }
+  }
+  if (threadIdx.x == 0) *gr.ticket = 0;
+}
+
+// ---------------------------------------------------------------------------
+// Elementwise kernels of the levels over K columns (grid stride over rows;
+// each element computed exactly as the single-column kernel computes it).
+// Narrow blocks take RowsPer<K> consecutive rows per thread, so that a thread
+// still moves 16 bytes of fp32 per access; the rows of a group are contiguous
+// (row-major interleaving), element e of a group is column e % K.
+// ---------------------------------------------------------------------------
+template <int K> struct RowsPer {
+  static constexpr int R = K >= 4 ? 1 : 4 / K;
+};
+// calls f(row0, std::integral_constant<int, ROWS>) for groups of R rows, then
+// for the remaining rows one at a time
+template <int R, typename F> __device__ __forceinline__ void for_row_groups(int64_t n, F f) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x, tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t ng = n / R;
+  for (int64_t q = tid; q < ng; q += stride) f(q * R, std::integral_constant<int, R>());
+  if constexpr (R > 1)
+    for (int64_t i = ng * R + tid; i < n; i += stride) f(i, std::integral_constant<int, 1>());
+}
+
+// Level-2 entry (k_level2_enter): V1(j)(:, c) *= 1/h_c in place, then
+// V2(0) = float(V1(j)); e_c(0) = 1.
+template <int K>
+__global__ void k_level2_enterK(double *const *__restrict__ in_slot, const double *__restrict__ inv,
+                                float *__restrict__ v0, float *e, int64_t e_stride, int64_t n) {
+  double *in = *in_slot;
+  double s[K];
+#pragma unroll
+  for (int c = 0; c < K; c++) s[c] = inv[c];
+  if (blockIdx.x == 0 && threadIdx.x < K) e[threadIdx.x * e_stride] = 1.0f;
+  for_row_groups<RowsPer<K>::R>(n, [&](int64_t i0, auto rows) {
+    constexpr int E = decltype(rows)::value * K;
+    double a[E];
+    float o[E];
+    RowK<double, E>::load(in + i0 * K, a);
+#pragma unroll
+    for (int q = 0; q < E; q++) {
+      a[q] *= s[q % K];
+      o[q] = (float)a[q];
+    }
+    RowK<double, E>::store(in + i0 * K, a);
+    RowK<float, E>::store(v0 + i0 * K, o);
+  });
+}
+
+// x(:, c) = Z y_c (inner levels) or x(:, c) += Z y_c for the columns in mask
+// (outer level), the sum in the level's type T (k_zy)
+template <typename T, typename Out, bool ACCUM, int K>
+__global__ void k_zyK(Cols<T> Z, const T *__restrict__ y, int64_t y_stride, int nz, Out *out_direct,
+                      Out *const *out_slot, uint32_t mask, int64_t n) {
+  __shared__ T sy[K][kMaxCols];
+  for (int t = threadIdx.x; t < nz * K; t += blockDim.x) {
+    const int c = t / nz, k = t % nz;
+    sy[c][k] = y[c * y_stride + k];
+  }
+  __syncthreads();
+  Out *out = out_slot ? *out_slot : out_direct;
+  for_row_groups<RowsPer<K>::R>(n, [&](int64_t i0, auto rows) {
+    constexpr int E = decltype(rows)::value * K;
+    T a[E], r[E];
+    RowK<T, E>::load(Z.p[0] + i0 * K, a);
+#pragma unroll
+    for (int q = 0; q < E; q++) r[q] = mul_rn(a[q], sy[q % K][0]);
+    for (int k = 1; k < nz; k++) {
+      T b[E];
+      RowK<T, E>::load(Z.p[k] + i0 * K, b);
+#pragma unroll
+      for (int q = 0; q < E; q++) r[q] = fmaT(b[q], sy[q % K][k], r[q]);
+    }
+    if (ACCUM) {
+#pragma unroll
+      for (int q = 0; q < E; q++)
+        if ((mask >> (q % K)) & 1u) out[i0 * K + q] = add_rn(out[i0 * K + q], (Out)r[q]);
+    } else {
+      Out o[E];
+#pragma unroll
+      for (int q = 0; q < E; q++) o[q] = (Out)r[q];
+      RowK<Out, E>::store(out + i0 * K, o);
+    }
+  });
+}
+
+// First half of R, diagonal M (k_rich_enter_diag), per column: the pending
+// normalisation of in(:, c) (in_inv[c], or none), hin = fp16(in * sc),
+// hout = M hin, times ome_c[0] on a call without a weight update; e_c(0) = 1
+// of the calling level when e_set is given.
+template <bool SCALE_BY_OME, int K>
+__global__ void k_rich_enter_diagK(float *__restrict__ in, const float *__restrict__ in_inv, float sc, DiagPre M,
+                                   __half *__restrict__ hin, __half *__restrict__ hout,
+                                   const RichState *__restrict__ rs, float *e_set, int64_t e_stride, int64_t n) {
+  if (e_set && blockIdx.x == 0 && threadIdx.x < K) e_set[threadIdx.x * e_stride] = 1.0f;
+  float om[K], s[K];
+#pragma unroll
+  for (int c = 0; c < K; c++) {
+    om[c] = SCALE_BY_OME ? h2f(rs[c].ome[0]) : 1.0f;
+    s[c] = in_inv ? in_inv[c] : 1.0f;
+  }
+  for_row_groups<RowsPer<K>::R>(n, [&](int64_t i0, auto rows) {
+    constexpr int NR = decltype(rows)::value, E = NR * K;
+    float v[E], hi[E], ho[E], w[NR], z[NR];
+    RowK<float, E>::load(in + i0 * K, v);
+    if (in_inv) {
+#pragma unroll
+      for (int q = 0; q < E; q++) v[q] *= s[q % K];
+      RowK<float, E>::store(in + i0 * K, v);
+    }
+    RowK<__half, NR>::load(M.w + i0, w);
+    RowK<__half, NR>::load(M.z + i0, z);
+#pragma unroll
+    for (int q = 0; q < E; q++) {
+      const __half h = f2h(v[q] * sc);
+      hi[q] = h2f(h);
+      const float t = h2f(f2h(w[q / K] * hi[q]));
+      float o = h2f(f2h(z[q / K] * t));
+      if (SCALE_BY_OME) o = h2f(f2h(o * om[q % K]));
+      ho[q] = o;
+    }
+    RowK<__half, E>::store(hin + i0 * K, hi);
+    RowK<__half, E>::store(hout + i0 * K, ho);
+  });
+}
+
+// General M: (normalise in place), hin = fp16(in * sc) (k_rich_cast_in)
+template <int K>
+__global__ void k_rich_cast_inK(float *__restrict__ in, const float *__restrict__ in_inv, float sc,
+                                __half *__restrict__ hin, float *e_set, int64_t e_stride, int64_t n) {
+  if (e_set && blockIdx.x == 0 && threadIdx.x < K) e_set[threadIdx.x * e_stride] = 1.0f;
+  for_row_groups<RowsPer<K>::R>(n, [&](int64_t i0, auto rows) {
+    constexpr int E = decltype(rows)::value * K;
+    float v[E], h[E];
+    RowK<float, E>::load(in + i0 * K, v);
+    if (in_inv) {
+#pragma unroll
+      for (int q = 0; q < E; q++) v[q] *= in_inv[q % K];
+      RowK<float, E>::store(in + i0 * K, v);
+    }
+#pragma unroll
+    for (int q = 0; q < E; q++) h[q] = v[q] * sc;
+    RowK<__half, E>::store(hin + i0 * K, h);
+  });
+}
+
+// hout(:, c) = fp16(hout * fp16(om_c[0])) (k_rich_scale_om)
+template <int K>
+__global__ void k_rich_scale_omK(__half *__restrict__ hout, const RichState *__restrict__ rs, int64_t n) {
+  float om[K];
+#pragma unroll
+  for (int c = 0; c < K; c++) om[c] = h2f(f2h(rs[c].om[0]));
+  for_row_groups<RowsPer<K>::R>(n, [&](int64_t i0, auto rows) {
+    constexpr int E = decltype(rows)::value * K;
+    float h[E];
+    RowK<__half, E>::load(hout + i0 * K, h);
+#pragma unroll
+    for (int q = 0; q < E; q++) h[q] = h[q] * om[q % K];
+    RowK<__half, E>::store(hout + i0 * K, h);
+  });
+}
+
+// hout(:, c) = fp16(hout + om_c[k] t2), or on the last step out = fp32(that)
+// / sc (k_rich_axpy); use_ome selects ome_c[k]
+template <int K>
+__global__ void k_rich_axpyK(__half *__restrict__ hout, const __half *__restrict__ t2,
+                             const RichState *__restrict__ rs, int k, int use_ome, float *__restrict__ out, float isc,
+                             int64_t n) {
+  float om[K];
+#pragma unroll
+  for (int c = 0; c < K; c++) om[c] = use_ome ? h2f(rs[c].ome[k]) : rs[c].om[k];
+  for_row_groups<RowsPer<K>::R>(n, [&](int64_t i0, auto rows) {
+    constexpr int E = decltype(rows)::value * K;
+    float h[E], t[E], hn[E];
+    RowK<__half, E>::load(hout + i0 * K, h);
+    RowK<__half, E>::load(t2 + i0 * K, t);
+#pragma unroll
+    for (int q = 0; q < E; q++) hn[q] = h2f(f2h(__fmaf_rn(om[q % K], t[q], h[q])));
+    if (out) {
+#pragma unroll
+      for (int q = 0; q < E; q++) hn[q] *= isc;
+      RowK<float, E>::store(out + i0 * K, hn);
+    } else {
+      RowK<__half, E>::store(hout + i0 * K, hn);
+    }
+  });
+}
+
+// out = fp32(hout) / sc (k_rich_exit)
+template <int K>
+__global__ void k_rich_exitK(const __half *__restrict__ hout, float *__restrict__ out, float isc, int64_t n) {
+  for_row_groups<RowsPer<K>::R>(n, [&](int64_t i0, auto rows) {
+    constexpr int E = decltype(rows)::value * K;
+    float h[E];
+    RowK<__half, E>::load(hout + i0 * K, h);
+#pragma unroll
+    for (int q = 0; q < E; q++) h[q] *= isc;
+    RowK<float, E>::store(out + i0 * K, h);
+  });
+}
+
+// gather / scatter of K interleaved columns through a row permutation
+template <int K>
+__global__ void k_permute_gatherK(const double *__restrict__ in, const int32_t *__restrict__ perm,
+                                  double *__restrict__ out, int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+#pragma unroll
+    for (int c = 0; c < K; c++) out[i * K + c] = in[(int64_t)perm[i] * K + c];
+}
+template <int K>
+__global__ void k_permute_scatterK(const double *__restrict__ in, const int32_t *__restrict__ perm,
+                                   double *__restrict__ out, int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+#pragma unroll
+    for (int c = 0; c < K; c++) out[(int64_t)perm[i] * K + c] = in[i * K + c];
+}
+
+// Columns of a host or device block (nrhs columns of stride ld) into and out
+// of the interleaved layout: out[i * K + c] = in[c * ld + i] for c < ncols
+// (zero for the padding columns)
+__global__ void k_interleave(const double *__restrict__ in, int64_t ld, int ncols, int K, double *__restrict__ out,
+                             int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    for (int c = 0; c < K; c++) out[i * K + c] = c < ncols ? in[c * ld + i] : 0.0;
+}
+__global__ void k_deinterleave(const double *__restrict__ in, int K, int ncols, double *__restrict__ out, int64_t ld,
+                               int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    for (int c = 0; c < ncols; c++) out[c * ld + i] = in[i * K + c];
+}
+
+}  // namespace f3r

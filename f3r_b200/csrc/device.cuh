@@ -49,11 +49,28 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
+// try_wait with a suspend-time hint: a thread whose phase has not completed
+// is suspended by the hardware until the phase completes or about hint_ns
+// have passed, instead of spinning through issue slots.
+__device__ __forceinline__ bool mbar_try_wait_suspend(uint64_t *bar, uint32_t parity, uint32_t hint_ns) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity), "r"(hint_ns)
+      : "memory");
+  return ok != 0;
+}
+// Suspend hint of the bounded waits: long enough that a waiting warp leaves
+// the schedulers to the working ones, short against the bound.
+constexpr uint32_t kSuspendHintNs = 1000000u;
 // Waits for the given phase parity with a time bound; false on timeout.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity) {
   if (mbar_try_wait(bar, parity)) return true;
   const unsigned long long t0 = global_ns();
-  while (!mbar_try_wait(bar, parity)) {
+  while (!mbar_try_wait_suspend(bar, parity, kSuspendHintNs)) {
     if (global_ns() - t0 > kWaitLimitNs) return false;
   }
   return true;

@@ -46,6 +46,9 @@ Status ilu0_bj(const HostCSR &A, int32_t blocks, double acc, HostCSR **L, HostCS
 // row count (solver.cu).
 const void *solver_context(const f3r_solver *s);
 int32_t solver_rows(const f3r_solver *s);
+// f3r_solver_solve_multi after its argument checks (solver.cu)
+Status solver_solve_multi(f3r_solver *s, int32_t nrhs, const double *b, int64_t ldb, double *x, int64_t ldx,
+                          f3r_cond_fn cond, void *user, f3r_result *results);
 
 }  // namespace f3r
 

@@ -46,6 +46,26 @@ template <typename T> struct GivensCtl {
   int *err;
 };
 
+// Scalar arithmetic of the Hessenberg / Givens / back-substitution updates
+// with every operation rounded on its own (no FMA contraction), so that the
+// result is the same in every kernel these are inlined into, as in the
+// reference's unfused scalar code (gmres.hpp:14-53).
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float sub_rn(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(a, b); }
+
+// Blas1::trsv (gmres.hpp:41-53): y(0..w-1) from the triangular H and e
+template <typename T> __device__ __forceinline__ void back_subst(const T *H, const T *e, T *y, int ldh, int w) {
+  for (int i = w - 1; i >= 0; i--) {
+    T s = e[i];
+    for (int q = w - 1; q > i; q--) s = sub_rn(s, mul_rn(H[(size_t)q * ldh + i], y[q]));
+    y[i] = s / H[(size_t)i * ldh + i];
+  }
+}
+
 // full_grot + final_grot (gmres.hpp:14-38) and, after the level's last step,
 // the back substitution Blas1::trsv (gmres.hpp:41-53).  One thread.
 template <typename T> __device__ void givens_step(const GivensCtl<T> &g, T nrm2) {
@@ -57,35 +77,18 @@ template <typename T> __device__ void givens_step(const GivensCtl<T> &g, T nrm2)
   if (!(h > T(0)) || !isfinite(h)) atomicExch(g.err, (int)DEV_BREAKDOWN);
   for (int i = 0; i < j; i++) {
     const T t = Hc[i];
-    Hc[i] = g.cs[i] * t + g.sn[i] * Hc[i + 1];
-    Hc[i + 1] = -g.sn[i] * t + g.cs[i] * Hc[i + 1];
+    Hc[i] = add_rn(mul_rn(g.cs[i], t), mul_rn(g.sn[i], Hc[i + 1]));
+    Hc[i + 1] = add_rn(mul_rn(-g.sn[i], t), mul_rn(g.cs[i], Hc[i + 1]));
   }
-  const T t = sqrt(Hc[j] * Hc[j] + Hc[j + 1] * Hc[j + 1]);
+  const T t = sqrt(add_rn(mul_rn(Hc[j], Hc[j]), mul_rn(Hc[j + 1], Hc[j + 1])));
   g.cs[j] = Hc[j] / t;
   g.sn[j] = Hc[j + 1] / t;
   Hc[j] = t;
   Hc[j + 1] = 0;
-  g.e[j + 1] = -g.sn[j] * g.e[j];
-  g.e[j] = g.cs[j] * g.e[j];
+  g.e[j + 1] = mul_rn(-g.sn[j], g.e[j]);
+  g.e[j] = mul_rn(g.cs[j], g.e[j]);
   if (g.abs_e) *g.abs_e = (double)fabs(g.e[j + 1]);
-  if (g.compute_y) {
-    const int w = j + 1;
-    for (int i = w - 1; i >= 0; i--) {
-      T s = g.e[i];
-      for (int q = w - 1; q > i; q--) s -= g.H[(size_t)q * g.ldh + i] * g.y[q];
-      g.y[i] = s / g.H[(size_t)i * g.ldh + i];
-    }
-  }
-}
-
-// Back substitution only (outer level, after a convergence stop), one thread.
-template <typename T> __global__ void k_trsv_y(T *H, const T *e, T *y, int ldh, int w) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  for (int i = w - 1; i >= 0; i--) {
-    T s = e[i];
-    for (int q = w - 1; q > i; q--) s -= H[(size_t)q * ldh + i] * y[q];
-    y[i] = s / H[(size_t)i * ldh + i];
-  }
+  if (g.compute_y) back_subst(g.H, g.e, g.y, g.ldh, j + 1);
 }
 
 // ---------------------------------------------------------------------------
@@ -405,15 +408,51 @@ struct DiagPre {
   }
 };
 
-// First half of R.  The level-3 basis vector is normalised here, in place,
+// First half of R.  The caller's basis vector is normalised here, in place,
 // when its 1/h factor is given (V(j+1) *= h.inv(), gmres.hpp:117 -- deferred
 // from the Gram-Schmidt step to save a pass); then hin = fp16(in * sc),
 // hout = M hin, and on a call without a weight update hout *= ome[0]
-// (f3r-gpu.cpp:231-243).
-template <bool SCALE_BY_OME>
-__global__ void k_rich_enter_diag(float *__restrict__ in, const float *__restrict__ in_inv, float sc, DiagPre M,
+// (f3r-gpu.cpp:231-243).  In is float (R below an fp32 level) or __half (R
+// below the fp16-vector level: the input already is R's fp16 working vector,
+// so hin is `in` itself and is not written; sc is 1 there).
+template <typename In> struct In4;
+template <> struct In4<float> {
+  static __device__ __forceinline__ void ld(const float *p, float (&v)[4]) {
+    const VecN<float, 4> a = ldv<float, 4>(p);
+#pragma unroll
+    for (int e = 0; e < 4; e++) v[e] = a.v[e];
+  }
+  static __device__ __forceinline__ void st(float *p, const float (&v)[4]) {
+    VecN<float, 4> a;
+#pragma unroll
+    for (int e = 0; e < 4; e++) a.v[e] = v[e];
+    stv<float, 4>(p, a);
+  }
+};
+template <> struct In4<__half> {
+  static __device__ __forceinline__ void ld(const __half *p, float (&v)[4]) {
+    const VecN<__half, 4> a = ldv<__half, 4>(p);
+#pragma unroll
+    for (int e = 0; e < 4; e++) v[e] = __half2float(a.v[e]);
+  }
+  static __device__ __forceinline__ void st(__half *p, const float (&v)[4]) {
+    VecN<__half, 4> a;
+#pragma unroll
+    for (int e = 0; e < 4; e++) a.v[e] = __float2half_rn(v[e]);
+    stv<__half, 4>(p, a);
+  }
+};
+__device__ __forceinline__ float as_float(float v) { return v; }
+__device__ __forceinline__ float as_float(__half v) { return __half2float(v); }
+template <typename T> __device__ __forceinline__ T from_float(float v);
+template <> __device__ __forceinline__ float from_float<float>(float v) { return v; }
+template <> __device__ __forceinline__ __half from_float<__half>(float v) { return __float2half_rn(v); }
+
+template <bool SCALE_BY_OME, typename In = float>
+__global__ void k_rich_enter_diag(In *__restrict__ in, const float *__restrict__ in_inv, float sc, DiagPre M,
                                   __half *__restrict__ hin, __half *__restrict__ hout,
                                   const RichState *__restrict__ rs, float *e_set, int64_t n) {
+  constexpr bool HALF_IN = std::is_same<In, __half>::value;
   if (e_set && blockIdx.x == 0 && threadIdx.x == 0) e_set[0] = 1.0f;
   const float om = SCALE_BY_OME ? h2f(rs->ome[0]) : 1.0f;
   const float s = in_inv ? *in_inv : 1.0f;
@@ -421,51 +460,55 @@ __global__ void k_rich_enter_diag(float *__restrict__ in, const float *__restric
   const int64_t nq = n / 4;
   for (int64_t q = tid; q < nq; q += stride) {
     const int64_t i = 4 * q;
-    VecN<float, 4> v = ldv<float, 4>(in + i);
+    float v[4];
+    In4<In>::ld(in + i, v);
     if (in_inv) {
 #pragma unroll
-      for (int e = 0; e < 4; e++) v.v[e] *= s;
-      stv<float, 4>(in + i, v);
+      for (int e = 0; e < 4; e++) v[e] *= s;
+      In4<In>::st(in + i, v);
     }
     const VecN<__half, 4> w = ldv<__half, 4>(M.w + i), z = ldv<__half, 4>(M.z + i);
     VecN<__half, 4> hi, ho;
 #pragma unroll
     for (int e = 0; e < 4; e++) {
-      hi.v[e] = f2h(v.v[e] * sc);
+      hi.v[e] = f2h(v[e] * sc);
       const float t = h2f(f2h(h2f(w.v[e]) * h2f(hi.v[e])));
       float o = h2f(f2h(h2f(z.v[e]) * t));
       if (SCALE_BY_OME) o = h2f(f2h(o * om));
       ho.v[e] = f2h(o);
     }
-    stv<__half, 4>(hin + i, hi);
+    if (!HALF_IN) stv<__half, 4>(hin + i, hi);
     stv<__half, 4>(hout + i, ho);
   }
   for (int64_t i = nq * 4 + tid; i < n; i += stride) {
-    float v = in[i];
+    float v = as_float(in[i]);
     if (in_inv) {
       v *= s;
-      in[i] = v;
+      in[i] = from_float<In>(v);
     }
     const __half hi = f2h(v * sc);
-    hin[i] = hi;
+    if (!HALF_IN) hin[i] = hi;
     float ho = M.apply(i, h2f(hi));
     if (SCALE_BY_OME) ho = h2f(f2h(ho * om));
     hout[i] = f2h(ho);
   }
 }
 
-// General preconditioner: (normalise in place), hin = fp16(in * sc) only.
-__global__ void k_rich_cast_in(float *__restrict__ in, const float *__restrict__ in_inv, float sc,
+// General preconditioner: (normalise in place), hin = fp16(in * sc) only
+// (nothing but the normalisation when the input is R's fp16 vector itself).
+template <typename In = float>
+__global__ void k_rich_cast_in(In *__restrict__ in, const float *__restrict__ in_inv, float sc,
                                __half *__restrict__ hin, float *e_set, int64_t n) {
+  constexpr bool HALF_IN = std::is_same<In, __half>::value;
   if (e_set && blockIdx.x == 0 && threadIdx.x == 0) e_set[0] = 1.0f;
   const float s = in_inv ? *in_inv : 1.0f;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    float v = in[i];
+    float v = as_float(in[i]);
     if (in_inv) {
       v *= s;
-      in[i] = v;
+      in[i] = from_float<In>(v);
     }
-    hin[i] = f2h(v * sc);
+    if (!HALF_IN) hin[i] = f2h(v * sc);
   }
 }
 
@@ -570,14 +613,16 @@ __global__ void k_rich_scale_om(__half *__restrict__ hout, const RichState *__re
 }
 
 // hout = fp16(hout + om[k] t2) (f3r-gpu.cpp:252), or on the last step out =
-// fp32(that) / sc.  use_ome selects ome[k] (no-update calls, general M).
+// fp32(that) / sc, or out16 = that (R below the fp16-vector level).  use_ome
+// selects ome[k] (no-update calls, general M).
 __global__ void k_rich_axpy(__half *__restrict__ hout, const __half *__restrict__ t2,
                             const RichState *__restrict__ rs, int k, int use_ome, float *__restrict__ out,
-                            float isc, int64_t n) {
+                            __half *__restrict__ out16, float isc, int64_t n) {
   const float om = use_ome ? h2f(rs->ome[k]) : rs->om[k];
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     const float hn = h2f(f2h(__fmaf_rn(om, h2f(t2[i]), h2f(hout[i]))));
     if (out) out[i] = hn * isc;
+    else if (out16) out16[i] = f2h(hn);
     else hout[i] = f2h(hn);
   }
 }
@@ -622,6 +667,212 @@ __global__ void k_permute_scatter(const double *__restrict__ in, const int32_t *
                                   double *__restrict__ out, int64_t n) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     out[perm[i]] = in[i];
+}
+
+// ---------------------------------------------------------------------------
+// The fp16-vector FGMRES level (FGMRES<_Float16>, depth.cpp:122-167): V and Z
+// stored in fp16, every dot, norm, update and Givens rotation computed in
+// fp32 (the reference computes them in fp16).  Vectors of the level start on
+// 16-byte boundaries (columns of ldn elements, ldn a multiple of 8), so a
+// thread moves 8 values per access.
+// ---------------------------------------------------------------------------
+
+// Entry: the caller's basis vector -- an fp32 column of an inner level, or
+// the outer level's fp64 column read through a slot -- is normalised in
+// place when its 1/h factor is given (deferred V(j+1) *= h.inv(),
+// gmres.hpp:117), then V(0) = fp16(in) (V(0).copy(rhs), gmres.hpp:102),
+// e(0) = 1 (normalize = false, gmres.hpp:100-101), and the caller's own e(0)
+// = 1 when e_parent is given (the caller's first inner call sets it).
+__device__ __forceinline__ __half round_half(float v) { return __float2half_rn(v); }
+__device__ __forceinline__ __half round_half(double v) { return __double2half(v); }  // one rounding
+
+template <typename In>
+__global__ void k_level_enter_h(In *in_direct, In *const *in_slot, const In *__restrict__ in_inv,
+                                __half *__restrict__ v0, float *e, float *e_parent, int64_t n) {
+  In *in = in_slot ? *in_slot : in_direct;
+  const In s = in_inv ? *in_inv : In(1);
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    e[0] = 1.0f;
+    if (e_parent) e_parent[0] = 1.0f;
+  }
+  constexpr int N = 16 / sizeof(In);
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x, tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t n8 = n / 8;
+  for (int64_t q = tid; q < n8; q += stride) {
+    const int64_t i = 8 * q;
+    VecN<__half, 8> o;
+#pragma unroll
+    for (int c = 0; c < 8 / N; c++) {
+      VecN<In, N> a = ldv<In, N>(in + i + c * N);
+      if (in_inv) {
+#pragma unroll
+        for (int e = 0; e < N; e++) a.v[e] *= s;
+        stv<In, N>(in + i + c * N, a);
+      }
+#pragma unroll
+      for (int e = 0; e < N; e++) o.v[c * N + e] = round_half(a.v[e]);
+    }
+    stv<__half, 8>(v0 + i, o);
+  }
+  for (int64_t i = n8 * 8 + tid; i < n; i += stride) {
+    In v = in[i];
+    if (in_inv) {
+      v *= s;
+      in[i] = v;
+    }
+    v0[i] = round_half(v);
+  }
+}
+
+// H(j, k) = <w, V(k)> for k < nv, fp16 vectors, fp32 accumulation (the CGS
+// dot phase, gmres.hpp:112-114): basis vectors in chunks of 8 per pass over
+// w, partial sums per block, then the last block adds them in block order.
+template <int WARPS>
+__global__ void __launch_bounds__(WARPS * 32) k_multidot_h(const __half *__restrict__ w, Cols<__half> V, int nv,
+                                                           int64_t n, GridRed gr, float *hcol) {
+  constexpr int CH = 8;
+  float *part = static_cast<float *>(gr.partials);
+  __shared__ float sred[WARPS][CH];
+  __shared__ bool last;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x, tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t n8 = n / 8;
+  for (int k0 = 0; k0 < nv; k0 += CH) {
+    float a[CH];
+#pragma unroll
+    for (int c = 0; c < CH; c++) a[c] = 0.0f;
+    for (int64_t q = tid; q < n8; q += stride) {
+      const VecN<__half, 8> wv = ldv<__half, 8>(w + 8 * q);
+#pragma unroll
+      for (int c = 0; c < CH; c++) {
+        if (k0 + c < nv) {
+          const VecN<__half, 8> v = ldv<__half, 8>(V.p[k0 + c] + 8 * q);
+#pragma unroll
+          for (int e = 0; e < 8; e++) a[c] = __fmaf_rn(__half2float(wv.v[e]), __half2float(v.v[e]), a[c]);
+        }
+      }
+    }
+    for (int64_t i = n8 * 8 + tid; i < n; i += stride) {
+      const float wi = __half2float(w[i]);
+#pragma unroll
+      for (int c = 0; c < CH; c++)
+        if (k0 + c < nv) a[c] = __fmaf_rn(wi, __half2float(V.p[k0 + c][i]), a[c]);
+    }
+#pragma unroll
+    for (int c = 0; c < CH; c++) {
+      const float t = warp_sum(a[c]);
+      if (lane == 0) sred[warp][c] = t;
+    }
+    __syncthreads();
+    if (threadIdx.x < CH && k0 + (int)threadIdx.x < nv) {
+      float t = 0;
+      for (int q = 0; q < WARPS; q++) t += sred[q][threadIdx.x];
+      part[(size_t)blockIdx.x * nv + k0 + threadIdx.x] = t;
+    }
+    __syncthreads();
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = (atomicAdd(gr.ticket, 1u) == gridDim.x - 1);
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  for (int k = warp; k < nv; k += WARPS) {
+    float t = 0;
+    for (int b = lane; b < (int)gridDim.x; b += 32) t += __ldcg(&part[(size_t)b * nv + k]);
+    t = warp_sum(t);
+    if (lane == 0) hcol[k] = t;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) *gr.ticket = 0;
+}
+
+// w = fp16(w - sum_k H(j,k) V(k)) (MULMV order, in fp32), then the squared
+// norm of the stored fp16 w -> h_{j+1,j}, 1/h, the Givens rotation and, after
+// the level's last step, the back substitution (gmres.hpp:115-121).
+template <int WARPS>
+__global__ void __launch_bounds__(WARPS * 32) k_cgs_update_h(__half *__restrict__ w, Cols<__half> V, int nv,
+                                                             int64_t n, GridRed gr, GivensCtl<float> g) {
+  __shared__ float sh[kMaxCols];
+  const float *hcol = g.H + (size_t)g.j * g.ldh;
+  for (int k = threadIdx.x; k < nv; k += blockDim.x) sh[k] = hcol[k];
+  __syncthreads();
+  float part[1] = {0.0f};
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x, tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t n8 = n / 8;
+  for (int64_t q = tid; q < n8; q += stride) {
+    const int64_t i = q * 8;
+    const VecN<__half, 8> a = ldv<__half, 8>(V.p[0] + i);
+    float r[8];
+#pragma unroll
+    for (int e = 0; e < 8; e++) r[e] = __half2float(a.v[e]) * sh[0];
+#pragma unroll 4
+    for (int k = 1; k < nv; k++) {
+      const VecN<__half, 8> b = ldv<__half, 8>(V.p[k] + i);
+      const float hk = sh[k];
+#pragma unroll
+      for (int e = 0; e < 8; e++) r[e] = __fmaf_rn(__half2float(b.v[e]), hk, r[e]);
+    }
+    VecN<__half, 8> wv = ldv<__half, 8>(w + i);
+#pragma unroll
+    for (int e = 0; e < 8; e++) {
+      wv.v[e] = __float2half_rn(__half2float(wv.v[e]) - r[e]);
+      const float u = __half2float(wv.v[e]);
+      part[0] = __fmaf_rn(u, u, part[0]);
+    }
+    stv<__half, 8>(w + i, wv);
+  }
+  for (int64_t i = n8 * 8 + tid; i < n; i += stride) {
+    float r = __half2float(V.p[0][i]) * sh[0];
+    for (int k = 1; k < nv; k++) r = __fmaf_rn(__half2float(V.p[k][i]), sh[k], r);
+    const __half wi = __float2half_rn(__half2float(w[i]) - r);
+    w[i] = wi;
+    const float u = __half2float(wi);
+    part[0] = __fmaf_rn(u, u, part[0]);
+  }
+  const GivensCtl<float> gg = g;
+  grid_reduce<float, 1, WARPS>(part, 1, gr, [gg](float *tot) { givens_step<float>(gg, tot[0]); });
+}
+
+// x = Z y of the fp16-vector level (with_init, gmres.hpp:127-128): fp16 Z,
+// fp32 y and sum, stored in the caller's type (fp32 column, or the outer
+// level's fp64 column through a slot).
+template <typename Out>
+__global__ void k_zy_h(Cols<__half> Z, const float *__restrict__ y, int nz, Out *out_direct, Out *const *out_slot,
+                       int64_t n) {
+  __shared__ float sy[kMaxCols];
+  for (int k = threadIdx.x; k < nz; k += blockDim.x) sy[k] = y[k];
+  __syncthreads();
+  Out *out = out_slot ? *out_slot : out_direct;
+  constexpr int N = 16 / sizeof(Out);
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x, tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t n8 = n / 8;
+  for (int64_t q = tid; q < n8; q += stride) {
+    const int64_t i = q * 8;
+    const VecN<__half, 8> a = ldv<__half, 8>(Z.p[0] + i);
+    float r[8];
+#pragma unroll
+    for (int e = 0; e < 8; e++) r[e] = __half2float(a.v[e]) * sy[0];
+#pragma unroll 4
+    for (int k = 1; k < nz; k++) {
+      const VecN<__half, 8> b = ldv<__half, 8>(Z.p[k] + i);
+      const float yk = sy[k];
+#pragma unroll
+      for (int e = 0; e < 8; e++) r[e] = __fmaf_rn(__half2float(b.v[e]), yk, r[e]);
+    }
+#pragma unroll
+    for (int c = 0; c < 8 / N; c++) {
+      VecN<Out, N> o;
+#pragma unroll
+      for (int e = 0; e < N; e++) o.v[e] = (Out)r[c * N + e];
+      stv<Out, N>(out + i + c * N, o);
+    }
+  }
+  for (int64_t i = n8 * 8 + tid; i < n; i += stride) {
+    float r = __half2float(Z.p[0][i]) * sy[0];
+    for (int k = 1; k < nz; k++) r = __fmaf_rn(__half2float(Z.p[k][i]), sy[k], r);
+    out[i] = (Out)r;
+  }
 }
 
 // <x, y> with the deterministic grid reduction (kmm::dot)

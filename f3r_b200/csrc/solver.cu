@@ -18,10 +18,12 @@
 #include <numeric>
 #include <random>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "internal.hpp"
 #include "kernels.cuh"
+#include "block.cuh"
 #include "ilu.cuh"
 #include "objects.cuh"
 #include "trsv.hpp"
@@ -394,11 +396,84 @@ __global__ void k_set_slots(double **in_slot, double **out_slot, double *in, dou
   *out_slot = out;
 }
 
+// Back substitution of the columns in mask (Blas1::trsv, gmres.hpp:41-53),
+// one thread per column.
+template <typename T, int K> __global__ void k_trsv_yK(LevelK<T> L, uint32_t mask, int w) {
+  const int c = threadIdx.x;
+  if (blockIdx.x != 0 || c >= K || !((mask >> c) & 1u)) return;
+  back_subst(L.H + c * L.hs, L.e + c * L.vs, L.y + c * L.vs, L.ldh, w);
+}
+
+// One FGMRES level over K columns: bases (inner levels: one allocation of
+// m (+1) columns of ldn * K values, column 0 of level 3 an alias of the
+// caller's column) and per-column scalars, column c's at LevelK offsets.
 template <typename T> struct Level {
   int m = 0;
-  T *V = nullptr, *Z = nullptr;  // column-major n x (m+1), n x m (level 3 V column 0 is an alias)
+  T *V = nullptr, *Z = nullptr;
   T *H = nullptr, *cs = nullptr, *sn = nullptr, *e = nullptr, *y = nullptr, *inv = nullptr;
+  LevelK<T> view() const { return LevelK<T>{H, cs, sn, e, y, inv, (int64_t)(m + 1) * m, m + 1, m + 1}; }
 };
+
+// The fp16-vector FGMRES level (single column): fp16 bases, fp32 Hessenberg and rotations.
+struct HLevel {
+  int m = 0;
+  __half *V = nullptr, *Z = nullptr;  // column-major n x (m+1), n x m
+  float *H = nullptr, *cs = nullptr, *sn = nullptr, *e = nullptr, *y = nullptr, *inv = nullptr;
+};
+
+struct Solver;
+
+// Device state of solves K columns wide: the levels' bases and scalars, R's
+// fp16 work vectors, K Richardson states, the right-hand side / solution
+// blocks, the reduction scratch and the captured level graphs.
+template <int K> struct Work {
+  Level<double> L1;  // outer bases in V1 / Z1 (allocated as the solve reaches them), scalars here
+  Level<float> L2, L3;
+  HLevel LH;         // K == 1 only
+  std::vector<double *> V1, Z1;
+  double *abs_e = nullptr;
+  __half *hin = nullptr, *hout = nullptr, *hout2 = nullptr, *tmp = nullptr, *tmp2 = nullptr, *hr = nullptr;
+  RichState *rs = nullptr;
+  double **in_slot = nullptr, **out_slot = nullptr;
+  double *b_d = nullptr, *x_d = nullptr, *bp_d = nullptr, *xp_d = nullptr, *r_d = nullptr;
+  uint32_t *active = nullptr;
+  double *nrm = nullptr;  // K norms read back by the host
+  GridRed gr{};
+  int64_t cnt = 0, r_calls = 0;
+  std::map<std::vector<bool>, std::pair<cudaGraphExec_t, int64_t>> graphs;  // exec, kernels in it
+  std::vector<void *> allocs;
+  ~Work() {
+    for (auto &kv : graphs) cudaGraphExecDestroy(kv.second.first);
+    for (void *q : allocs) cudaFree(q);
+  }
+  template <typename T> Status alloc(T **q, size_t count) {
+    cudaError_t e = cudaMalloc((void **)q, std::max<size_t>(count, 1) * sizeof(T));
+    if (e != cudaSuccess)
+      return fail(e == cudaErrorMemoryAllocation ? F3R_ERROR_OUT_OF_MEMORY : F3R_ERROR_CUDA,
+                  std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    allocs.push_back((void *)*q);
+    return F3R_SUCCESS;
+  }
+  template <typename T> Status make_level(Level<T> &L, int m, int64_t ldn, bool own_v0, bool bases = true) {
+    L.m = m;
+    const size_t nn = (size_t)std::max<int64_t>(ldn, 8) * K;
+    if (bases) {
+      F3R_TRY(alloc(&L.V, nn * (size_t)(m + (own_v0 ? 1 : 0))));
+      F3R_TRY(alloc(&L.Z, nn * (size_t)m));
+    }
+    F3R_TRY(alloc(&L.H, (size_t)K * (m + 1) * m));
+    F3R_TRY(alloc(&L.cs, (size_t)K * (m + 1)));
+    F3R_TRY(alloc(&L.sn, (size_t)K * (m + 1)));
+    F3R_TRY(alloc(&L.e, (size_t)K * (m + 1)));
+    F3R_TRY(alloc(&L.y, (size_t)K * (m + 1)));
+    F3R_TRY(alloc(&L.inv, (size_t)K));
+    CUDA_TRY(cudaMemset(L.H, 0, sizeof(T) * (size_t)K * (m + 1) * m));
+    CUDA_TRY(cudaMemset(L.e, 0, sizeof(T) * (size_t)K * (m + 1)));
+    return F3R_SUCCESS;
+  }
+};
+
+template <int K> struct Engine;
 
 struct Solver {
   f3r_context *ctx = nullptr;
@@ -415,272 +490,449 @@ struct Solver {
   IluDevice ilu;      // block-Jacobi ILU(0), level scheduled
   IluLevel ilul;      // global ILU(0), level scheduled over the whole GPU
   JacobiTrsv jl, ju;  // the same factors solved by Jacobi / BAJ sweeps
-  // levels
-  Level<double> L1;
-  Level<float> L2, L3;
-  double *abs_e = nullptr;
-  __half *hin = nullptr, *hout = nullptr, *hout2 = nullptr, *tmp = nullptr, *tmp2 = nullptr, *hr = nullptr;
-  RichState *rs = nullptr;
-  double **in_slot = nullptr;
-  double **out_slot = nullptr;
-  double *b_d = nullptr, *x_d = nullptr, *bp_d = nullptr, *xp_d = nullptr, *r_d = nullptr;
-  int64_t cnt = 0;
-  int64_t r_calls = 0;
   std::vector<void *> allocs;
-  std::map<std::vector<bool>, std::pair<cudaGraphExec_t, int64_t>> graphs;  // exec, kernels in it
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  Work<1> w1;  // single-column solves
+  std::unique_ptr<Work<2>> w2;
+  std::unique_ptr<Work<4>> w4;
+  std::unique_ptr<Work<8>> w8;
+  std::unique_ptr<Work<16>> w16;
 
   Context &C() { return *ctx; }
-  template <typename T> Status alloc(T **p, size_t count) {
-    F3R_TRY(ctx->alloc((void **)p, count * sizeof(T)));
-    allocs.push_back((void *)*p);
+  template <typename T> Status alloc(T **q, size_t count) {
+    F3R_TRY(ctx->alloc((void **)q, count * sizeof(T)));
+    allocs.push_back((void *)*q);
     return F3R_SUCCESS;
   }
   ~Solver() {
-    for (auto &kv : graphs) cudaGraphExecDestroy(kv.second.first);
+    w2.reset(); w4.reset(); w8.reset(); w16.reset();
     for (void *q : allocs) cudaFree(q);
     A.release(); W.release(); Z.release(); ilu.release(); ilul.release(); jl.release(); ju.release();
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
   }
+  // R calls per outer step (the product of the inner levels' steps)
+  int calls_per_outer() const { return std::max(p.m2, 1) * std::max(p.m3, 1) * std::max(p.half_m, 1); }
+  // Can the nest run K columns in lockstep?  The block product covers SDAINV
+  // (diagonal, or general factors in packed / fully aligned SELL) with FGMRES
+  // levels; other set-ups solve column by column.
+  bool block_ok() const {
+    auto layout_ok = [](const DeviceSell &d) { return !d.rptr && !d.xoff && !d.dcol; };
+    if (p.precond != F3R_PRECOND_SDAINV || p.inner_sstep || p.half_m > 0 || !layout_ok(A)) return false;
+    return precond_diag || (layout_ok(W) && layout_ok(Z));
+  }
+  template <int K> Status work(Work<K> **out);
+  Status solve(const double *b_user, double *x_user, f3r_cond_fn cond, void *user, f3r_result *res);
+  Status solve_multi(int32_t nrhs, const double *b, int64_t ldb, double *x, int64_t ldx, f3r_cond_fn cond, void *user,
+                     f3r_result *results);
+};
 
-  template <typename T> Status make_level(Level<T> &L, int m, bool own_v0) {
-    L.m = m;
-    const size_t nn = (size_t)std::max<int64_t>(ldn, 8);
-    F3R_TRY(alloc(&L.V, nn * (size_t)(m + (own_v0 ? 1 : 0))));
-    F3R_TRY(alloc(&L.Z, nn * (size_t)m));
-    F3R_TRY(alloc(&L.H, (size_t)(m + 1) * m));
-    F3R_TRY(alloc(&L.cs, (size_t)m));
-    F3R_TRY(alloc(&L.sn, (size_t)m));
-    F3R_TRY(alloc(&L.e, (size_t)m + 1));
-    F3R_TRY(alloc(&L.y, (size_t)m));
-    F3R_TRY(alloc(&L.inv, 1));
-    CUDA_TRY(cudaMemset(L.H, 0, sizeof(T) * (size_t)(m + 1) * m));
-    CUDA_TRY(cudaMemset(L.e, 0, sizeof(T) * (size_t)(m + 1)));
+// K-column block product on the context's stream (packed int32 or fully
+// aligned SELL); every instantiation raises its shared-memory limit once per
+// device, before any graph capture reaches it (Engine::prepare).
+template <typename V, typename X, typename Epi, int K, typename CI>
+Status launch_block_one(Context &c, const V *val, const DevSell &A, const X *x, const Epi &epi, bool attr_only) {
+  using Cfg = BlockCfg<V, K, CI>;
+  auto kern = k_sell_block<V, X, Epi, K, Cfg::WARPS, Cfg::STAGES, Cfg::KC, CI>;
+  static int done[64] = {0};
+  if (!done[c.device & 63]) {
+    CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)block_smem_bytes<V, K, CI>()));
+    done[c.device & 63] = 1;
+  }
+  if (attr_only || A.nslices == 0) return F3R_SUCCESS;
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(cdiv(A.nslices, Cfg::WARPS), c.sm_count));
+  launch_k(c, kern, grid, Cfg::WARPS * 32, block_smem_bytes<V, K, CI>(), c.stream, val, A, x, epi, c.err);
+  CUDA_TRY(cudaGetLastError());
+  return F3R_SUCCESS;
+}
+template <typename V, typename X, typename Epi, int K>
+Status launch_block(Context &c, const V *val, const DevSell &A, const X *x, const Epi &epi, bool attr_only = false) {
+  if (A.rptr || A.xoff || A.dcol) return fail(F3R_ERROR_UNSUPPORTED, "block product: packed or fully aligned SELL only");
+  if (attr_only) {
+    F3R_TRY((launch_block_one<V, X, Epi, K, int32_t>(c, val, A, x, epi, true)));
+    return launch_block_one<V, X, Epi, K, AllAlignedIdx>(c, val, A, x, epi, true);
+  }
+  if (A.cbase) return launch_block_one<V, X, Epi, K, AllAlignedIdx>(c, val, A, x, epi, false);
+  return launch_block_one<V, X, Epi, K, int32_t>(c, val, A, x, epi, false);
+}
+
+// The nested solve over K columns in lockstep (K = 1: the single solve).
+template <int K> struct Engine {
+  Solver &S;
+  Work<K> &w;
+  const f3r_params &p;
+  const int32_t n;
+  const int64_t ldn;
+  Engine(Solver &s, Work<K> &wk) : S(s), w(wk), p(s.p), n(s.n), ldn(s.ldn) {}
+  Context &C() { return *S.ctx; }
+  int64_t lk() const { return ldn * K; }  // column stride of a K-wide basis
+
+  // ---- products: the single-column kernel's epilogue (K = 1) or the block one
+  template <typename V, typename X, typename E1, typename EK>
+  Status mv(const V *vals, const DevSell &M, const X *x, const E1 &e1, const EK &ek) {
+    if constexpr (K == 1) return launch_sell(C(), vals, M, x, e1);
+    else return launch_block<V, X, EK, K>(C(), vals, M, x, ek);
+  }
+  template <typename V, typename X, typename Out> Status mv_store(const V *vals, const DevSell &M, const X *x, Out *y) {
+    return mv(vals, M, x, EpiStore<Out>{y, nullptr}, EpiStoreK<Out, K>{y});
+  }
+  // raises the shared-memory limit of every block product instantiation the solve uses
+  Status prepare() {
+    if constexpr (K > 1) {
+      const DevSell Av = S.A.view();
+      const double *d = nullptr;
+      const float *f = nullptr;
+      const __half *h = nullptr;
+      F3R_TRY((launch_block<double, double, EpiStoreK<double, K>, K>(C(), d, Av, d, {}, true)));
+      F3R_TRY((launch_block<double, double, EpiResidualK<double, double, K>, K>(C(), d, Av, d, {}, true)));
+      F3R_TRY((launch_block<float, float, EpiStoreK<float, K>, K>(C(), f, Av, f, {}, true)));
+      F3R_TRY((launch_block<__half, float, EpiStoreK<float, K>, K>(C(), h, Av, f, {}, true)));
+      F3R_TRY((launch_block<__half, __half, EpiStoreK<__half, K>, K>(C(), h, Av, h, {}, true)));
+      F3R_TRY((launch_block<__half, __half, EpiRichStepK<K>, K>(C(), h, Av, h, {}, true)));
+      F3R_TRY((launch_block<__half, __half, EpiRichResPreK<K>, K>(C(), h, Av, h, {}, true)));
+      F3R_TRY((launch_block<__half, __half, EpiResidualK<__half, __half, K>, K>(C(), h, Av, h, {}, true)));
+      F3R_TRY((launch_block<__half, __half, EpiZScaleK<K>, K>(C(), h, Av, h, {}, true)));
+    }
     return F3R_SUCCESS;
   }
 
-  // ---- level 4: R(in) -> out -------------------------------------------------
-  // in_inv: 1/h of the basis vector `in` when its normalisation is still
-  // pending (done in place by the first kernel), else nullptr
-  Status rich_apply(float *in, float *out, float *e_set, const float *in_inv) {
+  // ---- outer basis columns, allocated as the solve reaches them ---------------
+  Status ensure_outer(int j) {
+    while ((int)w.V1.size() < std::min(j + 2, p.m_outer + 1)) {
+      const int add = std::min<int>(8, p.m_outer + 1 - (int)w.V1.size());
+      for (int q = 0; q < add; q++) {
+        double *v = nullptr;
+        F3R_TRY(w.alloc(&v, (size_t)lk()));
+        w.V1.push_back(v);
+        if ((int)w.Z1.size() < p.m_outer) {
+          double *z = nullptr;
+          F3R_TRY(w.alloc(&z, (size_t)lk()));
+          w.Z1.push_back(z);
+        }
+      }
+    }
+    return F3R_SUCCESS;
+  }
+
+  // ---- level 4: R(in) -> out --------------------------------------------------
+  // in_inv: the K pending 1/h factors of the basis block `in` (its
+  // normalisation is done in place by the first kernel), else nullptr.  K = 1
+  // below the fp16-vector level: in16 / out16 are that level's fp16 columns.
+  Status rich_apply(float *in, float *out, float *e_set, int64_t e_stride, const float *in_inv,
+                    __half *in16 = nullptr, __half *out16 = nullptr) {
     const int64_t N = n;
     const int g = C().ew_grid(N);
-    const int gv = C().ew_grid(cdiv(N, 4));
     cudaStream_t st = C().stream;
-    ++cnt;
-    ++r_calls;
-    const bool upd = p.static_weight <= 0 && (cnt % p.c) == 0;  // F3R-Static never updates
-    const float sc = std::ldexp(1.0f, p.half_scale_log2), isc = std::ldexp(1.0f, -p.half_scale_log2);
-    const DevSell Av = A.view();
-    if (precond_diag) {
-      const DiagPre M{wd, zd};
+    ++w.cnt;
+    ++w.r_calls;
+    const bool upd = p.static_weight <= 0 && (w.cnt % p.c) == 0;  // F3R-Static never updates
+    const bool h16 = in16 != nullptr;
+    const float sc = h16 ? 1.0f : std::ldexp(1.0f, p.half_scale_log2);
+    const float isc = h16 ? 1.0f : std::ldexp(1.0f, -p.half_scale_log2);
+    const __half *hi = h16 ? in16 : w.hin;              // R's fp16 input
+    __half *h0 = (p.m4 == 1 && out16) ? out16 : w.hout;  // first result (the only one when m4 = 1)
+    float *out_last = out16 ? nullptr : out;            // fp32 result of the last step
+    const DevSell Av = S.A.view();
+    const GridRed gr = w.gr;
+    if (S.precond_diag) {
+      const DiagPre M{S.wd, S.zd};
+      if constexpr (K == 1) {
+        if (h16) {
+          if (!upd)
+            launch_k(C(), k_rich_enter_diag<true, __half>, C().ew_grid(cdiv(N, 4)), kEwThreads, 0, st, in16, in_inv,
+                     sc, M, w.hin, h0, w.rs, e_set, N);
+          else
+            launch_k(C(), k_rich_enter_diag<false, __half>, C().ew_grid(cdiv(N, 4)), kEwThreads, 0, st, in16, in_inv,
+                     sc, M, w.hin, h0, w.rs, e_set, N);
+        }
+      }
+      if (!h16) {
+        if (!upd)
+          launch_k(C(), k_rich_enter_diagK<true, K>, g, kEwThreads, 0, st, in, in_inv, sc, M, w.hin, h0, w.rs, e_set,
+                   e_stride, N);
+        else
+          launch_k(C(), k_rich_enter_diagK<false, K>, g, kEwThreads, 0, st, in, in_inv, sc, M, w.hin, h0, w.rs, e_set,
+                   e_stride, N);
+      }
       if (!upd) {
-        launch_k(C(), k_rich_enter_diag<true>, gv, kEwThreads, 0, st, in, in_inv, sc, M, hin, hout, rs, e_set, N);
-        __half *cur = hout, *nxt = hout2;
+        __half *cur = h0, *nxt = w.hout2;
         for (int k = 1; k < p.m4; k++) {
           const bool last = (k == p.m4 - 1);
-          EpiRichStep epi{hin, cur, M, rs, k, last ? nullptr : nxt, last ? out : nullptr, isc};
-          F3R_TRY(launch_sell(C(), A.v16, Av, (const __half *)cur, epi));
+          F3R_TRY(mv(S.A.v16, Av, (const __half *)cur,
+                     EpiRichStep{hi, cur, M, w.rs, k, last ? out16 : nxt, last ? out_last : nullptr, isc},
+                     EpiRichStepK<K>{hi, cur, M, w.rs, k, nxt, last ? out_last : nullptr, isc}));
           std::swap(cur, nxt);
         }
-        if (p.m4 == 1) launch_k(C(), k_rich_exit, g, kEwThreads, 0, st, hout, out, isc, N);
       } else {
-        launch_k(C(), k_rich_enter_diag<false>, gv, kEwThreads, 0, st, in, in_inv, sc, M, hin, hout, rs, e_set, N);
-        F3R_TRY(launch_sell(C(), A.v16, Av, (const __half *)hout, EpiRichWeight{tmp, hin, C().gred(), rs, 0}));
-        launch_k(C(), k_rich_scale_om, g, kEwThreads, 0, st, hout, rs, N);
+        F3R_TRY(mv_store(S.A.v16, Av, (const __half *)h0, w.tmp));
+        launch_k(C(), k_rich_weightK<8, K>, g, 256, 0, st, (const __half *)w.tmp, hi, N, gr, w.rs, 0);
+        launch_k(C(), k_rich_scale_omK<K>, g, kEwThreads, 0, st, h0, (const RichState *)w.rs, N);
         for (int k = 1; k < p.m4; k++) {
           const bool last = (k == p.m4 - 1);
-          F3R_TRY(launch_sell(C(), A.v16, Av, (const __half *)hout, EpiRichResPre{hin, M, hr, tmp2}));
-          F3R_TRY(launch_sell(C(), A.v16, Av, (const __half *)tmp2, EpiRichWeight{tmp, hr, C().gred(), rs, k}));
-          launch_k(C(), k_rich_axpy, g, kEwThreads, 0, st, hout, tmp2, rs, k, 0, last ? out : nullptr, isc, N);
+          F3R_TRY(mv(S.A.v16, Av, (const __half *)w.hout, EpiRichResPre{hi, M, w.hr, w.tmp2},
+                     EpiRichResPreK<K>{hi, M, w.hr, w.tmp2}));
+          F3R_TRY(mv_store(S.A.v16, Av, (const __half *)w.tmp2, w.tmp));
+          launch_k(C(), k_rich_weightK<8, K>, g, 256, 0, st, (const __half *)w.tmp, (const __half *)w.hr, N, gr, w.rs,
+                   k);
+          F3R_TRY(axpy(k, 0, last ? out_last : nullptr, last ? out16 : nullptr, isc));
         }
-        if (p.m4 == 1) launch_k(C(), k_rich_exit, g, kEwThreads, 0, st, hout, out, isc, N);
       }
     } else {
-      // general preconditioner: M = Z W^T (SDAINV) or U^-1 L^-1 (ILU)
-      launch_k(C(), k_rich_cast_in, g, kEwThreads, 0, st, in, in_inv, sc, hin, e_set, N);
-      F3R_TRY(prec_apply(hin, hout, !upd));
+      // general preconditioner: M = Z W^T (SDAINV) or U^-1 L^-1 (ILU, K = 1)
+      if constexpr (K == 1) {
+        if (h16) launch_k(C(), k_rich_cast_in<__half>, g, kEwThreads, 0, st, in16, in_inv, sc, w.hin, e_set, N);
+      }
+      if (!h16) launch_k(C(), k_rich_cast_inK<K>, g, kEwThreads, 0, st, in, in_inv, sc, w.hin, e_set, e_stride, N);
+      F3R_TRY(prec_apply(hi, h0, !upd));
       if (upd) {
-        F3R_TRY(launch_sell(C(), A.v16, Av, (const __half *)hout, EpiRichWeight{tmp, hin, C().gred(), rs, 0}));
-        launch_k(C(), k_rich_scale_om, g, kEwThreads, 0, st, hout, rs, N);
+        F3R_TRY(mv_store(S.A.v16, Av, (const __half *)h0, w.tmp));
+        launch_k(C(), k_rich_weightK<8, K>, g, 256, 0, st, (const __half *)w.tmp, hi, N, gr, w.rs, 0);
+        launch_k(C(), k_rich_scale_omK<K>, g, kEwThreads, 0, st, h0, (const RichState *)w.rs, N);
       }
       for (int k = 1; k < p.m4; k++) {
         const bool last = (k == p.m4 - 1);
-        F3R_TRY(launch_sell(C(), A.v16, Av, (const __half *)hout, EpiResidual<__half, __half>{hin, hr, nullptr}));
-        F3R_TRY(prec_apply(hr, tmp2, false));
-        if (upd) F3R_TRY(launch_sell(C(), A.v16, Av, (const __half *)tmp2, EpiRichWeight{tmp, hr, C().gred(), rs, k}));
-        launch_k(C(), k_rich_axpy, g, kEwThreads, 0, st, hout, tmp2, rs, k, upd ? 0 : 1, last ? out : nullptr, isc, N);
+        F3R_TRY(mv(S.A.v16, Av, (const __half *)w.hout, EpiResidual<__half, __half>{hi, w.hr, nullptr},
+                   EpiResidualK<__half, __half, K>{hi, w.hr}));
+        F3R_TRY(prec_apply(w.hr, w.tmp2, false));
+        if (upd) {
+          F3R_TRY(mv_store(S.A.v16, Av, (const __half *)w.tmp2, w.tmp));
+          launch_k(C(), k_rich_weightK<8, K>, g, 256, 0, st, (const __half *)w.tmp, (const __half *)w.hr, N, gr, w.rs,
+                   k);
+        }
+        F3R_TRY(axpy(k, upd ? 0 : 1, last ? out_last : nullptr, last ? out16 : nullptr, isc));
       }
-      if (p.m4 == 1) launch_k(C(), k_rich_exit, g, kEwThreads, 0, st, hout, out, isc, N);
     }
+    if (p.m4 == 1 && !out16) launch_k(C(), k_rich_exitK<K>, g, kEwThreads, 0, st, (const __half *)w.hout, out, isc, N);
     CUDA_TRY(cudaGetLastError());
+    return F3R_SUCCESS;
+  }
+
+  // hout = fp16(hout + om[k] t2), or the last step's result into out / out16
+  Status axpy(int k, int use_ome, float *out, __half *out16, float isc) {
+    const int g = C().ew_grid(n);
+    if constexpr (K == 1) {
+      if (out16) {
+        launch_k(C(), k_rich_axpy, g, kEwThreads, 0, C().stream, w.hout, (const __half *)w.tmp2,
+                 (const RichState *)w.rs, k, use_ome, (float *)nullptr, out16, isc, (int64_t)n);
+        return F3R_SUCCESS;
+      }
+    }
+    launch_k(C(), k_rich_axpyK<K>, g, kEwThreads, 0, C().stream, w.hout, (const __half *)w.tmp2,
+             (const RichState *)w.rs, k, use_ome, out, isc, (int64_t)n);
     return F3R_SUCCESS;
   }
 
   // out = M x for the general preconditioners; scale_ome multiplies by ome[0]
   Status prec_apply(const __half *x, __half *out, bool scale_ome) {
     if (p.precond == F3R_PRECOND_SDAINV) {
-      F3R_TRY(launch_sell(C(), W.v16, W.view(), x, EpiStore<__half>{tmp, nullptr}));
-      F3R_TRY(launch_sell(C(), Z.v16, Z.view(), (const __half *)tmp, EpiZScale{out, rs, scale_ome ? 1 : 0}));
-    } else if (p.precond == F3R_PRECOND_ILU0_BJ) {
-      F3R_TRY(ilu.apply(C().stream, x, tmp, out, scale_ome ? &rs->ome[0] : nullptr));
-      C().launches += 2;
-    } else if (p.precond == F3R_PRECOND_ILU0_LEVEL) {
-      F3R_TRY(ilul.apply(C().stream, x, tmp, out, scale_ome ? &rs->ome[0] : nullptr, C().err));
-      C().launches += 2;
-    } else {
-      F3R_TRY(jl.apply(C(), x, tmp, nullptr));
-      F3R_TRY(ju.apply(C(), tmp, out, scale_ome ? &rs->ome[0] : nullptr));
-    }
-    return F3R_SUCCESS;
-  }
-
-  // w = A z with H(j, 0..nv-1) = <w, V(k)> fused; the dot count picks the
-  // smallest epilogue instantiation (registers)
-  //
-  // The dots can ride in the SpMV epilogue (one read of w less) or run as a
-  // separate vectorised pass.  On B200 the SELL kernel is bound by the
-  // latency of each warp's slice loop, and the fused epilogue stretches it:
-  // 239 us fused against 187 + ~20 us separate for the 192^3 fp16 product, so
-  // the fp16 level uses the separate pass; the fp32 level keeps the fusion
-  // for up to 4 dots (its product streams more bytes per slice and hides the
-  // epilogue: 244 us fused against 228 + ~20 us) and separates wider ones.
-  // H(j, 0..nv-1) = <w, V(k)>, one vectorised pass
-  void dots(const float *w, const Cols<float> &Vc, int nv, float *hcol) {
-    const int gv = C().ew_grid(cdiv(n, 4));
-    if (nv <= 4)
-      launch_k(C(), k_multidot_f32<4, 8>, gv, 256, 0, C().stream, w, Vc, nv, (int64_t)n, C().gred(), hcol);
-    else if (nv <= 8)
-      launch_k(C(), k_multidot_f32<8, 8>, gv, 256, 0, C().stream, w, Vc, nv, (int64_t)n, C().gred(), hcol);
-    else
-      launch_k(C(), k_multidot_chunked<float, 8>, C().ew_grid(n), 256, 0, C().stream, w, Vc, nv, (int64_t)n,
-               C().gred(), hcol);
-  }
-
-  template <typename V>
-  Status spmv_dots(const V *vals, const float *z, float *w, const Cols<float> &Vc, int nv, float *hcol) {
-    if (sizeof(V) == 2 || nv > 4) {
-      F3R_TRY(launch_sell(C(), vals, A.view(), z, EpiStore<float>{w, nullptr}));
-      dots(w, Vc, nv, hcol);
+      F3R_TRY(mv_store(S.W.v16, S.W.view(), x, w.tmp));
+      F3R_TRY(mv(S.Z.v16, S.Z.view(), (const __half *)w.tmp, EpiZScale{out, w.rs, scale_ome ? 1 : 0},
+                 EpiZScaleK<K>{out, w.rs, scale_ome ? 1 : 0}));
       return F3R_SUCCESS;
     }
-    if (nv <= 4) return launch_sell(C(), vals, A.view(), z, EpiStoreDots<4>{w, Vc, nv, C().gred(), hcol});
-    return launch_sell(C(), vals, A.view(), z, EpiStoreDots<8>{w, Vc, nv, C().gred(), hcol});
+    if constexpr (K == 1) {
+      if (p.precond == F3R_PRECOND_ILU0_BJ) {
+        F3R_TRY(S.ilu.apply(C().stream, x, w.tmp, out, scale_ome ? &w.rs->ome[0] : nullptr));
+        C().launches += 2;
+      } else if (p.precond == F3R_PRECOND_ILU0_LEVEL) {
+        F3R_TRY(S.ilul.apply(C().stream, x, w.tmp, out, scale_ome ? &w.rs->ome[0] : nullptr, C().err));
+        C().launches += 2;
+      } else {
+        F3R_TRY(S.jl.apply(C(), x, w.tmp, nullptr));
+        F3R_TRY(S.ju.apply(C(), w.tmp, out, scale_ome ? &w.rs->ome[0] : nullptr));
+      }
+      return F3R_SUCCESS;
+    }
+    return fail(F3R_ERROR_UNSUPPORTED, "block solves take SDAINV only");
   }
 
-  // sFGMRES's second and third loops (gmres2.hpp:181-193): classical
+  // H(j, 0..nv-1) = <w, V(k)> per column, one pass over w and the basis
+  void dots(const float *wv, const Cols<float> &Vc, int nv, Level<float> &L, int j) {
+    float *hcol = L.H + (size_t)j * (L.m + 1);
+    const int64_t hs = (int64_t)(L.m + 1) * L.m;
+    if (nv <= 4)
+      launch_k(C(), k_multidot_f32K<4, 8, K>, C().ew_grid(cdiv(n, 4)), 256, 0, C().stream, wv, Vc, nv, (int64_t)n,
+               w.gr, hcol, hs);
+    else if (nv <= 8)
+      launch_k(C(), k_multidot_f32K<8, 8, K>, C().ew_grid(cdiv(n, 4)), 256, 0, C().stream, wv, Vc, nv, (int64_t)n,
+               w.gr, hcol, hs);
+    else
+      launch_k(C(), k_multidot_chunkedK<float, 8, K>, C().ew_grid(n), 256, 0, C().stream, wv, Vc, nv, (int64_t)n,
+               w.gr, hcol, hs);
+  }
+
+  // the Gram-Schmidt update, norm and Givens of step j of an inner level
+  void cgs(float *wv, const Cols<float> &Vc, int nv, Level<float> &L, int j, bool last) {
+    launch_k(C(), k_cgs_updateK<float, 8, K>, C().ew_grid(cdiv(n, 4)), 256, 0, C().stream, wv, Vc, nv, (int64_t)n,
+             w.gr, L.view(), j, last ? 1 : 0, (double *)nullptr, (const uint32_t *)w.active, C().err);
+  }
+
+  // sFGMRES's second and third loops (gmres2.hpp:181-193), K = 1: classical
   // Gram-Schmidt of the stored raw vectors W(1..m) against the basis built so
-  // far, with each Givens rotation fused into its step as in FGMRES (the
-  // rotation of column j needs only column j).  The next step reads V(j+1)
-  // through the dots and the update, so it is normalised explicitly here.
+  // far, with each Givens rotation fused into its step as in FGMRES.  The next
+  // step reads V(j+1) through the dots and the update, so it is normalised
+  // explicitly here.
   Status sstep_orthogonalise(Level<float> &L, float *const *Vp, const Cols<float> &V) {
     const int64_t N = n;
-    const int gv = C().ew_grid(cdiv(N, 4));
     for (int j = 0; j < L.m; j++) {
-      float *w = Vp[j + 1];
-      dots(w, V, j + 1, L.H + (size_t)j * (L.m + 1));
-      GivensCtl<float> g{L.H, L.cs, L.sn, L.e, L.y, L.inv, nullptr, L.m + 1, j, j == L.m - 1, C().err};
-      launch_k(C(), k_cgs_update<float, 8>, gv, 256, 0, C().stream, w, V, j + 1, N, C().gred(), g);
-      if (j + 1 < L.m) launch_k(C(), k_scale<float>, gv, kEwThreads, 0, C().stream, w, (const float *)L.inv, N);
+      float *wv = Vp[j + 1];
+      dots(wv, V, j + 1, L, j);
+      cgs(wv, V, j + 1, L, j, j == L.m - 1);
+      if (j + 1 < L.m)
+        launch_k(C(), k_scale<float>, C().ew_grid(cdiv(N, 4)), kEwThreads, 0, C().stream, wv, (const float *)L.inv, N);
     }
     CUDA_TRY(cudaGetLastError());
     return F3R_SUCCESS;
   }
 
-  // ---- level 3: FGMRES<float>(A16, R, m3), input V2 column, output Z2 col ----
-  // The normalisation V(j+1) *= 1/h of every basis vector is deferred to the
-  // first kernel that reads it next (the Richardson entry), which scales it
-  // in place; the last basis vector of a level is never read again and is
-  // left unscaled.  in_inv is the pending factor of `in` (nullptr if none).
+  // What an fp32 level calls as its preconditioner: R, or (K = 1) the
+  // fp16-vector level when there is one (which then calls R).
+  Status inner_apply(float *in, float *out, float *e_set, int64_t e_stride, const float *in_inv) {
+    if constexpr (K == 1) {
+      if (p.half_m > 0) return levelh(in, in_inv, out, e_set);
+    }
+    return rich_apply(in, out, e_set, e_stride, in_inv);
+  }
+
+  // ---- the fp16-vector level (K = 1): FGMRES<_Float16>(A16, R, half_m) ---------
+  // (work/src/depth.cpp:122-167).  in32 / out32: the calling fp32 level's
+  // columns (in32_inv the pending 1/h of in32, e_parent the caller's e to set
+  // on its first call); in32 = nullptr: called by the outer level, input and
+  // output through the slots.
+  Status levelh(float *in32, const float *in32_inv, float *out32, float *e_parent) {
+    if constexpr (K != 1) {
+      return fail(F3R_ERROR_UNSUPPORTED, "block solves have no fp16-vector level");
+    } else {
+      HLevel &L = w.LH;
+      const int64_t N = n;
+      const int gv = C().ew_grid(cdiv(N, 8));
+      cudaStream_t st = C().stream;
+      if (in32)
+        launch_k(C(), k_level_enter_h<float>, gv, kEwThreads, 0, st, in32, (float *const *)nullptr, in32_inv, L.V,
+                 L.e, e_parent, N);
+      else
+        launch_k(C(), k_level_enter_h<double>, gv, kEwThreads, 0, st, (double *)nullptr, (double *const *)w.in_slot,
+                 (const double *)w.L1.inv, L.V, L.e, (float *)nullptr, N);
+      Cols<__half> V{}, Zc{};
+      for (int k = 0; k <= L.m; k++) V.p[k] = L.V + (size_t)k * ldn;
+      for (int k = 0; k < L.m; k++) Zc.p[k] = L.Z + (size_t)k * ldn;
+      for (int j = 0; j < L.m; j++) {
+        __half *vj = L.V + (size_t)j * ldn, *zj = L.Z + (size_t)j * ldn, *wv = L.V + (size_t)(j + 1) * ldn;
+        // R normalises V(j) in place first (its 1/h is pending from step j - 1)
+        F3R_TRY(rich_apply(nullptr, nullptr, nullptr, 0, j == 0 ? nullptr : L.inv, vj, zj));
+        F3R_TRY(launch_sell(C(), S.A.v16, S.A.view(), (const __half *)zj, EpiStore<__half>{wv, nullptr}));
+        launch_k(C(), k_multidot_h<8>, gv, 256, 0, st, (const __half *)wv, V, j + 1, N, w.gr,
+                 L.H + (size_t)j * (L.m + 1));
+        GivensCtl<float> g{L.H, L.cs, L.sn, L.e, L.y, L.inv, nullptr, L.m + 1, j, j == L.m - 1, C().err};
+        launch_k(C(), k_cgs_update_h<8>, gv, 256, 0, st, wv, V, j + 1, N, w.gr, g);
+      }
+      if (out32)
+        launch_k(C(), k_zy_h<float>, gv, kEwThreads, 0, st, Zc, (const float *)L.y, L.m, out32,
+                 (float *const *)nullptr, N);
+      else
+        launch_k(C(), k_zy_h<double>, gv, kEwThreads, 0, st, Zc, (const float *)L.y, L.m, (double *)nullptr,
+                 (double *const *)w.out_slot, N);
+      CUDA_TRY(cudaGetLastError());
+      return F3R_SUCCESS;
+    }
+  }
+
+  // ---- level 3: FGMRES<float>(A16, R, m3), input a level-2 block column, output
+  // a level-2 Z column.  The normalisation V(j+1) *= 1/h of every basis vector
+  // is deferred to the first kernel that reads it next (R's entry), which
+  // scales it in place; the last basis vector of a level is never read again
+  // and is left unscaled.  in_inv: the pending factors of `in` (nullptr if none).
   Status level3(float *in, float *out, const float *in_inv) {
-    Level<float> &L = L3;
-    const int64_t N = n;
-    const int gv = C().ew_grid(cdiv(N, 4));
+    Level<float> &L = w.L3;
     float *Vp[kMaxCols];
     Cols<float> V{}, Zc{};
     Vp[0] = in;
-    for (int k = 1; k <= L.m; k++) Vp[k] = L.V + (size_t)(k - 1) * ldn;
+    for (int k = 1; k <= L.m; k++) Vp[k] = L.V + (size_t)(k - 1) * lk();
     for (int k = 0; k <= L.m; k++) V.p[k] = Vp[k];
-    for (int k = 0; k < L.m; k++) Zc.p[k] = L.Z + (size_t)k * ldn;
-    if (p.inner_sstep & 2) {
+    for (int k = 0; k < L.m; k++) Zc.p[k] = L.Z + (size_t)k * lk();
+    const int64_t es = L.m + 1;
+    if ((p.inner_sstep & 2) && K == 1) {
       // sFGMRES (gmres2.hpp:176-180): W(j+1) = A16 R W(j) on the raw vectors
       for (int j = 0; j < L.m; j++) {
-        float *zj = L.Z + (size_t)j * ldn;
-        F3R_TRY(rich_apply(Vp[j], zj, j == 0 ? L.e : nullptr, j == 0 ? in_inv : nullptr));
-        F3R_TRY(launch_sell(C(), A.v16, A.view(), (const float *)zj, EpiStore<float>{Vp[j + 1], nullptr}));
+        float *zj = L.Z + (size_t)j * lk();
+        F3R_TRY(inner_apply(Vp[j], zj, j == 0 ? L.e : nullptr, es, j == 0 ? in_inv : nullptr));
+        F3R_TRY(mv_store(S.A.v16, S.A.view(), (const float *)zj, Vp[j + 1]));
       }
       F3R_TRY(sstep_orthogonalise(L, Vp, V));
     } else {
       for (int j = 0; j < L.m; j++) {
-        float *zj = L.Z + (size_t)j * ldn;
-        float *w = Vp[j + 1];
-        F3R_TRY(rich_apply(Vp[j], zj, j == 0 ? L.e : nullptr, j == 0 ? in_inv : L.inv));
-        F3R_TRY(spmv_dots(A.v16, zj, w, V, j + 1, L.H + (size_t)j * (L.m + 1)));
-        GivensCtl<float> g{L.H, L.cs, L.sn, L.e, L.y, L.inv, nullptr, L.m + 1, j, j == L.m - 1, C().err};
-        launch_k(C(), k_cgs_update<float, 8>, gv, 256, 0, C().stream, w, V, j + 1, N, C().gred(), g);
+        float *zj = L.Z + (size_t)j * lk();
+        float *wv = Vp[j + 1];
+        F3R_TRY(inner_apply(Vp[j], zj, j == 0 ? L.e : nullptr, es, j == 0 ? in_inv : L.inv));
+        F3R_TRY(mv_store(S.A.v16, S.A.view(), (const float *)zj, wv));
+        dots(wv, V, j + 1, L, j);
+        cgs(wv, V, j + 1, L, j, j == L.m - 1);
       }
     }
-    launch_k(C(), k_zy<float, float, false>, gv, kEwThreads, 0, C().stream, Zc, L.y, L.m, out, nullptr, N);
+    launch_k(C(), k_zyK<float, float, false, K>, C().ew_grid(n), kEwThreads, 0, C().stream, Zc, (const float *)L.y,
+             (int64_t)(L.m + 1), L.m, out, (float *const *)nullptr, 0u, (int64_t)n);
     CUDA_TRY(cudaGetLastError());
     return F3R_SUCCESS;
   }
 
-  // ---- level 2: FGMRES<float>(A32, L3, m2); in/out through the slots -------
+  // ---- level 2: FGMRES<float>(A32, L3, m2); in / out through the slots -------
   Status level2() {
-    Level<float> &L = L2;
-    const int64_t N = n;
-    const int gv = C().ew_grid(cdiv(N, 4));
+    Level<float> &L = w.L2;
     float *Vp[kMaxCols];
     Cols<float> V{}, Zc{};
-    for (int k = 0; k <= L.m; k++) V.p[k] = Vp[k] = L.V + (size_t)k * ldn;
-    for (int k = 0; k < L.m; k++) Zc.p[k] = L.Z + (size_t)k * ldn;
-    // normalises the outer basis vector in place (its 1/h is L1.inv) and casts it
-    launch_k(C(), k_level2_enter, gv, kEwThreads, 0, C().stream, (double *const *)in_slot, (const double *)L1.inv, L.V,
-             L.e, N);
-    if (p.inner_sstep & 1) {
+    for (int k = 0; k <= L.m; k++) V.p[k] = Vp[k] = L.V + (size_t)k * lk();
+    for (int k = 0; k < L.m; k++) Zc.p[k] = L.Z + (size_t)k * lk();
+    // normalises the outer basis block in place (its 1/h are L1.inv) and casts it
+    launch_k(C(), k_level2_enterK<K>, C().ew_grid(n), kEwThreads, 0, C().stream, (double *const *)w.in_slot,
+             (const double *)w.L1.inv, L.V, L.e, (int64_t)(L.m + 1), (int64_t)n);
+    if ((p.inner_sstep & 1) && K == 1) {
       // sFGMRES (gmres2.hpp:176-180): W(j+1) = A32 M W(j) on the raw vectors
       for (int j = 0; j < L.m; j++) {
-        float *zj = L.Z + (size_t)j * ldn;
+        float *zj = L.Z + (size_t)j * lk();
         if (p.m3 > 0) F3R_TRY(level3(Vp[j], zj, nullptr));
-        else F3R_TRY(rich_apply(Vp[j], zj, nullptr, nullptr));
-        F3R_TRY(launch_sell(C(), A.v32, A.view(), (const float *)zj, EpiStore<float>{Vp[j + 1], nullptr}));
+        else F3R_TRY(inner_apply(Vp[j], zj, nullptr, 0, nullptr));
+        F3R_TRY(mv_store(S.A.v32, S.A.view(), (const float *)zj, Vp[j + 1]));
       }
       F3R_TRY(sstep_orthogonalise(L, Vp, V));
     } else {
       for (int j = 0; j < L.m; j++) {
-        float *zj = L.Z + (size_t)j * ldn;
-        float *w = Vp[j + 1];
+        float *zj = L.Z + (size_t)j * lk();
+        float *wv = Vp[j + 1];
         if (p.m3 > 0) F3R_TRY(level3(Vp[j], zj, j == 0 ? nullptr : L.inv));
-        else F3R_TRY(rich_apply(Vp[j], zj, nullptr, j == 0 ? nullptr : L.inv));  // depth 2: R directly
-        F3R_TRY(spmv_dots(A.v32, zj, w, V, j + 1, L.H + (size_t)j * (L.m + 1)));
-        GivensCtl<float> g{L.H, L.cs, L.sn, L.e, L.y, L.inv, nullptr, L.m + 1, j, j == L.m - 1, C().err};
-        launch_k(C(), k_cgs_update<float, 8>, gv, 256, 0, C().stream, w, V, j + 1, N, C().gred(), g);
+        else F3R_TRY(inner_apply(Vp[j], zj, nullptr, 0, j == 0 ? nullptr : L.inv));  // depth 2: R directly
+        F3R_TRY(mv_store(S.A.v32, S.A.view(), (const float *)zj, wv));
+        dots(wv, V, j + 1, L, j);
+        cgs(wv, V, j + 1, L, j, j == L.m - 1);
       }
     }
-    launch_k(C(), k_zy<float, double, false>, gv, kEwThreads, 0, C().stream, Zc, L.y, L.m, nullptr, out_slot, N);
+    launch_k(C(), k_zyK<float, double, false, K>, C().ew_grid(n), kEwThreads, 0, C().stream, Zc, (const float *)L.y,
+             (int64_t)(L.m + 1), L.m, (double *)nullptr, (double *const *)w.out_slot, 0u, (int64_t)n);
     CUDA_TRY(cudaGetLastError());
     return F3R_SUCCESS;
   }
+
+  // What the outer level calls for one column: level 2, or (m2 = 0) the
+  // fp16-vector level with its input and output through the slots.
+  Status outer_inner() { return p.m2 > 0 ? level2() : levelh(nullptr, nullptr, nullptr, nullptr); }
 
   // One call into level 2 for outer column j, replayed from a CUDA graph
   // keyed by which Richardson calls inside it update their weights.
   Status level2_call(double *in, double *out) {
     // the graph reads its input and output columns from two device slots,
     // set stream-ordered by a one-thread kernel (no host staging copy)
-    launch_k(C(), k_set_slots, 1, 1, 0, C().stream, in_slot, out_slot, in, out);
+    launch_k(C(), k_set_slots, 1, 1, 0, C().stream, w.in_slot, w.out_slot, in, out);
     // the legacy / per-thread default streams cannot be captured
     const cudaStream_t cs = C().stream;
-    if (!p.use_graphs || cs == 0 || cs == cudaStreamLegacy || cs == cudaStreamPerThread) return level2();
-    const int calls = p.m2 * std::max(p.m3, 1);
+    if (!p.use_graphs || cs == 0 || cs == cudaStreamLegacy || cs == cudaStreamPerThread) return outer_inner();
+    const int calls = S.calls_per_outer();
     std::vector<bool> key(calls);
-    for (int i = 0; i < calls; i++) key[i] = ((cnt + 1 + i) % p.c) == 0;
-    auto it = graphs.find(key);
-    if (it == graphs.end()) {
-      const int64_t cnt0 = cnt, rc0 = r_calls, l0 = C().launches;
+    for (int i = 0; i < calls; i++) key[i] = ((w.cnt + 1 + i) % p.c) == 0;
+    auto it = w.graphs.find(key);
+    if (it == w.graphs.end()) {
+      const int64_t cnt0 = w.cnt, rc0 = w.r_calls, l0 = C().launches;
       cudaGraph_t graph = nullptr;
       CUDA_TRY(cudaStreamBeginCapture(C().stream, cudaStreamCaptureModeThreadLocal));
-      Status s = level2();
+      Status s = outer_inner();
       cudaError_t ce = cudaStreamEndCapture(C().stream, &graph);
       if (s != F3R_SUCCESS) {
         if (graph) cudaGraphDestroy(graph);
@@ -691,169 +943,386 @@ struct Solver {
       ce = cudaGraphInstantiate(&exec, graph, 0);
       cudaGraphDestroy(graph);
       if (ce != cudaSuccess) return fail(F3R_ERROR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ce));
-      it = graphs.emplace(key, std::make_pair(exec, C().launches - l0)).first;
-      cnt = cnt0;  // capture advanced the counters without running anything
-      r_calls = rc0;
+      it = w.graphs.emplace(key, std::make_pair(exec, C().launches - l0)).first;
+      w.cnt = cnt0;  // capture advanced the counters without running anything
+      w.r_calls = rc0;
       C().launches = l0;
     }
     CUDA_TRY(cudaGraphLaunch(it->second.first, C().stream));
     C().launches += it->second.second;
-    cnt += calls;
-    r_calls += calls;
+    w.cnt += calls;
+    w.r_calls += calls;
     return F3R_SUCCESS;
   }
 
-  // |e| and the device error word come back together, one synchronisation per outer step
-  Status read_abs_e(double *v) {
+  // the K values of `dev` (|e| of the outer step) and the device error word
+  // come back together: one synchronisation per outer step
+  Status read_k(const double *dev, double *host) {
     int *e_h = reinterpret_cast<int *>(C().pinned + 7);
-    CUDA_TRY(cudaMemcpyAsync(C().pinned, abs_e, sizeof(double), cudaMemcpyDeviceToHost, C().stream));
+    double *pk = C().pinned;  // up to 6 values fit beside the active word and the error word
     CUDA_TRY(cudaMemcpyAsync(e_h, C().err, sizeof(int), cudaMemcpyDeviceToHost, C().stream));
+    CUDA_TRY(cudaMemcpyAsync(K <= 6 ? pk : host, dev, sizeof(double) * K, cudaMemcpyDeviceToHost, C().stream));
     CUDA_TRY(cudaStreamSynchronize(C().stream));
     if (*e_h != DEV_OK) return C().check_device_error();  // maps the word to a status and clears it
-    *v = C().pinned[0];
+    if (K <= 6)
+      for (int c = 0; c < K; c++) host[c] = pk[c];
+    return F3R_SUCCESS;
+  }
+  Status set_active(uint32_t mask) {
+    uint32_t *h = reinterpret_cast<uint32_t *>(C().pinned + 6);
+    *h = mask;
+    CUDA_TRY(cudaMemcpyAsync(w.active, h, sizeof(uint32_t), cudaMemcpyHostToDevice, C().stream));
+    CUDA_TRY(cudaStreamSynchronize(C().stream));  // the pinned word is reused by the next call
     return F3R_SUCCESS;
   }
 
-  // ---- level 1 inside Restarted (gmres.hpp:85-134, restart.hpp:26-36) -------
-  Status solve(const double *b_user, double *x_user, f3r_cond_fn cond, void *user, f3r_result *res) {
+  // ---- level 1 inside Restarted (gmres.hpp:85-134, restart.hpp:26-36) over K
+  // columns in lockstep.  b, x: device blocks of K interleaved columns in the
+  // solver's storage order (x holds the initial guesses); ncols <= K columns
+  // are real, the others padding (inactive from the start).  cond(i, |e|) is
+  // called for every active column after every outer step, in column order.
+  Status solve_block(const double *bs, double *xs, int ncols, f3r_cond_fn cond, void *user, f3r_result *res) {
     const int64_t N = n;
     cudaStream_t st = C().stream;
     const int g = C().ew_grid(N);
-    auto is_dev = [&](const void *q) {
-      cudaPointerAttributes a{};
-      if (cudaPointerGetAttributes(&a, q) != cudaSuccess) {
-        cudaGetLastError();
-        return false;
-      }
-      return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
-    };
-    const bool b_dev = is_dev(b_user), x_dev = is_dev(x_user);
-    // x is updated with 16-byte vector accesses: a device x that is not
-    // 16-byte aligned is worked on in an internal copy
-    const bool x_direct = x_dev && (reinterpret_cast<uintptr_t>(x_user) % 16 == 0);
-    const double *b = b_user;
-    double *x = x_user;
-    if (!b_dev) {
-      CUDA_TRY(cudaMemcpyAsync(b_d, b_user, sizeof(double) * N, cudaMemcpyHostToDevice, st));
-      b = b_d;
-    }
-    if (!x_direct) {
-      CUDA_TRY(cudaMemcpyAsync(x_d, x_user, sizeof(double) * N, x_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
-                               st));
-      x = x_d;
-    }
-    CUDA_TRY(cudaEventRecord(ev0, st));
+    CUDA_TRY(cudaEventRecord(S.ev0, st));
     const int64_t launches0 = C().launches;
-    // permuted system (SELL-C-sigma order)
-    const double *bs = b;
-    double *xs = x;
-    if (perm_d) {
-      launch_k(C(), k_permute_gather, g, kEwThreads, 0, st, b, perm_d, bp_d, N);
-      launch_k(C(), k_permute_gather, g, kEwThreads, 0, st, x, perm_d, xp_d, N);
-      bs = bp_d;
-      xs = xp_d;
-    }
-    // per-solve Richardson state (f3r-gpu.cpp:277-281)
-    cnt = p.c;
-    r_calls = 0;
+    // per-solve Richardson state (f3r-gpu.cpp:277-281), one per column
+    w.cnt = p.c;
+    w.r_calls = 0;
     {
-      RichState h{};
-      for (int k = 0; k < kMaxM4; k++) {
-        h.sum[k] = 1.0f;
-        // F3R-Static: the fixed weight in the reference's fp16 scalar (static.cpp:99-100)
-        h.ome[k] = __float2half(p.static_weight > 0 ? (float)p.static_weight : 1.0f);
-        h.om[k] = 0.0f;
+      RichState h[K];
+      for (int c = 0; c < K; c++) {
+        RichState &q = h[c];
+        std::memset(&q, 0, sizeof(q));
+        for (int k = 0; k < kMaxM4; k++) {
+          q.sum[k] = 1.0f;
+          // F3R-Static: the fixed weight in the reference's fp16 scalar (static.cpp:99-100)
+          q.ome[k] = __float2half(p.static_weight > 0 ? (float)p.static_weight : 1.0f);
+          q.om[k] = 0.0f;
+        }
+        q.den = 1;
       }
-      h.den = 1;
-      CUDA_TRY(cudaMemcpyAsync(rs, &h, sizeof(h), cudaMemcpyHostToDevice, st));
+      CUDA_TRY(cudaMemcpyAsync(w.rs, h, sizeof(h), cudaMemcpyHostToDevice, st));
       CUDA_TRY(cudaStreamSynchronize(st));
     }
-    // ||b|| for the relative stop test
-    double nb = 0;
-    launch_k(C(), k_dot<double, double, 8>, g, 256, 0, st, bs, bs, N, C().gred(), C().dscratch);
-    CUDA_TRY(cudaMemcpyAsync(C().pinned, C().dscratch, sizeof(double), cudaMemcpyDeviceToHost, st));
-    CUDA_TRY(cudaStreamSynchronize(st));
-    nb = std::sqrt(C().pinned[0]);
-    auto stop = [&](int i, double e) -> bool {
+    uint32_t active = ncols >= 32 ? 0xffffffffu : ((1u << ncols) - 1u);
+    F3R_TRY(set_active(active));
+    // ||b|| per column for the relative stop test
+    double nb[K];
+    launch_k(C(), k_dotK<double, double, 8, K>, g, 256, 0, st, bs, bs, N, w.gr, w.nrm);
+    F3R_TRY(read_k(w.nrm, nb));
+    for (int c = 0; c < K; c++) nb[c] = std::sqrt(nb[c]);
+    auto stop = [&](int c, int i, double e) -> bool {
       if (cond) return cond(i, e, user) != 0;
-      return nb > 0 ? (e / nb < p.rel_tol) : (e == 0);
+      return nb[c] > 0 ? (e / nb[c] < p.rel_tol) : (e == 0);
     };
-
-    Level<double> &L = L1;
-    Cols<double> V{}, Zc{};
-    const int gv = C().ew_grid(cdiv(N, 2));
-    for (int k = 0; k <= L.m; k++) V.p[k] = L.V + (size_t)k * ldn;
-    for (int k = 0; k < L.m; k++) Zc.p[k] = L.Z + (size_t)k * ldn;
-    f3r_result out{};
+    Level<double> &L = w.L1;
+    const LevelK<double> Lv = L.view();
+    f3r_result out[K];
+    std::memset(out, 0, sizeof(out));
+    double last_e[K] = {0}, ev[K];
     int restarts = 0;
-    double last_e = 0;
-    bool solved = false;
-    while (!solved && restarts < p.max_restarts) {
+    while (active && restarts < p.max_restarts) {
       restarts++;
-      // r = b - A x with ||r|| fused (gmres.hpp:87, 100)
-      F3R_TRY(launch_sell(C(), A.v64, A.view(), (const double *)xs,
-                          EpiResidualNorm{bs, L.V, C().gred(), L.e, L.inv, abs_e}));
-      double h0;
-      F3R_TRY(read_abs_e(&h0));
-      last_e = h0;
-      if (stop(0, h0)) {
-        solved = true;
-        break;
+      for (int c = 0; c < K; c++)
+        if ((active >> c) & 1u) out[c].restarts = restarts;
+      F3R_TRY(ensure_outer(0));
+      // r = b - A x and ||r|| per column (gmres.hpp:87, 100)
+      F3R_TRY(mv(S.A.v64, S.A.view(), (const double *)xs, EpiResidual<double, double>{bs, w.V1[0], nullptr},
+                 EpiResidualK<double, double, K>{bs, w.V1[0]}));
+      launch_k(C(), k_resnormK<8, K>, g, 256, 0, st, (const double *)w.V1[0], N, w.gr, Lv, w.abs_e,
+               (const uint32_t *)w.active);
+      F3R_TRY(read_k(w.abs_e, ev));
+      for (int c = 0; c < K; c++) {
+        if (!((active >> c) & 1u)) continue;
+        last_e[c] = ev[c];
+        if (stop(c, 0, ev[c])) {
+          out[c].is_solved = 1;
+          active &= ~(1u << c);
+        }
       }
+      if (!active) break;
+      F3R_TRY(set_active(active));
       // V(0) = r / ||r|| happens inside the level-2 entry kernel (in place)
       int j = 0;
-      bool conv = false;
-      for (; j < L.m; j++) {
-        double *zj = L.Z + (size_t)j * ldn;
-        double *w = L.V + (size_t)(j + 1) * ldn;
-        F3R_TRY(level2_call(L.V + (size_t)j * ldn, zj));
-        F3R_TRY(launch_sell(C(), A.v64, A.view(), (const double *)zj, EpiStore<double>{w, nullptr}));
-        launch_k(C(), k_multidot_chunked<double, 8>, g, 256, 0, st, w, V, j + 1, N, C().gred(), L.H + (size_t)j * (L.m + 1));
-        GivensCtl<double> gc{L.H, L.cs, L.sn, L.e, L.y, L.inv, abs_e, L.m + 1, j, 0, C().err};
-        launch_k(C(), k_cgs_update<double, 8>, gv, 256, 0, st, w, V, j + 1, N, C().gred(), gc);
+      uint32_t running = active;  // the columns of this cycle that have not converged
+      for (; j < L.m && running; j++) {
+        F3R_TRY(ensure_outer(j));
+        Cols<double> V{};
+        for (int k = 0; k <= j + 1; k++) V.p[k] = w.V1[k];
+        double *zj = w.Z1[j], *wv = w.V1[j + 1];
+        F3R_TRY(level2_call(w.V1[j], zj));
+        F3R_TRY(mv_store(S.A.v64, S.A.view(), (const double *)zj, wv));
+        launch_k(C(), k_multidot_chunkedK<double, 8, K>, g, 256, 0, st, (const double *)wv, V, j + 1, N, w.gr,
+                 L.H + (size_t)j * (L.m + 1), (int64_t)(L.m + 1) * L.m);
+        launch_k(C(), k_cgs_updateK<double, 8, K>, C().ew_grid(cdiv(N, 2)), 256, 0, st, wv, V, j + 1, N, w.gr, Lv, j,
+                 0, w.abs_e, (const uint32_t *)w.active, C().err);
         CUDA_TRY(cudaGetLastError());
-        double ej;
-        F3R_TRY(read_abs_e(&ej));
-        last_e = ej;
-        out.res_iter++;
-        if (stop(j + 1, ej)) {
-          j++;
-          conv = true;
-          break;
+        F3R_TRY(read_k(w.abs_e, ev));
+        uint32_t done = 0;
+        for (int c = 0; c < K; c++) {
+          if (!((running >> c) & 1u)) continue;
+          last_e[c] = ev[c];
+          out[c].res_iter++;
+          if (stop(c, j + 1, ev[c])) done |= 1u << c;
+        }
+        if (done) {
+          // x += Z y for the columns that converged at this step (gmres.hpp:121-131)
+          Cols<double> Zc{};
+          for (int k = 0; k <= j; k++) Zc.p[k] = w.Z1[k];
+          launch_k(C(), k_trsv_yK<double, K>, 1, 32, 0, st, Lv, done, j + 1);
+          launch_k(C(), k_zyK<double, double, true, K>, g, kEwThreads, 0, st, Zc, (const double *)L.y,
+                   (int64_t)(L.m + 1), j + 1, xs, (double *const *)nullptr, done, N);
+          for (int c = 0; c < K; c++)
+            if ((done >> c) & 1u) out[c].is_solved = 1;
+          running &= ~done;
+          active &= ~done;
+          F3R_TRY(set_active(running));
         }
         // w = V(j+1) is normalised by the next step's level-2 entry kernel
       }
-      launch_k(C(), k_trsv_y<double>, 1, 32, 0, st, L.H, L.e, L.y, L.m + 1, j);
-      launch_k(C(), k_zy<double, double, true>, gv, kEwThreads, 0, st, Zc, L.y, j, xs, nullptr, N);
-      CUDA_TRY(cudaGetLastError());
-      if (conv) solved = true;
+      if (running) {
+        // the restart length reached: x += Z y over all m columns, then restart
+        Cols<double> Zc{};
+        for (int k = 0; k < j; k++) Zc.p[k] = w.Z1[k];
+        launch_k(C(), k_trsv_yK<double, K>, 1, 32, 0, st, Lv, running, j);
+        launch_k(C(), k_zyK<double, double, true, K>, g, kEwThreads, 0, st, Zc, (const double *)L.y,
+                 (int64_t)(L.m + 1), j, xs, (double *const *)nullptr, running, N);
+        CUDA_TRY(cudaGetLastError());
+        F3R_TRY(set_active(active));
+      }
     }
-    if (perm_d) launch_k(C(), k_permute_scatter, g, kEwThreads, 0, st, xs, perm_d, x, N);
-    CUDA_TRY(cudaEventRecord(ev1, st));
-    out.kernel_launches = C().launches - launches0;
-    // explicit residual ||b - A x|| / ||b|| in fp64 (outside the timed region,
-    // as the drivers, f3r-gpu.cpp:99-102)
-    F3R_TRY(launch_sell(C(), A.v64, A.view(), (const double *)xs, EpiResidual<double, double>{bs, r_d, nullptr}));
-    launch_k(C(), k_dot<double, double, 8>, g, 256, 0, st, r_d, r_d, N, C().gred(), C().dscratch);
-    CUDA_TRY(cudaMemcpyAsync(C().pinned, C().dscratch, sizeof(double), cudaMemcpyDeviceToHost, st));
-    if (!x_direct)
-      CUDA_TRY(cudaMemcpyAsync(x_user, x, sizeof(double) * N, x_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
-                               st));
-    CUDA_TRY(cudaStreamSynchronize(st));
+    CUDA_TRY(cudaEventRecord(S.ev1, st));
+    const int64_t nl = C().launches - launches0;
+    // explicit residual ||b - A x|| / ||b|| in fp64 per column (outside the
+    // timed region, as the drivers, f3r-gpu.cpp:99-102)
+    F3R_TRY(mv(S.A.v64, S.A.view(), (const double *)xs, EpiResidual<double, double>{bs, w.r_d, nullptr},
+               EpiResidualK<double, double, K>{bs, w.r_d}));
+    double er[K];
+    launch_k(C(), k_dotK<double, double, 8, K>, g, 256, 0, st, (const double *)w.r_d, (const double *)w.r_d, N, w.gr,
+             w.nrm);
+    F3R_TRY(read_k(w.nrm, er));
     F3R_TRY(C().check_device_error());
     float ms = 0;
-    CUDA_TRY(cudaEventElapsedTime(&ms, ev0, ev1));
-    out.is_solved = solved ? 1 : 0;
-    out.res_nrm2 = last_e;
-    out.impl_rel_res = nb > 0 ? last_e / nb : last_e;
-    out.expl_rel_res = nb > 0 ? std::sqrt(C().pinned[0]) / nb : std::sqrt(C().pinned[0]);
-    out.restarts = restarts;
-    out.inner_applications = r_calls;
-    out.solve_seconds = ms * 1e-3;
-    if (res) *res = out;
+    CUDA_TRY(cudaEventElapsedTime(&ms, S.ev0, S.ev1));
+    for (int c = 0; c < ncols; c++) {
+      f3r_result &o = out[c];
+      o.res_nrm2 = last_e[c];
+      o.impl_rel_res = nb[c] > 0 ? last_e[c] / nb[c] : last_e[c];
+      o.expl_rel_res = nb[c] > 0 ? std::sqrt(er[c]) / nb[c] : std::sqrt(er[c]);
+      o.inner_applications = w.r_calls;
+      o.solve_seconds = ms * 1e-3;
+      o.kernel_launches = nl;
+      if (res) res[c] = o;
+    }
     return F3R_SUCCESS;
   }
 };
+
+// the workspace of K-column solves, made on first use
+template <int K> Status make_work(Solver &s, Work<K> &w) {
+  const size_t nn = (size_t)std::max(s.n, 1) * K;
+  const f3r_params &p = s.p;
+  F3R_TRY(w.make_level(w.L1, p.m_outer, s.ldn, true, false));
+  if (p.m2 > 0) F3R_TRY(w.make_level(w.L2, p.m2, s.ldn, true));
+  if (p.m3 > 0) F3R_TRY(w.make_level(w.L3, p.m3, s.ldn, false));
+  if (K == 1 && p.half_m > 0) {
+    HLevel &L = w.LH;
+    const int m = p.half_m;
+    L.m = m;
+    const size_t ln = (size_t)std::max<int64_t>(s.ldn, 8);
+    F3R_TRY(w.alloc(&L.V, ln * (size_t)(m + 1)));
+    F3R_TRY(w.alloc(&L.Z, ln * (size_t)m));
+    F3R_TRY(w.alloc(&L.H, (size_t)(m + 1) * m));
+    F3R_TRY(w.alloc(&L.cs, (size_t)m));
+    F3R_TRY(w.alloc(&L.sn, (size_t)m));
+    F3R_TRY(w.alloc(&L.e, (size_t)m + 1));
+    F3R_TRY(w.alloc(&L.y, (size_t)m));
+    F3R_TRY(w.alloc(&L.inv, 1));
+    CUDA_TRY(cudaMemset(L.H, 0, sizeof(float) * (size_t)(m + 1) * m));
+    CUDA_TRY(cudaMemset(L.e, 0, sizeof(float) * (size_t)(m + 1)));
+  }
+  F3R_TRY(w.alloc(&w.abs_e, K));
+  F3R_TRY(w.alloc(&w.nrm, K));
+  F3R_TRY(w.alloc(&w.hin, nn));
+  F3R_TRY(w.alloc(&w.hout, nn));
+  F3R_TRY(w.alloc(&w.hout2, nn));
+  F3R_TRY(w.alloc(&w.tmp, nn));
+  F3R_TRY(w.alloc(&w.tmp2, nn));
+  F3R_TRY(w.alloc(&w.hr, nn));
+  CUDA_TRY(cudaMemset(w.tmp2, 0, nn * sizeof(__half)));
+  F3R_TRY(w.alloc(&w.rs, K));
+  F3R_TRY(w.alloc(&w.in_slot, 1));
+  F3R_TRY(w.alloc(&w.out_slot, 1));
+  F3R_TRY(w.alloc(&w.b_d, nn));
+  F3R_TRY(w.alloc(&w.x_d, nn));
+  F3R_TRY(w.alloc(&w.r_d, nn));
+  F3R_TRY(w.alloc(&w.active, 1));
+  if (s.perm_d) {
+    F3R_TRY(w.alloc(&w.bp_d, nn));
+    F3R_TRY(w.alloc(&w.xp_d, nn));
+  }
+  // reduction scratch: partial sums of up to 8 blocks per SM, kMaxCols values per column
+  double *part = nullptr;
+  unsigned int *ticket = nullptr;
+  F3R_TRY(w.alloc(&part, (size_t)s.ctx->sm_count * 8 * kMaxCols * K + 64));
+  F3R_TRY(w.alloc(&ticket, 4));
+  CUDA_TRY(cudaMemset(ticket, 0, 4 * sizeof(unsigned int)));
+  w.gr = GridRed{part, ticket};
+  CUDA_TRY(cudaDeviceSynchronize());
+  return Engine<K>(s, w).prepare();
+}
+
+template <int K> Status Solver::work(Work<K> **out) {
+  std::unique_ptr<Work<K>> *slot = nullptr;
+  if constexpr (K == 2) slot = &w2;
+  if constexpr (K == 4) slot = &w4;
+  if constexpr (K == 8) slot = &w8;
+  if constexpr (K == 16) slot = &w16;
+  if (!*slot) {
+    auto wk = std::make_unique<Work<K>>();
+    F3R_TRY(make_work<K>(*this, *wk));
+    *slot = std::move(wk);
+  }
+  *out = slot->get();
+  return F3R_SUCCESS;
+}
+
+// Single solve: b, x host or device vectors of the original row order.
+Status Solver::solve(const double *b_user, double *x_user, f3r_cond_fn cond, void *user, f3r_result *res) {
+  const int64_t N = n;
+  cudaStream_t st = C().stream;
+  const int g = C().ew_grid(N);
+  auto is_dev = [&](const void *q) {
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, q) != cudaSuccess) {
+      cudaGetLastError();
+      return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+  };
+  const bool b_dev = is_dev(b_user), x_dev = is_dev(x_user);
+  // x is updated with 16-byte vector accesses: a device x that is not
+  // 16-byte aligned is worked on in an internal copy
+  const bool x_direct = x_dev && (reinterpret_cast<uintptr_t>(x_user) % 16 == 0);
+  Work<1> &w = w1;
+  const double *b = b_user;
+  double *x = x_user;
+  if (!b_dev) {
+    CUDA_TRY(cudaMemcpyAsync(w.b_d, b_user, sizeof(double) * N, cudaMemcpyHostToDevice, st));
+    b = w.b_d;
+  }
+  if (!x_direct) {
+    CUDA_TRY(cudaMemcpyAsync(w.x_d, x_user, sizeof(double) * N, x_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                             st));
+    x = w.x_d;
+  }
+  // permuted system (SELL-C-sigma order)
+  const double *bs = b;
+  double *xs = x;
+  if (perm_d) {
+    launch_k(C(), k_permute_gather, g, kEwThreads, 0, st, b, perm_d, w.bp_d, N);
+    launch_k(C(), k_permute_gather, g, kEwThreads, 0, st, x, perm_d, w.xp_d, N);
+    bs = w.bp_d;
+    xs = w.xp_d;
+  }
+  f3r_result out{};
+  F3R_TRY(Engine<1>(*this, w).solve_block(bs, xs, 1, cond, user, &out));
+  if (perm_d) launch_k(C(), k_permute_scatter, g, kEwThreads, 0, st, (const double *)xs, perm_d, x, N);
+  if (!x_direct)
+    CUDA_TRY(cudaMemcpyAsync(x_user, x, sizeof(double) * N, x_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                             st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  if (res) *res = out;
+  return F3R_SUCCESS;
+}
+
+// Several right-hand sides: blocks of up to 16 columns solved in lockstep
+// (the K-column engine, K the power of two at or above the block's width)
+// where the nest allows it, otherwise column by column.
+Status Solver::solve_multi(int32_t nrhs, const double *b, int64_t ldb, double *x, int64_t ldx, f3r_cond_fn cond,
+                           void *user, f3r_result *results) {
+  if (nrhs <= 1 || !block_ok()) {
+    for (int32_t k = 0; k < nrhs; k++) {
+      f3r_result r{};
+      F3R_TRY(solve(b + (size_t)k * ldb, x + (size_t)k * ldx, cond, user, &r));
+      if (results) results[k] = r;
+    }
+    return F3R_SUCCESS;
+  }
+  auto is_dev = [&](const void *q) {
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, q) != cudaSuccess) {
+      cudaGetLastError();
+      return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+  };
+  const bool b_dev = is_dev(b), x_dev = is_dev(x);
+  const int64_t N = n;
+  cudaStream_t st = C().stream;
+  const int g = C().ew_grid(N);
+  // host columns are staged through one device block of up to 16 columns
+  double *stage = nullptr;
+  if (!b_dev || !x_dev) CUDA_TRY(cudaMalloc((void **)&stage, sizeof(double) * (size_t)std::max<int64_t>(N, 1) * 16));
+  Status status = F3R_SUCCESS;
+  for (int32_t k0 = 0; k0 < nrhs && status == F3R_SUCCESS; k0 += 16) {
+    const int nc = std::min<int32_t>(16, nrhs - k0);
+    auto run = [&](auto kc) -> Status {
+      constexpr int K = decltype(kc)::value;
+      Work<K> *wk = nullptr;
+      F3R_TRY(work<K>(&wk));
+      Work<K> &w = *wk;
+      // b, x columns into the interleaved blocks (storage order)
+      double *bi = perm_d ? w.bp_d : w.b_d, *xi = perm_d ? w.xp_d : w.x_d;
+      const double *bsrc = b + (size_t)k0 * ldb;
+      double *xsrc = x + (size_t)k0 * ldx;
+      int64_t lb = ldb, lx = ldx;
+      if (!b_dev) {
+        for (int c = 0; c < nc; c++)
+          CUDA_TRY(cudaMemcpyAsync(stage + (size_t)c * N, bsrc + (size_t)c * ldb, sizeof(double) * N,
+                                   cudaMemcpyHostToDevice, st));
+        bsrc = stage;
+        lb = N;
+      }
+      launch_k(C(), k_interleave, g, kEwThreads, 0, st, bsrc, lb, nc, K, w.b_d, N);
+      if (!x_dev) {
+        for (int c = 0; c < nc; c++)
+          CUDA_TRY(cudaMemcpyAsync(stage + (size_t)c * N, xsrc + (size_t)c * ldx, sizeof(double) * N,
+                                   cudaMemcpyHostToDevice, st));
+        launch_k(C(), k_interleave, g, kEwThreads, 0, st, (const double *)stage, N, nc, K, w.x_d, N);
+      } else {
+        launch_k(C(), k_interleave, g, kEwThreads, 0, st, (const double *)xsrc, lx, nc, K, w.x_d, N);
+      }
+      if (perm_d) {
+        launch_k(C(), k_permute_gatherK<K>, g, kEwThreads, 0, st, (const double *)w.b_d, perm_d, bi, N);
+        launch_k(C(), k_permute_gatherK<K>, g, kEwThreads, 0, st, (const double *)w.x_d, perm_d, xi, N);
+      }
+      F3R_TRY(Engine<K>(*this, w).solve_block(bi, xi, nc, cond, user, results ? results + k0 : nullptr));
+      if (perm_d) launch_k(C(), k_permute_scatterK<K>, g, kEwThreads, 0, st, (const double *)xi, perm_d, w.x_d, N);
+      if (x_dev) {
+        launch_k(C(), k_deinterleave, g, kEwThreads, 0, st, (const double *)w.x_d, K, nc, xsrc, ldx, N);
+      } else {
+        launch_k(C(), k_deinterleave, g, kEwThreads, 0, st, (const double *)w.x_d, K, nc, stage, N, N);
+        for (int c = 0; c < nc; c++)
+          CUDA_TRY(cudaMemcpyAsync(xsrc + (size_t)c * ldx, stage + (size_t)c * N, sizeof(double) * N,
+                                   cudaMemcpyDeviceToHost, st));
+      }
+      CUDA_TRY(cudaStreamSynchronize(st));
+      return F3R_SUCCESS;
+    };
+    if (nc <= 2) status = run(std::integral_constant<int, 2>());
+    else if (nc <= 4) status = run(std::integral_constant<int, 4>());
+    else if (nc <= 8) status = run(std::integral_constant<int, 8>());
+    else status = run(std::integral_constant<int, 16>());
+  }
+  if (stage) {
+    cudaStreamSynchronize(st);
+    cudaFree(stage);
+  }
+  return status;
+}
 
 // Layout autotuner (f3r_params.sell_autotune): the fp16 copy of A is built in
 // every candidate layout and its fp16 x fp32 product timed on the context's
@@ -946,11 +1415,15 @@ static Status make_solver(f3r_context *ctx, const f3r_csr *a, const f3r_params *
       return fail(F3R_ERROR_INVALID_VALUE, "the factors must be square and of the matrix's size");
   }
   f3r_params p = *pp;
-  if (p.m_outer < 1 || p.m_outer + 1 > kMaxCols || p.m2 < 1 || p.m2 + 1 > kMaxCols || p.m3 < 0 ||
-      p.m3 + 1 > kMaxCols || p.m4 < 1 || p.m4 > kMaxM4 || p.c < 1 || p.max_restarts < 1 || p.static_weight < 0)
+  if (p.m_outer < 1 || p.m_outer + 1 > kMaxCols || p.m2 < 0 || p.m2 + 1 > kMaxCols || p.m3 < 0 ||
+      p.m3 + 1 > kMaxCols || p.half_m < 0 || p.half_m + 1 > kMaxCols || p.m4 < 1 || p.m4 > kMaxM4 || p.c < 1 ||
+      p.max_restarts < 1 || p.static_weight < 0)
     return fail(F3R_ERROR_INVALID_VALUE,
-                "need 1 <= m_outer, m2 <= 127, 0 <= m3 <= 127, 1 <= m4 <= 16, c >= 1, max_restarts >= 1, "
+                "need 1 <= m_outer <= 127, 0 <= m2, m3, half_m <= 127, 1 <= m4 <= 16, c >= 1, max_restarts >= 1, "
                 "static_weight >= 0");
+  if (p.m2 == 0 && (p.half_m == 0 || p.m3 > 0 || (p.inner_sstep & 3)))
+    return fail(F3R_ERROR_INVALID_VALUE,
+                "m2 = 0 (no fp32 level) needs half_m > 0, m3 = 0 and no s-step inner level");
   if (p.sell_c != 32) return fail(F3R_ERROR_UNSUPPORTED, "only SELL slice height 32 is implemented");
   if (p.format != F3R_FORMAT_SELL && p.format != F3R_FORMAT_CSR) return fail(F3R_ERROR_INVALID_VALUE, "unknown format");
   if (p.format == F3R_FORMAT_CSR && (p.sell_sigma != 1 || p.sell_align || p.sell_index16))
@@ -1077,50 +1550,21 @@ static Status make_solver(f3r_context *ctx, const f3r_csr *a, const f3r_params *
                           p.sell_sigma > 1 ? &hperm : nullptr));
     }
   }
-  // level storage
-  F3R_TRY(s->make_level(s->L1, p.m_outer, true));
-  F3R_TRY(s->make_level(s->L2, p.m2, true));
-  if (p.m3 > 0) F3R_TRY(s->make_level(s->L3, p.m3, false));
-  const size_t nn = (size_t)std::max(n, 1);
-  F3R_TRY(s->alloc(&s->abs_e, 1));
-  F3R_TRY(s->alloc(&s->hin, nn));
-  F3R_TRY(s->alloc(&s->hout, nn));
-  F3R_TRY(s->alloc(&s->hout2, nn));
-  F3R_TRY(s->alloc(&s->tmp, nn));
-  F3R_TRY(s->alloc(&s->tmp2, nn));
-  F3R_TRY(s->alloc(&s->hr, nn));
-  CUDA_TRY(cudaMemset(s->tmp2, 0, nn * sizeof(__half)));
-  F3R_TRY(s->alloc(&s->rs, 1));
-  F3R_TRY(s->alloc(&s->in_slot, 1));
-  F3R_TRY(s->alloc(&s->out_slot, 1));
-  F3R_TRY(s->alloc(&s->b_d, nn));
-  F3R_TRY(s->alloc(&s->x_d, nn));
-  F3R_TRY(s->alloc(&s->r_d, nn));
-  if (s->perm_d) {
-    F3R_TRY(s->alloc(&s->bp_d, nn));
-    F3R_TRY(s->alloc(&s->xp_d, nn));
-  }
   CUDA_TRY(cudaEventCreate(&s->ev0));
   CUDA_TRY(cudaEventCreate(&s->ev1));
-  // every SpMV instantiation the solve may launch, configured before capture
+  // every SpMV instantiation the single solve may launch, configured before capture
   Context &cx = *ctx;
-  F3R_TRY((sell_attr<double, double, EpiResidualNorm>(cx)));
   F3R_TRY((sell_attr<double, double, EpiStore<double>>(cx)));
   F3R_TRY((sell_attr<double, double, EpiResidual<double, double>>(cx)));
-  F3R_TRY((sell_attr<float, float, EpiStoreDots<4>>(cx)));
-  F3R_TRY((sell_attr<float, float, EpiStoreDots<8>>(cx)));
-  F3R_TRY((sell_attr<float, float, EpiStoreDots<kMaxDots>>(cx)));
-  F3R_TRY((sell_attr<__half, float, EpiStoreDots<4>>(cx)));
-  F3R_TRY((sell_attr<__half, float, EpiStoreDots<8>>(cx)));
-  F3R_TRY((sell_attr<__half, float, EpiStoreDots<kMaxDots>>(cx)));
   F3R_TRY((sell_attr<__half, __half, EpiRichStep>(cx)));
-  F3R_TRY((sell_attr<__half, __half, EpiRichWeight>(cx)));
   F3R_TRY((sell_attr<__half, __half, EpiRichResPre>(cx)));
   F3R_TRY((sell_attr<__half, __half, EpiResidual<__half, __half>>(cx)));
   F3R_TRY((sell_attr<__half, __half, EpiStore<__half>>(cx)));
   F3R_TRY((sell_attr<__half, float, EpiStore<float>>(cx)));
   F3R_TRY((sell_attr<float, float, EpiStore<float>>(cx)));
   F3R_TRY((sell_attr<__half, __half, EpiZScale>(cx)));
+  // the single-column workspace (wider ones are made by the first solve_multi that needs them)
+  F3R_TRY(make_work<1>(*s, s->w1));
   CUDA_TRY(cudaDeviceSynchronize());
   *out = s.release();
   return F3R_SUCCESS;
@@ -1135,6 +1579,11 @@ struct f3r_solver {
 namespace f3r {
 const void *solver_context(const f3r_solver *s) { return s && s->s ? (const void *)s->s->ctx : nullptr; }
 int32_t solver_rows(const f3r_solver *s) { return s && s->s ? s->s->n : 0; }
+Status solver_solve_multi(f3r_solver *s, int32_t nrhs, const double *b, int64_t ldb, double *x, int64_t ldx,
+                          f3r_cond_fn cond, void *user, f3r_result *results) {
+  CUDA_TRY(cudaSetDevice(s->s->ctx->device));
+  return s->s->solve_multi(nrhs, b, ldb, x, ldx, cond, user, results);
+}
 }  // namespace f3r
 
 // ===========================================================================

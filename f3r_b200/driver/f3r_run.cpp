@@ -10,18 +10,21 @@
 //   Problem,Method,Prec,M2,M3,M4,W,Precond,ACC,Time,Iter,ImplRes,ExplRes
 //
 //   Problem   the matrix argument without its last four characters
-//   Method    F3R | F3R-Static | F3 | F2
+//   Method    F3R | F3R-Static | F3 | F2 | F4 | F3H | F2H
 //   Prec      __half for F3R with SDAINV (the fp16 GPU build), _Float16 for
 //             the others (their CPU builds, work/Makefile:52-86)
 //   W         c for F3R, the weight for F3R-Static (static.cpp:121-125)
 //   Precond   SDAINV or BJILU0, then ACC as given on the command line
 //   Time      mean wall time of solver.solve over suite_iter solves, seconds
-//   Iter      sum(outer iterations) * m2 * m3 * m4 / suite_iter (integer)
+//   Iter      sum(outer iterations) * m2 * m3 * m4 / suite_iter (integer); for the depth
+//             ablations sum(outer iterations) * 64 / suite_iter (depth.cpp:185-186)
 //   ImplRes   |Givens residual estimate| / ||b||
 //   ExplRes   ||b - A x|| / ||b|| in fp64
 //
 // options:
-//   --method F3R|F3R-Static|F3|F2   default F3R; F3R-Static reads [weight]
+//   --method F3R|F3R-Static|F3|F2|F4|F3H|F2H
+//                                   default F3R; F3R-Static reads [weight]; F3 / F2 and the
+//                                   fp16-vector F4 / F3H / F2H are depth.cpp's fixed nests
 //   --precond SDAINV|BJILU0         default SDAINV for F3R (f3r-gpu.cpp:74),
 //                                   BJILU0 for the others (static.cpp:57-58)
 //   --blocks N                      block-Jacobi blocks, default 112
@@ -53,7 +56,7 @@ namespace {
 
 int usage(const char *msg) {
   std::fprintf(stderr,
-               "%s\nusage: f3r-run [--method F3R|F3R-Static|F3|F2] [--precond SDAINV|BJILU0] [--blocks N] "
+               "%s\nusage: f3r-run [--method F3R|F3R-Static|F3|F2|F4|F3H|F2H] [--precond SDAINV|BJILU0] [--blocks N] "
                "[--format SELL|CSR|AUTO] [--tol EPS] [--header] <matrix.mtx> <acc> <suite_iter> <m2> <m3> <m4> <c> "
                "<restart> [weight]\n",
                msg);
@@ -116,7 +119,9 @@ int main(int argc, char **argv) {
     }
   }
   const bool is_static = method == "F3R-Static";
-  if (method != "F3R" && !is_static && method != "F3" && method != "F2") return usage("unknown method");
+  const bool is_depth =
+      method == "F3" || method == "F2" || method == "F4" || method == "F3H" || method == "F2H";
+  if (method != "F3R" && !is_static && !is_depth) return usage("unknown method");
   if (pos.size() < 8 + (is_static ? 1u : 0u)) return usage("missing arguments");
   if (precond.empty()) precond = method == "F3R" ? "SDAINV" : "BJILU0";
   if (precond != "SDAINV" && precond != "BJILU0") return usage("unknown preconditioner");
@@ -152,11 +157,15 @@ int main(int argc, char **argv) {
     if (format == "AUTO") p.sell_autotune = 1;
     const bool gpu_build = method == "F3R" && precond == "SDAINV";  // the f3r16-gpu.exe configuration
     p.max_restarts = gpu_build ? 20 : restart;
-    if (method == "F3" || method == "F2") {
-      // depth.cpp:131-162: FGMRES(8) over FGMRES(8) over M, or FGMRES(64)
-      // over M, M the plain preconditioner (one step of weight 1)
-      p.m2 = method == "F3" ? 8 : 64;
-      p.m3 = method == "F3" ? 8 : 0;
+    if (is_depth) {
+      // depth.cpp:122-167, M the plain preconditioner (one step of weight 1):
+      //   F3  fp32 (A32, 8) / fp32 (A16, 8) / M      F2  fp32 (A32, 64) / M
+      //   F4  fp32 (A32, 8) / fp32 (A16, 4) / fp16 vectors (A16, 2) / M
+      //   F3H fp32 (A32, 8) / fp16 vectors (A16, 8) / M
+      //   F2H fp16 vectors (A16, 64) / M
+      p.m2 = method == "F2" ? 64 : method == "F2H" ? 0 : 8;
+      p.m3 = method == "F3" ? 8 : method == "F4" ? 4 : 0;
+      p.half_m = method == "F4" ? 2 : method == "F3H" ? 8 : method == "F2H" ? 64 : 0;
       p.m4 = 1;
       p.static_weight = 1.0;
     } else {
@@ -202,7 +211,8 @@ int main(int argc, char **argv) {
     std::printf("%s,%s,%s,%d,%d,%d,%s,%s,%s,", name.c_str(), method.c_str(), gpu_build ? "__half" : "_Float16",
                 m2, m3, m4, w.str().c_str(), precond.c_str(), arg_acc.c_str());
     std::printf("%e,", seconds / suite_iter);
-    std::printf("%d,%e,", (int)(itr_sum * m2 * m3 * m4 / suite_iter), flag.res_nrm2 / nrm_b);
+    const long long ww = is_depth ? 64 : (long long)m2 * m3 * m4;  // the test() lambda's ww
+    std::printf("%d,%e,", (int)(itr_sum * ww / suite_iter), flag.res_nrm2 / nrm_b);
     std::printf("%e\n", detail.expl_rel_res);
   } catch (const f3r::error &e) {
     std::fprintf(stderr, "f3r-run: %s\n", e.what());

@@ -118,7 +118,16 @@ typedef struct f3r_params {
                               product on it, and solve in the fastest; the layout fields above are
                               then ignored (f3r_solver_info reports the choice).  All give the same
                               sums at sigma 1; sigma 256 permutes the rows.  0 */
-  int32_t reserved[7];
+  int32_t half_m;          /* > 0: an FGMRES level whose basis vectors V and Z are stored in fp16
+                              (FGMRES<_Float16> of work/src/depth.cpp:122-167), half_m Arnoldi steps,
+                              directly above R: called by level 3, by level 2 when m3 = 0, or by the
+                              outer level when m2 = 0 (m2 = 0 is allowed only with half_m > 0).  Its
+                              products are fp16 x fp16 with fp32 accumulation, its dots, norms,
+                              Hessenberg and Givens rotations fp32 (the reference computes them in
+                              fp16), R's input and output its fp16 vectors.  The paper's F4 is m2 8,
+                              m3 4, half_m 2; F3H m2 8, m3 0, half_m 8; F2H m2 0, half_m 64; each with
+                              m4 1, static_weight 1 and block-Jacobi ILU(0).  0 */
+  int32_t reserved[6];
 } f3r_params;
 
 /* Solve outcome.  The first three fields are solve_res_t

@@ -702,7 +702,9 @@ typedef struct {
   int32_t pad_;
   double trsv_omega;   /* PRECOND_ILU0_JACOBI: damping omega */
   int32_t sstep;       /* bit 0: level 2 is sFGMRES, bit 1: level 3 (solver/gmres2.hpp:137-221) */
-  int32_t pad2_;
+  int32_t half_m;      /* > 0: an FGMRES level with fp16 vectors of half_m steps directly above R
+                          (FGMRES<_Float16>, work/src/depth.cpp:122-167); m2 = 0: the outer level
+                          calls it directly */
 } or_f3r_params;
 
 #define MAXM4 16
@@ -785,15 +787,14 @@ static float dot16(int32_t n, const f16 *a, const f16 *b) {
   return tot;
 }
 
-/* Level 4: the adaptive-weight Richardson operator R (f3r-gpu.cpp:229-260) */
-static void level4(f3r_ctx *c, const float *in, float *out) {
+/* Level 4: the adaptive-weight Richardson operator R (f3r-gpu.cpp:229-260),
+ * on R's fp16 input c->hin; the result is left in c->hout.                 */
+static void level4_core(f3r_ctx *c) {
   int32_t n = c->n;
   int ref = (c->p.arith == ARITH_REF);
-  float sc = ldexpf(1.0f, c->p.half_scale_log2), isc = ldexpf(1.0f, -c->p.half_scale_log2);
   c->r_calls++;
   ++c->cnt;
   int upd = (c->p.static_weight <= 0) && (c->cnt % c->p.c == 0);
-  for (int32_t i = 0; i < n; i++) c->hin[i] = (f16)(in[i] * sc);
   prec_apply(c, c->hin, c->hout, c->tmp);
   if (upd) {
     spmv16(c, c->hout, c->tmp, NULL);
@@ -827,7 +828,148 @@ static void level4(f3r_ctx *c, const float *in, float *out) {
       }
     }
   }
-  for (int32_t i = 0; i < n; i++) out[i] = (float)c->hout[i] * isc;
+}
+
+static void givens_f(float *cs, float *sn, float *H, float *e, int j);
+static void trsv_f(const float *U, const float *b, float *x, int h, int w);
+
+/* R below an fp32 level: fp32 in, hin = fp16(in * sc) (f3r-gpu.cpp:231),
+ * out = fp32(hout) / sc (f3r-gpu.cpp:259)                                  */
+static void level4(f3r_ctx *c, const float *in, float *out) {
+  float sc = ldexpf(1.0f, c->p.half_scale_log2), isc = ldexpf(1.0f, -c->p.half_scale_log2);
+  for (int32_t i = 0; i < c->n; i++) c->hin[i] = (f16)(in[i] * sc);
+  level4_core(c);
+  for (int32_t i = 0; i < c->n; i++) out[i] = (float)c->hout[i] * isc;
+}
+
+/* R below the fp16-vector level: its fp16 vectors in and out directly      */
+static void level4_h(f3r_ctx *c, const f16 *in, f16 *out) {
+  memcpy(c->hin, in, sizeof(f16) * (size_t)c->n);
+  level4_core(c);
+  memcpy(out, c->hout, sizeof(f16) * (size_t)c->n);
+}
+
+/* fp16 arithmetic of the reference's FGMRES<_Float16> scalars and vectors,
+ * one rounding per operation (ARITH_REF)                                   */
+static inline f16 hmul(f16 a, f16 b) { return (f16)((float)a * (float)b); }
+static inline f16 hadd(f16 a, f16 b) { return (f16)((float)a + (float)b); }
+static inline f16 hsub(f16 a, f16 b) { return (f16)((float)a - (float)b); }
+static inline f16 hdiv(f16 a, f16 b) { return (f16)((float)a / (float)b); }
+/* dot(a, b) with an _Float16 partial sum, one thread (tensor.hpp:509-537,
+ * loop.hpp exec<host>::para_reduce)                                        */
+static f16 hdot(int32_t n, const f16 *a, const f16 *b) {
+  f16 s = (f16)0.0f;
+  for (int32_t i = 0; i < n; i++) s = hadd(s, hmul(a[i], b[i]));
+  return s;
+}
+
+/* FGMRES<_Float16> in the reference's arithmetic: dots and norms summed in
+ * fp16, V(j+1) -= V H(j) in fp16 (MULMV, tensor.hpp:605-623), H, Givens and
+ * the back substitution in fp16 (gmres2.hpp:14-53, sqrt through float as the
+ * depth driver defines it, depth.cpp:26-31), x = Z y in fp16.             */
+static void level_half_ref(f3r_ctx *c, const float *in32, const double *in64, float *out32, double *out64) {
+  int32_t n = c->n;
+  int m = c->p.half_m;
+  f16 *V = (f16 *)malloc(sizeof(f16) * (size_t)n * (m + 1));
+  f16 *Z = (f16 *)malloc(sizeof(f16) * (size_t)n * m);
+  f16 *H = (f16 *)calloc((size_t)(m + 1) * m, sizeof(f16));
+  f16 cs[128], sn[128], e[129], y[128];
+  for (int k = 0; k < 129; k++) e[k] = (f16)0.0f;
+  e[0] = (f16)1.0f;
+  for (int32_t i = 0; i < n; i++) V[i] = in32 ? (f16)in32[i] : (f16)in64[i];
+  for (int j = 0; j < m; j++) {
+    f16 *vj = V + (size_t)n * j, *zj = Z + (size_t)n * j, *w = V + (size_t)n * (j + 1);
+    level4_h(c, vj, zj);
+    spmv16(c, zj, w, NULL);
+    f16 *Hj = H + (size_t)(m + 1) * j;
+    for (int k = 0; k <= j; k++) Hj[k] = hdot(n, w, V + (size_t)n * k);
+    for (int32_t i = 0; i < n; i++) {
+      f16 r = hmul(V[i], Hj[0]);
+      for (int k = 1; k <= j; k++) r = hadd(r, hmul(V[(size_t)n * k + i], Hj[k]));
+      w[i] = hsub(w[i], r);
+    }
+    f16 nr = (f16)sqrtf((float)hdot(n, w, w));
+    Hj[j + 1] = nr;
+    f16 inv = (f16)(1.0 / (double)nr);
+    for (int32_t i = 0; i < n; i++) w[i] = hmul(inv, w[i]);
+    for (int i = 0; i < j; i++) {
+      f16 t = Hj[i];
+      Hj[i] = hadd(hmul(cs[i], t), hmul(sn[i], Hj[i + 1]));
+      Hj[i + 1] = hadd(hmul((f16)(-(float)sn[i]), t), hmul(cs[i], Hj[i + 1]));
+    }
+    f16 t = (f16)sqrtf((float)hadd(hmul(Hj[j], Hj[j]), hmul(Hj[j + 1], Hj[j + 1])));
+    cs[j] = hdiv(Hj[j], t);
+    sn[j] = hdiv(Hj[j + 1], t);
+    Hj[j] = t;
+    Hj[j + 1] = (f16)0.0f;
+    e[j + 1] = hmul((f16)(-(float)sn[j]), e[j]);
+    e[j] = hmul(cs[j], e[j]);
+  }
+  for (int i = m - 1; i >= 0; i--) {
+    f16 t = e[i];
+    for (int q = m - 1; q > i; q--) t = hsub(t, hmul(H[(size_t)q * (m + 1) + i], y[q]));
+    y[i] = hdiv(t, H[(size_t)i * (m + 1) + i]);
+  }
+  for (int32_t i = 0; i < n; i++) {
+    f16 r = hmul(Z[i], y[0]);
+    for (int k = 1; k < m; k++) r = hadd(r, hmul(Z[(size_t)n * k + i], y[k]));
+    if (out32) out32[i] = (float)r;
+    else out64[i] = (double)r;
+  }
+  free(V); free(Z); free(H);
+}
+
+/* The fp16-vector level FGMRES<_Float16>::kernel<true> (gmres.hpp:96-134
+ * with normalize=false; instantiated at work/src/depth.cpp:122-167): V and
+ * Z stored in fp16; the product's arithmetic computes w = A16 z with fp32
+ * accumulation, every dot, norm and Gram-Schmidt update in fp32 (rounded
+ * once when stored), H and the Givens rotations in fp32.  in32 / in64: the
+ * calling level's vector (fp32 inner level, or the fp64 outer level when
+ * m2 = 0); the result goes to out32 or out64.  ARITH_REF: level_half_ref.  */
+static void level_half(f3r_ctx *c, const float *in32, const double *in64, float *out32, double *out64) {
+  if (c->p.arith == ARITH_REF) {
+    level_half_ref(c, in32, in64, out32, out64);
+    return;
+  }
+  int32_t n = c->n;
+  int m = c->p.half_m;
+  f16 *V = (f16 *)malloc(sizeof(f16) * (size_t)n * (m + 1));
+  f16 *Z = (f16 *)malloc(sizeof(f16) * (size_t)n * m);
+  float *H = (float *)calloc((size_t)(m + 1) * m, sizeof(float));
+  float *w32 = (float *)malloc(sizeof(float) * (size_t)n);
+  float cs[128], sn[128], e[129], y[128];
+  memset(e, 0, sizeof(e));
+  e[0] = 1.0f;
+  for (int32_t i = 0; i < n; i++) V[i] = in32 ? (f16)in32[i] : (f16)in64[i];
+  const or_mat *A = c->A;
+  for (int j = 0; j < m; j++) {
+    f16 *vj = V + (size_t)n * j, *zj = Z + (size_t)n * j, *w = V + (size_t)n * (j + 1);
+    level4_h(c, vj, zj);
+    spmv16(c, zj, w, NULL);
+    float *Hj = H + (size_t)(m + 1) * j;
+    for (int k = 0; k <= j; k++) Hj[k] = dot16(n, w, V + (size_t)n * k);
+    float nn = 0.0f;
+    for (int32_t i = 0; i < n; i++) {
+      float r = (float)V[i] * Hj[0];
+      for (int k = 1; k <= j; k++) r = fmaf((float)V[(size_t)n * k + i], Hj[k], r);
+      w[i] = (f16)((float)w[i] - r);
+      w32[i] = (float)w[i];
+    }
+    nn = dotf(n, w32, w32);
+    float nr = sqrtf(nn);
+    Hj[j + 1] = nr;
+    float inv = 1.0f / nr;
+    for (int32_t i = 0; i < n; i++) w[i] = (f16)((float)w[i] * inv);
+    givens_f(cs, sn, Hj, e, j);
+  }
+  trsv_f(H, e, y, m + 1, m);
+  for (int32_t i = 0; i < n; i++) {
+    float r = (float)Z[i] * y[0];
+    for (int k = 1; k < m; k++) r = fmaf((float)Z[(size_t)n * k + i], y[k], r);
+    if (out32) out32[i] = r;
+    else out64[i] = (double)r;
+  }
+  free(V); free(Z); free(H); free(w32);
 }
 
 /* Givens update of Hessenberg column j (gmres.hpp:24-38) and residual
@@ -887,6 +1029,7 @@ static void level_inner(f3r_ctx *c, int level, const float *in, float *out) {
     float *vj = V + (size_t)n * j, *zj = Z + (size_t)n * j, *w = V + (size_t)n * (j + 1);
     if (!sstep || pass == 0) {
       if (level == 2 && c->p.m3 > 0) level_inner(c, 3, vj, zj);
+      else if (c->p.half_m > 0) level_half(c, vj, NULL, zj, NULL);  /* the fp16-vector level (depth.cpp) */
       else level4(c, vj, zj);  /* level 3, or level 2 of the depth-2 form (work/src/depth.cpp:157-162) */
       for (int32_t i = 0; i < n; i++) {
         float t = 0.0f;
@@ -930,7 +1073,9 @@ int or_f3r_solve(const or_mat *A, const or_mat *P1, const or_mat *P2, const doub
   memset(&c, 0, sizeof(c));
   int32_t n = A->n;
   c.n = n; c.A = A; c.P1 = P1; c.P2 = P2; c.p = *p;
-  if (p->m2 > 127 || p->m3 > 127 || p->m3 < 0 || p->m4 > MAXM4 || p->m1 > 4096) return -1;
+  if (p->m2 > 127 || p->m3 > 127 || p->m3 < 0 || p->m4 > MAXM4 || p->m1 > 4096 || p->half_m < 0 ||
+      p->half_m > 127 || (p->m2 == 0 && p->half_m == 0))
+    return -1;
   c.v32 = (float *)malloc(sizeof(float) * (size_t)A->nnz);
   c.v16 = (f16 *)malloc(sizeof(f16) * (size_t)A->nnz);
   for (int32_t q = 0; q < A->nnz; q++) { c.v32[q] = (float)A->val[q]; c.v16[q] = (f16)A->val[q]; }
@@ -969,9 +1114,13 @@ int or_f3r_solve(const or_mat *A, const or_mat *P1, const or_mat *P2, const doub
     int j = 0;
     for (; j < m; j++) {
       double *vj = V + (size_t)n * j, *zj = Z + (size_t)n * j, *w = V + (size_t)n * (j + 1);
-      for (int32_t i = 0; i < n; i++) in32[i] = (float)vj[i];
-      level_inner(&c, 2, in32, out32);
-      for (int32_t i = 0; i < n; i++) zj[i] = (double)out32[i];
+      if (p->m2 > 0) {
+        for (int32_t i = 0; i < n; i++) in32[i] = (float)vj[i];
+        level_inner(&c, 2, in32, out32);
+        for (int32_t i = 0; i < n; i++) zj[i] = (double)out32[i];
+      } else {
+        level_half(&c, NULL, vj, NULL, zj);  /* F2H: the fp16-vector level under the outer level */
+      }
       or_spmv(n, A->rptr, A->idx, A->val, DT_F64, zj, DT_F64, w, DT_F64, DT_F64, 0, NULL, DT_F64);
       double *Hj = H + (size_t)(m + 1) * j;
       for (int k = 0; k <= j; k++) Hj[k] = dotd(n, w, V + (size_t)n * k);

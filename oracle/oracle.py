@@ -33,12 +33,16 @@ _f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
 _u16p = np.ctypeslib.ndpointer(np.uint16, flags="C_CONTIGUOUS")
 
 
+# The read-only reference checkout the _ref targets compile from (the Makefile's REF).
+REF_TREE = os.environ.get("F3R_REF", "/root/reference")
+
+
 def build() -> None:
     """Compile liboracle.so (and oracle/_ref when the reference tree exists)."""
     targets = ["liboracle.so"]
-    if os.path.isdir("/root/reference/library"):
+    if os.path.isdir(os.path.join(REF_TREE, "library")):
         targets.append("ref")
-    subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
+    subprocess.run(["make", "-s", "-C", HERE, f"REF={REF_TREE}"] + targets, check=True)
 
 
 _lib = None
@@ -95,13 +99,14 @@ class F3RParams(C.Structure):
                 ("m4", C.c_int32), ("c", C.c_int32), ("precond", C.c_int32), ("arith", C.c_int32),
                 ("half_scale_log2", C.c_int32), ("tol", C.c_double), ("static_weight", C.c_double),
                 ("trsv_iters", C.c_int32), ("pad_", C.c_int32), ("trsv_omega", C.c_double),
-                ("sstep", C.c_int32), ("pad2_", C.c_int32)]
+                ("sstep", C.c_int32), ("half_m", C.c_int32)]
 
 
 def params(m1=100, restarts=20, m2=8, m3=4, m4=2, c=64, precond=PRECOND_SDAINV, arith=ARITH_PRODUCT,
-           half_scale_log2=0, tol=1e-10, static_weight=0.0, trsv_iters=2, trsv_omega=1.0, sstep=0) -> F3RParams:
+           half_scale_log2=0, tol=1e-10, static_weight=0.0, trsv_iters=2, trsv_omega=1.0, sstep=0,
+           half_m=0) -> F3RParams:
     return F3RParams(m1, restarts, m2, m3, m4, c, precond, arith, half_scale_log2, tol, static_weight, trsv_iters,
-                     0, trsv_omega, sstep, 0)
+                     0, trsv_omega, sstep, half_m)
 
 
 class Mat:
@@ -453,6 +458,30 @@ class Ref:
         nh = self.L.ref_f3r_solve(config, n, len(idx), rptr, idx, np.ascontiguousarray(val, np.float64),
                                   np.ascontiguousarray(b, np.float64), x, m2, m3, m4, c, restarts, tol, acc,
                                   sdainv_tol, blocks, out, hist, hist_cap, stop_after, weight)
+        return dict(x=x, time_s=out[0], iters=int(out[1]), impl_res=out[2], expl_res=out[3],
+                    solved=bool(out[4]), hist=hist[:min(nh, hist_cap)].copy())
+
+    def f3r_solve_depth_half(self, variant, rptr, idx, val, b, restarts=20, tol=1e-10, acc=1.0, blocks=112,
+                             hist_cap=4096):
+        """the depth ablations with an fp16-vector innermost FGMRES level over
+        block-Jacobi ILU(0) (work/src/depth.cpp): variant 0 F4, 1 F3H, 2 F2H"""
+        if getattr(self, "D", None) is None:
+            path = os.path.join(REF_DIR, "libf3r_ref_depth.so")
+            if not os.path.exists(path):
+                raise FileNotFoundError(f"{path} missing: run `make -C oracle ref` where the reference tree exists")
+            self.D = C.CDLL(path)
+            self.D.ref_f3r_solve_depth_half.restype = C.c_int
+            self.D.ref_f3r_solve_depth_half.argtypes = [C.c_int, C.c_int32, C.c_int32, _i32p, _i32p, _f64p, _f64p,
+                                                        _f64p, C.c_int, C.c_double, C.c_double, C.c_int, _f64p, _f64p,
+                                                        C.c_int]
+        n = len(rptr) - 1
+        x = np.zeros(n)
+        out = np.zeros(5)
+        hist = np.zeros(hist_cap)
+        nh = self.D.ref_f3r_solve_depth_half(variant, n, len(idx), np.ascontiguousarray(rptr, np.int32),
+                                             np.ascontiguousarray(idx, np.int32), np.ascontiguousarray(val, np.float64),
+                                             np.ascontiguousarray(b, np.float64), x, restarts, tol, acc, blocks, out,
+                                             hist, hist_cap)
         return dict(x=x, time_s=out[0], iters=int(out[1]), impl_res=out[2], expl_res=out[3],
                     solved=bool(out[4]), hist=hist[:min(nh, hist_cap)].copy())
 

@@ -22,8 +22,13 @@ contraction, one OpenMP thread), and records its outputs:
 
 Usage (needs the reference tree; the fixtures are committed):
     OMP_NUM_THREADS=1 python tests/golden/gen_golden.py [--big]
+    python tests/golden/gen_golden.py --envelope [--big] [--only=name,name]
 --big adds the 64^3 CPU configuration and the 192^3 GPU configuration solve
-(about a minute of CPU each).
+(about a minute of CPU each).  --envelope re-runs every golden solve at 1, 2,
+3, 4 and 8 OpenMP threads (up to 64 for the fp16-vector depth ablations) and
+stores the reference's residual histories as <name>_env, the thread counts as
+<name>_env_threads: the spread the reference shows when only its summation
+order changes.
 """
 from __future__ import annotations
 
@@ -156,6 +161,93 @@ def trsv_fixtures(ref, s):
     np.savez_compressed(os.path.join(HERE, "trsv.npz"), **t)
 
 
+# F3R-Static (static.cpp) and the fp32 depth ablations (depth.cpp), BJ-ILU(0)
+VARIANTS = {"static_hpgmp16": dict(config=2, m2=8, m3=4, m4=2, weight=1.2),
+            "depth3_hpgmp16": dict(config=3, m2=8, m3=8, m4=1, weight=1.0),
+            "depth2_hpgmp16": dict(config=4, m2=64, m3=0, m4=1, weight=1.0)}
+# 7-point log-normal diffusion systems: (nx, sigma, correlation length, field seed).  diffs25_48 is the
+# precision-stress configuration (sigma 2.5, correlation length 8) at 48^3
+DIFFUSION = {"sdainv_diff12": (12, 1.5, 3.0, 9), "sdainv_diffs25_48": (48, 2.5, 8.0, 3)}
+# the depth ablations with an fp16-vector innermost FGMRES level (depth.cpp F4, F3H, F2H), BJ-ILU(0)
+DEPTH_HALF = {"f4_hpgmp16": 0, "f3h_hpgmp16": 1, "f2h_hpgmp16": 2}
+# OpenMP thread counts of the envelope: each changes only the summation order of the reference's reductions.
+# The fp16-vector levels accumulate their dot products and norms in fp16, one partial sum per thread, so
+# their accuracy grows with the thread count: their envelope reaches 64 threads.
+ENV_THREADS = (1, 2, 3, 4, 8)
+ENV_THREADS_WIDE = (1, 2, 3, 4, 8, 16, 32, 64)
+
+
+def solve_cases(big):
+    """(name, config, stencil spec or None for DIFFUSION, rhs seed) of every golden solve"""
+    cases = [("sdainv_hpgmp16", 0, (16, 16, 16, 1), 0), ("sdainv_half16", 0, (16, 16, 16, 2), 1),
+             ("sdainv_diff12", 0, None, 2), ("bjilu_hpcg16", 1, (16, 16, 16, 0), 3),
+             ("sdainv_diffs25_48", 0, None, 16)]
+    if big:
+        cases += [("bjilu_hpcg64", 1, (64, 64, 64, 0), 4), ("sdainv_half192", 0, (192, 192, 192, 2), 5)]
+    cases += [(k, v["config"], (16, 16, 16, 1), 6 + j) for j, (k, v) in enumerate(VARIANTS.items())]
+    # sFGMRES inner levels (solver/gmres2.hpp:137-221): mask bit 0 level 2, bit 1 level 3
+    cases += [(f"sstep{mask}_hpgmp16", 10 + mask, (16, 16, 16, 1), 12 + mask) for mask in (1, 2, 3)]
+    cases += [(name, 20 + v, (16, 16, 16, 1), 17 + v) for name, v in DEPTH_HALF.items()]
+    return cases
+
+
+def case_system(ref, name, spec):
+    """the scaled matrix of a golden solve"""
+    import f3r_b200 as F  # host-side generator only (no GPU needed)
+    if spec is None:
+        nx, sg, cl, fs = DIFFUSION[name]
+        rr, ii, vv = F.diffusion7(nx, nx, nx, sg, cl, fs).arrays()
+    else:
+        rr, ii, vv = ref.gen27(*spec[:3], variant=spec[3], beta=0.5)
+    return rr, ii, ref.scaling(rr, ii, vv)
+
+
+def case_blocks(spec):
+    return 16 if spec is not None and spec[0] == 16 else 112
+
+
+def run_case(ref, name, config, spec, seed):
+    rr, ii, vv = case_system(ref, name, spec)
+    xs, b = rhs_for(ref, rr, ii, vv, seed)
+    extra = {k: v for k, v in VARIANTS.get(name, {}).items() if k != "config"}
+    if config >= 20:
+        return ref.f3r_solve_depth_half(config - 20, rr, ii, vv, b, tol=1e-10, blocks=case_blocks(spec))
+    if config >= 10:
+        return ref.f3r_solve_sstep(config - 10, rr, ii, vv, b, tol=1e-10, c=8)
+    big = len(rr) - 1 >= 48 ** 3
+    return ref.f3r_solve(config, rr, ii, vv, b, tol=1e-10, c=64 if big else 8, blocks=case_blocks(spec), **extra)
+
+
+def envelope(big, only=None):
+    """The reference's residual history of every golden solve at each thread
+    count of ENV_THREADS, stored as <name>_env (rows: thread counts, NaN past a
+    run's last step).  The reference is not reproducible across thread counts
+    (OpenMP reductions), so its own spread bounds what any reimplementation can
+    match step by step."""
+    import ctypes
+    gomp = ctypes.CDLL("libgomp.so.1")
+    ref = O.Ref("golden")
+    path = os.path.join(HERE, "solves.npz")
+    sol = dict(np.load(path))
+    for name, config, spec, seed in solve_cases(big):
+        if only and name not in only:
+            continue
+        hs = []
+        threads = ENV_THREADS_WIDE if name in DEPTH_HALF else ENV_THREADS
+        for t in threads:
+            gomp.omp_set_num_threads(t)
+            hs.append(run_case(ref, name, config, spec, seed)["hist"])
+        w = max(len(h) for h in hs)
+        env = np.full((len(hs), w), np.nan)
+        for k, h in enumerate(hs):
+            env[k, :len(h)] = h
+        sol[name + "_env"] = env
+        sol[name + "_env_threads"] = np.array(threads)
+        print(name, [len(h) for h in hs])
+    gomp.omp_set_num_threads(1)
+    np.savez_compressed(path, **sol)
+
+
 def main(big: bool):
     O.build()
     ref = O.Ref("golden")
@@ -226,32 +318,10 @@ def main(big: bool):
 
     # ---- solves --------------------------------------------------------------
     sol = {}
-    cases = [("sdainv_hpgmp16", 0, (16, 16, 16, 1), 0), ("sdainv_half16", 0, (16, 16, 16, 2), 1),
-             ("sdainv_diff12", 0, None, 2), ("bjilu_hpcg16", 1, (16, 16, 16, 0), 3)]
-    if big:
-        cases += [("bjilu_hpcg64", 1, (64, 64, 64, 0), 4), ("sdainv_half192", 0, (192, 192, 192, 2), 5)]
-    # F3R-Static (static.cpp) and the fp32 depth ablations (depth.cpp), BJ-ILU(0)
-    variants = {"static_hpgmp16": dict(config=2, m2=8, m3=4, m4=2, weight=1.2),
-                "depth3_hpgmp16": dict(config=3, m2=8, m3=8, m4=1, weight=1.0),
-                "depth2_hpgmp16": dict(config=4, m2=64, m3=0, m4=1, weight=1.0)}
-    cases += [(k, v["config"], (16, 16, 16, 1), 6 + j) for j, (k, v) in enumerate(variants.items())]
-    # sFGMRES inner levels (solver/gmres2.hpp:137-221): mask bit 0 level 2, bit 1 level 3
-    cases += [(f"sstep{mask}_hpgmp16", 10 + mask, (16, 16, 16, 1), 12 + mask) for mask in (1, 2, 3)]
-    for name, config, spec, seed in cases:
-        if spec is None:
-            D = F.diffusion7(12, 12, 12, 1.5, 3.0, 9)
-            rr, ii, vv = D.arrays()
-        else:
-            rr, ii, vv = ref.gen27(*spec[:3], variant=spec[3], beta=0.5)
-        vv = ref.scaling(rr, ii, vv)
-        xs, b = rhs_for(ref, rr, ii, vv, seed)
-        blocks = 16 if spec is not None and spec[0] == 16 else 112
-        extra = {k: v for k, v in variants.get(name, {}).items() if k != "config"}
-        if config >= 10:
-            res = ref.f3r_solve_sstep(config - 10, rr, ii, vv, b, tol=1e-10, c=8)
-        else:
-            res = ref.f3r_solve(config, rr, ii, vv, b, tol=1e-10, c=64 if spec and spec[0] >= 64 else 8,
-                                blocks=blocks, **extra)
+    for name, config, spec, seed in solve_cases(big):
+        res = run_case(ref, name, config, spec, seed)
+        rr = case_system(ref, name, spec)[0]
+        blocks = case_blocks(spec)
         print(name, res["iters"], res["impl_res"], res["expl_res"], res["time_s"])
         sol[name + "_iters"] = np.array(res["iters"])
         sol[name + "_hist"] = res["hist"]
@@ -270,4 +340,8 @@ def main(big: bool):
 
 
 if __name__ == "__main__":
-    main("--big" in sys.argv)
+    if "--envelope" in sys.argv:
+        sel = [a.split("=", 1)[1].split(",") for a in sys.argv if a.startswith("--only=")]
+        envelope("--big" in sys.argv, sel[0] if sel else None)
+    else:
+        main("--big" in sys.argv)

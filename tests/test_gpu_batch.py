@@ -64,3 +64,78 @@ def test_batch_equals_single_solves():
             xk, rk = single(S, B[k].copy())
             assert np.array_equal(X[k], xk)
             assert res[k].is_solved and res[k].expl_rel_res < 1e-10 and res[k].res_iter == rk.res_iter
+
+
+def _check_block(S, B, X0=None):
+    """solve_multi of B's rows (K columns in lockstep) against one single solve
+    per row: the same iterate bit for bit and the same step count"""
+    X = np.zeros_like(B) if X0 is None else X0.copy()
+    res = S.solve_multi(B, X)
+    for k in range(B.shape[0]):
+        xk = np.zeros(B.shape[1]) if X0 is None else X0[k].copy()
+        rk = S.solve(B[k].copy(), xk)
+        assert np.array_equal(X[k], xk), k
+        assert res[k].res_iter == rk.res_iter and res[k].is_solved == rk.is_solved, (k, res[k], rk)
+        assert res[k].restarts == rk.restarts and res[k].expl_rel_res == rk.expl_rel_res, k
+    return res
+
+
+@pytest.mark.parametrize("nrhs", [2, 5, 8, 16, 19])
+@pytest.mark.parametrize("layout", [dict(sell_align=1), dict(sell_align=0), dict(sell_sigma=256)])
+def test_block_solve_columns_bit_identical(nrhs, layout):
+    """up to 16 right-hand sides per lockstep block (block SELL products over
+    interleaved columns; padding columns inactive), 19 = 16 + 3 in two
+    blocks: every column is its single solve, bit for bit"""
+    ctx = F.Context(0)
+    A = F.stencil27(18, 17, 16, 2, 0.5).scale()
+    S = F.Solver(ctx, A, rel_tol=1e-10, c=4, **layout)
+    B = np.ascontiguousarray(np.random.default_rng(nrhs).standard_normal((nrhs, A.shape[0])))
+    res = _check_block(S, B)
+    assert all(r.is_solved and r.expl_rel_res < 1e-10 for r in res)
+
+
+def test_block_solve_general_sdainv_and_uneven_convergence():
+    """non-diagonal SDAINV factors (block products of W^T and Z); columns that
+    finish at different steps (an exact initial guess stops at step 0, a
+    smooth right-hand side converges sooner than noise) leave the lockstep
+    without disturbing the others"""
+    ctx = F.Context(0)
+    A = F.diffusion7(16, 15, 14, 1.5, 3.0, 4).scale()
+    S = F.Solver(ctx, A, rel_tol=1e-10, c=4)
+    assert not S.info()[1]
+    n = A.shape[0]
+    rng = np.random.default_rng(9)
+    xs = F.random_uniform(2, -1.0, 1.0, n)
+    B = np.ascontiguousarray(np.stack([rng.standard_normal(n), A.spmv(np.ones(n)), A.spmv(xs),
+                                       rng.standard_normal(n) * 1e3]))
+    X0 = np.zeros_like(B)
+    X0[2] = xs  # already the solution
+    res = _check_block(S, B, X0)
+    assert res[2].res_iter == 0 and res[0].res_iter > 0
+
+
+def test_block_solve_restarts_in_lockstep():
+    """a short outer restart length: every column restarts (its x += Z y, then
+    a new residual) in the same step as its single solve"""
+    ctx = F.Context(0)
+    A = F.stencil27(16, 16, 16, 1, 0.5).scale()
+    S = F.Solver(ctx, A, rel_tol=1e-10, c=4, m_outer=1, max_restarts=30)
+    B = np.ascontiguousarray(np.random.default_rng(1).standard_normal((4, A.shape[0])))
+    res = _check_block(S, B)
+    assert all(r.restarts > 1 and r.is_solved for r in res)
+
+
+def test_block_solve_multi_rhs_device_and_static_weight():
+    """device blocks (torch), F3R-Static and m3 = 0 through the block engine"""
+    ctx = F.Context(0)
+    A = F.stencil27(14, 14, 14, 2, 0.5).scale()
+    for kw in (dict(static_weight=1.1), dict(m3=0, m2=16), dict(m4=3, c=2)):
+        S = F.Solver(ctx, A, rel_tol=1e-10, **kw)
+        B = np.ascontiguousarray(np.random.default_rng(4).standard_normal((6, A.shape[0])))
+        _check_block(S, B)
+        Bd = torch.from_numpy(B).cuda()
+        Xd = torch.zeros_like(Bd)
+        S.solve_multi(Bd, Xd)
+        Xh = np.zeros_like(B)
+        S.solve_multi(B, Xh)
+        assert np.array_equal(Xd.cpu().numpy(), Xh), kw

@@ -63,7 +63,8 @@ def test_static_and_depth_lines(suite_dirs):
     fc = run(["--method", "F3R-Static", "--blocks", "16", "--format", "CSR", "hpgmp_4_4_4.mtx", "1.0", "1", "8", "4",
               "2", "8", "3", "1.2"], cwd)[0].split(",")
     assert fc[:9] == f[:9] and fc[10:] == f[10:]
-    for method in ("F3", "F2"):
+    for method in ("F3", "F2", "F4", "F3H", "F2H"):
         f = run(["--method", method, "--blocks", "16", "hpgmp_4_4_4.mtx", "1.0", "1", "8", "4", "2", "8", "3"],
                 cwd)[0].split(",")
         assert f[1] == method and float(f[12]) < 1e-7
+        assert int(f[10]) % 64 == 0  # outer iterations * 64, as depth.cpp's test(..., 64)

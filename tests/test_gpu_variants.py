@@ -75,3 +75,52 @@ def test_sstep_large_level_and_graphs(ctx):
         assert res.is_solved and res.expl_rel_res < 1e-10
         xs.append(x)
     assert np.array_equal(xs[0], xs[1])
+
+
+HALF = {"f4_hpgmp16": (8, 4, 2), "f3h_hpgmp16": (8, 0, 8), "f2h_hpgmp16": (0, 0, 64)}
+
+
+@pytest.mark.parametrize("name", sorted(HALF))
+def test_half_level_variants(ctx, name):
+    """F4 / F3H / F2H (depth.cpp:122-167): the fp16-vector FGMRES level below
+    the fp32 levels (or directly below the outer level, m2 = 0) solves the
+    golden system to 1e-10 with the expected count of preconditioner calls;
+    graphs on and off give the same iterate (the history against the
+    reference is checked in test_gpu_history.py)"""
+    from history_band import CASES
+    r, i, v, b, xs, sol = golden_system(name)
+    m2, m3, mh = HALF[name]
+    assert (CASES[name]["m2"], CASES[name]["m3"], CASES[name]["half_m"]) == (m2, m3, mh)
+    xsol = []
+    for graphs in (1, 0):
+        S = F.Solver(ctx, F.HostMatrix.from_csr(r, i, v), rel_tol=1e-10, use_graphs=graphs, **CASES[name])
+        x = np.zeros(len(b))
+        res = S.solve(b, x)
+        assert res.is_solved and res.expl_rel_res < 1e-10
+        assert res.inner_applications == res.res_iter * max(m2, 1) * max(m3, 1) * mh
+        xsol.append(x)
+        S.close()
+    assert np.array_equal(xsol[0], xsol[1])
+    assert np.linalg.norm(xsol[0] - xs) / np.linalg.norm(xs) < 1e-7
+
+
+def test_half_level_with_sdainv_richardson(ctx):
+    """the fp16-vector level over the adaptive Richardson with diagonal SDAINV
+    (m4 = 2, weights updated every c-th call): R runs on the level's fp16
+    vectors in both the fused and the weight-update paths"""
+    A = F.stencil27(20, 20, 20, 2, 0.5).scale()
+    b = A.spmv(F.random_uniform(4, -1, 1, A.shape[0]))
+    for m2, m3, mh in ((8, 0, 4), (4, 2, 2), (0, 0, 16)):
+        S = F.Solver(ctx, A, rel_tol=1e-10, c=4, m2=m2, m3=m3, half_m=mh, m4=2)
+        assert S.info()[1]  # diagonal SDAINV
+        x = np.zeros(len(b))
+        res = S.solve(b, x)
+        assert res.is_solved and res.expl_rel_res < 1e-10, (m2, m3, mh)
+        S.close()
+
+
+def test_half_level_rejects_bad_nesting(ctx):
+    A = F.stencil27(8, 8, 8).scale()
+    for bad in (dict(m2=0), dict(m2=0, half_m=4, m3=2), dict(m2=0, half_m=4, inner_sstep=1), dict(half_m=128)):
+        with pytest.raises(F.F3RError):
+            F.Solver(ctx, A, **bad)
