@@ -50,9 +50,11 @@ NX = 192
 BETA = 0.5
 SIGMA = 1
 ALIGN = 1
-LAYOUTS = {"aligned": dict(sell_sigma=1, sell_align=1, format=0), "sigma256": dict(sell_sigma=256, sell_align=0, format=0),
-           "csr": dict(sell_sigma=1, sell_align=0, format=1),
-           "auto": dict(sell_sigma=1, sell_align=0, format=0, sell_autotune=1)}
+LAYOUTS = {"aligned": dict(sell_sigma=1, sell_align=1, format=0, sell_c=32),
+           "aligned64": dict(sell_sigma=1, sell_align=1, format=0, sell_c=64),
+           "sigma256": dict(sell_sigma=256, sell_align=0, format=0, sell_c=32),
+           "csr": dict(sell_sigma=1, sell_align=0, format=1, sell_c=32),
+           "auto": dict(sell_sigma=1, sell_align=0, format=0, sell_autotune=1, sell_c=32)}
 TOL = 1e-10
 PARAMS = dict(m_outer=100, max_restarts=20, m2=8, m3=4, m4=2, c=64, sdainv_tol=0.1, acc=1.0, sell_sigma=SIGMA,
               sell_align=ALIGN, format=0,
@@ -75,7 +77,8 @@ def set_size(nx):
 def layout_tag():
     if PARAMS.get("format"):
         return "CSR"
-    return "SELL32al" if PARAMS["sell_align"] else f"SELL32s{PARAMS['sell_sigma']}"
+    c = PARAMS.get("sell_c", 32)
+    return f"SELL{c}al" if PARAMS["sell_align"] else f"SELL{c}s{PARAMS['sell_sigma']}"
 
 
 def set_layout(name):
@@ -93,7 +96,7 @@ def layout_desc(p=None):
         return dict(AUTOTUNED["chosen"], autotuned=True)
     if p.get("format"):
         return {"format": "CSR", "index": "explicit int32"}
-    return {"C": 32, "sigma": p["sell_sigma"],
+    return {"C": p.get("sell_c", 32), "sigma": p["sell_sigma"],
             "index": "offset-aligned (no stored column index)" if p["sell_align"] else "explicit int32"}
 
 
@@ -250,13 +253,16 @@ def spmv_roofline(solver, A, torch, F):
     alg = nnz * (2 + 4) + 4 * (n + 1) + n * 4 + n * 4
     aligned = info.index_bits == 0
     csr = info.slice_height == 0
-    nslices = (n + 31) // 32
-    idx_bytes = (info.nnz_padded // 32) * 4 if aligned else info.nnz_padded * 4
+    h = info.slice_height or 32
+    nslices = (n + h - 1) // h
+    idx_bytes = (info.nnz_padded // h) * 4 if aligned else info.nnz_padded * 4
     stored = alg if csr else info.nnz_padded * 2 + idx_bytes + 4 * (nslices + 1) + n * 4 + n * 4
     peak, src = measured_peak()
     achieved = alg / dt / 1e9
     if csr:
         kern = "k_csr_cfg<__half,float,EpiStore<float>,24> (CSR, fp16 A, fp32 x, fp32 y)"
+    elif h == 64:
+        kern = "k_sell64<__half,float,EpiStore<float>,24,2,32> (64-row offset-aligned slices, fp16 A, fp32 x, fp32 y)"
     elif aligned:
         kern = ("k_sell_cfg<__half,float,EpiStore<float>,32,2,32,AllAlignedIdx> (SELL-32 sigma=1, offset-aligned, "
                 "fp16 A, fp32 x, fp32 y)")
@@ -344,7 +350,8 @@ def run_ours(args):
         # the layout the autotuner chose, in the config's terms
         info, _ = solver.info()
         PARAMS.update(format=1 if info.slice_height == 0 else 0, sell_sigma=info.sigma,
-                      sell_align=1 if info.index_bits == 0 else 0, sell_autotune=0)
+                      sell_align=1 if info.index_bits == 0 else 0, sell_autotune=0,
+                      sell_c=info.slice_height if info.slice_height else 32)
         AUTOTUNED["chosen"] = layout_desc()
     b_d = torch.from_numpy(b).cuda()
     x_d = torch.zeros_like(b_d)
@@ -491,8 +498,9 @@ def run_c4(args):
 
 
 def c4_line(args):
-    """C4: the batch solved concurrently (f3r_solve_batch, one context per
-    system) against the same solvers one after another; wall time around the
+    """C4: the batch solved at once (f3r_solve_batch: each system's
+    right-hand sides in lockstep blocks, systems on their own contexts
+    concurrently) against one right-hand side at a time; wall time around the
     whole batch with the device synchronised on both sides."""
     import torch
     import f3r_b200 as F
@@ -518,6 +526,17 @@ def c4_line(args):
         return time.perf_counter() - t0, res
 
     def sequential():
+        """one right-hand side at a time, system after system"""
+        for x in Xd:
+            x.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        res = [[S.solve(b[k], x[k]) for k in range(b.shape[0])] for S, b, x in batch]
+        torch.cuda.synchronize()
+        return time.perf_counter() - t0, res
+
+    def blocks():
+        """each system's right-hand sides in lockstep blocks, system after system"""
         for x in Xd:
             x.zero_()
         torch.cuda.synchronize()
@@ -528,8 +547,10 @@ def c4_line(args):
 
     for _ in range(max(args.warmup, 1)):
         batched()
+        blocks()
         sequential()
     tb = min(batched()[0] for _ in range(args.steps))
+    tk = min(blocks()[0] for _ in range(args.steps))
     ts, res = min((sequential() for _ in range(args.steps)), key=lambda t: t[0])
     _, resb = batched()
     nrhs = sum(B.shape[0] for _, _, _, B in systems)
@@ -544,7 +565,12 @@ def c4_line(args):
                        "systems": len(systems), "rhs": nrhs, "rows_x_rhs": rows,
                        "sell": layout_desc(), "timing": "host wall clock, device synchronised on both sides"},
             "batched_ms": round(tb * 1e3, 2), "sequential_ms": round(ts * 1e3, 2),
-            "speedup_batched_vs_sequential": round(ts / tb, 2), "solves_per_s": round(nrhs / tb, 1),
+            "blocks_one_system_at_a_time_ms": round(tk * 1e3, 2),
+            "speedup_batched_vs_sequential": round(ts / tb, 2), "speedup_blocks_vs_sequential": round(ts / tk, 2),
+            "solves_per_s": round(nrhs / tb, 1),
+            "modes": "batched: f3r_solve_batch (each system's right-hand sides in lockstep blocks of up to 16, "
+                     "systems on their own contexts concurrently); blocks: the same blocks, one system after "
+                     "another; sequential: one right-hand side at a time",
             "all_solved": all(r.is_solved for rs in resb for r in rs), "worst_expl_rel_res": worst,
             "outer_iters_total": sum(r.res_iter for rs in resb for r in rs), "setup_s": round(t_setup, 1)}
     for S in solvers:
@@ -749,9 +775,15 @@ def c5_line(args):
     """C5, the learned preconditioner: the network trained on the GPU on
     residual / error pairs of 256 seeded 7-point log-normal fields (sigma
     1.5, correlation length 6; 24^3 each, stacked), then held-out 128^3
-    fields solved to 1e-10 with plain SDAINV and with the learned correction
-    (BF16 tensor-core inference), one after another and batched
-    (f3r_solve_batch over one context per system)."""
+    fields solved to 1e-10:
+      * one at a time (device time of each solve, best of steps), with plain
+        SDAINV and with the learned correction (BF16 tensor-core inference),
+        in the headline's layout (offset-aligned SELL);
+      * batched: groups of C5_BATCH fields of the one 7-point pattern solved
+        together (f3r_batch: one lockstep solve, each column its own system
+        with its own values and factors), plain and learned; wall time of the
+        group's solve with the device synchronised on both sides.
+    learned+batched is compared with plain solves one after another."""
     import torch
     import f3r_b200 as F
     from f3r_b200.learned import Learned, training_set
@@ -769,8 +801,7 @@ def c5_line(args):
     final_loss = L.evaluate()
     n_train, n_pairs = ts.A.shape[0], ts.r.shape[0]
     del ts
-    rows, solvers_l, solvers_p, ctxs, bs, xs_d = [], [], [], [], [], []
-    probe_k = []
+    rows, held = [], []
     for s in range(10000, 10000 + args.c5_eval):
         A = F.diffusion7(nx, nx, nx, 1.5, 6.0, s).scale()
         n = A.shape[0]
@@ -780,9 +811,8 @@ def c5_line(args):
         Zc, Wc = L.correct(A, nx, nx, Z, Wt)
         t_inf = time.perf_counter() - t0
         b = A.spmv(F.random_uniform(s, -1.0, 1.0, n))
-        c = F.Context(0)
-        Sp = F.Solver(c, A, factors=(Z, Wt), **PARAMS)
-        Sl = F.Solver(c, A, factors=(Zc, Wc), **PARAMS)
+        Sp = F.Solver(ctx, A, factors=(Z, Wt), **PARAMS)
+        Sl = F.Solver(ctx, A, factors=(Zc, Wc), **PARAMS)
         b_d = torch.from_numpy(b).cuda()
         x_d = torch.zeros_like(b_d)
         rec = {"seed": s, "correct_call_ms": round(t_inf * 1e3, 1)}
@@ -804,69 +834,69 @@ def c5_line(args):
             x_d.zero_()
             r = S.solve(b_d, x_d, cond=lambda i, e, k=k: i >= k)
             rec[name][f"expl_rel_res_after_{k}"] = r.expl_rel_res
+        Sp.close()
+        Sl.close()
         rows.append(rec)
-        if len(solvers_p) < C5_BATCH:
-            ctxs.append(c)
-            solvers_p.append(Sp)
-            solvers_l.append(Sl)
-            bs.append(b_d)
-            xs_d.append(torch.zeros_like(b_d))
-        else:  # each 128^3 solver holds ~3.4 GB of fp64 Krylov bases: only C5_BATCH systems stay
-            Sp.close()
-            Sl.close()
-            c.close()
+        held.append((A, b, (Z, Wt), (Zc, Wc)))
 
-    def run(solvers, batched):
-        for x in xs_d:
-            x.zero_()
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        if batched:
-            res = [r[0] for r in F.solve_batch([(S, b.view(1, -1), x.view(1, -1))
-                                                 for S, b, x in zip(solvers, bs, xs_d)])]
-        else:
-            res = [S.solve(b, x) for S, b, x in zip(solvers, bs, xs_d)]
-        torch.cuda.synchronize()
-        return time.perf_counter() - t0, res
-
-    for _ in range(max(args.warmup, 1)):
-        run(solvers_p, False)
-        run(solvers_l, True)
-    tp, resp = min((run(solvers_p, False) for _ in range(args.steps)), key=lambda t: t[0])
-    tl, resl = min((run(solvers_l, False) for _ in range(args.steps)), key=lambda t: t[0])
-    tlb, reslb = min((run(solvers_l, True) for _ in range(args.steps)), key=lambda t: t[0])
-    tpb, _ = min((run(solvers_p, True) for _ in range(args.steps)), key=lambda t: t[0])
-    mean = lambda key, f: float(np.mean([f(r[key]) for r in rows]))
+    # batched: the held-out fields in groups of C5_BATCH, one f3r_batch each
+    bp = dict(PARAMS)
+    bp.update(sell_align=0)
+    bat = {"plain": [], "learned": []}
+    solved = True
+    for g0 in range(0, len(held), C5_BATCH):
+        grp = held[g0:g0 + C5_BATCH]
+        bs = [torch.from_numpy(b).cuda() for _, b, _, _ in grp]
+        xs = [torch.zeros_like(b) for b in bs]
+        for name, fi in (("plain", 2), ("learned", 3)):
+            B = F.Batch(ctx, [h[0] for h in grp], factors=[h[fi] for h in grp], **bp)
+            best = None
+            for it in range(max(args.warmup, 1) + args.steps):
+                for x in xs:
+                    x.zero_()
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                res = B.solve(bs, xs)
+                torch.cuda.synchronize()
+                dt = time.perf_counter() - t0
+                if it >= max(args.warmup, 1) and (best is None or dt < best[0]):
+                    best = (dt, res)
+            solved = solved and all(r.is_solved and r.expl_rel_res < 1e-10 for r in best[1])
+            bat[name].append({"systems": len(grp), "wall_ms": round(best[0] * 1e3, 2),
+                              "outer_iters": [r.res_iter for r in best[1]]})
+            B.close()
+    mean = lambda key: float(np.mean([r[key]["ms"] for r in rows]))
+    per_sys = {k: sum(g["wall_ms"] for g in v) / len(held) for k, v in bat.items()}
     gains = [r["plain"][k] / r["learned"][k] for r in rows for k in r["plain"] if k.startswith("expl_rel_res_after")]
-    line = {"metric": "time to 1e-10 FP64 relative residual, learned vs plain SDAINV (C5)",
-            "value": round(mean("learned", lambda d: d["ms"]), 2), "unit": "ms", "n_gpus": 1,
+    plain_ms = mean("plain")
+    line = {"metric": "time to 1e-10 FP64 relative residual per system, learned / batched vs plain SDAINV (C5)",
+            "value": round(per_sys["learned"], 2), "unit": "ms", "n_gpus": 1,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": False,
             "dtype": "mixed: f16 storage/f32 accumulate, f32, f64; MLP bf16 inference, f32 training",
             "data": "synthetic (seeded log-normal coefficient fields)",
             "config": {"workload": f"C5: 7-pt diffusion, log-normal sigma 1.5, corr 6, {nx}^3 held-out "
                                    f"(n={nx ** 3}), SDAINV vs learned SDAINV, tol 1e-10",
                        "train_fields": args.c5_train, "train_grid": "24^3 each, stacked", "train_rows": n_train,
-                       "eval_fields": args.c5_eval, "sell": layout_desc(),
-                       "timing": "per system: device solve time (CUDA events), best of steps; "
-                                 "whole set: host wall clock, device synchronised on both sides"},
-            "plain_ms": round(mean("plain", lambda d: d["ms"]), 2),
-            "learned_over_plain_time": round(mean("learned", lambda d: d["ms"]) / mean("plain", lambda d: d["ms"]), 3),
+                       "eval_fields": args.c5_eval, "batch": C5_BATCH, "sell_single": layout_desc(),
+                       "sell_batched": "packed SELL-32, int32 indices, values of the batch interleaved",
+                       "timing": "single: device solve time (CUDA events), best of steps; batched: host wall "
+                                 "clock around one batch solve, device synchronised on both sides, best of steps, "
+                                 "divided by the systems"},
+            "plain_ms": round(plain_ms, 2),
+            "learned_ms": round(mean("learned"), 2),
+            "plain_batched_ms_per_system": round(per_sys["plain"], 2),
+            "learned_batched_ms_per_system": round(per_sys["learned"], 2),
+            "learned_over_plain_time": round(mean("learned") / plain_ms, 3),
+            "speedup_learned_batched_vs_plain": round(plain_ms / per_sys["learned"], 3),
+            "speedup_plain_batched_vs_plain": round(plain_ms / per_sys["plain"], 3),
             "outer_iters": {"plain": [r["plain"]["outer_iters"] for r in rows],
                             "learned": [r["learned"]["outer_iters"] for r in rows]},
             "residual_gain_at_fixed_outer_steps": {"min": round(min(gains), 2), "max": round(max(gains), 2),
                                                    "geomean": round(float(np.exp(np.mean(np.log(gains)))), 2)},
-            "set_wall_ms": {"systems": len(solvers_p), "plain_sequential": round(tp * 1e3, 1),
-                            "learned_sequential": round(tl * 1e3, 1),
-                            "plain_batched": round(tpb * 1e3, 1), "learned_batched": round(tlb * 1e3, 1)},
-            "speedup_learned_batched_vs_plain_sequential": round(tp / tlb, 3),
-            "all_solved": all(r.is_solved for r in resl + reslb + resp),
+            "batched": bat, "all_solved": solved and all(r[k]["solved"] for r in rows for k in ("plain", "learned")),
             "training": {"pairs": n_pairs, "steps": args.c5_steps, "train_s": round(t_train, 2),
                          "data_s": round(t_data, 1), "loss_first": float(losses[0]), "loss_final": final_loss},
             "systems": rows}
-    for S in solvers_p + solvers_l:
-        S.close()
-    for c in ctxs:
-        c.close()
     L.close()
     ctx.close()
     return line

@@ -244,15 +244,16 @@ class Sell:
     compute_residual on device tensors."""
 
     def __init__(self, ctx: Context, A: HostMatrix, sigma: int = 1, dtypes=(F64, F32, F16), index16: bool = False,
-                 aligned: bool = False, csr: bool = False):
-        """csr: keep the matrix in CSR (F3R_SELL_CSR) instead of SELL-32"""
+                 aligned: bool = False, csr: bool = False, height: int = 32):
+        """csr: keep the matrix in CSR (F3R_SELL_CSR) instead of SELL-32;
+        height 64: 64-row offset-aligned slices (sigma 1)"""
         mask = ((_capi.SELL_INDEX16 if index16 else 0) | (_capi.SELL_ALIGNED if aligned else 0) |
                 (_capi.SELL_CSR if csr else 0))
         for d in dtypes:
             mask |= 1 << d
         h = C.c_void_p()
         v = A.view()
-        check(lib().f3r_sell_create(ctx._h, C.byref(v), 32, sigma, mask, C.byref(h)))
+        check(lib().f3r_sell_create(ctx._h, C.byref(v), height, sigma, mask, C.byref(h)))
         self._h = h
         _LIVE["sell"].add(self)
         self.ctx = ctx
@@ -401,6 +402,61 @@ class Solver:
     def close(self):
         if getattr(self, "_h", None) is not None and _capi is not None and _capi._lib is not None:
             _capi._lib.f3r_solver_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+
+class Batch:
+    """Up to 16 systems of one sparsity pattern solved together
+    (f3r_batch_*): one lockstep solve whose columns are the systems, each
+    with its own values and SDAINV factors (computed, or given as
+    factors=[(Z, W^T), ...])."""
+
+    def __init__(self, ctx: Context, systems, params: Optional[_capi.Params] = None, factors=None, **kw):
+        p = params if params is not None else Params(**kw)
+        self._views = [A.view() for A in systems]
+        count = len(systems)
+        arr = (C.POINTER(_capi.CSR) * count)(*[C.pointer(v) for v in self._views])
+        zarr = warr = None
+        if factors is not None:
+            self._fviews = [(Z.view(), W.view()) for Z, W in factors]
+            zarr = (C.POINTER(_capi.CSR) * count)(*[C.pointer(z) for z, _ in self._fviews])
+            warr = (C.POINTER(_capi.CSR) * count)(*[C.pointer(w) for _, w in self._fviews])
+        h = C.c_void_p()
+        check(lib().f3r_batch_create(ctx._h, count, arr, C.byref(p), zarr, warr, C.byref(h)))
+        self._h = h
+        _LIVE["solver"].add(self)
+        self.ctx = ctx
+        self.count = count
+        self.n = self._views[0].nrows
+
+    def info(self):
+        """(systems, block width K, diagonal SDAINV)"""
+        c, k, d = C.c_int32(), C.c_int32(), C.c_int32()
+        check(lib().f3r_batch_info(self._h, C.byref(c), C.byref(k), C.byref(d)))
+        return c.value, k.value, bool(d.value)
+
+    def solve(self, bs, xs, cond: Optional[Callable[[int, float], bool]] = None):
+        """Solve system i for bs[i] into xs[i] (numpy float64 or torch CUDA
+        float64 vectors; xs[i] holds the initial guess).  Returns one
+        solve_res_t per system."""
+        if len(bs) != self.count or len(xs) != self.count:
+            raise ValueError("one right-hand side and one solution vector per system")
+        for v in list(bs) + list(xs):
+            if tuple(v.shape) != (self.n,):
+                raise ValueError("vectors must have the systems' row count")
+        bp = (C.c_void_p * self.count)(*[_ptr(b) for b in bs])
+        xp = (C.c_void_p * self.count)(*[_ptr(x) for x in xs])
+        res = (_capi.Result * self.count)()
+        cb = COND_NONE if cond is None else _capi.COND_FN(lambda i, e, u: 1 if cond(i, e) else 0)
+        check(lib().f3r_batch_solve(self._h, bp, xp, cb, None, res))
+        return [_res(r) for r in res]
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and _capi is not None and _capi._lib is not None:
+            _capi._lib.f3r_batch_destroy(self._h)
             self._h = None
 
     def __del__(self):

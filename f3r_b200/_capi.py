@@ -118,6 +118,11 @@ SIGNATURES = {
     "f3r_solver_destroy": (None, [_vp]),
     "f3r_solver_create_factors": (C.c_int, [_vp, C.POINTER(CSR), C.POINTER(Params), C.POINTER(CSR), C.POINTER(CSR),
                                             _pp]),
+    "f3r_batch_create": (C.c_int, [_vp, C.c_int32, C.POINTER(C.POINTER(CSR)), C.POINTER(Params),
+                                   C.POINTER(C.POINTER(CSR)), C.POINTER(C.POINTER(CSR)), _pp]),
+    "f3r_batch_solve": (C.c_int, [_vp, C.POINTER(_vp), C.POINTER(_vp), COND_FN, _vp, C.POINTER(Result)]),
+    "f3r_batch_info": (C.c_int, [_vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+    "f3r_batch_destroy": (None, [_vp]),
     "f3r_learned_create": (C.c_int, [_vp, C.c_int32, C.c_uint64, _pp]),
     "f3r_learned_destroy": (None, [_vp]),
     "f3r_learned_params": (C.c_int, [_vp, _vp, C.c_int32, C.POINTER(C.c_int64)]),
@@ -127,6 +132,8 @@ SIGNATURES = {
     "f3r_learned_train": (C.c_int, [_vp, C.c_int32, C.c_double, _vp]),
     "f3r_learned_correct": (C.c_int, [_vp, C.POINTER(CSR), C.c_int32, C.c_int32, C.POINTER(CSR), C.POINTER(CSR),
                                       C.c_int32, _vp, _vp, _vp]),
+    "f3r_learned_time_inference": (C.c_int, [_vp, C.POINTER(CSR), C.c_int32, C.c_int32, C.POINTER(CSR),
+                                             C.POINTER(CSR), C.c_int32, C.c_int32, C.POINTER(C.c_double)]),
 }
 
 _lib = None

@@ -76,7 +76,9 @@ template <typename T, int K> struct RowK {
 // ---------------------------------------------------------------------------
 // Block SELL product: out(:, c) = A x(:, c) for c < K, one pass over A.
 // Same layouts and bulk-copy ring as k_sell_cfg (sell.cuh); the index forms
-// are the packed int32 one (MODE 0) and the fully offset-aligned one (MODE 3).
+// are the packed int32 one (MODE 0), the mixed offset-aligned one (MODE 2:
+// aligned slices with bases, the others with explicit indices) and the fully
+// offset-aligned one (MODE 3).
 // Each lane owns one row of a slice and K accumulators, summing the row's
 // entries in stored order with one FMA per column.
 // ---------------------------------------------------------------------------
@@ -87,23 +89,44 @@ template <int K> struct BlockCfg<double, K, int32_t> { static constexpr int WARP
 template <int K> struct BlockCfg<__half, K, AllAlignedIdx> { static constexpr int WARPS = 16, STAGES = 2, KC = 32; };
 template <int K> struct BlockCfg<float, K, AllAlignedIdx> { static constexpr int WARPS = 16, STAGES = 2, KC = 32; };
 template <int K> struct BlockCfg<double, K, AllAlignedIdx> { static constexpr int WARPS = 12, STAGES = 2, KC = 32; };
+template <int K> struct BlockCfg<__half, K, AlignedIdx> { static constexpr int WARPS = 16, STAGES = 2, KC = 16; };
+template <int K> struct BlockCfg<float, K, AlignedIdx> { static constexpr int WARPS = 16, STAGES = 2, KC = 16; };
+template <int K> struct BlockCfg<double, K, AlignedIdx> { static constexpr int WARPS = 12, STAGES = 2, KC = 16; };
 
 template <typename V, int K, typename CI> constexpr size_t block_smem_bytes() {
   using Cfg = BlockCfg<V, K, CI>;
   return sell_smem_bytes_cfg<V, CI, Cfg::WARPS, Cfg::STAGES, Cfg::KC>();
 }
+// Systems of one pattern, each with its own values (packed int32 layout, the
+// K values of an entry interleaved): chunks of at most 4 KB of values.
+template <typename V, int K> struct BlockCfgMM {
+  static constexpr int WARPS = sizeof(V) == 8 ? 12 : 16, STAGES = 2;
+  static constexpr int KC0 = 4096 / (32 * K * (int)sizeof(V));
+  static constexpr int KC = KC0 < 1 ? 1 : KC0 > 16 ? 16 : KC0;
+};
+template <typename V, int K> constexpr size_t block_mm_smem_bytes() {
+  using Cfg = BlockCfgMM<V, K>;
+  return (size_t)Cfg::WARPS * Cfg::STAGES * ((size_t)Cfg::KC * 32 * (K * sizeof(V) + 4)) +
+         (size_t)Cfg::WARPS * Cfg::STAGES * sizeof(uint64_t);
+}
 
-template <typename V, typename X, typename Epi, int K, int WARPS, int STAGES, int KC, typename CI>
+// MM: every column has its own matrix values (systems of one pattern); the
+// K values of an entry are contiguous, val[position * K + c].
+template <typename V, typename X, typename Epi, int K, int WARPS, int STAGES, int KC, typename CI, bool MM = false>
 __global__ void __launch_bounds__(WARPS * 32, 1)
     k_sell_block(const V *__restrict__ val, DevSell A, const X *__restrict__ x, Epi epi, int *err) {
   using Acc = typename acc_of<V>::type;
   constexpr int MODE = IdxForm<CI>::mode;
-  static_assert(MODE == 0 || MODE == 3, "block product: packed int32 or fully aligned slices");
+  static_assert(MODE == 0 || MODE == 2 || MODE == 3, "block product: packed int32 or offset-aligned slices");
+  static_assert(!MM || MODE == 0, "per-column values: packed int32 layout");
   static_assert(MODE != 3 || KC == kAllAlignedChunk, "fully aligned layout is built for kAllAlignedChunk columns");
-  constexpr uint32_t VB = KC * 32 * sizeof(V), CB = KC * 32 * IdxForm<CI>::bytes, BB = MODE != 0 ? KC * 4 : 0,
+  static_assert(MODE != 2 || KC == kAlignedChunk, "aligned layout is built for kAlignedChunk columns");
+  constexpr int VK = MM ? K : 1;  // values per entry
+  constexpr uint32_t VB = KC * 32 * sizeof(V) * VK, CB = KC * 32 * IdxForm<CI>::bytes, BB = MODE != 0 ? KC * 4 : 0,
                      SB = VB + CB + BB;
-  // entries gathered per pipelined sub-block: about 64 gathered values per lane
-  constexpr int SUB = K >= 16 ? 4 : K >= 8 ? 8 : 16;
+  // entries gathered per sub-block: about 32 gathered fp32 values (16 fp64) per lane
+  constexpr int SUB0 = (sizeof(Acc) == 8 ? 16 : 32) / (K * (MM ? 2 : 1));
+  constexpr int SUB = SUB0 > 0 ? SUB0 : 1;
   extern __shared__ __align__(128) unsigned char smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   unsigned char *buf = smem + (size_t)warp * STAGES * SB;
@@ -117,13 +140,14 @@ __global__ void __launch_bounds__(WARPS * 32, 1)
   const uint64_t pol = l2_evict_first_policy();
   const int TW = gridDim.x * WARPS;
   int fs = blockIdx.x * WARPS + warp, fk = 0, fst = 0, inflight = 0;
-  int fs0 = 0, fw = 0, fcb = 0;
+  int fs0 = 0, fw = 0, fcb = 0, fxo = 0;
   auto fetch = [&]() {
     while (inflight < STAGES && fs < A.nslices) {
       if (fk == 0) {
         fs0 = A.sptr[fs];
         fw = A.sptr[fs + 1] - fs0;
-        if (MODE == 3) fcb = A.cbptr[fs] & ~3;
+        if (MODE == 2) fxo = A.xoff[fs];
+        if (MODE != 0) fcb = A.cbptr[fs] & ~3;
       }
       if (fw == 0) {
         fs += TW;
@@ -134,12 +158,17 @@ __global__ void __launch_bounds__(WARPS * 32, 1)
       if (lane == 0) {
         const size_t off = ((size_t)fs0 + fk) * 32;
         fence_proxy_async_smem();
-        const uint32_t ib = MODE == 0 ? (uint32_t)kc * 32u * 4u : 0u;
-        const uint32_t bb = MODE == 3 ? (uint32_t)((kc + 3) & ~3) * 4u : 0u;
-        mbar_arrive_expect_tx(&bars[fst], (uint32_t)kc * 32u * (uint32_t)sizeof(V) + ib + bb);
-        bulk_g2s(buf + (size_t)fst * SB, val + off, (uint32_t)kc * 32u * (uint32_t)sizeof(V), &bars[fst], pol);
-        if (MODE == 0) bulk_g2s(buf + (size_t)fst * SB + VB, A.col + off, ib, &bars[fst], pol);
-        if (MODE == 3) bulk_g2s(buf + (size_t)fst * SB + VB + CB, A.cbase + fcb + fk, bb, &bars[fst], pol);
+        // mixed form: a slice carries either bases (aligned) or explicit indices (from xoff)
+        const bool want_idx = MODE == 0 || (MODE == 2 && fxo >= 0);
+        const bool want_base = MODE == 3 || (MODE == 2 && fxo < 0);
+        const uint32_t ib = want_idx ? (uint32_t)kc * 32u * 4u : 0u;
+        const uint32_t bb = want_base ? (uint32_t)((kc + 3) & ~3) * 4u : 0u;
+        const uint32_t vb = (uint32_t)kc * 32u * (uint32_t)sizeof(V) * (uint32_t)VK;
+        const int32_t *isrc = MODE == 2 ? A.col + (size_t)fxo + (size_t)fk * 32 : A.col + off;
+        mbar_arrive_expect_tx(&bars[fst], vb + ib + bb);
+        bulk_g2s(buf + (size_t)fst * SB, val + off * VK, vb, &bars[fst], pol);
+        if (want_idx) bulk_g2s(buf + (size_t)fst * SB + VB, isrc, ib, &bars[fst], pol);
+        if (want_base) bulk_g2s(buf + (size_t)fst * SB + VB + CB, A.cbase + fcb + fk, bb, &bars[fst], pol);
       }
       fst = (fst + 1 == STAGES) ? 0 : fst + 1;
       inflight++;
@@ -165,9 +194,11 @@ __global__ void __launch_bounds__(WARPS * 32, 1)
   for (int c = 0; c < K; c++) acc[c] = 0;
   int w = 0;
   bool clampc = false;
+  bool aligned = MODE == 3;  // the current slice is offset-aligned
   while (cs < A.nslices) {
     if (ck == 0) {
       w = A.sptr[cs + 1] - A.sptr[cs];
+      if (MODE == 2) aligned = A.xoff[cs] < 0;
       if (MODE == 3) clampc = (A.cbptr[cs] & 1) != 0;
     }
     const int64_t r = (int64_t)cs * 32 + lane;
@@ -191,7 +222,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1)
     // first (then the stage goes back to the copy engine), then the gathers
     // of the sub-block, then its multiply-adds
     constexpr int NSUB = (KC + SUB - 1) / SUB;
-    V vv[SUB];
+    Acc vv[SUB][VK];
     int32_t cc[SUB];
     const V *lv = sv + lane * kc;  // aligned form: lane-major values
     for (int h = 0; h < NSUB; h++) {
@@ -201,12 +232,16 @@ __global__ void __launch_bounds__(WARPS * 32, 1)
       for (int e = 0; e < SUB; e++) {
         const int k = k0 + e;
         if (k < kc) {
-          if (MODE == 3) {
-            vv[e] = lv[k];
-            const int32_t b = sb[k] + lane;
-            cc[e] = clampc ? min(max(b, 0), A.ncols - 1) : b;
+          if (MODE == 3 || MODE == 2) {
+            vv[e][0] = to_acc<Acc>(lv[k]);  // lane-major values
+            if (MODE == 2 && !aligned) {
+              cc[e] = sc[k * 32 + lane];
+            } else {
+              const int32_t b = sb[k] + lane;
+              cc[e] = clampc ? min(max(b, 0), A.ncols - 1) : b;
+            }
           } else {
-            vv[e] = sv[k * 32 + lane];
+            RowK<V, VK>::load(sv + ((size_t)k * 32 + lane) * VK, vv[e]);
             cc[e] = sc[k * 32 + lane];
           }
         }
@@ -219,9 +254,8 @@ __global__ void __launch_bounds__(WARPS * 32, 1)
 #pragma unroll
       for (int e = 0; e < SUB; e++)
         if (k0 + e < kc) {
-          const Acc v = to_acc<Acc>(vv[e]);
 #pragma unroll
-          for (int c = 0; c < K; c++) acc[c] = fmaT(v, xg[e][c], acc[c]);
+          for (int c = 0; c < K; c++) acc[c] = fmaT(vv[e][MM ? c : 0], xg[e][c], acc[c]);
         }
     }
     ck += kc;
@@ -268,7 +302,8 @@ template <typename B, typename Out, int K> struct EpiResidualK {
 // (EpiRichStepT, kernels.cuh, per column with the column's own weight):
 // hr = fp16(hin - A hout); t2 = z (w hr); hnew = fp16(hout + ome_c[k] t2); the
 // last step writes out = fp32(hnew) / sc instead.
-template <int K> struct EpiRichStepK {
+// MM: the diagonal preconditioner has one value per row and column, w[r * K + c]
+template <int K, bool MM = false> struct EpiRichStepK {
   const __half *hin, *hout;
   DiagPre M;
   const RichState *rs;  // K states
@@ -278,13 +313,15 @@ template <int K> struct EpiRichStepK {
   float isc;
   template <typename Acc> __device__ __forceinline__ void row(int64_t r, const Acc (&acc)[K]) const {
     float hi[K], ho[K], res[K];
+    __half w[MM ? K : 1], z[MM ? K : 1];
     RowK<__half, K>::load(hin + r * K, hi);
     RowK<__half, K>::load(hout + r * K, ho);
-    const __half w = M.w[r], z = M.z[r];
+    RowK<__half, MM ? K : 1>::load(M.w + r * (MM ? K : 1), w);
+    RowK<__half, MM ? K : 1>::load(M.z + r * (MM ? K : 1), z);
 #pragma unroll
     for (int c = 0; c < K; c++) {
       const __half hr = f2h(hi[c] - (float)acc[c]);
-      const __half t2 = __hmul(z, __hmul(w, hr));
+      const __half t2 = __hmul(z[MM ? c : 0], __hmul(w[MM ? c : 0], hr));
       res[c] = h2f(f2h(__fmaf_rn(h2f(rs[c].ome[k]), h2f(t2), ho[c])));
     }
     if (out) {
@@ -298,18 +335,19 @@ template <int K> struct EpiRichStepK {
 };
 
 // Residual step of an update call (diagonal M): hr and t2 = M hr stored
-template <int K> struct EpiRichResPreK {
+template <int K, bool MM = false> struct EpiRichResPreK {
   const __half *hin;
   DiagPre M;
   __half *hr, *t2;
   template <typename Acc> __device__ __forceinline__ void row(int64_t r, const Acc (&acc)[K]) const {
-    float hi[K], h[K], t[K];
+    float hi[K], h[K], t[K], w[MM ? K : 1], z[MM ? K : 1];
     RowK<__half, K>::load(hin + r * K, hi);
-    const float w = h2f(M.w[r]), z = h2f(M.z[r]);
+    RowK<__half, MM ? K : 1>::load(M.w + r * (MM ? K : 1), w);
+    RowK<__half, MM ? K : 1>::load(M.z + r * (MM ? K : 1), z);
 #pragma unroll
     for (int c = 0; c < K; c++) {
       h[c] = h2f(f2h(hi[c] - (float)acc[c]));
-      t[c] = z * h2f(f2h(w * h[c]));
+      t[c] = z[MM ? c : 0] * h2f(f2h(w[MM ? c : 0] * h[c]));
     }
     RowK<__half, K>::store(hr + r * K, h);
     RowK<__half, K>::store(t2 + r * K, t);
@@ -491,18 +529,21 @@ __global__ void __launch_bounds__(WARPS * 32) k_multidot_f32K(const float *__res
     float a[NQ];
 #pragma unroll
     for (int q = 0; q < NQ; q++) a[q] = 0.0f;
+    // the 4 rows of a thread, RG at a time as one contiguous run of RG * K values
+    constexpr int RG = (4 * K <= 16) ? 4 : 1, E = RG * K;
     for (int64_t q4 = tid; q4 < nq4; q4 += stride) {
 #pragma unroll
-      for (int e = 0; e < 4; e++) {
-        float wv[K];
-        RowK<float, K>::load(w + (4 * q4 + e) * K, wv);
+      for (int g = 0; g < 4 / RG; g++) {
+        const int64_t i0 = 4 * q4 + g * RG;
+        float wv[E];
+        RowK<float, E>::load(w + i0 * K, wv);
 #pragma unroll
         for (int v = 0; v < CV; v++) {
           if (k0 + v < nv) {
-            float vv[K];
-            RowK<float, K>::load(V.p[k0 + v] + (4 * q4 + e) * K, vv);
+            float vv[E];
+            RowK<float, E>::load(V.p[k0 + v] + i0 * K, vv);
 #pragma unroll
-            for (int c = 0; c < K; c++) a[v * K + c] = __fmaf_rn(wv[c], vv[c], a[v * K + c]);
+            for (int e = 0; e < E; e++) a[v * K + e % K] = __fmaf_rn(wv[e], vv[e], a[v * K + e % K]);
           }
         }
       }
@@ -551,32 +592,30 @@ __global__ void __launch_bounds__(WARPS * 32) k_cgs_updateK(T *__restrict__ w, C
   for (int c = 0; c < K; c++) part[c] = 0;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x, tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t nq = n / N;
+  // the N rows of a thread, RG at a time as one contiguous run of RG * K values
+  constexpr int RG = (N * K <= 16) ? N : 1, E = RG * K;
   for (int64_t q = tid; q < nq; q += stride) {
 #pragma unroll
-    for (int e = 0; e < N; e++) {
-      const int64_t i = q * N + e;
-      T a[K], r[K], wv[K];
-      RowK<T, K>::load(V.p[0] + i * K, a);
+    for (int g = 0; g < N / RG; g++) {
+      const int64_t i0 = q * N + g * RG;
+      T a[E], r[E], wv[E];
+      RowK<T, E>::load(V.p[0] + i0 * K, a);
 #pragma unroll
-      for (int c = 0; c < K; c++) r[c] = mul_rn(a[c], sh[c][0]);
+      for (int e = 0; e < E; e++) r[e] = mul_rn(a[e], sh[e % K][0]);
       for (int k = 1; k < nv; k++) {
-        T b[K];
-        RowK<T, K>::load(V.p[k] + i * K, b);
+        T b[E];
+        RowK<T, E>::load(V.p[k] + i0 * K, b);
 #pragma unroll
-        for (int c = 0; c < K; c++) r[c] = fmaT(b[c], sh[c][k], r[c]);
+        for (int e = 0; e < E; e++) r[e] = fmaT(b[e], sh[e % K][k], r[e]);
       }
-      RowK<T, K>::load(w + i * K, wv);
+      RowK<T, E>::load(w + i0 * K, wv);
+      // row by row, as the single-column kernel: update, then the squared norm
 #pragma unroll
-      for (int c = 0; c < K; c++) wv[c] = sub_rn(wv[c], r[c]);
-      RowK<T, K>::store(w + i * K, wv);
-    }
-    // the norm in the single-column kernel's order: element by element
-#pragma unroll
-    for (int e = 0; e < N; e++) {
-      T wv[K];
-      RowK<T, K>::load(w + (q * N + e) * K, wv);
-#pragma unroll
-      for (int c = 0; c < K; c++) part[c] = fmaT(wv[c], wv[c], part[c]);
+      for (int e = 0; e < E; e++) {
+        wv[e] = sub_rn(wv[e], r[e]);
+        part[e % K] = fmaT(wv[e], wv[e], part[e % K]);
+      }
+      RowK<T, E>::store(w + i0 * K, wv);
     }
   }
   for (int64_t i = nq * N + tid; i < n; i += stride) {
@@ -770,7 +809,34 @@ __global__ void k_zyK(Cols<T> Z, const T *__restrict__ y, int64_t y_stride, int 
 // normalisation of in(:, c) (in_inv[c], or none), hin = fp16(in * sc),
 // hout = M hin, times ome_c[0] on a call without a weight update; e_c(0) = 1
 // of the calling level when e_set is given.
-template <bool SCALE_BY_OME, int K>
+template <bool SCALE_BY_OME, int K, int NR, bool MM>
+__device__ __forceinline__ void rich_enter_rows(int64_t i0, float *__restrict__ in, bool normalise, const float (&s)[K],
+                                                const float (&om)[K], float sc, const DiagPre &M,
+                                                __half *__restrict__ hin, __half *__restrict__ hout) {
+  constexpr int E = NR * K, NM = MM ? E : NR;  // diagonal values: per row, or per row and column
+  float v[E], w[NM], z[NM];
+  __half hi[E], ho[E];
+  RowK<float, E>::load(in + i0 * K, v);
+  if (normalise) {
+#pragma unroll
+    for (int q = 0; q < E; q++) v[q] *= s[q % K];
+    RowK<float, E>::store(in + i0 * K, v);
+  }
+  RowK<__half, NM>::load(M.w + i0 * (MM ? K : 1), w);
+  RowK<__half, NM>::load(M.z + i0 * (MM ? K : 1), z);
+#pragma unroll
+  for (int q = 0; q < E; q++) {
+    hi[q] = f2h(v[q] * sc);
+    const float t = h2f(f2h(w[MM ? q : q / K] * h2f(hi[q])));
+    float o = h2f(f2h(z[MM ? q : q / K] * t));
+    if (SCALE_BY_OME) o = h2f(f2h(o * om[q % K]));
+    ho[q] = f2h(o);
+  }
+  RowK<__half, E>::store(hin + i0 * K, hi);
+  RowK<__half, E>::store(hout + i0 * K, ho);
+}
+
+template <bool SCALE_BY_OME, int K, bool MM = false>
 __global__ void k_rich_enter_diagK(float *__restrict__ in, const float *__restrict__ in_inv, float sc, DiagPre M,
                                    __half *__restrict__ hin, __half *__restrict__ hout,
                                    const RichState *__restrict__ rs, float *e_set, int64_t e_stride, int64_t n) {
@@ -781,29 +847,14 @@ __global__ void k_rich_enter_diagK(float *__restrict__ in, const float *__restri
     om[c] = SCALE_BY_OME ? h2f(rs[c].ome[0]) : 1.0f;
     s[c] = in_inv ? in_inv[c] : 1.0f;
   }
-  for_row_groups<RowsPer<K>::R>(n, [&](int64_t i0, auto rows) {
-    constexpr int NR = decltype(rows)::value, E = NR * K;
-    float v[E], hi[E], ho[E], w[NR], z[NR];
-    RowK<float, E>::load(in + i0 * K, v);
-    if (in_inv) {
-#pragma unroll
-      for (int q = 0; q < E; q++) v[q] *= s[q % K];
-      RowK<float, E>::store(in + i0 * K, v);
-    }
-    RowK<__half, NR>::load(M.w + i0, w);
-    RowK<__half, NR>::load(M.z + i0, z);
-#pragma unroll
-    for (int q = 0; q < E; q++) {
-      const __half h = f2h(v[q] * sc);
-      hi[q] = h2f(h);
-      const float t = h2f(f2h(w[q / K] * hi[q]));
-      float o = h2f(f2h(z[q / K] * t));
-      if (SCALE_BY_OME) o = h2f(f2h(o * om[q % K]));
-      ho[q] = o;
-    }
-    RowK<__half, E>::store(hin + i0 * K, hi);
-    RowK<__half, E>::store(hout + i0 * K, ho);
-  });
+  const bool normalise = in_inv != nullptr;
+  constexpr int R = RowsPer<K>::R;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x, tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t ng = n / R;
+  for (int64_t q = tid; q < ng; q += stride)
+    rich_enter_rows<SCALE_BY_OME, K, R, MM>(q * R, in, normalise, s, om, sc, M, hin, hout);
+  for (int64_t i = ng * R + tid; i < n; i += stride)
+    rich_enter_rows<SCALE_BY_OME, K, 1, MM>(i, in, normalise, s, om, sc, M, hin, hout);
 }
 
 // General M: (normalise in place), hin = fp16(in * sc) (k_rich_cast_in)

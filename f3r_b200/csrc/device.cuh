@@ -9,7 +9,7 @@
 namespace f3r {
 
 // Device-side error codes written to the context's error word.
-enum DevError : int { DEV_OK = 0, DEV_TIMEOUT_SPMV = 1, DEV_BREAKDOWN = 2, DEV_TIMEOUT_TRSV = 3 };
+enum DevError : int { DEV_OK = 0, DEV_TIMEOUT_SPMV = 1, DEV_BREAKDOWN = 2, DEV_TIMEOUT_TRSV = 3, DEV_TIMEOUT_MMA = 4 };
 
 // Threads per block of the elementwise / reduction kernels.
 constexpr int kEwThreads = 256;
@@ -123,6 +123,9 @@ template <> __device__ __forceinline__ __half cvt<__half>(float v) { return __fl
 template <> __device__ __forceinline__ float cvt<float>(double v) { return (float)v; }
 template <> __device__ __forceinline__ double cvt<double>(double v) { return v; }
 template <> __device__ __forceinline__ __half cvt<__half>(double v) { return __double2half(v); }
+template <typename To> __device__ __forceinline__ To cvt(__half v);
+template <> __device__ __forceinline__ __half cvt<__half>(__half v) { return v; }
+template <> __device__ __forceinline__ float cvt<float>(__half v) { return __half2float(v); }
 
 __device__ __forceinline__ float widen(float v) { return v; }
 __device__ __forceinline__ double widen(double v) { return v; }
@@ -131,6 +134,7 @@ __device__ __forceinline__ float widen(__half v) { return __half2float(v); }
 template <typename Acc> __device__ __forceinline__ Acc to_acc(double v) { return (Acc)v; }
 template <typename Acc> __device__ __forceinline__ Acc to_acc(float v) { return (Acc)v; }
 template <typename Acc> __device__ __forceinline__ Acc to_acc(__half v) { return (Acc)__half2float(v); }
+template <> __device__ __forceinline__ __half to_acc<__half>(__half v) { return v; }
 
 __device__ __forceinline__ float fmaT(float a, float b, float c) { return __fmaf_rn(a, b, c); }
 __device__ __forceinline__ double fmaT(double a, double b, double c) { return __fma_rn(a, b, c); }

@@ -27,8 +27,9 @@
 //              weight gradients as sums over the tile's rows into a shared
 //              accumulator, and adds that to the global gradient once
 //   Adam       one thread per parameter
-// Inference runs the same network in BF16 on tensor cores (mma.sync
-// m16n8k16, fp32 accumulation), one warp per 16-row tile, persistent CTAs.
+// Inference runs the same network in BF16 on the tensor cores with fp32
+// accumulation: tcgen05.mma with TMEM accumulators, one warpgroup per 128-row
+// tile (the default), or mma.sync m16n8k16, one warp per 16-row tile.
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -451,6 +452,239 @@ __global__ void __launch_bounds__(128) k_mlp_infer_bf16(int32_t n, const float *
   }
 }
 
+// ---- BF16 inference on the 5th-generation tensor cores (tcgen05) ----------
+// A warpgroup (128 threads) works one 128-row tile; a CTA holds two warpgroups
+// that share the staged weights and own 64 tensor-memory columns each.  Every
+// layer is a tcgen05.mma chain D[128 x N] = A[128 x K] . B[K x N] issued by one
+// thread, A (activations) and B (the weights, stored out x in = N x K) in
+// shared memory in the K-major no-swizzle canonical layout, D (fp32) in tensor
+// memory: row t of the tile is TMEM lane t, read back by thread t with
+// tcgen05.ld.  Layer 1: K 16 (the 7 inputs zero-padded), N 64; layer 2: K 64,
+// N 64; layer 3: K 64, N 16 (8 outputs and 8 zero weight rows).  The epilogue
+// of a layer adds the fp32 bias, applies relu and stores its row as bf16 into
+// the next layer's A, so the arithmetic is that of the mma.sync kernel above:
+// bf16 operands, fp32 accumulation, fp32 bias.
+//
+// Canonical K-major layout without swizzle: 8 x 8 bf16 core matrices of 128
+// contiguous bytes (row r % 8 at 16 r bytes); the K/8 core matrices of an
+// 8-row group follow each other at LBO = 128 bytes and the 8-row groups at
+// SBO = 16 K bytes.  One MMA instruction covers K = 16 (two core matrices), so
+// the k-th instruction of a chain starts 256 k bytes further.
+constexpr int kTcRows = 128;        // rows per tile: MMA M, TMEM lanes
+constexpr int kTcGroups = 2;        // warpgroups (tiles in flight) per CTA
+constexpr int kTcCols = 64;         // TMEM columns per warpgroup
+constexpr int kTcK1 = 16, kTcN3 = 16;
+constexpr uint32_t kTcW1 = kH * kTcK1 * 2, kTcW2 = kH * kH * 2, kTcW3 = kTcN3 * kH * 2;  // bytes
+constexpr uint32_t kTcA1 = kTcRows * kTcK1 * 2, kTcA2 = kTcRows * kH * 2;
+constexpr uint32_t kTcOffW2 = kTcW1, kTcOffW3 = kTcOffW2 + kTcW2, kTcOffA = kTcOffW3 + kTcW3;
+constexpr uint32_t kTcOffBias = kTcOffA + kTcGroups * (kTcA1 + kTcA2);
+constexpr uint32_t kTcOffBar = kTcOffBias + (2 * kH + kOut) * 4;
+constexpr size_t kTcSmem = kTcOffBar + kTcGroups * 8 + 16;
+// Four CTAs fill the 512 TMEM columns of an SM; a fifth never fits beside them
+// (shared memory), so no allocation waits on another CTA.
+constexpr int kTcCtasPerSm = 4;
+static_assert(kTcCtasPerSm * kTcGroups * kTcCols == 512, "TMEM columns of an SM");
+static_assert((kTcCtasPerSm + 1) * (kTcSmem + 1024) > 228 * 1024, "a fifth CTA would fit on an SM");
+static_assert(kTcOffA % 128 == 0 && kTcA1 % 128 == 0 && kTcOffBar % 8 == 0, "operand alignment");
+
+// byte offset of element (r, k) of a K-major no-swizzle operand with K columns
+__host__ __device__ constexpr uint32_t kmaj_off(int r, int k, int K) {
+  return (uint32_t)((r >> 3) * (K * 16) + (k >> 3) * 128 + (r & 7) * 16 + (k & 7) * 2);
+}
+// shared-memory matrix descriptor (tcgen05): start address, LBO, SBO (all
+// >> 4), version 1 (bits 46-47), base offset 0, no swizzle (bits 61-63 = 0)
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((saddr & 0x3FFFFu) >> 4) | ((uint64_t)(lbo >> 4) << 16) | ((uint64_t)(sbo >> 4) << 32) |
+         (1ull << 46);
+}
+// instruction descriptor, kind::f16: fp32 D (bits 4-5 = 1), bf16 A and B (bits
+// 7-9, 10-12 = 1), both K-major, N >> 3 at bit 17, M >> 4 at bit 24
+__host__ __device__ constexpr uint32_t umma_idesc_bf16(int M, int N) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+__device__ __forceinline__ void umma_bf16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accum) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+      "l"(a), "l"(b), "r"(idesc), "r"(accum)
+      : "memory");
+}
+// arrives once on bar when every MMA this thread issued before it completes
+__device__ __forceinline__ void umma_commit(uint64_t *bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+// 16 consecutive fp32 columns of this thread's TMEM lane; the wait takes the
+// registers as operands, so no use of them is scheduled before it
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;"
+               : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]),
+                 "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]), "+r"(r[14]), "+r"(r[15])
+               :
+               : "memory");
+#pragma unroll
+  for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+}
+// barrier over one warpgroup (named barrier id) that also ANDs a flag
+__device__ __forceinline__ bool group_sync_and(int id, bool ok) {
+  uint32_t out;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\tsetp.ne.b32 p, %1, 0;\n\t"
+      "bar.red.and.pred q, %2, 128, p;\n\tselp.u32 %0, 1, 0, q;\n\t}"
+      : "=r"(out)
+      : "r"((uint32_t)ok), "r"(id)
+      : "memory");
+  return out != 0;
+}
+// relu(acc + bias) of 16 columns of a row, stored as bf16 at A2 columns c0..c0+15
+__device__ __forceinline__ void tc_epilogue16(unsigned char *a2, int row, int c0, const float (&v)[16],
+                                              const float *bias) {
+  uint32_t p[8];
+#pragma unroll
+  for (int i = 0; i < 8; i++) p[i] = pack_bf16(relu(v[2 * i] + bias[c0 + 2 * i]), relu(v[2 * i + 1] + bias[c0 + 2 * i + 1]));
+  *reinterpret_cast<uint4 *>(a2 + kmaj_off(row, c0, kH)) = make_uint4(p[0], p[1], p[2], p[3]);
+  *reinterpret_cast<uint4 *>(a2 + kmaj_off(row, c0 + 8, kH)) = make_uint4(p[4], p[5], p[6], p[7]);
+}
+
+__global__ void __launch_bounds__(kTcRows * kTcGroups, kTcCtasPerSm)
+    k_mlp_infer_tc(int32_t n, const float *__restrict__ f, const float *__restrict__ p, float *__restrict__ o,
+                   int *err) {
+  extern __shared__ __align__(1024) unsigned char tcs[];
+  float *b1s = reinterpret_cast<float *>(tcs + kTcOffBias), *b2s = b1s + kH, *b3s = b2s + kH;
+  uint64_t *bars = reinterpret_cast<uint64_t *>(tcs + kTcOffBar);
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(tcs + kTcOffBar + kTcGroups * 8);
+  const int tid = threadIdx.x & (kTcRows - 1), g = threadIdx.x / kTcRows, warp = threadIdx.x >> 5;
+  // weights (bf16, canonical layout; the padding rows and columns zero) and biases
+  for (int q = threadIdx.x; q < kH * kTcK1; q += blockDim.x) {
+    const int j = q / kTcK1, c = q % kTcK1;
+    *reinterpret_cast<__nv_bfloat16 *>(tcs + kmaj_off(j, c, kTcK1)) =
+        __float2bfloat16_rn(c < kIn ? p[oW1 + j * kIn + c] : 0.f);
+  }
+  for (int q = threadIdx.x; q < kH * kH; q += blockDim.x) {
+    const int j = q / kH, c = q % kH;
+    *reinterpret_cast<__nv_bfloat16 *>(tcs + kTcOffW2 + kmaj_off(j, c, kH)) = __float2bfloat16_rn(p[oW2 + q]);
+  }
+  for (int q = threadIdx.x; q < kTcN3 * kH; q += blockDim.x) {
+    const int s = q / kH, c = q % kH;
+    *reinterpret_cast<__nv_bfloat16 *>(tcs + kTcOffW3 + kmaj_off(s, c, kH)) =
+        __float2bfloat16_rn(s < kOut ? p[oW3 + s * kH + c] : 0.f);
+  }
+  for (int q = threadIdx.x; q < kH; q += blockDim.x) {
+    b1s[q] = p[oB1 + q];
+    b2s[q] = p[oB2 + q];
+  }
+  if (threadIdx.x < kOut) b3s[threadIdx.x] = p[oB3 + threadIdx.x];
+  unsigned char *a1 = tcs + kTcOffA + g * (kTcA1 + kTcA2), *a2 = a1 + kTcA1;
+  // columns 8..15 of A1 stay zero
+  *reinterpret_cast<uint4 *>(a1 + kmaj_off(tid, 8, kTcK1)) = make_uint4(0, 0, 0, 0);
+  if (threadIdx.x == 0) {
+    for (int q = 0; q < kTcGroups; q++) mbar_init(&bars[q], 1);
+    fence_mbar_init();
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(kTcCols * kTcGroups)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  fence_proxy_async_smem();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot + g * kTcCols;     // this warpgroup's columns, lane 0
+  const uint32_t lane_addr = tmem + ((uint32_t)((warp & 3) * 32) << 16);  // this warp's 32 lanes
+  const uint32_t sa1 = smem_u32(a1), sa2 = smem_u32(a2), sw = smem_u32(tcs);
+  const uint64_t dA1 = umma_desc(sa1, 128, kTcK1 * 16), dW1 = umma_desc(sw, 128, kTcK1 * 16);
+  const uint64_t dA2 = umma_desc(sa2, 128, kH * 16), dW2 = umma_desc(sw + kTcOffW2, 128, kH * 16),
+                 dW3 = umma_desc(sw + kTcOffW3, 128, kH * 16);
+  constexpr uint32_t i64 = umma_idesc_bf16(kTcRows, kH), i16 = umma_idesc_bf16(kTcRows, kTcN3);
+  const bool issuer = tid == 0;
+  const int bar_id = 1 + g;
+  uint32_t phase = 0;
+  bool ok = true, pending = false;
+  const int64_t ntiles = (n + kTcRows - 1) / kTcRows, stride = (int64_t)gridDim.x * kTcGroups;
+  int64_t tile = (int64_t)blockIdx.x * kTcGroups + g;
+  float fx[kIn];
+  auto fetch = [&](int64_t t) {
+    const int64_t r = t * kTcRows + tid;
+#pragma unroll
+    for (int c = 0; c < kIn; c++) fx[c] = (t < ntiles && r < n) ? f[r * kIn + c] : 0.f;
+  };
+  fetch(tile);
+  // one MMA chain: issue, commit, and the warpgroup's wait for its completion
+  auto chain = [&](auto issue) -> bool {
+    fence_proxy_async_smem();
+    tc_fence_before();
+    group_sync_and(bar_id, true);
+    if (issuer) {
+      tc_fence_after();
+      issue();
+      umma_commit(&bars[g]);
+    }
+    pending = true;
+    const bool done = mbar_wait_bounded(&bars[g], phase);
+    if (!group_sync_and(bar_id, done)) return false;
+    phase ^= 1u;
+    pending = false;
+    tc_fence_after();
+    return true;
+  };
+#pragma unroll 1
+  for (; tile < ntiles; tile += stride) {
+    *reinterpret_cast<uint4 *>(a1 + kmaj_off(tid, 0, kTcK1)) =
+        make_uint4(pack_bf16(fx[0], fx[1]), pack_bf16(fx[2], fx[3]), pack_bf16(fx[4], fx[5]), pack_bf16(fx[6], 0.f));
+    fetch(tile + stride);  // the next tile's rows, in flight behind this tile's chains
+    if (!(ok = chain([&] { umma_bf16(tmem, dA1, dW1, i64, 0); }))) break;
+#pragma unroll
+    for (int q = 0; q < kH / 16; q++) {
+      float v[16];
+      tmem_ld16(lane_addr + q * 16, v);
+      tc_epilogue16(a2, tid, q * 16, v, b1s);
+    }
+    if (!(ok = chain([&] {
+            for (int k = 0; k < kH / 16; k++) umma_bf16(tmem, dA2 + 16 * k, dW2 + 16 * k, i64, k > 0);
+          })))
+      break;
+#pragma unroll
+    for (int q = 0; q < kH / 16; q++) {
+      float v[16];
+      tmem_ld16(lane_addr + q * 16, v);
+      tc_epilogue16(a2, tid, q * 16, v, b2s);
+    }
+    if (!(ok = chain([&] {
+            for (int k = 0; k < kH / 16; k++) umma_bf16(tmem, dA2 + 16 * k, dW3 + 16 * k, i16, k > 0);
+          })))
+      break;
+    float y[16];
+    tmem_ld16(lane_addr, y);
+    const int64_t r = tile * kTcRows + tid;
+    if (r < n) {
+      float4 *dst = reinterpret_cast<float4 *>(o + r * kOut);
+      dst[0] = make_float4(y[0] + b3s[0], y[1] + b3s[1], y[2] + b3s[2], y[3] + b3s[3]);
+      dst[1] = make_float4(y[4] + b3s[4], y[5] + b3s[5], y[6] + b3s[6], y[7] + b3s[7]);
+    }
+  }
+  if (!ok) {
+    if (tid == 0) atomicExch(err, (int)DEV_TIMEOUT_MMA);
+    if (pending) mbar_wait_bounded(&bars[g], phase);  // the chain still in flight (bounded)
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(*tmem_slot), "r"(kTcCols * kTcGroups)
+                 : "memory");
+  }
+}
+
 // slot of every entry: the index of (col - row) in the factor's offset list, or -1
 std::vector<int32_t> slots(const f3r_csr &m, const int32_t (&offs)[4]) {
   std::vector<int32_t> s(m.nnz, -1);
@@ -538,11 +772,17 @@ struct f3r_learned {
 
 namespace {
 
-// forward pass and corrected factors of a loaded system
-Status forward(Context &c, const float *params, SysDev &s, bool bf16) {
+// forward pass and corrected factors of a loaded system; mode 0: the fp32
+// training forward pass, 1: BF16 inference on tcgen05, 2: BF16 inference on
+// mma.sync
+Status forward(Context &c, const float *params, SysDev &s, int mode) {
   if (s.n == 0) return F3R_SUCCESS;
   // inference: a persistent grid, each CTA staging the weights once
-  if (bf16)
+  if (mode == 1) {
+    const int64_t tiles = cdiv(s.n, kTcRows);
+    launch_k(c, k_mlp_infer_tc, (int)std::min<int64_t>(cdiv(tiles, kTcGroups), (int64_t)c.sm_count * kTcCtasPerSm),
+             kTcRows * kTcGroups, kTcSmem, c.stream, s.n, (const float *)s.feat, params, s.out, c.err);
+  } else if (mode == 2)
     launch_k(c, k_mlp_infer_bf16, (int)std::min<int64_t>(cdiv(s.n, 64), (int64_t)c.sm_count * 8), 128, 0, c.stream,
              s.n, (const float *)s.feat, params, s.out);
   else
@@ -560,7 +800,7 @@ Status forward(Context &c, const float *params, SysDev &s, bool bf16) {
 Status loss_and_grad(f3r_learned *L, double *loss_d, bool want_grad) {
   Context &c = *L->ctx;
   SysDev &s = L->train;
-  F3R_TRY(forward(c, L->p, s, false));
+  F3R_TRY(forward(c, L->p, s, 0));
   const int32_t n = s.n, P = s.npairs;
   const dim3 grid((unsigned)cdiv(n, 256), (unsigned)P);
   launch_k(c, k_csr_mv, grid, 256, 0, c.stream, n, (const int32_t *)s.wr, (const int32_t *)s.wi,
@@ -605,6 +845,7 @@ f3r_status f3r_learned_create(f3r_context *ctx, int32_t hidden, uint64_t seed, f
   CUDA_TRY(cudaMemcpy(L->p, p.data(), sizeof(float) * kParams, cudaMemcpyHostToDevice));
   for (float *b : {L->g, L->m, L->v}) CUDA_TRY(cudaMemset(b, 0, sizeof(float) * kParams));
   CUDA_TRY(cudaFuncSetAttribute(k_mlp_backward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBackSmem));
+  CUDA_TRY(cudaFuncSetAttribute(k_mlp_infer_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
   int per_sm = 0;
   CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mlp_backward, kRows, kBackSmem));
   L->grid_back = std::max(1, per_sm) * c.sm_count;
@@ -727,7 +968,9 @@ f3r_status f3r_learned_correct(f3r_learned *L, const f3r_csr *a, int32_t nx, int
   Context &c = *L->ctx;
   SysDev s;
   Status st = load_system(c, s, a, nx, ny, z, wt);
-  if (st == F3R_SUCCESS) st = forward(c, L->p, s, bf16 != 0);
+  if (st == F3R_SUCCESS && (bf16 < 0 || bf16 > 2)) st = fail(F3R_ERROR_INVALID_VALUE, "bf16 must be 0, 1 or 2");
+  if (st == F3R_SUCCESS) st = forward(c, L->p, s, bf16);
+  if (st == F3R_SUCCESS && bf16 == 1) st = c.check_device_error();
   cudaError_t ce = cudaSuccess;
   if (st == F3R_SUCCESS && s.n > 0) {
     ce = cudaMemcpyAsync(z_val, s.zc, sizeof(double) * s.znnz, cudaMemcpyDeviceToHost, c.stream);
@@ -737,6 +980,51 @@ f3r_status f3r_learned_correct(f3r_learned *L, const f3r_csr *a, int32_t nx, int
   }
   if (ce == cudaSuccess) ce = cudaStreamSynchronize(c.stream);
   if (st == F3R_SUCCESS && ce != cudaSuccess) st = fail(F3R_ERROR_CUDA, cudaGetErrorString(ce));
+  cudaStreamSynchronize(c.stream);
+  s.release();
+  return st;
+}
+
+f3r_status f3r_learned_time_inference(f3r_learned *L, const f3r_csr *a, int32_t nx, int32_t ny, const f3r_csr *z,
+                                      const f3r_csr *wt, int32_t mode, int32_t reps, double *us) {
+  if (!L || !a || !z || !wt || !us) return fail(F3R_ERROR_INVALID_VALUE, "null argument");
+  if (mode < 0 || mode > 2 || reps < 1) return fail(F3R_ERROR_INVALID_VALUE, "mode must be 0, 1 or 2 and reps >= 1");
+  CUDA_TRY(cudaSetDevice(L->ctx->device));
+  Context &c = *L->ctx;
+  SysDev s;
+  Status st = load_system(c, s, a, nx, ny, z, wt);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (st == F3R_SUCCESS && (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess))
+    st = fail(F3R_ERROR_CUDA, "cudaEventCreate");
+  // the network alone: one warm-up launch, then reps launches between events
+  auto net = [&]() -> Status {
+    if (s.n == 0) return F3R_SUCCESS;
+    if (mode == 1) {
+      const int64_t tiles = cdiv(s.n, kTcRows);
+      launch_k(c, k_mlp_infer_tc, (int)std::min<int64_t>(cdiv(tiles, kTcGroups), (int64_t)c.sm_count * kTcCtasPerSm),
+               kTcRows * kTcGroups, kTcSmem, c.stream, s.n, (const float *)s.feat, (const float *)L->p, s.out, c.err);
+    } else if (mode == 2)
+      launch_k(c, k_mlp_infer_bf16, (int)std::min<int64_t>(cdiv(s.n, 64), (int64_t)c.sm_count * 8), 128, 0,
+               c.stream, s.n, (const float *)s.feat, (const float *)L->p, s.out);
+    else
+      launch_k(c, k_mlp_forward, (int)cdiv(s.n, kRows), kRows, 0, c.stream, s.n, (const float *)s.feat,
+               (const float *)L->p, s.out);
+    CUDA_TRY(cudaGetLastError());
+    return F3R_SUCCESS;
+  };
+  if (st == F3R_SUCCESS) st = net();
+  if (st == F3R_SUCCESS && cudaEventRecord(e0, c.stream) != cudaSuccess) st = fail(F3R_ERROR_CUDA, "cudaEventRecord");
+  for (int32_t k = 0; st == F3R_SUCCESS && k < reps; k++) st = net();
+  if (st == F3R_SUCCESS && cudaEventRecord(e1, c.stream) != cudaSuccess) st = fail(F3R_ERROR_CUDA, "cudaEventRecord");
+  if (st == F3R_SUCCESS && cudaEventSynchronize(e1) != cudaSuccess) st = fail(F3R_ERROR_CUDA, "cudaEventSynchronize");
+  float ms = 0.f;
+  if (st == F3R_SUCCESS) {
+    cudaEventElapsedTime(&ms, e0, e1);
+    *us = 1e3 * ms / reps;
+  }
+  if (st == F3R_SUCCESS && mode == 1) st = c.check_device_error();
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
   cudaStreamSynchronize(c.stream);
   s.release();
   return st;

@@ -64,6 +64,8 @@ struct Context {
     if (e == DEV_TIMEOUT_SPMV) return fail(F3R_ERROR_TIMEOUT, "a bulk-copy wait in the SpMV kernel exceeded its bound");
     if (e == DEV_TIMEOUT_TRSV)
       return fail(F3R_ERROR_TIMEOUT, "a dependency wait in the level-scheduled ILU solve exceeded its bound");
+    if (e == DEV_TIMEOUT_MMA)
+      return fail(F3R_ERROR_TIMEOUT, "a tensor-core completion wait in the MLP inference exceeded its bound");
     return fail(F3R_ERROR_BREAKDOWN, "zero or non-finite norm in an Arnoldi step");
   }
 };
@@ -85,6 +87,7 @@ struct DeviceSell {
   int32_t *col = nullptr, *sptr = nullptr, *perm = nullptr, *cbase = nullptr, *cbptr = nullptr;
   int32_t *xoff = nullptr;  // mixed aligned form: per slice, -1 or the explicit indices' offset
   int32_t *rptr = nullptr;  // CSR storage (col = CSR indices, values unpadded), else nullptr
+  int32_t height = 32;      // slice height: 32, or 64 (64-row aligned slices)
   uint16_t *dcol = nullptr;
   double *v64 = nullptr;
   float *v32 = nullptr;
@@ -92,7 +95,7 @@ struct DeviceSell {
   int dtypes = 0;
   // 32, 16, or 0 (offset-aligned slices, mixed with explicit ones or not)
   int index_bits() const { return (xoff || (cbase && !dcol)) ? 0 : dcol ? 16 : 32; }
-  DevSell view() const { return DevSell{col, dcol, cbase, cbptr, xoff, sptr, perm, n, ncols, nslices, rptr}; }
+  DevSell view() const { return DevSell{col, dcol, cbase, cbptr, xoff, sptr, perm, n, ncols, nslices, rptr, height}; }
   void release() {
     cudaFree(col); cudaFree(sptr); cudaFree(perm); cudaFree(cbase); cudaFree(cbptr); cudaFree(dcol);
     cudaFree(xoff);
@@ -127,6 +130,9 @@ inline Status sell_attr(Context &c) {
     F3R_TRY((sell_attr_one<V, X, Epi, AllAlignedIdx>()));
     CUDA_TRY(cudaFuncSetAttribute(k_csr_cfg<V, X, Epi, SellCfg<V, int32_t>::WARPS>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csr_smem_bytes<V>()));
+    using C64 = Sell64Cfg<V>;
+    CUDA_TRY(cudaFuncSetAttribute(k_sell64<V, X, Epi, C64::WARPS, C64::STAGES, C64::KC>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sell64_smem_bytes<V>()));
     attr_done[c.device & 63] = 1;
   }
   return F3R_SUCCESS;
@@ -144,7 +150,12 @@ template <typename V, typename X, typename Epi>
 inline Status launch_sell(Context &c, const V *val, const DevSell &A, const X *x, const Epi &epi) {
   if (A.nslices == 0) return F3R_SUCCESS;
   F3R_TRY((sell_attr<V, X, Epi>(c)));
-  if (A.rptr) {
+  if (A.height == 64) {
+    using C64 = Sell64Cfg<V>;
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(cdiv(A.nslices, C64::WARPS), c.sm_count));
+    launch_k(c, k_sell64<V, X, Epi, C64::WARPS, C64::STAGES, C64::KC>, grid, C64::WARPS * 32, sell64_smem_bytes<V>(),
+             c.stream, val, A, x, epi, c.err);
+  } else if (A.rptr) {
     // the packed kernel's geometry (rows per thread, CTAs), so sums and partials match it
     constexpr int W = SellCfg<V, int32_t>::WARPS;
     const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(cdiv(A.nslices, W), c.sm_count));
@@ -170,6 +181,7 @@ struct SellHost {
   std::vector<int32_t> cbptr;            // nslices + 1, multiples of 4 (aligned forms: bit 0 = clamp)
   std::vector<int32_t> xoff;             // mixed aligned form: per slice, -1 or explicit offset
   bool aligned_all = false;              // fully aligned form (no explicit index at all)
+  int32_t height = 32;                   // slice height (64: align64's 64-row slices)
 };
 
 // Rows sorted by decreasing length in windows of sigma (renumber: columns
@@ -183,6 +195,10 @@ bool compress_index16(SellHost &s);
 // the slice's width), otherwise the mixed form.  Returns the fraction of
 // slices aligned, or -1 when the padded matrix would exceed 2^31 entries.
 double align_offsets(const f3r_csr &a, bool renumber, SellHost &s);
+// 64-row fully aligned slices of a (rows in their natural order): true when
+// every 64-row slice's rows share their column offsets (offset set at most
+// 5/4 of the slice's width), false otherwise (s untouched).
+bool align64(const f3r_csr &a, SellHost &s);
 // Uploads the value copies selected by dtype_mask (bit 1 << f3r_dtype).
 Status upload_sell(Context &c, const SellHost &h, int dtype_mask, bool scatter_perm, DeviceSell &d);
 // CSR storage with the same value copies (the kernels' CSR path; sigma 1)

@@ -66,6 +66,7 @@ struct DevSell {
   int32_t ncols;
   int32_t nslices;
   const int32_t *rptr;    // CSR storage: row pointers (col holds the CSR indices), else nullptr
+  int32_t height;         // slice height: 32, or 64 (64-row aligned slices, k_sell64)
 };
 
 // Index form of a kernel instantiation.
@@ -378,6 +379,216 @@ __global__ void __launch_bounds__(WARPS * 32, 1)
   if (!ok) {
     if (lane == 0) atomicExch(err, (int)DEV_TIMEOUT_SPMV);
     // let the copies still in flight into this warp's buffers land (bounded)
+    for (int i = 0; i < inflight; i++) {
+      mbar_wait_bounded(&bars[cst], (phase >> cst) & 1u);
+      phase ^= 1u << cst;
+      cst = (cst + 1 == STAGES) ? 0 : cst + 1;
+    }
+  }
+  epi.template finish<WARPS>(dots);
+}
+
+// ---------------------------------------------------------------------------
+// 64-row offset-aligned slices (slice height 64, f3r_params.sell_c = 64).
+// Every slice is offset-aligned (the fully aligned form): slot k of slice s
+// holds, for each of its 64 rows, the entry at column offset D_k, its column
+// cbase[k] + row-in-slice; a chunk of up to kAllAlignedChunk slots stores
+// each row's values contiguously (row-major over the 64 rows).  Lane l works
+// rows l and l + 32 of a slice: both rows read one set of slot bases, their
+// gathers share one address (the second is 32 elements further), and the
+// lane keeps two independent multiply-add chains.  Sums are formed in slot
+// order, the order of the 32-row aligned layout: the results are bit for bit
+// those of every other layout.
+// ---------------------------------------------------------------------------
+template <typename V> struct Sell64Cfg;
+template <> struct Sell64Cfg<__half> { static constexpr int WARPS = 24, STAGES = 2, KC = 32; };
+// a stage holds a 64-row x 32-column chunk: the warps x stages products fill
+// up to ~200 KB of the 227 KB a block may hold
+template <> struct Sell64Cfg<float> { static constexpr int WARPS = 12, STAGES = 2, KC = 32; };
+template <> struct Sell64Cfg<double> { static constexpr int WARPS = 6, STAGES = 2, KC = 32; };
+
+template <typename V, int WARPS, int STAGES, int KC> constexpr size_t sell64_smem_bytes_cfg() {
+  return (size_t)WARPS * STAGES * ((size_t)KC * 64 * sizeof(V) + KC * 4) + (size_t)WARPS * STAGES * sizeof(uint64_t);
+}
+template <typename V> constexpr size_t sell64_smem_bytes() {
+  return sell64_smem_bytes_cfg<V, Sell64Cfg<V>::WARPS, Sell64Cfg<V>::STAGES, Sell64Cfg<V>::KC>();
+}
+static_assert(sell64_smem_bytes<__half>() <= 227 * 1024 && sell64_smem_bytes<float>() <= 227 * 1024 &&
+                  sell64_smem_bytes<double>() <= 227 * 1024,
+              "a 64-row launch shape exceeds the shared memory of a block");
+
+template <typename V, typename X, typename Epi, int WARPS, int STAGES, int KC>
+__global__ void __launch_bounds__(WARPS * 32, 1)
+    k_sell64(const V *__restrict__ val, DevSell A, const X *__restrict__ x, Epi epi, int *err) {
+  using Acc = typename acc_of<V>::type;
+  static_assert(KC == kAllAlignedChunk, "64-row aligned layout is built for kAllAlignedChunk columns");
+  constexpr uint32_t VB = KC * 64 * sizeof(V), BB = KC * 4, SB = VB + BB;
+  // slots per pipelined sub-block: 8, or 4 where the launch leaves under ~100 registers a thread
+  constexpr int SUB = ((sizeof(V) == 2 && WARPS > 20) || (sizeof(V) >= 4 && WARPS > 16)) ? 4 : 8;
+  extern __shared__ __align__(128) unsigned char smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  unsigned char *buf = smem + (size_t)warp * STAGES * SB;
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem + (size_t)WARPS * STAGES * SB) + warp * STAGES;
+  if (lane == 0) {
+#pragma unroll
+    for (int s = 0; s < STAGES; s++) mbar_init(&bars[s], 1);
+    fence_mbar_init();
+  }
+  __syncwarp();
+  const uint64_t pol = l2_evict_first_policy();
+  const int TW = gridDim.x * WARPS;
+  int fs = blockIdx.x * WARPS + warp, fk = 0, fst = 0, inflight = 0;
+  int fs0 = 0, fw = 0, fcb = 0;
+  auto fetch = [&]() {
+    while (inflight < STAGES && fs < A.nslices) {
+      if (fk == 0) {
+        fs0 = A.sptr[fs];
+        fw = A.sptr[fs + 1] - fs0;
+        fcb = A.cbptr[fs] & ~3;
+      }
+      if (fw == 0) {
+        fs += TW;
+        fk = 0;
+        continue;
+      }
+      const int kc = min(KC, fw - fk);
+      if (lane == 0) {
+        const size_t off = ((size_t)fs0 + fk) * 64;
+        fence_proxy_async_smem();
+        const uint32_t vb = (uint32_t)kc * 64u * (uint32_t)sizeof(V), bb = (uint32_t)((kc + 3) & ~3) * 4u;
+        mbar_arrive_expect_tx(&bars[fst], vb + bb);
+        bulk_g2s(buf + (size_t)fst * SB, val + off, vb, &bars[fst], pol);
+        bulk_g2s(buf + (size_t)fst * SB + VB, A.cbase + fcb + fk, bb, &bars[fst], pol);
+      }
+      fst = (fst + 1 == STAGES) ? 0 : fst + 1;
+      inflight++;
+      fk += kc;
+      if (fk >= fw) {
+        fk = 0;
+        fs += TW;
+      }
+    }
+  };
+  auto release = [&]() {
+    __syncwarp();
+    inflight--;
+    fetch();
+  };
+  fetch();
+
+  typename Epi::Red dots[Epi::NV > 0 ? Epi::NV : 1];
+#pragma unroll
+  for (int k = 0; k < (Epi::NV > 0 ? Epi::NV : 1); k++) dots[k] = 0;
+  int cs = blockIdx.x * WARPS + warp, ck = 0, cst = 0;
+  uint32_t phase = 0;
+  bool ok = true;
+  Acc acc0 = 0, acc1 = 0;
+  typename Epi::Pre pre0{}, pre1{};
+  int w = 0;
+  bool clampc = false;
+  const X *xl = x + lane;
+  while (cs < A.nslices) {
+    if (ck == 0) {
+      w = A.sptr[cs + 1] - A.sptr[cs];
+      clampc = (A.cbptr[cs] & 1) != 0;
+    }
+    const int64_t r0 = (int64_t)cs * 64 + lane, r1 = r0 + 32;
+    const bool live0 = r0 < A.n, live1 = r1 < A.n;
+    if (w == 0) {
+      if (live0) {
+        pre0 = epi.load(r0);
+        epi.row(r0, Acc(0), pre0, dots);
+      }
+      if (live1) {
+        pre1 = epi.load(r1);
+        epi.row(r1, Acc(0), pre1, dots);
+      }
+      cs += TW;
+      continue;
+    }
+    if (ck == 0) {  // epilogue operands, ahead of the chains
+      if (live0) pre0 = epi.load(r0);
+      if (live1) pre1 = epi.load(r1);
+    }
+    const int kc = min(KC, w - ck);
+    if (!mbar_wait_bounded(&bars[cst], (phase >> cst) & 1u)) {
+      ok = false;
+      break;
+    }
+    phase ^= 1u << cst;
+    const V *sv = reinterpret_cast<const V *>(buf + (size_t)cst * SB);
+    const int32_t *sb = reinterpret_cast<const int32_t *>(buf + (size_t)cst * SB + VB);
+    cst = (cst + 1 == STAGES) ? 0 : cst + 1;
+    const bool full = kc == KC;
+    const V *lv0 = sv + lane * kc, *lv1 = sv + (lane + 32) * kc;  // the two rows' values (kc a multiple of 4)
+    const int nsub = (kc + SUB - 1) / SUB;
+    constexpr int NS = KC / SUB;
+    V vb0[2][SUB], vb1[2][SUB];
+    Acc xb0[2][SUB], xb1[2][SUB];
+    auto load_sub = [&](int h, V (&v0)[SUB], V (&v1)[SUB], Acc (&g0)[SUB], Acc (&g1)[SUB]) {
+#pragma unroll
+      for (int g = 0; g < SUB / 4; g++) {
+        const int k0 = h * SUB + g * 4;
+        if (full || k0 < kc) {
+          V t0[4], t1[4];
+          Vec4Load<V>::ld(lv0 + k0, t0);
+          Vec4Load<V>::ld(lv1 + k0, t1);
+          const int4 q = *reinterpret_cast<const int4 *>(sb + k0);
+          const int32_t b[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+          for (int e = 0; e < 4; e++) {
+            v0[g * 4 + e] = t0[e];
+            v1[g * 4 + e] = t1[e];
+          }
+          if (!clampc) {
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+              const X *px = xl + b[e];
+              g0[g * 4 + e] = to_acc<Acc>(__ldg(px));
+              g1[g * 4 + e] = to_acc<Acc>(__ldg(px + 32));
+            }
+          } else {
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+              g0[g * 4 + e] = to_acc<Acc>(__ldg(x + min(max(b[e] + lane, 0), A.ncols - 1)));
+              g1[g * 4 + e] = to_acc<Acc>(__ldg(x + min(max(b[e] + lane + 32, 0), A.ncols - 1)));
+            }
+          }
+        }
+      }
+    };
+    load_sub(0, vb0[0], vb1[0], xb0[0], xb1[0]);
+    if (nsub == 1) release();
+#pragma unroll
+    for (int h = 0; h < NS; h++) {
+      if (h < nsub) {
+        if (h + 1 < NS && h + 1 < nsub) {
+          load_sub(h + 1, vb0[(h + 1) & 1], vb1[(h + 1) & 1], xb0[(h + 1) & 1], xb1[(h + 1) & 1]);
+          if (h + 2 == nsub) release();
+        }
+#pragma unroll
+        for (int g = 0; g < SUB / 4; g++)
+          if (full || h * SUB + g * 4 < kc) {
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+              acc0 = fmaT(to_acc<Acc>(vb0[h & 1][g * 4 + e]), xb0[h & 1][g * 4 + e], acc0);
+              acc1 = fmaT(to_acc<Acc>(vb1[h & 1][g * 4 + e]), xb1[h & 1][g * 4 + e], acc1);
+            }
+          }
+      }
+    }
+    ck += kc;
+    if (ck >= w) {
+      if (live0) epi.row(r0, acc0, pre0, dots);
+      if (live1) epi.row(r1, acc1, pre1, dots);
+      acc0 = 0;
+      acc1 = 0;
+      ck = 0;
+      cs += TW;
+    }
+  }
+  if (!ok) {
+    if (lane == 0) atomicExch(err, (int)DEV_TIMEOUT_SPMV);
     for (int i = 0; i < inflight; i++) {
       mbar_wait_bounded(&bars[cst], (phase >> cst) & 1u);
       phase ^= 1u << cst;

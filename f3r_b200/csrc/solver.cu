@@ -196,6 +196,82 @@ double align_offsets(const f3r_csr &a, bool renumber, SellHost &s) {
   return ns ? (double)na / ns : 0.0;
 }
 
+bool align64(const f3r_csr &a, SellHost &s) {
+  const int32_t n = a.nrows, nc = a.ncols, ns = (int32_t)cdiv(n, 64);
+  std::vector<std::vector<int32_t>> D(ns);
+  std::vector<char> in_range(ns, 1);
+  int64_t not_ok = 0;
+#pragma omp parallel for schedule(dynamic, 256) reduction(+ : not_ok)
+  for (int32_t sl = 0; sl < ns; sl++) {
+    std::vector<int32_t> d;
+    int32_t wstd = 0;
+    for (int32_t q = 0; q < 64; q++) {
+      const int64_t r = (int64_t)sl * 64 + q;
+      if (r >= n) break;
+      wstd = std::max(wstd, a.rptr[r + 1] - a.rptr[r]);
+      for (int32_t e = a.rptr[r]; e < a.rptr[r + 1]; e++) d.push_back(a.idx[e] - (int32_t)r);
+    }
+    std::sort(d.begin(), d.end());
+    d.erase(std::unique(d.begin(), d.end()), d.end());
+    if (d.empty() || (int64_t)d.size() * 4 > (int64_t)wstd * 5) {
+      not_ok++;
+      continue;
+    }
+    in_range[sl] = (int64_t)sl * 64 + d.front() >= 0 && (int64_t)sl * 64 + d.back() + 63 < nc;
+    D[sl] = std::move(d);
+  }
+  if (not_ok) return false;
+  std::vector<int32_t> sptr(ns + 1, 0), cbptr(ns + 1, 0), width(ns);
+  for (int32_t sl = 0; sl < ns; sl++) {
+    width[sl] = ((int32_t)D[sl].size() + 3) & ~3;
+    if ((int64_t)sptr[sl] + width[sl] > INT32_MAX / 64) return false;
+    sptr[sl + 1] = sptr[sl] + width[sl];
+    cbptr[sl + 1] = cbptr[sl] + width[sl];
+  }
+  const int64_t np = (int64_t)sptr[ns] * 64;
+  std::vector<double> val(np, 0.0);
+  std::vector<int32_t> cbase((size_t)cbptr[ns] + 4, 0);
+#pragma omp parallel for schedule(dynamic, 256)
+  for (int32_t sl = 0; sl < ns; sl++) {
+    const std::vector<int32_t> &d = D[sl];
+    const int32_t wp = width[sl];
+    const int64_t nb = (int64_t)sptr[sl] * 64;
+    for (int32_t k = 0; k < wp; k++) cbase[cbptr[sl] + k] = sl * 64 + d[std::min<size_t>(k, d.size() - 1)];
+    for (int32_t q = 0; q < 64; q++) {
+      const int64_t r = (int64_t)sl * 64 + q;
+      if (r >= n) break;
+      for (int32_t e = a.rptr[r]; e < a.rptr[r + 1]; e++) {
+        const int32_t k = (int32_t)(std::lower_bound(d.begin(), d.end(), a.idx[e] - (int32_t)r) - d.begin());
+        const int32_t k0 = k / kAllAlignedChunk * kAllAlignedChunk, kw = std::min(kAllAlignedChunk, wp - k0);
+        val[nb + (int64_t)k0 * 64 + (int64_t)q * kw + (k - k0)] = a.val[e];
+      }
+    }
+  }
+  for (int32_t sl = 0; sl < ns; sl++)
+    if (!in_range[sl]) cbptr[sl] |= 1;
+  int32_t mw = 0;
+  for (int32_t sl = 0; sl < ns; sl++) mw = std::max(mw, width[sl]);
+  s.n = n;
+  s.ncols = nc;
+  s.sigma = 1;
+  s.nnz = a.nnz;
+  s.nslices = ns;
+  s.perm.resize(n);
+  std::iota(s.perm.begin(), s.perm.end(), 0);
+  s.sptr = std::move(sptr);
+  s.val = std::move(val);
+  s.col.clear();
+  s.cbase = std::move(cbase);
+  s.cbptr = std::move(cbptr);
+  s.xoff.clear();
+  s.dcol.clear();
+  s.aligned_all = true;
+  s.nnz_pad = np;
+  s.max_width = mw;
+  s.height = 64;
+  return true;
+}
+
 Status build_sell(const f3r_csr &a, int32_t sigma, bool renumber, SellHost &s,
                   const std::vector<int32_t> *given_perm) {
   if (sigma < 1) return fail(F3R_ERROR_INVALID_VALUE, "sigma must be >= 1");
@@ -264,6 +340,7 @@ Status build_sell(const f3r_csr &a, int32_t sigma, bool renumber, SellHost &s,
 
 Status upload_sell(Context &c, const SellHost &h, int dtype_mask, bool scatter_perm, DeviceSell &d) {
   d.n = h.n; d.ncols = h.ncols; d.nslices = h.nslices; d.max_width = h.max_width; d.sigma = h.sigma;
+  d.height = h.height;
   d.nnz = h.nnz; d.nnz_pad = h.nnz_pad; d.dtypes = dtype_mask;
   const size_t np = (size_t)h.nnz_pad;
   if (!h.xoff.empty() || h.aligned_all) {
@@ -438,6 +515,7 @@ template <int K> struct Work {
   double *b_d = nullptr, *x_d = nullptr, *bp_d = nullptr, *xp_d = nullptr, *r_d = nullptr;
   uint32_t *active = nullptr;
   double *nrm = nullptr;  // K norms read back by the host
+  double *stage = nullptr;  // K host columns staged on the device (solve_multi)
   GridRed gr{};
   int64_t cnt = 0, r_calls = 0;
   std::map<std::vector<bool>, std::pair<cudaGraphExec_t, int64_t>> graphs;  // exec, kernels in it
@@ -467,10 +545,14 @@ template <int K> struct Work {
     F3R_TRY(alloc(&L.e, (size_t)K * (m + 1)));
     F3R_TRY(alloc(&L.y, (size_t)K * (m + 1)));
     F3R_TRY(alloc(&L.inv, (size_t)K));
-    CUDA_TRY(cudaMemset(L.H, 0, sizeof(T) * (size_t)K * (m + 1) * m));
-    CUDA_TRY(cudaMemset(L.e, 0, sizeof(T) * (size_t)K * (m + 1)));
+    CUDA_TRY(cudaMemsetAsync(L.H, 0, sizeof(T) * (size_t)K * (m + 1) * m, st));
+    CUDA_TRY(cudaMemsetAsync(L.e, 0, sizeof(T) * (size_t)K * (m + 1), st));
     return F3R_SUCCESS;
   }
+  // the context's stream: the set-up of a workspace is ordered on it and never
+  // touches the legacy default stream, which would invalidate a graph capture
+  // that a solve on another context (thread) runs meanwhile
+  cudaStream_t st = nullptr;
 };
 
 template <int K> struct Engine;
@@ -492,6 +574,11 @@ struct Solver {
   JacobiTrsv jl, ju;  // the same factors solved by Jacobi / BAJ sweeps
   std::vector<void *> allocs;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // A batch of systems of one pattern (f3r_batch): every column of the block
+  // solve is its own system; A, W^T, Z (or wd, zd) hold mm_k values per
+  // entry, interleaved.  Solves run the mm_k-column engine only.
+  bool mm = false;
+  int mm_k = 0, mm_count = 0;
   Work<1> w1;  // single-column solves
   std::unique_ptr<Work<2>> w2;
   std::unique_ptr<Work<4>> w4;
@@ -514,15 +601,17 @@ struct Solver {
   // R calls per outer step (the product of the inner levels' steps)
   int calls_per_outer() const { return std::max(p.m2, 1) * std::max(p.m3, 1) * std::max(p.half_m, 1); }
   // Can the nest run K columns in lockstep?  The block product covers SDAINV
-  // (diagonal, or general factors in packed / fully aligned SELL) with FGMRES
-  // levels; other set-ups solve column by column.
+  // (diagonal, or general factors) with FGMRES levels on SELL with 32-bit or
+  // no column indices; other set-ups (ILU, s-step levels, the fp16-vector
+  // level, CSR or 16-bit indices) solve column by column.
   bool block_ok() const {
-    auto layout_ok = [](const DeviceSell &d) { return !d.rptr && !d.xoff && !d.dcol; };
+    auto layout_ok = [](const DeviceSell &d) { return !d.rptr && !d.dcol && d.height == 32; };
     if (p.precond != F3R_PRECOND_SDAINV || p.inner_sstep || p.half_m > 0 || !layout_ok(A)) return false;
     return precond_diag || (layout_ok(W) && layout_ok(Z));
   }
   template <int K> Status work(Work<K> **out);
   Status solve(const double *b_user, double *x_user, f3r_cond_fn cond, void *user, f3r_result *res);
+  Status solve_batch(const double *const *b, double *const *x, f3r_cond_fn cond, void *user, f3r_result *results);
   Status solve_multi(int32_t nrhs, const double *b, int64_t ldb, double *x, int64_t ldx, f3r_cond_fn cond, void *user,
                      f3r_result *results);
 };
@@ -547,13 +636,33 @@ Status launch_block_one(Context &c, const V *val, const DevSell &A, const X *x, 
 }
 template <typename V, typename X, typename Epi, int K>
 Status launch_block(Context &c, const V *val, const DevSell &A, const X *x, const Epi &epi, bool attr_only = false) {
-  if (A.rptr || A.xoff || A.dcol) return fail(F3R_ERROR_UNSUPPORTED, "block product: packed or fully aligned SELL only");
+  if (A.rptr || A.dcol) return fail(F3R_ERROR_UNSUPPORTED, "block product: SELL with 32-bit indices or aligned slices");
   if (attr_only) {
     F3R_TRY((launch_block_one<V, X, Epi, K, int32_t>(c, val, A, x, epi, true)));
+    F3R_TRY((launch_block_one<V, X, Epi, K, AlignedIdx>(c, val, A, x, epi, true)));
     return launch_block_one<V, X, Epi, K, AllAlignedIdx>(c, val, A, x, epi, true);
   }
+  if (A.xoff) return launch_block_one<V, X, Epi, K, AlignedIdx>(c, val, A, x, epi, false);
   if (A.cbase) return launch_block_one<V, X, Epi, K, AllAlignedIdx>(c, val, A, x, epi, false);
   return launch_block_one<V, X, Epi, K, int32_t>(c, val, A, x, epi, false);
+}
+
+// K systems of one pattern, each column with its own values (packed int32 SELL)
+template <typename V, typename X, typename Epi, int K>
+Status launch_block_mm(Context &c, const V *val, const DevSell &A, const X *x, const Epi &epi, bool attr_only = false) {
+  if (A.rptr || A.xoff || A.dcol || A.cbase) return fail(F3R_ERROR_UNSUPPORTED, "batched systems: packed int32 SELL only");
+  using Cfg = BlockCfgMM<V, K>;
+  auto kern = k_sell_block<V, X, Epi, K, Cfg::WARPS, Cfg::STAGES, Cfg::KC, int32_t, true>;
+  static int done[64] = {0};
+  if (!done[c.device & 63]) {
+    CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)block_mm_smem_bytes<V, K>()));
+    done[c.device & 63] = 1;
+  }
+  if (attr_only || A.nslices == 0) return F3R_SUCCESS;
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(cdiv(A.nslices, Cfg::WARPS), c.sm_count));
+  launch_k(c, kern, grid, Cfg::WARPS * 32, block_mm_smem_bytes<V, K>(), c.stream, val, A, x, epi, c.err);
+  CUDA_TRY(cudaGetLastError());
+  return F3R_SUCCESS;
 }
 
 // The nested solve over K columns in lockstep (K = 1: the single solve).
@@ -571,6 +680,7 @@ template <int K> struct Engine {
   template <typename V, typename X, typename E1, typename EK>
   Status mv(const V *vals, const DevSell &M, const X *x, const E1 &e1, const EK &ek) {
     if constexpr (K == 1) return launch_sell(C(), vals, M, x, e1);
+    else if (S.mm) return launch_block_mm<V, X, EK, K>(C(), vals, M, x, ek);
     else return launch_block<V, X, EK, K>(C(), vals, M, x, ek);
   }
   template <typename V, typename X, typename Out> Status mv_store(const V *vals, const DevSell &M, const X *x, Out *y) {
@@ -592,6 +702,17 @@ template <int K> struct Engine {
       F3R_TRY((launch_block<__half, __half, EpiRichResPreK<K>, K>(C(), h, Av, h, {}, true)));
       F3R_TRY((launch_block<__half, __half, EpiResidualK<__half, __half, K>, K>(C(), h, Av, h, {}, true)));
       F3R_TRY((launch_block<__half, __half, EpiZScaleK<K>, K>(C(), h, Av, h, {}, true)));
+      if (S.mm) {
+        F3R_TRY((launch_block_mm<double, double, EpiStoreK<double, K>, K>(C(), d, Av, d, {}, true)));
+        F3R_TRY((launch_block_mm<double, double, EpiResidualK<double, double, K>, K>(C(), d, Av, d, {}, true)));
+        F3R_TRY((launch_block_mm<float, float, EpiStoreK<float, K>, K>(C(), f, Av, f, {}, true)));
+        F3R_TRY((launch_block_mm<__half, float, EpiStoreK<float, K>, K>(C(), h, Av, f, {}, true)));
+        F3R_TRY((launch_block_mm<__half, __half, EpiStoreK<__half, K>, K>(C(), h, Av, h, {}, true)));
+        F3R_TRY((launch_block_mm<__half, __half, EpiRichStepK<K, true>, K>(C(), h, Av, h, {}, true)));
+        F3R_TRY((launch_block_mm<__half, __half, EpiRichResPreK<K, true>, K>(C(), h, Av, h, {}, true)));
+        F3R_TRY((launch_block_mm<__half, __half, EpiResidualK<__half, __half, K>, K>(C(), h, Av, h, {}, true)));
+        F3R_TRY((launch_block_mm<__half, __half, EpiZScaleK<K>, K>(C(), h, Av, h, {}, true)));
+      }
     }
     return F3R_SUCCESS;
   }
@@ -635,8 +756,14 @@ template <int K> struct Engine {
     const DevSell Av = S.A.view();
     const GridRed gr = w.gr;
     if (S.precond_diag) {
-      const DiagPre M{S.wd, S.zd};
-      if constexpr (K == 1) {
+      if constexpr (K > 1) {
+        if (S.mm) {
+          F3R_TRY(rich_diag<true>(in, out, e_set, e_stride, in_inv, upd, sc, isc, hi, h0, out_last));
+        } else {
+          F3R_TRY(rich_diag<false>(in, out, e_set, e_stride, in_inv, upd, sc, isc, hi, h0, out_last));
+        }
+      } else {
+        const DiagPre M{S.wd, S.zd};
         if (h16) {
           if (!upd)
             launch_k(C(), k_rich_enter_diag<true, __half>, C().ew_grid(cdiv(N, 4)), kEwThreads, 0, st, in16, in_inv,
@@ -644,37 +771,34 @@ template <int K> struct Engine {
           else
             launch_k(C(), k_rich_enter_diag<false, __half>, C().ew_grid(cdiv(N, 4)), kEwThreads, 0, st, in16, in_inv,
                      sc, M, w.hin, h0, w.rs, e_set, N);
+        } else {
+          if (!upd)
+            launch_k(C(), k_rich_enter_diagK<true, 1>, g, kEwThreads, 0, st, in, in_inv, sc, M, w.hin, h0, w.rs, e_set,
+                     e_stride, N);
+          else
+            launch_k(C(), k_rich_enter_diagK<false, 1>, g, kEwThreads, 0, st, in, in_inv, sc, M, w.hin, h0, w.rs,
+                     e_set, e_stride, N);
         }
-      }
-      if (!h16) {
-        if (!upd)
-          launch_k(C(), k_rich_enter_diagK<true, K>, g, kEwThreads, 0, st, in, in_inv, sc, M, w.hin, h0, w.rs, e_set,
-                   e_stride, N);
-        else
-          launch_k(C(), k_rich_enter_diagK<false, K>, g, kEwThreads, 0, st, in, in_inv, sc, M, w.hin, h0, w.rs, e_set,
-                   e_stride, N);
-      }
-      if (!upd) {
-        __half *cur = h0, *nxt = w.hout2;
-        for (int k = 1; k < p.m4; k++) {
-          const bool last = (k == p.m4 - 1);
-          F3R_TRY(mv(S.A.v16, Av, (const __half *)cur,
-                     EpiRichStep{hi, cur, M, w.rs, k, last ? out16 : nxt, last ? out_last : nullptr, isc},
-                     EpiRichStepK<K>{hi, cur, M, w.rs, k, nxt, last ? out_last : nullptr, isc}));
-          std::swap(cur, nxt);
-        }
-      } else {
-        F3R_TRY(mv_store(S.A.v16, Av, (const __half *)h0, w.tmp));
-        launch_k(C(), k_rich_weightK<8, K>, g, 256, 0, st, (const __half *)w.tmp, hi, N, gr, w.rs, 0);
-        launch_k(C(), k_rich_scale_omK<K>, g, kEwThreads, 0, st, h0, (const RichState *)w.rs, N);
-        for (int k = 1; k < p.m4; k++) {
-          const bool last = (k == p.m4 - 1);
-          F3R_TRY(mv(S.A.v16, Av, (const __half *)w.hout, EpiRichResPre{hi, M, w.hr, w.tmp2},
-                     EpiRichResPreK<K>{hi, M, w.hr, w.tmp2}));
-          F3R_TRY(mv_store(S.A.v16, Av, (const __half *)w.tmp2, w.tmp));
-          launch_k(C(), k_rich_weightK<8, K>, g, 256, 0, st, (const __half *)w.tmp, (const __half *)w.hr, N, gr, w.rs,
-                   k);
-          F3R_TRY(axpy(k, 0, last ? out_last : nullptr, last ? out16 : nullptr, isc));
+        if (!upd) {
+          __half *cur = h0, *nxt = w.hout2;
+          for (int k = 1; k < p.m4; k++) {
+            const bool last = (k == p.m4 - 1);
+            F3R_TRY(launch_sell(C(), S.A.v16, Av, (const __half *)cur,
+                                EpiRichStep{hi, cur, M, w.rs, k, last ? out16 : nxt, last ? out_last : nullptr, isc}));
+            std::swap(cur, nxt);
+          }
+        } else {
+          F3R_TRY(mv_store(S.A.v16, Av, (const __half *)h0, w.tmp));
+          launch_k(C(), k_rich_weightK<8, K>, g, 256, 0, st, (const __half *)w.tmp, hi, N, gr, w.rs, 0);
+          launch_k(C(), k_rich_scale_omK<K>, g, kEwThreads, 0, st, h0, (const RichState *)w.rs, N);
+          for (int k = 1; k < p.m4; k++) {
+            const bool last = (k == p.m4 - 1);
+            F3R_TRY(launch_sell(C(), S.A.v16, Av, (const __half *)w.hout, EpiRichResPre{hi, M, w.hr, w.tmp2}));
+            F3R_TRY(mv_store(S.A.v16, Av, (const __half *)w.tmp2, w.tmp));
+            launch_k(C(), k_rich_weightK<8, K>, g, 256, 0, st, (const __half *)w.tmp, (const __half *)w.hr, N, gr,
+                     w.rs, k);
+            F3R_TRY(axpy(k, 0, last ? out_last : nullptr, last ? out16 : nullptr, isc));
+          }
         }
       }
     } else {
@@ -704,6 +828,49 @@ template <int K> struct Engine {
     }
     if (p.m4 == 1 && !out16) launch_k(C(), k_rich_exitK<K>, g, kEwThreads, 0, st, (const __half *)w.hout, out, isc, N);
     CUDA_TRY(cudaGetLastError());
+    return F3R_SUCCESS;
+  }
+
+  // R with the diagonal SDAINV fused, K > 1 columns (MMF: one diagonal per
+  // column, a batch of systems); the same steps as the single-column path
+  template <bool MMF>
+  Status rich_diag(float *in, float *out, float *e_set, int64_t e_stride, const float *in_inv, bool upd, float sc,
+                   float isc, const __half *hi, __half *h0, float *out_last) {
+    const int64_t N = n;
+    const int g = C().ew_grid(N);
+    cudaStream_t st = C().stream;
+    const DiagPre M{S.wd, S.zd};
+    const DevSell Av = S.A.view();
+    const GridRed gr = w.gr;
+    if (!upd)
+      launch_k(C(), k_rich_enter_diagK<true, K, MMF>, g, kEwThreads, 0, st, in, in_inv, sc, M, w.hin, h0, w.rs, e_set,
+               e_stride, N);
+    else
+      launch_k(C(), k_rich_enter_diagK<false, K, MMF>, g, kEwThreads, 0, st, in, in_inv, sc, M, w.hin, h0, w.rs, e_set,
+               e_stride, N);
+    if (!upd) {
+      __half *cur = h0, *nxt = w.hout2;
+      for (int k = 1; k < p.m4; k++) {
+        const bool last = (k == p.m4 - 1);
+        F3R_TRY(mv(S.A.v16, Av, (const __half *)cur, EpiRichStep{hi, cur, M, w.rs, k, nxt, nullptr, isc},
+                   EpiRichStepK<K, MMF>{hi, cur, M, w.rs, k, nxt, last ? out_last : nullptr, isc}));
+        std::swap(cur, nxt);
+      }
+    } else {
+      F3R_TRY(mv_store(S.A.v16, Av, (const __half *)h0, w.tmp));
+      launch_k(C(), k_rich_weightK<8, K>, g, 256, 0, st, (const __half *)w.tmp, hi, N, gr, w.rs, 0);
+      launch_k(C(), k_rich_scale_omK<K>, g, kEwThreads, 0, st, h0, (const RichState *)w.rs, N);
+      for (int k = 1; k < p.m4; k++) {
+        const bool last = (k == p.m4 - 1);
+        F3R_TRY(mv(S.A.v16, Av, (const __half *)w.hout, EpiRichResPre{hi, M, w.hr, w.tmp2},
+                   EpiRichResPreK<K, MMF>{hi, M, w.hr, w.tmp2}));
+        F3R_TRY(mv_store(S.A.v16, Av, (const __half *)w.tmp2, w.tmp));
+        launch_k(C(), k_rich_weightK<8, K>, g, 256, 0, st, (const __half *)w.tmp, (const __half *)w.hr, N, gr, w.rs,
+                 k);
+        F3R_TRY(axpy(k, 0, last ? out_last : nullptr, nullptr, isc));
+      }
+    }
+    (void)out;
     return F3R_SUCCESS;
   }
 
@@ -1124,6 +1291,7 @@ template <int K> struct Engine {
 template <int K> Status make_work(Solver &s, Work<K> &w) {
   const size_t nn = (size_t)std::max(s.n, 1) * K;
   const f3r_params &p = s.p;
+  w.st = s.ctx->stream;
   F3R_TRY(w.make_level(w.L1, p.m_outer, s.ldn, true, false));
   if (p.m2 > 0) F3R_TRY(w.make_level(w.L2, p.m2, s.ldn, true));
   if (p.m3 > 0) F3R_TRY(w.make_level(w.L3, p.m3, s.ldn, false));
@@ -1140,8 +1308,8 @@ template <int K> Status make_work(Solver &s, Work<K> &w) {
     F3R_TRY(w.alloc(&L.e, (size_t)m + 1));
     F3R_TRY(w.alloc(&L.y, (size_t)m));
     F3R_TRY(w.alloc(&L.inv, 1));
-    CUDA_TRY(cudaMemset(L.H, 0, sizeof(float) * (size_t)(m + 1) * m));
-    CUDA_TRY(cudaMemset(L.e, 0, sizeof(float) * (size_t)(m + 1)));
+    CUDA_TRY(cudaMemsetAsync(L.H, 0, sizeof(float) * (size_t)(m + 1) * m, w.st));
+    CUDA_TRY(cudaMemsetAsync(L.e, 0, sizeof(float) * (size_t)(m + 1), w.st));
   }
   F3R_TRY(w.alloc(&w.abs_e, K));
   F3R_TRY(w.alloc(&w.nrm, K));
@@ -1151,7 +1319,7 @@ template <int K> Status make_work(Solver &s, Work<K> &w) {
   F3R_TRY(w.alloc(&w.tmp, nn));
   F3R_TRY(w.alloc(&w.tmp2, nn));
   F3R_TRY(w.alloc(&w.hr, nn));
-  CUDA_TRY(cudaMemset(w.tmp2, 0, nn * sizeof(__half)));
+  CUDA_TRY(cudaMemsetAsync(w.tmp2, 0, nn * sizeof(__half), w.st));
   F3R_TRY(w.alloc(&w.rs, K));
   F3R_TRY(w.alloc(&w.in_slot, 1));
   F3R_TRY(w.alloc(&w.out_slot, 1));
@@ -1159,6 +1327,7 @@ template <int K> Status make_work(Solver &s, Work<K> &w) {
   F3R_TRY(w.alloc(&w.x_d, nn));
   F3R_TRY(w.alloc(&w.r_d, nn));
   F3R_TRY(w.alloc(&w.active, 1));
+  if (K > 1) F3R_TRY(w.alloc(&w.stage, nn));
   if (s.perm_d) {
     F3R_TRY(w.alloc(&w.bp_d, nn));
     F3R_TRY(w.alloc(&w.xp_d, nn));
@@ -1168,9 +1337,9 @@ template <int K> Status make_work(Solver &s, Work<K> &w) {
   unsigned int *ticket = nullptr;
   F3R_TRY(w.alloc(&part, (size_t)s.ctx->sm_count * 8 * kMaxCols * K + 64));
   F3R_TRY(w.alloc(&ticket, 4));
-  CUDA_TRY(cudaMemset(ticket, 0, 4 * sizeof(unsigned int)));
+  CUDA_TRY(cudaMemsetAsync(ticket, 0, 4 * sizeof(unsigned int), w.st));
   w.gr = GridRed{part, ticket};
-  CUDA_TRY(cudaDeviceSynchronize());
+  CUDA_TRY(cudaStreamSynchronize(w.st));
   return Engine<K>(s, w).prepare();
 }
 
@@ -1263,9 +1432,6 @@ Status Solver::solve_multi(int32_t nrhs, const double *b, int64_t ldb, double *x
   const int64_t N = n;
   cudaStream_t st = C().stream;
   const int g = C().ew_grid(N);
-  // host columns are staged through one device block of up to 16 columns
-  double *stage = nullptr;
-  if (!b_dev || !x_dev) CUDA_TRY(cudaMalloc((void **)&stage, sizeof(double) * (size_t)std::max<int64_t>(N, 1) * 16));
   Status status = F3R_SUCCESS;
   for (int32_t k0 = 0; k0 < nrhs && status == F3R_SUCCESS; k0 += 16) {
     const int nc = std::min<int32_t>(16, nrhs - k0);
@@ -1274,6 +1440,7 @@ Status Solver::solve_multi(int32_t nrhs, const double *b, int64_t ldb, double *x
       Work<K> *wk = nullptr;
       F3R_TRY(work<K>(&wk));
       Work<K> &w = *wk;
+      double *stage = w.stage;  // host columns pass through it
       // b, x columns into the interleaved blocks (storage order)
       double *bi = perm_d ? w.bp_d : w.b_d, *xi = perm_d ? w.xp_d : w.x_d;
       const double *bsrc = b + (size_t)k0 * ldb;
@@ -1317,10 +1484,6 @@ Status Solver::solve_multi(int32_t nrhs, const double *b, int64_t ldb, double *x
     else if (nc <= 8) status = run(std::integral_constant<int, 8>());
     else status = run(std::integral_constant<int, 16>());
   }
-  if (stage) {
-    cudaStreamSynchronize(st);
-    cudaFree(stage);
-  }
   return status;
 }
 
@@ -1331,10 +1494,12 @@ Status Solver::solve_multi(int32_t nrhs, const double *b, int64_t ldb, double *x
 // entries) are skipped.
 static Status autotune_layout(f3r_context *ctx, const f3r_csr *a, f3r_params &p) {
   struct Cand {
-    int32_t format, sigma, align, index16;
+    int32_t format, sigma, align, index16, height;
   };
-  const Cand cands[] = {{F3R_FORMAT_SELL, 1, 1, 0},   {F3R_FORMAT_SELL, 1, 0, 0}, {F3R_FORMAT_SELL, 1, 0, 1},
-                        {F3R_FORMAT_SELL, 256, 0, 0}, {F3R_FORMAT_SELL, 256, 1, 0}, {F3R_FORMAT_CSR, 1, 0, 0}};
+  const Cand cands[] = {{F3R_FORMAT_SELL, 1, 1, 0, 32},   {F3R_FORMAT_SELL, 1, 0, 0, 32},
+                        {F3R_FORMAT_SELL, 1, 0, 1, 32},   {F3R_FORMAT_SELL, 256, 0, 0, 32},
+                        {F3R_FORMAT_SELL, 256, 1, 0, 32}, {F3R_FORMAT_CSR, 1, 0, 0, 32},
+                        {F3R_FORMAT_SELL, 1, 1, 0, 64}};
   Context &c = *ctx;
   const int32_t n = a->nrows;
   float *xy = nullptr;
@@ -1355,7 +1520,9 @@ static Status autotune_layout(f3r_context *ctx, const f3r_csr *a, f3r_params &p)
       SellHost h;
       st = build_sell(*a, k.sigma, true, h);
       if (st != F3R_SUCCESS) break;
-      if (k.align) {
+      if (k.height == 64) {
+        if (!align64(*a, h)) continue;  // rows do not share offsets: not a candidate
+      } else if (k.align) {
         if (align_offsets(*a, true, h) < 0) continue;  // too large padded: not a candidate
       } else if (k.index16) {
         compress_index16(h);
@@ -1397,6 +1564,7 @@ static Status autotune_layout(f3r_context *ctx, const f3r_csr *a, f3r_params &p)
   p.sell_sigma = cands[besti].sigma;
   p.sell_align = cands[besti].align;
   p.sell_index16 = cands[besti].index16;
+  p.sell_c = cands[besti].height;
   return F3R_SUCCESS;
 }
 
@@ -1424,7 +1592,9 @@ static Status make_solver(f3r_context *ctx, const f3r_csr *a, const f3r_params *
   if (p.m2 == 0 && (p.half_m == 0 || p.m3 > 0 || (p.inner_sstep & 3)))
     return fail(F3R_ERROR_INVALID_VALUE,
                 "m2 = 0 (no fp32 level) needs half_m > 0, m3 = 0 and no s-step inner level");
-  if (p.sell_c != 32) return fail(F3R_ERROR_UNSUPPORTED, "only SELL slice height 32 is implemented");
+  if (p.sell_c != 32 && p.sell_c != 64) return fail(F3R_ERROR_UNSUPPORTED, "SELL slice height 32 or 64");
+  if (p.sell_c == 64 && (p.sell_sigma != 1 || p.format != F3R_FORMAT_SELL || p.sell_index16))
+    return fail(F3R_ERROR_INVALID_VALUE, "64-row slices: SELL, sigma 1, offset-aligned (no 16-bit indices)");
   if (p.format != F3R_FORMAT_SELL && p.format != F3R_FORMAT_CSR) return fail(F3R_ERROR_INVALID_VALUE, "unknown format");
   if (p.format == F3R_FORMAT_CSR && (p.sell_sigma != 1 || p.sell_align || p.sell_index16))
     return fail(F3R_ERROR_INVALID_VALUE, "format CSR takes no SELL options (sigma 1, no alignment, 32-bit indices)");
@@ -1455,7 +1625,10 @@ static Status make_solver(f3r_context *ctx, const f3r_csr *a, const f3r_params *
     SellHost h;
     F3R_TRY(build_sell(*a, p.sell_sigma, true, h));
     hperm = h.perm;
-    if (p.sell_align) {
+    if (p.sell_c == 64) {
+      if (!align64(*a, h))
+        return fail(F3R_ERROR_UNSUPPORTED, "64-row slices need every 64 rows to share their column offsets");
+    } else if (p.sell_align) {
       if (align_offsets(*a, true, h) < 0) return fail(F3R_ERROR_UNSUPPORTED, "padded matrix exceeds 2^31 entries");
     } else if (p.sell_index16) {
       compress_index16(h);
@@ -1568,6 +1741,277 @@ static Status make_solver(f3r_context *ctx, const f3r_csr *a, const f3r_params *
   CUDA_TRY(cudaDeviceSynchronize());
   *out = s.release();
   return F3R_SUCCESS;
+}
+
+// ---------------------------------------------------------------------------
+// Batches of systems of one pattern (f3r_batch_*)
+// ---------------------------------------------------------------------------
+
+// SELL position of every CSR entry of a (rows in the storage order of h, the
+// packed layout build_sell makes: entry c of storage row r at
+// (sptr[r / 32] + c) * 32 + r % 32)
+static std::vector<int64_t> sell_positions(const f3r_csr &a, const SellHost &h) {
+  std::vector<int64_t> pos((size_t)a.nnz);
+#pragma omp parallel for schedule(static)
+  for (int32_t r = 0; r < h.n; r++) {
+    const int32_t o = h.perm[r];
+    const int64_t base = (int64_t)h.sptr[r / 32] * 32 + (r % 32);
+    for (int32_t q = a.rptr[o], c = 0; q < a.rptr[o + 1]; q++, c++) pos[q] = base + (int64_t)c * 32;
+  }
+  return pos;
+}
+
+// The packed SELL of `pattern` (rows in the order perm) holding K systems'
+// values interleaved, vals[c] on the pattern's entries (count <= K systems;
+// the remaining columns hold zeros), with the value copies of dtype_mask.
+static Status upload_sell_mm(Context &c, const f3r_csr &pattern, const std::vector<int32_t> &perm,
+                             const std::vector<const double *> &vals, int K, int dtype_mask, DeviceSell &d) {
+  SellHost h;
+  F3R_TRY(build_sell(pattern, 1, true, h, &perm));
+  const std::vector<int64_t> pos = sell_positions(pattern, h);
+  const size_t np = (size_t)h.nnz_pad;
+  std::vector<double> v(np * K, 0.0);
+  for (size_t s = 0; s < vals.size(); s++)
+#pragma omp parallel for schedule(static)
+    for (int32_t q = 0; q < pattern.nnz; q++) v[(size_t)pos[q] * K + s] = vals[s][q];
+  d.n = h.n; d.ncols = h.ncols; d.nslices = h.nslices; d.max_width = h.max_width; d.sigma = 1;
+  d.nnz = h.nnz; d.nnz_pad = h.nnz_pad; d.dtypes = dtype_mask;
+  F3R_TRY(c.alloc((void **)&d.col, np * 4));
+  F3R_TRY(c.alloc((void **)&d.sptr, (size_t)(h.nslices + 1) * 4));
+  CUDA_TRY(cudaMemcpyAsync(d.col, h.col.data(), np * 4, cudaMemcpyHostToDevice, c.stream));
+  CUDA_TRY(cudaMemcpyAsync(d.sptr, h.sptr.data(), (size_t)(h.nslices + 1) * 4, cudaMemcpyHostToDevice, c.stream));
+  double *tmp64 = nullptr;
+  F3R_TRY(c.alloc((void **)&tmp64, np * K * 8));
+  CUDA_TRY(cudaMemcpyAsync(tmp64, v.data(), np * K * 8, cudaMemcpyHostToDevice, c.stream));
+  const int g = c.ew_grid((int64_t)(np * K));
+  if (dtype_mask & (1 << F3R_F32)) {
+    F3R_TRY(c.alloc((void **)&d.v32, np * K * 4));
+    launch_k(c, k_convert_vals<float>, g, kEwThreads, 0, c.stream, tmp64, d.v32, (int64_t)(np * K));
+  }
+  if (dtype_mask & (1 << F3R_F16)) {
+    F3R_TRY(c.alloc((void **)&d.v16, np * K * 2));
+    launch_k(c, k_convert_vals<__half>, g, kEwThreads, 0, c.stream, tmp64, d.v16, (int64_t)(np * K));
+  }
+  CUDA_TRY(cudaGetLastError());
+  CUDA_TRY(cudaStreamSynchronize(c.stream));
+  if (dtype_mask & (1 << F3R_F64)) d.v64 = tmp64;
+  else cudaFree(tmp64);
+  return F3R_SUCCESS;
+}
+
+// The union of several CSR patterns of one shape (each row's columns merged
+// and sorted), and every matrix's values on it (zero where it has no entry:
+// a zero entry adds 0 x to a row's sum, so the products are unchanged).
+static void union_pattern(const std::vector<const HostCSR *> &m, HostCSR &u, std::vector<std::vector<double>> &vals) {
+  const int32_t n = m[0]->n;
+  u.n = n;
+  u.m = m[0]->m;
+  u.rptr.assign(n + 1, 0);
+  std::vector<std::vector<int32_t>> cols(n);
+#pragma omp parallel for schedule(dynamic, 1024)
+  for (int32_t i = 0; i < n; i++) {
+    std::vector<int32_t> &c = cols[i];
+    for (const HostCSR *a : m)
+      for (int32_t q = a->rptr[i]; q < a->rptr[i + 1]; q++) c.push_back(a->idx[q]);
+    std::sort(c.begin(), c.end());
+    c.erase(std::unique(c.begin(), c.end()), c.end());
+  }
+  for (int32_t i = 0; i < n; i++) u.rptr[i + 1] = u.rptr[i] + (int32_t)cols[i].size();
+  u.idx.resize(u.rptr[n]);
+  u.val.assign(u.rptr[n], 0.0);
+  for (int32_t i = 0; i < n; i++) std::copy(cols[i].begin(), cols[i].end(), u.idx.begin() + u.rptr[i]);
+  vals.assign(m.size(), std::vector<double>(u.rptr[n], 0.0));
+#pragma omp parallel for schedule(dynamic, 1024)
+  for (int32_t i = 0; i < n; i++)
+    for (size_t s = 0; s < m.size(); s++) {
+      const HostCSR *a = m[s];
+      int32_t qu = u.rptr[i];
+      for (int32_t q = a->rptr[i]; q < a->rptr[i + 1]; q++) {
+        while (u.idx[qu] != a->idx[q]) qu++;
+        vals[s][qu] = a->val[q];
+      }
+    }
+}
+
+// zf / wf: given SDAINV factors per system (all or none)
+static Status make_batch(f3r_context *ctx, int32_t count, const f3r_csr *const *a, const f3r_params *pp, Solver **out,
+                         const f3r_csr *const *zf, const f3r_csr *const *wf) {
+  if (count < 1 || count > kMaxBlock) return fail(F3R_ERROR_INVALID_VALUE, "a batch holds 1 to 16 systems");
+  for (int32_t i = 0; i < count; i++) {
+    if (!a[i]) return fail(F3R_ERROR_INVALID_VALUE, "null system");
+    F3R_TRY(check_csr(a[i]));
+  }
+  const f3r_csr &a0 = *a[0];
+  if (a0.nrows != a0.ncols) return fail(F3R_ERROR_INVALID_VALUE, "the system matrices must be square");
+  for (int32_t i = 1; i < count; i++) {
+    const f3r_csr &ai = *a[i];
+    if (ai.nrows != a0.nrows || ai.ncols != a0.ncols || ai.nnz != a0.nnz ||
+        std::memcmp(ai.rptr, a0.rptr, sizeof(int32_t) * (a0.nrows + 1)) != 0 ||
+        (a0.nnz && std::memcmp(ai.idx, a0.idx, sizeof(int32_t) * a0.nnz) != 0))
+      return fail(F3R_ERROR_INVALID_VALUE, "the systems of a batch must share one sparsity pattern");
+  }
+  f3r_params p = *pp;
+  if (p.precond != F3R_PRECOND_SDAINV || p.inner_sstep || p.half_m > 0 || p.format != F3R_FORMAT_SELL)
+    return fail(F3R_ERROR_UNSUPPORTED, "a batch takes SDAINV, FGMRES levels and SELL storage");
+  if (p.m_outer < 1 || p.m_outer + 1 > kMaxCols || p.m2 < 1 || p.m2 + 1 > kMaxCols || p.m3 < 0 || p.m3 + 1 > kMaxCols ||
+      p.m4 < 1 || p.m4 > kMaxM4 || p.c < 1 || p.max_restarts < 1 || p.static_weight < 0 || p.sell_sigma < 1)
+    return fail(F3R_ERROR_INVALID_VALUE, "need 1 <= m_outer, m2 <= 127, 0 <= m3 <= 127, 1 <= m4 <= 16, c >= 1");
+  if (p.half_scale_log2 < 0 || p.half_scale_log2 > 20) return fail(F3R_ERROR_INVALID_VALUE, "half_scale_log2 in [0, 20]");
+  p.sell_align = 0;  // packed layout with per-column values
+  p.sell_index16 = 0;
+  p.sell_autotune = 0;
+  const int K = count <= 2 ? 2 : count <= 4 ? 4 : count <= 8 ? 8 : 16;
+  CUDA_TRY(cudaSetDevice(ctx->device));
+  auto s = std::make_unique<Solver>();
+  s->ctx = ctx;
+  s->p = p;
+  s->n = a0.nrows;
+  s->ldn = ((int64_t)a0.nrows + 7) / 8 * 8;
+  s->mm = true;
+  s->mm_k = K;
+  s->mm_count = count;
+  const int32_t n = a0.nrows;
+  const int all_types = (1 << F3R_F64) | (1 << F3R_F32) | (1 << F3R_F16);
+  // the row order of sigma-sorting (row lengths are the pattern's: one order for all)
+  std::vector<int32_t> hperm;
+  {
+    SellHost h;
+    F3R_TRY(build_sell(a0, p.sell_sigma, true, h));
+    hperm = h.perm;
+  }
+  std::vector<const double *> av;
+  for (int32_t i = 0; i < count; i++) av.push_back(a[i]->val);
+  F3R_TRY(upload_sell_mm(*ctx, a0, hperm, av, K, all_types, s->A));
+  s->A.sigma = p.sell_sigma;
+  s->perm = hperm;
+  if (p.sell_sigma > 1) {
+    F3R_TRY(s->alloc(&s->perm_d, (size_t)std::max(n, 1)));
+    CUDA_TRY(cudaMemcpy(s->perm_d, hperm.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice));
+  }
+  // every system's SDAINV factors (given, or computed here)
+  std::vector<std::unique_ptr<HostCSR>> Zs, Ws;
+  auto copy = [](const f3r_csr &m) {
+    HostCSR *h = new HostCSR(m.nrows, m.ncols, m.nnz);
+    std::memcpy(h->rptr.data(), m.rptr, sizeof(int32_t) * (m.nrows + 1));
+    std::memcpy(h->idx.data(), m.idx, sizeof(int32_t) * m.nnz);
+    std::memcpy(h->val.data(), m.val, sizeof(double) * m.nnz);
+    return h;
+  };
+  for (int32_t i = 0; i < count; i++) {
+    if (zf) {
+      if (!zf[i] || !wf[i]) return fail(F3R_ERROR_INVALID_VALUE, "give the factors of every system or of none");
+      F3R_TRY(check_csr(zf[i]));
+      F3R_TRY(check_csr(wf[i]));
+      if (zf[i]->nrows != n || zf[i]->ncols != n || wf[i]->nrows != n || wf[i]->ncols != n)
+        return fail(F3R_ERROR_INVALID_VALUE, "the factors must be square and of the matrix's size");
+      Zs.emplace_back(copy(*zf[i]));
+      Ws.emplace_back(copy(*wf[i]));
+    } else {
+      std::unique_ptr<HostCSR> Ah(copy(*a[i]));
+      HostCSR *zr = nullptr, *wr = nullptr;
+      F3R_TRY(sdainv(*Ah, p.sdainv_tol, p.acc, &zr, &wr));
+      Zs.emplace_back(zr);
+      Ws.emplace_back(wr);
+    }
+  }
+  bool diag = true;
+  for (int32_t i = 0; i < count && diag; i++)
+    for (int32_t r = 0; r < n && diag; r++) {
+      diag &= (Zs[i]->rptr[r + 1] - Zs[i]->rptr[r] == 1 && Zs[i]->idx[Zs[i]->rptr[r]] == r);
+      diag &= (Ws[i]->rptr[r + 1] - Ws[i]->rptr[r] == 1 && Ws[i]->idx[Ws[i]->rptr[r]] == r);
+    }
+  if (diag) {
+    // one diagonal value per row and system, interleaved, storage order
+    s->precond_diag = 1;
+    std::vector<double> wdv((size_t)n * K, 0.0), zdv((size_t)n * K, 0.0);
+    for (int32_t i = 0; i < count; i++)
+      for (int32_t r = 0; r < n; r++) {
+        wdv[(size_t)r * K + i] = Ws[i]->val[Ws[i]->rptr[hperm[r]]];
+        zdv[(size_t)r * K + i] = Zs[i]->val[Zs[i]->rptr[hperm[r]]];
+      }
+    double *tmp = nullptr;
+    const size_t nn = (size_t)std::max(n, 1) * K;
+    F3R_TRY(ctx->alloc((void **)&tmp, sizeof(double) * nn));
+    F3R_TRY(s->alloc(&s->wd, nn));
+    F3R_TRY(s->alloc(&s->zd, nn));
+    CUDA_TRY(cudaMemcpy(tmp, wdv.data(), sizeof(double) * nn, cudaMemcpyHostToDevice));
+    launch_k(*ctx, k_convert_vals<__half>, ctx->ew_grid((int64_t)nn), kEwThreads, 0, ctx->stream, tmp, s->wd,
+             (int64_t)nn);
+    CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    CUDA_TRY(cudaMemcpy(tmp, zdv.data(), sizeof(double) * nn, cudaMemcpyHostToDevice));
+    launch_k(*ctx, k_convert_vals<__half>, ctx->ew_grid((int64_t)nn), kEwThreads, 0, ctx->stream, tmp, s->zd,
+             (int64_t)nn);
+    CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    cudaFree(tmp);
+  } else {
+    // W^T and Z of every system on the union of their patterns, rows in the storage order
+    for (int which = 0; which < 2; which++) {
+      std::vector<const HostCSR *> ms;
+      for (int32_t i = 0; i < count; i++) ms.push_back(which == 0 ? Ws[i].get() : Zs[i].get());
+      HostCSR u;
+      std::vector<std::vector<double>> uv;
+      union_pattern(ms, u, uv);
+      std::vector<const double *> pv;
+      for (auto &vv : uv) pv.push_back(vv.data());
+      F3R_TRY(upload_sell_mm(*ctx, u.view(), hperm, pv, K, 1 << F3R_F16, which == 0 ? s->W : s->Z));
+    }
+  }
+  CUDA_TRY(cudaEventCreate(&s->ev0));
+  CUDA_TRY(cudaEventCreate(&s->ev1));
+  CUDA_TRY(cudaDeviceSynchronize());
+  *out = s.release();
+  return F3R_SUCCESS;
+}
+
+// One solve of every system of a batch: b[i], x[i] host or device vectors
+// (x[i] the initial guess on entry), in the K-column engine.
+Status Solver::solve_batch(const double *const *b, double *const *x, f3r_cond_fn cond, void *user,
+                           f3r_result *results) {
+  auto is_dev = [&](const void *q) {
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, q) != cudaSuccess) {
+      cudaGetLastError();
+      return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+  };
+  const int64_t N = n;
+  cudaStream_t st = C().stream;
+  const int g = C().ew_grid(N);
+  const int nc = mm_count;
+  auto run = [&](auto kc) -> Status {
+    constexpr int K = decltype(kc)::value;
+    Work<K> *wk = nullptr;
+    F3R_TRY(work<K>(&wk));
+    Work<K> &w = *wk;
+    double *bi = perm_d ? w.bp_d : w.b_d, *xi = perm_d ? w.xp_d : w.x_d;
+    for (int c = 0; c < nc; c++)
+      CUDA_TRY(cudaMemcpyAsync(w.stage + (size_t)c * N, b[c], sizeof(double) * N,
+                               is_dev(b[c]) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
+    launch_k(C(), k_interleave, g, kEwThreads, 0, st, (const double *)w.stage, N, nc, K, w.b_d, N);
+    for (int c = 0; c < nc; c++)
+      CUDA_TRY(cudaMemcpyAsync(w.stage + (size_t)c * N, x[c], sizeof(double) * N,
+                               is_dev(x[c]) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
+    launch_k(C(), k_interleave, g, kEwThreads, 0, st, (const double *)w.stage, N, nc, K, w.x_d, N);
+    if (perm_d) {
+      launch_k(C(), k_permute_gatherK<K>, g, kEwThreads, 0, st, (const double *)w.b_d, perm_d, bi, N);
+      launch_k(C(), k_permute_gatherK<K>, g, kEwThreads, 0, st, (const double *)w.x_d, perm_d, xi, N);
+    }
+    F3R_TRY(Engine<K>(*this, w).solve_block(bi, xi, nc, cond, user, results));
+    if (perm_d) launch_k(C(), k_permute_scatterK<K>, g, kEwThreads, 0, st, (const double *)xi, perm_d, w.x_d, N);
+    launch_k(C(), k_deinterleave, g, kEwThreads, 0, st, (const double *)w.x_d, K, nc, w.stage, N, N);
+    for (int c = 0; c < nc; c++)
+      CUDA_TRY(cudaMemcpyAsync(x[c], w.stage + (size_t)c * N, sizeof(double) * N,
+                               is_dev(x[c]) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    return F3R_SUCCESS;
+  };
+  switch (mm_k) {
+    case 2: return run(std::integral_constant<int, 2>());
+    case 4: return run(std::integral_constant<int, 4>());
+    case 8: return run(std::integral_constant<int, 8>());
+    default: return run(std::integral_constant<int, 16>());
+  }
 }
 
 }  // namespace f3r
@@ -1758,7 +2202,9 @@ f3r_status f3r_context_synchronize(f3r_context *ctx) {
 f3r_status f3r_sell_create(f3r_context *ctx, const f3r_csr *a, int32_t slice_height, int32_t sigma,
                            int32_t dtype_mask, f3r_sell **out) {
   if (!ctx || !out) return fail(F3R_ERROR_INVALID_VALUE, "null argument");
-  if (slice_height != 32) return fail(F3R_ERROR_UNSUPPORTED, "only slice height 32 is implemented");
+  if (slice_height != 32 && slice_height != 64) return fail(F3R_ERROR_UNSUPPORTED, "slice height 32 or 64");
+  if (slice_height == 64 && (sigma != 1 || (dtype_mask & (F3R_SELL_INDEX16 | F3R_SELL_CSR))))
+    return fail(F3R_ERROR_INVALID_VALUE, "slice height 64: sigma 1, offset-aligned slices");
   if ((dtype_mask & 7) == 0 || (dtype_mask & ~(7 | F3R_SELL_INDEX16 | F3R_SELL_ALIGNED | F3R_SELL_CSR)))
     return fail(F3R_ERROR_INVALID_VALUE,
                 "dtype_mask must select f64/f32/f16 (plus F3R_SELL_INDEX16, F3R_SELL_ALIGNED or F3R_SELL_CSR)");
@@ -1779,7 +2225,9 @@ f3r_status f3r_sell_create(f3r_context *ctx, const f3r_csr *a, int32_t slice_hei
   }
   SellHost h;
   F3R_TRY(build_sell(*a, sigma, false, h));
-  if (dtype_mask & F3R_SELL_ALIGNED) {
+  if (slice_height == 64) {
+    if (!align64(*a, h)) return fail(F3R_ERROR_UNSUPPORTED, "64-row slices need every 64 rows to share their offsets");
+  } else if (dtype_mask & F3R_SELL_ALIGNED) {
     if (align_offsets(*a, false, h) < 0) return fail(F3R_ERROR_UNSUPPORTED, "padded matrix exceeds 2^31 entries");
   } else if (dtype_mask & F3R_SELL_INDEX16) {
     compress_index16(h);
@@ -1799,7 +2247,7 @@ f3r_status f3r_sell_info_get(const f3r_sell *m, f3r_sell_info *info) {
   info->nrows = m->d.n;
   info->ncols = m->d.ncols;
   info->nnz = (int32_t)m->d.nnz;
-  info->slice_height = m->d.rptr ? 0 : 32;
+  info->slice_height = m->d.rptr ? 0 : m->d.height;
   info->sigma = m->d.sigma;
   info->nslices = m->d.nslices;
   info->nnz_padded = m->d.nnz_pad;
@@ -1939,7 +2387,7 @@ f3r_status f3r_solver_info(const f3r_solver *s, f3r_sell_info *a_info, int32_t *
     a_info->nrows = d.n;
     a_info->ncols = d.ncols;
     a_info->nnz = (int32_t)d.nnz;
-    a_info->slice_height = d.rptr ? 0 : 32;
+    a_info->slice_height = d.rptr ? 0 : d.height;
     a_info->sigma = d.sigma;
     a_info->nslices = d.nslices;
     a_info->nnz_padded = d.nnz_pad;
@@ -1968,6 +2416,33 @@ f3r_status f3r_solver_operate(f3r_solver *s, f3r_dtype val_t, f3r_dtype in_t, co
     return launch_sell(c, d.v16, A, (const __half *)in, EpiStore<float>{(float *)out, nullptr});
   return fail(F3R_ERROR_UNSUPPORTED, "unsupported (val, in, out) type combination");
 }
+
+f3r_status f3r_batch_create(f3r_context *ctx, int32_t count, const f3r_csr *const *a, const f3r_params *p,
+                            const f3r_csr *const *z, const f3r_csr *const *wt, f3r_batch **out) {
+  if (!ctx || !a || !p || !out || (z != nullptr) != (wt != nullptr)) return fail(F3R_ERROR_INVALID_VALUE, "bad argument");
+  Solver *s = nullptr;
+  F3R_TRY(make_batch(ctx, count, a, p, &s, z, wt));
+  *out = reinterpret_cast<f3r_batch *>(new f3r_solver{s});
+  return F3R_SUCCESS;
+}
+f3r_status f3r_batch_solve(f3r_batch *bt, const double *const *b, double *const *x, f3r_cond_fn cond, void *user,
+                           f3r_result *results) {
+  f3r_solver *s = reinterpret_cast<f3r_solver *>(bt);
+  if (!s || !b || !x) return fail(F3R_ERROR_INVALID_VALUE, "null argument");
+  for (int i = 0; i < s->s->mm_count; i++)
+    if (!b[i] || !x[i]) return fail(F3R_ERROR_INVALID_VALUE, "null vector");
+  CUDA_TRY(cudaSetDevice(s->s->ctx->device));
+  return s->s->solve_batch(b, x, cond, user, results);
+}
+f3r_status f3r_batch_info(const f3r_batch *bt, int32_t *count, int32_t *width, int32_t *precond_diagonal) {
+  const f3r_solver *s = reinterpret_cast<const f3r_solver *>(bt);
+  if (!s) return fail(F3R_ERROR_INVALID_VALUE, "null batch");
+  if (count) *count = s->s->mm_count;
+  if (width) *width = s->s->mm_k;
+  if (precond_diagonal) *precond_diagonal = s->s->precond_diag;
+  return F3R_SUCCESS;
+}
+void f3r_batch_destroy(f3r_batch *bt) { f3r_solver_destroy(reinterpret_cast<f3r_solver *>(bt)); }
 
 void f3r_solver_destroy(f3r_solver *s) {
   if (!s) return;

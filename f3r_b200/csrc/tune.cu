@@ -53,6 +53,62 @@ void time_shape_run(Context &c, const DeviceSell &d, const V *val, const X *x, Y
   out.push_back(t);
 }
 
+// the 64-row aligned kernel (k_sell64) at one launch shape
+template <typename V, typename X, typename Y, int W, int S>
+void time_shape64(Context &c, const DeviceSell &d, const V *val, const X *x, Y *y, int reps,
+                  std::vector<f3r_tune_entry> &out) {
+  auto k = k_sell64<V, X, EpiStore<Y>, W, S, kAllAlignedChunk>;
+  const size_t smem = sell64_smem_bytes_cfg<V, W, S, kAllAlignedChunk>();
+  int optin = 0;
+  if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c.device) != cudaSuccess ||
+      smem > (size_t)optin)
+    return;
+  if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return;
+  const DevSell A = d.view();
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(cdiv(A.nslices, W), c.sm_count));
+  const EpiStore<Y> epi{y, A.perm};
+  for (int i = 0; i < 2; i++) k<<<grid, W * 32, smem, c.stream>>>(val, A, x, epi, c.err);
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, c.stream);
+  for (int i = 0; i < reps; i++) k<<<grid, W * 32, smem, c.stream>>>(val, A, x, epi, c.err);
+  cudaEventRecord(e1, c.stream);
+  cudaEventSynchronize(e1);
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (cudaGetLastError() != cudaSuccess) return;
+  f3r_tune_entry t{};
+  t.warps = W;
+  t.stages = S;
+  t.kc = kAllAlignedChunk;
+  t.index_bits = 0;
+  t.is_default = (W == Sell64Cfg<V>::WARPS && S == Sell64Cfg<V>::STAGES) ? 1 : 0;
+  t.microseconds = ms * 1e3 / reps;
+  const double nnz = (double)d.nnz, n = (double)d.n;
+  t.gbs_algorithmic = (nnz * (sizeof(V) + 4) + 4 * (n + 1) + n * sizeof(X) + n * sizeof(Y)) / (t.microseconds * 1e3);
+  out.push_back(t);
+}
+
+template <typename V, typename X, typename Y>
+void sweep64(Context &c, const DeviceSell &d, const V *val, const X *x, Y *y, int reps,
+             std::vector<f3r_tune_entry> &out) {
+  time_shape64<V, X, Y, 32, 2>(c, d, val, x, y, reps, out);
+  time_shape64<V, X, Y, 28, 2>(c, d, val, x, y, reps, out);
+  time_shape64<V, X, Y, 24, 2>(c, d, val, x, y, reps, out);
+  time_shape64<V, X, Y, 24, 3>(c, d, val, x, y, reps, out);
+  time_shape64<V, X, Y, 20, 2>(c, d, val, x, y, reps, out);
+  time_shape64<V, X, Y, 16, 2>(c, d, val, x, y, reps, out);
+  time_shape64<V, X, Y, 16, 3>(c, d, val, x, y, reps, out);
+  time_shape64<V, X, Y, 12, 2>(c, d, val, x, y, reps, out);
+  time_shape64<V, X, Y, 10, 2>(c, d, val, x, y, reps, out);
+  time_shape64<V, X, Y, 8, 2>(c, d, val, x, y, reps, out);
+  time_shape64<V, X, Y, 6, 2>(c, d, val, x, y, reps, out);
+  time_shape64<V, X, Y, 4, 3>(c, d, val, x, y, reps, out);
+}
+
 // the aligned forms' value layouts are built for one chunk width each
 template <typename V, typename X, typename Y, int W, int S, int KC, typename CI>
 void time_shape(Context &c, const DeviceSell &d, const V *val, const X *x, Y *y, int reps,
@@ -104,7 +160,8 @@ Status run(Context &c, const DeviceSell &d, const V *val, int reps, std::vector<
     return s;
   }
   cudaMemsetAsync(x, 0, sizeof(X) * d.ncols, c.stream);
-  if (d.xoff) sweep<V, X, Y, AlignedIdx>(c, d, val, x, y, reps, out);
+  if (d.height == 64) sweep64<V, X, Y>(c, d, val, x, y, reps, out);
+  else if (d.xoff) sweep<V, X, Y, AlignedIdx>(c, d, val, x, y, reps, out);
   else if (d.cbase && !d.dcol) sweep<V, X, Y, AllAlignedIdx>(c, d, val, x, y, reps, out);
   else if (d.dcol) sweep<V, X, Y, uint16_t>(c, d, val, x, y, reps, out);
   else sweep<V, X, Y, int32_t>(c, d, val, x, y, reps, out);

@@ -77,19 +77,41 @@ class Learned:
         check(lib().f3r_learned_train(self._h, steps, lr, losses.ctypes.data))
         return losses
 
+    ENGINES = {"tcgen05": 1, "mma.sync": 2}
+
+    def _mode(self, bf16: bool, engine: str) -> int:
+        if not bf16:
+            return 0
+        if engine not in self.ENGINES:
+            raise ValueError(f"engine must be one of {sorted(self.ENGINES)}")
+        return self.ENGINES[engine]
+
     def correct(self, A: HostMatrix, nx: int, ny: int, Z: HostMatrix, Wt: HostMatrix, bf16: bool = True,
-                want_delta: bool = False):
-        """(Z', W'^T): the factors with corrected values (same pattern)."""
+                want_delta: bool = False, engine: str = "tcgen05"):
+        """(Z', W'^T): the factors with corrected values (same pattern).
+        bf16: BF16 tensor-core inference on `engine` ("tcgen05": TMEM
+        accumulators, 128-row tiles; "mma.sync": warp-level 16-row tiles),
+        else the fp32 training forward pass."""
+        mode = self._mode(bf16, engine)
         av, zv, wv = A.view(), Z.view(), Wt.view()
         zr, zi, _ = Z.arrays()
         wr, wi, _ = Wt.arrays()
         zval, wval = np.zeros(zv.nnz), np.zeros(wv.nnz)
         delta = np.zeros((av.nrows, 8), np.float32) if want_delta else None
-        check(lib().f3r_learned_correct(self._h, C.byref(av), nx, ny, C.byref(zv), C.byref(wv), 1 if bf16 else 0,
+        check(lib().f3r_learned_correct(self._h, C.byref(av), nx, ny, C.byref(zv), C.byref(wv), mode,
                                         zval.ctypes.data, wval.ctypes.data,
                                         None if delta is None else delta.ctypes.data))
         out = (HostMatrix.from_csr(zr, zi, zval), HostMatrix.from_csr(wr, wi, wval))
         return out + (delta,) if want_delta else out
+
+    def time_inference(self, A: HostMatrix, nx: int, ny: int, Z: HostMatrix, Wt: HostMatrix, bf16: bool = True,
+                       engine: str = "tcgen05", reps: int = 20) -> float:
+        """device microseconds of one launch of the network on A's features"""
+        av, zv, wv = A.view(), Z.view(), Wt.view()
+        us = C.c_double()
+        check(lib().f3r_learned_time_inference(self._h, C.byref(av), nx, ny, C.byref(zv), C.byref(wv),
+                                               self._mode(bf16, engine), reps, C.byref(us)))
+        return us.value
 
     def close(self):
         if getattr(self, "_h", None) is not None and _capi is not None and _capi._lib is not None:

@@ -20,8 +20,8 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--nx", type=int, default=192)
     ap.add_argument("--reps", type=int, default=20)
-    ap.add_argument("--forms", default="aligned,int32,index16,s256-int32,s256-index16",
-                    help="layouts to sweep: aligned, int32, index16 (sigma 1), s256-int32, s256-index16")
+    ap.add_argument("--forms", default="aligned64,aligned,int32,index16,s256-int32,s256-index16",
+                    help="layouts to sweep: aligned64, aligned, int32, index16 (sigma 1), s256-int32, s256-index16")
     ap.add_argument("--types", default="f16,f32,f64", help="value types to sweep")
     args = ap.parse_args()
     forms = set(args.forms.split(","))
@@ -29,12 +29,16 @@ def main():
     A = F.stencil27(args.nx, args.nx, args.nx, 2, 0.5).scale()
     ctx = F.Context(0)
     print(f"# SELL SpMV launch-shape sweep, {args.nx}^3 27-point (n={A.shape[0]}, nnz={A.nnz})\n")
-    for sigma, form in ((1, "aligned"), (1, "int32"), (1, "index16"), (256, "int32"), (256, "index16")):
+    for sigma, form in ((1, "aligned64"), (1, "aligned"), (1, "int32"), (1, "index16"), (256, "int32"),
+                        (256, "index16")):
         if (form if sigma == 1 else f"s256-{form}") not in forms:
             continue
-        S = F.Sell(ctx, A, sigma=sigma, index16=form == "index16", aligned=form == "aligned")
+        S = F.Sell(ctx, A, sigma=sigma, index16=form == "index16", aligned=form.startswith("aligned"),
+                   height=64 if form == "aligned64" else 32)
         bits = S.info().index_bits
         label = "offset-aligned (no stored index)" if bits == 0 else f"{bits}-bit indices"
+        if form == "aligned64":
+            label = "64-row offset-aligned slices (two rows a lane, no stored index)"
         for vt, name, key in ((F.F16, "fp16 values x fp32 vectors", "f16"), (F.F32, "fp32", "f32"),
                               (F.F64, "fp64", "f64")):
             if key not in types:

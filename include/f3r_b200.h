@@ -82,7 +82,9 @@ typedef struct f3r_params {
   int32_t ilu_blocks;      /* block-Jacobi blocks: 112 (f3r.cpp:57) */
   double sdainv_tol;       /* drop tolerance: 0.1 (f3r-gpu.cpp:74) */
   double acc;              /* diagonal shift for SDAINV / ILU: 1.0 */
-  int32_t sell_c;          /* SELL slice height: 32 (the only one the kernels take) */
+  int32_t sell_c;          /* SELL slice height: 32, or 64 (64-row offset-aligned slices, every
+                              64 rows sharing their column offsets, sigma 1: each lane of the
+                              product works two rows with one set of slot bases; the same sums) */
   int32_t sell_sigma;      /* SELL sorting window: 1 = no sorting */
   double rel_tol;          /* stop when |implicit residual| / ||b|| < rel_tol and no
                               cond callback is given: 1e-8 (f3r-gpu.cpp:18) */
@@ -113,8 +115,9 @@ typedef struct f3r_params {
                               sell_sigma = 1 a stencil aligns every slice.  Same sums in the same
                               order as the packed layout.  0 */
   int32_t sell_autotune;   /* 1: at set-up, build the fp16 copy of the matrix in each candidate
-                              layout (offset-aligned SELL sigma 1; packed SELL sigma 1 with 32- and
-                              16-bit indices; packed and aligned SELL sigma 256; CSR), time the fp16
+                              layout (offset-aligned SELL sigma 1 with 32- and 64-row slices; packed
+                              SELL sigma 1 with 32- and 16-bit indices; packed and aligned SELL
+                              sigma 256; CSR), time the fp16
                               product on it, and solve in the fastest; the layout fields above are
                               then ignored (f3r_solver_info reports the choice).  All give the same
                               sums at sigma 1; sigma 256 permutes the rows.  0 */
@@ -409,6 +412,33 @@ void f3r_solver_destroy(f3r_solver *s);
 f3r_status f3r_solver_create_factors(f3r_context *ctx, const f3r_csr *a, const f3r_params *p, const f3r_csr *z,
                                      const f3r_csr *wt, f3r_solver **out);
 
+/* ---- batches of systems of one sparsity pattern --------------------------
+ * Up to 16 systems that share one pattern (one grid and stencil with
+ * different coefficients, for example) solved together: one lockstep solve
+ * K columns wide (K = 2, 4, 8 or 16, the systems padded with inactive
+ * columns), each column its own system with its own matrix values and its
+ * own SDAINV factors, every product streaming the shared pattern once and
+ * the systems' values interleaved.  Each system's result is that of
+ * f3r_solver_solve on it with the same parameters, up to the layout: the
+ * batch stores the matrices in packed SELL (sell_align, sell_index16 and
+ * sell_autotune are ignored).  Takes F3R_PRECOND_SDAINV, FGMRES levels (no
+ * inner_sstep, no half_m) and format SELL.  The reference solves one
+ * system per run (work/src/f3r-gpu.cpp:88); it has no counterpart. */
+typedef struct f3r_batch f3r_batch;
+/* a[i]: system i (count of them, one pattern); z, wt: NULL (SDAINV computed
+ * per system) or count given factor pairs as f3r_solver_create_factors */
+f3r_status f3r_batch_create(f3r_context *ctx, int32_t count, const f3r_csr *const *a, const f3r_params *p,
+                            const f3r_csr *const *z, const f3r_csr *const *wt, f3r_batch **out);
+/* b[i], x[i]: system i's right-hand side and initial guess / solution, host
+ * or device vectors; results: one per system (may be NULL).  cond(i, |e|)
+ * is called for every unfinished system after every outer step, in order. */
+f3r_status f3r_batch_solve(f3r_batch *b, const double *const *bv, double *const *x, f3r_cond_fn cond, void *user,
+                           f3r_result *results);
+/* count: systems; width: the block's K; precond_diagonal: 1 when every
+ * system's SDAINV factors are diagonal */
+f3r_status f3r_batch_info(const f3r_batch *b, int32_t *count, int32_t *width, int32_t *precond_diagonal);
+void f3r_batch_destroy(f3r_batch *b);
+
 /* ---- learned correction of the SDAINV values ---------------------------
  * No reference counterpart.  A network 7 -> 64 -> 64 -> 8 (ReLU) maps the
  * seven coefficients of row i of a 7-point matrix in natural order (column
@@ -441,10 +471,18 @@ f3r_status f3r_learned_evaluate(f3r_learned *l, double *loss, float *grad);
  * receives the loss before each step */
 f3r_status f3r_learned_train(f3r_learned *l, int32_t steps, double lr, double *losses);
 /* Corrected factor values of a system: z_val / wt_val (nnz of z / wt) and,
- * when delta is not NULL, the raw network outputs (n x 8).  bf16 != 0 runs
- * the BF16 tensor-core inference, else the fp32 training forward pass. */
+ * when delta is not NULL, the raw network outputs (n x 8).  bf16 selects the
+ * forward pass: 0 the fp32 training forward pass, 1 BF16 inference on the
+ * tcgen05 tensor cores (TMEM accumulators), 2 BF16 inference on mma.sync
+ * (the warp-level tensor-core path, kept for comparison); 1 and 2 share their
+ * arithmetic (bf16 operands, fp32 accumulation and bias). */
 f3r_status f3r_learned_correct(f3r_learned *l, const f3r_csr *a, int32_t nx, int32_t ny, const f3r_csr *z,
                                const f3r_csr *wt, int32_t bf16, double *z_val, double *wt_val, float *delta);
+/* Device time of the network alone on a system's features (mode as bf16
+ * above): one warm-up launch, then reps launches timed with CUDA events on
+ * the context's stream; *us = microseconds per launch. */
+f3r_status f3r_learned_time_inference(f3r_learned *l, const f3r_csr *a, int32_t nx, int32_t ny, const f3r_csr *z,
+                                      const f3r_csr *wt, int32_t mode, int32_t reps, double *us);
 
 #ifdef __cplusplus
 }

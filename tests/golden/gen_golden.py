@@ -23,12 +23,14 @@ contraction, one OpenMP thread), and records its outputs:
 Usage (needs the reference tree; the fixtures are committed):
     OMP_NUM_THREADS=1 python tests/golden/gen_golden.py [--big]
     python tests/golden/gen_golden.py --envelope [--big] [--only=name,name]
+    python tests/golden/gen_golden.py --oracle [--big] [--only=name,name]
 --big adds the 64^3 CPU configuration and the 192^3 GPU configuration solve
 (about a minute of CPU each).  --envelope re-runs every golden solve at 1, 2,
 3, 4 and 8 OpenMP threads (up to 64 for the fp16-vector depth ablations) and
 stores the reference's residual histories as <name>_env, the thread counts as
 <name>_env_threads: the spread the reference shows when only its summation
-order changes.
+order changes.  --oracle stores the oracle's history of every golden solve in
+the library's arithmetic as <name>_oracle.
 """
 from __future__ import annotations
 
@@ -339,9 +341,43 @@ def main(big: bool):
     np.savez_compressed(existing, **sol)
 
 
+def oracle_rows(big, only=None):
+    """The oracle's history of every golden solve in the library's arithmetic
+    (oracle/f3r_oracle.c, ARITH_PRODUCT: fp16 products accumulated in fp32),
+    stored as <name>_oracle.  It restates the reference's algorithm exactly
+    and differs from it only in that arithmetic, so the band of
+    tests/history_band.py spans it beside the reference's own runs."""
+    sys.path.insert(0, os.path.dirname(HERE))
+    from history_band import CASES
+    path = os.path.join(HERE, "solves.npz")
+    sol = dict(np.load(path))
+    ref = O.Ref("golden")
+    for name, config, spec, seed in solve_cases(big):
+        if only and name not in only:
+            continue
+        rr, ii, vv = case_system(ref, name, spec)
+        xs, b = rhs_for(ref, rr, ii, vv, seed)
+        cfg = CASES[name]
+        A = O.Mat.from_csr(rr, ii, vv)
+        if cfg.get("precond", 0) == 1:
+            P1, P2 = O.ilu0_bj(A, cfg["ilu_blocks"])
+        else:
+            Z, W = O.sdainv(A)
+            P1, P2 = W, Z
+        kw = {k: cfg[k] for k in ("m2", "m3", "m4", "static_weight", "c", "half_m") if k in cfg}
+        if "inner_sstep" in cfg:
+            kw["sstep"] = cfg["inner_sstep"]
+        o = O.f3r_solve(A, P1, P2, b, O.params(precond=cfg.get("precond", 0), tol=1e-10, **kw))
+        sol[name + "_oracle"] = o["hist"]
+        print(name, "oracle", o["iters"], flush=True)
+    np.savez_compressed(path, **sol)
+
+
 if __name__ == "__main__":
+    sel = [a.split("=", 1)[1].split(",") for a in sys.argv if a.startswith("--only=")]
     if "--envelope" in sys.argv:
-        sel = [a.split("=", 1)[1].split(",") for a in sys.argv if a.startswith("--only=")]
         envelope("--big" in sys.argv, sel[0] if sel else None)
+    elif "--oracle" in sys.argv:
+        oracle_rows("--big" in sys.argv, sel[0] if sel else None)
     else:
         main("--big" in sys.argv)

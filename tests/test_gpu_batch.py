@@ -94,14 +94,15 @@ def test_block_solve_columns_bit_identical(nrhs, layout):
     assert all(r.is_solved and r.expl_rel_res < 1e-10 for r in res)
 
 
-def test_block_solve_general_sdainv_and_uneven_convergence():
-    """non-diagonal SDAINV factors (block products of W^T and Z); columns that
-    finish at different steps (an exact initial guess stops at step 0, a
-    smooth right-hand side converges sooner than noise) leave the lockstep
-    without disturbing the others"""
+@pytest.mark.parametrize("align", [0, 1])
+def test_block_solve_general_sdainv_and_uneven_convergence(align):
+    """non-diagonal SDAINV factors (block products of W^T and Z; aligned: the
+    mixed offset-aligned form); columns that finish at different steps (an
+    exact initial guess stops at step 0, a smooth right-hand side converges
+    sooner than noise) leave the lockstep without disturbing the others"""
     ctx = F.Context(0)
     A = F.diffusion7(16, 15, 14, 1.5, 3.0, 4).scale()
-    S = F.Solver(ctx, A, rel_tol=1e-10, c=4)
+    S = F.Solver(ctx, A, rel_tol=1e-10, c=4, sell_align=align)
     assert not S.info()[1]
     n = A.shape[0]
     rng = np.random.default_rng(9)
@@ -139,3 +140,72 @@ def test_block_solve_multi_rhs_device_and_static_weight():
         Xh = np.zeros_like(B)
         S.solve_multi(B, Xh)
         assert np.array_equal(Xd.cpu().numpy(), Xh), kw
+
+
+def _fields(kind, count, nx=14):
+    """count systems of one pattern: log-normal diffusion fields (general
+    SDAINV factors) or the 27-point stencil with different beta (diagonal)"""
+    out = []
+    for s in range(count):
+        if kind == "diffusion":
+            A = F.diffusion7(nx, nx - 1, nx + 1, 1.5, 3.0, 100 + s)
+        else:
+            A = F.stencil27(nx, nx - 1, nx + 1, 2, 0.1 + 0.1 * s)
+        out.append(A.scale())
+    return out
+
+
+@pytest.mark.parametrize("kind,count,sigma", [("diffusion", 3, 1), ("diffusion", 8, 1), ("stencil", 5, 1),
+                                              ("stencil", 2, 256), ("diffusion", 16, 256)])
+def test_batch_of_one_pattern_equals_single_solves(kind, count, sigma):
+    """systems of one pattern solved together (f3r_batch: every column of the
+    block solve its own system, values interleaved, SDAINV factors on the
+    union pattern): each system's iterate is its single solve's (packed SELL,
+    the batch's layout), bit for bit"""
+    ctx = F.Context(0)
+    systems = _fields(kind, count)
+    B = F.Batch(ctx, systems, rel_tol=1e-10, c=4, sell_sigma=sigma)
+    c, k, diag = B.info()
+    assert c == count and k >= count and diag == (kind == "stencil")
+    n = systems[0].shape[0]
+    rng = np.random.default_rng(count)
+    bs = [rng.standard_normal(n) for _ in range(count)]
+    xs = [np.zeros(n) for _ in range(count)]
+    res = B.solve(bs, xs)
+    for i, A in enumerate(systems):
+        S = F.Solver(ctx, A, rel_tol=1e-10, c=4, sell_sigma=sigma, sell_align=0)
+        x = np.zeros(n)
+        r = S.solve(bs[i].copy(), x)
+        assert np.array_equal(xs[i], x), i
+        assert res[i].res_iter == r.res_iter and res[i].is_solved and res[i].expl_rel_res < 1e-10, i
+        S.close()
+    # device vectors, and the same solve again (graphs replayed)
+    bd = [torch.from_numpy(b).cuda() for b in bs]
+    xd = [torch.zeros_like(b) for b in bd]
+    B.solve(bd, xd)
+    for i in range(count):
+        assert np.array_equal(xd[i].cpu().numpy(), xs[i])
+
+
+def test_batch_with_given_factors_and_rejections():
+    """given SDAINV factors per system (f3r_solver_create_factors' form), and
+    the batch's checks: one pattern, at most 16 systems, SDAINV only"""
+    ctx = F.Context(0)
+    systems = _fields("diffusion", 4)
+    fac = [A.sdainv() for A in systems]
+    B = F.Batch(ctx, systems, factors=fac, rel_tol=1e-10, c=4)
+    n = systems[0].shape[0]
+    bs = [np.ones(n) * (i + 1) for i in range(4)]
+    xs = [np.zeros(n) for _ in range(4)]
+    res = B.solve(bs, xs)
+    for i, A in enumerate(systems):
+        S = F.Solver(ctx, A, factors=fac[i], rel_tol=1e-10, c=4, sell_align=0)
+        x = np.zeros(n)
+        S.solve(bs[i].copy(), x)
+        assert np.array_equal(xs[i], x) and res[i].is_solved
+    with pytest.raises(F.F3RError, match="pattern"):
+        F.Batch(ctx, [systems[0], F.stencil27(14, 13, 15, 2, 0.5).scale()])
+    with pytest.raises(F.F3RError):
+        F.Batch(ctx, _fields("stencil", 17, nx=6))
+    with pytest.raises(F.F3RError):
+        F.Batch(ctx, systems, precond=F.PRECOND_ILU0_BJ, ilu_blocks=4)

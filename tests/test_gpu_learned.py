@@ -36,8 +36,8 @@ def random_params(L, seed, scale=0.05):
 def test_untrained_network_is_plain_sdainv(ctx):
     A, Z, Wt = stacked(8, (1, 2))
     L = Learned(ctx, seed=3)
-    for bf16 in (True, False):
-        Zc, Wc = L.correct(A, 8, 8, Z, Wt, bf16=bf16)
+    for bf16, engine in ((True, "tcgen05"), (True, "mma.sync"), (False, "tcgen05")):
+        Zc, Wc = L.correct(A, 8, 8, Z, Wt, bf16=bf16, engine=engine)
         assert np.array_equal(Zc.arrays()[2], Z.arrays()[2])
         assert np.array_equal(Wc.arrays()[2], Wt.arrays()[2])
 
@@ -78,6 +78,8 @@ def test_forward_and_bf16_inference_match_reference(ctx):
     Zb, Wb, d16 = L.correct(A, nt, nt, Z, Wt, bf16=True, want_delta=True)
     # bf16 weights and activations (8-bit mantissa), fp32 accumulation over 64 terms
     assert np.max(np.abs(d16 - want)) <= 3e-2 * scale
+    _, _, dm = L.correct(A, nt, nt, Z, Wt, bf16=True, want_delta=True, engine="mma.sync")
+    assert np.max(np.abs(dm - want)) <= 3e-2 * scale
     # corrected values v (1 + delta) on the fixed pattern
     zr, zi, zv = Z.arrays()
     rows = np.repeat(np.arange(len(zr) - 1), np.diff(zr))
@@ -85,6 +87,39 @@ def test_forward_and_bf16_inference_match_reference(ctx):
     expect = np.where(sl >= 0, zv * (1 + d32[rows, np.maximum(sl, 0)].astype(np.float64)), zv)
     assert np.allclose(Zc.arrays()[2], expect, rtol=1e-15, atol=0)
     assert np.array_equal(Zb.arrays()[1], zi)
+
+
+@pytest.mark.parametrize("nt", [9, 64, 71])
+def test_tcgen05_inference_matches_mma_sync(ctx, nt):
+    """The tcgen05 kernel (128-row tiles, TMEM accumulators) and the mma.sync
+    kernel round the same operands to bf16 and accumulate in fp32; only the
+    order of the fp32 sums differs, which can move an activation by one bf16
+    step.  729 rows: one ragged tile per warpgroup; 64^3 and 71^3: more tiles
+    than warpgroups (the persistent loop), 71^3 ragged."""
+    A = F.diffusion7(nt, nt, nt, 1.5, 6.0, 5).scale()
+    Z, Wt = A.sdainv()
+    L = Learned(ctx, seed=4)
+    p = random_params(L, 10, scale=0.2)
+    L.params = p
+    want = R.delta(p.astype(np.float64), A.arrays(), nt, nt)
+    scale = np.max(np.abs(want))
+    _, _, dt = L.correct(A, nt, nt, Z, Wt, bf16=True, want_delta=True, engine="tcgen05")
+    _, _, dm = L.correct(A, nt, nt, Z, Wt, bf16=True, want_delta=True, engine="mma.sync")
+    assert np.all(np.isfinite(dt))
+    assert np.max(np.abs(dt - want)) <= 3e-2 * scale
+    assert np.max(np.abs(dt - dm)) <= 1e-2 * scale
+    # most rows see no activation rounding flip at all
+    assert np.mean(np.all(np.abs(dt - dm) <= 1e-5 * scale, axis=1)) > 0.9
+    us_t = L.time_inference(A, nt, nt, Z, Wt, engine="tcgen05", reps=5)
+    us_m = L.time_inference(A, nt, nt, Z, Wt, engine="mma.sync", reps=5)
+    assert us_t > 0 and us_m > 0
+
+
+def test_inference_engine_is_checked(ctx):
+    A, Z, Wt = stacked(8, (1,))
+    L = Learned(ctx, seed=3)
+    with pytest.raises(ValueError):
+        L.correct(A, 8, 8, Z, Wt, engine="wmma")
 
 
 def test_solver_from_given_factors_is_the_plain_solver(ctx):

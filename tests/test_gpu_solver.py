@@ -187,6 +187,7 @@ def test_layout_autotuner(ctx, kind):
     r1 = S.solve(b, x1)
     assert r1.is_solved and r1.expl_rel_res < 1e-10
     kw = dict(format=fmt, sell_sigma=info.sigma, sell_align=1 if info.index_bits == 0 else 0,
+              sell_c=info.slice_height if info.slice_height else 32,
               sell_index16=1 if info.index_bits == 16 else 0)
     S2 = F.Solver(ctx, A, rel_tol=1e-10, c=8, **kw)
     i2, _ = S2.info()
@@ -209,3 +210,24 @@ def test_aligned_sell_solve_is_identical(ctx):
         assert r.is_solved and r.expl_rel_res < 1e-10
         xs.append(x)
     assert np.array_equal(xs[0], xs[1])
+
+
+def test_slice_height_64_solve_is_identical(ctx):
+    """the solver on 64-row slices (sell_c = 64) reproduces the 32-row
+    aligned layout's solve bit for bit, the fused Richardson steps and the
+    weight updates included"""
+    A = F.stencil27(24, 20, 18, 2, 0.5).scale()
+    b = A.spmv(F.random_uniform(7, -1, 1, A.shape[0]))
+    xs = []
+    for kw in (dict(sell_align=1), dict(sell_c=64)):
+        S = F.Solver(ctx, A, rel_tol=1e-10, c=4, **kw)
+        info, _ = S.info()
+        assert info.slice_height == kw.get("sell_c", 32)
+        x = np.zeros(len(b))
+        r = S.solve(b, x)
+        assert r.is_solved and r.expl_rel_res < 1e-10
+        xs.append(x)
+        S.close()
+    assert np.array_equal(xs[0], xs[1])
+    with pytest.raises(F.F3RError):
+        F.Solver(ctx, A, sell_c=64, sell_sigma=256)

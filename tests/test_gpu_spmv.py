@@ -152,6 +152,36 @@ def test_aligned_stencil_matches_packed(ctx, dims):
         assert np.array_equal(y1.cpu().numpy().view(np.uint8), y2.cpu().numpy().view(np.uint8)), (vt, dt)
 
 
+@pytest.mark.parametrize("dims", [(32, 20, 9), (16, 16, 16), (33, 7, 5), (64, 3, 3)])
+def test_slice_height_64_matches_32(ctx, dims):
+    """64-row offset-aligned slices (each lane two rows, one set of slot
+    bases): every value type's product, residual included, equals the 32-row
+    layouts' bit for bit, clamped first and last slices and a ragged last
+    slice included"""
+    A = F.stencil27(*dims, 2, 0.5).scale()
+    n = A.shape[0]
+    S32, S64 = F.Sell(ctx, A, aligned=True), F.Sell(ctx, A, height=64)
+    assert S64.info().slice_height == 64 and S64.info().index_bits == 0
+    assert S64.info().nslices == (n + 63) // 64
+    rng = np.random.default_rng(19)
+    for vt, dt in ((F.F16, torch.float32), (F.F32, torch.float32), (F.F64, torch.float64), (F.F16, torch.float16)):
+        x = torch.from_numpy(rng.standard_normal(n)).to(dt).cuda()
+        y1 = torch.zeros(n, dtype=dt, device="cuda")
+        y2 = torch.zeros_like(y1)
+        S32.operate(x, y1, val_t=vt)
+        S64.operate(x, y2, val_t=vt)
+        torch.cuda.synchronize()
+        assert np.array_equal(y1.cpu().numpy().view(np.uint8), y2.cpu().numpy().view(np.uint8)), (vt, dt)
+    b = torch.from_numpy(rng.standard_normal(n)).cuda()
+    x = torch.from_numpy(rng.standard_normal(n)).cuda()
+    r1, r2 = torch.zeros_like(b), torch.zeros_like(b)
+    S32.compute_residual(b, x, r1)
+    S64.compute_residual(b, x, r2)
+    assert torch.equal(r1, r2)
+    with pytest.raises(F.F3RError):  # a matrix whose rows do not share offsets
+        F.Sell(ctx, F.diffusion7(9, 8, 7, 1.5, 3.0, 2).scale().sdainv()[0], height=64)
+
+
 def test_fp16_within_reference_bound(ctx):
     """against the reference's fp16-accumulated SELL<32,__half>::operate"""
     ref = O.Ref("golden")
