@@ -50,6 +50,7 @@ NX = 192
 BETA = 0.5
 SIGMA = 1
 ALIGN = 1
+SELL_C = 64
 LAYOUTS = {"aligned": dict(sell_sigma=1, sell_align=1, format=0, sell_c=32),
            "aligned64": dict(sell_sigma=1, sell_align=1, format=0, sell_c=64),
            "sigma256": dict(sell_sigma=256, sell_align=0, format=0, sell_c=32),
@@ -57,10 +58,10 @@ LAYOUTS = {"aligned": dict(sell_sigma=1, sell_align=1, format=0, sell_c=32),
            "auto": dict(sell_sigma=1, sell_align=0, format=0, sell_autotune=1, sell_c=32)}
 TOL = 1e-10
 PARAMS = dict(m_outer=100, max_restarts=20, m2=8, m3=4, m4=2, c=64, sdainv_tol=0.1, acc=1.0, sell_sigma=SIGMA,
-              sell_align=ALIGN, format=0,
+              sell_align=ALIGN, format=0, sell_c=SELL_C,
               rel_tol=TOL, use_graphs=1)
 METRIC = "time to 1e-10 FP64 relative residual, plain F3R (fp64/fp32/fp16 nested FGMRES), 192^3 27-pt nonsymmetric"
-WORKLOAD = "F3R-SDAINV-SELL32al stencil27-halfspace beta0.5 192^3 (n=7077888, nnz=189119224), tol 1e-10"
+WORKLOAD = "F3R-SDAINV-SELL64al stencil27-halfspace beta0.5 192^3 (n=7077888, nnz=189119224), tol 1e-10"
 
 
 PRECONDS = {"sdainv": 0, "ilu-bj": 1, "ilu-jacobi": 2, "ilu-baj": 3, "ilu-level": 4}
@@ -425,7 +426,7 @@ def run_ours(args):
     ctx.close()
     if rank == 0:
         if world == 1 and not args.no_extra and NX == 192:  # the configurations' own sizes, headline runs only
-            line["extra"] = extra_block(args)
+            line["extra"] = extra_block(args, A)
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
@@ -510,7 +511,8 @@ def c4_line(args):
     ctxs, solvers = [], []
     for kind, e, A, B in systems:
         ctxs.append(F.Context(0))
-        solvers.append(F.Solver(ctxs[-1], A, **PARAMS))
+        # lockstep blocks take 32-row slices (64-row slices would solve the columns one after another)
+        solvers.append(F.Solver(ctxs[-1], A, **{**PARAMS, **LAYOUTS["aligned"]}))
     Bd = [torch.from_numpy(B).cuda() for _, _, _, B in systems]
     Xd = [torch.zeros_like(b) for b in Bd]
     batch = [(S, b, x) for S, b, x in zip(solvers, Bd, Xd)]
@@ -563,7 +565,8 @@ def c4_line(args):
             "config": {"workload": "C4 batched: 96 systems, 7-pt diffusion / 27-pt stencil, edge U{16..112}, "
                                    "nrhs U{1..16}, RHS N(0,1), tol 1e-10",
                        "systems": len(systems), "rhs": nrhs, "rows_x_rhs": rows,
-                       "sell": layout_desc(), "timing": "host wall clock, device synchronised on both sides"},
+                       "sell": layout_desc({**PARAMS, **LAYOUTS["aligned"]}),
+                       "timing": "host wall clock, device synchronised on both sides"},
             "batched_ms": round(tb * 1e3, 2), "sequential_ms": round(ts * 1e3, 2),
             "blocks_one_system_at_a_time_ms": round(tk * 1e3, 2),
             "speedup_batched_vs_sequential": round(ts / tb, 2), "speedup_blocks_vs_sequential": round(ts / tk, 2),
@@ -738,10 +741,61 @@ def run_c1(args):
 C5_BATCH = 8  # held-out systems kept for the batched comparison (two solvers each)
 
 
-def extra_block(args):
+def c2_block_line(args, A):
+    """K right-hand sides of the headline 192^3 system solved as one
+    lockstep block (f3r_solver_solve_multi) against the same K solved one at a
+    time on the same solver; device time (CUDA events) of each, and whether
+    every block column is bit for bit its single solve.  The block kernels
+    take 32-row slices, so this solver uses the 32-row offset-aligned layout."""
+    import torch
+    import f3r_b200 as F
+    K = args.block_k
+    torch.cuda.set_device(0)
+    ctx = F.Context(0)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    ctx.set_stream(stream.cuda_stream)
+    kw = {**PARAMS, **LAYOUTS["aligned"], "sell_autotune": 0}
+    S = F.Solver(ctx, A, **kw)
+    n = A.shape[0]
+    B = np.stack([A.spmv(F.random_uniform(100 + k, -1.0, 1.0, n)) for k in range(K)])
+    B_d = torch.from_numpy(B).cuda()
+    Xb, Xs = torch.zeros_like(B_d), torch.zeros_like(B_d)
+    S.solve_multi(B_d, Xb)      # warm-up: the block's work buffers and graphs
+    S.solve(B_d[0], Xs[0])
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        e0.record(stream)
+        out = fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1), out
+
+    Xb.zero_()
+    tb, rb = timed(lambda: S.solve_multi(B_d, Xb))
+    Xs.zero_()
+    ts, rs = timed(lambda: [S.solve(B_d[k], Xs[k]) for k in range(K)])
+    line = {"workload": f"C2 192^3 27-point stencil, {K} right-hand sides b_k = A x*_k, x*_k ~ U(-1, 1)",
+            "rhs": K, "sell": "32-row offset-aligned slices, sigma 1",
+            "timing": "device time, CUDA events on the solver's stream",
+            "block_ms": round(tb, 2), "singles_ms": round(ts, 2),
+            "block_ms_per_rhs": round(tb / K, 2), "single_ms_per_rhs": round(ts / K, 2),
+            "per_rhs_time_ratio_block_vs_single": round(tb / ts, 3),
+            "all_solved": all(r.is_solved for r in rb), "outer_iters": [r.res_iter for r in rb],
+            "columns_bit_identical_to_single_solves": bool(torch.equal(Xb, Xs)),
+            "worst_expl_rel_res": max(r.expl_rel_res for r in rb)}
+    S.close()
+    ctx.close()
+    return line
+
+
+def extra_block(args, A=None):
     """The learned / batched / precision-stress half of the metric, measured
     after the headline solve and outside its timed region, at the sizes of
-    their configurations: C5 (learned vs plain SDAINV, held-out 128^3
+    their configurations: C2 block (K right-hand sides of the headline system
+    in one lockstep block), C5 (learned vs plain SDAINV, held-out 128^3
     fields), C4 (the 96-system batch), C3 (the 256^3 precision stress).  Each
     is timed with its own clock (stated in its config) and reported in full;
     a part that fails is reported as an error string instead."""
@@ -752,7 +806,10 @@ def extra_block(args):
     sub.steps, sub.warmup, sub.nx = 2, 1, NX
     sub.c5_eval = max(args.c5_eval, 8)
     saved = dict(PARAMS)
-    for key, fn in (("c5", c5_line), ("c4", c4_line), ("c3", c3_line)):
+    parts = [("c5", c5_line), ("c4", c4_line), ("c3", c3_line)]
+    if A is not None:
+        parts.insert(0, ("c2_block", lambda a: c2_block_line(a, A)))
+    for key, fn in parts:
         t0 = time.perf_counter()
         try:
             PARAMS.clear()
@@ -914,18 +971,22 @@ def main():
                     help="innermost preconditioner of our arm (the headline is sdainv)")
     ap.add_argument("--ilu-blocks", type=int, default=112)
     ap.add_argument("--trsv-iters", type=int, default=2)
-    ap.add_argument("--layout", default="aligned", choices=sorted(LAYOUTS),
-                    help="matrix layout of our arm: offset-aligned SELL sigma=1 (default), packed SELL sigma=256, CSR, or "
-                         "auto (the library's layout autotuner picks at set-up)")
+    ap.add_argument("--layout", default="aligned64", choices=sorted(LAYOUTS),
+                    help="matrix layout of our arm: offset-aligned SELL sigma=1 with 64-row slices (default) or "
+                         "32-row slices (aligned), packed SELL sigma=256, CSR, or auto (the library's layout "
+                         "autotuner picks at set-up)")
     ap.add_argument("--no-alt-layout", action="store_true", help="skip timing the other layout")
     ap.add_argument("--no-extra", action="store_true",
-                    help="skip the C5 / C4 / C3 measurements the default C2 line carries under `extra`")
-    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c4", "c5"],
-                    help="c2: the headline solve; c3: the precision stress (256^3 diffusion, per-level errors); "
+                    help="skip the C2-block / C5 / C4 / C3 measurements the default C2 line carries under `extra`")
+    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c2block", "c3", "c4", "c5"],
+                    help="c2: the headline solve; c2block: --block-k right-hand sides of the c2 system as one "
+                         "lockstep block against one at a time; "
+                         "c3: the precision stress (256^3 diffusion, per-level errors); "
                          "c4: the batched configuration (96 systems, 1-16 RHS each); "
                          "c5: the learned preconditioner (training, then held-out 128^3 solves); "
                          "c1: the reference's CPU configuration (64^3 hpcg, BJ-ILU(0) x112, CSR) on the GPU and, "
                          "beside it, the reference's CPU solve")
+    ap.add_argument("--block-k", type=int, default=8, help="right-hand sides of the C2 block measurement")
     ap.add_argument("--c5-train", type=int, default=256, help="C5 training fields")
     ap.add_argument("--c5-eval", type=int, default=4, help="C5 held-out fields solved (32 for the full set)")
     ap.add_argument("--c5-steps", type=int, default=500, help="C5 Adam steps")
@@ -943,6 +1004,9 @@ def main():
         run_c4(args)
     elif args.config == "c3":
         run_c3(args)
+    elif args.config == "c2block":
+        A, _, _ = make_problem(seed=replica_seed(0))
+        print(json.dumps(c2_block_line(args, A)), flush=True)
     elif args.impl == "reference":
         run_reference(args)
     else:

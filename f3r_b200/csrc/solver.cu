@@ -200,8 +200,12 @@ bool align64(const f3r_csr &a, SellHost &s) {
   const int32_t n = a.nrows, nc = a.ncols, ns = (int32_t)cdiv(n, 64);
   std::vector<std::vector<int32_t>> D(ns);
   std::vector<char> in_range(ns, 1);
-  int64_t not_ok = 0;
-#pragma omp parallel for schedule(dynamic, 256) reduction(+ : not_ok)
+  // a slice's slots are the union D of its rows' offsets; the layout is taken
+  // when the slots of all slices together are at most 5/4 of the packed
+  // widths (slices that straddle a plane of a small grid gain a few), and no
+  // slice more than doubles its packed width
+  int64_t not_ok = 0, slots = 0, packed = 0;
+#pragma omp parallel for schedule(dynamic, 256) reduction(+ : not_ok, slots, packed)
   for (int32_t sl = 0; sl < ns; sl++) {
     std::vector<int32_t> d;
     int32_t wstd = 0;
@@ -213,14 +217,16 @@ bool align64(const f3r_csr &a, SellHost &s) {
     }
     std::sort(d.begin(), d.end());
     d.erase(std::unique(d.begin(), d.end()), d.end());
-    if (d.empty() || (int64_t)d.size() * 4 > (int64_t)wstd * 5) {
+    if (d.empty() || (int64_t)d.size() > 2 * (int64_t)wstd) {
       not_ok++;
       continue;
     }
+    slots += (int64_t)d.size();
+    packed += wstd;
     in_range[sl] = (int64_t)sl * 64 + d.front() >= 0 && (int64_t)sl * 64 + d.back() + 63 < nc;
     D[sl] = std::move(d);
   }
-  if (not_ok) return false;
+  if (not_ok || slots * 4 > packed * 5) return false;
   std::vector<int32_t> sptr(ns + 1, 0), cbptr(ns + 1, 0), width(ns);
   for (int32_t sl = 0; sl < ns; sl++) {
     width[sl] = ((int32_t)D[sl].size() + 3) & ~3;
