@@ -213,9 +213,12 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def profiled_traffic(aligned=False):
+def profiled_traffic(aligned=False, height=32):
     """dram bytes per launch of the dominant kernel from the committed ncu summary"""
-    name = "spmv_f16_aligned_c2_traffic.txt" if aligned else "spmv_f16_c2_traffic.txt"
+    if aligned and height == 64:
+        name = "spmv_f16_aligned64_c2_traffic.txt"
+    else:
+        name = "spmv_f16_aligned_c2_traffic.txt" if aligned else "spmv_f16_c2_traffic.txt"
     path = os.path.join(ROOT, "profiles", name)
     try:
         with open(path) as f:
@@ -270,7 +273,7 @@ def spmv_roofline(solver, A, torch, F):
     else:
         kern = f"k_sell_cfg<__half,float,EpiStore<float>,24,2,16,int> (SELL-32 sigma={info.sigma}, fp16 A, fp32 x, fp32 y)"
     return {"kernel": kern, "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "peak_source": src,
-            "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None if csr else profiled_traffic(aligned),
+            "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None if csr else profiled_traffic(aligned, h),
             "algorithmic_bytes": alg, "effective_rate": aligned, "stored_bytes": stored,
             "stored_achieved": round(stored / dt / 1e9, 1), "stored_frac": round(stored / dt / 1e9 / peak, 4),
             "launch_us": round(dt * 1e6, 2)}
@@ -765,18 +768,20 @@ def c2_block_line(args, A):
     S.solve(B_d[0], Xs[0])
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
 
-    def timed(fn):
+    def timed(fn, tag):
         torch.cuda.synchronize()
+        torch.cuda.nvtx.range_push(tag)
         e0.record(stream)
         out = fn()
         e1.record(stream)
+        torch.cuda.nvtx.range_pop()
         torch.cuda.synchronize()
         return e0.elapsed_time(e1), out
 
     Xb.zero_()
-    tb, rb = timed(lambda: S.solve_multi(B_d, Xb))
+    tb, rb = timed(lambda: S.solve_multi(B_d, Xb), "block")
     Xs.zero_()
-    ts, rs = timed(lambda: [S.solve(B_d[k], Xs[k]) for k in range(K)])
+    ts, rs = timed(lambda: [S.solve(B_d[k], Xs[k]) for k in range(K)], "singles")
     line = {"workload": f"C2 192^3 27-point stencil, {K} right-hand sides b_k = A x*_k, x*_k ~ U(-1, 1)",
             "rhs": K, "sell": "32-row offset-aligned slices, sigma 1",
             "timing": "device time, CUDA events on the solver's stream",
@@ -859,6 +864,8 @@ def c5_line(args):
     n_train, n_pairs = ts.A.shape[0], ts.r.shape[0]
     del ts
     rows, held = [], []
+    fallbacks = {"single": 0, "plain": 0, "learned": 0}
+    inference_us = {}
     for s in range(10000, 10000 + args.c5_eval):
         A = F.diffusion7(nx, nx, nx, 1.5, 6.0, s).scale()
         n = A.shape[0]
@@ -873,6 +880,9 @@ def c5_line(args):
         b_d = torch.from_numpy(b).cuda()
         x_d = torch.zeros_like(b_d)
         rec = {"seed": s, "correct_call_ms": round(t_inf * 1e3, 1)}
+        if not held:  # the network alone on the first field's features, both tensor-core engines
+            inference_us = {e: round(L.time_inference(A, nx, nx, Z, Wt, engine=e, reps=20), 2)
+                            for e in ("tcgen05", "mma.sync")}
         for name, S in (("plain", Sp), ("learned", Sl)):
             for _ in range(max(args.warmup, 1)):
                 x_d.zero_()
@@ -884,6 +894,11 @@ def c5_line(args):
                 best = r if best is None or r.solve_seconds < best.solve_seconds else best
             rec[name] = {"ms": round(best.solve_seconds * 1e3, 2), "outer_iters": best.res_iter,
                          "expl_rel_res": best.expl_rel_res, "solved": bool(best.is_solved)}
+        if not (rec["learned"]["solved"] and rec["learned"]["expl_rel_res"] < 1e-10):
+            # the learned solve fell short: plain SDAINV solves the field again, and its time counts
+            fallbacks["single"] += 1
+            rec["learned"]["fell_back"] = True
+            rec["learned"]["ms"] = round(rec["learned"]["ms"] + rec["plain"]["ms"], 2)
         # residual after a fixed number of outer steps (one fewer than plain needs): the
         # convergence gain that the whole-iteration count can hide
         k = max(1, rec["plain"]["outer_iters"] - 1)
@@ -918,8 +933,20 @@ def c5_line(args):
                 dt = time.perf_counter() - t0
                 if it >= max(args.warmup, 1) and (best is None or dt < best[0]):
                     best = (dt, res)
-            solved = solved and all(r.is_solved and r.expl_rel_res < 1e-10 for r in best[1])
-            bat[name].append({"systems": len(grp), "wall_ms": round(best[0] * 1e3, 2),
+            # a system the batch leaves unsolved is solved again alone with plain SDAINV, and that
+            # solve's time is added to the batch's
+            fb_s = 0.0
+            for (A, b, pf, _), r in zip(grp, best[1]):
+                if r.is_solved and r.expl_rel_res < 1e-10:
+                    continue
+                fallbacks[name] += 1
+                Sf = F.Solver(ctx, A, factors=pf, **PARAMS)
+                xf = torch.zeros(A.shape[0], dtype=torch.float64, device="cuda")
+                rf = Sf.solve(torch.from_numpy(b).cuda(), xf)
+                fb_s += rf.solve_seconds
+                solved = solved and rf.is_solved
+                Sf.close()
+            bat[name].append({"systems": len(grp), "wall_ms": round((best[0] + fb_s) * 1e3, 2),
                               "outer_iters": [r.res_iter for r in best[1]]})
             B.close()
     mean = lambda key: float(np.mean([r[key]["ms"] for r in rows]))
@@ -951,6 +978,9 @@ def c5_line(args):
             "residual_gain_at_fixed_outer_steps": {"min": round(min(gains), 2), "max": round(max(gains), 2),
                                                    "geomean": round(float(np.exp(np.mean(np.log(gains)))), 2)},
             "batched": bat, "all_solved": solved and all(r[k]["solved"] for r in rows for k in ("plain", "learned")),
+            "fallbacks_to_plain": {"learned_single": fallbacks["single"], "plain_batched": fallbacks["plain"],
+                                   "learned_batched": fallbacks["learned"]},
+            "inference_us_first_field": inference_us,
             "training": {"pairs": n_pairs, "steps": args.c5_steps, "train_s": round(t_train, 2),
                          "data_s": round(t_data, 1), "loss_first": float(losses[0]), "loss_final": final_loss},
             "systems": rows}

@@ -40,13 +40,39 @@ template <typename T, int N> __device__ __forceinline__ VecN<T, N> ldg_vec(const
   }
 }
 
+// 32 contiguous bytes (32-byte aligned) in one 256-bit access (sm_100's
+// ld / st .v8.b32): a lane's access then fills a whole 32-byte sector, where
+// two 16-byte accesses per lane fill half of each sector they touch
+__device__ __forceinline__ void ld32_nc(const void *p, uint32_t (&u)[8]) {
+  asm volatile("ld.global.nc.v8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+               : "=r"(u[0]), "=r"(u[1]), "=r"(u[2]), "=r"(u[3]), "=r"(u[4]), "=r"(u[5]), "=r"(u[6]), "=r"(u[7])
+               : "l"(p));
+}
+__device__ __forceinline__ void ld32(const void *p, uint32_t (&u)[8]) {
+  asm volatile("ld.global.v8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+               : "=r"(u[0]), "=r"(u[1]), "=r"(u[2]), "=r"(u[3]), "=r"(u[4]), "=r"(u[5]), "=r"(u[6]), "=r"(u[7])
+               : "l"(p)
+               : "memory");
+}
+__device__ __forceinline__ void st32(void *p, const uint32_t (&u)[8]) {
+  asm volatile("st.global.v8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"l"(p), "r"(u[0]), "r"(u[1]), "r"(u[2]),
+               "r"(u[3]), "r"(u[4]), "r"(u[5]), "r"(u[6]), "r"(u[7])
+               : "memory");
+}
+
 // ---------------------------------------------------------------------------
-// K contiguous values of one row, 16-byte accesses where K allows
+// K contiguous values of one row in global memory: 32-byte accesses where
+// the row is a multiple of 32 bytes (rows of a block vector start on 32-byte
+// boundaries: every vector this library allocates is 64-byte aligned), else
+// 16-byte ones where K allows.  load_any takes any address space (the stage
+// buffers in shared memory).
 // ---------------------------------------------------------------------------
 template <typename T, int K> struct RowK {
   static constexpr int BYTES = (int)sizeof(T) * K;
-  static constexpr int VEC = BYTES >= 16 ? 16 / (int)sizeof(T) : K;  // elements per access
-  template <typename Acc> static __device__ __forceinline__ void load(const T *p, Acc (&o)[K]) {
+  static constexpr bool WIDE = BYTES % 32 == 0;                 // 32-byte accesses
+  static constexpr int W = 32 / (int)sizeof(T);                 // elements per 32-byte access
+  static constexpr int VEC = BYTES >= 16 ? 16 / (int)sizeof(T) : K;  // elements per access otherwise
+  template <typename Acc> static __device__ __forceinline__ void load_any(const T *p, Acc (&o)[K]) {
 #pragma unroll
     for (int q = 0; q < K / VEC; q++) {
       const VecN<T, VEC> a = *reinterpret_cast<const VecN<T, VEC> *>(p + q * VEC);
@@ -54,21 +80,62 @@ template <typename T, int K> struct RowK {
       for (int e = 0; e < VEC; e++) o[q * VEC + e] = to_acc<Acc>(a.v[e]);
     }
   }
+  template <typename Acc> static __device__ __forceinline__ void load(const T *p, Acc (&o)[K]) {
+    if constexpr (WIDE) {
+#pragma unroll
+      for (int q = 0; q < K / W; q++) {
+        uint32_t u[8];
+        ld32(p + q * W, u);
+        const T *t = reinterpret_cast<const T *>(u);
+#pragma unroll
+        for (int e = 0; e < W; e++) o[q * W + e] = to_acc<Acc>(t[e]);
+      }
+    } else {
+#pragma unroll
+      for (int q = 0; q < K / VEC; q++) {
+        const VecN<T, VEC> a = *reinterpret_cast<const VecN<T, VEC> *>(p + q * VEC);
+#pragma unroll
+        for (int e = 0; e < VEC; e++) o[q * VEC + e] = to_acc<Acc>(a.v[e]);
+      }
+    }
+  }
   template <typename Acc> static __device__ __forceinline__ void ldg(const T *p, Acc (&o)[K]) {
+    if constexpr (WIDE) {
 #pragma unroll
-    for (int q = 0; q < K / VEC; q++) {
-      const VecN<T, VEC> a = ldg_vec(reinterpret_cast<const VecN<T, VEC> *>(p + q * VEC));
+      for (int q = 0; q < K / W; q++) {
+        uint32_t u[8];
+        ld32_nc(p + q * W, u);
+        const T *t = reinterpret_cast<const T *>(u);
 #pragma unroll
-      for (int e = 0; e < VEC; e++) o[q * VEC + e] = to_acc<Acc>(a.v[e]);
+        for (int e = 0; e < W; e++) o[q * W + e] = to_acc<Acc>(t[e]);
+      }
+    } else {
+#pragma unroll
+      for (int q = 0; q < K / VEC; q++) {
+        const VecN<T, VEC> a = ldg_vec(reinterpret_cast<const VecN<T, VEC> *>(p + q * VEC));
+#pragma unroll
+        for (int e = 0; e < VEC; e++) o[q * VEC + e] = to_acc<Acc>(a.v[e]);
+      }
     }
   }
   template <typename Acc> static __device__ __forceinline__ void store(T *p, const Acc (&v)[K]) {
+    if constexpr (WIDE) {
 #pragma unroll
-    for (int q = 0; q < K / VEC; q++) {
-      VecN<T, VEC> a;
+      for (int q = 0; q < K / W; q++) {
+        uint32_t u[8];
+        T *t = reinterpret_cast<T *>(u);
 #pragma unroll
-      for (int e = 0; e < VEC; e++) a.v[e] = cvt<T>(v[q * VEC + e]);
-      *reinterpret_cast<VecN<T, VEC> *>(p + q * VEC) = a;
+        for (int e = 0; e < W; e++) t[e] = cvt<T>(v[q * W + e]);
+        st32(p + q * W, u);
+      }
+    } else {
+#pragma unroll
+      for (int q = 0; q < K / VEC; q++) {
+        VecN<T, VEC> a;
+#pragma unroll
+        for (int e = 0; e < VEC; e++) a.v[e] = cvt<T>(v[q * VEC + e]);
+        *reinterpret_cast<VecN<T, VEC> *>(p + q * VEC) = a;
+      }
     }
   }
 };
@@ -241,7 +308,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1)
               cc[e] = clampc ? min(max(b, 0), A.ncols - 1) : b;
             }
           } else {
-            RowK<V, VK>::load(sv + ((size_t)k * 32 + lane) * VK, vv[e]);
+            RowK<V, VK>::load_any(sv + ((size_t)k * 32 + lane) * VK, vv[e]);  // shared memory
             cc[e] = sc[k * 32 + lane];
           }
         }
@@ -572,11 +639,24 @@ __global__ void __launch_bounds__(WARPS * 32) k_multidot_f32K(const float *__res
   if (threadIdx.x == 0) *gr.ticket = 0;
 }
 
+// shared memory of k_cgs_updateK's staging tiles: per warp 32 threads x N
+// rows x K values, each thread's run padded by 16 bytes (conflict-free
+// 16-byte reads)
+template <typename T, int WARPS, int K> constexpr size_t cgs_stage_bytes() {
+  return K == 1 ? 0 : (size_t)WARPS * 32 * (16 / sizeof(T) * K + 16 / sizeof(T)) * sizeof(T);
+}
+
 // w(:, c) -= sum_k H(j, k)(c) V(k)(:, c) (MULMV order), then ||w(:, c)||^2 ->
 // Givens of column c for the columns in *active (k_cgs_update): N elements
 // per thread (16 bytes of one column), block-strided final stage.
+// For K > 1 a thread's N rows (the single-column kernel's, so that every
+// column's partial sums are its single solve's) are N * K = 16 K contiguous
+// bytes; the warp moves its 32 threads' runs, one contiguous tile, between
+// global and shared memory with coalesced 16-byte accesses, and each thread
+// reads its own run from shared memory (launched with cgs_stage_bytes of
+// dynamic shared memory).
 template <typename T, int WARPS, int K>
-__global__ void __launch_bounds__(WARPS * 32) k_cgs_updateK(T *__restrict__ w, Cols<T> V, int nv, int64_t n,
+__global__ void __launch_bounds__(WARPS * 32, K > 1 ? 1 : 8) k_cgs_updateK(T *__restrict__ w, Cols<T> V, int nv, int64_t n,
                                                             GridRed gr, LevelK<T> L, int j, int compute_y,
                                                             double *abs_e, const uint32_t *active, int *err) {
   constexpr int N = 16 / sizeof(T);
@@ -592,9 +672,62 @@ __global__ void __launch_bounds__(WARPS * 32) k_cgs_updateK(T *__restrict__ w, C
   for (int c = 0; c < K; c++) part[c] = 0;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x, tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t nq = n / N;
+  if constexpr (K > 1) {
+    constexpr int S = N * K, P = S + N, TILE = 32 * S;  // values a thread, its padded pitch, a warp tile
+    extern __shared__ __align__(16) unsigned char cgs_stage[];
+    const int lane = threadIdx.x & 31;
+    T *tile = reinterpret_cast<T *>(cgs_stage) + (size_t)(threadIdx.x >> 5) * 32 * P;
+    T *mine = tile + lane * P;
+    for (int64_t q0 = tid - lane; q0 < nq; q0 += stride) {
+      const int64_t base = q0 * S;
+      const int lim = (int)((nq - q0 < 32 ? nq - q0 : 32) * S);  // values of the tile inside the vector
+      auto stage_in = [&](const T *src) {
+        __syncwarp();
+#pragma unroll 4
+        for (int i = lane * N; i < TILE; i += 32 * N)
+          if (i < lim) *reinterpret_cast<uint4 *>(tile + (i / S) * P + i % S) = *reinterpret_cast<const uint4 *>(src + base + i);
+        __syncwarp();
+      };
+      using Vec = VecN<T, N>;  // 16 bytes of the run
+      T r[S];
+      stage_in(V.p[0]);
+#pragma unroll
+      for (int e0 = 0; e0 < S; e0 += N) {
+        const Vec a = *reinterpret_cast<const Vec *>(mine + e0);
+#pragma unroll
+        for (int e = 0; e < N; e++) r[e0 + e] = mul_rn(a.v[e], sh[(e0 + e) % K][0]);
+      }
+      for (int k = 1; k < nv; k++) {
+        stage_in(V.p[k]);
+#pragma unroll
+        for (int e0 = 0; e0 < S; e0 += N) {
+          const Vec a = *reinterpret_cast<const Vec *>(mine + e0);
+#pragma unroll
+          for (int e = 0; e < N; e++) r[e0 + e] = fmaT(a.v[e], sh[(e0 + e) % K][k], r[e0 + e]);
+        }
+      }
+      stage_in(w);
+      const bool own = q0 + lane < nq;
+      // row by row, as the single-column kernel: update, then the squared norm
+#pragma unroll
+      for (int e0 = 0; e0 < S; e0 += N) {
+        Vec a = *reinterpret_cast<const Vec *>(mine + e0);
+#pragma unroll
+        for (int e = 0; e < N; e++) {
+          a.v[e] = sub_rn(a.v[e], r[e0 + e]);
+          if (own) part[(e0 + e) % K] = fmaT(a.v[e], a.v[e], part[(e0 + e) % K]);
+        }
+        *reinterpret_cast<Vec *>(mine + e0) = a;
+      }
+      __syncwarp();
+#pragma unroll 4
+      for (int i = lane * N; i < TILE; i += 32 * N)
+        if (i < lim) *reinterpret_cast<uint4 *>(w + base + i) = *reinterpret_cast<const uint4 *>(tile + (i / S) * P + i % S);
+    }
+  }
   // the N rows of a thread, RG at a time as one contiguous run of RG * K values
   constexpr int RG = (N * K <= 16) ? N : 1, E = RG * K;
-  for (int64_t q = tid; q < nq; q += stride) {
+  for (int64_t q = tid; K == 1 && q < nq; q += stride) {
 #pragma unroll
     for (int g = 0; g < N / RG; g++) {
       const int64_t i0 = q * N + g * RG;

@@ -485,7 +485,8 @@ constexpr size_t kTcSmem = kTcOffBar + kTcGroups * 8 + 16;
 constexpr int kTcCtasPerSm = 4;
 static_assert(kTcCtasPerSm * kTcGroups * kTcCols == 512, "TMEM columns of an SM");
 static_assert((kTcCtasPerSm + 1) * (kTcSmem + 1024) > 228 * 1024, "a fifth CTA would fit on an SM");
-static_assert(kTcOffA % 128 == 0 && kTcA1 % 128 == 0 && kTcOffBar % 8 == 0, "operand alignment");
+static_assert(kTcOffA % 128 == 0 && kTcA1 % 128 == 0 && kTcOffBias % 16 == 0 && kTcOffBar % 8 == 0,
+              "operand alignment");
 
 // byte offset of element (r, k) of a K-major no-swizzle operand with K columns
 __host__ __device__ constexpr uint32_t kmaj_off(int r, int k, int K) {
@@ -547,9 +548,18 @@ __device__ __forceinline__ bool group_sync_and(int id, bool ok) {
 // relu(acc + bias) of 16 columns of a row, stored as bf16 at A2 columns c0..c0+15
 __device__ __forceinline__ void tc_epilogue16(unsigned char *a2, int row, int c0, const float (&v)[16],
                                               const float *bias) {
+  float b[16];  // the 16 biases as four broadcast 16-byte loads
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    const float4 q = reinterpret_cast<const float4 *>(bias + c0)[i];
+    b[4 * i] = q.x;
+    b[4 * i + 1] = q.y;
+    b[4 * i + 2] = q.z;
+    b[4 * i + 3] = q.w;
+  }
   uint32_t p[8];
 #pragma unroll
-  for (int i = 0; i < 8; i++) p[i] = pack_bf16(relu(v[2 * i] + bias[c0 + 2 * i]), relu(v[2 * i + 1] + bias[c0 + 2 * i + 1]));
+  for (int i = 0; i < 8; i++) p[i] = pack_bf16(relu(v[2 * i] + b[2 * i]), relu(v[2 * i + 1] + b[2 * i + 1]));
   *reinterpret_cast<uint4 *>(a2 + kmaj_off(row, c0, kH)) = make_uint4(p[0], p[1], p[2], p[3]);
   *reinterpret_cast<uint4 *>(a2 + kmaj_off(row, c0 + 8, kH)) = make_uint4(p[4], p[5], p[6], p[7]);
 }
@@ -667,9 +677,10 @@ __global__ void __launch_bounds__(kTcRows * kTcGroups, kTcCtasPerSm)
     tmem_ld16(lane_addr, y);
     const int64_t r = tile * kTcRows + tid;
     if (r < n) {
+      const float4 c0 = reinterpret_cast<const float4 *>(b3s)[0], c1 = reinterpret_cast<const float4 *>(b3s)[1];
       float4 *dst = reinterpret_cast<float4 *>(o + r * kOut);
-      dst[0] = make_float4(y[0] + b3s[0], y[1] + b3s[1], y[2] + b3s[2], y[3] + b3s[3]);
-      dst[1] = make_float4(y[4] + b3s[4], y[5] + b3s[5], y[6] + b3s[6], y[7] + b3s[7]);
+      dst[0] = make_float4(y[0] + c0.x, y[1] + c0.y, y[2] + c0.z, y[3] + c0.w);
+      dst[1] = make_float4(y[4] + c1.x, y[5] + c1.y, y[6] + c1.z, y[7] + c1.w);
     }
   }
   if (!ok) {

@@ -708,6 +708,11 @@ template <int K> struct Engine {
       F3R_TRY((launch_block<__half, __half, EpiRichResPreK<K>, K>(C(), h, Av, h, {}, true)));
       F3R_TRY((launch_block<__half, __half, EpiResidualK<__half, __half, K>, K>(C(), h, Av, h, {}, true)));
       F3R_TRY((launch_block<__half, __half, EpiZScaleK<K>, K>(C(), h, Av, h, {}, true)));
+      // the Gram-Schmidt update's staging tiles (above 48 KB from K = 16)
+      CUDA_TRY(cudaFuncSetAttribute(k_cgs_updateK<float, 8, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)cgs_stage_bytes<float, 8, K>()));
+      CUDA_TRY(cudaFuncSetAttribute(k_cgs_updateK<double, 8, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)cgs_stage_bytes<double, 8, K>()));
       if (S.mm) {
         F3R_TRY((launch_block_mm<double, double, EpiStoreK<double, K>, K>(C(), d, Av, d, {}, true)));
         F3R_TRY((launch_block_mm<double, double, EpiResidualK<double, double, K>, K>(C(), d, Av, d, {}, true)));
@@ -936,8 +941,9 @@ template <int K> struct Engine {
 
   // the Gram-Schmidt update, norm and Givens of step j of an inner level
   void cgs(float *wv, const Cols<float> &Vc, int nv, Level<float> &L, int j, bool last) {
-    launch_k(C(), k_cgs_updateK<float, 8, K>, C().ew_grid(cdiv(n, 4)), 256, 0, C().stream, wv, Vc, nv, (int64_t)n,
-             w.gr, L.view(), j, last ? 1 : 0, (double *)nullptr, (const uint32_t *)w.active, C().err);
+    launch_k(C(), k_cgs_updateK<float, 8, K>, C().ew_grid(cdiv(n, 4)), 256, cgs_stage_bytes<float, 8, K>(),
+             C().stream, wv, Vc, nv, (int64_t)n, w.gr, L.view(), j, last ? 1 : 0, (double *)nullptr,
+             (const uint32_t *)w.active, C().err);
   }
 
   // sFGMRES's second and third loops (gmres2.hpp:181-193), K = 1: classical
@@ -1229,8 +1235,8 @@ template <int K> struct Engine {
         F3R_TRY(mv_store(S.A.v64, S.A.view(), (const double *)zj, wv));
         launch_k(C(), k_multidot_chunkedK<double, 8, K>, g, 256, 0, st, (const double *)wv, V, j + 1, N, w.gr,
                  L.H + (size_t)j * (L.m + 1), (int64_t)(L.m + 1) * L.m);
-        launch_k(C(), k_cgs_updateK<double, 8, K>, C().ew_grid(cdiv(N, 2)), 256, 0, st, wv, V, j + 1, N, w.gr, Lv, j,
-                 0, w.abs_e, (const uint32_t *)w.active, C().err);
+        launch_k(C(), k_cgs_updateK<double, 8, K>, C().ew_grid(cdiv(N, 2)), 256, cgs_stage_bytes<double, 8, K>(), st,
+                 wv, V, j + 1, N, w.gr, Lv, j, 0, w.abs_e, (const uint32_t *)w.active, C().err);
         CUDA_TRY(cudaGetLastError());
         F3R_TRY(read_k(w.abs_e, ev));
         uint32_t done = 0;

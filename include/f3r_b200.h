@@ -377,10 +377,16 @@ f3r_status f3r_solver_solve(f3r_solver *s, const double *b, double *x, f3r_cond_
 f3r_status f3r_solver_info(const f3r_solver *s, f3r_sell_info *a_info, int32_t *precond_diagonal);
 /* Several right-hand sides: column k of B (b + k * ldb) is solved into
  * column k of X (x + k * ldx), x holding the initial guesses; ldb, ldx >= n;
- * host or device pointers.  Each column is its own F3R solve on this
- * solver's device objects (matrix, preconditioner, captured graphs), in
- * column order; results (may be NULL) gets one entry per column.  The
- * nrhs argument of the planned boundary's solve call. */
+ * host or device pointers; results (may be NULL) gets one entry per column.
+ * With SDAINV and 32-row SELL slices (packed or offset-aligned) the columns
+ * run in lockstep blocks of up to 16: every product streams the matrix once
+ * for the block, each column keeps its own Hessenberg matrix, rotations and
+ * Richardson weights, and its result is its single solve's bit for bit.  cond
+ * is then called once per outer step for each column still running, in
+ * column order; a column stops when its cond (or rel_tol) says so, and the
+ * block restarts until every column has stopped.  Other configurations solve
+ * the columns one after another on this solver's device objects.  The nrhs
+ * argument of the planned boundary's solve call. */
 f3r_status f3r_solver_solve_multi(f3r_solver *s, int32_t nrhs, const double *b, int64_t ldb, double *x, int64_t ldx,
                                   f3r_cond_fn cond, void *user, f3r_result *results);
 /* Independent systems at once: system i is f3r_solver_solve_multi(solvers[i],

@@ -133,17 +133,25 @@ def test_solver_from_given_factors_is_the_plain_solver(ctx):
     assert np.array_equal(x1, x2)
 
 
-def test_training_gains_on_held_out_systems(ctx):
-    """Trained on the solver's residual / error pairs of 16 seeded 12^3
-    fields, the correction lowers the training loss; on held-out 32^3 fields
-    the learned solve reaches 1e-10 without the plain fallback, and its
-    residual after a fixed number of outer steps is compared with plain
-    SDAINV's."""
+@pytest.fixture(scope="module")
+def trained(ctx):
+    """the network trained on the solver's residual / error pairs of 16
+    seeded 12^3 fields (300 Adam steps), with its loss history"""
     ts = training_set(ctx, seeds=range(16), nt=12, rel_tol=1e-10)
     assert ts.r.shape == (7, 16 * 12 ** 3)
     L = Learned(ctx, seed=0)
     L.set_data(**ts.data())
     losses = L.train(300, lr=2e-3)
+    return L, losses
+
+
+def test_training_gains_on_held_out_systems(ctx, trained):
+    """Trained on the solver's residual / error pairs of 16 seeded 12^3
+    fields, the correction lowers the training loss; on held-out 32^3 fields
+    the learned solve reaches 1e-10 without the plain fallback, and its
+    residual after a fixed number of outer steps is compared with plain
+    SDAINV's."""
+    L, losses = trained
     assert np.all(np.isfinite(losses))
     final = L.evaluate()
     assert final < losses[0], (losses[0], final)
@@ -164,6 +172,51 @@ def test_training_gains_on_held_out_systems(ctx):
         ratios.append(rp / rl)
     print("residual gain at fixed outer steps", ratios)
     assert np.exp(np.mean(np.log(ratios))) > 1.0, ratios
+
+
+def test_learned_batched_time_to_solution(ctx, trained):
+    """Time to 1e-10 over 8 held-out 32^3 fields: the learned factors solved
+    as one same-pattern batch (f3r_batch) against plain SDAINV solved one
+    field after another, each solver built beforehand; host wall clock with
+    the device synchronised on both sides, best of 3.  Every field reaches
+    1e-10 in both, and the learned batch takes at most 1/1.5 of the time."""
+    import time
+    import torch
+    L, _ = trained
+    seeds = range(2001, 2009)
+    fields = [F.diffusion7(32, 32, 32, 1.5, 6.0, s).scale() for s in seeds]
+    plain = [A.sdainv() for A in fields]
+    learned = [L.correct(A, 32, 32, Z, Wt) for A, (Z, Wt) in zip(fields, plain)]
+    bs = [A.spmv(F.random_uniform(s, -1, 1, A.shape[0])) for A, s in zip(fields, seeds)]
+    kw = dict(rel_tol=1e-10, m2=8, m3=4, m4=2, c=64)
+    solvers = [F.Solver(ctx, A, factors=f, **kw) for A, f in zip(fields, plain)]
+    batch = F.Batch(ctx, fields, factors=learned, **kw)
+
+    def run_plain():
+        xs = [np.zeros(len(b)) for b in bs]
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        res = [S.solve(b, x) for S, b, x in zip(solvers, bs, xs)]
+        torch.cuda.synchronize()
+        return time.perf_counter() - t0, res
+
+    def run_batch():
+        xs = [np.zeros(len(b)) for b in bs]
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        res = batch.solve(bs, xs)
+        torch.cuda.synchronize()
+        return time.perf_counter() - t0, res
+
+    run_plain(), run_batch()  # warm-up: work buffers and graphs
+    tp, rp = min((run_plain() for _ in range(3)), key=lambda t: t[0])
+    tb, rb = min((run_batch() for _ in range(3)), key=lambda t: t[0])
+    assert all(r.is_solved and r.expl_rel_res < 1e-9 for r in rp + rb)
+    print(f"plain one after another {tp * 1e3:.2f} ms, learned batch {tb * 1e3:.2f} ms: {tp / tb:.2f}x")
+    assert tb * 1.5 <= tp, (tp, tb)
+    batch.close()
+    for S in solvers:
+        S.close()
 
 
 def test_fallback_to_plain_sdainv(ctx):
