@@ -747,9 +747,8 @@ C5_BATCH = 8  # held-out systems kept for the batched comparison (two solvers ea
 def c2_block_line(args, A):
     """K right-hand sides of the headline 192^3 system solved as one
     lockstep block (f3r_solver_solve_multi) against the same K solved one at a
-    time on the same solver; device time (CUDA events) of each, and whether
-    every block column is bit for bit its single solve.  The block kernels
-    take 32-row slices, so this solver uses the 32-row offset-aligned layout."""
+    time on the same solver, in the bench's layout; device time (CUDA events)
+    of each, and whether every block column is bit for bit its single solve."""
     import torch
     import f3r_b200 as F
     K = args.block_k
@@ -758,7 +757,7 @@ def c2_block_line(args, A):
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     ctx.set_stream(stream.cuda_stream)
-    kw = {**PARAMS, **LAYOUTS["aligned"], "sell_autotune": 0}
+    kw = {**PARAMS, "sell_autotune": 0}
     S = F.Solver(ctx, A, **kw)
     n = A.shape[0]
     B = np.stack([A.spmv(F.random_uniform(100 + k, -1.0, 1.0, n)) for k in range(K)])
@@ -783,7 +782,7 @@ def c2_block_line(args, A):
     Xs.zero_()
     ts, rs = timed(lambda: [S.solve(B_d[k], Xs[k]) for k in range(K)], "singles")
     line = {"workload": f"C2 192^3 27-point stencil, {K} right-hand sides b_k = A x*_k, x*_k ~ U(-1, 1)",
-            "rhs": K, "sell": "32-row offset-aligned slices, sigma 1",
+            "rhs": K, "sell": layout_desc(kw),
             "timing": "device time, CUDA events on the solver's stream",
             "block_ms": round(tb, 2), "singles_ms": round(ts, 2),
             "block_ms_per_rhs": round(tb / K, 2), "single_ms_per_rhs": round(ts / K, 2),

@@ -344,6 +344,165 @@ __global__ void __launch_bounds__(WARPS * 32, 1)
   }
 }
 
+// ---------------------------------------------------------------------------
+// Block product on 64-row offset-aligned slices (sell_c = 64): each lane owns
+// rows l and l + 32 of a slice and K accumulators for each, summing every
+// row's entries in slot (column) order with one FMA per column, as the
+// 32-row kernels do, so the sums are theirs bit for bit.  A chunk of up to 32
+// slots holds 64 rows of values, row after row, and one base per slot; the
+// two rows of a lane gather x at base + lane and base + lane + 32.
+// ---------------------------------------------------------------------------
+template <typename V, int K> constexpr int block64_warps() {
+  // a stage holds 64 x 32 values and 32 bases; two stages a warp within ~200 KB
+  return sizeof(V) == 2 ? 16 : sizeof(V) == 4 ? 12 : 6;
+}
+template <typename V, int K> constexpr size_t block64_smem_bytes() {
+  return (size_t)block64_warps<V, K>() * 2 * ((size_t)kAllAlignedChunk * 64 * sizeof(V) + kAllAlignedChunk * 4) +
+         (size_t)block64_warps<V, K>() * 2 * sizeof(uint64_t);
+}
+
+template <typename V, typename X, typename Epi, int K, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32, 1)
+    k_sell_block64(const V *__restrict__ val, DevSell A, const X *__restrict__ x, Epi epi, int *err) {
+  using Acc = typename acc_of<V>::type;
+  constexpr int STAGES = 2, KC = kAllAlignedChunk;
+  constexpr uint32_t VB = KC * 64 * sizeof(V), BB = KC * 4, SB = VB + BB;
+  // slots gathered per sub-block: about 32 gathered fp32 values (16 fp64) per lane over its two rows
+  constexpr int SUB0 = (sizeof(Acc) == 8 ? 16 : 32) / (2 * K);
+  constexpr int SUB = SUB0 > 0 ? SUB0 : 1;
+  extern __shared__ __align__(128) unsigned char smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  unsigned char *buf = smem + (size_t)warp * STAGES * SB;
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem + (size_t)WARPS * STAGES * SB) + warp * STAGES;
+  if (lane == 0) {
+#pragma unroll
+    for (int s = 0; s < STAGES; s++) mbar_init(&bars[s], 1);
+    fence_mbar_init();
+  }
+  __syncwarp();
+  const uint64_t pol = l2_evict_first_policy();
+  const int TW = gridDim.x * WARPS;
+  int fs = blockIdx.x * WARPS + warp, fk = 0, fst = 0, inflight = 0;
+  int fs0 = 0, fw = 0, fcb = 0;
+  auto fetch = [&]() {
+    while (inflight < STAGES && fs < A.nslices) {
+      if (fk == 0) {
+        fs0 = A.sptr[fs];
+        fw = A.sptr[fs + 1] - fs0;
+        fcb = A.cbptr[fs] & ~3;
+      }
+      if (fw == 0) {
+        fs += TW;
+        fk = 0;
+        continue;
+      }
+      const int kc = min(KC, fw - fk);
+      if (lane == 0) {
+        const size_t off = ((size_t)fs0 + fk) * 64;
+        fence_proxy_async_smem();
+        const uint32_t vb = (uint32_t)kc * 64u * (uint32_t)sizeof(V), bb = (uint32_t)((kc + 3) & ~3) * 4u;
+        mbar_arrive_expect_tx(&bars[fst], vb + bb);
+        bulk_g2s(buf + (size_t)fst * SB, val + off, vb, &bars[fst], pol);
+        bulk_g2s(buf + (size_t)fst * SB + VB, A.cbase + fcb + fk, bb, &bars[fst], pol);
+      }
+      fst = (fst + 1 == STAGES) ? 0 : fst + 1;
+      inflight++;
+      fk += kc;
+      if (fk >= fw) {
+        fk = 0;
+        fs += TW;
+      }
+    }
+  };
+  auto release = [&]() {
+    __syncwarp();
+    inflight--;
+    fetch();
+  };
+  fetch();
+
+  int cs = blockIdx.x * WARPS + warp, ck = 0, cst = 0;
+  uint32_t phase = 0;
+  bool ok = true;
+  Acc acc0[K], acc1[K];
+#pragma unroll
+  for (int c = 0; c < K; c++) acc0[c] = acc1[c] = 0;
+  int w = 0;
+  bool clampc = false;
+  while (cs < A.nslices) {
+    if (ck == 0) {
+      w = A.sptr[cs + 1] - A.sptr[cs];
+      clampc = (A.cbptr[cs] & 1) != 0;
+    }
+    const int64_t r0 = (int64_t)cs * 64 + lane, r1 = r0 + 32;
+    if (w == 0) {
+      if (r0 < A.n) epi.row(r0, acc0);
+      if (r1 < A.n) epi.row(r1, acc1);
+      cs += TW;
+      continue;
+    }
+    const int kc = min(KC, w - ck);
+    if (!mbar_wait_bounded(&bars[cst], (phase >> cst) & 1u)) {
+      ok = false;
+      break;
+    }
+    phase ^= 1u << cst;
+    const V *sv = reinterpret_cast<const V *>(buf + (size_t)cst * SB);
+    const int32_t *sb = reinterpret_cast<const int32_t *>(buf + (size_t)cst * SB + VB);
+    cst = (cst + 1 == STAGES) ? 0 : cst + 1;
+    const V *lv0 = sv + lane * kc, *lv1 = sv + (lane + 32) * kc;  // the two rows' values
+    for (int k0 = 0; k0 < kc; k0 += SUB) {
+      Acc v0[SUB], v1[SUB];
+      int32_t c0[SUB], c1[SUB];
+#pragma unroll
+      for (int e = 0; e < SUB; e++) {
+        const int k = k0 + e;
+        if (k < kc) {
+          v0[e] = to_acc<Acc>(lv0[k]);
+          v1[e] = to_acc<Acc>(lv1[k]);
+          const int32_t b = sb[k] + lane;
+          c0[e] = clampc ? min(max(b, 0), A.ncols - 1) : b;
+          c1[e] = clampc ? min(max(b + 32, 0), A.ncols - 1) : b + 32;
+        }
+      }
+      if (k0 + SUB >= kc) release();  // last sub-block of the chunk: its shared data is in registers
+      Acc x0[SUB][K], x1[SUB][K];
+#pragma unroll
+      for (int e = 0; e < SUB; e++)
+        if (k0 + e < kc) {
+          RowK<X, K>::ldg(x + (size_t)c0[e] * K, x0[e]);
+          RowK<X, K>::ldg(x + (size_t)c1[e] * K, x1[e]);
+        }
+#pragma unroll
+      for (int e = 0; e < SUB; e++)
+        if (k0 + e < kc) {
+#pragma unroll
+          for (int c = 0; c < K; c++) {
+            acc0[c] = fmaT(v0[e], x0[e][c], acc0[c]);
+            acc1[c] = fmaT(v1[e], x1[e][c], acc1[c]);
+          }
+        }
+    }
+    ck += kc;
+    if (ck >= w) {
+      if (r0 < A.n) epi.row(r0, acc0);
+      if (r1 < A.n) epi.row(r1, acc1);
+#pragma unroll
+      for (int c = 0; c < K; c++) acc0[c] = acc1[c] = 0;
+      ck = 0;
+      cs += TW;
+    }
+  }
+  if (!ok) {
+    if (lane == 0) atomicExch(err, (int)DEV_TIMEOUT_SPMV);
+    for (int i = 0; i < inflight; i++) {
+      mbar_wait_bounded(&bars[cst], (phase >> cst) & 1u);
+      phase ^= 1u << cst;
+      cst = (cst + 1 == STAGES) ? 0 : cst + 1;
+    }
+  }
+}
+
 // ---- epilogues of the block product (one row, K columns) --------------------
 // y(:, c) = A x(:, c)
 template <typename Out, int K> struct EpiStoreK {

@@ -611,7 +611,7 @@ struct Solver {
   // no column indices; other set-ups (ILU, s-step levels, the fp16-vector
   // level, CSR or 16-bit indices) solve column by column.
   bool block_ok() const {
-    auto layout_ok = [](const DeviceSell &d) { return !d.rptr && !d.dcol && d.height == 32; };
+    auto layout_ok = [](const DeviceSell &d) { return !d.rptr && !d.dcol; };
     if (p.precond != F3R_PRECOND_SDAINV || p.inner_sstep || p.half_m > 0 || !layout_ok(A)) return false;
     return precond_diag || (layout_ok(W) && layout_ok(Z));
   }
@@ -640,9 +640,26 @@ Status launch_block_one(Context &c, const V *val, const DevSell &A, const X *x, 
   CUDA_TRY(cudaGetLastError());
   return F3R_SUCCESS;
 }
+// the K-column product on 64-row offset-aligned slices
+template <typename V, typename X, typename Epi, int K>
+Status launch_block64(Context &c, const V *val, const DevSell &A, const X *x, const Epi &epi, bool attr_only) {
+  constexpr int W = block64_warps<V, K>();
+  auto kern = k_sell_block64<V, X, Epi, K, W>;
+  static int done[64] = {0};
+  if (!done[c.device & 63]) {
+    CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)block64_smem_bytes<V, K>()));
+    done[c.device & 63] = 1;
+  }
+  if (attr_only || A.nslices == 0) return F3R_SUCCESS;
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(cdiv(A.nslices, W), c.sm_count));
+  launch_k(c, kern, grid, W * 32, block64_smem_bytes<V, K>(), c.stream, val, A, x, epi, c.err);
+  CUDA_TRY(cudaGetLastError());
+  return F3R_SUCCESS;
+}
 template <typename V, typename X, typename Epi, int K>
 Status launch_block(Context &c, const V *val, const DevSell &A, const X *x, const Epi &epi, bool attr_only = false) {
   if (A.rptr || A.dcol) return fail(F3R_ERROR_UNSUPPORTED, "block product: SELL with 32-bit indices or aligned slices");
+  if (A.height == 64) return launch_block64<V, X, Epi, K>(c, val, A, x, epi, attr_only);
   if (attr_only) {
     F3R_TRY((launch_block_one<V, X, Epi, K, int32_t>(c, val, A, x, epi, true)));
     F3R_TRY((launch_block_one<V, X, Epi, K, AlignedIdx>(c, val, A, x, epi, true)));
@@ -1445,8 +1462,18 @@ Status Solver::solve_multi(int32_t nrhs, const double *b, int64_t ldb, double *x
   cudaStream_t st = C().stream;
   const int g = C().ew_grid(N);
   Status status = F3R_SUCCESS;
-  for (int32_t k0 = 0; k0 < nrhs && status == F3R_SUCCESS; k0 += 16) {
-    const int nc = std::min<int32_t>(16, nrhs - k0);
+  // block width: up to 16 columns, 8 on systems of 2^20 rows or more (on the
+  // 192^3 system a 16-column block took 0.482 of 16 single solves' time, an
+  // 8-column block 0.451 of 8); a single column left over is solved alone
+  const int32_t kmax = N >= (1 << 20) ? 8 : 16;
+  for (int32_t k0 = 0, nc = 0; k0 < nrhs && status == F3R_SUCCESS; k0 += nc) {
+    nc = std::min<int32_t>(kmax, nrhs - k0);
+    if (nc == 1) {
+      f3r_result r{};
+      status = solve(b + (size_t)k0 * ldb, x + (size_t)k0 * ldx, cond, user, &r);
+      if (results) results[k0] = r;
+      continue;
+    }
     auto run = [&](auto kc) -> Status {
       constexpr int K = decltype(kc)::value;
       Work<K> *wk = nullptr;

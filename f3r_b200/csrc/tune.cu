@@ -107,6 +107,11 @@ void sweep64(Context &c, const DeviceSell &d, const V *val, const X *x, Y *y, in
   time_shape64<V, X, Y, 8, 2>(c, d, val, x, y, reps, out);
   time_shape64<V, X, Y, 6, 2>(c, d, val, x, y, reps, out);
   time_shape64<V, X, Y, 4, 3>(c, d, val, x, y, reps, out);
+  // one stage a warp: twice the warps in the same shared memory
+  time_shape64<V, X, Y, 32, 1>(c, d, val, x, y, reps, out);
+  time_shape64<V, X, Y, 24, 1>(c, d, val, x, y, reps, out);
+  time_shape64<V, X, Y, 16, 1>(c, d, val, x, y, reps, out);
+  time_shape64<V, X, Y, 12, 1>(c, d, val, x, y, reps, out);
 }
 
 // the aligned forms' value layouts are built for one chunk width each

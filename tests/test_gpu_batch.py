@@ -80,12 +80,14 @@ def _check_block(S, B, X0=None):
     return res
 
 
-@pytest.mark.parametrize("nrhs", [2, 5, 8, 16, 19])
-@pytest.mark.parametrize("layout", [dict(sell_align=1), dict(sell_align=0), dict(sell_sigma=256)])
+@pytest.mark.parametrize("nrhs", [2, 5, 8, 16, 17, 19])
+@pytest.mark.parametrize("layout", [dict(sell_align=1), dict(sell_align=0), dict(sell_sigma=256),
+                                    dict(sell_align=1, sell_c=64)])
 def test_block_solve_columns_bit_identical(nrhs, layout):
     """up to 16 right-hand sides per lockstep block (block SELL products over
     interleaved columns; padding columns inactive), 19 = 16 + 3 in two
-    blocks: every column is its single solve, bit for bit"""
+    blocks, 17 = 16 + one column solved alone: every column is its single
+    solve, bit for bit"""
     ctx = F.Context(0)
     A = F.stencil27(18, 17, 16, 2, 0.5).scale()
     S = F.Solver(ctx, A, rel_tol=1e-10, c=4, **layout)
@@ -94,15 +96,16 @@ def test_block_solve_columns_bit_identical(nrhs, layout):
     assert all(r.is_solved and r.expl_rel_res < 1e-10 for r in res)
 
 
-@pytest.mark.parametrize("align", [0, 1])
-def test_block_solve_general_sdainv_and_uneven_convergence(align):
+@pytest.mark.parametrize("layout", [dict(sell_align=0), dict(sell_align=1), dict(sell_align=1, sell_c=64)])
+def test_block_solve_general_sdainv_and_uneven_convergence(layout):
     """non-diagonal SDAINV factors (block products of W^T and Z; aligned: the
-    mixed offset-aligned form); columns that finish at different steps (an
-    exact initial guess stops at step 0, a smooth right-hand side converges
-    sooner than noise) leave the lockstep without disturbing the others"""
+    mixed offset-aligned form, or 64-row slices); columns that finish at
+    different steps (an exact initial guess stops at step 0, a smooth
+    right-hand side converges sooner than noise) leave the lockstep without
+    disturbing the others"""
     ctx = F.Context(0)
     A = F.diffusion7(16, 15, 14, 1.5, 3.0, 4).scale()
-    S = F.Solver(ctx, A, rel_tol=1e-10, c=4, sell_align=align)
+    S = F.Solver(ctx, A, rel_tol=1e-10, c=4, **layout)
     assert not S.info()[1]
     n = A.shape[0]
     rng = np.random.default_rng(9)
