@@ -266,7 +266,7 @@ def spmv_roofline(solver, A, torch, F):
     if csr:
         kern = "k_csr_cfg<__half,float,EpiStore<float>,24> (CSR, fp16 A, fp32 x, fp32 y)"
     elif h == 64:
-        kern = "k_sell64<__half,float,EpiStore<float>,24,2,32> (64-row offset-aligned slices, fp16 A, fp32 x, fp32 y)"
+        kern = "k_sell64<__half,float,EpiStore<float>,32,1,32> (64-row offset-aligned slices, fp16 A, fp32 x, fp32 y)"
     elif aligned:
         kern = ("k_sell_cfg<__half,float,EpiStore<float>,32,2,32,AllAlignedIdx> (SELL-32 sigma=1, offset-aligned, "
                 "fp16 A, fp32 x, fp32 y)")

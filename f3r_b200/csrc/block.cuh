@@ -352,20 +352,20 @@ __global__ void __launch_bounds__(WARPS * 32, 1)
 // slots holds 64 rows of values, row after row, and one base per slot; the
 // two rows of a lane gather x at base + lane and base + lane + 32.
 // ---------------------------------------------------------------------------
-template <typename V, int K> constexpr int block64_warps() {
-  // a stage holds 64 x 32 values and 32 bases; two stages a warp within ~200 KB
-  return sizeof(V) == 2 ? 16 : sizeof(V) == 4 ? 12 : 6;
-}
+// one stage a warp (released once its chunk is in registers), the warps the
+// registers allow: K accumulators for each of a lane's two rows
+template <typename V, int K> constexpr int block64_warps() { return sizeof(V) == 2 ? 16 : sizeof(V) == 4 ? 12 : 8; }
+template <typename V, int K> constexpr int block64_stages() { return 1; }
 template <typename V, int K> constexpr size_t block64_smem_bytes() {
-  return (size_t)block64_warps<V, K>() * 2 * ((size_t)kAllAlignedChunk * 64 * sizeof(V) + kAllAlignedChunk * 4) +
-         (size_t)block64_warps<V, K>() * 2 * sizeof(uint64_t);
+  constexpr size_t ws = (size_t)block64_warps<V, K>() * block64_stages<V, K>();
+  return ws * ((size_t)kAllAlignedChunk * 64 * sizeof(V) + kAllAlignedChunk * 4) + ws * sizeof(uint64_t);
 }
 
-template <typename V, typename X, typename Epi, int K, int WARPS>
+template <typename V, typename X, typename Epi, int K, int WARPS, int STAGES>
 __global__ void __launch_bounds__(WARPS * 32, 1)
     k_sell_block64(const V *__restrict__ val, DevSell A, const X *__restrict__ x, Epi epi, int *err) {
   using Acc = typename acc_of<V>::type;
-  constexpr int STAGES = 2, KC = kAllAlignedChunk;
+  constexpr int KC = kAllAlignedChunk;
   constexpr uint32_t VB = KC * 64 * sizeof(V), BB = KC * 4, SB = VB + BB;
   // slots gathered per sub-block: about 32 gathered fp32 values (16 fp64) per lane over its two rows
   constexpr int SUB0 = (sizeof(Acc) == 8 ? 16 : 32) / (2 * K);

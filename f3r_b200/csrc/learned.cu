@@ -840,6 +840,7 @@ Status loss_and_grad(f3r_learned *L, double *loss_d, bool want_grad) {
 extern "C" {
 
 f3r_status f3r_learned_create(f3r_context *ctx, int32_t hidden, uint64_t seed, f3r_learned **out) {
+  clear_stale_error();
   if (!ctx || !out) return fail(F3R_ERROR_INVALID_VALUE, "null argument");
   if (hidden != kH) return fail(F3R_ERROR_UNSUPPORTED, "the network's hidden width is 64");
   CUDA_TRY(cudaSetDevice(ctx->device));
@@ -892,6 +893,7 @@ f3r_status f3r_learned_params(f3r_learned *L, float *params, int32_t set, int64_
 
 f3r_status f3r_learned_set_data(f3r_learned *L, const f3r_csr *a, int32_t nx, int32_t ny, const f3r_csr *z,
                                 const f3r_csr *wt, int32_t npairs, const double *r, const double *e) {
+  clear_stale_error();
   if (!L || !a || !z || !wt || npairs < 1 || npairs > 1024 || !r || !e)
     return fail(F3R_ERROR_INVALID_VALUE, "bad argument (npairs in 1..1024)");
   CUDA_TRY(cudaSetDevice(L->ctx->device));
@@ -924,6 +926,7 @@ f3r_status f3r_learned_set_data(f3r_learned *L, const f3r_csr *a, int32_t nx, in
 }
 
 f3r_status f3r_learned_evaluate(f3r_learned *L, double *loss, float *grad) {
+  clear_stale_error();
   if (!L || !loss) return fail(F3R_ERROR_INVALID_VALUE, "null argument");
   if (L->train.npairs == 0) return fail(F3R_ERROR_INVALID_VALUE, "no training data set");
   CUDA_TRY(cudaSetDevice(L->ctx->device));
@@ -944,6 +947,7 @@ f3r_status f3r_learned_evaluate(f3r_learned *L, double *loss, float *grad) {
 }
 
 f3r_status f3r_learned_train(f3r_learned *L, int32_t steps, double lr, double *losses) {
+  clear_stale_error();
   if (!L || steps < 0 || !(lr > 0)) return fail(F3R_ERROR_INVALID_VALUE, "bad argument");
   if (L->train.npairs == 0) return fail(F3R_ERROR_INVALID_VALUE, "no training data set");
   if (steps == 0) return F3R_SUCCESS;
@@ -974,6 +978,7 @@ f3r_status f3r_learned_train(f3r_learned *L, int32_t steps, double lr, double *l
 
 f3r_status f3r_learned_correct(f3r_learned *L, const f3r_csr *a, int32_t nx, int32_t ny, const f3r_csr *z,
                                const f3r_csr *wt, int32_t bf16, double *z_val, double *wt_val, float *delta) {
+  clear_stale_error();
   if (!L || !a || !z || !wt || !z_val || !wt_val) return fail(F3R_ERROR_INVALID_VALUE, "null argument");
   CUDA_TRY(cudaSetDevice(L->ctx->device));
   Context &c = *L->ctx;
@@ -998,6 +1003,7 @@ f3r_status f3r_learned_correct(f3r_learned *L, const f3r_csr *a, int32_t nx, int
 
 f3r_status f3r_learned_time_inference(f3r_learned *L, const f3r_csr *a, int32_t nx, int32_t ny, const f3r_csr *z,
                                       const f3r_csr *wt, int32_t mode, int32_t reps, double *us) {
+  clear_stale_error();
   if (!L || !a || !z || !wt || !us) return fail(F3R_ERROR_INVALID_VALUE, "null argument");
   if (mode < 0 || mode > 2 || reps < 1) return fail(F3R_ERROR_INVALID_VALUE, "mode must be 0, 1 or 2 and reps >= 1");
   CUDA_TRY(cudaSetDevice(L->ctx->device));

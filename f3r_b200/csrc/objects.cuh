@@ -23,6 +23,13 @@ namespace f3r {
 
 inline int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
+// Entry points that run CUDA work start here: the runtime keeps the last
+// non-sticky error of any earlier call on this thread (the caller's, another
+// library's) until someone reads it, and the launch checks below read it, so
+// it is cleared first.  A sticky error (a lost context) is returned by every
+// later call anyway.
+inline void clear_stale_error() { (void)cudaGetLastError(); }
+
 // ---------------------------------------------------------------------------
 // context
 // ---------------------------------------------------------------------------

@@ -127,7 +127,8 @@ template <typename CI> struct SellCfg<__half, CI> { static constexpr int WARPS =
 template <typename CI> struct SellCfg<float, CI> { static constexpr int WARPS = 24, STAGES = 2, KC = 16; };
 template <typename CI> struct SellCfg<double, CI> { static constexpr int WARPS = 16, STAGES = 2, KC = 16; };
 template <> struct SellCfg<__half, AllAlignedIdx> { static constexpr int WARPS = 32, STAGES = 2, KC = 32; };
-template <> struct SellCfg<float, AllAlignedIdx> { static constexpr int WARPS = 24, STAGES = 2, KC = 32; };
+// fp32, fully aligned: one stage a warp, 32 warps (151 us at 192^3 against 161 us at 24 x 2)
+template <> struct SellCfg<float, AllAlignedIdx> { static constexpr int WARPS = 32, STAGES = 1, KC = 32; };
 template <> struct SellCfg<double, AllAlignedIdx> { static constexpr int WARPS = 12, STAGES = 2, KC = 32; };
 
 template <typename V, typename CI, int WARPS, int STAGES, int KC>
@@ -401,11 +402,15 @@ __global__ void __launch_bounds__(WARPS * 32, 1)
 // those of every other layout.
 // ---------------------------------------------------------------------------
 template <typename V> struct Sell64Cfg;
-template <> struct Sell64Cfg<__half> { static constexpr int WARPS = 24, STAGES = 2, KC = 32; };
-// a stage holds a 64-row x 32-column chunk: the warps x stages products fill
-// up to ~200 KB of the 227 KB a block may hold
-template <> struct Sell64Cfg<float> { static constexpr int WARPS = 12, STAGES = 2, KC = 32; };
-template <> struct Sell64Cfg<double> { static constexpr int WARPS = 6, STAGES = 2, KC = 32; };
+// A stage holds a 64-row x 32-column chunk and is released as soon as the
+// chunk's values and bases sit in registers, so one stage a warp keeps the
+// copy engine ahead and leaves the shared memory to more warps (and to L1 for
+// the x gathers).  Measured at 192^3 (f3r_sell_tune): fp16 89 us at 32 warps x
+// 1 stage against 102 us at 24 x 2; fp32 130 against 155 us (24 x 1 against
+// 12 x 2); fp64 267 against 355 us (12 x 1 against 6 x 2).
+template <> struct Sell64Cfg<__half> { static constexpr int WARPS = 32, STAGES = 1, KC = 32; };
+template <> struct Sell64Cfg<float> { static constexpr int WARPS = 24, STAGES = 1, KC = 32; };
+template <> struct Sell64Cfg<double> { static constexpr int WARPS = 12, STAGES = 1, KC = 32; };
 
 template <typename V, int WARPS, int STAGES, int KC> constexpr size_t sell64_smem_bytes_cfg() {
   return (size_t)WARPS * STAGES * ((size_t)KC * 64 * sizeof(V) + KC * 4) + (size_t)WARPS * STAGES * sizeof(uint64_t);

@@ -644,7 +644,7 @@ Status launch_block_one(Context &c, const V *val, const DevSell &A, const X *x, 
 template <typename V, typename X, typename Epi, int K>
 Status launch_block64(Context &c, const V *val, const DevSell &A, const X *x, const Epi &epi, bool attr_only) {
   constexpr int W = block64_warps<V, K>();
-  auto kern = k_sell_block64<V, X, Epi, K, W>;
+  auto kern = k_sell_block64<V, X, Epi, K, W, block64_stages<V, K>()>;
   static int done[64] = {0};
   if (!done[c.device & 63]) {
     CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)block64_smem_bytes<V, K>()));
@@ -2064,6 +2064,7 @@ const void *solver_context(const f3r_solver *s) { return s && s->s ? (const void
 int32_t solver_rows(const f3r_solver *s) { return s && s->s ? s->s->n : 0; }
 Status solver_solve_multi(f3r_solver *s, int32_t nrhs, const double *b, int64_t ldb, double *x, int64_t ldx,
                           f3r_cond_fn cond, void *user, f3r_result *results) {
+  clear_stale_error();
   CUDA_TRY(cudaSetDevice(s->s->ctx->device));
   return s->s->solve_multi(nrhs, b, ldb, x, ldx, cond, user, results);
 }
@@ -2182,6 +2183,7 @@ f3r_status f3r_host_ilu0_bj(const f3r_csr *a, int32_t blocks, double acc, f3r_ho
 
 // ---- context ----------------------------------------------------------------
 f3r_status f3r_context_create(int32_t device, f3r_context **out) {
+  clear_stale_error();
   if (!out) return fail(F3R_ERROR_INVALID_VALUE, "out is null");
   int count = 0;
   if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
@@ -2240,6 +2242,7 @@ f3r_status f3r_context_synchronize(f3r_context *ctx) {
 // ---- SELL -------------------------------------------------------------------
 f3r_status f3r_sell_create(f3r_context *ctx, const f3r_csr *a, int32_t slice_height, int32_t sigma,
                            int32_t dtype_mask, f3r_sell **out) {
+  clear_stale_error();
   if (!ctx || !out) return fail(F3R_ERROR_INVALID_VALUE, "null argument");
   if (slice_height != 32 && slice_height != 64) return fail(F3R_ERROR_UNSUPPORTED, "slice height 32 or 64");
   if (slice_height == 64 && (sigma != 1 || (dtype_mask & (F3R_SELL_INDEX16 | F3R_SELL_CSR))))
@@ -2304,6 +2307,7 @@ void f3r_sell_destroy(f3r_sell *m) {
 }
 
 f3r_status f3r_sell_operate(f3r_sell *m, f3r_dtype val_t, f3r_dtype in_t, const void *in, f3r_dtype out_t, void *out) {
+  clear_stale_error();
   if (!m || !in || !out) return fail(F3R_ERROR_INVALID_VALUE, "null argument");
   Context &c = *m->ctx;
   const DeviceSell &d = m->d;
@@ -2324,6 +2328,7 @@ f3r_status f3r_sell_operate(f3r_sell *m, f3r_dtype val_t, f3r_dtype in_t, const 
 
 f3r_status f3r_sell_compute_residual(f3r_sell *m, f3r_dtype val_t, f3r_dtype rhs_t, const void *rhs, f3r_dtype in_t,
                                      const void *in, f3r_dtype res_t, void *res) {
+  clear_stale_error();
   if (!m || !rhs || !in || !res) return fail(F3R_ERROR_INVALID_VALUE, "null argument");
   Context &c = *m->ctx;
   const DeviceSell &d = m->d;
@@ -2339,6 +2344,7 @@ f3r_status f3r_sell_compute_residual(f3r_sell *m, f3r_dtype val_t, f3r_dtype rhs
 }
 
 f3r_status f3r_context_wait_probe(f3r_context *ctx, int32_t set, int32_t limit_ms) {
+  clear_stale_error();
   if (!ctx || limit_ms < 1 || limit_ms > 10000) return fail(F3R_ERROR_INVALID_VALUE, "need 1 <= limit_ms <= 10000");
   Context &c = *ctx;
   CUDA_TRY(cudaSetDevice(c.device));
@@ -2353,6 +2359,7 @@ f3r_status f3r_context_wait_probe(f3r_context *ctx, int32_t set, int32_t limit_m
 }
 
 f3r_status f3r_dot(f3r_context *ctx, f3r_dtype t, int64_t n, const void *x, const void *y, double *result) {
+  clear_stale_error();
   if (!ctx || !result || n < 0 || (n > 0 && (!x || !y))) return fail(F3R_ERROR_INVALID_VALUE, "bad argument");
   Context &c = *ctx;
   const int g = c.ew_grid(n);
@@ -2399,6 +2406,7 @@ void f3r_params_default(f3r_params *p) {
 }
 
 f3r_status f3r_solver_create(f3r_context *ctx, const f3r_csr *a, const f3r_params *p, f3r_solver **out) {
+  clear_stale_error();
   if (!ctx || !a || !p || !out) return fail(F3R_ERROR_INVALID_VALUE, "null argument");
   Solver *s = nullptr;
   F3R_TRY(make_solver(ctx, a, p, &s));
@@ -2407,6 +2415,7 @@ f3r_status f3r_solver_create(f3r_context *ctx, const f3r_csr *a, const f3r_param
 }
 f3r_status f3r_solver_create_factors(f3r_context *ctx, const f3r_csr *a, const f3r_params *p, const f3r_csr *z,
                                      const f3r_csr *wt, f3r_solver **out) {
+  clear_stale_error();
   if (!ctx || !a || !p || !z || !wt || !out) return fail(F3R_ERROR_INVALID_VALUE, "null argument");
   Solver *s = nullptr;
   F3R_TRY(make_solver(ctx, a, p, &s, z, wt));
@@ -2415,6 +2424,7 @@ f3r_status f3r_solver_create_factors(f3r_context *ctx, const f3r_csr *a, const f
 }
 f3r_status f3r_solver_solve(f3r_solver *s, const double *b, double *x, f3r_cond_fn cond, void *user,
                             f3r_result *result) {
+  clear_stale_error();
   if (!s || !b || !x) return fail(F3R_ERROR_INVALID_VALUE, "null argument");
   CUDA_TRY(cudaSetDevice(s->s->ctx->device));
   return s->s->solve(b, x, cond, user, result);
@@ -2439,6 +2449,7 @@ f3r_status f3r_solver_info(const f3r_solver *s, f3r_sell_info *a_info, int32_t *
 }
 f3r_status f3r_solver_operate(f3r_solver *s, f3r_dtype val_t, f3r_dtype in_t, const void *in, f3r_dtype out_t,
                               void *out) {
+  clear_stale_error();
   if (!s || !in || !out) return fail(F3R_ERROR_INVALID_VALUE, "null argument");
   Context &c = *s->s->ctx;
   const DeviceSell &d = s->s->A;
@@ -2458,6 +2469,7 @@ f3r_status f3r_solver_operate(f3r_solver *s, f3r_dtype val_t, f3r_dtype in_t, co
 
 f3r_status f3r_batch_create(f3r_context *ctx, int32_t count, const f3r_csr *const *a, const f3r_params *p,
                             const f3r_csr *const *z, const f3r_csr *const *wt, f3r_batch **out) {
+  clear_stale_error();
   if (!ctx || !a || !p || !out || (z != nullptr) != (wt != nullptr)) return fail(F3R_ERROR_INVALID_VALUE, "bad argument");
   Solver *s = nullptr;
   F3R_TRY(make_batch(ctx, count, a, p, &s, z, wt));
@@ -2466,6 +2478,7 @@ f3r_status f3r_batch_create(f3r_context *ctx, int32_t count, const f3r_csr *cons
 }
 f3r_status f3r_batch_solve(f3r_batch *bt, const double *const *b, double *const *x, f3r_cond_fn cond, void *user,
                            f3r_result *results) {
+  clear_stale_error();
   f3r_solver *s = reinterpret_cast<f3r_solver *>(bt);
   if (!s || !b || !x) return fail(F3R_ERROR_INVALID_VALUE, "null argument");
   for (int i = 0; i < s->s->mm_count; i++)

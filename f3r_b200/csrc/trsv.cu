@@ -215,6 +215,7 @@ extern "C" {
 
 f3r_status f3r_trsv_create(f3r_context *ctx, const f3r_csr *m, int32_t form, int32_t kind, int32_t iters,
                            double omega, f3r_trsv **out) {
+  clear_stale_error();
   if (!ctx || !out) return fail(F3R_ERROR_INVALID_VALUE, "null argument");
   F3R_TRY(check_csr(m));
   CUDA_TRY(cudaSetDevice(ctx->device));
@@ -235,6 +236,7 @@ f3r_status f3r_trsv_create(f3r_context *ctx, const f3r_csr *m, int32_t form, int
 }
 
 f3r_status f3r_trsv_solve(f3r_trsv *t, const void *in, void *out) {
+  clear_stale_error();
   if (!t || !in || !out) return fail(F3R_ERROR_INVALID_VALUE, "null argument");
   CUDA_TRY(cudaSetDevice(t->ctx->device));
   return t->t.apply(*t->ctx, (const __half *)in, (__half *)out, nullptr);

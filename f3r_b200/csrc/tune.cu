@@ -141,6 +141,8 @@ void sweep(Context &c, const DeviceSell &d, const V *val, const X *x, Y *y, int 
     time_shape<V, X, Y, 12, 2, 32, CI>(c, d, val, x, y, reps, out);
     time_shape<V, X, Y, 8, 4, 32, CI>(c, d, val, x, y, reps, out);
     time_shape<V, X, Y, 8, 2, 32, CI>(c, d, val, x, y, reps, out);
+    time_shape<V, X, Y, 32, 1, 32, CI>(c, d, val, x, y, reps, out);
+    time_shape<V, X, Y, 24, 1, 32, CI>(c, d, val, x, y, reps, out);
   } else {
     time_shape<V, X, Y, 24, 2, 16, CI>(c, d, val, x, y, reps, out);
     time_shape<V, X, Y, 20, 2, 16, CI>(c, d, val, x, y, reps, out);
@@ -151,6 +153,8 @@ void sweep(Context &c, const DeviceSell &d, const V *val, const X *x, Y *y, int 
     time_shape<V, X, Y, 32, 2, 8, CI>(c, d, val, x, y, reps, out);
     time_shape<V, X, Y, 24, 3, 8, CI>(c, d, val, x, y, reps, out);
     time_shape<V, X, Y, 8, 4, 16, CI>(c, d, val, x, y, reps, out);
+    time_shape<V, X, Y, 32, 1, 16, CI>(c, d, val, x, y, reps, out);
+    time_shape<V, X, Y, 24, 1, 16, CI>(c, d, val, x, y, reps, out);
   }
 }
 
@@ -183,6 +187,7 @@ using namespace f3r;
 
 extern "C" f3r_status f3r_sell_tune(f3r_sell *m, f3r_dtype val_t, int32_t reps, f3r_tune_entry *out, int32_t cap,
                                     int32_t *count) {
+  clear_stale_error();
   if (!m || !out || !count || cap < 1 || reps < 1) return fail(F3R_ERROR_INVALID_VALUE, "bad argument");
   const DeviceSell &d = m->d;
   if (!(d.dtypes & (1 << val_t))) return fail(F3R_ERROR_INVALID_VALUE, "matrix holds no copy of that value type");

@@ -378,8 +378,9 @@ f3r_status f3r_solver_info(const f3r_solver *s, f3r_sell_info *a_info, int32_t *
 /* Several right-hand sides: column k of B (b + k * ldb) is solved into
  * column k of X (x + k * ldx), x holding the initial guesses; ldb, ldx >= n;
  * host or device pointers; results (may be NULL) gets one entry per column.
- * With SDAINV and 32-row SELL slices (packed or offset-aligned) the columns
- * run in lockstep blocks of up to 16: every product streams the matrix once
+ * With SDAINV and SELL storage (packed or offset-aligned, 32- or 64-row
+ * slices) the columns run in lockstep blocks of up to 16 (8 from 2^20 rows;
+ * a single column left over is solved alone): every product streams the matrix once
  * for the block, each column keeps its own Hessenberg matrix, rotations and
  * Richardson weights, and its result is its single solve's bit for bit.  cond
  * is then called once per outer step for each column still running, in
