@@ -852,7 +852,7 @@ def c5_line(args):
     nx = args.nx if args.nx != NX else 128
     ctx = F.Context(0)
     t0 = time.perf_counter()
-    ts = training_set(ctx, range(args.c5_train), nt=24, **PARAMS)
+    ts = training_set(ctx, range(args.c5_train), nt=args.c5_train_grid, **PARAMS)
     t_data = time.perf_counter() - t0
     L = Learned(ctx, seed=0)
     L.set_data(**ts.data())
@@ -959,7 +959,7 @@ def c5_line(args):
             "data": "synthetic (seeded log-normal coefficient fields)",
             "config": {"workload": f"C5: 7-pt diffusion, log-normal sigma 1.5, corr 6, {nx}^3 held-out "
                                    f"(n={nx ** 3}), SDAINV vs learned SDAINV, tol 1e-10",
-                       "train_fields": args.c5_train, "train_grid": "24^3 each, stacked", "train_rows": n_train,
+                       "train_fields": args.c5_train, "train_grid": f"{args.c5_train_grid}^3 each, stacked", "train_rows": n_train,
                        "eval_fields": args.c5_eval, "batch": C5_BATCH, "sell_single": layout_desc(),
                        "sell_batched": "packed SELL-32, int32 indices, values of the batch interleaved",
                        "timing": "single: device solve time (CUDA events), best of steps; batched: host wall "
@@ -1017,6 +1017,7 @@ def main():
                          "beside it, the reference's CPU solve")
     ap.add_argument("--block-k", type=int, default=8, help="right-hand sides of the C2 block measurement")
     ap.add_argument("--c5-train", type=int, default=256, help="C5 training fields")
+    ap.add_argument("--c5-train-grid", type=int, default=24, help="C5 training field edge")
     ap.add_argument("--c5-eval", type=int, default=4, help="C5 held-out fields solved (32 for the full set)")
     ap.add_argument("--c5-steps", type=int, default=500, help="C5 Adam steps")
     args = ap.parse_args()
