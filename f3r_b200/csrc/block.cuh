@@ -289,7 +289,10 @@ __global__ void __launch_bounds__(WARPS * 32, 1)
     // first (then the stage goes back to the copy engine), then the gathers
     // of the sub-block, then its multiply-adds
     constexpr int NSUB = (KC + SUB - 1) / SUB;
-    Acc vv[SUB][VK];
+    // fp16 values with fp16 x stay fp16 for the mixed-precision FMA, else widened
+    constexpr bool H2 = std::is_same<V, __half>::value && std::is_same<X, __half>::value;
+    using VB = typename std::conditional<H2, __half, Acc>::type;
+    VB vv[SUB][VK];
     int32_t cc[SUB];
     const V *lv = sv + lane * kc;  // aligned form: lane-major values
     for (int h = 0; h < NSUB; h++) {
@@ -300,7 +303,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1)
         const int k = k0 + e;
         if (k < kc) {
           if (MODE == 3 || MODE == 2) {
-            vv[e][0] = to_acc<Acc>(lv[k]);  // lane-major values
+            vv[e][0] = to_acc<VB>(lv[k]);  // lane-major values
             if (MODE == 2 && !aligned) {
               cc[e] = sc[k * 32 + lane];
             } else {
@@ -314,7 +317,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1)
         }
       }
       if (k0 + SUB >= kc) release();  // last sub-block of the chunk: its shared data is in registers
-      Acc xg[SUB][K];
+      VB xg[SUB][K];
 #pragma unroll
       for (int e = 0; e < SUB; e++)
         if (k0 + e < kc) RowK<X, K>::ldg(x + (size_t)cc[e] * K, xg[e]);
@@ -322,7 +325,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1)
       for (int e = 0; e < SUB; e++)
         if (k0 + e < kc) {
 #pragma unroll
-          for (int c = 0; c < K; c++) acc[c] = fmaT(vv[e][MM ? c : 0], xg[e][c], acc[c]);
+          for (int c = 0; c < K; c++) acc[c] = fma_vx<Acc>(vv[e][MM ? c : 0], xg[e][c], acc[c]);
         }
     }
     ck += kc;
@@ -451,22 +454,25 @@ __global__ void __launch_bounds__(WARPS * 32, 1)
     const int32_t *sb = reinterpret_cast<const int32_t *>(buf + (size_t)cst * SB + VB);
     cst = (cst + 1 == STAGES) ? 0 : cst + 1;
     const V *lv0 = sv + lane * kc, *lv1 = sv + (lane + 32) * kc;  // the two rows' values
+    // fp16 values with fp16 x stay fp16 for the mixed-precision FMA, else widened
+    constexpr bool H2 = std::is_same<V, __half>::value && std::is_same<X, __half>::value;
+    using VB = typename std::conditional<H2, __half, Acc>::type;
     for (int k0 = 0; k0 < kc; k0 += SUB) {
-      Acc v0[SUB], v1[SUB];
+      VB v0[SUB], v1[SUB];
       int32_t c0[SUB], c1[SUB];
 #pragma unroll
       for (int e = 0; e < SUB; e++) {
         const int k = k0 + e;
         if (k < kc) {
-          v0[e] = to_acc<Acc>(lv0[k]);
-          v1[e] = to_acc<Acc>(lv1[k]);
+          v0[e] = to_acc<VB>(lv0[k]);
+          v1[e] = to_acc<VB>(lv1[k]);
           const int32_t b = sb[k] + lane;
           c0[e] = clampc ? min(max(b, 0), A.ncols - 1) : b;
           c1[e] = clampc ? min(max(b + 32, 0), A.ncols - 1) : b + 32;
         }
       }
       if (k0 + SUB >= kc) release();  // last sub-block of the chunk: its shared data is in registers
-      Acc x0[SUB][K], x1[SUB][K];
+      VB x0[SUB][K], x1[SUB][K];
 #pragma unroll
       for (int e = 0; e < SUB; e++)
         if (k0 + e < kc) {
@@ -478,8 +484,8 @@ __global__ void __launch_bounds__(WARPS * 32, 1)
         if (k0 + e < kc) {
 #pragma unroll
           for (int c = 0; c < K; c++) {
-            acc0[c] = fmaT(v0[e], x0[e][c], acc0[c]);
-            acc1[c] = fmaT(v1[e], x1[e][c], acc1[c]);
+            acc0[c] = fma_vx<Acc>(v0[e], x0[e][c], acc0[c]);
+            acc1[c] = fma_vx<Acc>(v1[e], x1[e][c], acc1[c]);
           }
         }
     }

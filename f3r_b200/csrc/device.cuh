@@ -139,6 +139,19 @@ template <> __device__ __forceinline__ __half to_acc<__half>(__half v) { return 
 __device__ __forceinline__ float fmaT(float a, float b, float c) { return __fmaf_rn(a, b, c); }
 __device__ __forceinline__ double fmaT(double a, double b, double c) { return __fma_rn(a, b, c); }
 
+// acc + v x with one rounding.  Two fp16 operands go through sm_100's
+// mixed-precision FMA (fp16 sources, fp32 addend and result): the product of
+// two fp16 values is exact in fp32, so this is fmaf(float(v), float(x), acc)
+// bit for bit, without the two conversions.
+template <typename Acc, typename V, typename X> __device__ __forceinline__ Acc fma_vx(V v, X x, Acc acc) {
+  return fmaT(to_acc<Acc>(v), to_acc<Acc>(x), acc);
+}
+template <> __device__ __forceinline__ float fma_vx<float, __half, __half>(__half v, __half x, float acc) {
+  asm("fma.rn.f32.f16 %0, %1, %2, %0;" : "+f"(acc) : "h"(__half_as_ushort(v)), "h"(__half_as_ushort(x)));
+  return acc;
+}
+
+
 // ---- deterministic grid reduction --------------------------------------------
 // Every block contributes NV partial sums; the last block to arrive adds the
 // partials in block order and calls fin(totals) on thread 0.  The ticket

@@ -545,6 +545,13 @@ __device__ __forceinline__ bool group_sync_and(int id, bool ok) {
       : "memory");
   return out != 0;
 }
+// relu of two fp32 values rounded to bf16 and packed (lo in the low half) in one
+// instruction: for finite values the bits of pack_bf16(relu(lo), relu(hi))
+__device__ __forceinline__ uint32_t pack_relu_bf16(float lo, float hi) {
+  uint32_t d;
+  asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(hi), "f"(lo));
+  return d;
+}
 // relu(acc + bias) of 16 columns of a row, stored as bf16 at A2 columns c0..c0+15
 __device__ __forceinline__ void tc_epilogue16(unsigned char *a2, int row, int c0, const float (&v)[16],
                                               const float *bias) {
@@ -559,7 +566,7 @@ __device__ __forceinline__ void tc_epilogue16(unsigned char *a2, int row, int c0
   }
   uint32_t p[8];
 #pragma unroll
-  for (int i = 0; i < 8; i++) p[i] = pack_bf16(relu(v[2 * i] + b[2 * i]), relu(v[2 * i + 1] + b[2 * i + 1]));
+  for (int i = 0; i < 8; i++) p[i] = pack_relu_bf16(v[2 * i] + b[2 * i], v[2 * i + 1] + b[2 * i + 1]);
   *reinterpret_cast<uint4 *>(a2 + kmaj_off(row, c0, kH)) = make_uint4(p[0], p[1], p[2], p[3]);
   *reinterpret_cast<uint4 *>(a2 + kmaj_off(row, c0 + 8, kH)) = make_uint4(p[4], p[5], p[6], p[7]);
 }

@@ -148,6 +148,9 @@ template <typename V, typename X, typename Epi, int WARPS, int STAGES, int KC, t
 __global__ void __launch_bounds__(WARPS * 32, 1)
     k_sell_cfg(const V *__restrict__ val, DevSell A, const X *__restrict__ x, Epi epi, int *err) {
   using Acc = typename acc_of<V>::type;
+  // gathered x kept as fp16 where value and x are both fp16 (the mixed-precision FMA takes them)
+  using XB = typename std::conditional<std::is_same<V, __half>::value && std::is_same<X, __half>::value, __half,
+                                       Acc>::type;
   constexpr int MODE = IdxForm<CI>::mode;
   constexpr bool C16 = MODE == 1;
   using SI = typename std::conditional<C16, uint16_t, int32_t>::type;  // stored index type
@@ -270,9 +273,9 @@ __global__ void __launch_bounds__(WARPS * 32, 1)
       const V *lv = sv + lane * kc;  // lane-major values (kc a multiple of 4)
       const int nsub = (kc + SUB - 1) / SUB;
       V vb[2][SUB];
-      Acc xb[2][SUB];
+      XB xb[2][SUB];
       const X *xl = x + lane;  // this lane's column is base + lane
-      auto load_sub = [&](int h, V (&v)[SUB], Acc (&xg)[SUB]) {
+      auto load_sub = [&](int h, V (&v)[SUB], XB (&xg)[SUB]) {
 #pragma unroll
         for (int g = 0; g < SUB / 4; g++) {
           const int k0 = h * SUB + g * 4;
@@ -285,10 +288,10 @@ __global__ void __launch_bounds__(WARPS * 32, 1)
             for (int e = 0; e < 4; e++) v[g * 4 + e] = t[e];
             if (!clampc) {
 #pragma unroll
-              for (int e = 0; e < 4; e++) xg[g * 4 + e] = to_acc<Acc>(__ldg(xl + b[e]));
+              for (int e = 0; e < 4; e++) xg[g * 4 + e] = to_acc<XB>(__ldg(xl + b[e]));
             } else {
 #pragma unroll
-              for (int e = 0; e < 4; e++) xg[g * 4 + e] = to_acc<Acc>(__ldg(x + min(max(b[e] + lane, 0), A.ncols - 1)));
+              for (int e = 0; e < 4; e++) xg[g * 4 + e] = to_acc<XB>(__ldg(x + min(max(b[e] + lane, 0), A.ncols - 1)));
             }
           }
         }
@@ -306,7 +309,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1)
           for (int g = 0; g < SUB / 4; g++)
             if (full || h * SUB + g * 4 < kc) {
 #pragma unroll
-              for (int e = 0; e < 4; e++) acc = fmaT(to_acc<Acc>(vb[h & 1][g * 4 + e]), xb[h & 1][g * 4 + e], acc);
+              for (int e = 0; e < 4; e++) acc = fma_vx<Acc>(vb[h & 1][g * 4 + e], xb[h & 1][g * 4 + e], acc);
             }
         }
       }
@@ -354,19 +357,19 @@ __global__ void __launch_bounds__(WARPS * 32, 1)
       }
       // the chunk is in registers: release the stage to the copy engine now
       release();
-      Acc xv[KC];
+      XB xv[KC];
       if (full) {
 #pragma unroll
-        for (int k = 0; k < KC; k++) xv[k] = to_acc<Acc>(__ldg(x + cc[k]));
+        for (int k = 0; k < KC; k++) xv[k] = to_acc<XB>(__ldg(x + cc[k]));
 #pragma unroll
-        for (int k = 0; k < KC; k++) acc = fmaT(to_acc<Acc>(vv[k]), xv[k], acc);
+        for (int k = 0; k < KC; k++) acc = fma_vx<Acc>(vv[k], xv[k], acc);
       } else {
 #pragma unroll
         for (int k = 0; k < KC; k++)
-          if (k < kc) xv[k] = to_acc<Acc>(__ldg(x + cc[k]));
+          if (k < kc) xv[k] = to_acc<XB>(__ldg(x + cc[k]));
 #pragma unroll
         for (int k = 0; k < KC; k++)
-          if (k < kc) acc = fmaT(to_acc<Acc>(vv[k]), xv[k], acc);
+          if (k < kc) acc = fma_vx<Acc>(vv[k], xv[k], acc);
       }
     }
     ck += kc;
@@ -528,9 +531,12 @@ __global__ void __launch_bounds__(WARPS * 32, 1)
     const V *lv0 = sv + lane * kc, *lv1 = sv + (lane + 32) * kc;  // the two rows' values (kc a multiple of 4)
     const int nsub = (kc + SUB - 1) / SUB;
     constexpr int NS = KC / SUB;
+    // gathered x: kept as fp16 where value and x are both fp16 (the mixed FMA takes them), else widened
+    using XB = typename std::conditional<std::is_same<V, __half>::value && std::is_same<X, __half>::value, __half,
+                                         Acc>::type;
     V vb0[2][SUB], vb1[2][SUB];
-    Acc xb0[2][SUB], xb1[2][SUB];
-    auto load_sub = [&](int h, V (&v0)[SUB], V (&v1)[SUB], Acc (&g0)[SUB], Acc (&g1)[SUB]) {
+    XB xb0[2][SUB], xb1[2][SUB];
+    auto load_sub = [&](int h, V (&v0)[SUB], V (&v1)[SUB], XB (&g0)[SUB], XB (&g1)[SUB]) {
 #pragma unroll
       for (int g = 0; g < SUB / 4; g++) {
         const int k0 = h * SUB + g * 4;
@@ -549,14 +555,14 @@ __global__ void __launch_bounds__(WARPS * 32, 1)
 #pragma unroll
             for (int e = 0; e < 4; e++) {
               const X *px = xl + b[e];
-              g0[g * 4 + e] = to_acc<Acc>(__ldg(px));
-              g1[g * 4 + e] = to_acc<Acc>(__ldg(px + 32));
+              g0[g * 4 + e] = to_acc<XB>(__ldg(px));
+              g1[g * 4 + e] = to_acc<XB>(__ldg(px + 32));
             }
           } else {
 #pragma unroll
             for (int e = 0; e < 4; e++) {
-              g0[g * 4 + e] = to_acc<Acc>(__ldg(x + min(max(b[e] + lane, 0), A.ncols - 1)));
-              g1[g * 4 + e] = to_acc<Acc>(__ldg(x + min(max(b[e] + lane + 32, 0), A.ncols - 1)));
+              g0[g * 4 + e] = to_acc<XB>(__ldg(x + min(max(b[e] + lane, 0), A.ncols - 1)));
+              g1[g * 4 + e] = to_acc<XB>(__ldg(x + min(max(b[e] + lane + 32, 0), A.ncols - 1)));
             }
           }
         }
@@ -576,8 +582,8 @@ __global__ void __launch_bounds__(WARPS * 32, 1)
           if (full || h * SUB + g * 4 < kc) {
 #pragma unroll
             for (int e = 0; e < 4; e++) {
-              acc0 = fmaT(to_acc<Acc>(vb0[h & 1][g * 4 + e]), xb0[h & 1][g * 4 + e], acc0);
-              acc1 = fmaT(to_acc<Acc>(vb1[h & 1][g * 4 + e]), xb1[h & 1][g * 4 + e], acc1);
+              acc0 = fma_vx<Acc>(vb0[h & 1][g * 4 + e], xb0[h & 1][g * 4 + e], acc0);
+              acc1 = fma_vx<Acc>(vb1[h & 1][g * 4 + e], xb1[h & 1][g * 4 + e], acc1);
             }
           }
       }
