@@ -29,7 +29,8 @@
 //   Adam       one thread per parameter
 // Inference runs the same network in BF16 on the tensor cores with fp32
 // accumulation: tcgen05.mma with TMEM accumulators, one warpgroup per 128-row
-// tile (the default), or mma.sync m16n8k16, one warp per 16-row tile.
+// tile, the biases inside the MMAs (the default), or mma.sync m16n8k16, one
+// warp per 16-row tile, the biases added in fp32.
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -459,11 +460,12 @@ __global__ void __launch_bounds__(128) k_mlp_infer_bf16(int32_t n, const float *
 // thread, A (activations) and B (the weights, stored out x in = N x K) in
 // shared memory in the K-major no-swizzle canonical layout, D (fp32) in tensor
 // memory: row t of the tile is TMEM lane t, read back by thread t with
-// tcgen05.ld.  Layer 1: K 16 (the 7 inputs zero-padded), N 64; layer 2: K 64,
-// N 64; layer 3: K 64, N 16 (8 outputs and 8 zero weight rows).  The epilogue
-// of a layer adds the fp32 bias, applies relu and stores its row as bf16 into
-// the next layer's A, so the arithmetic is that of the mma.sync kernel above:
-// bf16 operands, fp32 accumulation, fp32 bias.
+// tcgen05.ld.  Layer 1: K 16 (the 7 inputs, two bias columns, zeros), N 64;
+// layer 2: K 64 + 16, N 64; layer 3: K 64 + 16, N 16 (8 outputs and 8 zero
+// weight rows).  Each bias is a weight against a constant one, split into two
+// bf16 parts (hi = bf16(b), lo = bf16(b - hi)), so the accumulator holds
+// W x + b and the epilogue of a layer only applies relu and stores its row as
+// bf16 into the next layer's A (one cvt.rn.relu.bf16x2 per two values).
 //
 // Canonical K-major layout without swizzle: 8 x 8 bf16 core matrices of 128
 // contiguous bytes (row r % 8 at 16 r bytes); the K/8 core matrices of an
@@ -473,19 +475,26 @@ __global__ void __launch_bounds__(128) k_mlp_infer_bf16(int32_t n, const float *
 constexpr int kTcRows = 128;        // rows per tile: MMA M, TMEM lanes
 constexpr int kTcGroups = 2;        // warpgroups (tiles in flight) per CTA
 constexpr int kTcCols = 64;         // TMEM columns per warpgroup
-constexpr int kTcK1 = 16, kTcN3 = 16;
-constexpr uint32_t kTcW1 = kH * kTcK1 * 2, kTcW2 = kH * kH * 2, kTcW3 = kTcN3 * kH * 2;  // bytes
-constexpr uint32_t kTcA1 = kTcRows * kTcK1 * 2, kTcA2 = kTcRows * kH * 2;
-constexpr uint32_t kTcOffW2 = kTcW1, kTcOffW3 = kTcOffW2 + kTcW2, kTcOffA = kTcOffW3 + kTcW3;
-constexpr uint32_t kTcOffBias = kTcOffA + kTcGroups * (kTcA1 + kTcA2);
-constexpr uint32_t kTcOffBar = kTcOffBias + (2 * kH + kOut) * 4;
+constexpr int kTcK1 = 16, kTcN3 = 16, kTcKB = 16;
+// bytes of the operands: weights W1 (64 x 16), W2 (64 x 64), W3 (16 x 64); the
+// bias blocks WB2 (64 x 16), WB3 (16 x 16) and the constant ONES (128 x 16,
+// columns 0 and 1 one); per warpgroup the activations A2 (128 x 64), whose
+// first 4 KB hold layer 1's A1 (128 x 16) until layer 1's MMA has read it
+constexpr uint32_t kTcW1 = kH * kTcK1 * 2, kTcW2 = kH * kH * 2, kTcW3 = kTcN3 * kH * 2;
+constexpr uint32_t kTcWB2 = kH * kTcKB * 2, kTcWB3 = kTcN3 * kTcKB * 2, kTcOnes = kTcRows * kTcKB * 2;
+constexpr uint32_t kTcA2 = kTcRows * kH * 2;
+constexpr uint32_t kTcOffW2 = kTcW1, kTcOffW3 = kTcOffW2 + kTcW2, kTcOffWB2 = kTcOffW3 + kTcW3,
+                   kTcOffWB3 = kTcOffWB2 + kTcWB2, kTcOffOnes = kTcOffWB3 + kTcWB3, kTcOffA = kTcOffOnes + kTcOnes;
+constexpr uint32_t kTcOffBar = kTcOffA + kTcGroups * kTcA2;
 constexpr size_t kTcSmem = kTcOffBar + kTcGroups * 8 + 16;
 // Four CTAs fill the 512 TMEM columns of an SM; a fifth never fits beside them
 // (shared memory), so no allocation waits on another CTA.
 constexpr int kTcCtasPerSm = 4;
 static_assert(kTcCtasPerSm * kTcGroups * kTcCols == 512, "TMEM columns of an SM");
+static_assert(kTcCtasPerSm * (kTcSmem + 1024) <= 228 * 1024, "four CTAs fit on an SM");
 static_assert((kTcCtasPerSm + 1) * (kTcSmem + 1024) > 228 * 1024, "a fifth CTA would fit on an SM");
-static_assert(kTcOffA % 128 == 0 && kTcA1 % 128 == 0 && kTcOffBias % 16 == 0 && kTcOffBar % 8 == 0,
+static_assert(kTcOffA % 128 == 0 && kTcOffOnes % 128 == 0 && kTcOffWB2 % 128 == 0 && kTcOffWB3 % 128 == 0 &&
+                  kTcOffBar % 8 == 0,
               "operand alignment");
 
 // byte offset of element (r, k) of a K-major no-swizzle operand with K columns
@@ -552,56 +561,71 @@ __device__ __forceinline__ uint32_t pack_relu_bf16(float lo, float hi) {
   asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(hi), "f"(lo));
   return d;
 }
-// relu(acc + bias) of 16 columns of a row, stored as bf16 at A2 columns c0..c0+15
-__device__ __forceinline__ void tc_epilogue16(unsigned char *a2, int row, int c0, const float (&v)[16],
-                                              const float *bias) {
-  float b[16];  // the 16 biases as four broadcast 16-byte loads
-#pragma unroll
-  for (int i = 0; i < 4; i++) {
-    const float4 q = reinterpret_cast<const float4 *>(bias + c0)[i];
-    b[4 * i] = q.x;
-    b[4 * i + 1] = q.y;
-    b[4 * i + 2] = q.z;
-    b[4 * i + 3] = q.w;
-  }
+// relu of 16 accumulator columns of a row (the bias is in the accumulator),
+// stored as bf16 at A2 columns c0..c0+15
+__device__ __forceinline__ void tc_epilogue16(unsigned char *a2, int row, int c0, const float (&v)[16]) {
   uint32_t p[8];
 #pragma unroll
-  for (int i = 0; i < 8; i++) p[i] = pack_relu_bf16(v[2 * i] + b[2 * i], v[2 * i + 1] + b[2 * i + 1]);
+  for (int i = 0; i < 8; i++) p[i] = pack_relu_bf16(v[2 * i], v[2 * i + 1]);
   *reinterpret_cast<uint4 *>(a2 + kmaj_off(row, c0, kH)) = make_uint4(p[0], p[1], p[2], p[3]);
   *reinterpret_cast<uint4 *>(a2 + kmaj_off(row, c0 + 8, kH)) = make_uint4(p[4], p[5], p[6], p[7]);
+}
+// a bias as two bf16 parts (hi + lo carries 16 of its bits)
+__device__ __forceinline__ void split_bf16(float b, __nv_bfloat16 &hi, __nv_bfloat16 &lo) {
+  hi = __float2bfloat16_rn(b);
+  lo = __float2bfloat16_rn(b - __bfloat162float(hi));
 }
 
 __global__ void __launch_bounds__(kTcRows * kTcGroups, kTcCtasPerSm)
     k_mlp_infer_tc(int32_t n, const float *__restrict__ f, const float *__restrict__ p, float *__restrict__ o,
                    int *err) {
   extern __shared__ __align__(1024) unsigned char tcs[];
-  float *b1s = reinterpret_cast<float *>(tcs + kTcOffBias), *b2s = b1s + kH, *b3s = b2s + kH;
   uint64_t *bars = reinterpret_cast<uint64_t *>(tcs + kTcOffBar);
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(tcs + kTcOffBar + kTcGroups * 8);
   const int tid = threadIdx.x & (kTcRows - 1), g = threadIdx.x / kTcRows, warp = threadIdx.x >> 5;
-  // weights (bf16, canonical layout; the padding rows and columns zero) and biases
+  // weights (bf16, canonical layout; the padding rows and columns zero).  The
+  // biases enter the MMAs: layer 1 through columns 7 and 8 of W1 (hi and lo
+  // parts) against ones in columns 7 and 8 of A1; layers 2 and 3 through one
+  // more K = 16 step, ONES x WB.
+  auto bf = [](float v) { return __float2bfloat16_rn(v); };
   for (int q = threadIdx.x; q < kH * kTcK1; q += blockDim.x) {
     const int j = q / kTcK1, c = q % kTcK1;
-    *reinterpret_cast<__nv_bfloat16 *>(tcs + kmaj_off(j, c, kTcK1)) =
-        __float2bfloat16_rn(c < kIn ? p[oW1 + j * kIn + c] : 0.f);
+    __nv_bfloat16 v = bf(0.f), hi, lo;
+    if (c < kIn) v = bf(p[oW1 + j * kIn + c]);
+    else if (c == kIn || c == kIn + 1) {
+      split_bf16(p[oB1 + j], hi, lo);
+      v = c == kIn ? hi : lo;
+    }
+    *reinterpret_cast<__nv_bfloat16 *>(tcs + kmaj_off(j, c, kTcK1)) = v;
   }
   for (int q = threadIdx.x; q < kH * kH; q += blockDim.x) {
     const int j = q / kH, c = q % kH;
-    *reinterpret_cast<__nv_bfloat16 *>(tcs + kTcOffW2 + kmaj_off(j, c, kH)) = __float2bfloat16_rn(p[oW2 + q]);
+    *reinterpret_cast<__nv_bfloat16 *>(tcs + kTcOffW2 + kmaj_off(j, c, kH)) = bf(p[oW2 + q]);
   }
   for (int q = threadIdx.x; q < kTcN3 * kH; q += blockDim.x) {
     const int s = q / kH, c = q % kH;
-    *reinterpret_cast<__nv_bfloat16 *>(tcs + kTcOffW3 + kmaj_off(s, c, kH)) =
-        __float2bfloat16_rn(s < kOut ? p[oW3 + s * kH + c] : 0.f);
+    *reinterpret_cast<__nv_bfloat16 *>(tcs + kTcOffW3 + kmaj_off(s, c, kH)) = bf(s < kOut ? p[oW3 + s * kH + c] : 0.f);
   }
-  for (int q = threadIdx.x; q < kH; q += blockDim.x) {
-    b1s[q] = p[oB1 + q];
-    b2s[q] = p[oB2 + q];
+  for (int q = threadIdx.x; q < kH * kTcKB; q += blockDim.x) {
+    const int j = q / kTcKB, c = q % kTcKB;
+    __nv_bfloat16 hi, lo;
+    split_bf16(p[oB2 + j], hi, lo);
+    *reinterpret_cast<__nv_bfloat16 *>(tcs + kTcOffWB2 + kmaj_off(j, c, kTcKB)) = c == 0 ? hi : c == 1 ? lo : bf(0.f);
   }
-  if (threadIdx.x < kOut) b3s[threadIdx.x] = p[oB3 + threadIdx.x];
-  unsigned char *a1 = tcs + kTcOffA + g * (kTcA1 + kTcA2), *a2 = a1 + kTcA1;
-  // columns 8..15 of A1 stay zero
-  *reinterpret_cast<uint4 *>(a1 + kmaj_off(tid, 8, kTcK1)) = make_uint4(0, 0, 0, 0);
+  for (int q = threadIdx.x; q < kTcN3 * kTcKB; q += blockDim.x) {
+    const int s = q / kTcKB, c = q % kTcKB;
+    __nv_bfloat16 hi = bf(0.f), lo = bf(0.f);
+    if (s < kOut) split_bf16(p[oB3 + s], hi, lo);
+    *reinterpret_cast<__nv_bfloat16 *>(tcs + kTcOffWB3 + kmaj_off(s, c, kTcKB)) = c == 0 ? hi : c == 1 ? lo : bf(0.f);
+  }
+  for (int q = threadIdx.x; q < kTcRows * kTcKB; q += blockDim.x) {
+    const int r = q / kTcKB, c = q % kTcKB;
+    *reinterpret_cast<__nv_bfloat16 *>(tcs + kTcOffOnes + kmaj_off(r, c, kTcKB)) = bf(c < 2 ? 1.f : 0.f);
+  }
+  // A1 (layer 1's operand) in the first 4 KB of A2: features in columns 0..6,
+  // ones in 7 and 8, zeros beyond; A2 overwrites it after layer 1's MMA
+  unsigned char *a2 = tcs + kTcOffA + g * kTcA2, *a1 = a2;
+  const uint32_t one = pack_bf16(1.f, 0.f);
   if (threadIdx.x == 0) {
     for (int q = 0; q < kTcGroups; q++) mbar_init(&bars[q], 1);
     fence_mbar_init();
@@ -622,6 +646,8 @@ __global__ void __launch_bounds__(kTcRows * kTcGroups, kTcCtasPerSm)
   const uint64_t dA1 = umma_desc(sa1, 128, kTcK1 * 16), dW1 = umma_desc(sw, 128, kTcK1 * 16);
   const uint64_t dA2 = umma_desc(sa2, 128, kH * 16), dW2 = umma_desc(sw + kTcOffW2, 128, kH * 16),
                  dW3 = umma_desc(sw + kTcOffW3, 128, kH * 16);
+  const uint64_t dOnes = umma_desc(sw + kTcOffOnes, 128, kTcKB * 16), dB2 = umma_desc(sw + kTcOffWB2, 128, kTcKB * 16),
+                 dB3 = umma_desc(sw + kTcOffWB3, 128, kTcKB * 16);
   constexpr uint32_t i64 = umma_idesc_bf16(kTcRows, kH), i16 = umma_idesc_bf16(kTcRows, kTcN3);
   const bool issuer = tid == 0;
   const int bar_id = 1 + g;
@@ -657,37 +683,39 @@ __global__ void __launch_bounds__(kTcRows * kTcGroups, kTcCtasPerSm)
 #pragma unroll 1
   for (; tile < ntiles; tile += stride) {
     *reinterpret_cast<uint4 *>(a1 + kmaj_off(tid, 0, kTcK1)) =
-        make_uint4(pack_bf16(fx[0], fx[1]), pack_bf16(fx[2], fx[3]), pack_bf16(fx[4], fx[5]), pack_bf16(fx[6], 0.f));
+        make_uint4(pack_bf16(fx[0], fx[1]), pack_bf16(fx[2], fx[3]), pack_bf16(fx[4], fx[5]), pack_bf16(fx[6], 1.f));
+    *reinterpret_cast<uint4 *>(a1 + kmaj_off(tid, 8, kTcK1)) = make_uint4(one, 0, 0, 0);
     fetch(tile + stride);  // the next tile's rows, in flight behind this tile's chains
     if (!(ok = chain([&] { umma_bf16(tmem, dA1, dW1, i64, 0); }))) break;
 #pragma unroll
     for (int q = 0; q < kH / 16; q++) {
       float v[16];
       tmem_ld16(lane_addr + q * 16, v);
-      tc_epilogue16(a2, tid, q * 16, v, b1s);
+      tc_epilogue16(a2, tid, q * 16, v);
     }
     if (!(ok = chain([&] {
             for (int k = 0; k < kH / 16; k++) umma_bf16(tmem, dA2 + 16 * k, dW2 + 16 * k, i64, k > 0);
+            umma_bf16(tmem, dOnes, dB2, i64, 1);  // + b2
           })))
       break;
 #pragma unroll
     for (int q = 0; q < kH / 16; q++) {
       float v[16];
       tmem_ld16(lane_addr + q * 16, v);
-      tc_epilogue16(a2, tid, q * 16, v, b2s);
+      tc_epilogue16(a2, tid, q * 16, v);
     }
     if (!(ok = chain([&] {
             for (int k = 0; k < kH / 16; k++) umma_bf16(tmem, dA2 + 16 * k, dW3 + 16 * k, i16, k > 0);
+            umma_bf16(tmem, dOnes, dB3, i16, 1);  // + b3
           })))
       break;
     float y[16];
     tmem_ld16(lane_addr, y);
     const int64_t r = tile * kTcRows + tid;
     if (r < n) {
-      const float4 c0 = reinterpret_cast<const float4 *>(b3s)[0], c1 = reinterpret_cast<const float4 *>(b3s)[1];
       float4 *dst = reinterpret_cast<float4 *>(o + r * kOut);
-      dst[0] = make_float4(y[0] + c0.x, y[1] + c0.y, y[2] + c0.z, y[3] + c0.w);
-      dst[1] = make_float4(y[4] + c1.x, y[5] + c1.y, y[6] + c1.z, y[7] + c1.w);
+      dst[0] = make_float4(y[0], y[1], y[2], y[3]);
+      dst[1] = make_float4(y[4], y[5], y[6], y[7]);
     }
   }
   if (!ok) {

@@ -92,10 +92,12 @@ def test_forward_and_bf16_inference_match_reference(ctx):
 @pytest.mark.parametrize("nt", [9, 64, 71])
 def test_tcgen05_inference_matches_mma_sync(ctx, nt):
     """The tcgen05 kernel (128-row tiles, TMEM accumulators) and the mma.sync
-    kernel round the same operands to bf16 and accumulate in fp32; only the
-    order of the fp32 sums differs, which can move an activation by one bf16
-    step.  729 rows: one ragged tile per warpgroup; 64^3 and 71^3: more tiles
-    than warpgroups (the persistent loop), 71^3 ragged."""
+    kernel round the same operands to bf16 and accumulate in fp32.  They
+    differ in the order of the fp32 sums and in the bias, which the tcgen05
+    kernel adds inside the MMA as two bf16 parts (16 of its bits) where the
+    mma.sync kernel adds it in fp32; either can move an activation by one
+    bf16 step.  729 rows: one ragged tile per warpgroup; 64^3 and 71^3: more
+    tiles than warpgroups (the persistent loop), 71^3 ragged."""
     A = F.diffusion7(nt, nt, nt, 1.5, 6.0, 5).scale()
     Z, Wt = A.sdainv()
     L = Learned(ctx, seed=4)
@@ -109,7 +111,7 @@ def test_tcgen05_inference_matches_mma_sync(ctx, nt):
     assert np.max(np.abs(dt - want)) <= 3e-2 * scale
     assert np.max(np.abs(dt - dm)) <= 1e-2 * scale
     # most rows see no activation rounding flip at all
-    assert np.mean(np.all(np.abs(dt - dm) <= 1e-5 * scale, axis=1)) > 0.9
+    assert np.mean(np.all(np.abs(dt - dm) <= 1e-5 * scale, axis=1)) > 0.8
     us_t = L.time_inference(A, nt, nt, Z, Wt, engine="tcgen05", reps=5)
     us_m = L.time_inference(A, nt, nt, Z, Wt, engine="mma.sync", reps=5)
     assert us_t > 0 and us_m > 0

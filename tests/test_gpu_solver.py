@@ -212,11 +212,13 @@ def test_aligned_sell_solve_is_identical(ctx):
     assert np.array_equal(xs[0], xs[1])
 
 
-def test_slice_height_64_solve_is_identical(ctx):
+@pytest.mark.parametrize("dims", [(24, 20, 18), (3, 3, 3), (5, 4, 7)])
+def test_slice_height_64_solve_is_identical(ctx, dims):
     """the solver on 64-row slices (sell_c = 64) reproduces the 32-row
     aligned layout's solve bit for bit, the fused Richardson steps and the
-    weight updates included"""
-    A = F.stencil27(24, 20, 18, 2, 0.5).scale()
+    weight updates included; 27 and 140 rows: one partial slice, and a
+    partial last slice"""
+    A = F.stencil27(*dims, 2, 0.5).scale()
     b = A.spmv(F.random_uniform(7, -1, 1, A.shape[0]))
     xs = []
     for kw in (dict(sell_align=1), dict(sell_c=64)):
