@@ -1068,8 +1068,8 @@ __global__ void k_level2_enterK(double *const *__restrict__ in_slot, const doubl
 
 // x(:, c) = Z y_c (inner levels) or x(:, c) += Z y_c for the columns in mask
 // (outer level), the sum in the level's type T (k_zy)
-template <typename T, typename Out, bool ACCUM, int K>
-__global__ void k_zyK(Cols<T> Z, const T *__restrict__ y, int64_t y_stride, int nz, Out *out_direct,
+template <typename T, typename Out, bool ACCUM, int K, typename ZT = T>
+__global__ void k_zyK(Cols<ZT> Z, const T *__restrict__ y, int64_t y_stride, int nz, Out *out_direct,
                       Out *const *out_slot, uint32_t mask, int64_t n) {
   __shared__ T sy[K][kMaxCols];
   for (int t = threadIdx.x; t < nz * K; t += blockDim.x) {
@@ -1081,12 +1081,12 @@ __global__ void k_zyK(Cols<T> Z, const T *__restrict__ y, int64_t y_stride, int 
   for_row_groups<RowsPer<K>::R>(n, [&](int64_t i0, auto rows) {
     constexpr int E = decltype(rows)::value * K;
     T a[E], r[E];
-    RowK<T, E>::load(Z.p[0] + i0 * K, a);
+    RowK<ZT, E>::load(Z.p[0] + i0 * K, a);  // ZT fp16: widened exactly
 #pragma unroll
     for (int q = 0; q < E; q++) r[q] = mul_rn(a[q], sy[q % K][0]);
     for (int k = 1; k < nz; k++) {
       T b[E];
-      RowK<T, E>::load(Z.p[k] + i0 * K, b);
+      RowK<ZT, E>::load(Z.p[k] + i0 * K, b);
 #pragma unroll
       for (int q = 0; q < E; q++) r[q] = fmaT(b[q], sy[q % K][k], r[q]);
     }

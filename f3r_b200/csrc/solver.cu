@@ -516,6 +516,7 @@ template <int K> struct Work {
   std::vector<double *> V1, Z1;
   double *abs_e = nullptr;
   __half *hin = nullptr, *hout = nullptr, *hout2 = nullptr, *tmp = nullptr, *tmp2 = nullptr, *hr = nullptr;
+  __half *Z16 = nullptr;  // level 3's Z basis in fp16 (Solver::z16)
   RichState *rs = nullptr;
   double **in_slot = nullptr, **out_slot = nullptr;
   double *b_d = nullptr, *x_d = nullptr, *bp_d = nullptr, *xp_d = nullptr, *r_d = nullptr;
@@ -584,6 +585,11 @@ struct Solver {
   // solve is its own system; A, W^T, Z (or wd, zd) hold mm_k values per
   // entry, interleaved.  Solves run the mm_k-column engine only.
   bool mm = false;
+  // Level 3 keeps its Z basis in fp16 (single-column solves).  Each z_j is R's
+  // result, fp16 values written to fp32 (hout times 1 when R's input is not
+  // scaled), so the fp16 copy is exact: the level-3 product and x = Z y see
+  // the same values, with half the bytes.
+  bool z16 = false;
   int mm_k = 0, mm_count = 0;
   Work<1> w1;  // single-column solves
   std::unique_ptr<Work<2>> w2;
@@ -983,11 +989,12 @@ template <int K> struct Engine {
 
   // What an fp32 level calls as its preconditioner: R, or (K = 1) the
   // fp16-vector level when there is one (which then calls R).
-  Status inner_apply(float *in, float *out, float *e_set, int64_t e_stride, const float *in_inv) {
+  Status inner_apply(float *in, float *out, float *e_set, int64_t e_stride, const float *in_inv,
+                     __half *out16 = nullptr) {
     if constexpr (K == 1) {
       if (p.half_m > 0) return levelh(in, in_inv, out, e_set);
     }
-    return rich_apply(in, out, e_set, e_stride, in_inv);
+    return rich_apply(in, out, e_set, e_stride, in_inv, nullptr, out16);
   }
 
   // ---- the fp16-vector level (K = 1): FGMRES<_Float16>(A16, R, half_m) ---------
@@ -1055,6 +1062,23 @@ template <int K> struct Engine {
         F3R_TRY(mv_store(S.A.v16, S.A.view(), (const float *)zj, Vp[j + 1]));
       }
       F3R_TRY(sstep_orthogonalise(L, Vp, V));
+    } else if (K == 1 && S.z16) {
+      if constexpr (K == 1) {
+        Cols<__half> Z16{};
+        for (int k = 0; k < L.m; k++) Z16.p[k] = w.Z16 + (size_t)k * ldn;
+        for (int j = 0; j < L.m; j++) {
+          __half *zj = w.Z16 + (size_t)j * ldn;
+          float *wv = Vp[j + 1];
+          F3R_TRY(inner_apply(Vp[j], nullptr, j == 0 ? L.e : nullptr, es, j == 0 ? in_inv : L.inv, zj));
+          F3R_TRY(mv_store(S.A.v16, S.A.view(), (const __half *)zj, wv));
+          dots(wv, V, j + 1, L, j);
+          cgs(wv, V, j + 1, L, j, j == L.m - 1);
+        }
+        launch_k(C(), k_zyK<float, float, false, K, __half>, C().ew_grid(n), kEwThreads, 0, C().stream, Z16,
+                 (const float *)L.y, (int64_t)(L.m + 1), L.m, out, (float *const *)nullptr, 0u, (int64_t)n);
+        CUDA_TRY(cudaGetLastError());
+        return F3R_SUCCESS;
+      }
     } else {
       for (int j = 0; j < L.m; j++) {
         float *zj = L.Z + (size_t)j * lk();
@@ -1345,6 +1369,7 @@ template <int K> Status make_work(Solver &s, Work<K> &w) {
   F3R_TRY(w.alloc(&w.hin, nn));
   F3R_TRY(w.alloc(&w.hout, nn));
   F3R_TRY(w.alloc(&w.hout2, nn));
+  if (K == 1 && s.z16) F3R_TRY(w.alloc(&w.Z16, (size_t)s.ldn * p.m3));
   F3R_TRY(w.alloc(&w.tmp, nn));
   F3R_TRY(w.alloc(&w.tmp2, nn));
   F3R_TRY(w.alloc(&w.hr, nn));
@@ -1773,9 +1798,11 @@ static Status make_solver(f3r_context *ctx, const f3r_csr *a, const f3r_params *
   F3R_TRY((sell_attr<__half, __half, EpiResidual<__half, __half>>(cx)));
   F3R_TRY((sell_attr<__half, __half, EpiStore<__half>>(cx)));
   F3R_TRY((sell_attr<__half, float, EpiStore<float>>(cx)));
+  F3R_TRY((sell_attr<__half, __half, EpiStore<float>>(cx)));
   F3R_TRY((sell_attr<float, float, EpiStore<float>>(cx)));
   F3R_TRY((sell_attr<__half, __half, EpiZScale>(cx)));
   // the single-column workspace (wider ones are made by the first solve_multi that needs them)
+  s->z16 = p.m3 > 0 && p.half_scale_log2 == 0 && !(p.inner_sstep & 2) && p.half_m == 0;
   F3R_TRY(make_work<1>(*s, s->w1));
   CUDA_TRY(cudaDeviceSynchronize());
   *out = s.release();
