@@ -1196,7 +1196,7 @@ __global__ void k_rich_scale_omK(__half *__restrict__ hout, const RichState *__r
 template <int K>
 __global__ void k_rich_axpyK(__half *__restrict__ hout, const __half *__restrict__ t2,
                              const RichState *__restrict__ rs, int k, int use_ome, float *__restrict__ out, float isc,
-                             int64_t n) {
+                             int64_t n, __half *__restrict__ out16) {
   float om[K];
 #pragma unroll
   for (int c = 0; c < K; c++) om[c] = use_ome ? h2f(rs[c].ome[k]) : rs[c].om[k];
@@ -1212,7 +1212,7 @@ __global__ void k_rich_axpyK(__half *__restrict__ hout, const __half *__restrict
       for (int q = 0; q < E; q++) hn[q] *= isc;
       RowK<float, E>::store(out + i0 * K, hn);
     } else {
-      RowK<__half, E>::store(hout + i0 * K, hn);
+      RowK<__half, E>::store((out16 ? out16 : hout) + i0 * K, hn);
     }
   });
 }

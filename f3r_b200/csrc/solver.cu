@@ -726,6 +726,7 @@ template <int K> struct Engine {
       F3R_TRY((launch_block<double, double, EpiResidualK<double, double, K>, K>(C(), d, Av, d, {}, true)));
       F3R_TRY((launch_block<float, float, EpiStoreK<float, K>, K>(C(), f, Av, f, {}, true)));
       F3R_TRY((launch_block<__half, float, EpiStoreK<float, K>, K>(C(), h, Av, f, {}, true)));
+      F3R_TRY((launch_block<__half, __half, EpiStoreK<float, K>, K>(C(), h, Av, h, {}, true)));
       F3R_TRY((launch_block<__half, __half, EpiStoreK<__half, K>, K>(C(), h, Av, h, {}, true)));
       F3R_TRY((launch_block<__half, __half, EpiRichStepK<K>, K>(C(), h, Av, h, {}, true)));
       F3R_TRY((launch_block<__half, __half, EpiRichResPreK<K>, K>(C(), h, Av, h, {}, true)));
@@ -741,6 +742,7 @@ template <int K> struct Engine {
         F3R_TRY((launch_block_mm<double, double, EpiResidualK<double, double, K>, K>(C(), d, Av, d, {}, true)));
         F3R_TRY((launch_block_mm<float, float, EpiStoreK<float, K>, K>(C(), f, Av, f, {}, true)));
         F3R_TRY((launch_block_mm<__half, float, EpiStoreK<float, K>, K>(C(), h, Av, f, {}, true)));
+        F3R_TRY((launch_block_mm<__half, __half, EpiStoreK<float, K>, K>(C(), h, Av, h, {}, true)));
         F3R_TRY((launch_block_mm<__half, __half, EpiStoreK<__half, K>, K>(C(), h, Av, h, {}, true)));
         F3R_TRY((launch_block_mm<__half, __half, EpiRichStepK<K, true>, K>(C(), h, Av, h, {}, true)));
         F3R_TRY((launch_block_mm<__half, __half, EpiRichResPreK<K, true>, K>(C(), h, Av, h, {}, true)));
@@ -792,9 +794,9 @@ template <int K> struct Engine {
     if (S.precond_diag) {
       if constexpr (K > 1) {
         if (S.mm) {
-          F3R_TRY(rich_diag<true>(in, out, e_set, e_stride, in_inv, upd, sc, isc, hi, h0, out_last));
+          F3R_TRY(rich_diag<true>(in, out, e_set, e_stride, in_inv, upd, sc, isc, hi, h0, out_last, out16));
         } else {
-          F3R_TRY(rich_diag<false>(in, out, e_set, e_stride, in_inv, upd, sc, isc, hi, h0, out_last));
+          F3R_TRY(rich_diag<false>(in, out, e_set, e_stride, in_inv, upd, sc, isc, hi, h0, out_last, out16));
         }
       } else {
         const DiagPre M{S.wd, S.zd};
@@ -869,7 +871,7 @@ template <int K> struct Engine {
   // column, a batch of systems); the same steps as the single-column path
   template <bool MMF>
   Status rich_diag(float *in, float *out, float *e_set, int64_t e_stride, const float *in_inv, bool upd, float sc,
-                   float isc, const __half *hi, __half *h0, float *out_last) {
+                   float isc, const __half *hi, __half *h0, float *out_last, __half *out16) {
     const int64_t N = n;
     const int g = C().ew_grid(N);
     cudaStream_t st = C().stream;
@@ -887,7 +889,8 @@ template <int K> struct Engine {
       for (int k = 1; k < p.m4; k++) {
         const bool last = (k == p.m4 - 1);
         F3R_TRY(mv(S.A.v16, Av, (const __half *)cur, EpiRichStep{hi, cur, M, w.rs, k, nxt, nullptr, isc},
-                   EpiRichStepK<K, MMF>{hi, cur, M, w.rs, k, nxt, last ? out_last : nullptr, isc}));
+                   EpiRichStepK<K, MMF>{hi, cur, M, w.rs, k, last && out16 ? out16 : nxt, last ? out_last : nullptr,
+                                        isc}));
         std::swap(cur, nxt);
       }
     } else {
@@ -901,7 +904,7 @@ template <int K> struct Engine {
         F3R_TRY(mv_store(S.A.v16, Av, (const __half *)w.tmp2, w.tmp));
         launch_k(C(), k_rich_weightK<8, K>, g, 256, 0, st, (const __half *)w.tmp, (const __half *)w.hr, N, gr, w.rs,
                  k);
-        F3R_TRY(axpy(k, 0, last ? out_last : nullptr, nullptr, isc));
+        F3R_TRY(axpy(k, 0, last ? out_last : nullptr, last ? out16 : nullptr, isc));
       }
     }
     (void)out;
@@ -919,7 +922,7 @@ template <int K> struct Engine {
       }
     }
     launch_k(C(), k_rich_axpyK<K>, g, kEwThreads, 0, C().stream, w.hout, (const __half *)w.tmp2,
-             (const RichState *)w.rs, k, use_ome, out, isc, (int64_t)n);
+             (const RichState *)w.rs, k, use_ome, out, isc, (int64_t)n, out16);
     return F3R_SUCCESS;
   }
 
@@ -1062,12 +1065,12 @@ template <int K> struct Engine {
         F3R_TRY(mv_store(S.A.v16, S.A.view(), (const float *)zj, Vp[j + 1]));
       }
       F3R_TRY(sstep_orthogonalise(L, Vp, V));
-    } else if (K == 1 && S.z16) {
-      if constexpr (K == 1) {
+    } else if (S.z16) {
+      {
         Cols<__half> Z16{};
-        for (int k = 0; k < L.m; k++) Z16.p[k] = w.Z16 + (size_t)k * ldn;
+        for (int k = 0; k < L.m; k++) Z16.p[k] = w.Z16 + (size_t)k * lk();
         for (int j = 0; j < L.m; j++) {
-          __half *zj = w.Z16 + (size_t)j * ldn;
+          __half *zj = w.Z16 + (size_t)j * lk();
           float *wv = Vp[j + 1];
           F3R_TRY(inner_apply(Vp[j], nullptr, j == 0 ? L.e : nullptr, es, j == 0 ? in_inv : L.inv, zj));
           F3R_TRY(mv_store(S.A.v16, S.A.view(), (const __half *)zj, wv));
@@ -1369,7 +1372,7 @@ template <int K> Status make_work(Solver &s, Work<K> &w) {
   F3R_TRY(w.alloc(&w.hin, nn));
   F3R_TRY(w.alloc(&w.hout, nn));
   F3R_TRY(w.alloc(&w.hout2, nn));
-  if (K == 1 && s.z16) F3R_TRY(w.alloc(&w.Z16, (size_t)s.ldn * p.m3));
+  if (s.z16) F3R_TRY(w.alloc(&w.Z16, (size_t)s.ldn * K * p.m3));
   F3R_TRY(w.alloc(&w.tmp, nn));
   F3R_TRY(w.alloc(&w.tmp2, nn));
   F3R_TRY(w.alloc(&w.hr, nn));
@@ -1936,6 +1939,7 @@ static Status make_batch(f3r_context *ctx, int32_t count, const f3r_csr *const *
   s->mm = true;
   s->mm_k = K;
   s->mm_count = count;
+  s->z16 = p.m3 > 0 && p.half_scale_log2 == 0 && !(p.inner_sstep & 2) && p.half_m == 0;
   const int32_t n = a0.nrows;
   const int all_types = (1 << F3R_F64) | (1 << F3R_F32) | (1 << F3R_F16);
   // the row order of sigma-sorting (row lengths are the pattern's: one order for all)
