@@ -231,18 +231,20 @@ def profiled_traffic(aligned=False, height=32):
 
 
 def spmv_roofline(solver, A, torch, F):
-    """Dominant kernel: the fp16-matrix SELL SpMV of level 3 (fp16 values,
-    fp32 x and y) on the solver's own matrix, timed with CUDA events on the
-    stream the library launches on.  `achieved` / `frac` use the
-    CSR-equivalent algorithmic bytes, nnz * (2 + 4) + 4 (n + 1) + 4 n + 4 n,
-    whatever the stored layout; the offset-aligned layout stores no column
-    index, so there they are an effective rate that can exceed the copy peak,
-    and `stored_*` give the rate over the bytes the layout actually holds
-    (padded values, slice-column bases, row pointers, x and y)."""
+    """Dominant kernel: the fp16-matrix SELL SpMV of level 3 on the solver's
+    own matrix, as the solve runs it (fp16 values, x from level 3's fp16 Z
+    basis, fp32 y; the Richardson step, the largest share, is the same
+    product with a fused epilogue), timed with CUDA events on the stream the
+    library launches on.  `achieved` / `frac` use the CSR-equivalent
+    algorithmic bytes, nnz * (2 + 4) + 4 (n + 1) + 2 n + 4 n, whatever the
+    stored layout; the offset-aligned layout stores no column index, so there
+    they are an effective rate that can exceed the copy peak, and `stored_*`
+    give the rate over the bytes the layout actually holds (padded values,
+    slice-column bases, row pointers, x and y)."""
     n, nnz = A.shape[0], A.nnz
     info, _ = solver.info()
-    x = torch.randn(n, dtype=torch.float32, device="cuda")
-    y = torch.empty_like(x)
+    x = torch.randn(n, dtype=torch.float32, device="cuda").to(torch.float16)
+    y = torch.empty(n, dtype=torch.float32, device="cuda")
     for _ in range(5):
         solver.operate(x, y, val_t=F.F16)
     torch.cuda.synchronize()
@@ -254,24 +256,25 @@ def spmv_roofline(solver, A, torch, F):
     e1.record(torch.cuda.current_stream())
     torch.cuda.synchronize()
     dt = e0.elapsed_time(e1) * 1e-3 / reps
-    alg = nnz * (2 + 4) + 4 * (n + 1) + n * 4 + n * 4
+    alg = nnz * (2 + 4) + 4 * (n + 1) + n * 2 + n * 4
     aligned = info.index_bits == 0
     csr = info.slice_height == 0
     h = info.slice_height or 32
     nslices = (n + h - 1) // h
     idx_bytes = (info.nnz_padded // h) * 4 if aligned else info.nnz_padded * 4
-    stored = alg if csr else info.nnz_padded * 2 + idx_bytes + 4 * (nslices + 1) + n * 4 + n * 4
+    stored = alg if csr else info.nnz_padded * 2 + idx_bytes + 4 * (nslices + 1) + n * 2 + n * 4
     peak, src = measured_peak()
     achieved = alg / dt / 1e9
     if csr:
-        kern = "k_csr_cfg<__half,float,EpiStore<float>,24> (CSR, fp16 A, fp32 x, fp32 y)"
+        kern = "k_csr_cfg<__half,__half,EpiStore<float>,24> (CSR, fp16 A, fp16 x, fp32 y)"
     elif h == 64:
-        kern = "k_sell64<__half,float,EpiStore<float>,32,1,32> (64-row offset-aligned slices, fp16 A, fp32 x, fp32 y)"
+        kern = "k_sell64<__half,__half,EpiStore<float>,32,1,32> (64-row offset-aligned slices, fp16 A, fp16 x, fp32 y)"
     elif aligned:
-        kern = ("k_sell_cfg<__half,float,EpiStore<float>,32,2,32,AllAlignedIdx> (SELL-32 sigma=1, offset-aligned, "
-                "fp16 A, fp32 x, fp32 y)")
+        kern = ("k_sell_cfg<__half,__half,EpiStore<float>,32,2,32,AllAlignedIdx> (SELL-32 sigma=1, offset-aligned, "
+                "fp16 A, fp16 x, fp32 y)")
     else:
-        kern = f"k_sell_cfg<__half,float,EpiStore<float>,24,2,16,int> (SELL-32 sigma={info.sigma}, fp16 A, fp32 x, fp32 y)"
+        kern = (f"k_sell_cfg<__half,__half,EpiStore<float>,24,2,16,int> (SELL-32 sigma={info.sigma}, fp16 A, fp16 x, "
+                "fp32 y)")
     return {"kernel": kern, "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "peak_source": src,
             "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None if csr else profiled_traffic(aligned, h),
             "algorithmic_bytes": alg, "effective_rate": aligned, "stored_bytes": stored,
