@@ -118,6 +118,19 @@ def test_block_solve_general_sdainv_and_uneven_convergence(layout):
     assert res[2].res_iter == 0 and res[0].res_iter > 0
 
 
+@pytest.mark.parametrize("scale", [0, 4])
+def test_block_solve_with_scaled_richardson_input(scale):
+    """with half_scale_log2 > 0 level 3 keeps an fp32 Z basis (R's output is
+    hout x 2^-k), without it an fp16 one; either way every block column is
+    its single solve bit for bit"""
+    ctx = F.Context(0)
+    A = F.stencil27(14, 13, 12, 2, 0.5).scale()
+    S = F.Solver(ctx, A, rel_tol=1e-10, c=4, half_scale_log2=scale)
+    B = np.ascontiguousarray(np.random.default_rng(5).standard_normal((6, A.shape[0])))
+    res = _check_block(S, B)
+    assert all(r.is_solved and r.expl_rel_res < 1e-10 for r in res)
+
+
 def test_block_solve_restarts_in_lockstep():
     """a short outer restart length: every column restarts (its x += Z y, then
     a new residual) in the same step as its single solve"""

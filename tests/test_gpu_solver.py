@@ -50,6 +50,22 @@ def test_solve_matches_oracle(ctx, nx, graphs, index16):
     assert np.linalg.norm(x - xs) / np.linalg.norm(xs) < 1e-7
 
 
+@pytest.mark.parametrize("scale", [3, 6])
+def test_scaled_richardson_input_matches_oracle(ctx, scale):
+    """half_scale_log2 = k scales R's fp16 input by 2^k and its output back by
+    2^-k, so level 3 keeps its Z basis in fp32 (R's output is no longer an
+    fp16 value): the solve converges as the oracle's with the same scaling"""
+    A, b, xs = system(20)
+    S = F.Solver(ctx, A, rel_tol=1e-10, half_scale_log2=scale)
+    x = np.zeros_like(b)
+    r = S.solve(b, x)
+    o = oracle_solve(A, b, tol=1e-10, half_scale_log2=scale)
+    assert r.is_solved and o["solved"]
+    assert r.expl_rel_res <= 1e-10
+    assert abs(r.res_iter - o["iters"]) <= 1
+    assert np.linalg.norm(x - xs) / np.linalg.norm(xs) < 1e-7
+
+
 def test_solve_matches_reference(ctx):
     ref = O.Ref("golden")
     A, b, _ = system(24, variant=1)
