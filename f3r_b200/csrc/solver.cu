@@ -539,12 +539,13 @@ template <int K> struct Work {
     allocs.push_back((void *)*q);
     return F3R_SUCCESS;
   }
-  template <typename T> Status make_level(Level<T> &L, int m, int64_t ldn, bool own_v0, bool bases = true) {
+  template <typename T>
+  Status make_level(Level<T> &L, int m, int64_t ldn, bool own_v0, bool bases = true, bool z_basis = true) {
     L.m = m;
     const size_t nn = (size_t)std::max<int64_t>(ldn, 8) * K;
     if (bases) {
       F3R_TRY(alloc(&L.V, nn * (size_t)(m + (own_v0 ? 1 : 0))));
-      F3R_TRY(alloc(&L.Z, nn * (size_t)m));
+      if (z_basis) F3R_TRY(alloc(&L.Z, nn * (size_t)m));
     }
     F3R_TRY(alloc(&L.H, (size_t)K * (m + 1) * m));
     F3R_TRY(alloc(&L.cs, (size_t)K * (m + 1)));
@@ -1055,7 +1056,8 @@ template <int K> struct Engine {
     Vp[0] = in;
     for (int k = 1; k <= L.m; k++) Vp[k] = L.V + (size_t)(k - 1) * lk();
     for (int k = 0; k <= L.m; k++) V.p[k] = Vp[k];
-    for (int k = 0; k < L.m; k++) Zc.p[k] = L.Z + (size_t)k * lk();
+    if (L.Z)  // fp32 basis (an fp16 one lives in Work::Z16)
+      for (int k = 0; k < L.m; k++) Zc.p[k] = L.Z + (size_t)k * lk();
     const int64_t es = L.m + 1;
     if ((p.inner_sstep & 2) && K == 1) {
       // sFGMRES (gmres2.hpp:176-180): W(j+1) = A16 R W(j) on the raw vectors
@@ -1350,7 +1352,7 @@ template <int K> Status make_work(Solver &s, Work<K> &w) {
   w.st = s.ctx->stream;
   F3R_TRY(w.make_level(w.L1, p.m_outer, s.ldn, true, false));
   if (p.m2 > 0) F3R_TRY(w.make_level(w.L2, p.m2, s.ldn, true));
-  if (p.m3 > 0) F3R_TRY(w.make_level(w.L3, p.m3, s.ldn, false));
+  if (p.m3 > 0) F3R_TRY(w.make_level(w.L3, p.m3, s.ldn, false, true, !s.z16));  // fp16 Z: Work::Z16
   if (K == 1 && p.half_m > 0) {
     HLevel &L = w.LH;
     const int m = p.half_m;
