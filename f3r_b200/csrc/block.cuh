@@ -22,6 +22,9 @@
 namespace f3r {
 
 constexpr int kMaxBlock = 16;  // widest block of right-hand sides
+// The single-column (K = 1) BLAS-1 kernels launch 8 blocks of 256 threads per
+// SM (Context::ew_grid) and declare so (__launch_bounds__(256, 8), at most 32
+// registers a thread), so that the whole grid is resident in one wave.
 
 // a VecN (an aggregate of at most 16 bytes) through the read-only path
 template <typename T, int N> __device__ __forceinline__ VecN<T, N> ldg_vec(const VecN<T, N> *p) {
@@ -706,7 +709,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_dotK(const T *__restrict__ x, co
 // level and inner fp32 levels with more than 8 basis vectors.  Column c's
 // values go to hcol + c * hstride.
 template <typename T, int WARPS, int K>
-__global__ void __launch_bounds__(WARPS * 32) k_multidot_chunkedK(const T *__restrict__ w, Cols<T> V, int nv,
+__global__ void __launch_bounds__(WARPS * 32, K == 1 ? 8 : 1) k_multidot_chunkedK(const T *__restrict__ w, Cols<T> V, int nv,
                                                                   int64_t n, GridRed gr, T *hcol, int64_t hstride) {
   constexpr int CH = K >= 8 ? 1 : 8 / K;  // basis vectors per pass over w
   constexpr int NQ = CH * K;
@@ -748,7 +751,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_multidot_chunkedK(const T *__res
 // H(j, k)(c) = <w(:, c), V(k)(:, c)> for nv <= MAXV basis vectors in fp32
 // (k_multidot_f32): rows in groups of 4 per thread, block-strided final stage
 template <int MAXV, int WARPS, int K>
-__global__ void __launch_bounds__(WARPS * 32) k_multidot_f32K(const float *__restrict__ w, Cols<float> V, int nv,
+__global__ void __launch_bounds__(WARPS * 32, K == 1 ? 8 : 1) k_multidot_f32K(const float *__restrict__ w, Cols<float> V, int nv,
                                                               int64_t n, GridRed gr, float *hcol, int64_t hstride) {
   constexpr int CV = (MAXV * K > 32) ? (32 / K > 0 ? 32 / K : 1) : MAXV;  // basis vectors per pass
   constexpr int NQ = CV * K;
@@ -1069,7 +1072,7 @@ __global__ void k_level2_enterK(double *const *__restrict__ in_slot, const doubl
 // x(:, c) = Z y_c (inner levels) or x(:, c) += Z y_c for the columns in mask
 // (outer level), the sum in the level's type T (k_zy)
 template <typename T, typename Out, bool ACCUM, int K, typename ZT = T>
-__global__ void k_zyK(Cols<ZT> Z, const T *__restrict__ y, int64_t y_stride, int nz, Out *out_direct,
+__global__ void __launch_bounds__(kEwThreads, K == 1 ? 8 : 1) k_zyK(Cols<ZT> Z, const T *__restrict__ y, int64_t y_stride, int nz, Out *out_direct,
                       Out *const *out_slot, uint32_t mask, int64_t n) {
   __shared__ T sy[K][kMaxCols];
   for (int t = threadIdx.x; t < nz * K; t += blockDim.x) {
@@ -1135,7 +1138,7 @@ __device__ __forceinline__ void rich_enter_rows(int64_t i0, float *__restrict__ 
 }
 
 template <bool SCALE_BY_OME, int K, bool MM = false>
-__global__ void k_rich_enter_diagK(float *__restrict__ in, const float *__restrict__ in_inv, float sc, DiagPre M,
+__global__ void __launch_bounds__(kEwThreads, K == 1 ? 8 : 1) k_rich_enter_diagK(float *__restrict__ in, const float *__restrict__ in_inv, float sc, DiagPre M,
                                    __half *__restrict__ hin, __half *__restrict__ hout,
                                    const RichState *__restrict__ rs, float *e_set, int64_t e_stride, int64_t n) {
   if (e_set && blockIdx.x == 0 && threadIdx.x < K) e_set[threadIdx.x * e_stride] = 1.0f;
