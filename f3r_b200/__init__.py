@@ -373,6 +373,15 @@ class Solver:
         check(lib().f3r_solver_info(self._h, C.byref(i), C.byref(d)))
         return i, bool(d.value)
 
+    @property
+    def unit_diagonal(self) -> bool:
+        """True when the diagonal SDAINV factors are 1 in fp16 and the
+        Richardson kernels take the constant instead of loading them"""
+        i = _capi.SellInfo()
+        d = C.c_int32()
+        check(lib().f3r_solver_info(self._h, C.byref(i), C.byref(d)))
+        return d.value == 2
+
     def operate(self, x, y, val_t=None) -> None:
         """y = A x with the solver's own device matrix (storage order P A P^T)."""
         xt, yt = _torch_dt(x), _torch_dt(y)
@@ -437,6 +446,14 @@ class Batch:
         c, k, d = C.c_int32(), C.c_int32(), C.c_int32()
         check(lib().f3r_batch_info(self._h, C.byref(c), C.byref(k), C.byref(d)))
         return c.value, k.value, bool(d.value)
+
+    @property
+    def unit_diagonal(self) -> bool:
+        """True when every system's diagonal SDAINV factors are 1 in fp16
+        (the Richardson kernels take the constant)"""
+        c, k, d = C.c_int32(), C.c_int32(), C.c_int32()
+        check(lib().f3r_batch_info(self._h, C.byref(c), C.byref(k), C.byref(d)))
+        return d.value == 2
 
     def solve(self, bs, xs, cond: Optional[Callable[[int, float], bool]] = None):
         """Solve system i for bs[i] into xs[i] (numpy float64 or torch CUDA

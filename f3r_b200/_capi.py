@@ -43,7 +43,7 @@ class Params(C.Structure):
                 ("sell_index16", C.c_int32), ("static_weight", C.c_double), ("trsv_iters", C.c_int32),
                 ("format", C.c_int32), ("trsv_omega", C.c_double), ("inner_sstep", C.c_int32),
                 ("sell_align", C.c_int32), ("sell_autotune", C.c_int32), ("half_m", C.c_int32),
-                ("reserved", C.c_int32 * 6)]
+                ("diag_load", C.c_int32), ("reserved", C.c_int32 * 5)]
 
 
 class Result(C.Structure):

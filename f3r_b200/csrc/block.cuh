@@ -143,6 +143,17 @@ template <typename T, int K> struct RowK {
   }
 };
 
+// N diagonal preconditioner values from p, or N ones where the diagonal is
+// the identity in fp16 (DiagPre with null pointers: nothing is loaded)
+template <int N, typename Acc> __device__ __forceinline__ void diag_load(const __half *p, Acc (&o)[N]) {
+  if (p) {
+    RowK<__half, N>::load(p, o);
+  } else {
+#pragma unroll
+    for (int q = 0; q < N; q++) o[q] = Acc(1.0f);
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Block SELL product: out(:, c) = A x(:, c) for c < K, one pass over A.
 // Same layouts and bulk-copy ring as k_sell_cfg (sell.cuh); the index forms
@@ -551,8 +562,8 @@ template <int K, bool MM = false> struct EpiRichStepK {
     __half w[MM ? K : 1], z[MM ? K : 1];
     RowK<__half, K>::load(hin + r * K, hi);
     RowK<__half, K>::load(hout + r * K, ho);
-    RowK<__half, MM ? K : 1>::load(M.w + r * (MM ? K : 1), w);
-    RowK<__half, MM ? K : 1>::load(M.z + r * (MM ? K : 1), z);
+    diag_load<MM ? K : 1>(M.w ? M.w + r * (MM ? K : 1) : nullptr, w);
+    diag_load<MM ? K : 1>(M.z ? M.z + r * (MM ? K : 1) : nullptr, z);
 #pragma unroll
     for (int c = 0; c < K; c++) {
       const __half hr = f2h(hi[c] - (float)acc[c]);
@@ -577,8 +588,8 @@ template <int K, bool MM = false> struct EpiRichResPreK {
   template <typename Acc> __device__ __forceinline__ void row(int64_t r, const Acc (&acc)[K]) const {
     float hi[K], h[K], t[K], w[MM ? K : 1], z[MM ? K : 1];
     RowK<__half, K>::load(hin + r * K, hi);
-    RowK<__half, MM ? K : 1>::load(M.w + r * (MM ? K : 1), w);
-    RowK<__half, MM ? K : 1>::load(M.z + r * (MM ? K : 1), z);
+    diag_load<MM ? K : 1>(M.w ? M.w + r * (MM ? K : 1) : nullptr, w);
+    diag_load<MM ? K : 1>(M.z ? M.z + r * (MM ? K : 1) : nullptr, z);
 #pragma unroll
     for (int c = 0; c < K; c++) {
       h[c] = h2f(f2h(hi[c] - (float)acc[c]));
@@ -1123,8 +1134,8 @@ __device__ __forceinline__ void rich_enter_rows(int64_t i0, float *__restrict__ 
     for (int q = 0; q < E; q++) v[q] *= s[q % K];
     RowK<float, E>::store(in + i0 * K, v);
   }
-  RowK<__half, NM>::load(M.w + i0 * (MM ? K : 1), w);
-  RowK<__half, NM>::load(M.z + i0 * (MM ? K : 1), z);
+  diag_load<NM>(M.w ? M.w + i0 * (MM ? K : 1) : nullptr, w);
+  diag_load<NM>(M.z ? M.z + i0 * (MM ? K : 1) : nullptr, z);
 #pragma unroll
   for (int q = 0; q < E; q++) {
     hi[q] = f2h(v[q] * sc);

@@ -576,6 +576,23 @@ struct Solver {
   // preconditioner
   int precond_diag = 0;
   __half *wd = nullptr, *zd = nullptr;
+  // every fp16 value of wd and zd is exactly 1: the kernels take the constant
+  // (DiagPre with null pointers) and the two diagonals are not read
+  bool diag_unit = false;
+  DiagPre diag() const { return diag_unit ? DiagPre{nullptr, nullptr} : DiagPre{wd, zd}; }
+  // set diag_unit from the fp16 values as stored (unless p.diag_load asks to
+  // load them always); nn values each
+  Status detect_unit_diag(size_t nn) {
+    diag_unit = false;
+    if (p.diag_load || nn == 0) return F3R_SUCCESS;
+    std::vector<uint16_t> hw(nn), hz(nn);
+    CUDA_TRY(cudaMemcpy(hw.data(), wd, nn * sizeof(uint16_t), cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(hz.data(), zd, nn * sizeof(uint16_t), cudaMemcpyDeviceToHost));
+    bool unit = true;
+    for (size_t i = 0; i < nn && unit; i++) unit = hw[i] == 0x3C00u && hz[i] == 0x3C00u;
+    diag_unit = unit;
+    return F3R_SUCCESS;
+  }
   DeviceSell W, Z;    // general SDAINV factors (permuted system)
   IluDevice ilu;      // block-Jacobi ILU(0), level scheduled
   IluLevel ilul;      // global ILU(0), level scheduled over the whole GPU
@@ -800,7 +817,7 @@ template <int K> struct Engine {
           F3R_TRY(rich_diag<false>(in, out, e_set, e_stride, in_inv, upd, sc, isc, hi, h0, out_last, out16));
         }
       } else {
-        const DiagPre M{S.wd, S.zd};
+        const DiagPre M = S.diag();
         if (h16) {
           if (!upd)
             launch_k(C(), k_rich_enter_diag<true, __half>, C().ew_grid(cdiv(N, 4)), kEwThreads, 0, st, in16, in_inv,
@@ -876,7 +893,7 @@ template <int K> struct Engine {
     const int64_t N = n;
     const int g = C().ew_grid(N);
     cudaStream_t st = C().stream;
-    const DiagPre M{S.wd, S.zd};
+    const DiagPre M = S.diag();
     const DevSell Av = S.A.view();
     const GridRed gr = w.gr;
     if (!upd)
@@ -1671,6 +1688,7 @@ static Status make_solver(f3r_context *ctx, const f3r_csr *a, const f3r_params *
     return fail(F3R_ERROR_INVALID_VALUE, "unknown preconditioner");
   if (p.half_scale_log2 < 0 || p.half_scale_log2 > 20) return fail(F3R_ERROR_INVALID_VALUE, "half_scale_log2 in [0, 20]");
   if (p.inner_sstep < 0 || p.inner_sstep > 3) return fail(F3R_ERROR_INVALID_VALUE, "inner_sstep is a 2-bit mask");
+  if (p.diag_load != 0 && p.diag_load != 1) return fail(F3R_ERROR_INVALID_VALUE, "diag_load is 0 or 1");
   if (p.sell_autotune) {
     CUDA_TRY(cudaSetDevice(ctx->device));
     F3R_TRY(autotune_layout(ctx, a, p));
@@ -1753,6 +1771,7 @@ static Status make_solver(f3r_context *ctx, const f3r_csr *a, const f3r_params *
       launch_k(*ctx, k_convert_vals<__half>, ctx->ew_grid(n), kEwThreads, 0, ctx->stream, tmp, s->zd, n);
       CUDA_TRY(cudaStreamSynchronize(ctx->stream));
       cudaFree(tmp);
+      F3R_TRY(s->detect_unit_diag((size_t)n));
     } else {
       // W^T and Z as SELL matrices of the permuted system (same sigma order), or CSR
       SellHost hw, hz;
@@ -1928,6 +1947,7 @@ static Status make_batch(f3r_context *ctx, int32_t count, const f3r_csr *const *
       p.m4 < 1 || p.m4 > kMaxM4 || p.c < 1 || p.max_restarts < 1 || p.static_weight < 0 || p.sell_sigma < 1)
     return fail(F3R_ERROR_INVALID_VALUE, "need 1 <= m_outer, m2 <= 127, 0 <= m3 <= 127, 1 <= m4 <= 16, c >= 1");
   if (p.half_scale_log2 < 0 || p.half_scale_log2 > 20) return fail(F3R_ERROR_INVALID_VALUE, "half_scale_log2 in [0, 20]");
+  if (p.diag_load != 0 && p.diag_load != 1) return fail(F3R_ERROR_INVALID_VALUE, "diag_load is 0 or 1");
   p.sell_align = 0;  // packed layout with per-column values
   p.sell_index16 = 0;
   p.sell_autotune = 0;
@@ -2015,6 +2035,7 @@ static Status make_batch(f3r_context *ctx, int32_t count, const f3r_csr *const *
              (int64_t)nn);
     CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     cudaFree(tmp);
+    F3R_TRY(s->detect_unit_diag(nn));
   } else {
     // W^T and Z of every system on the union of their patterns, rows in the storage order
     for (int which = 0; which < 2; which++) {
@@ -2477,7 +2498,7 @@ f3r_status f3r_solver_info(const f3r_solver *s, f3r_sell_info *a_info, int32_t *
     a_info->dtypes = d.dtypes;
     a_info->index_bits = d.index_bits();
   }
-  if (precond_diagonal) *precond_diagonal = s->s->precond_diag;
+  if (precond_diagonal) *precond_diagonal = s->s->precond_diag ? (s->s->diag_unit ? 2 : 1) : 0;
   return F3R_SUCCESS;
 }
 f3r_status f3r_solver_operate(f3r_solver *s, f3r_dtype val_t, f3r_dtype in_t, const void *in, f3r_dtype out_t,
@@ -2524,7 +2545,7 @@ f3r_status f3r_batch_info(const f3r_batch *bt, int32_t *count, int32_t *width, i
   if (!s) return fail(F3R_ERROR_INVALID_VALUE, "null batch");
   if (count) *count = s->s->mm_count;
   if (width) *width = s->s->mm_k;
-  if (precond_diagonal) *precond_diagonal = s->s->precond_diag;
+  if (precond_diagonal) *precond_diagonal = s->s->precond_diag ? (s->s->diag_unit ? 2 : 1) : 0;
   return F3R_SUCCESS;
 }
 void f3r_batch_destroy(f3r_batch *bt) { f3r_solver_destroy(reinterpret_cast<f3r_solver *>(bt)); }

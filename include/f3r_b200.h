@@ -130,7 +130,12 @@ typedef struct f3r_params {
                               fp16), R's input and output its fp16 vectors.  The paper's F4 is m2 8,
                               m3 4, half_m 2; F3H m2 8, m3 0, half_m 8; F2H m2 0, half_m 64; each with
                               m4 1, static_weight 1 and block-Jacobi ILU(0).  0 */
-  int32_t reserved[6];
+  int32_t diag_load;       /* diagonal SDAINV factors (W^T and Z both diagonal): where every fp16
+                              value of both is exactly 1 (what tol 0.1 leaves of a diagonally
+                              scaled stencil), the Richardson kernels multiply by the constant 1
+                              instead of loading it -- the same arithmetic, 4 bytes a row fewer.
+                              1: load the factors always.  0 */
+  int32_t reserved[5];
 } f3r_params;
 
 /* Solve outcome.  The first three fields are solve_res_t
@@ -374,6 +379,9 @@ f3r_status f3r_solver_create(f3r_context *ctx, const f3r_csr *a, const f3r_param
  * models.hpp:207-211). */
 f3r_status f3r_solver_solve(f3r_solver *s, const double *b, double *x, f3r_cond_fn cond,
                             void *user, f3r_result *result);
+/* a_info: the stored matrix; precond_diagonal: 0 for general factors, 1 when
+ * W^T and Z are both diagonal, 2 when moreover every fp16 value of both is
+ * exactly 1 and the Richardson kernels take the constant (diag_load = 0) */
 f3r_status f3r_solver_info(const f3r_solver *s, f3r_sell_info *a_info, int32_t *precond_diagonal);
 /* Several right-hand sides: column k of B (b + k * ldb) is solved into
  * column k of X (x + k * ldx), x holding the initial guesses; ldb, ldx >= n;
@@ -442,7 +450,8 @@ f3r_status f3r_batch_create(f3r_context *ctx, int32_t count, const f3r_csr *cons
 f3r_status f3r_batch_solve(f3r_batch *b, const double *const *bv, double *const *x, f3r_cond_fn cond, void *user,
                            f3r_result *results);
 /* count: systems; width: the block's K; precond_diagonal: 1 when every
- * system's SDAINV factors are diagonal */
+ * system's SDAINV factors are diagonal, 2 when moreover all their fp16 values
+ * (padding columns of a partial block included) are exactly 1 */
 f3r_status f3r_batch_info(const f3r_batch *b, int32_t *count, int32_t *width, int32_t *precond_diagonal);
 void f3r_batch_destroy(f3r_batch *b);
 

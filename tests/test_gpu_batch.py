@@ -225,3 +225,39 @@ def test_batch_with_given_factors_and_rejections():
         F.Batch(ctx, _fields("stencil", 17, nx=6))
     with pytest.raises(F.F3RError):
         F.Batch(ctx, systems, precond=F.PRECOND_ILU0_BJ, ilu_blocks=4)
+
+
+@pytest.mark.parametrize("layout", ["aligned64", "packed"])
+def test_block_solve_unit_diagonal_is_identical(layout):
+    """the lockstep block solve (4 right-hand sides) and a full batch of 4
+    stencil systems with unit fp16 diagonal factors: taking the constant gives
+    the iterates of the solves that load the factors, bit for bit"""
+    ctx = F.Context(0)
+    kw = dict(sell_c=64) if layout == "aligned64" else dict(sell_align=0)
+    A = F.stencil27(16, 15, 14, 2, 0.5).scale()
+    n = A.shape[0]
+    rng = np.random.default_rng(21)
+    B = np.ascontiguousarray(rng.standard_normal((4, n)))
+    outs = []
+    for load in (0, 1):
+        S = F.Solver(ctx, A, rel_tol=1e-10, c=4, diag_load=load, **kw)
+        assert S.unit_diagonal == (load == 0)
+        X = np.zeros_like(B)
+        res = S.solve_multi(B, X)
+        assert all(r.is_solved for r in res)
+        outs.append((X, [r.res_iter for r in res]))
+        S.close()
+    assert outs[0][1] == outs[1][1] and np.array_equal(outs[0][0], outs[1][0])
+    systems = _fields("stencil", 4)
+    bs = [rng.standard_normal(systems[0].shape[0]) for _ in range(4)]
+    got = []
+    for load in (0, 1):
+        Bt = F.Batch(ctx, systems, rel_tol=1e-10, c=4, diag_load=load)
+        assert Bt.unit_diagonal == (load == 0)
+        xs = [np.zeros_like(b) for b in bs]
+        res = Bt.solve(bs, xs)
+        assert all(r.is_solved for r in res)
+        got.append(xs)
+        Bt.close()
+    for i in range(4):
+        assert np.array_equal(got[0][i], got[1][i]), i

@@ -249,3 +249,42 @@ def test_slice_height_64_solve_is_identical(ctx, dims):
     assert np.array_equal(xs[0], xs[1])
     with pytest.raises(F.F3RError):
         F.Solver(ctx, A, sell_c=64, sell_sigma=256)
+
+
+@pytest.mark.parametrize("kw", [dict(c=4), dict(sell_c=64, c=4), dict(m4=3, c=2), dict(sell_sigma=256, c=8)])
+def test_unit_diagonal_solve_is_identical(ctx, kw):
+    """the scaled stencil's SDAINV factors are diagonal and 1 in fp16: the
+    Richardson kernels then take the constant 1 instead of loading it, and the
+    solve is the one that loads the factors (diag_load = 1) bit for bit --
+    plain steps, weight updates (c small), three Richardson steps, 64-row
+    slices and sigma-sorted rows"""
+    A = F.stencil27(20, 18, 16, 2, 0.5).scale()
+    b = A.spmv(F.random_uniform(11, -1, 1, A.shape[0]))
+    xs, its = [], []
+    for load in (0, 1):
+        S = F.Solver(ctx, A, rel_tol=1e-10, diag_load=load, **kw)
+        assert S.info()[1] and S.unit_diagonal == (load == 0)
+        x = np.zeros(len(b))
+        r = S.solve(b, x)
+        assert r.is_solved and r.expl_rel_res < 1e-10
+        xs.append(x)
+        its.append(r.res_iter)
+        S.close()
+    assert its[0] == its[1] and np.array_equal(xs[0], xs[1])
+
+
+def test_non_unit_diagonal_loads_factors(ctx):
+    """diagonal factors that are not all 1 in fp16 (an unscaled stencil) keep
+    the loads; diag_load takes 0 or 1 only"""
+    A = F.stencil27(12, 12, 12, 2, 0.5)
+    S = F.Solver(ctx, A, rel_tol=1e-10, c=8)
+    info, diag = S.info()
+    if diag:
+        assert not S.unit_diagonal
+    b = A.spmv(F.random_uniform(4, -1, 1, A.shape[0]))
+    x = np.zeros(len(b))
+    r = S.solve(b, x)
+    assert r.is_solved and r.expl_rel_res < 1e-10
+    S.close()
+    with pytest.raises(F.F3RError):
+        F.Solver(ctx, A, diag_load=2)
