@@ -673,18 +673,37 @@ __device__ __forceinline__ bool last_block(unsigned int *ticket) {
   return last;
 }
 
-// final stage, block-strided: value q of ntot -> returned on thread 0
-template <typename T, int WARPS> __device__ __forceinline__ T final_block_strided(const T *part, int q, int ntot) {
-  __shared__ T sw[WARPS];
+// final stage, block-strided, for nq <= QB values at once (q0 .. q0 + nq - 1
+// of ntot partials per block): value q is summed by thread t over the
+// partials of blocks t, t + blockDim.x, ... in that order, then by the warp
+// butterfly, then over warps 0 .. WARPS-1 in order -- a fixed order for every
+// column count and launch, so that the K-column kernels' sums are the single
+// column's.  The values' loads and reductions overlap instead of running one
+// value after another.  Value q0 + i is returned on thread i (i < nq).
+template <typename T, int WARPS, int QB>
+__device__ __forceinline__ T final_block_multi(const T *part, int q0, int nq, int ntot) {
+  __shared__ T sw[WARPS][QB];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  T s = 0;
-  for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) s += __ldcg(&part[(size_t)b * ntot + q]);
-  s = warp_sum(s);
-  if (lane == 0) sw[warp] = s;
+  T s[QB];
+#pragma unroll
+  for (int i = 0; i < QB; i++) s[i] = 0;
+  for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) {
+    const T *pb = part + (size_t)b * ntot + q0;
+#pragma unroll
+    for (int i = 0; i < QB; i++)
+      if (i < nq) s[i] += __ldcg(pb + i);
+  }
+#pragma unroll
+  for (int i = 0; i < QB; i++) {
+    if (i < nq) {
+      s[i] = warp_sum(s[i]);
+      if (lane == 0) sw[warp][i] = s[i];
+    }
+  }
   __syncthreads();
   T t = 0;
-  if (threadIdx.x == 0)
-    for (int w = 0; w < WARPS; w++) t += sw[w];
+  if ((int)threadIdx.x < nq)
+    for (int w = 0; w < WARPS; w++) t += sw[w][threadIdx.x];
   __syncthreads();
   return t;
 }
@@ -708,10 +727,8 @@ __global__ void __launch_bounds__(WARPS * 32) k_dotK(const T *__restrict__ x, co
   Acc *part = static_cast<Acc *>(gr.partials);
   block_partials<Acc, K, WARPS>(a, K, 0, K, part, sred);
   if (!last_block(gr.ticket)) return;
-  for (int c = 0; c < K; c++) {
-    const Acc t = final_block_strided<Acc, WARPS>(part, c, K);
-    if (threadIdx.x == 0) out[c] = t;
-  }
+  const Acc t = final_block_multi<Acc, WARPS, K>(part, 0, K, K);
+  if ((int)threadIdx.x < K) out[threadIdx.x] = t;
   if (threadIdx.x == 0) *gr.ticket = 0;
 }
 
@@ -811,9 +828,12 @@ __global__ void __launch_bounds__(WARPS * 32, K == 1 ? 8 : 1) k_multidot_f32K(co
     block_partials<float, NQ, WARPS>(a, nq, k0 * K, ntot, part, sred);
   }
   if (!last_block(gr.ticket)) return;
-  for (int q = 0; q < ntot; q++) {
-    const float t = final_block_strided<float, WARPS>(part, q, ntot);
-    if (threadIdx.x == 0) hcol[(q % K) * hstride + q / K] = t;
+  constexpr int QB = NQ < 16 ? NQ : 16;
+  for (int q0 = 0; q0 < ntot; q0 += QB) {
+    const int nq = min(QB, ntot - q0);
+    const float t = final_block_multi<float, WARPS, QB>(part, q0, nq, ntot);
+    const int q = q0 + (int)threadIdx.x;
+    if ((int)threadIdx.x < nq) hcol[(q % K) * hstride + q / K] = t;
   }
   if (threadIdx.x == 0) *gr.ticket = 0;
 }
@@ -953,10 +973,10 @@ __global__ void __launch_bounds__(WARPS * 32, K > 1 ? 1 : 8) k_cgs_updateK(T *__
   block_partials<T, K, WARPS>(part, K, 0, K, parts, sred);
   if (!last_block(gr.ticket)) return;
   const uint32_t act = *active;
-  for (int c = 0; c < K; c++) {
-    const T t = final_block_strided<T, WARPS>(parts, c, K);
-    if (threadIdx.x == 0 && ((act >> c) & 1u)) givens_step<T>(L.col(c, j, compute_y, abs_e ? abs_e + c : nullptr, err), t);
-  }
+  // column c's norm and Givens step on thread c (each column's state is its own)
+  const T t = final_block_multi<T, WARPS, K>(parts, 0, K, K);
+  const int c = threadIdx.x;
+  if (c < K && ((act >> c) & 1u)) givens_step<T>(L.col(c, j, compute_y, abs_e ? abs_e + c : nullptr, err), t);
   if (threadIdx.x == 0) *gr.ticket = 0;
 }
 
@@ -981,14 +1001,13 @@ __global__ void __launch_bounds__(WARPS * 32) k_resnormK(const double *__restric
   block_partials<double, K, WARPS>(part, K, 0, K, parts, sred);
   if (!last_block(gr.ticket)) return;
   const uint32_t act = *active;
-  for (int c = 0; c < K; c++) {
-    const double t = final_block_strided<double, WARPS>(parts, c, K);
-    if (threadIdx.x == 0 && ((act >> c) & 1u)) {
-      const double h = sqrt(t);
-      L.e[c * L.vs] = h;
-      L.inv[c] = 1.0 / h;
-      abs_e[c] = fabs(h);
-    }
+  const double t = final_block_multi<double, WARPS, K>(parts, 0, K, K);
+  const int c = threadIdx.x;
+  if (c < K && ((act >> c) & 1u)) {
+    const double h = sqrt(t);
+    L.e[c * L.vs] = h;
+    L.inv[c] = 1.0 / h;
+    abs_e[c] = fabs(h);
   }
   if (threadIdx.x == 0) *gr.ticket = 0;
 }
@@ -1020,10 +1039,15 @@ __global__ void __launch_bounds__(WARPS * 32) k_rich_weightK(const __half *__res
   float *parts = static_cast<float *>(gr.partials);
   block_partials<float, 2 * K, WARPS>(d, 2 * K, 0, 2 * K, parts, sred);
   if (!last_block(gr.ticket)) return;
-  for (int c = 0; c < K; c++) {
-    const float tt = final_block_strided<float, WARPS>(parts, c, 2 * K);
-    const float to = final_block_strided<float, WARPS>(parts, K + c, 2 * K);
-    if (threadIdx.x == 0) {
+  // <t, t> of column c on thread c, <t, o> on thread K + c
+  __shared__ float sto[K];
+  const float v = final_block_multi<float, WARPS, 2 * K>(parts, 0, 2 * K, 2 * K);
+  if ((int)threadIdx.x >= K && (int)threadIdx.x < 2 * K) sto[threadIdx.x - K] = v;
+  __syncthreads();
+  {
+    const int c = threadIdx.x;
+    if (c < K) {
+      const float tt = v, to = sto[c];
       RichState *s = rs + c;
       const float om = to / tt;
       s->om[k] = om;
