@@ -196,6 +196,7 @@ template <typename V, int K> constexpr size_t block_mm_smem_bytes() {
 template <typename V, typename X, typename Epi, int K, int WARPS, int STAGES, int KC, typename CI, bool MM = false>
 __global__ void __launch_bounds__(WARPS * 32, 1)
     k_sell_block(const V *__restrict__ val, DevSell A, const X *__restrict__ x, Epi epi, int *err) {
+  epi_setup(epi, 0);
   using Acc = typename acc_of<V>::type;
   constexpr int MODE = IdxForm<CI>::mode;
   static_assert(MODE == 0 || MODE == 2 || MODE == 3, "block product: packed int32 or offset-aligned slices");
@@ -381,6 +382,7 @@ template <typename V, int K> constexpr size_t block64_smem_bytes() {
 template <typename V, typename X, typename Epi, int K, int WARPS, int STAGES>
 __global__ void __launch_bounds__(WARPS * 32, 1)
     k_sell_block64(const V *__restrict__ val, DevSell A, const X *__restrict__ x, Epi epi, int *err) {
+  epi_setup(epi, 0);
   using Acc = typename acc_of<V>::type;
   constexpr int KC = kAllAlignedChunk;
   constexpr uint32_t VB = KC * 64 * sizeof(V), BB = KC * 4, SB = VB + BB;
@@ -545,7 +547,8 @@ template <typename B, typename Out, int K> struct EpiResidualK {
 };
 
 // Richardson step without a weight update, diagonal preconditioner fused
-// (EpiRichStepT, kernels.cuh, per column with the column's own weight):
+// (EpiRichStepT, kernels.cuh, per column with the column's own weight, read
+// once per thread by setup()):
 // hr = fp16(hin - A hout); t2 = z (w hr); hnew = fp16(hout + ome_c[k] t2); the
 // last step writes out = fp32(hnew) / sc instead.
 // MM: the diagonal preconditioner has one value per row and column, w[r * K + c]
@@ -557,6 +560,11 @@ template <int K, bool MM = false> struct EpiRichStepK {
   __half *hnext;
   float *out;
   float isc;
+  float ome[K] = {};  // fp32(ome_c[k]) of every column, set by setup()
+  __device__ __forceinline__ void setup() {
+#pragma unroll
+    for (int c = 0; c < K; c++) ome[c] = h2f(rs[c].ome[k]);
+  }
   template <typename Acc> __device__ __forceinline__ void row(int64_t r, const Acc (&acc)[K]) const {
     float hi[K], ho[K], res[K];
     __half w[MM ? K : 1], z[MM ? K : 1];
@@ -568,7 +576,7 @@ template <int K, bool MM = false> struct EpiRichStepK {
     for (int c = 0; c < K; c++) {
       const __half hr = f2h(hi[c] - (float)acc[c]);
       const __half t2 = __hmul(z[MM ? c : 0], __hmul(w[MM ? c : 0], hr));
-      res[c] = h2f(f2h(__fmaf_rn(h2f(rs[c].ome[k]), h2f(t2), ho[c])));
+      res[c] = h2f(f2h(__fmaf_rn(ome[c], h2f(t2), ho[c])));
     }
     if (out) {
 #pragma unroll

@@ -41,6 +41,7 @@ template <int N> __device__ __forceinline__ void cp_async_wait() {
 template <typename V, typename X, typename Epi, int WARPS>
 __global__ void __launch_bounds__(WARPS * 32, 1)
     k_csr_cfg(const V *__restrict__ val, DevSell A, const X *__restrict__ x, Epi epi, int *) {
+  epi_setup(epi, 0);
   using Acc = typename acc_of<V>::type;
   constexpr uint32_t VS = csr_vstage<V>(), IS = csr_istage();
   extern __shared__ __align__(16) unsigned char smem[];

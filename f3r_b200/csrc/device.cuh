@@ -143,6 +143,13 @@ __device__ __forceinline__ double fmaT(double a, double b, double c) { return __
 // mixed-precision FMA (fp16 sources, fp32 addend and result): the product of
 // two fp16 values is exact in fp32, so this is fmaf(float(v), float(x), acc)
 // bit for bit, without the two conversions.
+// Per-launch set-up of a product epilogue: an epilogue with a setup() method
+// reads its loop-invariant device values there, once per thread, instead of
+// once per row; the others have nothing to do.  Every kernel that takes an
+// epilogue calls this first.
+template <typename E> __device__ __forceinline__ auto epi_setup(E &e, int) -> decltype(e.setup(), void()) { e.setup(); }
+template <typename E> __device__ __forceinline__ void epi_setup(E &, long) {}
+
 template <typename Acc, typename V, typename X> __device__ __forceinline__ Acc fma_vx(V v, X x, Acc acc) {
   return fmaT(to_acc<Acc>(v), to_acc<Acc>(x), acc);
 }

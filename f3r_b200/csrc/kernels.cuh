@@ -529,13 +529,22 @@ __global__ void k_rich_cast_in(In *__restrict__ in, const float *__restrict__ in
 
 // Residual step of R with the diagonal preconditioner fused (no weight
 // update): hr = fp16(hin - A16 hout); t2 = M hr; hnew = fp16(hout + ome[k] t2);
-// the last step writes out = fp32(hnew) / sc (out.copy(hout)).
-template <bool PREFETCH = true> struct EpiRichStepT {
+// the last step writes out = fp32(hnew) / sc (out.copy(hout)).  ome[k] is read
+// once per thread (setup).  UNIT: both diagonal factors are 1 in fp16, so
+// t2 = 1 * (1 * hr) = hr exactly (an fp16 multiply by one returns its operand,
+// a NaN as the canonical NaN the update then produces anyway); the row's own
+// operands are hin and hout only, held as one half2 through the chain.
+template <bool PREFETCH = true, bool UNIT = false> struct EpiRichStepT {
   using Red = float;
   static constexpr int NV = 0;
-  struct Pre {
-    __half hin, hout, w, z, ome;
+  struct PreUnit {
+    __half2 io;  // hin, hout
   };
+  struct PreDiag {
+    __half2 io;
+    __half w, z;
+  };
+  using Pre = typename std::conditional<UNIT, PreUnit, PreDiag>::type;
   const __half *hin, *hout;
   DiagPre M;
   const RichState *rs;
@@ -543,26 +552,38 @@ template <bool PREFETCH = true> struct EpiRichStepT {
   __half *hnext;  // next hout (steps before the last)
   float *out;     // fp32 result (last step)
   float isc;
+  float ome = 0.0f;  // fp32(ome[k]), set by setup()
+  __device__ __forceinline__ void setup() { ome = h2f(rs->ome[k]); }
+  __device__ __forceinline__ void fetch(int64_t r, Pre &p) const {
+    p.io = __halves2half2(hin[r], hout[r]);
+    if constexpr (!UNIT) {
+      p.w = M.wv(r);
+      p.z = M.zv(r);
+    }
+  }
   __device__ __forceinline__ Pre load(int64_t r) const {
-    if (PREFETCH) return {hin[r], hout[r], M.wv(r), M.zv(r), rs->ome[k]};
-    return {};
+    Pre p{};
+    if (PREFETCH) fetch(r, p);
+    return p;
   }
   template <typename Acc> __device__ __forceinline__ void row(int64_t r, Acc acc, const Pre &pp, Red (&)[1]) const {
-    const Pre p = PREFETCH ? pp : Pre{hin[r], hout[r], M.wv(r), M.zv(r), rs->ome[k]};
+    Pre p = pp;
+    if (!PREFETCH) fetch(r, p);
     // The product of two fp16 values is exact in fp32, so the fp16 multiply
     // (one correctly rounded result) gives the bits of fp16(float(a) * float(b))
     // in one instruction; the subtraction (fp32 acc) and the fused update keep
     // their fp32 arithmetic.
-    const __half hr = f2h(h2f(p.hin) - (float)acc);
-    const __half t = __hmul(p.w, hr);
-    const __half t2 = __hmul(p.z, t);
-    const float hn = h2f(f2h(__fmaf_rn(h2f(p.ome), h2f(t2), h2f(p.hout))));
+    const __half hr = f2h(h2f(__low2half(p.io)) - (float)acc);
+    __half t2 = hr;
+    if constexpr (!UNIT) t2 = __hmul(p.z, __hmul(p.w, hr));
+    const float hn = h2f(f2h(__fmaf_rn(ome, h2f(t2), h2f(__high2half(p.io)))));
     if (out) out[r] = hn * isc;
     else hnext[r] = f2h(hn);
   }
   template <int W> __device__ __forceinline__ void finish(Red (&)[1]) const {}
 };
 using EpiRichStep = EpiRichStepT<true>;
+using EpiRichStepUnit = EpiRichStepT<true, true>;
 
 // Residual step of an update call (diagonal M): stores hr and t2 = M hr.
 struct EpiRichResPre {

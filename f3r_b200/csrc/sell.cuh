@@ -147,6 +147,7 @@ constexpr size_t sell_smem_bytes() {
 template <typename V, typename X, typename Epi, int WARPS, int STAGES, int KC, typename CI = int32_t>
 __global__ void __launch_bounds__(WARPS * 32, 1)
     k_sell_cfg(const V *__restrict__ val, DevSell A, const X *__restrict__ x, Epi epi, int *err) {
+  epi_setup(epi, 0);
   using Acc = typename acc_of<V>::type;
   // gathered x kept as fp16 where value and x are both fp16 (the mixed-precision FMA takes them)
   using XB = typename std::conditional<std::is_same<V, __half>::value && std::is_same<X, __half>::value, __half,
@@ -428,6 +429,7 @@ static_assert(sell64_smem_bytes<__half>() <= 227 * 1024 && sell64_smem_bytes<flo
 template <typename V, typename X, typename Epi, int WARPS, int STAGES, int KC>
 __global__ void __launch_bounds__(WARPS * 32, 1)
     k_sell64(const V *__restrict__ val, DevSell A, const X *__restrict__ x, Epi epi, int *err) {
+  epi_setup(epi, 0);
   using Acc = typename acc_of<V>::type;
   static_assert(KC == kAllAlignedChunk, "64-row aligned layout is built for kAllAlignedChunk columns");
   constexpr uint32_t VB = KC * 64 * sizeof(V), BB = KC * 4, SB = VB + BB;

@@ -837,8 +837,12 @@ template <int K> struct Engine {
           __half *cur = h0, *nxt = w.hout2;
           for (int k = 1; k < p.m4; k++) {
             const bool last = (k == p.m4 - 1);
-            F3R_TRY(launch_sell(C(), S.A.v16, Av, (const __half *)cur,
-                                EpiRichStep{hi, cur, M, w.rs, k, last ? out16 : nxt, last ? out_last : nullptr, isc}));
+            __half *hn = last ? out16 : nxt;
+            float *fo = last ? out_last : nullptr;
+            if (S.diag_unit)
+              F3R_TRY(launch_sell(C(), S.A.v16, Av, (const __half *)cur, EpiRichStepUnit{hi, cur, M, w.rs, k, hn, fo, isc}));
+            else
+              F3R_TRY(launch_sell(C(), S.A.v16, Av, (const __half *)cur, EpiRichStep{hi, cur, M, w.rs, k, hn, fo, isc}));
             std::swap(cur, nxt);
           }
         } else {
@@ -1818,6 +1822,7 @@ static Status make_solver(f3r_context *ctx, const f3r_csr *a, const f3r_params *
   F3R_TRY((sell_attr<double, double, EpiStore<double>>(cx)));
   F3R_TRY((sell_attr<double, double, EpiResidual<double, double>>(cx)));
   F3R_TRY((sell_attr<__half, __half, EpiRichStep>(cx)));
+  F3R_TRY((sell_attr<__half, __half, EpiRichStepUnit>(cx)));
   F3R_TRY((sell_attr<__half, __half, EpiRichResPre>(cx)));
   F3R_TRY((sell_attr<__half, __half, EpiResidual<__half, __half>>(cx)));
   F3R_TRY((sell_attr<__half, __half, EpiStore<__half>>(cx)));
