@@ -52,6 +52,31 @@ def test_params_default_match_drivers():
     assert C.sizeof(p) == 144
 
 
+def test_struct_layouts_match_header(tmp_path):
+    """every ctypes mirror has the C header's field offsets and size: a small
+    C program built with the host compiler against include/f3r_b200.h prints
+    offsetof / sizeof for each field the binding declares"""
+    structs = {"f3r_csr": _capi.CSR, "f3r_params": _capi.Params, "f3r_result": _capi.Result,
+               "f3r_sell_info": _capi.SellInfo, "f3r_tune_entry": _capi.TuneEntry}
+    lines = ["#include <stddef.h>", "#include <stdio.h>", '#include "f3r_b200.h"', "int main(void) {"]
+    expect = []
+    for cname, py in structs.items():
+        lines.append(f'  printf("%zu\\n", sizeof({cname}));')
+        expect.append(C.sizeof(py))
+        for fname, _ in py._fields_:
+            lines.append(f'  printf("%zu\\n", offsetof({cname}, {fname}));')
+            expect.append(getattr(py, fname).offset)
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c11", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = [int(v) for v in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()]
+    assert got == expect
+    # the newest field keeps its documented default
+    assert F.Params().diag_load == 0
+
+
 def test_errors_are_status_codes():
     # non-monotone rptr
     with pytest.raises(F.F3RError) as e:
