@@ -789,7 +789,9 @@ __global__ void __launch_bounds__(WARPS * 32, K == 1 ? 8 : 1) k_multidot_chunked
 template <int MAXV, int WARPS, int K>
 __global__ void __launch_bounds__(WARPS * 32, K == 1 ? 8 : 1) k_multidot_f32K(const float *__restrict__ w, Cols<float> V, int nv,
                                                               int64_t n, GridRed gr, float *hcol, int64_t hstride) {
-  constexpr int CV = (MAXV * K > 32) ? (32 / K > 0 ? 32 / K : 1) : MAXV;  // basis vectors per pass
+  // basis vectors per pass: single columns take at most 4 (more float4 loads in flight than 32
+  // registers hold spill), K columns up to 32 values
+  constexpr int CV = (MAXV * K > 32) ? (32 / K > 0 ? 32 / K : 1) : (K == 1 && MAXV > 4) ? 4 : MAXV;
   constexpr int NQ = CV * K;
   __shared__ float sred[WARPS][NQ];
   float *part = static_cast<float *>(gr.partials);
