@@ -567,6 +567,7 @@ template <int K, bool MM = false> struct EpiRichStepK {
   }
   template <typename Acc> __device__ __forceinline__ void row(int64_t r, const Acc (&acc)[K]) const {
     float hi[K], ho[K], res[K];
+    __half hn[K];
     __half w[MM ? K : 1], z[MM ? K : 1];
     RowK<__half, K>::load(hin + r * K, hi);
     RowK<__half, K>::load(hout + r * K, ho);
@@ -576,14 +577,14 @@ template <int K, bool MM = false> struct EpiRichStepK {
     for (int c = 0; c < K; c++) {
       const __half hr = f2h(hi[c] - (float)acc[c]);
       const __half t2 = __hmul(z[MM ? c : 0], __hmul(w[MM ? c : 0], hr));
-      res[c] = h2f(f2h(__fmaf_rn(ome[c], h2f(t2), ho[c])));
+      hn[c] = f2h(__fmaf_rn(ome[c], h2f(t2), ho[c]));  // rounded to fp16 once, stored as it is
     }
     if (out) {
 #pragma unroll
-      for (int c = 0; c < K; c++) res[c] *= isc;
+      for (int c = 0; c < K; c++) res[c] = h2f(hn[c]) * isc;
       RowK<float, K>::store(out + r * K, res);
     } else {
-      RowK<__half, K>::store(hnext + r * K, res);
+      RowK<__half, K>::store(hnext + r * K, hn);
     }
   }
 };

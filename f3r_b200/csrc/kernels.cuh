@@ -576,9 +576,11 @@ template <bool PREFETCH = true, bool UNIT = false> struct EpiRichStepT {
     const __half hr = f2h(h2f(__low2half(p.io)) - (float)acc);
     __half t2 = hr;
     if constexpr (!UNIT) t2 = __hmul(p.z, __hmul(p.w, hr));
-    const float hn = h2f(f2h(__fmaf_rn(ome, h2f(t2), h2f(__high2half(p.io)))));
-    if (out) out[r] = hn * isc;
-    else hnext[r] = f2h(hn);
+    // hnew is rounded to fp16 once; the fp16 store takes it as it is (widening
+    // and rounding it again would give the same bits)
+    const __half hn = f2h(__fmaf_rn(ome, h2f(t2), h2f(__high2half(p.io))));
+    if (out) out[r] = h2f(hn) * isc;
+    else hnext[r] = hn;
   }
   template <int W> __device__ __forceinline__ void finish(Red (&)[1]) const {}
 };
